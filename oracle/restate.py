@@ -1,0 +1,503 @@
+"""CPU restatement of the reference solve path's per-node kernels (oracle; test
+infrastructure only - never imported by the product library or timed as it).
+
+Each function restates one routine of the reference core semiconductor_3d.c in
+vectorised numpy and cites the lines it follows.  The parity tests pin these
+restatements against golden vectors dumped from the reference itself
+(tests/golden/make_golden.py, oracle/harness.c) and then use them as the checker for
+the CUDA kernels on seeded inputs.
+
+A device is a dict of numpy arrays (the golden fixture layout):
+  dims (Nx,Ny,Nz); xs, ys, zs; kind, con, gate (int, per node); mat (int per node);
+  Nd, Na, Nf, bgn (per node); phi, phin, phip, n, p, mun, mup (state); fmu (6,N);
+  mats: (n_mats, F) records in the field order MAT_FIELDS; models; caxis; rob_k,
+  rob_A, rob_c; con_V, con_tox, con_qox, con_pm (per contact); Cref; ref_mat.
+Node index k = i + Nx*(j + Ny*l) (semiconductor_3d.c:114).
+"""
+import numpy as np
+
+Q = 1.602176634e-19            # semiconductor_3d.c:95-99
+KB = 1.380649e-23
+EPS0 = 8.8541878128e-12
+EPS_OX = 3.9 * EPS0
+LN_MIN, LN_MAX, NFLOOR = -230.0, 150.0, 1e-100   # semiconductor_3d.c:108-110
+K_SEMI, K_INS, K_METAL = 0, 1, 2
+PH_NONE = -1e300
+
+# field order of the material records written by oracle/harness.c (hx_mat)
+MAT_FIELDS = ["T", "VT", "Eg", "chi", "eps_r", "Nc", "Nv", "ni",
+              "mu_n_max", "mu_p_max", "mu_n_min", "mu_p_min", "Nref_n", "Nref_p", "alpha_n", "alpha_p",
+              "mt_min", "mt_max_n", "mt_max_p", "mt_Nref", "mt_alpha", "mas_on",
+              "vsat_n", "vsat_p", "beta_n", "beta_p", "tau_n0", "tau_p0", "Cn", "Cp", "Brad", "tau_Nref",
+              "bgn_E", "bgn_N", "bgn_C", "lnc", "lnv", "insulator", "ani_n", "ani_p"]
+MF = {n: i for i, n in enumerate(MAT_FIELDS)}
+
+
+def matp(dev, name):
+    """Per-node value of material field `name`."""
+    return dev["mats"][dev["mat"], MF[name]]
+
+
+# ------------------------------------------------------------------ scalar physics
+def bernoulli(x):
+    """B(x) = x/(e^x-1): series below 1e-6, limits beyond +-700 (semiconductor_3d.c:670-675)."""
+    x = np.asarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    small = np.abs(x) < 1e-6
+    big = x > 700.0
+    neg = x < -700.0
+    mid = ~(small | big | neg)
+    out[small] = 1.0 - x[small] / 2.0 + x[small] ** 2 / 12.0
+    out[big] = 0.0
+    out[neg] = -x[neg]
+    with np.errstate(over="ignore", divide="ignore", invalid="ignore"):
+        out[mid] = x[mid] / np.expm1(x[mid])
+    return out
+
+
+def clampe(e):
+    """semiconductor_3d.c:677"""
+    return np.clip(e, LN_MIN, LN_MAX)
+
+
+def lncK(dev):
+    """ln of the electron effective density incl. band-gap narrowing (semiconductor_3d.c:736)."""
+    return matp(dev, "lnc") + dev["bgn"]
+
+
+def lnvK(dev):
+    """semiconductor_3d.c:737"""
+    return matp(dev, "lnv") + dev["bgn"]
+
+
+def niK(dev):
+    """semiconductor_3d.c:738 (no quantum correction in scope)"""
+    return matp(dev, "ni") * np.exp(dev["bgn"])
+
+
+def nK(dev, psi, qn):
+    """semiconductor_3d.c:739-741"""
+    with np.errstate(over="ignore", invalid="ignore"):
+        return np.exp(clampe(lncK(dev) + (psi - qn) / matp(dev, "VT")))
+
+
+def pK(dev, psi, qp):
+    """semiconductor_3d.c:742-744"""
+    with np.errstate(over="ignore", invalid="ignore"):
+        return np.exp(clampe(lnvK(dev) + (qp - psi) / matp(dev, "VT")))
+
+
+def tauf(dev):
+    """SRH lifetime doping factor (semiconductor_3d.c:787-791)."""
+    tn = matp(dev, "tau_Nref")
+    f = 1.0 / (1.0 + (dev["Nd"] + dev["Na"]) / np.where(tn > 0, tn, 1.0))
+    on = (dev["models"] & 2) != 0
+    return np.where(on & (tn > 0), f, 1.0)
+
+
+def recomb(dev, n, p):
+    """SRH + Auger + radiative with derivatives (semiconductor_3d.c:686-697)."""
+    ni = niK(dev)
+    tf = tauf(dev)
+    tp0, tn0 = matp(dev, "tau_p0"), matp(dev, "tau_n0")
+    Cn, Cp, Br = matp(dev, "Cn"), matp(dev, "Cp"), matp(dev, "Brad")
+    ni2 = ni * ni
+    np_ = n * p - ni2
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        den = tf * (tp0 * (n + ni) + tn0 * (p + ni)) + 1e-300
+        Rs = np_ / den
+        dsn = (p * den - np_ * tf * tp0) / (den * den)
+        dsp = (n * den - np_ * tf * tn0) / (den * den)
+        Au = Cn * n + Cp * p
+        R = Rs + Au * np_ + Br * np_
+        dRn = dsn + Cn * np_ + Au * p + Br * p
+        dRp = dsp + Cp * np_ + Au * n + Br * n
+    return R, dRn, dRp
+
+
+def mob_hf(mu0, E, vsat, beta):
+    """Caughey-Thomas saturation (semiconductor_3d.c:664-668)."""
+    r = mu0 * np.abs(E) / vsat
+    with np.errstate(over="ignore", divide="ignore", invalid="ignore"):
+        s = mu0 / np.power(1.0 + np.power(r, beta), 1.0 / beta)
+    return np.where(r < 1e-12, mu0, s)
+
+
+def heat_field(dq, dps, h):
+    """Harmonic-mean driving field (semiconductor_3d.c:2882-2886)."""
+    a, b = np.abs(dq), np.abs(dps)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        F = 2.0 * a * b / ((a + b) * h)
+    return np.where(dq * dps <= 0.0, 0.0, F)
+
+
+# ------------------------------------------------------------------ geometry
+def fv_len(c):
+    """Finite-volume lengths with half cells on the faces (semiconductor_3d.c:700-705)."""
+    c = np.asarray(c, float)
+    N = len(c)
+    L = np.empty(N)
+    if N < 2:
+        return np.ones(N)
+    L[0] = 0.5 * (c[1] - c[0])
+    L[-1] = 0.5 * (c[-1] - c[-2])
+    L[1:-1] = 0.5 * (c[2:] - c[:-2])
+    return L
+
+
+class Grid:
+    """Neighbour bookkeeping of nbr() (semiconductor_3d.c:709-719) as per-direction
+    index / validity / spacing / area arrays over the flattened nodes."""
+
+    def __init__(self, dev):
+        Nx, Ny, Nz = (int(v) for v in dev["dims"])
+        self.Nx, self.Ny, self.Nz = Nx, Ny, Nz
+        self.N = Nx * Ny * Nz
+        xs, ys, zs = (np.asarray(dev[a], float) for a in ("xs", "ys", "zs"))
+        Lx, Ly, Lz = fv_len(xs), fv_len(ys), fv_len(zs)
+        l, j, i = np.meshgrid(np.arange(Nz), np.arange(Ny), np.arange(Nx), indexing="ij")
+        i, j, l = i.ravel(), j.ravel(), l.ravel()
+        self.i, self.j, self.l = i, j, l
+        k = np.arange(self.N)
+        self.vol = Lx[i] * Ly[j] * Lz[l]
+        self.valid, self.kb, self.h, self.ar = [], [], [], []
+        for d in range(6):
+            ax, up = d // 2, d % 2
+            idx = (i, j, l)[ax]
+            nmax = (Nx, Ny, Nz)[ax]
+            st = (1, Nx, Nx * Ny)[ax]
+            c = (xs, ys, zs)[ax]
+            if up:
+                v = idx < nmax - 1
+                kb = np.where(v, k + st, k)
+                h = np.where(v, c[np.minimum(idx + 1, nmax - 1)] - c[idx], 1.0)
+            else:
+                v = idx > 0
+                kb = np.where(v, k - st, k)
+                h = np.where(v, c[idx] - c[np.maximum(idx - 1, 0)], 1.0)
+            ar = (Ly[j] * Lz[l], Lx[i] * Lz[l], Lx[i] * Ly[j])[ax]
+            self.valid.append(v)
+            self.kb.append(kb)
+            self.h.append(h)
+            self.ar.append(ar)
+
+
+# ------------------------------------------------------------------ Poisson
+def poisson_eval(dev, phi, g=None):
+    """F, 7-point Jacobian (c,xm,xp,ym,yp,zm,zp), sc and ||F/sc|| (semiconductor_3d.c:2732-2789)."""
+    g = g or Grid(dev)
+    N = g.N
+    kind, con = dev["kind"], dev["con"]
+    isdir = con != 0
+    eps = matp(dev, "eps_r") * EPS0
+    F = np.zeros(N)
+    dg = np.zeros(N)
+    off = np.zeros((6, N))
+    for d in range(6):
+        v, kb = g.valid[d], g.kb[d]
+        ek, eb = eps, eps[kb]
+        cf = np.where(v, (2.0 * ek * eb / (ek + eb)) * g.ar[d] / g.h[d], 0.0)
+        F += cf * (phi[kb] - phi)
+        dg += cf
+        off[d] = np.where(v & ~isdir[kb], -cf, 0.0)
+    semi = kind == K_SEMI
+    n = nK(dev, phi, dev["phin"])
+    p = pK(dev, phi, dev["phip"])
+    VT = matp(dev, "VT")
+    F += np.where(semi, g.vol * Q * (p - n + dev["Nd"] - dev["Na"] + dev["Nf"]), g.vol * Q * dev["Nf"])
+    dg += np.where(semi, g.vol * Q * (n + p) / VT, 0.0)
+    A = np.vstack([dg[None, :], off])
+    sc = dg.copy()
+    F[isdir] = 0.0
+    A[:, isdir] = 0.0
+    A[0, isdir] = 1.0
+    sc[isdir] = 1.0
+    for r in range(len(dev["rob_k"])):
+        k, c = int(dev["rob_k"][r]), int(dev["rob_c"][r])
+        tox = dev["con_tox"][c] if dev["con_tox"][c] > 0 else 10e-9
+        Cox = EPS_OX / tox
+        pm = dev["con_pm"][c] if dev["con_pm"][c] > 0 else dev["Cref"]
+        VG = dev["con_V"][c] + dev["Cref"] - pm
+        F[k] += dev["rob_A"][r] * (Cox * (VG - phi[k]) + dev["con_qox"][c])
+        A[0, k] += Cox * dev["rob_A"][r]
+        sc[k] = A[0, k]
+    return F, A, sc, float(np.sqrt(np.sum((F / sc) ** 2)))
+
+
+# ------------------------------------------------------------------ mobility
+def upd_mob(dev, g=None):
+    """Face mobilities fmu[6][N] from node mobility and the potentials
+    (semiconductor_3d.c:2962-3006; Lombardi/Coulomb branches out of scope)."""
+    g = g or Grid(dev)
+    kind = dev["kind"]
+    semi = kind == K_SEMI
+    fmu = np.zeros((6, g.N))
+    sat = (dev["models"] & 4) != 0
+    for ax in range(3):
+        d = 2 * ax + 1
+        v, kb, h = g.valid[d], g.kb[d], g.h[d]
+        ok = semi & v & semi[kb]
+        mn = 0.5 * (dev["mun"] + dev["mun"][kb])
+        mp = 0.5 * (dev["mup"] + dev["mup"][kb])
+        if ax == dev["caxis"]:
+            an, ap = matp(dev, "ani_n"), matp(dev, "ani_p")
+            mn = np.where(an > 0, mn * an, mn)
+            mp = np.where(ap > 0, mp * ap, mp)
+        if sat:
+            dps = dev["phi"][kb] - dev["phi"]
+            Fn = heat_field(dev["phin"][kb] - dev["phin"], dps, h)
+            Fp = heat_field(dev["phip"][kb] - dev["phip"], dps, h)
+            mn = mob_hf(mn, Fn, matp(dev, "vsat_n"), matp(dev, "beta_n"))
+            mp = mob_hf(mp, Fp, matp(dev, "vsat_p"), matp(dev, "beta_p"))
+        fmu[ax] = np.where(ok, mn, 0.0)
+        fmu[3 + ax] = np.where(ok, mp, 0.0)
+    return fmu
+
+
+# ------------------------------------------------------------------ continuity
+def car_fix(dev):
+    """Contact nodes keep fixed carrier densities (semiconductor_3d.c:796-799; no
+    thermionic-emission contacts in scope)."""
+    return dev["con"] != 0
+
+
+def cont_assemble(dev, hole, g=None):
+    """Scaled SG system for u = c/s: A (7,N), rhs, sc, dsc (semiconductor_3d.c:3067-3106)."""
+    g = g or Grid(dev)
+    N = g.N
+    kind = dev["kind"]
+    semi = kind == K_SEMI
+    fix = car_fix(dev)
+    car = dev["p"] if hole else dev["n"]
+    VT = matp(dev, "VT")
+    lc = lnvK(dev) if hole else lncK(dev)
+    sk = np.maximum(car, NFLOOR)
+    dg = np.zeros(N)
+    b = np.zeros(N)
+    off = np.zeros((6, N))
+    fmu = dev["fmu"]
+    for d in range(6):
+        v, kb, h, ar = g.valid[d], g.kb[d], g.h[d], g.ar[d]
+        ok = v & semi[kb]
+        dl = lc[kb] - lc
+        D = (dev["phi"][kb] - dev["phi"]) / VT + (-dl if hole else dl)
+        kl = np.minimum(np.arange(N), kb)
+        gg = ar * fmu[(3 if hole else 0) + d // 2][kl] * VT / h
+        self_ = gg * (bernoulli(D) if hole else bernoulli(-D))
+        nb = gg * (bernoulli(-D) if hole else bernoulli(D))
+        dg += np.where(ok, self_, 0.0)
+        b += np.where(ok & fix[kb], nb * car[kb], 0.0)
+        off[d] = np.where(ok & ~fix[kb], -nb * np.maximum(car[kb], NFLOOR), 0.0)
+    R, dRn, dRp = recomb(dev, dev["n"], dev["p"])
+    dR = np.maximum(dRp if hole else dRn, 0.0)
+    dg += g.vol * dR
+    b += g.vol * (dR * car - R)
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        w = 1.0 / (dg * sk)
+    A = np.vstack([np.ones((1, N)), off * w])
+    rhs = b * w
+    sc = sk.copy()
+    dsc = dg * sk
+    ident = ~semi | fix
+    A[:, ident] = 0.0
+    A[0, ident] = 1.0
+    rhs[ident] = np.where(semi[ident], 1.0, 0.0)
+    sc[ident] = np.where(semi[ident], car[ident], 0.0)
+    dsc[ident] = 0.0
+    return A, rhs, sc, dsc
+
+
+def cont_update(dev, hole, sol, sc, lo, hi):
+    """u -> carrier and quasi-Fermi potential, weighted max |dq| (semiconductor_3d.c:3112-3146).
+    Returns (qf_new, car_new, dq, dmax); other carrier taken from dev."""
+    semi = dev["kind"] == K_SEMI
+    act = semi & ~car_fix(dev)
+    u = np.where(~(sol > 1e-30), 1e-30, np.minimum(sol, 1e30))
+    c = sc * u
+    VT = matp(dev, "VT")
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if hole:
+            qn = dev["phi"] + VT * (np.log(c) - lnvK(dev))
+        else:
+            qn = dev["phi"] - VT * (np.log(c) - lncK(dev))
+    qn = np.clip(qn, lo, hi)
+    qf_old = dev["phip"] if hole else dev["phin"]
+    ch = qn - qf_old
+    cn = pK(dev, dev["phi"], qn) if hole else nK(dev, dev["phi"], qn)
+    qf = np.where(act, qn, qf_old)
+    car = np.where(act, cn, dev["p"] if hole else dev["n"])
+    dq = np.where(act, ch, 0.0)
+    nn = dev["n"] if hole else car
+    pp = car if hole else dev["p"]
+    scale = nn + pp + np.abs(dev["Nd"] - dev["Na"])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(scale > 0, cn / scale, 0.0)
+    wgt = np.where(r >= 1e-3, 1.0, r * 1e3)
+    a = np.where(act & (r > 1e-6), wgt * np.abs(ch), 0.0)
+    return qf, car, dq, float(a.max() if a.size else 0.0)
+
+
+def terminal_currents(dev, ncon, g=None):
+    """Contact fluxes I, scales S and electron parts In (semiconductor_3d.c:2843-2854,
+    3598-3623)."""
+    g = g or Grid(dev)
+    N = g.N
+    kind, con = dev["kind"], dev["con"]
+    semi = kind == K_SEMI
+    I = np.zeros(ncon)
+    S = np.zeros(ncon)
+    In = np.zeros(ncon)
+    VT = matp(dev, "VT")
+    lc, lv = lncK(dev), lnvK(dev)
+    for d in range(6):
+        v, kb, h, ar = g.valid[d], g.kb[d], g.h[d], g.ar[d]
+        ok = (con != 0) & semi & v & semi[kb] & (con[kb] != con)
+        if not ok.any():
+            continue
+        k = np.nonzero(ok)[0]
+        b = kb[k]
+        dps = (dev["phi"][b] - dev["phi"][k]) / VT[k]
+        Dn = dps + (lc[b] - lc[k])
+        Dp = dps - (lv[b] - lv[k])
+        kl = np.minimum(k, b)
+        gn = Q * ar[k] * dev["fmu"][d // 2][kl] * VT[k] / h[k]
+        gp = Q * ar[k] * dev["fmu"][3 + d // 2][kl] * VT[k] / h[k]
+        a1 = gn * dev["n"][b] * bernoulli(Dn)
+        a2 = gn * dev["n"][k] * bernoulli(-Dn)
+        b1 = gp * dev["p"][k] * bernoulli(Dp)
+        b2 = gp * dev["p"][b] * bernoulli(-Dp)
+        c = con[k] - 1
+        np.add.at(I, c, (a1 - a2) + (b1 - b2))
+        np.add.at(S, c, (a1 + a2) + (b1 + b2))
+        np.add.at(In, c, a1 - a2)
+    return I, S, In
+
+
+# ------------------------------------------------------------------ linear algebra
+def matvec(A, dims, x):
+    """7-point stencil product (semiconductor_3d.c:1975-1993)."""
+    Nx, Ny, Nz = dims
+    X = x.reshape(Nz, Ny, Nx)
+    Y = (A[0] * x).reshape(Nz, Ny, Nx).copy()
+    C = [a.reshape(Nz, Ny, Nx) for a in A]
+    Y[:, :, 1:] += C[1][:, :, 1:] * X[:, :, :-1]
+    Y[:, :, :-1] += C[2][:, :, :-1] * X[:, :, 1:]
+    Y[:, 1:, :] += C[3][:, 1:, :] * X[:, :-1, :]
+    Y[:, :-1, :] += C[4][:, :-1, :] * X[:, 1:, :]
+    Y[1:, :, :] += C[5][1:, :, :] * X[:-1, :, :]
+    Y[:-1, :, :] += C[6][:-1, :, :] * X[1:, :, :]
+    return Y.ravel()
+
+
+def bicg_floor(A, dims, b, x):
+    """sqrt(sum_a (sum_b |A_ab x_b| + |b_a|)^2) (semiconductor_3d.c:2244-2268)."""
+    absA = [np.abs(a) for a in A]
+    s = matvec(absA, dims, np.abs(x)) + np.abs(b)
+    return float(np.sqrt(np.sum(s * s)))
+
+
+def mg_dims(dims):
+    """Level shapes and coarsening flags of the 2x2x2 aggregation (semiconductor_3d.c:1894-1921)."""
+    levs = [(tuple(int(v) for v in dims), None)]
+    while len(levs) < 24:
+        (Nx, Ny, Nz), _ = levs[-1]
+        if Nx * Ny * Nz <= 64:
+            break
+        cx, cy, cz = Nx > 2, Ny > 2, Nz > 2
+        if not (cx or cy or cz):
+            break
+        levs[-1] = ((Nx, Ny, Nz), (cx, cy, cz))
+        levs.append((((Nx + 1) // 2 if cx else Nx, (Ny + 1) // 2 if cy else Ny,
+                      (Nz + 1) // 2 if cz else Nz), None))
+    return levs
+
+
+def _parent(dims, cflags):
+    """Coarse index of every fine node (2x2x2 aggregates)."""
+    Nx, Ny, Nz = dims
+    cx, cy, cz = cflags
+    Cx = (Nx + 1) // 2 if cx else Nx
+    Cy = (Ny + 1) // 2 if cy else Ny
+    l, j, i = np.meshgrid(np.arange(Nz), np.arange(Ny), np.arange(Nx), indexing="ij")
+    I = i >> 1 if cx else i
+    J = j >> 1 if cy else j
+    L = l >> 1 if cz else l
+    return (I + Cx * (J + Cy * L)).ravel()
+
+
+def mg_weights(levs, ph0):
+    """Slotboom prolongation weights (semiconductor_3d.c:2092-2117). ph0: level-0
+    reference potential per node in units of VT (PH_NONE where none), or None for
+    plain aggregation.  Returns the list of pw per fine level."""
+    pws = []
+    ph = ph0
+    for L in range(len(levs) - 1):
+        dims, cf = levs[L]
+        N = int(np.prod(dims))
+        if ph0 is None:
+            pws.append(np.ones(N))
+            continue
+        par = _parent(dims, cf)
+        Nc = int(np.prod(levs[L + 1][0]))
+        mx = np.full(Nc, PH_NONE)
+        np.maximum.at(mx, par, ph)
+        e = np.where(ph <= 0.5 * PH_NONE, -800.0, ph - mx[par])
+        pws.append(np.where(e < -700.0, 0.0, np.exp(np.maximum(e, -700.0))))
+        ph = mx
+    return pws
+
+
+def galerkin(A, dims, cf, pw, w=None):
+    """Coarse 7-point operator P^T W A P (semiconductor_3d.c:2003-2027)."""
+    Nx, Ny, Nz = dims
+    N = Nx * Ny * Nz
+    par = _parent(dims, cf)
+    cx, cy, cz = cf
+    Cdims = ((Nx + 1) // 2 if cx else Nx, (Ny + 1) // 2 if cy else Ny, (Nz + 1) // 2 if cz else Nz)
+    Nc = int(np.prod(Cdims))
+    wk = np.ones(N) if w is None else w
+    l, j, i = np.meshgrid(np.arange(Nz), np.arange(Ny), np.arange(Nx), indexing="ij")
+    i, j, l = i.ravel(), j.ravel(), l.ravel()
+    k = np.arange(N)
+    Ac = np.zeros((7, Nc))
+    np.add.at(Ac[0], par, wk * A[0] * pw)
+    strides = (1, Nx, Nx * Ny)
+    idxs = (i, j, l)
+    ns = (Nx, Ny, Nz)
+    for d in range(6):
+        ax, up = d // 2, d % 2
+        v = idxs[ax] < ns[ax] - 1 if up else idxs[ax] > 0
+        kb = np.where(v, k + strides[ax] if up else k - strides[ax], k)
+        a = np.where(v, wk * A[1 + d] * pw[kb], 0.0)
+        same = par[kb] == par
+        np.add.at(Ac[0], par, np.where(v & same, a, 0.0))
+        np.add.at(Ac[1 + d], par, np.where(v & ~same, a, 0.0))
+    zero = np.all(Ac == 0.0, axis=0)
+    Ac[0, zero] = 1.0
+    return Ac, Cdims
+
+
+def restrict(dims, cf, r, w=None):
+    """Aggregate sums (semiconductor_3d.c:2028-2037)."""
+    par = _parent(dims, cf)
+    Nx, Ny, Nz = dims
+    cx, cy, cz = cf
+    Nc = ((Nx + 1) // 2 if cx else Nx) * ((Ny + 1) // 2 if cy else Ny) * ((Nz + 1) // 2 if cz else Nz)
+    out = np.zeros(Nc)
+    np.add.at(out, par, r if w is None else w * r)
+    return out
+
+
+def prolong_add(dims, cf, pw, xc, x, alpha=1.0):
+    """x += alpha pw P xc (semiconductor_3d.c:2038-2048)."""
+    return x + alpha * pw * xc[_parent(dims, cf)]
+
+
+def ph0(dev, qsign):
+    """Level-0 reference potential / VT of the Slotboom weights (semiconductor_3d.c:2085-2090)."""
+    if qsign == 0:
+        return None
+    VT = dev["mats"][dev["ref_mat"], MF["VT"]]
+    val = dev["phin"] / VT if qsign > 0 else -dev["phip"] / VT
+    none = (dev["kind"] != K_SEMI) | car_fix(dev)
+    return np.where(none, PH_NONE, val)

@@ -1,0 +1,219 @@
+"""Synthetic device builders for the benchmark and parity workloads.
+
+Every builder drives a library through the ``api3_*`` ABI only (the calls main.py's
+``setup_device`` makes, main.py:3286-3361), so the same builder sets up the B200 solver
+library and the reference core identically.  Sizes, doping and biases follow the
+workload definitions:
+
+* ``pn_diode``   Si abrupt pn diode, 1x1x1 um, uniform tensor mesh (40^3 by default),
+                 N_A 1e17 cm^-3 for x < 0.5 um, N_D 1e17 cm^-3 for x >= 0.5 um, 300 K,
+                 constant mobility 1350 / 480 cm^2/Vs, tau_n = tau_p = 1e-7 s, ohmic
+                 contacts on x = 0 (anode) and x = L (cathode), models = 0.
+* ``nmosfet``    n-MOSFET on a 120x80x60 mesh: p-body 1e17 cm^-3, Gaussian n+ source /
+                 drain (peak 1e20 cm^-3, sigma 20 nm), 2 nm SiO2 gate oxide as the oxide
+                 Robin condition of a face gate (tox = 2 nm, eps_r 3.9), velocity
+                 saturation (models = 4), Id-Vg sweep 0..1.2 V in 0.05 V steps at
+                 Vd = 0.05 V and 1.0 V.
+* ``diode_variant``  the batched pn-diode family: node counts between 32^3 and 72^3,
+                 doping log-uniform in [1e15, 1e18] cm^-3, junction depth in
+                 [0.2, 0.8] um, from a recorded seed.
+
+Concentrations are given in cm^-3 and converted to m^-3 at the ABI, as main.py does.
+"""
+import ctypes
+import numpy as np
+
+from .abi import dptr, iptr
+
+SI, SIO2 = 0, 8                     # material ids of semiconductor_3d.c:430, :560
+GUI_SOLVER = (2000, 1000, 500, 1e-8, 1e-6, 1.0, 1.0)   # main.py:3286 default tuple
+
+
+class Workload:
+    """What a builder set up: mesh shape, contact ids and the bias sweep(s)."""
+
+    def __init__(self, name, shape, contacts, sweeps, info=None):
+        self.name = name
+        self.shape = tuple(shape)                # (Nx, Ny, Nz)
+        self.contacts = dict(contacts)           # label -> contact id
+        self.sweeps = sweeps                     # list of dicts: {"fixed": {label: V}, "swept": label, "V": array}
+        self.info = dict(info or {})
+
+    @property
+    def N(self):
+        return int(np.prod(self.shape))
+
+    @property
+    def points(self):
+        return int(sum(len(s["V"]) for s in self.sweeps))
+
+
+def _grid(lib, xs, ys, zs):
+    xs, ys, zs = (np.ascontiguousarray(a, dtype=np.float64) for a in (xs, ys, zs))
+    ok = lib.api3_set_grid_coords(len(xs), len(ys), len(zs), dptr(xs), dptr(ys), dptr(zs))
+    if not ok:
+        raise MemoryError("api3_set_grid_coords failed")
+    return xs, ys, zs
+
+
+def pn_diode(lib, n=(40, 40, 40), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj=0.5e-6,
+             mobility=(1350.0, 480.0), tau=1e-7, models=0, solver=GUI_SOLVER, vmax=0.6,
+             dv=0.05):
+    """Abrupt Si pn diode; the anode (x = 0, p side) is swept 0..vmax."""
+    lib.api3_init()
+    xs = np.linspace(0.0, L[0], n[0])
+    ys = np.linspace(0.0, L[1], n[1])
+    zs = np.linspace(0.0, L[2], n[2])
+    _grid(lib, xs, ys, zs)
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    si = lib.api3_add_material(SI, 300.0)
+    if mobility is not None:
+        if not lib.api3_set_mat_mobility(si, mobility[0] * 1e-4, mobility[1] * 1e-4):
+            raise RuntimeError("api3_set_mat_mobility failed")
+    if tau is not None:
+        lib.api3_set_mat_tau(si, tau, tau)
+    ij = int(np.searchsorted(xs, xj, side="left"))          # first node with x >= xj
+    lib.api3_set_region(0, 0, 0, ij - 1, n[1] - 1, n[2] - 1, si, 0.0, NA * 1e6)
+    lib.api3_set_region(ij, 0, 0, n[0] - 1, n[1] - 1, n[2] - 1, si, ND * 1e6, 0.0)
+    lib.api3_clear_contacts()
+    ca = lib.api3_add_contact_ex(0, 0, n[1] - 1, 0, n[2] - 1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cc = lib.api3_add_contact_ex(1, 0, n[1] - 1, 0, n[2] - 1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    npts = int(round(vmax / dv)) + 1
+    V = np.round(np.linspace(0.0, vmax, npts), 12)
+    return Workload("pn_diode", n, {"anode": ca, "cathode": cc},
+                    [{"fixed": {"cathode": 0.0}, "swept": "anode", "V": V}],
+                    {"NA_cm3": NA, "ND_cm3": ND, "xj_m": xj, "models": models, "L_m": L})
+
+
+def graded_axis(L, n, h0):
+    """n coordinates on [0, L] whose spacing grows geometrically from h0 at 0."""
+    if n < 3:
+        return np.linspace(0.0, L, n)
+    lo, hi = 1.0, 2.0
+    f = lambda g: h0 * (g ** (n - 1) - 1.0) / (g - 1.0) - L
+    while f(hi) < 0:
+        hi *= 2.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if f(mid) < 0:
+            lo = mid
+        else:
+            hi = mid
+    g = 0.5 * (lo + hi)
+    h = h0 * g ** np.arange(n - 1)
+    x = np.concatenate([[0.0], np.cumsum(h)])
+    x *= L / x[-1]
+    return x
+
+
+def _gauss_sd(xs, ys, x0, x1, peak, sigma):
+    """n+ implant: peak*exp(-y^2/2s^2) inside [x0, x1], Gaussian lateral falloff outside."""
+    X, Y = np.meshgrid(xs, ys, indexing="xy")          # (Ny, Nx)
+    d = np.where(X < x0, x0 - X, np.where(X > x1, X - x1, 0.0))
+    return peak * np.exp(-0.5 * (Y / sigma) ** 2) * np.exp(-0.5 * (d / sigma) ** 2)
+
+
+def nmosfet(lib, n=(120, 80, 60), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e17,
+            Nsd=1e20, sigma=20e-9, sd_len=100e-9, tox=2e-9, phi_m=4.6, models=4,
+            solver=GUI_SOLVER, vds=(0.05, 1.0), vg_max=1.2, dvg=0.05, h0=0.5e-9):
+    """n-MOSFET: x along the channel, y into the substrate (y = 0 the gate surface),
+    z across the width.  Contacts: source / drain ohmic on the surface over the n+
+    windows, gate as a Robin face gate (oxide tox) over the channel, body ohmic on
+    the back face."""
+    lib.api3_init()
+    xs = np.linspace(0.0, Lx, n[0])
+    ys = graded_axis(Ly, n[1], h0)
+    zs = np.linspace(0.0, Lz, n[2])
+    _grid(lib, xs, ys, zs)
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    si = lib.api3_add_material(SI, 300.0)
+    Nd2 = _gauss_sd(xs, ys, 0.0, sd_len, Nsd, sigma) + _gauss_sd(xs, ys, Lx - sd_len, Lx, Nsd, sigma)
+    Nd = np.ascontiguousarray(np.broadcast_to(Nd2[None, :, :], (n[2], n[1], n[0])).ravel() * 1e6)
+    Na = np.full(Nd.shape, Nbody * 1e6)
+    mat = np.full(Nd.shape, si, dtype=np.int32)
+    Nf = np.zeros(Nd.shape)
+    lib.api3_set_node_data(iptr(mat), dptr(Nd), dptr(Na), dptr(Nf))
+    lib.api3_clear_contacts()
+    iS1 = int(np.searchsorted(xs, 0.8 * sd_len, side="right")) - 1
+    iD0 = int(np.searchsorted(xs, Lx - 0.8 * sd_len, side="left"))
+    iG0 = int(np.searchsorted(xs, sd_len - 0.5 * sigma, side="left"))
+    iG1 = int(np.searchsorted(xs, Lx - sd_len + 0.5 * sigma, side="right")) - 1
+    nz = n[2] - 1
+    cs = lib.api3_add_contact_ex(2, 0, iS1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cd = lib.api3_add_contact_ex(2, iD0, n[0] - 1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cg = lib.api3_add_contact_ex(2, iG0, iG1, 0, nz, 0, 0, 2, 0.0, phi_m, tox, 0.0)
+    cb = lib.api3_add_contact_ex(3, 0, n[0] - 1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    npts = int(round(vg_max / dvg)) + 1
+    V = np.round(np.linspace(0.0, vg_max, npts), 12)
+    sweeps = [{"fixed": {"drain": vd, "source": 0.0, "body": 0.0}, "swept": "gate", "V": V} for vd in vds]
+    return Workload("nmosfet", n, {"source": cs, "drain": cd, "gate": cg, "body": cb}, sweeps,
+                    {"Lx_m": Lx, "Ly_m": Ly, "Lz_m": Lz, "tox_m": tox, "phi_m_eV": phi_m,
+                     "models": models, "Nbody_cm3": Nbody, "Nsd_cm3": Nsd, "sigma_m": sigma})
+
+
+def diode_variants(count=64, seed=20261203, nmin=32, nmax=72):
+    """Parameters of the batched pn-diode family (recorded seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nn = int(rng.integers(nmin ** 3, nmax ** 3 + 1))
+        a = int(round(nn ** (1.0 / 3.0)))
+        b = int(round((nn / a) ** 0.5))
+        c = max(2, int(round(nn / (a * b))))
+        NA = 10.0 ** rng.uniform(15.0, 18.0)
+        ND = 10.0 ** rng.uniform(15.0, 18.0)
+        xj = rng.uniform(0.2e-6, 0.8e-6)
+        out.append({"n": (a, b, c), "NA": NA, "ND": ND, "xj": xj})
+    return out
+
+
+def diode_variant(lib, v, vmax=0.7, dv=0.025, solver=GUI_SOLVER):
+    """One member of the batched family (constant mobility, tau 1e-7 s, models 0)."""
+    w = pn_diode(lib, n=v["n"], NA=v["NA"], ND=v["ND"], xj=v["xj"], solver=solver,
+                 vmax=vmax, dv=dv)
+    w.name = "diode_variant"
+    return w
+
+
+def bias_vector(w, sweep, Vswept):
+    """Contact voltages (by contact id) of one sweep point."""
+    V = {w.contacts[k]: v for k, v in sweep["fixed"].items()}
+    V[w.contacts[sweep["swept"]]] = float(Vswept)
+    return V
+
+
+def run_sweep(lib, w, sweep, timer=None, on_point=None):
+    """Sweep one contact the way main.run_sweep does (main.py:3638-3730): set the
+    voltages, api3_resolve per point.  Returns (V, I[npts, ncon], Iflr, conv)."""
+    nc = lib.api3_get_ncon()
+    V = np.asarray(sweep["V"], dtype=np.float64)
+    I = np.zeros((len(V), nc))
+    F = np.zeros((len(V), nc))
+    conv = np.zeros(len(V), dtype=bool)
+    for q, v in enumerate(V):
+        for cid, vv in bias_vector(w, sweep, v).items():
+            lib.api3_set_contact_V(cid, vv)
+        conv[q] = bool(lib.api3_resolve())
+        for c in range(nc):
+            I[q, c] = lib.api3_get_contact_I(c)
+            F[q, c] = lib.api3_get_contact_Ifloor(c)
+        if on_point is not None:
+            on_point(q, v)
+    return V, I, F, conv
+
+
+def start_sweep(lib, w, sweep):
+    """Equilibrium + ramp to the first point of a sweep (api3_solve at that bias)."""
+    for cid, vv in bias_vector(w, sweep, sweep["V"][0]).items():
+        lib.api3_set_contact_V(cid, vv)
+    return bool(lib.api3_solve())
+
+
+def field(lib, which, shape):
+    """api3_bulk_copy of one quantity as an (Nz, Ny, Nx) array."""
+    N = int(np.prod(shape))
+    buf = np.zeros(N)
+    lib.api3_bulk_copy(which, dptr(buf))
+    return buf.reshape(shape[2], shape[1], shape[0])
