@@ -1,0 +1,62 @@
+"""B200-native solve path of SemiSim 3D (kotmariusz/Semiconductor_devices_simulator).
+
+The product is the shared library lib/libsemisim_b200.so: the reference core's C ABI
+(the 89 ``api3_*`` entry points of semiconductor_3d.c) over CUDA kernels built for
+sm_100a.  main.py and validate.py of the reference load it unchanged through
+``SEMISIM_SO=<path to libsemisim_b200.so>``.
+
+``load()`` returns the library bound with the ABI's ctypes signatures (abi.API3) and the
+kernel-level test hooks; it raises if the library has not been built
+(``python -m semiconductor_devices_simulator_b200.build``).
+"""
+import ctypes
+import os
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libsemisim_b200.so")
+
+_I, _D, _LL = ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+_DP, _IP = ctypes.POINTER(_D), ctypes.POINTER(_I)
+HOOKS = {
+    "b200x_prepare": (_I, []),
+    "b200x_masks": (_I, [_IP, _IP, _IP, _DP]),
+    "b200x_set": (_I, [_I, _DP]),
+    "b200x_get": (_I, [_I, _DP]),
+    "b200x_vlo": (_D, []),
+    "b200x_vhi": (_D, []),
+    "b200x_apply_bc": (None, []),
+    "b200x_rebuild_np": (None, []),
+    "b200x_upd_mob": (None, []),
+    "b200x_clamp_qf": (None, []),
+    "b200x_poisson": (_D, [_DP, _DP, _DP, _DP]),
+    "b200x_cont_assemble": (None, [_I, _DP, _DP, _DP, _DP]),
+    "b200x_cont_update": (_D, [_I, _DP, _D, _D, _DP]),
+    "b200x_currents": (None, [_DP, _DP, _DP]),
+    "b200x_mg_setup": (_I, [_I]),
+    "b200x_mg_level": (_I, [_I, _IP, _DP, _DP]),
+    "b200x_bicgstab": (_I, [_I, _D, _D, _I, _DP, _DP, _DP, _DP]),
+    "b200x_pcg": (_I, [_I, _D, _DP]),
+    "b200x_float_fix": (_I, [_I, _DP]),
+    "b200x_device_bytes": (_LL, []),
+}
+# state arrays reachable through b200x_set / b200x_get
+ST_PHI, ST_PHIN, ST_PHIP, ST_N, ST_P, ST_MU0N, ST_MU0P, ST_SOL, ST_RHS, ST_SC, ST_DSC = range(11)
+ST_FMU = 16
+
+_lib = None
+
+
+def load(path=None):
+    """The solver library with every ABI signature declared (loaded once)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or os.environ.get("SEMISIM_B200_SO") or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"solver library not built: {p} (python -m semiconductor_devices_simulator_b200.build)")
+    lib = abi.bind(ctypes.CDLL(p), HOOKS)
+    if path is None:
+        _lib = lib
+    return lib

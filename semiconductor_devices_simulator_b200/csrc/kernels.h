@@ -1,0 +1,60 @@
+// Host-side launchers of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "semisim.h"
+
+namespace ss {
+
+// Launch context: the device parameter records of `ninst` instances (dP), the host copy
+// of instance 0's record (sizes), the stream.
+struct Ctx {
+    const DevP *dP = nullptr;
+    DevP h{};
+    int ninst = 1;
+    int maxN = 0;
+    cudaStream_t st = 0;
+    int grid_cap = 148 * 8;
+    int nodes_blocks() const;
+};
+
+// ---- physics (kernels_phys.cu)
+void launch_poisson(const Ctx &c, const double *phi, int build, double *F);   // res[R_PNORM]
+void launch_rebuild_np(const Ctx &c);
+void launch_upd_mob(const Ctx &c);
+void launch_cont_assemble(const Ctx &c, int hole);
+void launch_cont_update(const Ctx &c, int hole, double lo, double hi);          // res[R_DQ]
+void launch_apply_bc(const Ctx &c, int have_solution);
+void launch_init_eq(const Ctx &c);
+void launch_clamp_qf(const Ctx &c, double lo, double hi);
+void launch_currents(const Ctx &c);                                             // res[R_I..]
+void launch_predictor(const Ctx &c);
+void launch_dpsi(const Ctx &c);                                                 // res[R_DPSI]
+void launch_upd_J(const Ctx &c);
+void launch_mob_display(const Ctx &c);
+void launch_node_val(const Ctx &c, int which, double *out);
+void launch_face_J(const Ctx &c, int ax, int carrier, double *out);
+void launch_extrap(const Ctx &c, double r, int s1, int s2);     // history selectors 0 h1, 1 h2, 2 e2
+void launch_region_mark(const Ctx &c, int con1, int type, double dV, int *mark, int *changed);
+void launch_floating_blocks(const Ctx &c, int hole, int *nblocks);
+
+// ---- linear algebra (kernels_la.cu)
+void launch_absmax(const Ctx &c, const double *x, int slot);                   // res[slot]
+void launch_axpy(const Ctx &c, double *y, const double *x, double a, const double *z);  // y = x + a z
+void launch_fill(const Ctx &c, double *y, double v);
+void launch_copy(const Ctx &c, double *y, const double *x);
+
+template <class T> struct MGCtx;
+int mg_levels(int Nx, int Ny, int Nz, int dims[][6]);
+
+// multigrid set-up and the Krylov solvers (FP64 plain path)
+void mg_setup(const Ctx &c, int qsign);
+void pcg_solve(const Ctx &c, const double *b, double *x, int maxit, double rtol, int *its);
+void bicgstab_solve(const Ctx &c, const double *b, double *x, int maxit, double rtol, double atol, int *its,
+                    double *rn_out, double *r0_out, int mg_on);
+
+// ---- Anderson (kernels_aa.cu)
+void launch_aa_step(const Ctx &c, int M, int have, int pos, int nfill, double *const *x, double *const *g,
+                    int *nfill_out, int *ok);
+
+}  // namespace ss

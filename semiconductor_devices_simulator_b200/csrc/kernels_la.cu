@@ -1,0 +1,754 @@
+// Linear algebra of the solve path on 7-point stencils: level-0 SpMV fused with the
+// Krylov dot products, the geometric 2x2x2 aggregation multigrid (Slotboom-weighted
+// prolongation, Petrov-Galerkin coarse operators, red-black D-ILU smoother, dense
+// coarsest level) and device-resident PCG / BiCGSTAB.
+//
+// The reference smooths with a chunked natural-order D-ILU(0) (semiconductor_3d.c:
+// 1923-1972), a sequential recurrence.  Here the smoother is D-ILU(0) in red-black
+// order: red nodes (i+j+l even) have only black neighbours, so the forward sweep is a
+// pointwise divide on red and one stencil pass on black, the backward sweep one pass on
+// red.  It changes Krylov iteration counts, not the converged solution.
+//
+// Krylov scalars stay on the device (KrylovS): each reducing kernel's last block
+// computes the next coefficients and the stop test.  Every kernel of an iteration first
+// reads the instance's `active` word, so the host can queue several iterations and
+// read the status once.
+#include <cstdio>
+#include <vector>
+
+#include "device_common.cuh"
+#include "kernels.h"
+#include "solver_ctx.h"
+
+namespace ss {
+
+static inline dim3 grid_nodes(const Ctx &c) { return dim3(c.nodes_blocks(), c.ninst); }
+static inline dim3 grid_n(const Ctx &c, int n) {
+    int b = (n + TPB - 1) / TPB;
+    if (b > c.grid_cap) b = c.grid_cap;
+    if (b < 1) b = 1;
+    return dim3(b, c.ninst);
+}
+
+// vector selectors of the level-0 Krylov vectors
+__device__ __forceinline__ double *vsel(const DevP &P, int s) {
+    if (s < 8) return P.wk[s];
+    switch (s) {
+    case V_RHS: return P.rhs;
+    case V_SOL: return P.sol;
+    case V_F: return P.F;
+    case V_TR: return P.tr;
+    case V_PHI: return P.phi;
+    default: return P.dsc;
+    }
+}
+
+// y = A x on a level (7-point, boundary terms skipped as in semiconductor_3d.c:1975-1993)
+template <class T>
+__device__ __forceinline__ double stencil_apply(T *const *A, const T *x, int k, int i, int j, int l, int Nx, int Ny,
+                                                int Nz) {
+    const int NxNy = Nx * Ny;
+    double s = (double)A[0][k] * (double)x[k];
+    if (i > 0) s += (double)A[1][k] * (double)x[k - 1];
+    if (i < Nx - 1) s += (double)A[2][k] * (double)x[k + 1];
+    if (j > 0) s += (double)A[3][k] * (double)x[k - Nx];
+    if (j < Ny - 1) s += (double)A[4][k] * (double)x[k + Nx];
+    if (l > 0) s += (double)A[5][k] * (double)x[k - NxNy];
+    if (l < Nz - 1) s += (double)A[6][k] * (double)x[k + NxNy];
+    return s;
+}
+// sum over the off-diagonal couplings only
+template <class T>
+__device__ __forceinline__ double offdiag_apply(T *const *A, const T *x, int k, int i, int j, int l, int Nx, int Ny,
+                                                int Nz) {
+    const int NxNy = Nx * Ny;
+    double s = 0.0;
+    if (i > 0) s += (double)A[1][k] * (double)x[k - 1];
+    if (i < Nx - 1) s += (double)A[2][k] * (double)x[k + 1];
+    if (j > 0) s += (double)A[3][k] * (double)x[k - Nx];
+    if (j < Ny - 1) s += (double)A[4][k] * (double)x[k + Nx];
+    if (l > 0) s += (double)A[5][k] * (double)x[k - NxNy];
+    if (l < Nz - 1) s += (double)A[6][k] * (double)x[k + NxNy];
+    return s;
+}
+// sum of a_kj x_j / D_j over the neighbours (forward sweep of the black rows)
+template <class T>
+__device__ __forceinline__ double offdiag_apply_div(T *const *A, const T *x, const T *D, int k, int i, int j, int l,
+                                                    int Nx, int Ny, int Nz) {
+    const int NxNy = Nx * Ny;
+    double s = 0.0;
+    if (i > 0) s += (double)A[1][k] * (double)x[k - 1] / (double)D[k - 1];
+    if (i < Nx - 1) s += (double)A[2][k] * (double)x[k + 1] / (double)D[k + 1];
+    if (j > 0) s += (double)A[3][k] * (double)x[k - Nx] / (double)D[k - Nx];
+    if (j < Ny - 1) s += (double)A[4][k] * (double)x[k + Nx] / (double)D[k + Nx];
+    if (l > 0) s += (double)A[5][k] * (double)x[k - NxNy] / (double)D[k - NxNy];
+    if (l < Nz - 1) s += (double)A[6][k] * (double)x[k + NxNy] / (double)D[k + NxNy];
+    return s;
+}
+
+// ------------------------------------------------------------------ multigrid levels
+// level accessors: level 0 reads the instance's system arrays and the caller's vectors
+struct LevView {
+    double *A[7];
+    double *D, *x, *b, *r, *pw, *ph;
+    int Nx, Ny, Nz, N, cx, cy, cz, last;
+};
+__device__ __forceinline__ LevView levview(const DevP &P, int L, int bsel, int xsel) {
+    const LevelT<double> &lv = P.lev[L];
+    LevView v;
+#pragma unroll
+    for (int q = 0; q < 7; q++) v.A[q] = L == 0 ? P.A[q] : lv.A[q];
+    v.D = lv.D; v.r = lv.r; v.pw = lv.pw; v.ph = lv.ph;
+    v.x = L == 0 ? vsel(P, xsel) : lv.x;
+    v.b = L == 0 ? vsel(P, bsel) : lv.b;
+    v.Nx = lv.Nx; v.Ny = lv.Ny; v.Nz = lv.Nz; v.N = lv.N;
+    v.cx = lv.cx; v.cy = lv.cy; v.cz = lv.cz; v.last = lv.last;
+    return v;
+}
+__device__ __forceinline__ bool ks_running(const DevP &P) { return P.ks->active != 0; }
+
+// red-black D-ILU pivots: red D = a_kk; black D = a_kk - sum a_kr a_rk / a_rr, guarded
+// as the reference guards its ILU pivots (semiconductor_3d.c:1937-1938)
+__global__ void k_ilu_diag(const DevP *__restrict__ Ps, int L) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L > 0 && L >= P.nlev - 1) return;
+    const LevView v = levview(P, L, 0, 0);
+    SS_GRID_LOOP(k, v.N) {
+        const Node a = unidx(k, v.Nx, v.Ny);
+        const double c = v.A[0][k];
+        double d = c;
+        if ((a.i + a.j + a.l) & 1) {
+            const int NxNy = v.Nx * v.Ny;
+            double s = 0.0;
+            if (a.i > 0) s += v.A[1][k] * v.A[2][k - 1] / v.A[0][k - 1];
+            if (a.i < v.Nx - 1) s += v.A[2][k] * v.A[1][k + 1] / v.A[0][k + 1];
+            if (a.j > 0) s += v.A[3][k] * v.A[4][k - v.Nx] / v.A[0][k - v.Nx];
+            if (a.j < v.Ny - 1) s += v.A[4][k] * v.A[3][k + v.Nx] / v.A[0][k + v.Nx];
+            if (a.l > 0) s += v.A[5][k] * v.A[6][k - NxNy] / v.A[0][k - NxNy];
+            if (a.l < v.Nz - 1) s += v.A[6][k] * v.A[5][k + NxNy] / v.A[0][k + NxNy];
+            d = c - s;
+            if (!(d > 1e-8 * fabs(c))) d = c;
+        }
+        if (!(d != 0.0)) d = 1.0;
+        v.D[k] = d;
+    }
+}
+
+// pre-smoothing from x = 0: black rows then red rows of the two triangular sweeps
+// mode 0: x = M^-1 b (from zero).  mode 1: post-smoothing, z = M^-1 r with r the level's
+// residual array, x += z (the black z is parked in r for the red sweep).
+__global__ void k_smooth_black(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int mode, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if ((L > 0 && L >= P.nlev - 1) || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const LevView v = levview(P, L, bsel, xsel);
+    const double *src = mode ? v.r : v.b;
+    SS_GRID_LOOP(k, v.N) {
+        const Node a = unidx(k, v.Nx, v.Ny);
+        if (!((a.i + a.j + a.l) & 1)) continue;
+        const double s = offdiag_apply_div<double>(v.A, src, v.D, k, a.i, a.j, a.l, v.Nx, v.Ny, v.Nz);
+        const double z = (src[k] - s) / v.D[k];
+        if (mode) { v.x[k] += z; v.r[k] = z; }
+        else v.x[k] = z;
+    }
+}
+__global__ void k_smooth_red(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int mode, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if ((L > 0 && L >= P.nlev - 1) || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const LevView v = levview(P, L, bsel, xsel);
+    const double *src = mode ? v.r : v.b;
+    const double *zb = mode ? v.r : v.x;
+    SS_GRID_LOOP(k, v.N) {
+        const Node a = unidx(k, v.Nx, v.Ny);
+        if ((a.i + a.j + a.l) & 1) continue;
+        const double s = offdiag_apply<double>(v.A, zb, k, a.i, a.j, a.l, v.Nx, v.Ny, v.Nz);
+        const double z = (src[k] - s) / v.D[k];
+        if (mode) v.x[k] += z;
+        else v.x[k] = z;
+    }
+}
+
+// coarse aggregate (I,J,L) -> fine index range (AGG_RANGE, semiconductor_3d.c:1996-1999)
+struct Agg { int i0, i1, j0, j1, l0, l1; };
+__device__ __forceinline__ Agg agg_range(const LevView &f, int I, int J, int K) {
+    Agg g;
+    g.i0 = f.cx ? 2 * I : I; g.i1 = f.cx ? 2 * I + 1 : I; if (g.i1 > f.Nx - 1) g.i1 = f.Nx - 1;
+    g.j0 = f.cy ? 2 * J : J; g.j1 = f.cy ? 2 * J + 1 : J; if (g.j1 > f.Ny - 1) g.j1 = f.Ny - 1;
+    g.l0 = f.cz ? 2 * K : K; g.l1 = f.cz ? 2 * K + 1 : K; if (g.l1 > f.Nz - 1) g.l1 = f.Nz - 1;
+    return g;
+}
+
+// residual b - A x of the fine level summed over every aggregate (restriction), with
+// the level-0 row weights w (semiconductor_3d.c:2028-2037 applied to 1984-1991)
+__global__ void k_resid_restrict(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int wsel, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L >= P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const LevView f = levview(P, L, bsel, xsel);
+    const LevelT<double> &cl = P.lev[L + 1];
+    const double *w = (L == 0 && wsel) ? P.dsc : nullptr;
+    SS_GRID_LOOP(K, cl.N) {
+        const Node c = unidx(K, cl.Nx, cl.Ny);
+        const Agg g = agg_range(f, c.i, c.j, c.l);
+        double s = 0.0;
+        for (int l = g.l0; l <= g.l1; l++)
+            for (int j = g.j0; j <= g.j1; j++)
+                for (int i = g.i0; i <= g.i1; i++) {
+                    const int k = i + f.Nx * (j + f.Ny * l);
+                    const double r = f.b[k] - stencil_apply<double>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
+                    s += w ? w[k] * r : r;
+                }
+        cl.b[K] = s;
+    }
+}
+
+// x += alpha pw P xc (semiconductor_3d.c:2038-2048), then nothing else: the residual
+// needs every prolonged neighbour and is a separate pass
+__global__ void k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L >= P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const LevView f = levview(P, L, bsel, xsel);
+    const LevelT<double> &cl = P.lev[L + 1];
+    SS_GRID_LOOP(k, f.N) {
+        const Node a = unidx(k, f.Nx, f.Ny);
+        const int I = f.cx ? a.i >> 1 : a.i, J = f.cy ? a.j >> 1 : a.j, K = f.cz ? a.l >> 1 : a.l;
+        f.x[k] += alpha * f.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+    }
+}
+__global__ void k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L >= P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const LevView f = levview(P, L, bsel, xsel);
+    SS_GRID_LOOP(k, f.N) {
+        const Node a = unidx(k, f.Nx, f.Ny);
+        f.r[k] = f.b[k] - stencil_apply<double>(f.A, f.x, k, a.i, a.j, a.l, f.Nx, f.Ny, f.Nz);
+    }
+}
+
+// coarsest level: x = M^-1 b with the dense inverse formed at set-up (one block per instance)
+__global__ void k_coarse_solve(const DevP *__restrict__ Ps, int L, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L != P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const LevelT<double> &v = P.lev[L];
+    const int n = v.N;
+    __shared__ double sb[COARSE_MAX];
+    double *b = v.b, *x = v.x;
+    if (L == 0) return;                    // a single-level hierarchy is not built
+    for (int q = threadIdx.x; q < n; q += blockDim.x) sb[q] = b[q];
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        double s = 0.0;
+        for (int q = 0; q < n; q++) s += v.D[r * n + q] * sb[q];
+        x[r] = s;
+    }
+}
+
+// coarsest level set-up: dense matrix of the stencil, Gauss-Jordan inverse with partial
+// pivoting (tiny pivots guarded as semiconductor_3d.c:2066 does)
+__global__ void k_coarse_setup(const DevP *__restrict__ Ps, int L) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L != P.nlev - 1 || L == 0) return;
+    const LevelT<double> &v = P.lev[L];
+    const int n = v.N;
+    __shared__ double M[COARSE_MAX][COARSE_MAX + 1];
+    __shared__ int perm[COARSE_MAX];
+    __shared__ int piv;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) M[e / n][e % n] = 0.0;
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        const Node a = unidx(r, v.Nx, v.Ny);
+        const int NxNy = v.Nx * v.Ny;
+        M[r][r] = v.A[0][r];
+        if (a.i > 0) M[r][r - 1] = v.A[1][r];
+        if (a.i < v.Nx - 1) M[r][r + 1] = v.A[2][r];
+        if (a.j > 0) M[r][r - v.Nx] = v.A[3][r];
+        if (a.j < v.Ny - 1) M[r][r + v.Nx] = v.A[4][r];
+        if (a.l > 0) M[r][r - NxNy] = v.A[5][r];
+        if (a.l < v.Nz - 1) M[r][r + NxNy] = v.A[6][r];
+    }
+    __syncthreads();
+    // in-place Gauss-Jordan inversion with row interchanges (columns unswapped at the end)
+    for (int c = 0; c < n; c++) {
+        if (threadIdx.x == 0) {
+            int p = c;
+            double mx = fabs(M[c][c]);
+            for (int r = c + 1; r < n; r++)
+                if (fabs(M[r][c]) > mx) { mx = fabs(M[r][c]); p = r; }
+            piv = p;
+            perm[c] = p;
+            if (!(mx > 1e-300)) M[p][c] = 1e-300;
+        }
+        __syncthreads();
+        const int p = piv;
+        if (p != c)
+            for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                const double t = M[c][q]; M[c][q] = M[p][q]; M[p][q] = t;
+            }
+        __syncthreads();
+        const double dg = M[c][c];
+        __syncthreads();
+        if (threadIdx.x == 0) M[c][c] = 1.0;
+        __syncthreads();
+        for (int q = threadIdx.x; q < n; q += blockDim.x) M[c][q] /= dg;
+        __syncthreads();
+        // eliminate column c from every other row: each thread owns whole rows
+        for (int r = threadIdx.x; r < n; r += blockDim.x) {
+            if (r == c) continue;
+            const double fct = M[r][c];
+            M[r][c] = 0.0;
+            for (int q = 0; q < n; q++) M[r][q] -= fct * M[c][q];
+        }
+        __syncthreads();
+    }
+    for (int c = n - 1; c >= 0; c--) {
+        const int p = perm[c];
+        if (p != c)
+            for (int r = threadIdx.x; r < n; r += blockDim.x) {
+                const double t = M[r][c]; M[r][c] = M[r][p]; M[r][p] = t;
+            }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, q = e % n;
+        v.D[r * n + q] = M[r][q];
+    }
+}
+
+// Slotboom weights of one level (semiconductor_3d.c:2092-2117): qsign 0 gives pw = 1
+__device__ __forceinline__ double ph0(const DevP &P, int k, int qsign) {
+    const uint32_t f = P.flags[k];
+    if (fl_kind(f) != K_SEMI || fl_fix(f)) return PH_NONE;
+    return qsign > 0 ? P.phin[k] / P.VTref : -P.phip[k] / P.VTref;
+}
+__global__ void k_mg_weights(const DevP *__restrict__ Ps, int L, int qsign) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L >= P.nlev - 1) return;
+    const LevView f = levview(P, L, 0, 0);
+    const LevelT<double> &cl = P.lev[L + 1];
+    SS_GRID_LOOP(K, cl.N) {
+        const Node c = unidx(K, cl.Nx, cl.Ny);
+        const Agg g = agg_range(f, c.i, c.j, c.l);
+        if (qsign == 0) {
+            for (int l = g.l0; l <= g.l1; l++)
+                for (int j = g.j0; j <= g.j1; j++)
+                    for (int i = g.i0; i <= g.i1; i++) f.pw[i + f.Nx * (j + f.Ny * l)] = 1.0;
+            continue;
+        }
+        double mx = PH_NONE;
+        for (int l = g.l0; l <= g.l1; l++)
+            for (int j = g.j0; j <= g.j1; j++)
+                for (int i = g.i0; i <= g.i1; i++) {
+                    const int k = i + f.Nx * (j + f.Ny * l);
+                    const double p = L == 0 ? ph0(P, k, qsign) : f.ph[k];
+                    if (p > mx) mx = p;
+                }
+        cl.ph[K] = mx;
+        for (int l = g.l0; l <= g.l1; l++)
+            for (int j = g.j0; j <= g.j1; j++)
+                for (int i = g.i0; i <= g.i1; i++) {
+                    const int k = i + f.Nx * (j + f.Ny * l);
+                    const double p = L == 0 ? ph0(P, k, qsign) : f.ph[k];
+                    const double e = (p <= 0.5 * PH_NONE) ? -800.0 : p - mx;
+                    f.pw[k] = e < -700.0 ? 0.0 : exp(e);
+                }
+    }
+}
+
+// Petrov-Galerkin coarse operator P^T W A P (semiconductor_3d.c:2003-2027)
+__global__ void k_galerkin(const DevP *__restrict__ Ps, int L, int wsel) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L >= P.nlev - 1) return;
+    const LevView f = levview(P, L, 0, 0);
+    const LevelT<double> &cl = P.lev[L + 1];
+    const double *w = (L == 0 && wsel) ? P.dsc : nullptr;
+    const int NxNy = f.Nx * f.Ny;
+    SS_GRID_LOOP(K, cl.N) {
+        const Node c = unidx(K, cl.Nx, cl.Ny);
+        const Agg g = agg_range(f, c.i, c.j, c.l);
+        double cc = 0, xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
+        for (int l = g.l0; l <= g.l1; l++)
+            for (int j = g.j0; j <= g.j1; j++)
+                for (int i = g.i0; i <= g.i1; i++) {
+                    const int k = i + f.Nx * (j + f.Ny * l);
+                    const double wk = w ? w[k] : 1.0;
+                    double a;
+                    cc += wk * f.A[0][k] * f.pw[k];
+                    if (i > 0) { a = wk * f.A[1][k] * f.pw[k - 1]; if (i - 1 >= g.i0) cc += a; else xm += a; }
+                    if (i < f.Nx - 1) { a = wk * f.A[2][k] * f.pw[k + 1]; if (i + 1 <= g.i1) cc += a; else xp += a; }
+                    if (j > 0) { a = wk * f.A[3][k] * f.pw[k - f.Nx]; if (j - 1 >= g.j0) cc += a; else ym += a; }
+                    if (j < f.Ny - 1) { a = wk * f.A[4][k] * f.pw[k + f.Nx]; if (j + 1 <= g.j1) cc += a; else yp += a; }
+                    if (l > 0) { a = wk * f.A[5][k] * f.pw[k - NxNy]; if (l - 1 >= g.l0) cc += a; else zm += a; }
+                    if (l < f.Nz - 1) { a = wk * f.A[6][k] * f.pw[k + NxNy]; if (l + 1 <= g.l1) cc += a; else zp += a; }
+                }
+        if (cc == 0. && xm == 0. && xp == 0. && ym == 0. && yp == 0. && zm == 0. && zp == 0.) cc = 1.;
+        cl.A[0][K] = cc; cl.A[1][K] = xm; cl.A[2][K] = xp; cl.A[3][K] = ym;
+        cl.A[4][K] = yp; cl.A[5][K] = zm; cl.A[6][K] = zp;
+    }
+}
+
+// ------------------------------------------------------------------ vector kernels
+__global__ void k_absmax(const DevP *__restrict__ Ps, int xsel, int slot) {
+    const DevP &P = Ps[blockIdx.y];
+    const double *x = vsel(P, xsel);
+    double m = 0.0;
+    SS_GRID_LOOP(k, P.N) {
+        const double a = fabs(x[k]);
+        m = (a > m || a != a) ? a : m;
+    }
+    if (grid_max(m, P.part, P.ticket + 3)) P.res[slot] = m;
+}
+// y = x + a z  (selectors)
+__global__ void k_axpy(const DevP *__restrict__ Ps, int ysel, int xsel, double a, int zsel) {
+    const DevP &P = Ps[blockIdx.y];
+    double *y = vsel(P, ysel);
+    const double *x = vsel(P, xsel), *z = vsel(P, zsel);
+    SS_GRID_LOOP(k, P.N) y[k] = x[k] + a * z[k];
+}
+__global__ void k_fill(const DevP *__restrict__ Ps, int ysel, double v) {
+    const DevP &P = Ps[blockIdx.y];
+    double *y = vsel(P, ysel);
+    SS_GRID_LOOP(k, P.N) y[k] = v;
+}
+__global__ void k_copy(const DevP *__restrict__ Ps, int ysel, int xsel) {
+    const DevP &P = Ps[blockIdx.y];
+    double *y = vsel(P, ysel);
+    const double *x = vsel(P, xsel);
+    SS_GRID_LOOP(k, P.N) y[k] = x[k];
+}
+
+void launch_absmax_sel(const Ctx &c, int xsel, int slot) { k_absmax<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, xsel, slot); }
+void launch_axpy_sel(const Ctx &c, int ysel, int xsel, double a, int zsel) {
+    k_axpy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, ysel, xsel, a, zsel);
+}
+void launch_fill_sel(const Ctx &c, int ysel, double v) { k_fill<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, ysel, v); }
+void launch_copy_sel(const Ctx &c, int ysel, int xsel) { k_copy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, ysel, xsel); }
+
+// ------------------------------------------------------------------ multigrid driver
+void mg_setup(const Ctx &c, const MGHost &mg, int qsign) {
+    for (int L = 0; L < mg.maxlev - 1; L++) {
+        const int nc = mg.maxN[L + 1];
+        k_mg_weights<<<grid_n(c, nc), TPB, 0, c.st>>>(c.dP, L, qsign);
+        k_galerkin<<<grid_n(c, nc), TPB, 0, c.st>>>(c.dP, L, qsign != 0);
+        k_ilu_diag<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L);
+    }
+    for (int L = 1; L < mg.maxlev; L++) k_coarse_setup<<<dim3(1, c.ninst), TPB, 0, c.st>>>(c.dP, L);
+}
+
+// one V(1,1) cycle x = M^-1 b on the level-0 vectors (bsel -> xsel); mg_on = 0 applies
+// the level-0 smoother alone (the reference's ILU-only fallback).  gate: 0 always run,
+// 1 only while the instance's Krylov loop is active, 2 also not after a half-step exit.
+void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
+    if (!mg_on || mg.maxlev < 2) {
+        k_smooth_black<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, bsel, xsel, 0, gate);
+        k_smooth_red<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, bsel, xsel, 0, gate);
+        return;
+    }
+    for (int L = 0; L < mg.maxlev; L++) {
+        if (L < mg.maxlev - 1) {
+            k_smooth_black<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, 0, gate);
+            k_smooth_red<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, 0, gate);
+            k_resid_restrict<<<grid_n(c, mg.maxN[L + 1]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, wsel, gate);
+        }
+        if (L >= 1 && L >= mg.minlev - 1) k_coarse_solve<<<dim3(1, c.ninst), 64, 0, c.st>>>(c.dP, L, gate);
+    }
+    for (int L = mg.maxlev - 2; L >= 0; L--) {
+        k_prolong<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, mg.alpha, gate);
+        k_level_resid<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, gate);
+        k_smooth_black<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, 1, gate);
+        k_smooth_red<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, 1, gate);
+    }
+}
+
+// ------------------------------------------------------------------ PCG (semiconductor_3d.c:2182-2210)
+// r = b - A x; z = M r; rz = r.z
+__global__ void k_pcg_init_r(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    const double *b = P.rhs, *x = P.sol;
+    double *r = P.wk[0];
+    SS_GRID_LOOP(k, P.N) {
+        const Node a = unidx(k, P.Nx, P.Ny);
+        r[k] = b[k] - stencil_apply<double>(P.A, x, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+    }
+}
+// rz = r.z; mode 0 initial (rz0), mode 1 iteration end (stop test, beta)
+__global__ void k_pcg_rz(const DevP *__restrict__ Ps, int mode, double rtol2, int maxit) {
+    const DevP &P = Ps[blockIdx.y];
+    if (mode && !ks_running(P)) return;
+    const double *r = P.wk[0], *z = P.wk[1];
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) acc[0] += r[k] * z[k];
+    if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        const double rz = acc[0];
+        if (!mode) {
+            s.rz = s.rz0 = rz; s.it = 0; s.status = 0;
+            s.active = (rz > 0.0) ? 1 : 0;
+            if (!(rz > 0.0)) s.status = 2;
+        } else {
+            if (!(rz > rtol2 * s.rz0)) { s.active = 0; s.status = 1; }
+            else if (s.it >= maxit) { s.active = 0; s.status = 3; }
+            else { s.be = rz / s.rz; s.rz = rz; }
+        }
+    }
+}
+// p = z (init) or p = z + be p
+__global__ void k_pcg_p(const DevP *__restrict__ Ps, int init) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P)) return;
+    const double be = init ? 0.0 : P.ks->be;
+    double *p = P.wk[2];
+    const double *z = P.wk[1];
+    SS_GRID_LOOP(k, P.N) p[k] = z[k] + (init ? 0.0 : be * p[k]);
+}
+// q = A p; pq = p.q; al = rz / pq
+__global__ void k_pcg_q(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P)) return;
+    const double *p = P.wk[2];
+    double *q = P.wk[3];
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const Node a = unidx(k, P.Nx, P.Ny);
+        const double v = stencil_apply<double>(P.A, p, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+        q[k] = v;
+        acc[0] += p[k] * v;
+    }
+    if (grid_sum<1>(acc, P.part, P.ticket + 5)) {
+        KrylovS &s = *P.ks;
+        s.it++;
+        const double pq = acc[0];
+        if (!(pq > 0.0)) { s.active = 0; s.status = 2; s.al = 0.0; }
+        else s.al = s.rz / pq;
+    }
+}
+// x += al p; r -= al q
+__global__ void k_pcg_xr(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P)) return;
+    const double al = P.ks->al;
+    double *x = P.sol, *r = P.wk[0];
+    const double *p = P.wk[2], *q = P.wk[3];
+    SS_GRID_LOOP(k, P.N) { x[k] += al * p[k]; r[k] -= al * q[k]; }
+}
+
+int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every) {
+    KrylovS ks0{};
+    ks0.active = 1;
+    cudaMemcpyAsync(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
+    mg_setup(c, mg, 0);
+    k_pcg_init_r<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+    vcycle(c, mg, 0, 1, 0, 1, 0);                  // z = M r
+    k_pcg_rz<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, rtol * rtol, maxit);
+    k_pcg_p<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 1);
+    KrylovS hs{};
+    for (int it = 0; it < maxit;) {
+        const int nb = check_every;
+        for (int q = 0; q < nb && it < maxit; q++, it++) {
+            k_pcg_q<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            k_pcg_xr<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            vcycle(c, mg, 0, 1, 0, 1, 1);
+            k_pcg_rz<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 1, rtol * rtol, maxit);
+            k_pcg_p<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0);
+        }
+        cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
+        cudaStreamSynchronize(c.st);
+        if (!hs.active) break;
+    }
+    if (hs.active) {                                // ran out of iterations
+        cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
+        cudaStreamSynchronize(c.st);
+    }
+    return hs.it;
+}
+
+// ------------------------------------------------------------------ BiCGSTAB (semiconductor_3d.c:2216-2320)
+// work vectors: 0 r, 1 rh, 2 p, 3 v, 4 ph, 5 sh, 6 t, 7 x0 (start backup)
+// r = b - A x; rh = r; p = v = 0; rr = r.r; fl = sum (sum|A x| + |b|)^2; tgt
+__global__ void k_bicg_init(const DevP *__restrict__ Ps, double rtol, double atol) {
+    const DevP &P = Ps[blockIdx.y];
+    const double *b = P.rhs, *x = P.sol;
+    double *r = P.wk[0], *rh = P.wk[1], *p = P.wk[2], *v = P.wk[3];
+    const int NxNy = P.Nx * P.Ny;
+    double acc[2] = {0.0, 0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const Node a = unidx(k, P.Nx, P.Ny);
+        const int i = a.i, j = a.j, l = a.l;
+        double s = P.A[0][k] * x[k], fl = fabs(P.A[0][k] * x[k]) + fabs(b[k]), t;
+        if (i > 0) { t = P.A[1][k] * x[k - 1]; s += t; fl += fabs(t); }
+        if (i < P.Nx - 1) { t = P.A[2][k] * x[k + 1]; s += t; fl += fabs(t); }
+        if (j > 0) { t = P.A[3][k] * x[k - P.Nx]; s += t; fl += fabs(t); }
+        if (j < P.Ny - 1) { t = P.A[4][k] * x[k + P.Nx]; s += t; fl += fabs(t); }
+        if (l > 0) { t = P.A[5][k] * x[k - NxNy]; s += t; fl += fabs(t); }
+        if (l < P.Nz - 1) { t = P.A[6][k] * x[k + NxNy]; s += t; fl += fabs(t); }
+        const double rk = b[k] - s;
+        r[k] = rk; rh[k] = rk; p[k] = 0.0; v[k] = 0.0;
+        acc[0] += rk * rk;
+        acc[1] += fl * fl;
+    }
+    if (grid_sum<2>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        s.rr = acc[0]; s.fl = acc[1];
+        s.r0 = sqrt(acc[0]);
+        s.tgt = fmax(rtol * s.r0, atol * sqrt(acc[1]));
+        s.rho = s.al = s.om = 1.0; s.rbest = s.r0; s.stall = 0; s.it = 0; s.half = 0;
+        if (!(s.r0 > s.tgt)) { s.active = 0; s.status = 1; }
+        else { s.active = 1; s.status = 0; }
+    }
+}
+// rho1 = rh.r; restart on breakdown; be
+__global__ void k_bicg_rho(const DevP *__restrict__ Ps, int maxit) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P)) return;
+    const double *r = P.wk[0], *rh = P.wk[1];
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) acc[0] += rh[k] * r[k];
+    if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        if (s.it >= maxit) { s.active = 0; s.status = 3; return; }
+        s.it++;
+        double rho1 = acc[0];
+        s.pad0 = 0;
+        if (fabs(rho1) < 1e-300) {              // breakdown: restart the shadow residual
+            rho1 = s.rr;
+            s.rho = s.al = s.om = 1.0;
+            s.pad0 = 1;
+            if (!(rho1 > 0.0)) { s.active = 0; s.status = 2; return; }
+        }
+        s.rho1 = rho1;
+        s.be = (rho1 / s.rho) * (s.al / s.om);
+    }
+}
+// p = r + be (p - om v); on a restart rh = r, p = r, v = 0
+__global__ void k_bicg_p(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P)) return;
+    const KrylovS &s = *P.ks;
+    const double be = s.be, om = s.om;
+    const int restart = s.pad0;
+    double *p = P.wk[2], *v = P.wk[3], *rh = P.wk[1];
+    const double *r = P.wk[0];
+    SS_GRID_LOOP(k, P.N) {
+        if (restart) { rh[k] = r[k]; p[k] = r[k]; v[k] = 0.0; }
+        else p[k] = r[k] + be * (p[k] - om * v[k]);
+    }
+}
+// v = A ph; rv = rh.v; al
+__global__ void k_bicg_v(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P)) return;
+    const double *ph = P.wk[4], *rh = P.wk[1];
+    double *v = P.wk[3];
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const Node a = unidx(k, P.Nx, P.Ny);
+        const double t = stencil_apply<double>(P.A, ph, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+        v[k] = t;
+        acc[0] += rh[k] * t;
+    }
+    if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        if (fabs(acc[0]) < 1e-300) { s.active = 0; s.status = 2; return; }
+        s.rv = acc[0];
+        s.al = s.rho1 / acc[0];
+    }
+}
+// r -= al v; ss = r.r; half-step exit test
+__global__ void k_bicg_s(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P)) return;
+    const double al = P.ks->al;
+    double *r = P.wk[0];
+    const double *v = P.wk[3];
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const double t = r[k] - al * v[k];
+        r[k] = t;
+        acc[0] += t * t;
+    }
+    if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        s.ss = acc[0];
+        if (sqrt(acc[0]) <= s.tgt) { s.half = 1; s.rr = acc[0]; }
+    }
+}
+// t = A sh; tt = t.t; ts = t.r; om
+__global__ void k_bicg_t(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P) || P.ks->half) return;
+    const double *sh = P.wk[5], *r = P.wk[0];
+    double *t = P.wk[6];
+    double acc[2] = {0.0, 0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const Node a = unidx(k, P.Nx, P.Ny);
+        const double q = stencil_apply<double>(P.A, sh, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+        t[k] = q;
+        acc[0] += q * q;
+        acc[1] += q * r[k];
+    }
+    if (grid_sum<2>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        s.tt = acc[0]; s.ts = acc[1];
+        s.om = acc[0] > 0.0 ? acc[1] / acc[0] : 0.0;
+    }
+}
+// x += al ph + om sh; r -= om t; rr = r.r; stop tests (or the half-step x update)
+__global__ void k_bicg_x(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!ks_running(P)) return;
+    const KrylovS &s0 = *P.ks;
+    const double al = s0.al, om = s0.om;
+    const int half = s0.half;
+    double *x = P.sol, *r = P.wk[0];
+    const double *ph = P.wk[4], *sh = P.wk[5], *t = P.wk[6];
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) {
+        if (half) { x[k] += al * ph[k]; continue; }
+        x[k] += al * ph[k] + om * sh[k];
+        const double q = r[k] - om * t[k];
+        r[k] = q;
+        acc[0] += q * q;
+    }
+    if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        if (half) { s.active = 0; s.status = 1; return; }
+        s.rr = acc[0];
+        const double rn = sqrt(acc[0]);
+        if (rn <= s.tgt || s.om == 0.0) { s.active = 0; s.status = 1; return; }
+        if (rn < 0.99 * s.rbest) { s.rbest = rn; s.stall = 0; }
+        else if (++s.stall > 40) { s.active = 0; s.status = 2; return; }
+        s.rho = s.rho1;
+    }
+}
+
+// One BiCGSTAB solve of P.A sol = rhs from the present sol.  Returns the iterations;
+// rn / r0 the final and initial residual norms.
+int bicgstab_core(const Ctx &c, const MGHost &mg, int maxit, double rtol, double atol, int mg_on, int check_every,
+                  double *rn, double *r0, int qsign) {
+    if (mg_on) mg_setup(c, mg, qsign);
+    else {
+        k_ilu_diag<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0);
+    }
+    k_bicg_init<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, rtol, atol);
+    KrylovS hs{};
+    const int wsel = qsign != 0;
+    for (int it = 0; it < maxit;) {
+        for (int q = 0; q < check_every && it < maxit; q++, it++) {
+            k_bicg_rho<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, maxit);
+            k_bicg_p<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            vcycle(c, mg, 2, 4, wsel, mg_on, 1);            // ph = M p
+            k_bicg_v<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            k_bicg_s<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            vcycle(c, mg, 0, 5, wsel, mg_on, 2);            // sh = M r
+            k_bicg_t<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            k_bicg_x<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+        }
+        cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
+        cudaStreamSynchronize(c.st);
+        if (!hs.active) break;
+    }
+    cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
+    cudaStreamSynchronize(c.st);
+    *rn = sqrt(hs.rr);
+    *r0 = hs.r0;
+    return hs.it;
+}
+
+}  // namespace ss

@@ -1,0 +1,169 @@
+// Material tables of the 14 reference materials.  The numbers must equal the
+// reference's (semiconductor_3d.c:423-627) for results to agree; the code that holds
+// them is this library's own: one descriptor per material, applied by a common routine.
+#include "materials.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "semisim.h"
+
+namespace ss {
+
+namespace {
+
+// Bandgap Varshni form Eg(T) = E0 - a T^2 / (T + b)
+double varshni(double E0, double a, double b, double T) { return E0 - a * T * T / (T + b); }
+
+struct Lowfield {   // Arora / Caughey-Thomas parameters (mobilities in m^2/Vs, N in m^-3)
+    double mun_max, mup_max, mun_min, mup_min, Nref_n, Nref_p, alpha_n, alpha_p;
+    double mt_min, mt_max_n, mt_max_p, mt_Nref, mt_alpha;
+};
+struct Recomb { double tau_n0, tau_p0, Cn, Cp, Brad; };
+struct Sat { double vsat_n, vsat_p, beta_n, beta_p; };
+
+void set_lowfield(Material &m, const Lowfield &l) {
+    m.mu_n_max = l.mun_max; m.mu_p_max = l.mup_max; m.mu_n_min = l.mun_min; m.mu_p_min = l.mup_min;
+    m.Nref_n = l.Nref_n; m.Nref_p = l.Nref_p; m.alpha_n = l.alpha_n; m.alpha_p = l.alpha_p;
+    m.mt_min = l.mt_min; m.mt_max_n = l.mt_max_n; m.mt_max_p = l.mt_max_p;
+    m.mt_Nref = l.mt_Nref; m.mt_alpha = l.mt_alpha;
+}
+void set_recomb(Material &m, const Recomb &r) {
+    m.tau_n0 = r.tau_n0; m.tau_p0 = r.tau_p0; m.Cn = r.Cn; m.Cp = r.Cp; m.Brad = r.Brad;
+}
+void set_sat(Material &m, const Sat &s) {
+    m.vsat_n = s.vsat_n; m.vsat_p = s.vsat_p; m.beta_n = s.beta_n; m.beta_p = s.beta_p;
+}
+
+// Semiconductor band data: Eg(T) Varshni, affinity, permittivity, Nc/Nv at 300 K with
+// power-law temperature exponents.
+struct Band { double E0, a, b, chi, eps_r, Nc300, Nc_exp, Nv300, Nv_exp; };
+void set_band(Material &m, const Band &bd) {
+    const double tr = m.T / 300.0;
+    m.Eg = varshni(bd.E0, bd.a, bd.b, m.T);
+    m.chi = bd.chi; m.eps_r = bd.eps_r;
+    m.Nc = bd.Nc300 * std::pow(tr, bd.Nc_exp);
+    m.Nv = bd.Nv300 * std::pow(tr, bd.Nv_exp);
+}
+
+}  // namespace
+
+void material_init(Material &m, int id, double T) {
+    m = Material();
+    m.id = id; m.T = T; m.VT = KB * T / Q;
+    const double tr = T / 300.0;
+    switch (id) {
+    case 0: {   // Si: Masetti low-field mobility, Canali saturation laws, Klaassen BGN
+        set_band(m, {1.170, 4.73e-4, 636., 4.05, 11.7, 2.86e25, 1.58, 3.10e25, 1.85});
+        m.mas_on = 1; m.mt_max_n = -2.5; m.mt_max_p = -2.2;
+        m.mu_n_max = 0.1417; m.mu_p_max = 0.04705; m.mu_n_min = 0.00522; m.mu_p_min = 0.00449;
+        const double mm1[2] = {0.00522, 0.00449}, mm2[2] = {0.00522, 0.0}, mu1[2] = {0.00434, 0.00290};
+        const double Pc[2] = {0.0, 9.23e22}, Cr[2] = {9.68e22, 2.23e23}, Cs[2] = {3.43e26, 6.10e26};
+        const double ma[2] = {0.680, 0.719}, mb[2] = {2.0, 2.0};
+        for (int c = 0; c < 2; c++) {
+            m.mas_min1[c] = mm1[c]; m.mas_min2[c] = mm2[c]; m.mas_mu1[c] = mu1[c]; m.mas_Pc[c] = Pc[c];
+            m.mas_Cr[c] = Cr[c]; m.mas_Cs[c] = Cs[c]; m.mas_a[c] = ma[c]; m.mas_b[c] = mb[c];
+        }
+        m.Nref_n = 9.68e22; m.Nref_p = 2.23e23; m.alpha_n = 0.680; m.alpha_p = 0.719;
+        set_sat(m, {1.07e5 * std::pow(tr, -0.87), 8.37e4 * std::pow(tr, -0.52),
+                    1.109 * std::pow(tr, 0.66), 1.213 * std::pow(tr, 0.17)});
+        set_recomb(m, {1e-5, 1e-5, 2.8e-43, 9.9e-44, 4.73e-21});
+        m.tau_Nref = 1e22;
+        m.bgn_E = 6.92e-3; m.bgn_N = 1.3e23; m.bgn_C = 0.5;
+        m.lb_on = 3; m.ii_on = 1;
+        break;
+    }
+    case 1:     // Ge
+        set_band(m, {0.742, 4.77e-4, 235., 4.00, 16.2, 1.04e25, 1.5, 6.0e24, 1.5});
+        set_lowfield(m, {0.39, 0.19, 0.040, 0.020, 1.30e23, 1.00e23, 0.56, 0.43, 0., -1.66, -2.33, 0., 0.});
+        set_sat(m, {6e4, 5.4e4, 1., 1.});
+        set_recomb(m, {1e-3, 1e-3, 1e-42, 1e-42, 6.4e-20});
+        break;
+    case 2:     // GaAs
+        set_band(m, {1.519, 5.405e-4, 204., 4.07, 12.9, 4.37e23, 1.5, 8.68e24, 1.5});
+        set_lowfield(m, {0.94, 0.040, 0.050, 0.0020, 6.0e22, 2.75e23, 0.394, 0.394, 0., -2.1, -2.1, 3.0, 0.});
+        set_sat(m, {7.7e4, 7.7e4, 1., 1.});
+        set_recomb(m, {1e-9, 1e-9, 1e-43, 1e-43, 1.5e-16});
+        m.ii_on = 1;
+        break;
+    case 3:     // InP
+        set_band(m, {1.4236, 3.63e-4, 162., 4.38, 12.5, 5.7e23, 1.5, 1.1e25, 1.5});
+        set_lowfield(m, {0.52, 0.015, 0.040, 0.0010, 3.00e23, 4.90e23, 0.47, 0.40, 0., -2.0, -2.0, 3.25, 0.});
+        set_sat(m, {1e5, 5e4, 1., 1.});
+        set_recomb(m, {1e-8, 1e-8, 1e-43, 1e-43, 8.5e-17});
+        break;
+    case 4:     // 4H-SiC
+        set_band(m, {3.265, 6.5e-4, 1300., 3.7, 9.7, 1.73e25, 1.5, 2.64e25, 1.5});
+        set_lowfield(m, {0.095, 0.0124, 0.0040, 0.00159, 1.94e23, 1.76e25, 0.61, 0.34, -0.5, -2.40, -2.15, 0., 0.});
+        set_sat(m, {2.2e5, 1.6e5, 1.2, 1.});
+        set_recomb(m, {1e-6, 1e-7, 5e-44, 2e-44, 1.5e-18});
+        m.ii_on = 1; m.lb_on = 1; m.lbc_on = 1; m.ion_on = 1;
+        m.ani_n = 1. / 0.83; m.ani_p = 1. / 1.15;
+        break;
+    case 5:     // GaN
+        set_band(m, {3.507, 9.09e-4, 830., 4.1, 8.9, 2.3e24, 1.5, 4.6e25, 1.5});
+        set_lowfield(m, {0.120, 0.0030, 0.0055, 0.00030, 1.00e23, 3.00e23, 1.0, 2.0, -1.02, -3.84, -3.84, 0., 0.});
+        set_sat(m, {2.5e5, 2e5, 1., 1.});
+        set_recomb(m, {1e-8, 1e-8, 1e-43, 1e-43, 1.1e-16});
+        m.ii_on = 1;
+        break;
+    case 6:     // Al0.3Ga0.7As
+        set_band(m, {1.882, 5.58e-4, 295., 3.827, 12.24, 7.2e23, 1.5, 1.05e25, 1.5});
+        set_lowfield(m, {0.35, 0.025, 0.020, 0.0015, 6.00e22, 1.00e23, 0.394, 0.394, 0., -2.1, -2.1, 3.0, 0.});
+        set_sat(m, {6e4, 5e4, 1., 1.});
+        set_recomb(m, {1e-9, 1e-9, 1e-43, 1e-43, 5e-17});
+        break;
+    case 7:     // Al0.25Ga0.75N
+        set_band(m, {3.990, 9.09e-4, 830., 3.76, 8.8, 3.2e24, 1.5, 4.6e25, 1.5});
+        set_lowfield(m, {0.030, 0.0010, 0.0030, 0.00020, 1.00e23, 3.00e23, 1.0, 2.0, -1.02, -3.84, -3.84, 0., 0.});
+        set_sat(m, {1.5e5, 1e5, 1., 1.});
+        set_recomb(m, {1e-9, 1e-9, 1e-43, 1e-43, 1e-16});
+        break;
+    // insulators: gap, affinity, permittivity
+    case 8:  m.insulator = 1; m.Eg = 9.0;  m.chi = 0.95; m.eps_r = 3.9;  break;   // SiO2
+    case 9:  m.insulator = 1; m.Eg = 6.8;  m.chi = 1.35; m.eps_r = 9.0;  break;   // Al2O3
+    case 10: m.insulator = 1; m.Eg = 5.8;  m.chi = 2.55; m.eps_r = 22.0; break;   // HfO2
+    case 11: m.insulator = 1; m.Eg = 5.1;  m.chi = 2.05; m.eps_r = 7.5;  break;   // Si3N4
+    case 12: m.insulator = 1; m.Eg = 10.;  m.chi = 0.;   m.eps_r = 1.0;  break;   // void
+    case 13: m.insulator = 1; m.Eg = 10.;  m.chi = 0.;   m.eps_r = 1.0e3; break;  // metal inclusion
+    default:
+        std::fprintf(stderr, "semisim-b200: WARNING unknown material id %d, using Si\n", id);
+        material_init(m, 0, T);
+        return;
+    }
+    if (m.insulator) {
+        // insulators carry no mobility / recombination data; keep the defaults neutral
+        m.mt_min = m.mt_max_n = m.mt_max_p = m.mt_Nref = m.mt_alpha = 0.;
+    }
+    m.ni = m.insulator ? 0. : std::sqrt(m.Nc * m.Nv) * std::exp(-m.Eg / (2. * m.VT));
+}
+
+// Low-field mobility: Masetti (mas_on) or Arora / Caughey-Thomas (semiconductor_3d.c:646-662)
+double mobility_low(const Material &m, double Ntot, int hole) {
+    if (Ntot < 1.) Ntot = 1.;
+    const double tr = m.T / 300.;
+    if (m.mas_on) {
+        const int c = hole ? 1 : 0;
+        const double muL = (hole ? m.mu_p_max : m.mu_n_max) * std::pow(tr, hole ? m.mt_max_p : m.mt_max_n);
+        const double mu = m.mas_min1[c] * std::exp(-m.mas_Pc[c] / Ntot) +
+                          (muL - m.mas_min2[c]) / (1. + std::pow(Ntot / m.mas_Cr[c], m.mas_a[c])) -
+                          m.mas_mu1[c] / (1. + std::pow(m.mas_Cs[c] / Ntot, m.mas_b[c]));
+        return mu > 1e-6 ? mu : 1e-6;
+    }
+    const double mumin = (hole ? m.mu_p_min : m.mu_n_min) * std::pow(tr, m.mt_min);
+    double mumax = (hole ? m.mu_p_max : m.mu_n_max) * std::pow(tr, hole ? m.mt_max_p : m.mt_max_n);
+    const double Nref = (hole ? m.Nref_p : m.Nref_n) * std::pow(tr, m.mt_Nref);
+    const double alpha = (hole ? m.alpha_p : m.alpha_n) * std::pow(tr, m.mt_alpha);
+    if (mumax < mumin) mumax = mumin;
+    return mumin + (mumax - mumin) / (1. + std::pow(Ntot / Nref, alpha));
+}
+
+// Half the band-gap narrowing in units of VT, Klaassen form (semiconductor_3d.c:839-843)
+double bgn_half(const Material &m, double N) {
+    if (!(m.bgn_E > 0.) || N < 1.) return 0.;
+    const double L = std::log(N / m.bgn_N);
+    return 0.5 * m.bgn_E * (L + std::sqrt(L * L + m.bgn_C)) / m.VT;
+}
+
+}  // namespace ss

@@ -1,0 +1,33 @@
+// Host-side material model of the solver library.
+#pragma once
+
+namespace ss {
+
+// Parameters of one material at temperature T (SI units).  The field set covers the
+// physics of the solve path (Poisson, Scharfetter-Gummel continuity with SRH + Auger +
+// radiative recombination, low-field and velocity-saturated mobility, band-gap
+// narrowing) plus flags naming the reference models this library does not implement.
+struct Material {
+    int id = 0, insulator = 0;
+    double T = 300, VT = 0, Eg = 0, chi = 0, eps_r = 1, Nc = 0, Nv = 0, ni = 0;
+    // low-field mobility: Arora / Caughey-Thomas form or Masetti (mas_on)
+    double mu_n_max = 0, mu_p_max = 0, mu_n_min = 0, mu_p_min = 0;
+    double Nref_n = 1, Nref_p = 1, alpha_n = 1, alpha_p = 1;
+    double mt_min = -0.57, mt_max_n = -2.33, mt_max_p = -2.23, mt_Nref = 2.4, mt_alpha = -0.146;
+    int mas_on = 0;
+    double mas_min1[2] = {0, 0}, mas_min2[2] = {0, 0}, mas_mu1[2] = {0, 0}, mas_Pc[2] = {0, 0};
+    double mas_Cr[2] = {1, 1}, mas_Cs[2] = {1, 1}, mas_a[2] = {1, 1}, mas_b[2] = {1, 1};
+    double vsat_n = 0, vsat_p = 0, beta_n = 1, beta_p = 1;
+    double tau_n0 = 0, tau_p0 = 0, Cn = 0, Cp = 0, Brad = 0, tau_Nref = 0;
+    double bgn_E = 0, bgn_N = 1, bgn_C = 0;
+    double ani_n = 0, ani_p = 0;
+    // models outside this library's scope that the material would switch on
+    int lb_on = 0, lbc_on = 0, ion_on = 0, ii_on = 0;
+    double lnc = 0, lnv = 0;      // effective ln Nc / ln Nv in the common gauge (mat_prepare)
+};
+
+void material_init(Material &m, int id, double T);
+double mobility_low(const Material &m, double Ntot, int hole);
+double bgn_half(const Material &m, double N);
+
+}  // namespace ss

@@ -1,0 +1,127 @@
+// Internal declarations of the B200 solver library (not part of the public ABI).
+//
+// Data model: one device instance ("Inst") per simulated device.  Node arrays live in
+// HBM as structure-of-arrays, x fastest (node k = i + Nx*(j + Ny*l), the reference's
+// IDX, semiconductor_3d.c:114).  Kernels address an instance through a device-resident
+// parameter record (DevP) selected by blockIdx.y, so the same kernels run one instance
+// or a batch of instances per launch.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ss {
+
+constexpr double Q = 1.602176634e-19;
+constexpr double KB = 1.380649e-23;
+constexpr double EPS0 = 8.8541878128e-12;
+constexpr double EPS_OX = 3.9 * EPS0;
+constexpr double LN_MIN = -230.0, LN_MAX = 150.0, NFLOOR = 1e-100;
+constexpr double PH_NONE = -1e300;
+constexpr int NM_MAX = 16, NC_MAX = 32, AA_MAX = 12, MAXLEV = 24;
+constexpr int K_SEMI = 0, K_INS = 1, K_METAL = 2;
+constexpr int TPB = 256;            // threads per block of the node kernels
+constexpr int RED_MAX_BLOCKS = 2048; // grid cap of reducing kernels (partials per instance)
+constexpr int RED_NV = 16;          // doubles per block partial record
+constexpr int COARSE_MAX = 64;      // unknowns of the coarsest multigrid level
+
+// per-node flag word: kind(2) | contact+1 (6) | gate+1 (6) | material (4) | car_fix (1)
+__host__ __device__ inline int fl_kind(uint32_t f) { return int(f & 3u); }
+__host__ __device__ inline int fl_con(uint32_t f) { return int((f >> 2) & 63u); }
+__host__ __device__ inline int fl_gate(uint32_t f) { return int((f >> 8) & 63u); }
+__host__ __device__ inline int fl_mat(uint32_t f) { return int((f >> 14) & 15u); }
+__host__ __device__ inline bool fl_fix(uint32_t f) { return (f >> 18) & 1u; }
+__host__ __device__ inline uint32_t make_flags(int kind, int con, int gate, int mat, bool fix) {
+    return uint32_t(kind) | (uint32_t(con) << 2) | (uint32_t(gate) << 8) | (uint32_t(mat) << 14) |
+           (uint32_t(fix ? 1 : 0) << 18);
+}
+
+// material constants the kernels need (semiconductor_3d.c:127-188, derived by mat_prepare)
+struct MatD {
+    double VT, lnc, lnv, ni, eps;
+    double tau_n0, tau_p0, Cn, Cp, Brad, tau_Nref;
+    double vsat_n, vsat_p, beta_n, beta_p, ani_n, ani_p;
+    double chi, Eg;
+    int insulator, pad;
+};
+
+// contact constants the kernels need
+struct ConD {
+    double V, phi_m, tox, qox;   // applied voltage of the stage, work function, oxide
+    int bc, pad;
+};
+
+// one multigrid level of scalar type T (7-point stencil, 2x2x2 aggregation)
+template <class T>
+struct LevelT {
+    int Nx, Ny, Nz, N;
+    int cx, cy, cz, last;        // coarsened along x/y/z; last = coarsest (dense) level
+    T *A[7];                     // c, xm, xp, ym, yp, zm, zp
+    T *D;                        // red-black D-ILU pivots (or the dense inverse on the last level)
+    T *x, *b, *r;
+    double *pw, *ph;             // prolongation weights (to the parent), reference level / VT
+};
+
+// per-instance Krylov scalars (device resident; written by the reduction finalisers)
+struct KrylovS {
+    double rho, al, om, rho1, be, rv, ss, tt, ts, rr, r0, tgt, rbest, fl;
+    double rz, rz0, pq;
+    int it, stall, active, status;   // status: 0 running, 1 converged, 2 breakdown/stop
+    int half, pad0, pad1, pad2;
+};
+
+// everything a kernel needs about one instance
+struct DevP {
+    int Nx, Ny, Nz, N;
+    int models, caxis, ncon, ref_mat;
+    double VTref, Cref;
+    const double *xs, *ys, *zs, *Lx, *Ly, *Lz;
+    const uint32_t *flags;
+    const double *Nd, *Na, *Nf, *bgn, *robA;
+    const MatD *mats;
+    const ConD *cons;
+    const int *cnode;             // contact-node list (semiconductor nodes of carrier contacts)
+    int ncnode, nlev;
+    // state
+    double *phi, *phin, *phip, *n, *p;
+    double *mu0n, *mu0p;          // low-field node mobility (fixed after set-up)
+    double *mudn, *mudp;          // display mobility (after a resolve)
+    double *fmu[6];               // face mobility k -> k+e_ax: 0-2 electrons, 3-5 holes
+    // level-0 system, FP64
+    double *A[7], *rhs, *sc, *dsc, *sol, *F;
+    double *wk[8];                // Krylov work vectors
+    double *qn0, *qp0, *dqn, *dqp, *xk, *tr;
+    double *Jx, *Jy, *Jz, *Rt;    // display current density and recombination
+    double *h1[3], *h2[3], *e2[3];
+    // Anderson
+    float *aaF, *aaG;             // AA_MAX slots of 3N each
+    double *aaf, *aag;            // 3N each
+    double *gram;                 // AA_MAX*AA_MAX
+    double *aagam;                // AA_MAX coefficients
+    // reductions
+    double *part;                 // RED_MAX_BLOCKS*RED_NV
+    unsigned *ticket;             // one counter per reduction slot (8)
+    double *res;                  // scalar results (64)
+    KrylovS *ks;
+    // multigrid (FP64 and FP32 hierarchies)
+    LevelT<double> *lev;          // device array of nlev levels
+    LevelT<float> *levf;
+    int *ccl;                     // labels for connected-component work
+    int *cclaux;
+};
+
+// slots of DevP::res
+enum ResSlot {
+    R_PNORM = 0,     // poisson ||F/diag||
+    R_DMAX = 1,      // max |dx| (Newton step)
+    R_DQ = 2,        // cont_update weighted max |dq|
+    R_DPSI = 3,      // max |psi - xk|
+    R_FLOOR = 4,
+    R_AUX = 5,
+    R_I = 8,         // terminal currents I[NC_MAX] at 8..39
+    R_S = 40,        // scales S[NC_MAX] at 40..71 (res has 128 doubles)
+    R_IN = 72,       // electron components at 72..103
+    R_TOTAL = 128
+};
+
+}  // namespace ss

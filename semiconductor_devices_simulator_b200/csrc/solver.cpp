@@ -1,0 +1,833 @@
+// Host control of the solve path over device-resident state: device set-up (prepare),
+// equilibrium, damped Newton-Poisson with PCG, the continuity solves with BiCGSTAB and
+// the floating-block balance, the Gummel loop with Anderson mixing and the adaptive
+// continuation with the sweep predictor.  The control logic follows the reference
+// routine named beside each function; all O(N) work runs in the CUDA kernels.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "solver_ctx.h"
+
+namespace ss {
+
+Knobs g_knobs;
+std::atomic<int> g_stop{0};
+volatile double g_prog[8];
+
+static double wtime() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+#define CK(x)                                                                                   \
+    do {                                                                                        \
+        cudaError_t e_ = (x);                                                                   \
+        if (e_ != cudaSuccess) {                                                                \
+            std::fprintf(stderr, "semisim-b200: CUDA error %s at %s:%d\n", cudaGetErrorString(e_), \
+                         __FILE__, __LINE__);                                                   \
+            return 0;                                                                           \
+        }                                                                                       \
+    } while (0)
+
+bool gpu_available() {
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+}
+
+Ctx make_ctx(Inst &d) {
+    Ctx c;
+    c.dP = d.g.d;
+    c.h = d.g.h;
+    c.ninst = 1;
+    c.maxN = (int)d.N;
+    c.st = d.g.st;
+    return c;
+}
+
+static double read_res(Inst &d, int slot) {
+    cudaMemcpyAsync(d.g.pin, d.g.h.res + slot, sizeof(double), cudaMemcpyDeviceToHost, d.g.st);
+    cudaStreamSynchronize(d.g.st);
+    return d.g.pin[0];
+}
+
+// ------------------------------------------------------------------ device memory
+static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Carver {
+    char *base = nullptr;
+    size_t off = 0;
+    template <class T> T *take(size_t n) {
+        T *p = reinterpret_cast<T *>(base ? base + off : nullptr);
+        off += align_up(n * sizeof(T));
+        return p;
+    }
+};
+
+// Lay out every device array of an instance in one block (two passes: size, then place).
+static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &levs, int nlev, const int dims[][6]) {
+    const size_t N = d.N;
+    P.flags = cv.take<uint32_t>(N);
+    P.Nd = cv.take<double>(N); P.Na = cv.take<double>(N); P.Nf = cv.take<double>(N);
+    P.bgn = cv.take<double>(N); P.robA = cv.take<double>(N);
+    P.xs = cv.take<double>(d.Nx); P.ys = cv.take<double>(d.Ny); P.zs = cv.take<double>(d.Nz);
+    P.Lx = cv.take<double>(d.Nx); P.Ly = cv.take<double>(d.Ny); P.Lz = cv.take<double>(d.Nz);
+    P.mats = cv.take<MatD>(NM_MAX);
+    P.cons = cv.take<ConD>(NC_MAX);
+    P.cnode = cv.take<int>(N > 0 ? N : 1);
+    P.phi = cv.take<double>(N); P.phin = cv.take<double>(N); P.phip = cv.take<double>(N);
+    P.n = cv.take<double>(N); P.p = cv.take<double>(N);
+    P.mu0n = cv.take<double>(N); P.mu0p = cv.take<double>(N);
+    P.mudn = cv.take<double>(N); P.mudp = cv.take<double>(N);
+    for (int q = 0; q < 6; q++) P.fmu[q] = cv.take<double>(N);
+    for (int q = 0; q < 7; q++) P.A[q] = cv.take<double>(N);
+    P.rhs = cv.take<double>(N); P.sc = cv.take<double>(N); P.dsc = cv.take<double>(N);
+    P.sol = cv.take<double>(N); P.F = cv.take<double>(N);
+    for (int q = 0; q < 8; q++) P.wk[q] = cv.take<double>(N);
+    P.qn0 = cv.take<double>(N); P.qp0 = cv.take<double>(N); P.dqn = cv.take<double>(N);
+    P.dqp = cv.take<double>(N); P.xk = cv.take<double>(N); P.tr = cv.take<double>(N);
+    P.Jx = cv.take<double>(N); P.Jy = cv.take<double>(N); P.Jz = cv.take<double>(N); P.Rt = cv.take<double>(N);
+    for (int a = 0; a < 3; a++) { P.h1[a] = cv.take<double>(N); P.h2[a] = cv.take<double>(N); P.e2[a] = cv.take<double>(N); }
+    P.aaF = cv.take<float>((size_t)AA_MAX * 3 * N);
+    P.aaG = cv.take<float>((size_t)AA_MAX * 3 * N);
+    P.aaf = cv.take<double>(3 * N); P.aag = cv.take<double>(3 * N);
+    P.gram = cv.take<double>(AA_MAX * AA_MAX); P.aagam = cv.take<double>(AA_MAX);
+    P.part = cv.take<double>((size_t)RED_MAX_BLOCKS * RED_NV);
+    P.ticket = cv.take<unsigned>(16);
+    P.res = cv.take<double>(R_TOTAL);
+    P.ks = cv.take<KrylovS>(1);
+    P.lev = cv.take<LevelT<double>>(MAXLEV);
+    P.levf = nullptr;
+    P.ccl = cv.take<int>(N); P.cclaux = cv.take<int>(N);
+    levs.assign(nlev, LevelT<double>{});
+    for (int L = 0; L < nlev; L++) {
+        LevelT<double> &v = levs[L];
+        v.Nx = dims[L][0]; v.Ny = dims[L][1]; v.Nz = dims[L][2];
+        v.N = v.Nx * v.Ny * v.Nz;
+        v.cx = dims[L][3]; v.cy = dims[L][4]; v.cz = dims[L][5];
+        v.last = L == nlev - 1;
+        const size_t n = (size_t)v.N;
+        if (L == 0) {
+            for (int q = 0; q < 7; q++) v.A[q] = P.A[q];
+            v.x = nullptr; v.b = nullptr;
+        } else {
+            for (int q = 0; q < 7; q++) v.A[q] = cv.take<double>(n);
+            v.x = cv.take<double>(n); v.b = cv.take<double>(n);
+        }
+        v.D = cv.take<double>(v.last && L > 0 ? n * n : n);
+        v.r = cv.take<double>(n);
+        v.pw = cv.take<double>(n);
+        v.ph = cv.take<double>(n);
+    }
+}
+
+// 2x2x2 aggregation hierarchy shape (semiconductor_3d.c:1894-1921)
+int mg_levels(int Nx, int Ny, int Nz, int dims[][6]) {
+    int nl = 1;
+    dims[0][0] = Nx; dims[0][1] = Ny; dims[0][2] = Nz; dims[0][3] = dims[0][4] = dims[0][5] = 0;
+    while (nl < MAXLEV) {
+        int *f = dims[nl - 1];
+        if ((size_t)f[0] * f[1] * f[2] <= 64) break;
+        const int cx = f[0] > 2, cy = f[1] > 2, cz = f[2] > 2;
+        if (!cx && !cy && !cz) break;
+        f[3] = cx; f[4] = cy; f[5] = cz;
+        int *c = dims[nl];
+        c[0] = cx ? (f[0] + 1) / 2 : f[0];
+        c[1] = cy ? (f[1] + 1) / 2 : f[1];
+        c[2] = cz ? (f[2] + 1) / 2 : f[2];
+        c[3] = c[4] = c[5] = 0;
+        nl++;
+    }
+    return nl;
+}
+
+void gpu_free(Inst &d) {
+    if (d.g.block) cudaFree(d.g.block);
+    if (d.g.d) cudaFree(d.g.d);
+    if (d.g.pin) cudaFreeHost(d.g.pin);
+    if (d.g.scratch) cudaFree(d.g.scratch);
+    if (d.g.flag) cudaFree(d.g.flag);
+    if (d.g.st) cudaStreamDestroy(d.g.st);
+    d.g = Gpu();
+}
+
+static int gpu_alloc(Inst &d) {
+    if (d.g.ready && d.g.h.Nx == d.Nx && d.g.h.Ny == d.Ny && d.g.h.Nz == d.Nz) return 1;
+    gpu_free(d);
+    if (!gpu_available()) {
+        std::fprintf(stderr, "semisim-b200: no CUDA device available - the solver has no CPU path\n");
+        return 0;
+    }
+    int dims[MAXLEV][6];
+    const int nl = mg_levels(d.Nx, d.Ny, d.Nz, dims);
+    Carver cv;
+    DevP P{};
+    std::vector<LevelT<double>> levs;
+    carve(d, cv, P, levs, nl, dims);              // sizing pass
+    const size_t bytes = cv.off;
+    void *blk = nullptr;
+    CK(cudaMalloc(&blk, bytes));
+    CK(cudaMemset(blk, 0, bytes));
+    Carver cv2;
+    cv2.base = static_cast<char *>(blk);
+    P = DevP{};
+    carve(d, cv2, P, levs, nl, dims);
+    P.Nx = d.Nx; P.Ny = d.Ny; P.Nz = d.Nz; P.N = (int)d.N; P.nlev = nl;
+    d.g.block = blk;
+    d.g.bytes = bytes;
+    d.g.N = d.N;
+    d.g.levs = levs;
+    d.g.h = P;
+    CK(cudaMalloc(&d.g.d, sizeof(DevP)));
+    CK(cudaStreamCreateWithFlags(&d.g.st, cudaStreamNonBlocking));
+    CK(cudaMallocHost(&d.g.pin, sizeof(double) * 256));
+    CK(cudaMalloc(&d.g.scratch, sizeof(double) * (d.N > 0 ? d.N : 1)));
+    CK(cudaMalloc(&d.g.flag, sizeof(int) * 16));
+    CK(cudaMemcpy(P.lev, levs.data(), sizeof(LevelT<double>) * nl, cudaMemcpyHostToDevice));
+    MGHost &mg = d.g.mg;
+    mg.maxlev = mg.minlev = nl;
+    for (int L = 0; L < nl; L++) mg.maxN[L] = levs[L].N;
+    d.g.ready = true;
+    return 1;
+}
+
+// ------------------------------------------------------------------ prepare
+// Contact node iteration over a node list, a face or a box (FOR_CON_ANY / FOR_CON_NODES,
+// semiconductor_3d.c:1045-1065, 1422-1426)
+template <class F>
+static void for_con_nodes(const Inst &d, const Contact &cn, F body) {
+    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
+    const int cid = int(&cn - d.cons);
+    if (cid >= 0 && cid < NC_MAX && !d.cnodes[cid].empty()) {
+        for (size_t q = 0; q < d.cnodes[cid].size(); q++) {
+            const size_t k = (size_t)d.cnodes[cid][q];
+            const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny);
+            body(rem % Nx, rem / Nx, l, k, d.careas[cid][q]);
+        }
+        return;
+    }
+    int ia = 0, ib = Nx - 1, ja = 0, jb = Ny - 1, la = 0, lb = Nz - 1;
+    switch (cn.face) {
+    case 0: ia = ib = 0; ja = cn.i0; jb = cn.i1; la = cn.j0; lb = cn.j1; break;
+    case 1: ia = ib = Nx - 1; ja = cn.i0; jb = cn.i1; la = cn.j0; lb = cn.j1; break;
+    case 2: ja = jb = 0; ia = cn.i0; ib = cn.i1; la = cn.j0; lb = cn.j1; break;
+    case 3: ja = jb = Ny - 1; ia = cn.i0; ib = cn.i1; la = cn.j0; lb = cn.j1; break;
+    case 4: la = lb = 0; ia = cn.i0; ib = cn.i1; ja = cn.j0; jb = cn.j1; break;
+    case 5: la = lb = Nz - 1; ia = cn.i0; ib = cn.i1; ja = cn.j0; jb = cn.j1; break;
+    default: ia = cn.i0; ib = cn.i1; ja = cn.j0; jb = cn.j1; la = cn.k0; lb = cn.k1;
+    }
+    if (ia < 0) ia = 0; if (ja < 0) ja = 0; if (la < 0) la = 0;
+    if (ib > Nx - 1) ib = Nx - 1; if (jb > Ny - 1) jb = Ny - 1; if (lb > Nz - 1) lb = Nz - 1;
+    for (int l = la; l <= lb; l++)
+        for (int j = ja; j <= jb; j++)
+            for (int i = ia; i <= ib; i++) {
+                const size_t k = (size_t)l * Nx * Ny + (size_t)j * Nx + i;
+                const double area = cn.face <= 1 ? d.Ly[j] * d.Lz[l]
+                                  : (cn.face <= 3 ? d.Lx[i] * d.Lz[l] : (cn.face <= 5 ? d.Lx[i] * d.Ly[j] : 0.));
+                body(i, j, l, k, area);
+            }
+}
+
+// Material band offsets in the common gauge (mat_prepare, semiconductor_3d.c:631-642)
+static void mat_prepare(Inst &d) {
+    d.ref_mat = 0;
+    for (int i = 0; i < d.n_mats; i++)
+        if (!d.mats[i].insulator) { d.ref_mat = i; break; }
+    const Material &r = d.mats[d.ref_mat];
+    d.Cref = r.insulator ? 4.6 : r.chi + 0.5 * r.Eg + 0.5 * r.VT * std::log(r.Nc / r.Nv);
+    for (int i = 0; i < d.n_mats; i++) {
+        Material &m = d.mats[i];
+        if (m.insulator) { m.lnc = m.lnv = -1e300; continue; }
+        m.lnc = std::log(m.Nc) + (m.chi - d.Cref) / m.VT;
+        m.lnv = std::log(m.Nv) + (d.Cref - m.chi - m.Eg) / m.VT;
+    }
+}
+
+// Reject inputs that need models this library does not build.
+static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
+    bool any_ins = false, any_gate = false;
+    for (size_t k = 0; k < d.N; k++) if (kind[k] == K_INS) { any_ins = true; break; }
+    for (int c = 0; c < d.n_cons; c++) if (d.cons[c].bc == 2) any_gate = true;
+    auto used = [&](int mi) {
+        for (size_t k = 0; k < d.N; k++) if (d.mat_idx[k] == mi && kind[k] == K_SEMI) return true;
+        return false;
+    };
+    const char *why = nullptr;
+    if (d.n_trap_entries > 0) why = "deep-level traps";
+    if ((d.models & 8) && (any_ins || any_gate)) why = "quantum confinement (models bit 3)";
+    if ((d.models & 32) && any_ins) why = "gate tunnelling (models bit 5)";
+    if (d.models & 64)
+        for (int c = 0; c < d.n_cons; c++)
+            if (d.cons[c].bc == 1 && d.cons[c].face <= 5) why = "thermionic-emission metal contacts (models bit 6)";
+    for (int mi = 0; mi < d.n_mats; mi++) {
+        const Material &m = d.mats[mi];
+        if (m.insulator) continue;
+        if ((d.models & 16) && m.lb_on && (any_ins || any_gate) && used(mi)) why = "surface mobility (models bit 4)";
+        if ((d.models & 256) && m.ii_on && used(mi)) why = "impact ionisation (models bit 8)";
+        if ((d.models & 512) && m.ion_on && used(mi)) why = "incomplete ionisation (models bit 9)";
+    }
+    if (why) {
+        std::fprintf(stderr, "semisim-b200: %s is not supported by this solver library\n", why);
+        return 0;
+    }
+    return 1;
+}
+
+// prepare (semiconductor_3d.c:1638-1775): node kinds, contact and gate masks, Robin gate
+// areas, contact areas, band-gap narrowing; uploaded to the device with the geometry.
+int prepare(Inst &d) {
+    if (!d.allocated || d.n_mats < 1) return 0;
+    if (!d.dirty && d.g.ready) return 1;       // set-up unchanged since the last upload
+    const size_t N = d.N;
+    mat_prepare(d);
+    std::vector<unsigned char> kind(N);
+    std::vector<int> con(N, 0), gate(N, 0);
+    d.bgn.assign(N, 0.0);
+    for (size_t k = 0; k < N; k++) {
+        int mi = d.mat_idx[k];
+        if (mi < 0 || mi >= d.n_mats) mi = d.mat_idx[k] = 0;
+        const Material &m = d.mats[mi];
+        kind[k] = m.insulator ? K_INS : K_SEMI;
+        d.bgn[k] = (!m.insulator && (d.models & 1)) ? bgn_half(m, d.Nd[k] + d.Na[k]) : 0.;
+    }
+    int nrob = 0;
+    for (int c = 0; c < d.n_cons; c++) {
+        Contact &cn = d.cons[c];
+        cn.A = 0.;
+        for_con_nodes(d, cn, [&](int, int, int, size_t k, double area) {
+            if (cn.face <= 5) cn.A += area;
+            if (cn.bc == 2 && cn.face <= 5 && kind[k] == K_SEMI) {
+                gate[k] = c + 1; nrob++;
+            } else if (cn.bc == 2 || kind[k] != K_SEMI) {
+                kind[k] = K_METAL; con[k] = c + 1; gate[k] = 0;
+            } else {
+                con[k] = c + 1; gate[k] = 0;
+            }
+        });
+    }
+    d.robA.assign(N, 0.0);
+    d.n_rob = 0;
+    for (int c = 0; c < d.n_cons; c++) {
+        const Contact &cn = d.cons[c];
+        if (cn.bc != 2 || cn.face > 5) continue;
+        for_con_nodes(d, cn, [&](int, int, int, size_t k, double area) {
+            if (gate[k] == c + 1 && !con[k] && d.n_rob < nrob && d.robA[k] == 0.0) {
+                d.robA[k] = area; d.n_rob++;
+            }
+        });
+    }
+    // box contacts: area = interface with non-contact semiconductor
+    for (int c = 0; c < d.n_cons; c++) {
+        Contact &cn = d.cons[c];
+        if (cn.face <= 5) continue;
+        double A = 0.;
+        for_con_nodes(d, cn, [&](int i, int j, int l, size_t k, double) {
+            if (con[k] != c + 1) return;
+            const int Nx = d.Nx, Ny = d.Ny;
+            const int ii[6] = {i - 1, i + 1, i, i, i, i}, jj[6] = {j, j, j - 1, j + 1, j, j}, ll[6] = {l, l, l, l, l - 1, l + 1};
+            for (int dir = 0; dir < 6; dir++) {
+                if (ii[dir] < 0 || ii[dir] >= Nx || jj[dir] < 0 || jj[dir] >= Ny || ll[dir] < 0 || ll[dir] >= d.Nz) continue;
+                const size_t kb = (size_t)ll[dir] * Nx * Ny + (size_t)jj[dir] * Nx + ii[dir];
+                const double ar = dir < 2 ? d.Ly[j] * d.Lz[l] : (dir < 4 ? d.Lx[i] * d.Lz[l] : d.Lx[i] * d.Ly[j]);
+                if (kind[kb] == K_SEMI && con[kb] != c + 1) A += ar;
+            }
+        });
+        cn.A = A;
+    }
+    if (!check_scope(d, kind)) return 0;
+    // flags, contact-node list, low-field mobility
+    d.flags.assign(N, 0);
+    d.cnode.clear();
+    d.mu0n.assign(N, 0.0);
+    d.mu0p.assign(N, 0.0);
+    for (size_t k = 0; k < N; k++) {
+        const bool fix = con[k] != 0;          // no thermionic-emission contacts: every contact node is fixed
+        d.flags[k] = make_flags(kind[k], con[k], gate[k], d.mat_idx[k], fix);
+        if (con[k] && kind[k] == K_SEMI) d.cnode.push_back((int)k);
+        if (kind[k] == K_SEMI) {
+            const Material &m = d.mats[d.mat_idx[k]];
+            const double Nt = d.Nd[k] + d.Na[k];
+            d.mu0n[k] = mobility_low(m, Nt, 0);
+            d.mu0p[k] = mobility_low(m, Nt, 1);
+        }
+    }
+    if (!gpu_alloc(d)) return 0;
+    // upload
+    DevP &P = d.g.h;
+    P.models = d.models; P.caxis = d.caxis; P.ncon = d.n_cons; P.ref_mat = d.ref_mat;
+    P.VTref = d.mats[d.ref_mat].VT; P.Cref = d.Cref;
+    P.ncnode = (int)d.cnode.size();
+    MatD md[NM_MAX];
+    std::memset(md, 0, sizeof md);
+    for (int i = 0; i < d.n_mats; i++) {
+        const Material &m = d.mats[i];
+        MatD &o = md[i];
+        o.VT = m.VT; o.lnc = m.lnc; o.lnv = m.lnv; o.ni = m.ni; o.eps = m.eps_r * EPS0;
+        o.tau_n0 = m.tau_n0; o.tau_p0 = m.tau_p0; o.Cn = m.Cn; o.Cp = m.Cp; o.Brad = m.Brad; o.tau_Nref = m.tau_Nref;
+        o.vsat_n = m.vsat_n; o.vsat_p = m.vsat_p; o.beta_n = m.beta_n; o.beta_p = m.beta_p;
+        o.ani_n = m.ani_n; o.ani_p = m.ani_p; o.chi = m.chi; o.Eg = m.Eg; o.insulator = m.insulator;
+    }
+    cudaStream_t st = d.g.st;
+    CK(cudaMemcpyAsync((void *)P.mats, md, sizeof md, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.flags, d.flags.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.Nd, d.Nd.data(), N * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.Na, d.Na.data(), N * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.Nf, d.Nf.data(), N * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.bgn, d.bgn.data(), N * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.robA, d.robA.data(), N * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(P.mu0n, d.mu0n.data(), N * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(P.mu0p, d.mu0p.data(), N * 8, cudaMemcpyHostToDevice, st));
+    if (!d.cnode.empty())
+        CK(cudaMemcpyAsync((void *)P.cnode, d.cnode.data(), d.cnode.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.xs, d.xs.data(), d.Nx * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.ys, d.ys.data(), d.Ny * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.zs, d.zs.data(), d.Nz * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.Lx, d.Lx.data(), d.Nx * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.Ly, d.Ly.data(), d.Ny * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.Lz, d.Lz.data(), d.Nz * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d.g.d, &P, sizeof(DevP), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    d.g.mg.alpha = g_knobs.mg_alpha;
+    d.dirty = 0;
+    return 1;
+}
+
+void upload_voltages(Inst &d, const double *Va) {
+    ConD cd[NC_MAX];
+    std::memset(cd, 0, sizeof cd);
+    for (int c = 0; c < d.n_cons; c++) {
+        cd[c].V = Va[c]; cd[c].phi_m = d.cons[c].phi_m; cd[c].tox = d.cons[c].tox;
+        cd[c].qox = d.cons[c].qox; cd[c].bc = d.cons[c].bc;
+    }
+    cudaMemcpyAsync((void *)d.g.h.cons, cd, sizeof(ConD) * (d.n_cons > 0 ? d.n_cons : 1), cudaMemcpyHostToDevice,
+                    d.g.st);
+    cudaStreamSynchronize(d.g.st);     // cd is a stack buffer
+}
+
+// ------------------------------------------------------------------ small pieces
+void set_vrange(Inst &d, const double *Va) {   // semiconductor_3d.c:3660-3668
+    int any = 0;
+    double lo = 0., hi = 0.;
+    for (int c = 0; c < d.n_cons; c++) {
+        if (d.cons[c].bc == 2) continue;       // a gate without tunnelling is no carrier terminal
+        if (!any) { lo = hi = Va[c]; any = 1; }
+        else { if (Va[c] < lo) lo = Va[c]; if (Va[c] > hi) hi = Va[c]; }
+    }
+    d.vlo = lo; d.vhi = hi;
+}
+static double newton_tol(const Inst &d, const double *Va) {   // semiconductor_3d.c:3670-3674
+    double s = 1.;
+    for (int c = 0; c < d.n_cons; c++) if (std::fabs(Va[c]) > s) s = std::fabs(Va[c]);
+    return 2e-14 + 2e-15 * s;
+}
+void apply_bc(Inst &d, const double *Va) {
+    upload_voltages(d, Va);
+    launch_apply_bc(make_ctx(d), d.have_solution);
+}
+void clamp_qf(Inst &d) {
+    launch_clamp_qf(make_ctx(d), d.vlo - g_knobs.qf_margin, d.vhi + g_knobs.qf_margin);
+}
+void rebuild_np(Inst &d) { launch_rebuild_np(make_ctx(d)); }
+void upd_mob(Inst &d) { launch_upd_mob(make_ctx(d)); }
+
+void terminal_currents(Inst &d, double *I, double *S) {
+    Ctx c = make_ctx(d);
+    const int nc = d.n_cons;
+    launch_currents(c);
+    cudaMemcpyAsync(d.g.pin, d.g.h.res, sizeof(double) * R_TOTAL, cudaMemcpyDeviceToHost, d.g.st);
+    cudaStreamSynchronize(d.g.st);
+    for (int q = 0; q < nc; q++) {
+        I[q] = d.g.pin[R_I + q];
+        S[q] = d.g.pin[R_S + q];
+        d.cons[q].In = d.g.pin[R_IN + q];
+    }
+}
+
+static void copy_dev(Inst &d, double *dst, const double *src) {
+    cudaMemcpyAsync(dst, src, d.N * 8, cudaMemcpyDeviceToDevice, d.g.st);
+}
+static void save_state(Inst &d, double *const *h) {
+    copy_dev(d, h[0], d.g.h.phi); copy_dev(d, h[1], d.g.h.phin); copy_dev(d, h[2], d.g.h.phip);
+}
+static void load_state(Inst &d, double *const *h) {
+    copy_dev(d, d.g.h.phi, h[0]); copy_dev(d, d.g.h.phin, h[1]); copy_dev(d, d.g.h.phip, h[2]);
+}
+
+// ------------------------------------------------------------------ Newton-Poisson
+// Damped Newton with PCG and a backtracking line search on ||F/diag||
+// (semiconductor_3d.c:2791-2823)
+static int poisson_newton(Inst &d, const double *Va, double ntol, int maxit) {
+    Ctx c = make_ctx(d);
+    upload_voltages(d, Va);
+    for (int it = 0; it < maxit; it++) {
+        d.newton_its++;
+        launch_poisson(c, nullptr, 1, nullptr);
+        const double f0 = read_res(d, R_PNORM);
+        if (!(f0 > 0.)) return f0 == 0.;
+        launch_fill_sel(c, V_SOL, 0.0);
+        const int its = pcg_solve(c, d.g.mg, d.max_iter_p > 0 ? d.max_iter_p : 2000, d.pcg_rtol, g_knobs.check_every);
+        d.pcg_its += its;
+        launch_absmax_sel(c, V_SOL, R_DMAX);
+        const double dm = read_res(d, R_DMAX);
+        if (dm != dm) return 0;
+        if (dm < ntol) {
+            launch_axpy_sel(c, V_PHI, V_PHI, 1.0, V_SOL);   // psi += dx
+            return 1;
+        }
+        double lam = 1.;
+        for (int ls = 0; ls < 40; ls++) {
+            launch_axpy_sel(c, V_TR, V_PHI, lam, V_SOL);    // trial psi + lam dx
+            launch_poisson(c, d.g.h.tr, 0, nullptr);
+            const double f1 = read_res(d, R_PNORM);
+            if (f1 <= (1. - 1e-4 * lam) * f0) break;
+            lam *= 0.5;
+        }
+        cudaMemcpyAsync(d.g.h.phi, d.g.h.tr, d.N * 8, cudaMemcpyDeviceToDevice, d.g.st);
+        if (d.verbose > 4) std::fprintf(stderr, "      newton it=%d f0=%.3e dm=%.3e lam=%.3e\n", it, f0, dm, lam);
+        if (lam * dm < ntol) return 1;
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------ floating blocks
+int float_fix(Inst &d, int hole);   // kernels_ccl.cu
+
+// ------------------------------------------------------------------ continuity
+// assemble -> BiCGSTAB from u = 1 (ILU-only retry, keep the start if worse) ->
+// floating-block balance -> update (semiconductor_3d.c:2216-2232, 3580-3594)
+static int solve_cont(Inst &d, int hole, double lo, double hi, double *dmax) {
+    Ctx c = make_ctx(d);
+    launch_cont_assemble(c, hole);
+    launch_fill_sel(c, V_SOL, 1.0);
+    const double atol = g_knobs.cont_atol * d.cont_atol_f;
+    const int maxit = d.max_iter_c > 0 ? d.max_iter_c : 1000;
+    launch_copy_sel(c, 7, V_SOL);                        // x0 backup
+    double rn = 0, r0 = 0;
+    int its = bicgstab_core(c, d.g.mg, maxit, d.bicg_rtol, atol, 1, g_knobs.check_every, &rn, &r0, hole ? -1 : 1);
+    if (!(rn <= std::fmax(r0, 1e-300)) && d.g.mg.maxlev > 1) {
+        if (d.verbose) std::fprintf(stderr, "semisim-b200: MG-BiCGSTAB diverged (%.2e > %.2e), retry ILU\n", rn, r0);
+        launch_copy_sel(c, V_SOL, 7);
+        its += bicgstab_core(c, d.g.mg, 4 * maxit, d.bicg_rtol, atol, 0, g_knobs.check_every, &rn, &r0, hole ? -1 : 1);
+    }
+    d.bicg_its += its;
+    if (!(rn <= std::fmax(r0, 1e-300)) || !std::isfinite(rn)) {
+        launch_copy_sel(c, V_SOL, 7);
+        rn = INFINITY;
+    }
+    if (d.verbose > 2) std::fprintf(stderr, "    bicgstab(%c) its=%d |r|=%.3e\n", hole ? 'p' : 'n', its, rn);
+    const int ok = std::isfinite(rn);
+    if (ok) float_fix(d, hole);
+    launch_cont_update(c, hole, lo, hi);
+    *dmax = read_res(d, R_DQ);
+    return ok;
+}
+
+// ------------------------------------------------------------------ Anderson
+static void aa_reset(Inst &d) { d.aa_n = 0; d.aa_pos = 0; d.aa_have = 0; }
+static void aa_step(Inst &d) {                      // semiconductor_3d.c:3709-3757
+    Ctx c = make_ctx(d);
+    const int M = d.aa_m < g_knobs.aa_depth ? d.aa_m : g_knobs.aa_depth;
+    if (M > 0 && d.aa_have) {
+        const int s = d.aa_pos;
+        if (d.aa_n < M) d.aa_n++;
+        aa_update_history(c, s, d.aa_n);
+        d.aa_pos = (s + 1) % M;
+    }
+    aa_store_fg(c);
+    d.aa_have = 1;
+    const int m = d.aa_n;
+    if (m == 0) return;
+    aa_solve_mix(c, m, nullptr);
+}
+
+// ------------------------------------------------------------------ Gummel
+// One Gummel solve at fixed terminal voltages (semiconductor_3d.c:3781-3930; the
+// impact-ionisation and metal-contact branches belong to models this library does not
+// build)
+static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters, double *res) {
+    Ctx c = make_ctx(d);
+    const int nc = d.n_cons;
+    const double lo = d.vlo - g_knobs.qf_margin, hi = d.vhi + g_knobs.qf_margin, nt0 = newton_tol(d, Va);
+    double I[NC_MAX], S[NC_MAX], Iold[NC_MAX];
+    int haveI = 0;
+    const double itol = d.tol_c > 0. ? d.tol_c : 1e-6;
+    apply_bc(d, Va);
+    aa_reset(d);
+    poisson_newton(d, Va, std::fmax(nt0, 1e-6), 100);
+    int it, conv = 0, it_mark = 0;
+    double dpsi = 1., dq = 1., best = 1e300, prev = 1., best_mark = 1e300;
+    for (it = 1; it <= maxit; it++) {
+        if (g_stop.load()) break;
+        const double t0 = wtime();
+        clamp_qf(d);
+        copy_dev(d, d.g.h.qn0, d.g.h.phin);
+        copy_dev(d, d.g.h.qp0, d.g.h.phip);
+        rebuild_np(d);
+        upd_mob(d);
+        const double t1 = wtime();
+        d.t_mob += t1 - t0;
+        double dn = 0., dp = 0.;
+        if (!solve_cont(d, 0, lo, hi, &dn)) break;
+        if (!solve_cont(d, 1, lo, hi, &dp)) break;
+        const double t2 = wtime();
+        d.t_cont += t2 - t1;
+        dq = std::fmax(dn, dp);
+        terminal_currents(d, I, S);
+        d.t_cur += wtime() - t2;
+        int icv = haveI;
+        if (haveI)
+            for (int q = 0; q < nc; q++)
+                if (std::fabs(I[q] - Iold[q]) > std::fmax(itol * std::fabs(I[q]), 3e-14 * S[q])) icv = 0;
+        std::memcpy(Iold, I, sizeof(double) * nc);
+        haveI = 1;
+        launch_predictor(c);                               // xk = psi; neutral-region predictor
+        const double ntol = std::fmax(nt0, d.ntol_fac * std::fmin(prev, 1.));
+        const double t3 = wtime();
+        poisson_newton(d, Va, ntol, 100);
+        d.t_pois += wtime() - t3;
+        launch_dpsi(c);
+        dpsi = read_res(d, R_DPSI);
+        if (d.verbose > 1)
+            std::fprintf(stderr, "  gummel %3d dpsi=%.3e dq=%.3e I0=%.6e aa=%d\n", it, dpsi, dq, nc ? I[0] : 0., d.aa_n);
+        if (dpsi != dpsi || dq != dq) break;
+        const double r = std::fmax(dpsi, dq);
+        g_prog[1] = it; g_prog[2] = r; g_prog[5] = (double)(d.gummel_its + it);
+        if (dq < gtol && dpsi < gtol && icv) {            // accept psi_k with its carriers
+            copy_dev(d, d.g.h.phi, d.g.h.xk);
+            conv = 1;
+            break;
+        }
+        prev = r;
+        if (r < 0.5 * best_mark) { best_mark = r; it_mark = it; }
+        if (it - it_mark > 20 && r <= 1e3 * gtol && icv) {
+            copy_dev(d, d.g.h.phi, d.g.h.xk);
+            conv = 1;
+            if (d.verbose) std::fprintf(stderr, "semisim-b200: accepted at noise floor (res %.2e)\n", r);
+            break;
+        }
+        if (it - it_mark > 60) break;
+        if (r < best) best = r;
+        else if (r > 30. * best) aa_reset(d);
+        const double t4 = wtime();
+        aa_step(d);
+        d.t_aa += wtime() - t4;
+    }
+    if (it > maxit) it = maxit;
+    cudaStreamSynchronize(d.g.st);
+    d.gummel_its += it;
+    *iters = it;
+    *res = std::fmax(dpsi, dq);
+    return conv;
+}
+
+// ------------------------------------------------------------------ continuation
+static void region_shift(Inst &d, const double *dV) {      // semiconductor_3d.c:3956-3987
+    Ctx c = make_ctx(d);
+    int *mark = d.g.h.ccl;
+    cudaMemsetAsync(mark, 0, d.N * sizeof(int), d.g.st);
+    for (int q = 0; q < d.n_cons; q++) {
+        if (d.cons[q].bc != 0 || std::fabs(dV[q]) < 1e-15) continue;
+        int type = 0;
+        for (size_t k = 0; k < d.N && !type; k++) {
+            const uint32_t f = d.flags[k];
+            if (fl_con(f) == q + 1 && fl_kind(f) == K_SEMI) {
+                const double D = d.Nd[k] - d.Na[k];
+                type = D > 0. ? 1 : (D < 0. ? -1 : 0);
+            }
+        }
+        if (!type) continue;
+        launch_region_mark(c, q + 1, type, dV[q], mark, d.g.flag);
+    }
+}
+
+int equilibrium(Inst &d) {                                  // semiconductor_3d.c:3989-4004
+    double Va[NC_MAX];
+    d.e_n = 0;
+    for (int q = 0; q < d.n_cons; q++) Va[q] = d.cons[q].bc == 2 ? d.cons[q].V : 0.;
+    Ctx c = make_ctx(d);
+    launch_init_eq(c);
+    set_vrange(d, Va);
+    apply_bc(d, Va);
+    g_prog[4] = 1.;
+    const int ok = poisson_newton(d, Va, newton_tol(d, Va), 300);
+    rebuild_np(d);
+    upd_mob(d);
+    for (int q = 0; q < d.n_cons; q++) d.cons[q].Vprev = Va[q];
+    d.have_solution = 1;
+    if (d.verbose) std::fprintf(stderr, "semisim-b200: equilibrium %s (newton its %lld)\n", ok ? "ok" : "NOT converged", d.newton_its);
+    return ok;
+}
+
+static double gummel_tol(const Inst &d) {
+    double g = d.tol_p;
+    if (!(g > 0.)) g = 1e-9;
+    if (g > 1e-4) g = 1e-4;
+    if (g < 1e-13) g = 1e-13;
+    return g;
+}
+
+// Adaptive continuation from Vprev to V, all contacts together, with the secant sweep
+// predictor (semiconductor_3d.c:4018-4133)
+static int cont_path(Inst &d) {
+    const int nc = d.n_cons;
+    double Vf[NC_MAX], Vt[NC_MAX], Va[NC_MAX], dV[NC_MAX];
+    double span = 0.;
+    for (int q = 0; q < nc; q++) {
+        Vf[q] = d.cons[q].Vprev; Vt[q] = d.cons[q].V;
+        if (std::fabs(Vt[q] - Vf[q]) > span) span = std::fabs(Vt[q] - Vf[q]);
+    }
+    const int maxg = d.max_gummel > 0 ? d.max_gummel : 100;
+    const double gtol = gummel_tol(d);
+    Ctx c = make_ctx(d);
+    upd_mob(d);
+    save_state(d, d.g.h.h1);
+    double rx = 0.;
+    if (g_knobs.pred_on && d.e_n >= 1 && span > 0.) {
+        double num = 0., den = 0., err = 0.;
+        int same = 1;
+        for (int q = 0; q < nc; q++) {
+            const double a = Vt[q] - Vf[q], b = Vf[q] - d.Ve2[q];
+            num += a * b; den += b * b;
+            if (std::fabs(Vf[q] - d.Ve1[q]) > 1e-12) same = 0;
+        }
+        if (same && den > 0.) {
+            const double r = num / den;
+            for (int q = 0; q < nc; q++) {
+                const double a = Vt[q] - Vf[q], b = Vf[q] - d.Ve2[q];
+                err = std::fmax(err, std::fabs(a - r * b));
+            }
+            if (r >= -2. && r <= 3. && std::fabs(r) > 1e-12 && err <= 1e-9 + 1e-6 * span) rx = r;
+        }
+    }
+    int first = 1;
+    double t = 0., tp = -1., dt = span > 0. ? std::fmin(1., 0.1 / span) : 1.;
+    int ok_all = 0, its = 0, steps = 0;
+    double res = 0.;
+    g_prog[0] = 0.; g_prog[3] = 0.;
+    for (int guard = 0; guard < 5000; guard++) {
+        if (g_stop.load()) break;
+        const double tn = std::fmin(1., t + dt);
+        for (int q = 0; q < nc; q++) Va[q] = Vf[q] + tn * (Vt[q] - Vf[q]);
+        set_vrange(d, Va);
+        if (tp >= 0.) {
+            launch_extrap(c, (tn - t) / (t - tp), 0, 1);
+        } else if (rx != 0.) {
+            launch_extrap(c, tn * rx, 0, 2);
+        } else {
+            load_state(d, d.g.h.h1);
+            if (span > 0.) {
+                for (int q = 0; q < nc; q++) dV[q] = (tn - t) * (Vt[q] - Vf[q]);
+                region_shift(d, dV);
+            }
+        }
+        if (first) {
+            for (int a = 0; a < 3; a++) copy_dev(d, d.g.h.e2[a], d.g.h.h1[a]);
+            first = 0;
+        }
+        clamp_qf(d);
+        apply_bc(d, Va);
+        rebuild_np(d);
+        const int ok = gummel(d, Va, maxg, gtol, &its, &res);
+        d.conv_iter = its;
+        d.conv_res = res;
+        if (d.verbose)
+            std::fprintf(stderr, "semisim-b200: step t=%.4f (V0=%.4f) %s its=%d res=%.2e\n", tn, nc ? Va[0] : 0.,
+                         ok ? "ok" : "FAIL", its, res);
+        if (ok) {
+            for (int a = 0; a < 3; a++) std::swap(d.g.h.h1[a], d.g.h.h2[a]);
+            cudaMemcpyAsync(d.g.d, &d.g.h, sizeof(DevP), cudaMemcpyHostToDevice, d.g.st);
+            c = make_ctx(d);
+            save_state(d, d.g.h.h1);
+            tp = t; t = tn; steps++;
+            g_prog[0] = t; g_prog[3] = steps;
+            for (int q = 0; q < nc; q++) d.cons[q].Vprev = Va[q];
+            if (t >= 1.) { ok_all = 1; break; }
+            dt *= its <= 8 ? 2.0 : (its <= 25 ? 1.5 : g_knobs.grow_slow);
+        } else {
+            rx = 0.;
+            if (span == 0. || dt * span < 2e-5) break;
+            dt *= 0.3;
+        }
+    }
+    if (ok_all && span > 0.) {
+        for (int q = 0; q < nc; q++) { d.Ve2[q] = Vf[q]; d.Ve1[q] = Vt[q]; }
+        d.e_n = d.e_n < 2 ? d.e_n + 1 : 2;
+    } else if (!ok_all) d.e_n = 0;
+    if (!ok_all && (span > 0. || g_stop.load())) {
+        load_state(d, d.g.h.h1);
+        for (int q = 0; q < nc; q++) Va[q] = d.cons[q].Vprev;
+        set_vrange(d, Va);
+        apply_bc(d, Va);
+        rebuild_np(d);
+        upd_mob(d);
+        if (d.verbose) std::fprintf(stderr, "semisim-b200: continuation stopped at t=%.4f\n", t);
+    }
+    cudaStreamSynchronize(d.g.st);
+    return ok_all;
+}
+
+// Gate-first bias path, then terminal currents with the Kirchhoff choice and their
+// resolution floors (semiconductor_3d.c:4135-4173)
+int run_continuation(Inst &d) {
+    const int nc = d.n_cons;
+    int gch = 0, cch = 0, ok_all;
+    for (int q = 0; q < nc; q++) {
+        if (std::fabs(d.cons[q].V - d.cons[q].Vprev) <= 1e-12) continue;
+        if (d.cons[q].bc == 2) gch = 1;
+        else cch = 1;
+    }
+    if (gch && cch) {
+        double Vt[NC_MAX];
+        for (int q = 0; q < nc; q++) {
+            Vt[q] = d.cons[q].V;
+            if (d.cons[q].bc != 2) d.cons[q].V = d.cons[q].Vprev;
+        }
+        g_prog[4] = 2.;
+        ok_all = cont_path(d);
+        for (int q = 0; q < nc; q++) d.cons[q].V = Vt[q];
+        g_prog[4] = 3.;
+        if (ok_all) ok_all = cont_path(d);
+    } else {
+        g_prog[4] = gch ? 2. : 3.;
+        ok_all = cont_path(d);
+    }
+    double I[NC_MAX], S[NC_MAX];
+    terminal_currents(d, I, S);
+    double ks = 0., F = 0., fl[NC_MAX];
+    int ncar = 0;
+    for (int q = 0; q < nc; q++) {
+        ks += I[q]; fl[q] = 3e-14 * S[q]; F += fl[q];
+        if (d.cons[q].bc != 2) ncar++;
+    }
+    const double scl = F > 0. ? std::fmax(1., 2. * std::fabs(ks) / F) : 1.;
+    for (int q = 0; q < nc; q++) {
+        double Iv = I[q], fv = fl[q];
+        const double fo = F - fl[q];
+        if (d.cons[q].bc != 2 && ncar > 1 && fo < fv) { Iv = -(ks - I[q]); fv = fo; }
+        d.cons[q].I = Iv;
+        d.cons[q].Iflr = fv * scl;
+        d.cons[q].Iraw = I[q];
+    }
+    return ok_all;
+}
+
+void finish_point(Inst &d) {
+    Ctx c = make_ctx(d);
+    launch_upd_J(c);
+    launch_mob_display(c);
+    cudaStreamSynchronize(d.g.st);
+    for (auto &v : d.cache_ok) v = 0;
+}
+
+int do_solve(Inst &d, int keep) {                           // semiconductor_3d.c:4910-4916
+    if (!prepare(d)) return 0;
+    if (!keep || !d.have_solution) equilibrium(d);
+    const int ok = run_continuation(d);
+    finish_point(d);
+    d.converged = ok;
+    g_prog[4] = 0.;
+    return ok;
+}
+
+}  // namespace ss

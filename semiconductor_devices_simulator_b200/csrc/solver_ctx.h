@@ -1,0 +1,133 @@
+// Host-side state of one simulated device and its GPU buffers.
+#pragma once
+#include <atomic>
+#include <cstdint>
+#include <vector>
+
+#include "kernels.h"
+#include "materials.h"
+#include "semisim.h"
+
+namespace ss {
+
+// level-0 vector selectors understood by the linear-algebra kernels (0..7 = DevP::wk)
+enum VecSel { V_RHS = 8, V_SOL = 9, V_F = 10, V_TR = 11, V_DSC = 12, V_PHI = 13 };
+
+// multigrid shape over all instances of a launch
+struct MGHost {
+    int maxlev = 0, minlev = 0;
+    int maxN[MAXLEV] = {0};
+    double alpha = 1.0;
+};
+
+struct Contact {
+    int face = 0, i0 = 0, i1 = 0, j0 = 0, j1 = 0, k0 = 0, k1 = 0, bc = 0;
+    double V = 0, phi_m = 0, tox = 10e-9, qox = 0;
+    double Vprev = 0, I = 0, A = 0, In = 0, Iflr = 0, Iraw = 0;
+    int snl = 0;                 // gate stack layers (tunnelling, not built)
+};
+
+struct Gpu {
+    bool ready = false;
+    int dev = 0;
+    size_t N = 0, bytes = 0;
+    void *block = nullptr;       // one allocation for all node arrays
+    DevP h{};                    // host copy of the device record
+    DevP *d = nullptr;           // device record
+    MGHost mg;
+    std::vector<LevelT<double>> levs;
+    cudaStream_t st = nullptr;
+    double *pin = nullptr;       // pinned host scratch (results)
+    double *scratch = nullptr;   // device scratch (bulk output)
+    int *flag = nullptr;         // device int scratch
+};
+
+struct Inst {
+    // ---- configuration (the reference's Dev, semiconductor_3d.c:234-364)
+    int Nx = 0, Ny = 0, Nz = 0;
+    size_t N = 0;
+    std::vector<double> xs, ys, zs, Lx, Ly, Lz;
+    std::vector<int> mat_idx;
+    std::vector<double> Nd, Na, Nf;
+    Material mats[NM_MAX];
+    int n_mats = 0;
+    Contact cons[NC_MAX];
+    int n_cons = 0;
+    std::vector<int> cnodes[NC_MAX];       // node-list contacts (api3_set_con_nodes)
+    std::vector<double> careas[NC_MAX];
+    int max_iter_p = 2000, max_iter_c = 1000, max_gummel = 500;
+    double tol_p = 1e-9, tol_c = 1e-6, omega_p = 1, omega_c = 1;
+    int converged = 0, conv_iter = 0;
+    double conv_res = 0;
+    int allocated = 0, have_solution = 0, dirty = 1, verbose = 0;
+    double vlo = 0, vhi = 0;
+    long long pcg_its = 0, bicg_its = 0, newton_its = 0, gummel_its = 0;
+    double t_pois = 0, t_cont = 0, t_mob = 0, t_cur = 0, t_aa = 0, t_mg = 0;
+    double pcg_rtol = 1e-3, ntol_fac = 0.1, bicg_rtol = 1e-4, cont_atol_f = 1;
+    int nthreads = 1, caxis = 1, models = 7;
+    int n_trap_entries = 0;
+    double Cref = 0;
+    int ref_mat = 0;
+    double Ve1[NC_MAX] = {0}, Ve2[NC_MAX] = {0};
+    int e_n = 0;
+    int aa_m = 0, aa_n = 0, aa_pos = 0, aa_have = 0;
+    // ---- derived by prepare (host copies)
+    std::vector<uint32_t> flags;
+    std::vector<double> bgn, robA, mu0n, mu0p;
+    std::vector<int> cnode;
+    int n_rob = 0;
+    // ---- device
+    Gpu g;
+    // host mirrors of device results for the getters (valid while `mirror_ok`)
+    std::vector<std::vector<double>> cache;
+    std::vector<int> cache_ok;
+};
+
+// global knobs (the reference's static tunables, read by api3_init)
+struct Knobs {
+    double mg_alpha = 1.0;
+    int aa_depth = AA_MAX;
+    int pred_on = 1;
+    double grow_slow = 2.2;
+    double cont_atol = 2e-14;
+    double qf_margin = 0.0;
+    int check_every = 1;        // Krylov iterations queued between status reads
+};
+extern Knobs g_knobs;
+extern std::atomic<int> g_stop;
+extern volatile double g_prog[8];
+
+// solver entry points (solver.cpp)
+bool gpu_available();
+int prepare(Inst &d);
+int equilibrium(Inst &d);
+int run_continuation(Inst &d);
+int do_solve(Inst &d, int keep);
+void finish_point(Inst &d);
+void set_vrange(Inst &d, const double *Va);
+void upload_voltages(Inst &d, const double *Va);
+void apply_bc(Inst &d, const double *Va);
+void clamp_qf(Inst &d);
+void rebuild_np(Inst &d);
+void upd_mob(Inst &d);
+void terminal_currents(Inst &d, double *I, double *S);
+Ctx make_ctx(Inst &d);
+void gpu_free(Inst &d);
+
+// linear-algebra drivers (kernels_la.cu)
+void mg_setup(const Ctx &c, const MGHost &mg, int qsign);
+void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate);
+int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every);
+int bicgstab_core(const Ctx &c, const MGHost &mg, int maxit, double rtol, double atol, int mg_on, int check_every,
+                  double *rn, double *r0, int qsign);
+void launch_absmax_sel(const Ctx &c, int xsel, int slot);
+void launch_axpy_sel(const Ctx &c, int ysel, int xsel, double a, int zsel);
+void launch_fill_sel(const Ctx &c, int ysel, double v);
+void launch_copy_sel(const Ctx &c, int ysel, int xsel);
+
+// Anderson (kernels_aa.cu)
+void aa_update_history(const Ctx &c, int slot, int nfill);
+void aa_store_fg(const Ctx &c);
+void aa_solve_mix(const Ctx &c, int m, int *ok_host);
+
+}  // namespace ss

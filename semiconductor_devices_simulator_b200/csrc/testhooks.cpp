@@ -1,0 +1,188 @@
+// Kernel-level test hooks (b200x_*): run one device kernel of the solve path on the
+// prepared global device and copy its inputs / outputs through caller buffers.  The
+// parity tests use them to compare every kernel with the oracle on seeded states.
+// They are not part of the reference ABI.
+#include <cmath>
+#include <cstring>
+
+#include "solver_ctx.h"
+
+using namespace ss;
+
+namespace ss {
+int float_fix(Inst &d, int hole);
+}
+namespace {
+Inst *dev();
+}
+extern Inst *b200_global_dev();
+
+namespace {
+Inst *dev() { return b200_global_dev(); }
+double *arr(Inst &d, int which) {
+    DevP &P = d.g.h;
+    switch (which) {
+    case 0: return P.phi; case 1: return P.phin; case 2: return P.phip;
+    case 3: return P.n; case 4: return P.p; case 5: return P.mu0n; case 6: return P.mu0p;
+    case 7: return P.sol; case 8: return P.rhs; case 9: return P.sc; case 10: return P.dsc;
+    }
+    if (which >= 16 && which < 22) return P.fmu[which - 16];
+    return nullptr;
+}
+void dump7(Inst &d, double *const *A, size_t n, double *A7) {
+    if (!A7) return;
+    for (int q = 0; q < 7; q++) cudaMemcpyAsync(A7 + q * n, A[q], n * 8, cudaMemcpyDeviceToHost, d.g.st);
+}
+void sync(Inst &d) { cudaStreamSynchronize(d.g.st); }
+double res(Inst &d, int slot) {
+    double v = 0;
+    cudaMemcpyAsync(&v, d.g.h.res + slot, 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    return v;
+}
+void voltages(Inst &d) {
+    double Va[NC_MAX];
+    for (int c = 0; c < d.n_cons; c++) Va[c] = d.cons[c].V;
+    set_vrange(d, Va);
+    upload_voltages(d, Va);
+}
+}  // namespace
+
+extern "C" {
+
+int b200x_prepare(void) {
+    Inst &d = *dev();
+    if (!prepare(d)) return 0;
+    voltages(d);
+    return 1;
+}
+int b200x_masks(int *kind, int *con, int *gate, double *robA) {
+    Inst &d = *dev();
+    if (d.flags.size() != d.N) return 0;
+    for (size_t k = 0; k < d.N; k++) {
+        kind[k] = fl_kind(d.flags[k]); con[k] = fl_con(d.flags[k]); gate[k] = fl_gate(d.flags[k]);
+        if (robA) robA[k] = d.robA.empty() ? 0.0 : d.robA[k];
+    }
+    return 1;
+}
+int b200x_set(int which, const double *in) {
+    Inst &d = *dev();
+    double *a = arr(d, which);
+    if (!a) return 0;
+    cudaMemcpyAsync(a, in, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
+    sync(d);
+    return 1;
+}
+int b200x_get(int which, double *out) {
+    Inst &d = *dev();
+    double *a = arr(d, which);
+    if (!a) return 0;
+    cudaMemcpyAsync(out, a, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    return 1;
+}
+double b200x_vlo(void) { return dev()->vlo; }
+double b200x_vhi(void) { return dev()->vhi; }
+void b200x_apply_bc(void) {
+    Inst &d = *dev();
+    double Va[NC_MAX];
+    for (int c = 0; c < d.n_cons; c++) Va[c] = d.cons[c].V;
+    set_vrange(d, Va);
+    apply_bc(d, Va);
+    sync(d);
+}
+void b200x_rebuild_np(void) { rebuild_np(*dev()); sync(*dev()); }
+void b200x_upd_mob(void) { upd_mob(*dev()); sync(*dev()); }
+void b200x_clamp_qf(void) { clamp_qf(*dev()); sync(*dev()); }
+
+// F, stencil and sc of the Poisson system at psi (build) and ||F/diag||
+double b200x_poisson(const double *phi, double *F, double *A7, double *sc) {
+    Inst &d = *dev();
+    voltages(d);
+    Ctx c = make_ctx(d);
+    cudaMemcpyAsync(d.g.h.phi, phi, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
+    launch_poisson(c, nullptr, 1, nullptr);
+    const double nrm = res(d, R_PNORM);
+    if (F) cudaMemcpyAsync(F, d.g.h.rhs, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    dump7(d, d.g.h.A, d.N, A7);
+    if (sc) cudaMemcpyAsync(sc, d.g.h.sc, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    return nrm;
+}
+void b200x_cont_assemble(int hole, double *A7, double *rhs, double *sc, double *dsc) {
+    Inst &d = *dev();
+    Ctx c = make_ctx(d);
+    launch_cont_assemble(c, hole);
+    dump7(d, d.g.h.A, d.N, A7);
+    if (rhs) cudaMemcpyAsync(rhs, d.g.h.rhs, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    if (sc) cudaMemcpyAsync(sc, d.g.h.sc, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    if (dsc) cudaMemcpyAsync(dsc, d.g.h.dsc, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+}
+double b200x_cont_update(int hole, const double *sol, double lo, double hi, double *dq) {
+    Inst &d = *dev();
+    Ctx c = make_ctx(d);
+    cudaMemcpyAsync(d.g.h.sol, sol, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
+    launch_cont_update(c, hole, lo, hi);
+    const double dm = res(d, R_DQ);
+    if (dq) cudaMemcpyAsync(dq, hole ? d.g.h.dqp : d.g.h.dqn, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    return dm;
+}
+void b200x_currents(double *I, double *S, double *In) {
+    Inst &d = *dev();
+    double Iw[NC_MAX], Sw[NC_MAX];
+    terminal_currents(d, Iw, Sw);
+    for (int c = 0; c < d.n_cons; c++) { I[c] = Iw[c]; S[c] = Sw[c]; if (In) In[c] = d.cons[c].In; }
+}
+// multigrid hierarchy of the system now in A (qsign 0 Poisson, +-1 continuity)
+int b200x_mg_setup(int qsign) {
+    Inst &d = *dev();
+    mg_setup(make_ctx(d), d.g.mg, qsign);
+    sync(d);
+    return d.g.mg.maxlev;
+}
+int b200x_mg_level(int L, int *dims, double *A7, double *pw) {
+    Inst &d = *dev();
+    if (L < 0 || L >= (int)d.g.levs.size()) return 0;
+    const LevelT<double> &v = d.g.levs[L];
+    if (dims) { dims[0] = v.Nx; dims[1] = v.Ny; dims[2] = v.Nz; dims[3] = v.cx; dims[4] = v.cy; dims[5] = v.cz; }
+    dump7(d, v.A, (size_t)v.N, A7);
+    if (pw) cudaMemcpyAsync(pw, v.pw, (size_t)v.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    return 1;
+}
+// BiCGSTAB on the system now in A / rhs from sol = x0 (or 1); returns iterations
+int b200x_bicgstab(int maxit, double rtol, double atol, int qsign, const double *x0, double *sol, double *rn,
+                   double *r0) {
+    Inst &d = *dev();
+    Ctx c = make_ctx(d);
+    if (x0) cudaMemcpyAsync(d.g.h.sol, x0, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
+    else launch_fill_sel(c, V_SOL, 1.0);
+    const int its = bicgstab_core(c, d.g.mg, maxit, rtol, atol, 1, 1, rn, r0, qsign);
+    if (sol) cudaMemcpyAsync(sol, d.g.h.sol, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    return its;
+}
+// PCG on the Poisson system now in A / rhs from sol = 0
+int b200x_pcg(int maxit, double rtol, double *sol) {
+    Inst &d = *dev();
+    Ctx c = make_ctx(d);
+    launch_fill_sel(c, V_SOL, 0.0);
+    const int its = pcg_solve(c, d.g.mg, maxit, rtol, 1);
+    if (sol) cudaMemcpyAsync(sol, d.g.h.sol, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    return its;
+}
+int b200x_float_fix(int hole, double *sol) {
+    Inst &d = *dev();
+    cudaMemcpyAsync(d.g.h.sol, sol, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
+    const int r = float_fix(d, hole);
+    cudaMemcpyAsync(sol, d.g.h.sol, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    return r;
+}
+// device memory of the instance (bytes) and the multigrid depth
+long long b200x_device_bytes(void) { return (long long)dev()->g.bytes; }
+
+}  // extern "C"
