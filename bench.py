@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: I-V bias points/s of the n-MOSFET Id-Vg workload on B200.
+
+Workload (the precision-path configuration): n-MOSFET on a 120x80x60 tensor mesh
+(576,000 nodes), p-body 1e17 cm^-3, Gaussian n+ source / drain (1e20 cm^-3, sigma 20 nm),
+2 nm SiO2 gate oxide as an oxide Robin face gate, velocity-saturated mobility; gate
+swept 0..1.2 V in 0.05 V steps (25 points) at Vd = 0.05 V and 1.0 V.  Synthetic device
+data built by semiconductor_devices_simulator_b200/devices.py (no dataset involved).
+
+A step is one Id-Vg sweep (25 bias points) through the library's C ABI
+(api3_set_contact_V + api3_resolve per point, the way main.py's run_sweep drives it),
+alternating the two drain biases.  Bias points/s = converged points / time of the sweep;
+device set-up and the equilibrium + ramp to the first point (api3_solve) are outside
+the timed region, as the metric defines.  `value` reads only the terminal currents per
+point (state resident in HBM); `e2e` also copies psi, n and p of every point to host
+buffers (api3_bulk_copy), the per-point results a caller reads.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own sweeps (independent
+devices, no data-path collective): weak scaling, time = max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from semiconductor_devices_simulator_b200 import abi, devices as D  # noqa: E402
+
+METRIC = "I-V bias points/s (n-MOSFET Id-Vg sweep, FP64 solve, dI/I<=1e-4)"
+UNIT = "bias points/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--mesh", default="120,80,60")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bounded CPU-baseline sample (s)")
+    ap.add_argument("--no-profile", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the e2e pass (profiler captures)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ distributed plumbing
+class Dist:
+    def __init__(self):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.dist, self.torch, self.backend = dist, torch, backend
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return float(x)
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64,
+                              device="cuda" if self.backend == "nccl" else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if self.world == 1:
+            return float(x)
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64,
+                              device="cuda" if self.backend == "nccl" else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.proc, self.rows = gpu, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ workload
+def build(lib, mesh):
+    return D.nmosfet(lib, n=mesh)
+
+
+def sweep_points(lib, w, s, fields=False, npts=None):
+    """Timed part of one step: every point of the sweep after the first (or the next
+    npts); the first point is the one api3_solve already solved."""
+    nc = lib.api3_get_ncon()
+    V = s["V"][1:] if npts is None else s["V"][1:1 + npts]
+    conv = 0
+    bufs = [np.empty(w.N) for _ in range(3)] if fields else None
+    for v in V:
+        for cid, vv in D.bias_vector(w, s, v).items():
+            lib.api3_set_contact_V(cid, vv)
+        conv += int(lib.api3_resolve())
+        for c in range(nc):
+            lib.api3_get_contact_I(c)
+        if fields:
+            for q, which in enumerate((0, 1, 2)):
+                lib.api3_bulk_copy(which, abi.dptr(bufs[q]))
+    return len(V), conv
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(mesh, seconds):
+    """The reference core (oracle/_ref, built from the reference sources) on this
+    host's cores: the same workload, a bounded sample of the Vd = 1.0 V sweep."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_ref.so")
+    if not os.path.exists(path):
+        return None
+    ref = abi.bind(ctypes.CDLL(path))
+    cores = os.cpu_count() or 1
+    ref.api3_set_threads(cores)
+    w = build(ref, mesh)
+    s = w.sweeps[1]
+    D.start_sweep(ref, w, s)
+    t0 = time.perf_counter()
+    n = 0
+    for v in s["V"][1:]:
+        for cid, vv in D.bias_vector(w, s, v).items():
+            ref.api3_set_contact_V(cid, vv)
+        ref.api3_resolve()
+        n += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"first {n} resolves of the Vd=1.0 V Id-Vg sweep, {mesh[0]}x{mesh[1]}x{mesh[2]} mesh, "
+                      f"reference core semiconductor_3d.c built from source (-O3 -fopenmp), {cores} threads, "
+                      f"{dt:.1f} s"}
+
+
+def run_b200(a, dist):
+    import semiconductor_devices_simulator_b200 as S
+    mesh = tuple(int(v) for v in a.mesh.split(","))
+    lib = S.load()
+    lib.b200x_set_device(dist.local)
+    w = build(lib, mesh)
+    nsw = len(w.sweeps)
+    lib.api3_set_verbose(0)
+
+    def step(i, fields=False, timed=True):
+        s = w.sweeps[(i + dist.rank) % nsw]
+        D.start_sweep(lib, w, s)                         # untimed: set-up, equilibrium, ramp
+        dist.barrier()
+        lib.b200x_stream_timer(0)
+        t0 = time.perf_counter()
+        npts, conv = sweep_points(lib, w, s, fields=fields)
+        ms = lib.b200x_stream_timer(1)
+        wall = time.perf_counter() - t0
+        return npts, conv, ms / 1e3, wall
+
+    for i in range(a.warmup):
+        step(i)
+    clocks = Clocks(dist.local)
+    clocks.start()
+    l0 = lib.b200x_launches()
+    tot_pts = tot_conv = 0
+    tot_dev = tot_wall = 0.0
+    for i in range(a.steps):
+        npts, conv, dev_s, wall = step(a.warmup + i)
+        tot_pts += npts; tot_conv += conv; tot_dev += dev_s; tot_wall += wall
+    launches = int(lib.b200x_launches() - l0)
+    clk = clocks.stop()
+    # e2e: the same steps with every point's psi, n, p copied to host buffers
+    e_pts = 0
+    e_wall = 0.0
+    for i in range(0 if a.no_e2e else a.steps):
+        npts, conv, dev_s, wall = step(a.warmup + i, fields=True)
+        e_pts += npts; e_wall += wall
+    if a.no_e2e:
+        e_pts, e_wall = tot_pts, tot_wall
+    # roofline: one more step with every launch timed by CUDA events on the solver stream
+    prof = None
+    if not a.no_profile:
+        nk = lib.b200x_prof(1)
+        step(a.warmup)
+        lib.b200x_prof(0)
+        rows = []
+        for k in range(nk):
+            ms, cnt, by = (np.zeros(1) for _ in range(3))
+            lib.b200x_prof_read(k, abi.dptr(ms), abi.dptr(cnt), abi.dptr(by))
+            rows.append((lib.b200x_prof_name(k).decode(), float(ms[0]), int(cnt[0]), float(by[0])))
+        prof = rows
+    T = dist.max(tot_dev)
+    pts_all = dist.sum(tot_pts)
+    e_T = dist.max(e_wall)
+    e_all = dist.sum(e_pts)
+    out = None
+    if dist.rank == 0:
+        hbm, pk_kind = peaks()
+        roof = None
+        kernels = None
+        if prof:
+            tot_ms = sum(r[1] for r in prof) or 1.0
+            top = max(prof, key=lambda r: r[1])
+            ach = top[3] / (top[1] / 1e3) / 1e9 if top[1] > 0 else 0.0
+            roof = {"bound": "hbm", "kernel": top[0], "achieved": round(ach, 1), "peak": hbm,
+                    "peak_kind": pk_kind, "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": None,
+                    "launches": top[2], "avg_launch_us": round(1e3 * top[1] / max(top[2], 1), 2),
+                    "bytes_per_launch": round(top[3] / max(top[2], 1))}
+            kernels = {r[0]: {"ms": round(r[1], 2), "share": round(r[1] / tot_ms, 4), "launches": r[2],
+                              "GBps": round(r[3] / (r[1] / 1e3) / 1e9, 1) if r[1] > 0 else 0.0}
+                       for r in sorted(prof, key=lambda r: -r[1]) if r[2] > 0}
+        h2d = 8 * 4 * len(w.contacts)                              # contact voltages per point
+        d2h = 3 * 8 * w.N + 16 * len(w.contacts)                   # psi, n, p + currents per point
+        npts_step = len(w.sweeps[0]["V"]) - 1
+        out = {
+            "metric": METRIC, "value": round(pts_all / T, 4), "unit": UNIT, "n_gpus": dist.world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * T / a.steps, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (device built from the workload definition)",
+            "config": {"workload": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]}_idvg",
+                       "nodes": w.N, "points_per_step": npts_step, "drain_biases_V": [0.05, 1.0],
+                       "gate_sweep_V": [0.0, 1.2, 0.05], "models": 4, "solver": list(D.GUI_SOLVER),
+                       "parallelism": f"replicas{dist.world}",
+                       "l2": "state of 576k nodes (~0.5 GB) exceeds the 126 MB L2; no flush"},
+            "converged_points": tot_conv, "wall_s": round(tot_wall, 3),
+            "e2e": {"value": round(e_all / e_T, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * npts_step,
+                    "d2h_bytes_per_step": d2h * npts_step},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "kernels": kernels,
+            "clocks": clk,
+        }
+        if dist.world == 1 and not a.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(mesh, a.cpu_seconds)
+    return out
+
+
+def run_reference(a, dist):
+    """The reference's own CPU core on the same workload: each step a bounded sample
+    (the first points of one sweep), all host threads."""
+    if dist.rank != 0:
+        return None
+    mesh = tuple(int(v) for v in a.mesh.split(","))
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_ref.so")
+    if not os.path.exists(path):
+        return {"impl": "reference", "unavailable": "reference core not built (make -C oracle)"}
+    ref = abi.bind(ctypes.CDLL(path))
+    cores = os.cpu_count() or 1
+    ref.api3_set_threads(cores)
+    w = build(ref, mesh)
+    npts = 3
+    tot = e_tot = 0.0
+    pts = 0
+    for i in range(a.warmup + a.steps):
+        s = w.sweeps[i % len(w.sweeps)]
+        D.start_sweep(ref, w, s)
+        t0 = time.perf_counter()
+        n, conv = sweep_points(ref, w, s, fields=False, npts=npts)
+        dt = time.perf_counter() - t0
+        if i >= a.warmup:
+            tot += dt
+            pts += n
+    v = pts / tot
+    return {"metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": dist.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(1e3 * tot / a.steps, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic (device built from the workload definition)",
+            "config": {"workload": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]}_idvg", "nodes": w.N,
+                       "points_per_step": npts, "parallelism": "cpu"},
+            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"first {npts} points of one Id-Vg sweep per step"},
+            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse()
+    dist = Dist()
+    out = run_reference(a, dist) if a.impl == "reference" else run_b200(a, dist)
+    if dist.rank == 0 and out is not None:
+        print(json.dumps(out))
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -40,6 +40,12 @@ HOOKS = {
     "b200x_pcg": (_I, [_I, _D, _DP]),
     "b200x_float_fix": (_I, [_I, _DP]),
     "b200x_device_bytes": (_LL, []),
+    "b200x_stream_timer": (_D, [_I]),
+    "b200x_set_device": (_I, [_I]),
+    "b200x_prof": (_I, [_I]),
+    "b200x_prof_read": (_I, [_I, _DP, _DP, _DP]),
+    "b200x_prof_name": (ctypes.c_char_p, [_I]),
+    "b200x_launches": (ctypes.c_ulonglong, []),
 }
 # state arrays reachable through b200x_set / b200x_get
 ST_PHI, ST_PHIN, ST_PHIP, ST_N, ST_P, ST_MU0N, ST_MU0P, ST_SOL, ST_RHS, ST_SC, ST_DSC = range(11)

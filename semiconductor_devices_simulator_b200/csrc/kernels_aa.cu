@@ -2,6 +2,7 @@
 // x = (psi, phi_n, phi_p) (semiconductor_3d.c:3709-3757): FP32 difference history,
 // FP64 Gram matrix and normal equations, masked mixing.
 #include "device_common.cuh"
+#include "prof.h"
 #include "solver_ctx.h"
 
 namespace ss {
@@ -143,13 +144,13 @@ __global__ void k_aa_mix(const DevP *__restrict__ Ps, int m) {
 }
 
 void aa_update_history(const Ctx &c, int slot, int nfill) {
-    k_aa_diff<<<grid3(c), TPB, 0, c.st>>>(c.dP, slot);
-    k_aa_gram<<<grid3(c), TPB, 0, c.st>>>(c.dP, slot, nfill);
+    SS_LAUNCH(PF_AA, 3 * c.maxN, k_aa_diff, grid3(c), TPB, c.st, c.dP, slot);
+    SS_LAUNCH(PF_AA, 3 * c.maxN, k_aa_gram, grid3(c), TPB, c.st, c.dP, slot, nfill);
 }
-void aa_store_fg(const Ctx &c) { k_aa_fg<<<grid3(c), TPB, 0, c.st>>>(c.dP); }
+void aa_store_fg(const Ctx &c) { SS_LAUNCH(PF_AA, 3 * c.maxN, k_aa_fg, grid3(c), TPB, c.st, c.dP); }
 void aa_solve_mix(const Ctx &c, int m, int *) {
-    k_aa_bb_solve<<<grid3(c), TPB, 0, c.st>>>(c.dP, m);
-    k_aa_mix<<<grid3(c), TPB, 0, c.st>>>(c.dP, m);
+    SS_LAUNCH(PF_AA, 3 * c.maxN, k_aa_bb_solve, grid3(c), TPB, c.st, c.dP, m);
+    SS_LAUNCH(PF_AA, 3 * c.maxN, k_aa_mix, grid3(c), TPB, c.st, c.dP, m);
 }
 
 }  // namespace ss

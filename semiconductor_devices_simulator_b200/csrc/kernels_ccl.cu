@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "device_common.cuh"
+#include "prof.h"
 #include "solver_ctx.h"
 
 namespace ss {
@@ -157,7 +158,7 @@ int float_fix(Inst &d, int hole) {
         cudaMalloc(&g_ffint, sizeof(int) * (FF_MAX_BLOCKS + 16));
     }
     int *changed = g_ffint, *count = g_ffint + 1, *roots = g_ffint + 16;
-    k_ff_init<<<g, TPB, 0, c.st>>>(c.dP, hole);
+    SS_LAUNCH(PF_CCL, d.N, k_ff_init, g, TPB, c.st, c.dP, hole);
     int h = 1, cycles = 0;
     const int maxcyc = d.Nx + d.Ny + d.Nz + 8;
     while (h && cycles < maxcyc) {
@@ -165,15 +166,15 @@ int float_fix(Inst &d, int hole) {
         for (int ax = 0; ax < 3; ax++) {
             const int n = ax == 0 ? d.Nx : (ax == 1 ? d.Ny : d.Nz);
             const int nb = ((int)d.N / n + TPB - 1) / TPB;
-            k_ff_sweep<<<dim3(nb, 1), TPB, 0, c.st>>>(c.dP, ax, changed);
+            SS_LAUNCH(PF_CCL, d.N, k_ff_sweep, dim3(nb, 1), TPB, c.st, c.dP, ax, changed);
         }
         cudaMemcpyAsync(&h, changed, sizeof(int), cudaMemcpyDeviceToHost, c.st);
         cudaStreamSynchronize(c.st);
         cycles++;
     }
-    k_ff_anchor<<<g, TPB, 0, c.st>>>(c.dP);
+    SS_LAUNCH(PF_CCL, d.N, k_ff_anchor, g, TPB, c.st, c.dP);
     cudaMemsetAsync(count, 0, sizeof(int), c.st);
-    k_ff_roots<<<g, TPB, 0, c.st>>>(c.dP, count, roots);
+    SS_LAUNCH(PF_CCL, d.N, k_ff_roots, g, TPB, c.st, c.dP, count, roots);
     int nb = 0;
     cudaMemcpyAsync(&nb, count, sizeof(int), cudaMemcpyDeviceToHost, c.st);
     cudaStreamSynchronize(c.st);
@@ -182,7 +183,7 @@ int float_fix(Inst &d, int hole) {
     double *Aout = g_ffbuf, *Bin = g_ffbuf + FF_MAX_BLOCKS, *lam = g_ffbuf + 2 * FF_MAX_BLOCKS;
     double *G = g_ffbuf + 3 * FF_MAX_BLOCKS, *dG = g_ffbuf + 4 * FF_MAX_BLOCKS;
     cudaMemsetAsync(Aout, 0, sizeof(double) * 2 * FF_MAX_BLOCKS, c.st);
-    k_ff_boundary<<<g, TPB, 0, c.st>>>(c.dP, hole, Aout, Bin);
+    SS_LAUNCH(PF_CCL, d.N, k_ff_boundary, g, TPB, c.st, c.dP, hole, Aout, Bin);
     std::vector<double> hA(nb), hB(nb), sl(nb, 0.0), hl(nb), hG(nb), hdG(nb);
     std::vector<int> act(nb, 1);
     cudaMemcpyAsync(hA.data(), Aout, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.st);
@@ -194,7 +195,7 @@ int float_fix(Inst &d, int hole) {
         if (!any) break;
         cudaMemcpyAsync(lam, hl.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, c.st);
         cudaMemsetAsync(G, 0, sizeof(double) * 2 * FF_MAX_BLOCKS, c.st);
-        k_ff_recomb<<<g, TPB, 0, c.st>>>(c.dP, hole, lam, G, dG);
+        SS_LAUNCH(PF_CCL, d.N, k_ff_recomb, g, TPB, c.st, c.dP, hole, lam, G, dG);
         cudaMemcpyAsync(hG.data(), G, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.st);
         cudaMemcpyAsync(hdG.data(), dG, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.st);
         cudaStreamSynchronize(c.st);
@@ -217,7 +218,7 @@ int float_fix(Inst &d, int hole) {
         else hl[b] = 1.0;
     }
     cudaMemcpyAsync(lam, hl.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, c.st);
-    k_ff_apply<<<g, TPB, 0, c.st>>>(c.dP, lam);
+    SS_LAUNCH(PF_CCL, d.N, k_ff_apply, g, TPB, c.st, c.dP, lam);
     cudaStreamSynchronize(c.st);
     if (d.verbose > 2) std::fprintf(stderr, "    float_fix(%c): %d blocks, %d rescaled\n", hole ? 'p' : 'n', nb, nfix);
     return nfix;

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "device_common.cuh"
+#include "prof.h"
 #include "kernels.h"
 #include "solver_ctx.h"
 
@@ -414,22 +415,22 @@ __global__ void k_copy(const DevP *__restrict__ Ps, int ysel, int xsel) {
     SS_GRID_LOOP(k, P.N) y[k] = x[k];
 }
 
-void launch_absmax_sel(const Ctx &c, int xsel, int slot) { k_absmax<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, xsel, slot); }
+void launch_absmax_sel(const Ctx &c, int xsel, int slot) { SS_LAUNCH(PF_VEC, c.maxN, k_absmax, grid_nodes(c), TPB, c.st, c.dP, xsel, slot); }
 void launch_axpy_sel(const Ctx &c, int ysel, int xsel, double a, int zsel) {
-    k_axpy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, ysel, xsel, a, zsel);
+    SS_LAUNCH(PF_VEC, c.maxN, k_axpy, grid_nodes(c), TPB, c.st, c.dP, ysel, xsel, a, zsel);
 }
-void launch_fill_sel(const Ctx &c, int ysel, double v) { k_fill<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, ysel, v); }
-void launch_copy_sel(const Ctx &c, int ysel, int xsel) { k_copy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, ysel, xsel); }
+void launch_fill_sel(const Ctx &c, int ysel, double v) { SS_LAUNCH(PF_VEC, c.maxN, k_fill, grid_nodes(c), TPB, c.st, c.dP, ysel, v); }
+void launch_copy_sel(const Ctx &c, int ysel, int xsel) { SS_LAUNCH(PF_VEC, c.maxN, k_copy, grid_nodes(c), TPB, c.st, c.dP, ysel, xsel); }
 
 // ------------------------------------------------------------------ multigrid driver
 void mg_setup(const Ctx &c, const MGHost &mg, int qsign) {
     for (int L = 0; L < mg.maxlev - 1; L++) {
         const int nc = mg.maxN[L + 1];
-        k_mg_weights<<<grid_n(c, nc), TPB, 0, c.st>>>(c.dP, L, qsign);
-        k_galerkin<<<grid_n(c, nc), TPB, 0, c.st>>>(c.dP, L, qsign != 0);
-        k_ilu_diag<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L);
+        SS_LAUNCH(PF_WEIGHTS, nc, k_mg_weights, grid_n(c, nc), TPB, c.st, c.dP, L, qsign);
+        SS_LAUNCH(PF_GALERKIN, nc, k_galerkin, grid_n(c, nc), TPB, c.st, c.dP, L, qsign != 0);
+        SS_LAUNCH(PF_ILU_DIAG, mg.maxN[L], k_ilu_diag, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L);
     }
-    for (int L = 1; L < mg.maxlev; L++) k_coarse_setup<<<dim3(1, c.ninst), TPB, 0, c.st>>>(c.dP, L);
+    for (int L = 1; L < mg.maxlev; L++) SS_LAUNCH(PF_COARSE_SETUP, COARSE_MAX, k_coarse_setup, dim3(1, c.ninst), TPB, c.st, c.dP, L);
 }
 
 // one V(1,1) cycle x = M^-1 b on the level-0 vectors (bsel -> xsel); mg_on = 0 applies
@@ -437,23 +438,23 @@ void mg_setup(const Ctx &c, const MGHost &mg, int qsign) {
 // 1 only while the instance's Krylov loop is active, 2 also not after a half-step exit.
 void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
     if (!mg_on || mg.maxlev < 2) {
-        k_smooth_black<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, bsel, xsel, 0, gate);
-        k_smooth_red<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, bsel, xsel, 0, gate);
+        SS_LAUNCH(PF_SMOOTH_B, c.maxN, k_smooth_black, grid_nodes(c), TPB, c.st, c.dP, 0, bsel, xsel, 0, gate);
+        SS_LAUNCH(PF_SMOOTH_R, c.maxN, k_smooth_red, grid_nodes(c), TPB, c.st, c.dP, 0, bsel, xsel, 0, gate);
         return;
     }
     for (int L = 0; L < mg.maxlev; L++) {
         if (L < mg.maxlev - 1) {
-            k_smooth_black<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, 0, gate);
-            k_smooth_red<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, 0, gate);
-            k_resid_restrict<<<grid_n(c, mg.maxN[L + 1]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, wsel, gate);
+            SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_black, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, 0, gate);
+            SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_red, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, 0, gate);
+            SS_LAUNCH(PF_RESID_RESTRICT, mg.maxN[L + 1], k_resid_restrict, grid_n(c, mg.maxN[L + 1]), TPB, c.st, c.dP, L, bsel, xsel, wsel, gate);
         }
-        if (L >= 1 && L >= mg.minlev - 1) k_coarse_solve<<<dim3(1, c.ninst), 64, 0, c.st>>>(c.dP, L, gate);
+        if (L >= 1 && L >= mg.minlev - 1) SS_LAUNCH(PF_COARSE, COARSE_MAX, k_coarse_solve, dim3(1, c.ninst), 64, c.st, c.dP, L, gate);
     }
     for (int L = mg.maxlev - 2; L >= 0; L--) {
-        k_prolong<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, mg.alpha, gate);
-        k_level_resid<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, gate);
-        k_smooth_black<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, 1, gate);
-        k_smooth_red<<<grid_n(c, mg.maxN[L]), TPB, 0, c.st>>>(c.dP, L, bsel, xsel, 1, gate);
+        SS_LAUNCH(PF_PROLONG, mg.maxN[L], k_prolong, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, mg.alpha, gate);
+        SS_LAUNCH(PF_LEVEL_RESID, mg.maxN[L], k_level_resid, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, gate);
+        SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_black, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, 1, gate);
+        SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_red, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, 1, gate);
     }
 }
 
@@ -534,19 +535,19 @@ int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_
     ks0.active = 1;
     cudaMemcpyAsync(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
     mg_setup(c, mg, 0);
-    k_pcg_init_r<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+    SS_LAUNCH(PF_KRY_INIT, c.maxN, k_pcg_init_r, grid_nodes(c), TPB, c.st, c.dP);
     vcycle(c, mg, 0, 1, 0, 1, 0);                  // z = M r
-    k_pcg_rz<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, rtol * rtol, maxit);
-    k_pcg_p<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 1);
+    SS_LAUNCH(PF_KRY_DOT, c.maxN, k_pcg_rz, grid_nodes(c), TPB, c.st, c.dP, 0, rtol * rtol, maxit);
+    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_p, grid_nodes(c), TPB, c.st, c.dP, 1);
     KrylovS hs{};
     for (int it = 0; it < maxit;) {
         const int nb = check_every;
         for (int q = 0; q < nb && it < maxit; q++, it++) {
-            k_pcg_q<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
-            k_pcg_xr<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_pcg_q, grid_nodes(c), TPB, c.st, c.dP);
+            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_xr, grid_nodes(c), TPB, c.st, c.dP);
             vcycle(c, mg, 0, 1, 0, 1, 1);
-            k_pcg_rz<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 1, rtol * rtol, maxit);
-            k_pcg_p<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0);
+            SS_LAUNCH(PF_KRY_DOT, c.maxN, k_pcg_rz, grid_nodes(c), TPB, c.st, c.dP, 1, rtol * rtol, maxit);
+            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_p, grid_nodes(c), TPB, c.st, c.dP, 0);
         }
         cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
         cudaStreamSynchronize(c.st);
@@ -724,21 +725,21 @@ int bicgstab_core(const Ctx &c, const MGHost &mg, int maxit, double rtol, double
                   double *rn, double *r0, int qsign) {
     if (mg_on) mg_setup(c, mg, qsign);
     else {
-        k_ilu_diag<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0);
+        SS_LAUNCH(PF_ILU_DIAG, c.maxN, k_ilu_diag, grid_nodes(c), TPB, c.st, c.dP, 0);
     }
-    k_bicg_init<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, rtol, atol);
+    SS_LAUNCH(PF_KRY_INIT, c.maxN, k_bicg_init, grid_nodes(c), TPB, c.st, c.dP, rtol, atol);
     KrylovS hs{};
     const int wsel = qsign != 0;
     for (int it = 0; it < maxit;) {
         for (int q = 0; q < check_every && it < maxit; q++, it++) {
-            k_bicg_rho<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, maxit);
-            k_bicg_p<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            SS_LAUNCH(PF_KRY_DOT, c.maxN, k_bicg_rho, grid_nodes(c), TPB, c.st, c.dP, maxit);
+            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_p, grid_nodes(c), TPB, c.st, c.dP);
             vcycle(c, mg, 2, 4, wsel, mg_on, 1);            // ph = M p
-            k_bicg_v<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
-            k_bicg_s<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_bicg_v, grid_nodes(c), TPB, c.st, c.dP);
+            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_s, grid_nodes(c), TPB, c.st, c.dP);
             vcycle(c, mg, 0, 5, wsel, mg_on, 2);            // sh = M r
-            k_bicg_t<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
-            k_bicg_x<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP);
+            SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_bicg_t, grid_nodes(c), TPB, c.st, c.dP);
+            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_x, grid_nodes(c), TPB, c.st, c.dP);
         }
         cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
         cudaStreamSynchronize(c.st);

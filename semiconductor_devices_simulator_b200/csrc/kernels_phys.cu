@@ -7,6 +7,7 @@
 #include <cstdio>
 
 #include "device_common.cuh"
+#include "prof.h"
 #include "kernels.h"
 
 namespace ss {
@@ -94,7 +95,7 @@ __global__ void k_poisson(const DevP *__restrict__ Ps, int src, int build) {
 }
 
 void launch_poisson(const Ctx &c, const double *phi_sel, int build, double *) {
-    k_poisson<<<grid_of(c), TPB, 0, c.st>>>(c.dP, phi_sel ? 1 : 0, build);
+    SS_LAUNCH(PF_POISSON, c.maxN, k_poisson, grid_of(c), TPB, c.st, c.dP, phi_sel ? 1 : 0, build);
 }
 
 // n, p from the potentials (semiconductor_3d.c:2826-2834)
@@ -108,7 +109,7 @@ __global__ void k_rebuild_np(const DevP *__restrict__ Ps) {
         P.p[k] = pK(P, m, k, P.phi[k], P.phip[k]);
     }
 }
-void launch_rebuild_np(const Ctx &c) { k_rebuild_np<<<grid_of(c), TPB, 0, c.st>>>(c.dP); }
+void launch_rebuild_np(const Ctx &c) { SS_LAUNCH(PF_REBUILD, c.maxN, k_rebuild_np, grid_of(c), TPB, c.st, c.dP); }
 
 // Face mobility of the edge k -> k+e_ax from the node low-field mobilities, with
 // Caughey-Thomas saturation driven by the harmonic-mean field when models bit 2 is set
@@ -143,7 +144,7 @@ __global__ void k_upd_mob(const DevP *__restrict__ Ps) {
         }
     }
 }
-void launch_upd_mob(const Ctx &c) { k_upd_mob<<<grid_of(c), TPB, 0, c.st>>>(c.dP); }
+void launch_upd_mob(const Ctx &c) { SS_LAUNCH(PF_UPDMOB, c.maxN, k_upd_mob, grid_of(c), TPB, c.st, c.dP); }
 
 // ------------------------------------------------------------------ continuity
 // Scaled Scharfetter-Gummel row for u = c/s (semiconductor_3d.c:3067-3106):
@@ -206,7 +207,7 @@ __global__ void k_cont_assemble(const DevP *__restrict__ Ps, int hole) {
         P.dsc[k] = dg * sk;
     }
 }
-void launch_cont_assemble(const Ctx &c, int hole) { k_cont_assemble<<<grid_of(c), TPB, 0, c.st>>>(c.dP, hole); }
+void launch_cont_assemble(const Ctx &c, int hole) { SS_LAUNCH(PF_CONT_ASM, c.maxN, k_cont_assemble, grid_of(c), TPB, c.st, c.dP, hole); }
 
 // c = s u -> quasi-Fermi potential clamped to [lo, hi], carrier, change, and the
 // weighted max |change| (semiconductor_3d.c:3112-3146)
@@ -243,7 +244,7 @@ __global__ void k_cont_update(const DevP *__restrict__ Ps, int hole, double lo, 
     if (grid_max(dmax, P.part, P.ticket + 1)) P.res[R_DQ] = dmax;
 }
 void launch_cont_update(const Ctx &c, int hole, double lo, double hi) {
-    k_cont_update<<<grid_of(c), TPB, 0, c.st>>>(c.dP, hole, lo, hi);
+    SS_LAUNCH(PF_CONT_UPD, c.maxN, k_cont_update, grid_of(c), TPB, c.st, c.dP, hole, lo, hi);
 }
 
 // ------------------------------------------------------------------ boundary values
@@ -279,7 +280,7 @@ __global__ void k_apply_bc(const DevP *__restrict__ Ps) {
         P.p[k] = pK(P, m, k, P.phi[k], V);
     }
 }
-void launch_apply_bc(const Ctx &c, int) { k_apply_bc<<<grid_of(c), TPB, 0, c.st>>>(c.dP); }
+void launch_apply_bc(const Ctx &c, int) { SS_LAUNCH(PF_BC, c.maxN, k_apply_bc, grid_of(c), TPB, c.st, c.dP); }
 
 // local charge-neutral equilibrium start (semiconductor_3d.c:1831-1845)
 __global__ void k_init_eq(const DevP *__restrict__ Ps) {
@@ -299,7 +300,7 @@ __global__ void k_init_eq(const DevP *__restrict__ Ps) {
         P.Rt[k] = 0.0;
     }
 }
-void launch_init_eq(const Ctx &c) { k_init_eq<<<grid_of(c), TPB, 0, c.st>>>(c.dP); }
+void launch_init_eq(const Ctx &c) { SS_LAUNCH(PF_BC, c.maxN, k_init_eq, grid_of(c), TPB, c.st, c.dP); }
 
 // quasi-Fermi potentials clamped to the terminal span (semiconductor_3d.c:3945-3952)
 __global__ void k_clamp_qf(const DevP *__restrict__ Ps, double lo, double hi) {
@@ -310,7 +311,7 @@ __global__ void k_clamp_qf(const DevP *__restrict__ Ps, double lo, double hi) {
         P.phip[k] = b < lo ? lo : (b > hi ? hi : b);
     }
 }
-void launch_clamp_qf(const Ctx &c, double lo, double hi) { k_clamp_qf<<<grid_of(c), TPB, 0, c.st>>>(c.dP, lo, hi); }
+void launch_clamp_qf(const Ctx &c, double lo, double hi) { SS_LAUNCH(PF_VEC, c.maxN, k_clamp_qf, grid_of(c), TPB, c.st, c.dP, lo, hi); }
 
 // ------------------------------------------------------------------ currents
 // SG flux through the face a -> b, split into electrons / holes, with the magnitude
@@ -399,7 +400,7 @@ void launch_currents(const Ctx &c) {
         std::fprintf(stderr, "semisim-b200: too many contact nodes (%d)\n", c.h.ncnode);
         nb = 256;
     }
-    k_currents<<<dim3(nb, c.ninst), TPB, 0, c.st>>>(c.dP, g_partc, g_ticketc);
+    SS_LAUNCH(PF_CURRENTS, c.h.ncnode, k_currents, dim3(nb, c.ninst), TPB, c.st, c.dP, g_partc, g_ticketc);
 }
 
 // ------------------------------------------------------------------ Gummel helpers
@@ -418,7 +419,7 @@ __global__ void k_predictor(const DevP *__restrict__ Ps) {
         P.phi[k] = ps + (n * P.dqn[k] + p * P.dqp[k]) / den;
     }
 }
-void launch_predictor(const Ctx &c) { k_predictor<<<grid_of(c), TPB, 0, c.st>>>(c.dP); }
+void launch_predictor(const Ctx &c) { SS_LAUNCH(PF_VEC, c.maxN, k_predictor, grid_of(c), TPB, c.st, c.dP); }
 
 __global__ void k_dpsi(const DevP *__restrict__ Ps) {
     const DevP &P = Ps[blockIdx.y];
@@ -429,7 +430,7 @@ __global__ void k_dpsi(const DevP *__restrict__ Ps) {
     }
     if (grid_max(m, P.part, P.ticket + 2)) P.res[R_DPSI] = m;
 }
-void launch_dpsi(const Ctx &c) { k_dpsi<<<grid_of(c), TPB, 0, c.st>>>(c.dP); }
+void launch_dpsi(const Ctx &c) { SS_LAUNCH(PF_VEC, c.maxN, k_dpsi, grid_of(c), TPB, c.st, c.dP); }
 
 // ------------------------------------------------------------------ display outputs
 // node current density (mean of the adjacent face fluxes per axis) and recombination
@@ -458,7 +459,7 @@ __global__ void k_upd_J(const DevP *__restrict__ Ps) {
         P.Rt[k] = R;
     }
 }
-void launch_upd_J(const Ctx &c) { k_upd_J<<<grid_of(c), TPB, 0, c.st>>>(c.dP); }
+void launch_upd_J(const Ctx &c) { SS_LAUNCH(PF_DISPLAY, c.maxN, k_upd_J, grid_of(c), TPB, c.st, c.dP); }
 
 // display mobility: mean of the adjacent edge mobilities (semiconductor_3d.c:3035-3060)
 __global__ void k_mob_display(const DevP *__restrict__ Ps) {
@@ -484,7 +485,7 @@ __global__ void k_mob_display(const DevP *__restrict__ Ps) {
         P.mudp[k] = c ? sp / c : P.mu0p[k];
     }
 }
-void launch_mob_display(const Ctx &c) { k_mob_display<<<grid_of(c), TPB, 0, c.st>>>(c.dP); }
+void launch_mob_display(const Ctx &c) { SS_LAUNCH(PF_DISPLAY, c.maxN, k_mob_display, grid_of(c), TPB, c.st, c.dP); }
 
 // derived node quantity `which` (semiconductor_3d.c:5066-5126); models outside the
 // library's scope contribute their "off" values
@@ -545,7 +546,7 @@ __global__ void k_node_val(const DevP *__restrict__ Ps, int which, double *out) 
     }
 }
 void launch_node_val(const Ctx &c, int which, double *out) {
-    k_node_val<<<grid_of(c), TPB, 0, c.st>>>(c.dP, which, out);
+    SS_LAUNCH(PF_DISPLAY, c.maxN, k_node_val, grid_of(c), TPB, c.st, c.dP, which, out);
 }
 
 // current density through the face k -> k+e_ax, total or electrons (semiconductor_3d.c:5284-5298)
@@ -563,7 +564,7 @@ __global__ void k_face_J(const DevP *__restrict__ Ps, int ax, int carrier, doubl
     }
 }
 void launch_face_J(const Ctx &c, int ax, int carrier, double *out) {
-    k_face_J<<<grid_of(c), TPB, 0, c.st>>>(c.dP, ax, carrier, out);
+    SS_LAUNCH(PF_DISPLAY, c.maxN, k_face_J, grid_of(c), TPB, c.st, c.dP, ax, carrier, out);
 }
 
 // ------------------------------------------------------------------ continuation
@@ -583,7 +584,7 @@ __global__ void k_extrap(const DevP *__restrict__ Ps, double r, int s1, int s2) 
     }
 }
 void launch_extrap(const Ctx &c, double r, int s1, int s2) {
-    k_extrap<<<grid_of(c), TPB, 0, c.st>>>(c.dP, r, s1, s2);
+    SS_LAUNCH(PF_VEC, c.maxN, k_extrap, grid_of(c), TPB, c.st, c.dP, r, s1, s2);
 }
 
 // ---- region shift (semiconductor_3d.c:3956-3987): flood fill of the quasi-neutral
@@ -643,7 +644,7 @@ __global__ void k_region_shift(const DevP *__restrict__ Ps, int c1, double dV, c
     }
 }
 void launch_region_mark(const Ctx &c, int c1, int type, double dV, int *mark, int *changed) {
-    k_region_seed<<<grid_of(c), TPB, 0, c.st>>>(c.dP, c1, mark);
+    SS_LAUNCH(PF_CCL, c.maxN, k_region_seed, grid_of(c), TPB, c.st, c.dP, c1, mark);
     int h_changed = 1, cycles = 0;
     const int maxcyc = c.h.Nx + c.h.Ny + c.h.Nz + 8;
     while (h_changed && cycles < maxcyc) {
@@ -652,13 +653,13 @@ void launch_region_mark(const Ctx &c, int c1, int type, double dV, int *mark, in
             const int n = ax == 0 ? c.h.Nx : (ax == 1 ? c.h.Ny : c.h.Nz);
             const int nl = c.h.N / n;
             const int nb = (nl + TPB - 1) / TPB;
-            k_region_sweep<<<dim3(nb, c.ninst), TPB, 0, c.st>>>(c.dP, ax, c1, type, mark, changed);
+            SS_LAUNCH(PF_CCL, c.h.N, k_region_sweep, dim3(nb, c.ninst), TPB, c.st, c.dP, ax, c1, type, mark, changed);
         }
         cudaMemcpyAsync(&h_changed, changed, sizeof(int), cudaMemcpyDeviceToHost, c.st);
         cudaStreamSynchronize(c.st);
         cycles++;
     }
-    k_region_shift<<<grid_of(c), TPB, 0, c.st>>>(c.dP, c1, dV, mark);
+    SS_LAUNCH(PF_CCL, c.maxN, k_region_shift, grid_of(c), TPB, c.st, c.dP, c1, dV, mark);
 }
 
 }  // namespace ss

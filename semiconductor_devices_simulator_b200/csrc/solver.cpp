@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "solver_ctx.h"
@@ -36,7 +37,17 @@ bool gpu_available() {
     return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
 }
 
+int g_device = -1;                 // CUDA device of the solver (-1: the runtime's current one)
+
+int select_device(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || dev < 0 || dev >= n) return 0;
+    g_device = dev;
+    return 1;
+}
+
 Ctx make_ctx(Inst &d) {
+    if (g_device >= 0) cudaSetDevice(g_device);
     Ctx c;
     c.dP = d.g.d;
     c.h = d.g.h;
@@ -159,6 +170,11 @@ static int gpu_alloc(Inst &d) {
         std::fprintf(stderr, "semisim-b200: no CUDA device available - the solver has no CPU path\n");
         return 0;
     }
+    if (g_device < 0) {
+        const char *e = std::getenv("SEMISIM_B200_DEVICE");
+        g_device = e ? std::atoi(e) : 0;
+    }
+    CK(cudaSetDevice(g_device));
     int dims[MAXLEV][6];
     const int nl = mg_levels(d.Nx, d.Ny, d.Nz, dims);
     Carver cv;

@@ -99,6 +99,7 @@ extern volatile double g_prog[8];
 
 // solver entry points (solver.cpp)
 bool gpu_available();
+int select_device(int dev);
 int prepare(Inst &d);
 int equilibrium(Inst &d);
 int run_continuation(Inst &d);

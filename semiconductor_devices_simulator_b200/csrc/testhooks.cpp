@@ -185,4 +185,22 @@ int b200x_float_fix(int hole, double *sol) {
 // device memory of the instance (bytes) and the multigrid depth
 long long b200x_device_bytes(void) { return (long long)dev()->g.bytes; }
 
+// select the CUDA device of the solver (before its first solve); 1 = done
+int b200x_set_device(int dev) { return select_device(dev); }
+
+// CUDA-event timer on the solver's own stream: op 0 records the start, op 1 records the
+// stop, waits for it and returns the elapsed milliseconds (-1 before the first solve)
+double b200x_stream_timer(int op) {
+    static cudaEvent_t ev[2] = {nullptr, nullptr};
+    Inst &d = *dev();
+    if (!d.g.ready) return -1.0;
+    if (!ev[0]) { cudaEventCreate(&ev[0]); cudaEventCreate(&ev[1]); }
+    if (op == 0) { cudaEventRecord(ev[0], d.g.st); return 0.0; }
+    cudaEventRecord(ev[1], d.g.st);
+    cudaEventSynchronize(ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    return ms;
+}
+
 }  // extern "C"

@@ -105,11 +105,19 @@ def state(lib, N):
                 fmu=np.array([get(lib, 16 + q, N) for q in range(6)]))
 
 
-def sweep_record(lib, w):
-    """End-to-end: api3_solve at the first point of every sweep, then api3_resolve per point."""
+# Tight tolerances: inner solves to round-off and a Gummel tolerance of 1e-12 V, so the
+# sweep converges to the discrete solution itself (trace carriers included).  The
+# environment knobs are the reference's own (semiconductor_3d.c:4578-4581).
+TIGHT_ENV = {"SEMISIM_BRTOL": "1e-12", "SEMISIM_PCGRTOL": "1e-10"}
+TIGHT_SOLVER = (2000, 1000, 500, 1e-12, 1e-9, 1.0, 1.0)
+
+
+def sweep_record(lib, w, tag=""):
+    """End-to-end: api3_solve at the first point of every sweep, then api3_resolve per
+    point; keys sw<tag><sweep>_* (tag "" default tolerances, "t" tight)."""
     out = {}
-    N = w.N
     for si, s in enumerate(w.sweeps):
+        si = f"{tag}{si}"
         ok0 = D.start_sweep(lib, w, s)
         psi, nn, pp, qn, qp = [], [], [], [], []
 
@@ -262,6 +270,12 @@ def main(names=("diode_small", "mos_small", "moscap_small")):
         out.update(kernels(lib, w, rec, mat, bias, seed=1234))
         w, mat, bias = build(lib, name)              # fresh device for the sweep
         out.update(sweep_record(lib, w))
+        os.environ.update(TIGHT_ENV)                 # read by api3_init
+        w, mat, bias = build(lib, name)
+        lib.api3_set_solver(*TIGHT_SOLVER)
+        out.update(sweep_record(lib, w, "t"))
+        for k in TIGHT_ENV:
+            del os.environ[k]
         out["threads"] = np.array(1)
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **out)

@@ -68,15 +68,47 @@ def check_currents(I, rI, rF):
 
 
 @pytest.mark.parametrize("name", NAMES)
-def test_small_sweeps_match_reference(lib, name):
+def test_small_sweeps_tight_match_reference(lib, name, monkeypatch):
+    """Both codes converged to the discrete solution (inner solves to round-off, Gummel
+    tolerance 1e-12 V): every target holds on every node and terminal."""
+    g = golden(name)
+    for k, v in MG.TIGHT_ENV.items():
+        monkeypatch.setenv(k, v)                 # read by api3_init, as the reference reads them
+    w, mat, bias = MG.build(lib, name)
+    lib.api3_set_solver(*MG.TIGHT_SOLVER)
+    s = w.sweeps[0]
+    ok0, V, I, F, conv, psi, n, p = sweep_fields(lib, w, s)
+    assert ok0 and conv.all()
+    np.testing.assert_allclose(V, g["swt0_V"])
+    check_currents(I, g["swt0_I"], g["swt0_Iflr"])
+    check_fields(psi, n, p, g["swt0_psi"], g["swt0_n"], g["swt0_p"], g["kind"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_small_sweeps_default_match_reference(lib, name):
+    """Production tolerances (the GUI's solver tuple).  The reference then converges
+    the quasi-Fermi level of a carrier only where it is >= 1e-3 of the local charge
+    scale (its Gummel weight, semiconductor_3d.c:3136-3144), and its terminal currents
+    only to its own tolerance: n, p are compared on those nodes, and a current may
+    differ by the reference's own distance to its converged value."""
     g = golden(name)
     w, mat, bias = MG.build(lib, name)
     s = w.sweeps[0]
     ok0, V, I, F, conv, psi, n, p = sweep_fields(lib, w, s)
     assert ok0 and conv.all()
     np.testing.assert_allclose(V, g["sw0_V"])
-    check_currents(I, g["sw0_I"], g["sw0_Iflr"])
-    check_fields(psi, n, p, g["sw0_psi"], g["sw0_n"], g["sw0_p"], g["kind"])
+    own = 2.0 * np.abs(g["sw0_I"] - g["swt0_I"])
+    check_currents(I, g["sw0_I"], np.maximum(g["sw0_Iflr"], own))
+    dpsi = np.abs(psi - g["sw0_psi"]).max()
+    assert dpsi <= PSI_TOL, f"psi differs by {dpsi:.3e} V"
+    D_ = np.abs(g["Nd"] - g["Na"])
+    free = (g["kind"] == 0) & (g["con"] == 0)
+    for a, b, o, lab in ((n, g["sw0_n"], g["sw0_p"], "n"), (p, g["sw0_p"], g["sw0_n"], "p")):
+        sig = free[None, :] & (b > NP_FLOOR) & (b >= 1e-3 * (b + o + D_[None, :]))
+        if not sig.any():
+            continue
+        rel = np.abs(a[sig] - b[sig]) / b[sig]
+        assert rel.max() <= NP_RTOL, f"{lab} differs by {rel.max():.3e} relative"
 
 
 def reference_lib():
@@ -86,16 +118,31 @@ def reference_lib():
     return abi.bind(ctypes.CDLL(path))
 
 
-def test_pn_diode_40cubed_matches_reference(lib):
-    """The 40^3 Si pn diode sweep 0..0.6 V (13 points) on both libraries."""
+def test_pn_diode_40cubed_matches_reference(lib, monkeypatch):
+    """The 40^3 Si pn diode sweep 0..0.6 V (13 points) on both libraries, run live:
+    converged tightly, every target on every node; at the production tolerances, the
+    currents within the reference's own error bar (its distance to its converged value,
+    or its round-off floor)."""
     ref = reference_lib()
     ref.api3_set_threads(os.cpu_count() or 1)
     out = {}
-    for tag, L in (("gpu", lib), ("ref", ref)):
-        w = D.pn_diode(L)
-        out[tag] = sweep_fields(L, w, w.sweeps[0])
-    ok0, V, I, F, conv, psi, n, p = out["gpu"]
-    rok0, rV, rI, rF, rconv, rpsi, rn, rp = out["ref"]
-    assert ok0 and conv.all() and rconv.all()
-    check_currents(I, rI, rF)
-    check_fields(psi, n, p, rpsi, rn, rp, np.zeros(psi.shape[1], int))     # all nodes silicon
+    for tight in (0, 1):
+        for k, v in MG.TIGHT_ENV.items():
+            if tight:
+                monkeypatch.setenv(k, v)
+            else:
+                monkeypatch.delenv(k, raising=False)
+        for tag, L in (("gpu", lib), ("ref", ref)):
+            w = D.pn_diode(L)
+            if tight:
+                L.api3_set_solver(*MG.TIGHT_SOLVER)
+            out[tag, tight] = sweep_fields(L, w, w.sweeps[0])
+    allsi = np.zeros(out["gpu", 0][5].shape[1], int)           # every node silicon
+    for tight in (0, 1):
+        assert out["gpu", tight][0] and out["gpu", tight][4].all() and out["ref", tight][4].all()
+    g1, r1 = out["gpu", 1], out["ref", 1]
+    check_currents(g1[2], r1[2], r1[3])
+    check_fields(g1[5], g1[6], g1[7], r1[5], r1[6], r1[7], allsi)
+    g0, r0 = out["gpu", 0], out["ref", 0]
+    check_currents(g0[2], r0[2], np.maximum(r0[3], 2.0 * np.abs(r0[2] - r1[2])))
+    assert np.abs(g0[5] - r0[5]).max() <= PSI_TOL
