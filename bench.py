@@ -7,9 +7,12 @@ Workload (the precision-path configuration): n-MOSFET on a 120x80x60 tensor mesh
 swept 0..1.2 V in 0.05 V steps (25 points) at Vd = 0.05 V and 1.0 V.  Synthetic device
 data built by semiconductor_devices_simulator_b200/devices.py (no dataset involved).
 
-A step is one Id-Vg sweep (25 bias points) through the library's C ABI
-(api3_set_contact_V + api3_resolve per point, the way main.py's run_sweep drives it),
-alternating the two drain biases.  Bias points/s = converged points / time of the sweep;
+A step is the workload's two Id-Vg sweeps (24 resolved bias points each after the first,
+which api3_solve solves) through the library's C ABI (api3_set_contact_V + api3_resolve
+per point, the way main.py's run_sweep drives it), the two sweeps solved concurrently by
+two solver instances (api3b_new / api3b_use), each on its own host thread and CUDA
+stream.  Bias points/s = converged points / time of the step (the slower stream's
+CUDA-event time);
 device set-up and the equilibrium + ramp to the first point (api3_solve) are outside
 the timed region, as the metric defines.  `value` reads only the terminal currents per
 point (state resident in HBM); `e2e` also copies psi, n and p of every point to host
@@ -198,28 +201,64 @@ def cpu_baseline(mesh, seconds):
                       f"{dt:.1f} s"}
 
 
+class Sweeper:
+    """One solver instance on its own host thread and CUDA stream, solving one sweep."""
+
+    def __init__(self, lib, mesh, sweep_index, dev):
+        self.lib, self.mesh, self.si = lib, mesh, sweep_index
+        self.h = lib.api3b_new()
+        self.dev = dev
+        self.w = None
+
+    def _use(self):
+        self.lib.api3b_use(self.h)
+        self.lib.b200x_set_device(self.dev)
+
+    def prepare(self):
+        self._use()
+        if self.w is None:
+            self.w = build(self.lib, self.mesh)
+            self.lib.api3_set_verbose(0)
+        D.start_sweep(self.lib, self.w, self.w.sweeps[self.si])   # untimed: equilibrium + ramp
+
+    def run(self, fields):
+        self._use()
+        self.lib.b200x_stream_timer(0)
+        t0 = time.perf_counter()
+        self.npts, self.conv = sweep_points(self.lib, self.w, self.w.sweeps[self.si], fields=fields)
+        self.dev_s = self.lib.b200x_stream_timer(1) / 1e3
+        self.wall = time.perf_counter() - t0
+
+
+def concurrent(workers, fn):
+    th = [threading.Thread(target=fn, args=(w,)) for w in workers]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+
+
 def run_b200(a, dist):
     import semiconductor_devices_simulator_b200 as S
     mesh = tuple(int(v) for v in a.mesh.split(","))
     lib = S.load()
     lib.b200x_set_device(dist.local)
-    w = build(lib, mesh)
-    nsw = len(w.sweeps)
-    lib.api3_set_verbose(0)
+    nsw = 2                                   # the two drain biases of the workload
+    workers = [Sweeper(lib, mesh, (q + dist.rank) % nsw, dist.local) for q in range(nsw)]
+    w = None
 
     def step(i, fields=False, timed=True):
-        s = w.sweeps[(i + dist.rank) % nsw]
-        D.start_sweep(lib, w, s)                         # untimed: set-up, equilibrium, ramp
+        """Both sweeps, concurrently (one instance, thread and stream each)."""
+        concurrent(workers, lambda s: s.prepare())
         dist.barrier()
-        lib.b200x_stream_timer(0)
         t0 = time.perf_counter()
-        npts, conv = sweep_points(lib, w, s, fields=fields)
-        ms = lib.b200x_stream_timer(1)
+        concurrent(workers, lambda s: s.run(fields))
         wall = time.perf_counter() - t0
-        return npts, conv, ms / 1e3, wall
+        return (sum(s.npts for s in workers), sum(s.conv for s in workers), max(s.dev_s for s in workers), wall)
 
     for i in range(a.warmup):
         step(i)
+    w = workers[0].w
     clocks = Clocks(dist.local)
     clocks.start()
     l0 = lib.b200x_launches()
@@ -240,9 +279,11 @@ def run_b200(a, dist):
         e_pts, e_wall = tot_pts, tot_wall
     # roofline: one more step with every launch timed by CUDA events on the solver stream
     prof = None
-    if not a.no_profile:
+    if not a.no_profile:                      # event timing is per thread: one sweep alone
+        s0 = workers[0]
+        s0.prepare()
         nk = lib.b200x_prof(1)
-        step(a.warmup)
+        s0.run(False)
         lib.b200x_prof(0)
         rows = []
         for k in range(nk):
@@ -272,7 +313,7 @@ def run_b200(a, dist):
                        for r in sorted(prof, key=lambda r: -r[1]) if r[2] > 0}
         h2d = 8 * 4 * len(w.contacts)                              # contact voltages per point
         d2h = 3 * 8 * w.N + 16 * len(w.contacts)                   # psi, n, p + currents per point
-        npts_step = len(w.sweeps[0]["V"]) - 1
+        npts_step = (len(w.sweeps[0]["V"]) - 1) * nsw
         out = {
             "metric": METRIC, "value": round(pts_all / T, 4), "unit": UNIT, "n_gpus": dist.world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * T / a.steps, 2),
@@ -281,7 +322,7 @@ def run_b200(a, dist):
             "config": {"workload": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]}_idvg",
                        "nodes": w.N, "points_per_step": npts_step, "drain_biases_V": [0.05, 1.0],
                        "gate_sweep_V": [0.0, 1.2, 0.05], "models": 4, "solver": list(D.GUI_SOLVER),
-                       "parallelism": f"replicas{dist.world}",
+                       "parallelism": f"replicas{dist.world}, {nsw} concurrent sweeps per GPU (instance + stream each)",
                        "l2": "state of 576k nodes (~0.5 GB) exceeds the 126 MB L2; no flush"},
             "converged_points": tot_conv, "wall_s": round(tot_wall, 3),
             "e2e": {"value": round(e_all / e_T, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * npts_step,

@@ -1,0 +1,229 @@
+/*
+ * libsemisim_b200 - C ABI of the B200 solve path of SemiSim 3D.
+ *
+ * The library is a drop-in for the reference core semiconductor_3d.c: it exports every
+ * api3_* entry point with the reference's exact C signature and semantics (one global
+ * device; 1 = ok / 0 = failure; getters NaN for a bad index or no solution), so the
+ * reference's main.py, its sweeps and validate.py load it unchanged through
+ *     SEMISIM_SO=<path>/libsemisim_b200.so
+ * (semibuild.py:516-522).  Each declaration names the reference function it replaces
+ * (semiconductor_3d.c:<line>) and, where one exists, the ctypes binding that loads it.
+ *
+ * The solve path (prepare, equilibrium, Newton-Poisson, Scharfetter-Gummel continuity,
+ * Gummel / Anderson, continuation, terminal currents) runs on the GPU; set-up calls only
+ * record the device and work without one.  Models outside the library's scope (gate
+ * tunnelling, thermionic-emission contacts, impact and incomplete ionisation, quantum
+ * confinement, surface mobility, deep traps) and prism meshes make the solve return 0
+ * with a message on stderr; their standalone evaluators return NaN.
+ */
+#ifndef SEMISIM_B200_H
+#define SEMISIM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* replaces semiconductor_3d.c:4570; bound at main.py:176 */
+void api3_init(void);
+/* replaces semiconductor_3d.c:4599; bound at main.py:3498 */
+void api3_set_threads(int n);
+/* replaces semiconductor_3d.c:4607 */
+void api3_set_verbose(int v);
+/* replaces semiconductor_3d.c:4618; bound at main.py:3509 */
+int api3_trap_species(int type, int ref, double E, double sn, double sp);
+/* replaces semiconductor_3d.c:4629; bound at main.py:3510 */
+int api3_trap_add(int sid, int n, const int *nodes, const double *dens);
+/* replaces semiconductor_3d.c:4645 */
+void api3_traps_clear(void);
+/* replaces semiconductor_3d.c:4646; bound at main.py:3511 */
+int api3_charge_add(int n, const int *nodes, const double *rho);
+/* replaces semiconductor_3d.c:4653 */
+int api3_n_trap_entries(void);
+/* replaces semiconductor_3d.c:4657; bound at main.py:187 */
+void api3_set_models(int flags);
+/* replaces semiconductor_3d.c:4660; bound at main.py:188 */
+void api3_set_caxis(int ax);
+/* replaces semiconductor_3d.c:4661 */
+int api3_get_caxis(void);
+/* replaces semiconductor_3d.c:4663; bound at main.py:177 */
+int api3_add_material(int id, double T);
+/* replaces semiconductor_3d.c:4671; bound at main.py:3512 */
+int api3_set_mat_tau(int mi, double tn, double tp);
+/* replaces semiconductor_3d.c:4679; bound at main.py:179 */
+int api3_set_grid_coords(int Nx,int Ny,int Nz,const double *xs,const double *ys,const double *zs);
+/* replaces semiconductor_3d.c:4693; bound at main.py:178 */
+void api3_set_grid(int Nx,int Ny,int Nz,double Lx,double Ly,double Lz);
+/* replaces semiconductor_3d.c:4708; bound at main.py:180 */
+void api3_set_solver(int mp,int mc,int mg,double tp,double tc,double op,double oc);
+/* replaces semiconductor_3d.c:4718; bound at main.py:181 */
+void api3_set_region(int x0,int y0,int z0,int x1,int y1,int z1,int midx,double Nd,double Na);
+/* replaces semiconductor_3d.c:4731 */
+void api3_add_fixed_charge(int x0,int y0,int z0,int x1,int y1,int z1,double Nf);
+/* replaces semiconductor_3d.c:4742; bound at main.py:186 */
+void api3_add_sheet_charge(int axis,int idx,int a0,int a1,int b0,int b1,double sigma);
+/* replaces semiconductor_3d.c:4757; bound at main.py:184 */
+int api3_add_contact_ex(int face,int i0,int i1,int j0,int j1,int k0,int k1, int bc,double V,double pm,double tox,double Nox);
+/* replaces semiconductor_3d.c:4772; bound at main.py:182 */
+void api3_add_contact(int face,int i0,int i1,int j0,int j1,int bc,double V,double pm);
+/* replaces semiconductor_3d.c:4775; bound at main.py:185 */
+void api3_clear_contacts(void);
+/* replaces semiconductor_3d.c:4779; bound at main.py:3500 */
+int api3_set_gate_stack(int cid,int nl,const int *mat,const double *t);
+/* replaces semiconductor_3d.c:4795; bound at main.py:3503 */
+int api3_set_mesh_graph(int N,int E,const int *rp,const int *cj,const double *h, const double *ar,const double *vol,const double *pos);
+/* replaces semiconductor_3d.c:4806; bound at main.py:3504 */
+int api3_is_graph(void);
+/* replaces semiconductor_3d.c:4808; bound at main.py:3505 */
+void api3_set_node_data(const int *mat,const double *Nd,const double *Na,const double *Nf);
+/* replaces semiconductor_3d.c:4821; bound at main.py:3506 */
+int api3_set_con_nodes(int cid,int n,const int *nodes,const double *areas);
+/* replaces semiconductor_3d.c:4838; bound at main.py:3507 */
+void api3_set_walls(const double *w);
+/* replaces semiconductor_3d.c:4844; bound at main.py:3501 */
+int api3_get_ntp(int cid);
+/* replaces semiconductor_3d.c:4855; bound at validate.py:42 */
+double api3_tun_eval(int smat,int nl,const int *mat,const double *t,double psi, double phin,double phip,double Vg,double pm,double *out);
+/* replaces semiconductor_3d.c:4869; bound at validate.py:43 */
+double api3_mlda_factor(int mi,double a,double b,int hole);
+/* replaces semiconductor_3d.c:4878; bound at validate.py:46 */
+double api3_coulomb_inv(int mi,double F,double n,double NC,double NA);
+/* replaces semiconductor_3d.c:4885 */
+int api3_set_surface_mobility(int mi,double delta,double eta,double mu1);
+/* replaces semiconductor_3d.c:4894; bound at validate.py:44 */
+double api3_lombardi(int mi,double mub,double F,double Nt,double Dw,int hole);
+/* replaces semiconductor_3d.c:4898; bound at main.py:191 */
+void api3_set_contact_V(int cid,double V);
+/* replaces semiconductor_3d.c:4899; bound at main.py:3449 */
+int api3_get_ncon(void);
+/* replaces semiconductor_3d.c:4900; bound at main.py:192 */
+double api3_get_contact_I(int cid);
+/* replaces semiconductor_3d.c:4901; bound at main.py:193 */
+double api3_get_contact_A(int cid);
+/* replaces semiconductor_3d.c:4902; bound at main.py:194 */
+double api3_get_contact_In(int cid);
+/* replaces semiconductor_3d.c:4904; bound at main.py:195 */
+double api3_get_contact_Ifloor(int cid);
+/* replaces semiconductor_3d.c:4906; bound at main.py:196 */
+double api3_get_contact_Iraw(int cid);
+/* replaces semiconductor_3d.c:4907; bound at main.py:3499 */
+int api3_get_aa_depth(void);
+/* replaces semiconductor_3d.c:4908; bound at main.py:3497 */
+double api3_get_contact_Vsolved(int cid);
+/* replaces semiconductor_3d.c:4922; bound at main.py:3494 */
+void api3_request_stop(void);
+/* replaces semiconductor_3d.c:4923; bound at main.py:3495 */
+void api3_clear_stop(void);
+/* replaces semiconductor_3d.c:4924 */
+int api3_stop_requested(void);
+/* replaces semiconductor_3d.c:4926; bound at main.py:3496 */
+void api3_get_progress(double *out);
+/* replaces semiconductor_3d.c:4928; bound at main.py:189 */
+int api3_solve(void);
+/* replaces semiconductor_3d.c:4930; bound at main.py:190 */
+int api3_resolve(void);
+/* replaces semiconductor_3d.c:4934; bound at main.py:215 */
+void api3_iv_sweep(int cid,double Vs,double Ve,int Npts,double *Varr,double *Jarr,int *Carr);
+/* replaces semiconductor_3d.c:4958; bound at main.py:217 */
+void api3_iv_sweep2(int cid,double Vs,double Ve,int Npts,double *Varr, double *Iarr,double *Farr,int *Carr);
+/* replaces semiconductor_3d.c:4981; bound at main.py:204 */
+double api3_get_Emax(void);
+/* replaces semiconductor_3d.c:5003; bound at main.py:198 */
+int api3_get_Nx(void);
+/* replaces semiconductor_3d.c:5004; bound at main.py:198 */
+int api3_get_Ny(void);
+/* replaces semiconductor_3d.c:5005; bound at main.py:198 */
+int api3_get_Nz(void);
+/* replaces semiconductor_3d.c:5006; bound at main.py:199 */
+int api3_get_conv(void);
+/* replaces semiconductor_3d.c:5007; bound at main.py:199 */
+int api3_get_iter(void);
+/* replaces semiconductor_3d.c:5008; bound at main.py:199 */
+double api3_get_res(void);
+/* replaces semiconductor_3d.c:5009; bound at main.py:200 */
+double api3_get_xs(int i);
+/* replaces semiconductor_3d.c:5010; bound at main.py:200 */
+double api3_get_ys(int j);
+/* replaces semiconductor_3d.c:5011; bound at main.py:200 */
+double api3_get_zs(int l);
+/* replaces semiconductor_3d.c:5012; bound at validate.py:41 */
+double api3_get_Cref(void);
+/* replaces semiconductor_3d.c:5013; bound at main.py:197 */
+long long api3_get_stat(int w);
+/* replaces semiconductor_3d.c:5019; bound at validate.py:45 */
+void api3_set_predictor(int on);
+/* replaces semiconductor_3d.c:5023; bound at main.py:3999 */
+int api3_get_state(double *phi, double *phin, double *phip);
+/* replaces semiconductor_3d.c:5030; bound at main.py:4000 */
+int api3_set_state(const double *phi, const double *phin, const double *phip);
+/* replaces semiconductor_3d.c:5043 */
+double api3_get_time(int w);
+/* replaces semiconductor_3d.c:5048; bound at main.py:201 */
+double api3_mat_ni(int mi);
+/* replaces semiconductor_3d.c:5049; bound at main.py:201 */
+double api3_mat_Eg(int mi);
+/* replaces semiconductor_3d.c:5127; bound at main.py:202 */
+void api3_bulk_copy(int which,double *out);
+/* replaces semiconductor_3d.c:5137; bound at main.py:3513 */
+void api3_carrier_sums(double *out);
+/* replaces semiconductor_3d.c:5192; bound at main.py:208 */
+int api3_charge_partition(const int *cterm);
+/* replaces semiconductor_3d.c:5248; bound at main.py:209 */
+int api3_terminal_charges(int nt, double *Qt);
+/* replaces semiconductor_3d.c:5284; bound at main.py:212 */
+int api3_face_J(int ax, int carrier, double *out);
+/* replaces semiconductor_3d.c:5300; bound at main.py:210 */
+int api3_charge_owner(int *out);
+/* replaces semiconductor_3d.c:5308; bound at main.py:211 */
+double api3_ins_field_max(double *pos);
+/* replaces semiconductor_3d.c:5341; bound at validate.py:1229 */
+double api3_get_phi(int k);
+/* replaces semiconductor_3d.c:5342 */
+double api3_get_n(int k);
+/* replaces semiconductor_3d.c:5343 */
+double api3_get_p(int k);
+/* replaces semiconductor_3d.c:5344 */
+double api3_get_Ec(int k);
+/* replaces semiconductor_3d.c:5345 */
+double api3_get_Ev(int k);
+/* replaces semiconductor_3d.c:5346 */
+double api3_get_Efn(int k);
+/* replaces semiconductor_3d.c:5347 */
+double api3_get_Efp(int k);
+/* replaces semiconductor_3d.c:5348 */
+double api3_get_Jx(int k);
+/* replaces semiconductor_3d.c:5349 */
+double api3_get_Jy(int k);
+/* replaces semiconductor_3d.c:5350 */
+double api3_get_Jz(int k);
+/* replaces semiconductor_3d.c:5351 */
+double api3_get_mun(int k);
+/* replaces semiconductor_3d.c:5352 */
+double api3_get_mup(int k);
+/* replaces semiconductor_3d.c:5353 */
+double api3_get_R(int k);
+
+/* ---- additive entries (no counterpart in the reference) ---- */
+
+/* Pin the low-field mobility of material mi to constants mun / mup (m^2/Vs),
+   independent of doping and temperature; 1 = done, 0 = bad index or value.  The oracle
+   harness exports the same entry so both libraries are set up identically. */
+int api3_set_mat_mobility(int mi, double mun, double mup);
+
+/* More solver instances.  The reference core has one global device; here every
+   api3_* call acts on the calling thread's current instance (instance 0 = the global
+   device of the reference ABI).  Independent devices solved from different host
+   threads run concurrently on the GPU, each instance on its own CUDA stream.
+   api3b_new: a new, empty instance; returns its handle (>= 1).
+   api3b_use: make instance h current for the calling thread (0: the global one);
+              1 = done, 0 = no such instance.
+   api3b_current: the calling thread's current instance.
+   api3b_free: release an instance and its device memory; 1 = done. */
+int api3b_new(void);
+int api3b_use(int h);
+int api3b_current(void);
+int api3b_free(int h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEMISIM_B200_H */

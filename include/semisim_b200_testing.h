@@ -1,0 +1,65 @@
+/*
+ * libsemisim_b200 - kernel-level test and measurement hooks (b200x_*).
+ *
+ * Not part of the reference ABI (no counterpart in semiconductor_3d.c).  They run one
+ * device kernel of the solve path on the calling thread's current instance, with inputs
+ * and outputs through host buffers, so the parity tests can compare every kernel with
+ * the oracle on seeded states, and bench.py can time kernels with CUDA events.
+ */
+#ifndef SEMISIM_B200_TESTING_H
+#define SEMISIM_B200_TESTING_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* prepare the recorded device on the GPU (masks, Robin areas, materials); 1 = done */
+int b200x_prepare(void);
+/* per node: kind, contact id + 1, gate id + 1, Robin area (m^2) */
+int b200x_masks(int *kind, int *con, int *gate, double *robA);
+/* device state arrays: 0 psi, 1 phi_n, 2 phi_p, 3 n, 4 p, 5/6 low-field mobility n/p,
+   7 sol, 8 rhs, 9 sc, 10 dsc, 16..21 face mobility (n x,y,z; p x,y,z) */
+int b200x_set(int which, const double *in);
+int b200x_get(int which, double *out);
+double b200x_vlo(void);
+double b200x_vhi(void);
+void b200x_apply_bc(void);
+void b200x_rebuild_np(void);
+void b200x_upd_mob(void);
+void b200x_clamp_qf(void);
+/* Poisson residual, Jacobian (7 x N) and sc at psi; returns ||F/diag|| */
+double b200x_poisson(const double *phi, double *F, double *A7, double *sc);
+/* scaled SG continuity system of carrier `hole` at the present state */
+void b200x_cont_assemble(int hole, double *A7, double *rhs, double *sc, double *dsc);
+/* carrier / quasi-Fermi update from sol; returns the weighted max |dq| */
+double b200x_cont_update(int hole, const double *sol, double lo, double hi, double *dq);
+/* terminal currents, scales and electron parts per contact */
+void b200x_currents(double *I, double *S, double *In);
+/* multigrid hierarchy of the system now in A (qsign 0 Poisson, +1/-1 continuity) */
+int b200x_mg_setup(int qsign);
+int b200x_mg_level(int L, int *dims, double *A7, double *pw);
+/* Krylov solves of the system now in A / rhs */
+int b200x_bicgstab(int maxit, double rtol, double atol, int qsign, const double *x0, double *sol, double *rn,
+                   double *r0);
+int b200x_pcg(int maxit, double rtol, double *sol);
+/* floating-block balance of a continuity solution (in place) */
+int b200x_float_fix(int hole, double *sol);
+/* device memory of the instance (bytes) */
+long long b200x_device_bytes(void);
+/* CUDA device of the solver (before its first solve); 1 = done */
+int b200x_set_device(int dev);
+/* microseconds per launch of one kernel over `reps` back-to-back launches */
+double b200x_bench(int which, int reps);
+/* CUDA-event timer on the instance's stream: op 0 start, op 1 stop -> elapsed ms */
+double b200x_stream_timer(int op);
+/* launch accounting and per-kernel-class event timing */
+int b200x_prof(int on);
+int b200x_prof_read(int id, double *ms, double *count, double *bytes);
+const char *b200x_prof_name(int id);
+int b200x_prof_detail(int q, int *id, double *nodes, double *ms, double *count);
+unsigned long long b200x_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEMISIM_B200_TESTING_H */

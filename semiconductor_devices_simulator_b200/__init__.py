@@ -42,9 +42,11 @@ HOOKS = {
     "b200x_device_bytes": (_LL, []),
     "b200x_stream_timer": (_D, [_I]),
     "b200x_set_device": (_I, [_I]),
+    "b200x_bench": (_D, [_I, _I]),
     "b200x_prof": (_I, [_I]),
     "b200x_prof_read": (_I, [_I, _DP, _DP, _DP]),
     "b200x_prof_name": (ctypes.c_char_p, [_I]),
+    "b200x_prof_detail": (_I, [_I, _IP, _DP, _DP, _DP]),
     "b200x_launches": (ctypes.c_ulonglong, []),
 }
 # state arrays reachable through b200x_set / b200x_get

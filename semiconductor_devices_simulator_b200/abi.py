@@ -113,6 +113,11 @@ API3 = {
 EXTRA = {
     # constant low-field mobility (m^2/Vs) of a material; no reference counterpart
     "api3_set_mat_mobility": (_I, [_I, _D, _D]),
+    # more solver instances (the reference has one global device); per-thread selection
+    "api3b_new": (_I, []),
+    "api3b_use": (_I, [_I]),
+    "api3b_current": (_I, []),
+    "api3b_free": (_I, [_I]),
 }
 
 

@@ -10,6 +10,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 #include "solver_ctx.h"
@@ -18,10 +20,23 @@ using namespace ss;
 
 namespace {
 
-Inst g_dev;
-int g_n_trap_species = 0;
-struct TrapSpec { int type, ref; double E, sn, sp; };
-TrapSpec g_tsp[512];
+// Instances: 0 is the reference ABI's single global device (semiconductor_3d.c:366);
+// api3b_new adds more.  Every api3_* call acts on the calling thread's current
+// instance (api3b_use), so independent devices can be solved from several host threads
+// at once, each on its own CUDA stream.
+Inst g_dev0;
+std::mutex g_reg_mu;
+std::vector<std::unique_ptr<Inst>> g_reg;       // g_reg[h-1] = instance h
+thread_local Inst *t_cur = nullptr;
+Inst &ss_cur() { return t_cur ? *t_cur : g_dev0; }
+
+}  // namespace
+#define g_dev (ss_cur())
+#define g_qown (g_dev.qown)
+#define g_qct (g_dev.qct)
+#define g_n_trap_species (g_dev.n_tsp)
+#define g_tsp (g_dev.tsp)
+namespace {
 
 const char *env_get(const char *n) { return std::getenv(n); }
 
@@ -86,12 +101,9 @@ int qnbrs(const Inst &d, size_t k, size_t *nb, double *cf, double *hh) {
     return m;
 }
 
-std::vector<int> g_qown;
-int g_qct[NC_MAX];
-
 }  // namespace
 
-// the reference ABI's single global device (semiconductor_3d.c:366), for the test hooks
+// the calling thread's current instance, for the test hooks
 Inst *b200_global_dev() { return &g_dev; }
 
 extern "C" {
@@ -118,6 +130,7 @@ void api3_init(void) {                                      // semiconductor_3d.
     if (const char *m = env_get("SEMISIM_CATOL")) g_knobs.cont_atol = std::atof(m);
     if (const char *m = env_get("SEMISIM_QFM")) g_knobs.qf_margin = std::atof(m);
     if (const char *m = env_get("SEMISIM_B200_CHECK")) { const int q = std::atoi(m); if (q >= 1 && q <= 64) g_knobs.check_every = q; }
+    if (const char *m = env_get("SEMISIM_B200_GRAPHS")) g_use_graphs = std::atoi(m) != 0;
     g_n_trap_species = 0;
 }
 
@@ -658,6 +671,38 @@ double api3_ins_field_max(double *pos) {                    // semiconductor_3d.
     }
     return best;
 }
+// ------------------------------------------------------------------ instances (additive)
+// Additive entries with no counterpart in the reference (whose core has one global
+// device): more solver instances, each with its own device memory and CUDA stream.
+// api3b_use selects the instance the calling thread's api3_* calls act on.
+int api3b_new(void) {
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_reg.emplace_back(new Inst());
+    return (int)g_reg.size();
+}
+int api3b_use(int h) {
+    if (h == 0) { t_cur = nullptr; return 1; }
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    if (h < 1 || h > (int)g_reg.size() || !g_reg[h - 1]) return 0;
+    t_cur = g_reg[h - 1].get();
+    return 1;
+}
+int api3b_current(void) {
+    if (!t_cur) return 0;
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    for (size_t q = 0; q < g_reg.size(); q++)
+        if (g_reg[q].get() == t_cur) return (int)q + 1;
+    return -1;
+}
+int api3b_free(int h) {
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    if (h < 1 || h > (int)g_reg.size() || !g_reg[h - 1]) return 0;
+    if (t_cur == g_reg[h - 1].get()) t_cur = nullptr;
+    gpu_free(*g_reg[h - 1]);
+    g_reg[h - 1].reset();
+    return 1;
+}
+
 double api3_get_phi(int k) { return node_val1(0, k); }
 double api3_get_n(int k) { return node_val1(1, k); }
 double api3_get_p(int k) { return node_val1(2, k); }

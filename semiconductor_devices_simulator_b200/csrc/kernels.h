@@ -6,9 +6,17 @@
 
 namespace ss {
 
+// instantiated device-looped Krylov graphs of one instance (kernels_la.cu)
+struct LoopGraphs {
+    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+    int kernels[3] = {0, 0, 0};
+    int failed = 0;
+};
+
 // Launch context: the device parameter records of `ninst` instances (dP), the host copy
 // of instance 0's record (sizes), the stream.
 struct Ctx {
+    LoopGraphs *lg = nullptr;
     const DevP *dP = nullptr;
     DevP h{};
     int ninst = 1;

@@ -147,16 +147,11 @@ __global__ void k_ff_apply(const DevP *__restrict__ Ps, const double *scale) {
     }
 }
 
-static double *g_ffbuf = nullptr;
-static int *g_ffint = nullptr;
-
 int float_fix(Inst &d, int hole) {
     Ctx c = make_ctx(d);
     const dim3 g(c.nodes_blocks(), 1);
-    if (!g_ffbuf) {
-        cudaMalloc(&g_ffbuf, sizeof(double) * FF_MAX_BLOCKS * 6);
-        cudaMalloc(&g_ffint, sizeof(int) * (FF_MAX_BLOCKS + 16));
-    }
+    double *const g_ffbuf = d.g.h.ffbuf;
+    int *const g_ffint = d.g.h.ffint;
     int *changed = g_ffint, *count = g_ffint + 1, *roots = g_ffint + 16;
     SS_LAUNCH(PF_CCL, d.N, k_ff_init, g, TPB, c.st, c.dP, hole);
     int h = 1, cycles = 0;

@@ -14,12 +14,18 @@
 // reads the instance's `active` word, so the host can queue several iterations and
 // read the status once.
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
+
+#include <cooperative_groups.h>
 
 #include "device_common.cuh"
 #include "prof.h"
 #include "kernels.h"
 #include "solver_ctx.h"
+
+namespace cg = cooperative_groups;
 
 namespace ss {
 
@@ -436,26 +442,298 @@ void mg_setup(const Ctx &c, const MGHost &mg, int qsign) {
 // one V(1,1) cycle x = M^-1 b on the level-0 vectors (bsel -> xsel); mg_on = 0 applies
 // the level-0 smoother alone (the reference's ILU-only fallback).  gate: 0 always run,
 // 1 only while the instance's Krylov loop is active, 2 also not after a half-step exit.
-void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
-    if (!mg_on || mg.maxlev < 2) {
-        SS_LAUNCH(PF_SMOOTH_B, c.maxN, k_smooth_black, grid_nodes(c), TPB, c.st, c.dP, 0, bsel, xsel, 0, gate);
-        SS_LAUNCH(PF_SMOOTH_R, c.maxN, k_smooth_red, grid_nodes(c), TPB, c.st, c.dP, 0, bsel, xsel, 0, gate);
+// ---- fine levels: one kernel per pass, all SMs
+// Smoother half sweep over the nodes of one colour only: thread t of a row (j,l) takes
+// i = 2t + ((j + l + colour) & 1), so every lane does work (colour 1 = black, 0 = red).
+__global__ void k_smooth_c(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int mode, int color, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if ((L > 0 && L >= P.nlev - 1) || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const LevView v = levview(P, L, bsel, xsel);
+    const int hx = (v.Nx + 1) >> 1, rows = v.Ny * v.Nz;
+    const double *src = mode ? v.r : v.b;
+    const double *zb = mode ? v.r : v.x;
+    SS_GRID_LOOP(t, hx * rows) {
+        const int row = t / hx, ti = t - row * hx;
+        const int l = row / v.Ny, j = row - l * v.Ny;
+        const int i = 2 * ti + ((j + l + color) & 1);
+        if (i >= v.Nx) continue;
+        const int k = i + v.Nx * row;
+        double z;
+        if (color) {
+            const double s = offdiag_apply_div<double>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
+            z = (src[k] - s) / v.D[k];
+            if (mode) { v.x[k] += z; v.r[k] = z; }
+            else v.x[k] = z;
+        } else {
+            const double s = offdiag_apply<double>(v.A, zb, k, i, j, l, v.Nx, v.Ny, v.Nz);
+            z = (src[k] - s) / v.D[k];
+            if (mode) v.x[k] += z;
+            else v.x[k] = z;
+        }
+    }
+}
+
+// Weighted residual of every fine node summed into its 2x2x2 aggregate.  Block (32, 4):
+// threadIdx.x runs along fine x, threadIdx.y picks the (j, l) parity inside the coarse
+// row blockIdx.z; pairs along x meet through a shuffle, the four parities through
+// shared memory.  One thread per fine node (the restriction of semiconductor_3d.c:
+// 2028-2037 applied to the residual of 1984-1991).
+__global__ void __launch_bounds__(128) k_resid_restrict2(const DevP *__restrict__ Ps, int L, int bsel, int xsel,
+                                                         int wsel, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if (L >= P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const LevView f = levview(P, L, bsel, xsel);
+    const LevelT<double> &cl = P.lev[L + 1];
+    const double *w = (L == 0 && wsel) ? P.dsc : nullptr;
+    const int R = blockIdx.z;                         // coarse row J + Cy*Lc
+    const bool rowok = R < cl.Ny * cl.Nz;
+    const int Lc = rowok ? R / cl.Ny : 0, Jc = rowok ? R - Lc * cl.Ny : 0;
+    const int dj = threadIdx.y & 1, dl = threadIdx.y >> 1;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = f.cy ? 2 * Jc + dj : Jc, l = f.cz ? 2 * Lc + dl : Lc;
+    const bool ok = rowok && i < f.Nx && j < f.Ny && l < f.Nz && (f.cy || dj == 0) && (f.cz || dl == 0);
+    double val = 0.0;
+    if (ok) {
+        const int k = i + f.Nx * (j + f.Ny * l);
+        const double r = f.b[k] - stencil_apply<double>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
+        val = w ? w[k] * r : r;
+    }
+    __shared__ double sh[4][32];
+    sh[threadIdx.y][threadIdx.x] = val;
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        double s = sh[0][threadIdx.x] + sh[1][threadIdx.x] + sh[2][threadIdx.x] + sh[3][threadIdx.x];
+        if (f.cx) {
+            s += __shfl_down_sync(0xffffffffu, s, 1);
+            if (rowok && !(threadIdx.x & 1) && i < f.Nx) cl.b[(i >> 1) + cl.Nx * R] = s;
+        } else if (rowok && i < f.Nx) {
+            cl.b[i + cl.Nx * R] = s;
+        }
+    }
+}
+
+// ---- small levels: the rest of the V-cycle in one thread-block cluster per instance
+// The CTAs of a cluster split every pass (cluster-stride loops); a hardware cluster
+// barrier (release / acquire at cluster scope) separates the passes, so each pass sees
+// the global writes of the one before.  One launch replaces ~7 launches per level.
+__device__ __forceinline__ int cl_first() {
+    return (int)cg::this_cluster().block_rank() * blockDim.x + threadIdx.x;
+}
+__device__ __forceinline__ int cl_stride() { return (int)cg::this_cluster().num_blocks() * blockDim.x; }
+__device__ __forceinline__ void cl_sync() { cg::this_cluster().sync(); }
+
+__device__ __forceinline__ void cta_smooth(const LevView &v, int color, int mode) {
+    const double *src = mode ? v.r : v.b;
+    const double *zb = mode ? v.r : v.x;
+    const int hx = (v.Nx + 1) >> 1, rows = v.Ny * v.Nz;
+    for (int t = cl_first(); t < hx * rows; t += cl_stride()) {
+        const int row = t / hx, ti = t - row * hx;
+        const int l = row / v.Ny, j = row - l * v.Ny;
+        const int i = 2 * ti + ((j + l + color) & 1);
+        if (i >= v.Nx) continue;
+        const int k = i + v.Nx * row;
+        if (color) {
+            const double s = offdiag_apply_div<double>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
+            const double z = (src[k] - s) / v.D[k];
+            if (mode) { v.x[k] += z; v.r[k] = z; }
+            else v.x[k] = z;
+        } else {
+            const double s = offdiag_apply<double>(v.A, zb, k, i, j, l, v.Nx, v.Ny, v.Nz);
+            const double z = (src[k] - s) / v.D[k];
+            if (mode) v.x[k] += z;
+            else v.x[k] = z;
+        }
+    }
+    cl_sync();
+}
+__device__ __forceinline__ void cta_resid_restrict(const LevView &f, const LevelT<double> &cl, const double *w) {
+    for (int K = cl_first(); K < cl.N; K += cl_stride()) {
+        const Node c = unidx(K, cl.Nx, cl.Ny);
+        const Agg g = agg_range(f, c.i, c.j, c.l);
+        double s = 0.0;
+        for (int l = g.l0; l <= g.l1; l++)
+            for (int j = g.j0; j <= g.j1; j++)
+                for (int i = g.i0; i <= g.i1; i++) {
+                    const int k = i + f.Nx * (j + f.Ny * l);
+                    const double r = f.b[k] - stencil_apply<double>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
+                    s += w ? w[k] * r : r;
+                }
+        cl.b[K] = s;
+    }
+    cl_sync();
+}
+__device__ __forceinline__ void cta_prolong(const LevView &f, const LevelT<double> &cl, double alpha) {
+    for (int k = cl_first(); k < f.N; k += cl_stride()) {
+        const Node a = unidx(k, f.Nx, f.Ny);
+        const int I = f.cx ? a.i >> 1 : a.i, J = f.cy ? a.j >> 1 : a.j, K = f.cz ? a.l >> 1 : a.l;
+        f.x[k] += alpha * f.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+    }
+    cl_sync();
+}
+__device__ __forceinline__ void cta_resid(const LevView &f) {
+    for (int k = cl_first(); k < f.N; k += cl_stride()) {
+        const Node a = unidx(k, f.Nx, f.Ny);
+        f.r[k] = f.b[k] - stencil_apply<double>(f.A, f.x, k, a.i, a.j, a.l, f.Nx, f.Ny, f.Nz);
+    }
+    cl_sync();
+}
+__device__ __forceinline__ void cta_dense(const LevelT<double> &v) {
+    const int n = v.N;
+    for (int r = cl_first(); r < n; r += cl_stride()) {
+        double s = 0.0;
+        for (int q = 0; q < n; q++) s += v.D[r * n + q] * v.b[q];
+        v.x[r] = s;
+    }
+    cl_sync();
+}
+
+constexpr int SMALL_TPB = 1024;
+__global__ void __launch_bounds__(SMALL_TPB) k_vcycle_small(const DevP *__restrict__ Ps, int Ls, int bsel, int xsel,
+                                                            int wsel, double alpha, int gate) {
+    const DevP &P = Ps[blockIdx.y];
+    if ((gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    const int nl = P.nlev;
+    if (nl == 1) {                                 // a single level: the smoother alone
+        const LevView v = levview(P, 0, bsel, xsel);
+        cta_smooth(v, 1, 0);
+        cta_smooth(v, 0, 0);
         return;
     }
-    for (int L = 0; L < mg.maxlev; L++) {
-        if (L < mg.maxlev - 1) {
-            SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_black, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, 0, gate);
-            SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_red, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, 0, gate);
-            SS_LAUNCH(PF_RESID_RESTRICT, mg.maxN[L + 1], k_resid_restrict, grid_n(c, mg.maxN[L + 1]), TPB, c.st, c.dP, L, bsel, xsel, wsel, gate);
-        }
-        if (L >= 1 && L >= mg.minlev - 1) SS_LAUNCH(PF_COARSE, COARSE_MAX, k_coarse_solve, dim3(1, c.ninst), 64, c.st, c.dP, L, gate);
+    for (int L = Ls; L < nl - 1; L++) {
+        const LevView v = levview(P, L, bsel, xsel);
+        cta_smooth(v, 1, 0);
+        cta_smooth(v, 0, 0);
+        cta_resid_restrict(v, P.lev[L + 1], (L == 0 && wsel) ? P.dsc : nullptr);
     }
-    for (int L = mg.maxlev - 2; L >= 0; L--) {
+    cta_dense(P.lev[nl - 1]);
+    for (int L = nl - 2; L >= Ls; L--) {
+        const LevView v = levview(P, L, bsel, xsel);
+        cta_prolong(v, P.lev[L + 1], alpha);
+        cta_resid(v);
+        cta_smooth(v, 1, 1);
+        cta_smooth(v, 0, 1);
+    }
+}
+
+int g_small_nodes = 2048;           // levels at or below this size run in the cluster kernel
+static int g_cluster = 0;           // CTAs per cluster of the small-level kernel (set on first use)
+
+// cluster size of the small-level kernel (16 CTAs when the device allows non-portable
+// clusters of 16, else 8) and the size split, read once (SEMISIM_B200_CLUSTER / _SMALL)
+static void small_init() {
+    if (!g_cluster) {
+        const char *e = std::getenv("SEMISIM_B200_CLUSTER");
+        g_cluster = (e && std::atoi(e) == 8) ? 8 : 16;
+        if (const char *s = std::getenv("SEMISIM_B200_SMALL")) g_small_nodes = std::atoi(s);
+        if (cudaFuncSetAttribute(k_vcycle_small, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+            g_cluster = 8;
+        cudaGetLastError();
+        cudaLaunchConfig_t q = {};
+        q.gridDim = dim3(g_cluster, 1);
+        q.blockDim = dim3(SMALL_TPB);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = g_cluster; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        q.attrs = at;
+        q.numAttrs = 1;
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, k_vcycle_small, &q) != cudaSuccess || ncl < 1) g_cluster = 8;
+        cudaGetLastError();
+    }
+}
+
+// launch the small-level V-cycle as clusters of g_cluster CTAs, one cluster per instance
+static void launch_small(const Ctx &c, int nodes, int Ls, int bsel, int xsel, int wsel, double alpha, int gate) {
+    small_init();
+    g_launches++;
+    t_launches++;
+    if (g_prof_on) prof_begin(PF_COARSE, c.st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g_cluster, c.ninst);
+    cfg.blockDim = dim3(SMALL_TPB);
+    cfg.stream = c.st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = g_cluster; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_vcycle_small, c.dP, Ls, bsel, xsel, wsel, alpha, gate);
+    if (g_prof_on) prof_end(PF_COARSE, c.st, nodes);
+}
+
+static inline dim3 grid_half(const Ctx &c, int L, const MGHost &mg) {
+    return grid_n(c, ((mg.maxNx[L] + 1) / 2) * (mg.maxN[L] / (mg.maxNx[L] > 0 ? mg.maxNx[L] : 1)));
+}
+
+void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
+    if (!mg_on) {
+        SS_LAUNCH(PF_SMOOTH_B, c.maxN, k_smooth_c, grid_half(c, 0, mg), TPB, c.st, c.dP, 0, bsel, xsel, 0, 1, gate);
+        SS_LAUNCH(PF_SMOOTH_R, c.maxN, k_smooth_c, grid_half(c, 0, mg), TPB, c.st, c.dP, 0, bsel, xsel, 0, 0, gate);
+        return;
+    }
+    small_init();
+    int Ls = 0;
+    while (Ls < mg.maxlev - 1 && mg.maxN[Ls] > g_small_nodes) Ls++;
+    for (int L = 0; L < Ls; L++) {
+        SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 1, gate);
+        SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 0, gate);
+        const dim3 gr((mg.maxNx[L] + 31) / 32, c.ninst, mg.maxRows[L + 1]);
+        SS_LAUNCH(PF_RESID_RESTRICT, mg.maxN[L + 1], k_resid_restrict2, gr, dim3(32, 4), c.st, c.dP, L, bsel, xsel, wsel, gate);
+    }
+    launch_small(c, mg.maxN[Ls], Ls, bsel, xsel, wsel, mg.alpha, gate);
+    for (int L = Ls - 1; L >= 0; L--) {
         SS_LAUNCH(PF_PROLONG, mg.maxN[L], k_prolong, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, mg.alpha, gate);
         SS_LAUNCH(PF_LEVEL_RESID, mg.maxN[L], k_level_resid, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, gate);
-        SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_black, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, 1, gate);
-        SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_red, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, 1, gate);
+        SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 1, gate);
+        SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 0, gate);
     }
+}
+
+__global__ void k_bicg_v(const DevP *__restrict__ Ps);
+__global__ void k_bicg_x(const DevP *__restrict__ Ps);
+__global__ void k_bicg_rho(const DevP *__restrict__ Ps);
+
+// Time `reps` launches of one kernel of the solve path on the instance's present state
+// (test hook for per-kernel roofline numbers; it overwrites work vectors).  Returns
+// microseconds per launch.
+double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
+    KrylovS ks0{};
+    ks0.active = 1;
+    ks0.maxit = 1 << 30;
+    cudaMemcpy(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice);
+    small_init();
+    int Ls = 0;
+    while (Ls < mg.maxlev - 1 && mg.maxN[Ls] > g_small_nodes) Ls++;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    auto one = [&]() {
+        switch (which) {
+        case 0: k_bicg_v<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        case 1: k_smooth_c<<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 1, 0); break;
+        case 2: k_smooth_c<<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 0, 0); break;
+        case 3: k_resid_restrict2<<<dim3((mg.maxNx[0] + 31) / 32, c.ninst, mg.maxRows[1]), dim3(32, 4), 0, c.st>>>(
+                    c.dP, 0, 2, 4, 1, 0); break;
+        case 4: k_level_resid<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
+        case 5: k_prolong<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 1.0, 0); break;
+        case 6: k_bicg_x<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        case 7: launch_small(c, mg.maxN[Ls], Ls, 2, 4, 1, 1.0, 0); break;
+        case 8: vcycle(c, mg, 2, 4, 1, 1, 0); break;
+        case 9: k_copy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 5, 6); break;
+        case 10: k_bicg_rho<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        default: break;
+        }
+    };
+    for (int r = 0; r < 3; r++) one();
+    cudaEventRecord(a, c.st);
+    for (int r = 0; r < reps; r++) one();
+    cudaEventRecord(b, c.st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return 1e3 * ms / reps;
 }
 
 // ------------------------------------------------------------------ PCG (semiconductor_3d.c:2182-2210)
@@ -470,7 +748,7 @@ __global__ void k_pcg_init_r(const DevP *__restrict__ Ps) {
     }
 }
 // rz = r.z; mode 0 initial (rz0), mode 1 iteration end (stop test, beta)
-__global__ void k_pcg_rz(const DevP *__restrict__ Ps, int mode, double rtol2, int maxit) {
+__global__ void k_pcg_rz(const DevP *__restrict__ Ps, int mode) {
     const DevP &P = Ps[blockIdx.y];
     if (mode && !ks_running(P)) return;
     const double *r = P.wk[0], *z = P.wk[1];
@@ -484,8 +762,8 @@ __global__ void k_pcg_rz(const DevP *__restrict__ Ps, int mode, double rtol2, in
             s.active = (rz > 0.0) ? 1 : 0;
             if (!(rz > 0.0)) s.status = 2;
         } else {
-            if (!(rz > rtol2 * s.rz0)) { s.active = 0; s.status = 1; }
-            else if (s.it >= maxit) { s.active = 0; s.status = 3; }
+            if (!(rz > s.rtol * s.rtol * s.rz0)) { s.active = 0; s.status = 1; }
+            else if (s.it >= s.maxit) { s.active = 0; s.status = 3; }
             else { s.be = rz / s.rz; s.rz = rz; }
         }
     }
@@ -530,33 +808,128 @@ __global__ void k_pcg_xr(const DevP *__restrict__ Ps) {
     SS_GRID_LOOP(k, P.N) { x[k] += al * p[k]; r[k] -= al * q[k]; }
 }
 
-int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every) {
-    KrylovS ks0{};
-    ks0.active = 1;
-    cudaMemcpyAsync(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
-    mg_setup(c, mg, 0);
-    SS_LAUNCH(PF_KRY_INIT, c.maxN, k_pcg_init_r, grid_nodes(c), TPB, c.st, c.dP);
-    vcycle(c, mg, 0, 1, 0, 1, 0);                  // z = M r
-    SS_LAUNCH(PF_KRY_DOT, c.maxN, k_pcg_rz, grid_nodes(c), TPB, c.st, c.dP, 0, rtol * rtol, maxit);
-    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_p, grid_nodes(c), TPB, c.st, c.dP, 1);
+// one PCG iteration (every kernel gated on the instance's active word)
+static void pcg_body(const Ctx &c, const MGHost &mg) {
+    SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_pcg_q, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_xr, grid_nodes(c), TPB, c.st, c.dP);
+    vcycle(c, mg, 0, 1, 0, 1, 1);
+    SS_LAUNCH(PF_KRY_DOT, c.maxN, k_pcg_rz, grid_nodes(c), TPB, c.st, c.dP, 1);
+    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_p, grid_nodes(c), TPB, c.st, c.dP, 0);
+}
+static void bicg_body(const Ctx &c, const MGHost &mg, int mg_on);
+
+// ------------------------------------------------------------------ device-looped solves
+// A Krylov solve runs as one CUDA graph: a conditional WHILE node whose body is one
+// iteration; the body's last kernel sets the loop condition from the instances' active
+// words, so the iteration loop runs on the device with no host round trip.
+__global__ void k_loop_cond(const DevP *__restrict__ Ps, int ninst, cudaGraphConditionalHandle h, int body) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned any = 0;
+    for (int i = 0; i < ninst; i++) {
+        KrylovS *s = Ps[i].ks;
+        if (body) s->body_runs++;
+        any |= s->active ? 1u : 0u;
+    }
+    cudaGraphSetConditional(h, any);
+}
+
+static bool g_graph_warned = false;
+#define GCK(x)                                                                                     \
+    do {                                                                                           \
+        if ((x) != cudaSuccess) {                                                                  \
+            if (!g_graph_warned)                                                                   \
+                std::fprintf(stderr, "semisim-b200: graph build failed (%s), iterating from the host\n", \
+                             cudaGetErrorString(cudaGetLastError()));                              \
+            g_graph_warned = true;                                                                 \
+            if (g) cudaGraphDestroy(g);                                                            \
+            return nullptr;                                                                        \
+        }                                                                                          \
+    } while (0)
+
+// kind 0: PCG; 1: BiCGSTAB with the multigrid preconditioner; 2: BiCGSTAB, smoother only
+static cudaGraphExec_t build_loop(const Ctx &c, const MGHost &mg, int kind, int *nkern) {
+    cudaGraph_t g = nullptr;
+    GCK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    GCK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    const DevP *dp = c.dP;
+    int ninst = c.ninst, body0 = 0;
+    void *args[] = {(void *)&dp, (void *)&ninst, (void *)&h, (void *)&body0};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void *)k_loop_cond;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = args;
+    cudaGraphNode_t n0, cn;
+    GCK(cudaGraphAddKernelNode(&n0, g, nullptr, 0, &kp));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    GCK(cudaGraphAddNode(&cn, g, &n0, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    GCK(cudaStreamBeginCaptureToGraph(c.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const unsigned long long l0 = t_launches;
+    if (kind == 0) pcg_body(c, mg);
+    else bicg_body(c, mg, kind == 1);
+    k_loop_cond<<<1, 32, 0, c.st>>>(c.dP, c.ninst, h, 1);
+    const unsigned long long nb = t_launches - l0;
+    *nkern = int(nb) + 1;
+    g_launches -= nb;                                  // counted per executed body instead
+    t_launches = l0;
+    cudaGraph_t out = nullptr;
+    GCK(cudaStreamEndCapture(c.st, &out));
+    cudaGraphExec_t ex = nullptr;
+    GCK(cudaGraphInstantiate(&ex, g, 0));
+    cudaGraphDestroy(g);
+    return ex;
+}
+
+bool g_use_graphs = true;
+
+// run the iteration loop of `kind` to completion; returns the final Krylov record
+static KrylovS run_loop(const Ctx &c, const MGHost &mg, int kind, int maxit, int check_every) {
     KrylovS hs{};
-    for (int it = 0; it < maxit;) {
-        const int nb = check_every;
-        for (int q = 0; q < nb && it < maxit; q++, it++) {
-            SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_pcg_q, grid_nodes(c), TPB, c.st, c.dP);
-            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_xr, grid_nodes(c), TPB, c.st, c.dP);
-            vcycle(c, mg, 0, 1, 0, 1, 1);
-            SS_LAUNCH(PF_KRY_DOT, c.maxN, k_pcg_rz, grid_nodes(c), TPB, c.st, c.dP, 1, rtol * rtol, maxit);
-            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_p, grid_nodes(c), TPB, c.st, c.dP, 0);
+    LoopGraphs *lg = c.lg;
+    if (lg && g_use_graphs && !g_prof_on && !lg->failed) {
+        if (!lg->exec[kind]) {
+            lg->exec[kind] = build_loop(c, mg, kind, &lg->kernels[kind]);
+            if (!lg->exec[kind]) lg->failed = 1;
+        }
+        if (lg->exec[kind]) {
+            cudaGraphLaunch(lg->exec[kind], c.st);
+            cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
+            cudaStreamSynchronize(c.st);
+            const unsigned long long ran = 1ull + (unsigned long long)lg->kernels[kind] * (unsigned long long)hs.body_runs;
+            g_launches += ran;
+            t_launches += ran;
+            return hs;
+        }
+    }
+    for (int it = 0; it < maxit + 1;) {
+        for (int q = 0; q < check_every && it < maxit + 1; q++, it++) {
+            if (kind == 0) pcg_body(c, mg);
+            else bicg_body(c, mg, kind == 1);
         }
         cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
         cudaStreamSynchronize(c.st);
         if (!hs.active) break;
     }
-    if (hs.active) {                                // ran out of iterations
-        cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
-        cudaStreamSynchronize(c.st);
-    }
+    return hs;
+}
+
+int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every) {
+    KrylovS ks0{};
+    ks0.active = 1;
+    ks0.maxit = maxit;
+    ks0.rtol = rtol;
+    cudaMemcpyAsync(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
+    mg_setup(c, mg, 0);
+    SS_LAUNCH(PF_KRY_INIT, c.maxN, k_pcg_init_r, grid_nodes(c), TPB, c.st, c.dP);
+    vcycle(c, mg, 0, 1, 0, 1, 0);                  // z = M r
+    SS_LAUNCH(PF_KRY_DOT, c.maxN, k_pcg_rz, grid_nodes(c), TPB, c.st, c.dP, 0);
+    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_p, grid_nodes(c), TPB, c.st, c.dP, 1);
+    const KrylovS hs = run_loop(c, mg, 0, maxit, check_every);
     return hs.it;
 }
 
@@ -595,7 +968,7 @@ __global__ void k_bicg_init(const DevP *__restrict__ Ps, double rtol, double ato
     }
 }
 // rho1 = rh.r; restart on breakdown; be
-__global__ void k_bicg_rho(const DevP *__restrict__ Ps, int maxit) {
+__global__ void k_bicg_rho(const DevP *__restrict__ Ps) {
     const DevP &P = Ps[blockIdx.y];
     if (!ks_running(P)) return;
     const double *r = P.wk[0], *rh = P.wk[1];
@@ -603,7 +976,7 @@ __global__ void k_bicg_rho(const DevP *__restrict__ Ps, int maxit) {
     SS_GRID_LOOP(k, P.N) acc[0] += rh[k] * r[k];
     if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
         KrylovS &s = *P.ks;
-        if (s.it >= maxit) { s.active = 0; s.status = 3; return; }
+        if (s.it >= s.maxit) { s.active = 0; s.status = 3; return; }
         s.it++;
         double rho1 = acc[0];
         s.pad0 = 0;
@@ -721,32 +1094,33 @@ __global__ void k_bicg_x(const DevP *__restrict__ Ps) {
 
 // One BiCGSTAB solve of P.A sol = rhs from the present sol.  Returns the iterations;
 // rn / r0 the final and initial residual norms.
+// one BiCGSTAB iteration (the continuity systems use the Slotboom-weighted hierarchy)
+static void bicg_body(const Ctx &c, const MGHost &mg, int mg_on) {
+    SS_LAUNCH(PF_KRY_DOT, c.maxN, k_bicg_rho, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_p, grid_nodes(c), TPB, c.st, c.dP);
+    vcycle(c, mg, 2, 4, 1, mg_on, 1);            // ph = M p
+    SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_bicg_v, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_s, grid_nodes(c), TPB, c.st, c.dP);
+    vcycle(c, mg, 0, 5, 1, mg_on, 2);            // sh = M r
+    SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_bicg_t, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_x, grid_nodes(c), TPB, c.st, c.dP);
+}
+
+// One BiCGSTAB solve of P.A sol = rhs from the present sol.  Returns the iterations;
+// rn / r0 the final and initial residual norms.
 int bicgstab_core(const Ctx &c, const MGHost &mg, int maxit, double rtol, double atol, int mg_on, int check_every,
                   double *rn, double *r0, int qsign) {
+    KrylovS ks0{};
+    ks0.maxit = maxit;
+    ks0.rtol = rtol;
+    ks0.atol = atol;
+    cudaMemcpyAsync(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
     if (mg_on) mg_setup(c, mg, qsign);
     else {
         SS_LAUNCH(PF_ILU_DIAG, c.maxN, k_ilu_diag, grid_nodes(c), TPB, c.st, c.dP, 0);
     }
     SS_LAUNCH(PF_KRY_INIT, c.maxN, k_bicg_init, grid_nodes(c), TPB, c.st, c.dP, rtol, atol);
-    KrylovS hs{};
-    const int wsel = qsign != 0;
-    for (int it = 0; it < maxit;) {
-        for (int q = 0; q < check_every && it < maxit; q++, it++) {
-            SS_LAUNCH(PF_KRY_DOT, c.maxN, k_bicg_rho, grid_nodes(c), TPB, c.st, c.dP, maxit);
-            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_p, grid_nodes(c), TPB, c.st, c.dP);
-            vcycle(c, mg, 2, 4, wsel, mg_on, 1);            // ph = M p
-            SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_bicg_v, grid_nodes(c), TPB, c.st, c.dP);
-            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_s, grid_nodes(c), TPB, c.st, c.dP);
-            vcycle(c, mg, 0, 5, wsel, mg_on, 2);            // sh = M r
-            SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_bicg_t, grid_nodes(c), TPB, c.st, c.dP);
-            SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_x, grid_nodes(c), TPB, c.st, c.dP);
-        }
-        cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
-        cudaStreamSynchronize(c.st);
-        if (!hs.active) break;
-    }
-    cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
-    cudaStreamSynchronize(c.st);
+    const KrylovS hs = run_loop(c, mg, mg_on ? 1 : 2, maxit, check_every);
     *rn = sqrt(hs.rr);
     *r0 = hs.r0;
     return hs.it;

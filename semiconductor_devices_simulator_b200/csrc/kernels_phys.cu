@@ -334,31 +334,27 @@ __device__ __forceinline__ void face_flux(const DevP &P, int ka, int kb, int ax,
 // Flux out of every contact's nodes into semiconductor nodes of other contacts or none:
 // I, S and the electron part per contact (semiconductor_3d.c:3598-3623).  Per-contact
 // block sums with a deterministic finish in the last block.
-__global__ void k_currents(const DevP *__restrict__ Ps, double *__restrict__ partc, unsigned *ticket) {
+__global__ void k_currents(const DevP *__restrict__ Ps) {
     const DevP &P = Ps[blockIdx.y];
     const int nc = P.ncon;
-    double *pc = partc + (size_t)blockIdx.y * 256 * 96;
-    double I = 0.0, S = 0.0, In = 0.0;
-    int myc = -1;
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < P.ncnode) {
-        const int k = P.cnode[q];
-        const uint32_t f = P.flags[k];
-        const int c = fl_con(f);
-        myc = c - 1;
-        const Node a = unidx(k, P.Nx, P.Ny);
-        for (int dir = 0; dir < 6; dir++) {
-            int kb; double h, ar;
-            if (!nbr(P, a, k, dir, kb, h, ar)) continue;
-            const uint32_t fb = P.flags[kb];
-            if (fl_kind(fb) != K_SEMI || fl_con(fb) == c) continue;
-            double Jn, Jp, Sn, Sp;
-            face_flux(P, k, kb, dir >> 1, h, ar, Jn, Jp, Sn, Sp);
-            I += Jn + Jp; S += Sn + Sp; In += Jn;
-        }
-    }
+    double *pc = P.partc;
+    unsigned *ticket = P.ticket + 7;
     for (int c = 0; c < nc; c++) {
-        double v[3] = {myc == c ? I : 0.0, myc == c ? S : 0.0, myc == c ? In : 0.0};
+        double v[3] = {0.0, 0.0, 0.0};
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < P.ncnode; q += gridDim.x * blockDim.x) {
+            const int k = P.cnode[q];
+            if (fl_con(P.flags[k]) != c + 1) continue;
+            const Node a = unidx(k, P.Nx, P.Ny);
+            for (int dir = 0; dir < 6; dir++) {
+                int kb; double h, ar;
+                if (!nbr(P, a, k, dir, kb, h, ar)) continue;
+                const uint32_t fb = P.flags[kb];
+                if (fl_kind(fb) != K_SEMI || fl_con(fb) == c + 1) continue;
+                double Jn, Jp, Sn, Sp;
+                face_flux(P, k, kb, dir >> 1, h, ar, Jn, Jp, Sn, Sp);
+                v[0] += Jn + Jp; v[1] += Sn + Sp; v[2] += Jn;
+            }
+        }
         block_sum<3>(v);
         if (threadIdx.x == 0) {
             pc[blockIdx.x * 96 + 3 * c + 0] = v[0];
@@ -369,7 +365,7 @@ __global__ void k_currents(const DevP *__restrict__ Ps, double *__restrict__ par
     __shared__ bool is_last;
     if (threadIdx.x == 0) {
         __threadfence();
-        is_last = atomicAdd(ticket + blockIdx.y, 1u) == gridDim.x - 1;
+        is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if (!is_last) return;
@@ -380,27 +376,14 @@ __global__ void k_currents(const DevP *__restrict__ Ps, double *__restrict__ par
         const int c = threadIdx.x / 3, w = threadIdx.x % 3;
         P.res[(w == 0 ? R_I : (w == 1 ? R_S : R_IN)) + c] = s;
     }
-    if (threadIdx.x == 0) ticket[blockIdx.y] = 0u;
+    if (threadIdx.x == 0) *ticket = 0u;
 }
 
-static double *g_partc = nullptr;
-static unsigned *g_ticketc = nullptr;
-static int g_partc_inst = 0;
 void launch_currents(const Ctx &c) {
-    if (c.ninst > g_partc_inst) {
-        if (g_partc) { cudaFree(g_partc); cudaFree(g_ticketc); }
-        cudaMalloc(&g_partc, sizeof(double) * 256 * 96 * c.ninst);
-        cudaMalloc(&g_ticketc, sizeof(unsigned) * c.ninst);
-        cudaMemset(g_ticketc, 0, sizeof(unsigned) * c.ninst);
-        g_partc_inst = c.ninst;
-    }
     int nb = (c.h.ncnode + TPB - 1) / TPB;
     if (nb < 1) nb = 1;
-    if (nb > 256) {
-        std::fprintf(stderr, "semisim-b200: too many contact nodes (%d)\n", c.h.ncnode);
-        nb = 256;
-    }
-    SS_LAUNCH(PF_CURRENTS, c.h.ncnode, k_currents, dim3(nb, c.ninst), TPB, c.st, c.dP, g_partc, g_ticketc);
+    if (nb > 256) nb = 256;                    // grid-stride beyond 256 blocks (partial buffer size)
+    SS_LAUNCH(PF_CURRENTS, c.h.ncnode, k_currents, dim3(nb, c.ninst), TPB, c.st, c.dP);
 }
 
 // ------------------------------------------------------------------ Gummel helpers

@@ -1,6 +1,8 @@
 // Launch accounting and CUDA-event kernel timing (see prof.h).
 #include "prof.h"
 
+#include <map>
+#include <utility>
 #include <vector>
 
 namespace ss {
@@ -45,7 +47,8 @@ const char *kProfName[PF_NPROF] = {
     "anderson", "boundary", "vector", "labelling", "display"};
 
 bool g_prof_on = false;
-unsigned long long g_launches = 0;
+std::atomic<unsigned long long> g_launches{0};
+thread_local unsigned long long t_launches = 0;
 
 namespace {
 struct Rec {
@@ -56,6 +59,7 @@ struct Rec {
 std::vector<Rec> g_recs;
 size_t g_used = 0;
 double g_ms[PF_NPROF], g_cnt[PF_NPROF], g_bytes[PF_NPROF];
+std::map<std::pair<int, long long>, std::pair<double, double>> g_detail;   // (class, nodes) -> (ms, launches)
 }  // namespace
 
 void prof_begin(int id, cudaStream_t st) {
@@ -85,12 +89,16 @@ void prof_collect() {
         g_ms[r.id] += ms;
         g_cnt[r.id] += 1.0;
         g_bytes[r.id] += r.nodes * kProfBytesPerNode[r.id];
+        auto &e = g_detail[{r.id, (long long)r.nodes}];
+        e.first += ms;
+        e.second += 1.0;
     }
     g_used = 0;
 }
 void prof_reset() {
     prof_collect();
     for (int i = 0; i < PF_NPROF; i++) g_ms[i] = g_cnt[i] = g_bytes[i] = 0.0;
+    g_detail.clear();
 }
 void prof_read(int id, double *ms, double *count, double *bytes) {
     prof_collect();
@@ -116,6 +124,17 @@ int b200x_prof_read(int id, double *ms, double *count, double *bytes) {
     return 1;
 }
 const char *b200x_prof_name(int id) { return (id >= 0 && id < ss::PF_NPROF) ? ss::kProfName[id] : ""; }
+// q-th (class, launch size) bucket: class id, nodes per launch, total ms, launches; 0 past the end
+int b200x_prof_detail(int q, int *id, double *nodes, double *ms, double *count) {
+    ss::prof_collect();
+    int i = 0;
+    for (const auto &e : ss::g_detail) {
+        if (i++ != q) continue;
+        *id = e.first.first; *nodes = (double)e.first.second; *ms = e.second.first; *count = e.second.second;
+        return 1;
+    }
+    return 0;
+}
 // kernel launches of this library since it was loaded
-unsigned long long b200x_launches(void) { return ss::g_launches; }
+unsigned long long b200x_launches(void) { return ss::g_launches.load(); }
 }

@@ -5,6 +5,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 namespace ss {
 
 enum ProfId {
@@ -19,7 +21,8 @@ extern const double kProfBytesPerNode[PF_NPROF];
 extern const char *kProfName[PF_NPROF];
 
 extern bool g_prof_on;
-extern unsigned long long g_launches;
+extern std::atomic<unsigned long long> g_launches;     // all threads
+extern thread_local unsigned long long t_launches;     // this thread
 void prof_begin(int id, cudaStream_t st);
 void prof_end(int id, cudaStream_t st, double nodes);
 void prof_collect();
@@ -31,6 +34,7 @@ void prof_read(int id, double *ms, double *count, double *bytes);
 #define SS_LAUNCH(ID, NODES, KERN, GRID, BLOCK, ST, ...)                \
     do {                                                                \
         ss::g_launches++;                                               \
+        ss::t_launches++;                                               \
         if (ss::g_prof_on) ss::prof_begin((ID), (ST));                  \
         KERN<<<(GRID), (BLOCK), 0, (ST)>>>(__VA_ARGS__);                \
         if (ss::g_prof_on) ss::prof_end((ID), (ST), (double)(NODES));   \

@@ -66,8 +66,9 @@ struct LevelT {
 struct KrylovS {
     double rho, al, om, rho1, be, rv, ss, tt, ts, rr, r0, tgt, rbest, fl;
     double rz, rz0, pq;
-    int it, stall, active, status;   // status: 0 running, 1 converged, 2 breakdown/stop
-    int half, pad0, pad1, pad2;
+    double rtol, atol;               // stop rule of the running solve (set by the host)
+    int it, stall, active, status;   // status: 0 running, 1 converged, 2 breakdown/stop, 3 iteration cap
+    int half, pad0, maxit, body_runs;
 };
 
 // everything a kernel needs about one instance
@@ -100,7 +101,10 @@ struct DevP {
     double *aagam;                // AA_MAX coefficients
     // reductions
     double *part;                 // RED_MAX_BLOCKS*RED_NV
-    unsigned *ticket;             // one counter per reduction slot (8)
+    unsigned *ticket;             // one counter per reduction slot (16)
+    double *partc;                // terminal-current partials: 256 blocks x 96
+    double *ffbuf;                // floating-block sums: 6 x 1024
+    int *ffint;                   // floating-block flags / counts / roots: 16 + 1024
     double *res;                  // scalar results (64)
     KrylovS *ks;
     // multigrid (FP64 and FP32 hierarchies)

@@ -54,6 +54,7 @@ Ctx make_ctx(Inst &d) {
     c.ninst = 1;
     c.maxN = (int)d.N;
     c.st = d.g.st;
+    c.lg = &d.g.lg;
     return c;
 }
 
@@ -106,6 +107,9 @@ static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &lev
     P.gram = cv.take<double>(AA_MAX * AA_MAX); P.aagam = cv.take<double>(AA_MAX);
     P.part = cv.take<double>((size_t)RED_MAX_BLOCKS * RED_NV);
     P.ticket = cv.take<unsigned>(16);
+    P.partc = cv.take<double>(256 * 96);
+    P.ffbuf = cv.take<double>(6 * 1024);
+    P.ffint = cv.take<int>(16 + 1024);
     P.res = cv.take<double>(R_TOTAL);
     P.ks = cv.take<KrylovS>(1);
     P.lev = cv.take<LevelT<double>>(MAXLEV);
@@ -154,6 +158,10 @@ int mg_levels(int Nx, int Ny, int Nz, int dims[][6]) {
 }
 
 void gpu_free(Inst &d) {
+    for (auto &e : d.g.lg.exec)
+        if (e) cudaGraphExecDestroy(e);
+    for (auto &e : d.g.tev)
+        if (e) cudaEventDestroy(e);
     if (d.g.block) cudaFree(d.g.block);
     if (d.g.d) cudaFree(d.g.d);
     if (d.g.pin) cudaFreeHost(d.g.pin);
@@ -203,7 +211,11 @@ static int gpu_alloc(Inst &d) {
     CK(cudaMemcpy(P.lev, levs.data(), sizeof(LevelT<double>) * nl, cudaMemcpyHostToDevice));
     MGHost &mg = d.g.mg;
     mg.maxlev = mg.minlev = nl;
-    for (int L = 0; L < nl; L++) mg.maxN[L] = levs[L].N;
+    for (int L = 0; L < nl; L++) {
+        mg.maxN[L] = levs[L].N;
+        mg.maxNx[L] = levs[L].Nx;
+        mg.maxRows[L] = levs[L].Ny * levs[L].Nz;
+    }
     d.g.ready = true;
     return 1;
 }

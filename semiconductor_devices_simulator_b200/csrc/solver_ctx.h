@@ -17,8 +17,12 @@ enum VecSel { V_RHS = 8, V_SOL = 9, V_F = 10, V_TR = 11, V_DSC = 12, V_PHI = 13 
 struct MGHost {
     int maxlev = 0, minlev = 0;
     int maxN[MAXLEV] = {0};
+    int maxNx[MAXLEV] = {0};       // largest x extent of the level
+    int maxRows[MAXLEV] = {0};     // largest Ny*Nz of the level
     double alpha = 1.0;
 };
+double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps);
+extern int g_small_nodes;
 
 struct Contact {
     int face = 0, i0 = 0, i1 = 0, j0 = 0, j1 = 0, k0 = 0, k1 = 0, bc = 0;
@@ -37,10 +41,14 @@ struct Gpu {
     MGHost mg;
     std::vector<LevelT<double>> levs;
     cudaStream_t st = nullptr;
+    LoopGraphs lg;               // device-looped Krylov solves
+    cudaEvent_t tev[2] = {nullptr, nullptr};   // stream timer (test hook)
     double *pin = nullptr;       // pinned host scratch (results)
     double *scratch = nullptr;   // device scratch (bulk output)
     int *flag = nullptr;         // device int scratch
 };
+
+struct TrapSpec { int type, ref; double E, sn, sp; };   // deep-level species (stored, not solved)
 
 struct Inst {
     // ---- configuration (the reference's Dev, semiconductor_3d.c:234-364)
@@ -81,6 +89,11 @@ struct Inst {
     // host mirrors of device results for the getters (valid while `mirror_ok`)
     std::vector<std::vector<double>> cache;
     std::vector<int> cache_ok;
+    // terminal partition of the quasi-static charges; trap species table
+    std::vector<int> qown;
+    int qct[NC_MAX] = {0};
+    TrapSpec tsp[512];
+    int n_tsp = 0;
 };
 
 // global knobs (the reference's static tunables, read by api3_init)
@@ -94,6 +107,7 @@ struct Knobs {
     int check_every = 1;        // Krylov iterations queued between status reads
 };
 extern Knobs g_knobs;
+extern bool g_use_graphs;           // Krylov loops as device-looped CUDA graphs (SEMISIM_B200_GRAPHS=0: off)
 extern std::atomic<int> g_stop;
 extern volatile double g_prog[8];
 

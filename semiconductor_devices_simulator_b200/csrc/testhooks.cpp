@@ -185,15 +185,42 @@ int b200x_float_fix(int hole, double *sol) {
 // device memory of the instance (bytes) and the multigrid depth
 long long b200x_device_bytes(void) { return (long long)dev()->g.bytes; }
 
+// microseconds per launch of one kernel of the solve path, `reps` back-to-back launches
+// on the present state (it overwrites work vectors): 0-10 linear algebra (see
+// bench_la_kernel), 20 continuity assembly, 21 Poisson build
+double b200x_bench(int which, int reps) {
+    Inst &d = *dev();
+    if (!d.g.ready || reps < 1) return -1.0;
+    Ctx c = make_ctx(d);
+    if (which < 20) return bench_la_kernel(c, d.g.mg, which, reps);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    auto one = [&]() {
+        if (which == 20) launch_cont_assemble(c, 0);
+        else launch_poisson(c, nullptr, 1, nullptr);
+    };
+    for (int r = 0; r < 3; r++) one();
+    cudaEventRecord(a, c.st);
+    for (int r = 0; r < reps; r++) one();
+    cudaEventRecord(b, c.st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return 1e3 * ms / reps;
+}
+
 // select the CUDA device of the solver (before its first solve); 1 = done
 int b200x_set_device(int dev) { return select_device(dev); }
 
 // CUDA-event timer on the solver's own stream: op 0 records the start, op 1 records the
 // stop, waits for it and returns the elapsed milliseconds (-1 before the first solve)
 double b200x_stream_timer(int op) {
-    static cudaEvent_t ev[2] = {nullptr, nullptr};
     Inst &d = *dev();
     if (!d.g.ready) return -1.0;
+    cudaEvent_t *ev = d.g.tev;
     if (!ev[0]) { cudaEventCreate(&ev[0]); cudaEventCreate(&ev[1]); }
     if (op == 0) { cudaEventRecord(ev[0], d.g.st); return 0.0; }
     cudaEventRecord(ev[1], d.g.st);

@@ -111,6 +111,38 @@ def test_small_sweeps_default_match_reference(lib, name):
         assert rel.max() <= NP_RTOL, f"{lab} differs by {rel.max():.3e} relative"
 
 
+def test_concurrent_instances(lib):
+    """Three devices solved at once from three host threads, one solver instance (and
+    CUDA stream) each: every sweep still matches the reference."""
+    import threading
+    names = ["diode_small", "mos_small", "moscap_small"]
+    hs = [lib.api3b_new() for _ in names]
+    out = {}
+
+    def work(name, h):
+        lib.api3b_use(h)
+        w, mat, bias = MG.build(lib, name)
+        out[name] = sweep_fields(lib, w, w.sweeps[0])
+        lib.api3b_use(0)
+
+    th = [threading.Thread(target=work, args=(nm, h)) for nm, h in zip(names, hs)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    try:
+        for name in names:
+            g = golden(name)
+            ok0, V, I, F, conv, psi, n, p = out[name]
+            assert ok0 and conv.all(), name
+            own = 2.0 * np.abs(g["sw0_I"] - g["swt0_I"])
+            check_currents(I, g["sw0_I"], np.maximum(g["sw0_Iflr"], own))
+            assert np.abs(psi - g["sw0_psi"]).max() <= PSI_TOL, name
+    finally:
+        for h in hs:
+            lib.api3b_free(h)
+
+
 def reference_lib():
     path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_harness.so")
     if not os.path.exists(path):
