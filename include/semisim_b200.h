@@ -223,6 +223,19 @@ int api3b_use(int h);
 int api3b_current(void);
 int api3b_free(int h);
 
+/* No counterpart in the reference.  For callers that cannot allocate device memory
+   (their memory belongs to another allocator, or a cudaMalloc / cudaFree on their path is
+   not acceptable): r = b - A x for a 7-point stencil A (7 arrays of N = Nx*Ny*Nz doubles:
+   diagonal, x-, x+, y-, y+, z-, z+), norms[0] = ||r||_2 and norms[1] = the BiCGSTAB
+   rounding floor sqrt(sum_a (sum_b |A_ab x_b| + |b_a|)^2).  A7, x, b, r: the caller's
+   device buffers on one GPU; norms: host.  Allocates nothing: its reduction scratch is a
+   fixed ~38 KB device array that every GPU loading the library holds until exit.  At most
+   2^30 nodes (larger sizes are refused with a message).  The first call on a GPU looks up
+   that array (cudaGetSymbolAddress): make it before any stream capture.  Calls share the
+   array and use the default stream; calls that overlap on one GPU race.  1 = done. */
+int api3b_stencil_residual_noalloc(const double *A7, const double *x, const double *b, int Nx, int Ny, int Nz,
+                                   double *r, double *norms);
+
 #ifdef __cplusplus
 }
 #endif

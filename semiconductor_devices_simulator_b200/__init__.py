@@ -43,6 +43,7 @@ HOOKS = {
     "b200x_stream_timer": (_D, [_I]),
     "b200x_set_device": (_I, [_I]),
     "b200x_bench": (_D, [_I, _I]),
+    "api3b_stencil_residual_noalloc": (_I, [_DP, _DP, _DP, _I, _I, _I, _DP, _DP]),
     "b200x_prof": (_I, [_I]),
     "b200x_prof_read": (_I, [_I, _DP, _DP, _DP]),
     "b200x_prof_name": (ctypes.c_char_p, [_I]),
