@@ -55,7 +55,30 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bounded CPU-baseline sample (s)")
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the e2e pass (profiler captures)")
+    ap.add_argument("--probe", type=int, default=0, metavar="ITS",
+                    help="profiler probe: one continuity system of the workload device at its charge-neutral "
+                         "start, multigrid set-up and ITS BiCGSTAB iterations (a few hundred launches)")
     return ap.parse_args()
+
+
+def run_probe(a):
+    """Few-launch case for ncu: the workload's device, one electron continuity system."""
+    import semiconductor_devices_simulator_b200 as S
+    mesh = tuple(int(v) for v in a.mesh.split(","))
+    lib = S.load()
+    w = build(lib, mesh)
+    s = w.sweeps[1]
+    for cid, vv in D.bias_vector(w, s, 0.6).items():
+        lib.api3_set_contact_V(cid, vv)
+    assert lib.b200x_prepare() == 1
+    lib.b200x_init_state()
+    l0 = lib.b200x_launches()
+    lib.b200x_cont_assemble(0, None, None, None, None)
+    rn, r0 = np.zeros(1), np.zeros(1)
+    its = lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
+    print(json.dumps({"probe": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]} electron continuity", "nodes": w.N,
+                      "bicgstab_its": its, "r0": r0[0], "rn": rn[0],
+                      "launches": int(lib.b200x_launches() - l0)}))
 
 
 # ------------------------------------------------------------------ distributed plumbing
@@ -376,6 +399,8 @@ def run_reference(a, dist):
 
 def main():
     a = parse()
+    if a.probe:
+        return run_probe(a)
     dist = Dist()
     out = run_reference(a, dist) if a.impl == "reference" else run_b200(a, dist)
     if dist.rank == 0 and out is not None:

@@ -25,6 +25,8 @@ double b200x_vlo(void);
 double b200x_vhi(void);
 void b200x_apply_bc(void);
 void b200x_rebuild_np(void);
+/* charge-neutral start state at the present contact voltages (no Newton solve) */
+void b200x_init_state(void);
 void b200x_upd_mob(void);
 void b200x_clamp_qf(void);
 /* Poisson residual, Jacobian (7 x N) and sc at psi; returns ||F/diag|| */

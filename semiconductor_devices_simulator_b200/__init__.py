@@ -28,6 +28,7 @@ HOOKS = {
     "b200x_vhi": (_D, []),
     "b200x_apply_bc": (None, []),
     "b200x_rebuild_np": (None, []),
+    "b200x_init_state": (None, []),
     "b200x_upd_mob": (None, []),
     "b200x_clamp_qf": (None, []),
     "b200x_poisson": (_D, [_DP, _DP, _DP, _DP]),

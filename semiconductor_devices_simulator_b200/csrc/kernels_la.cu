@@ -459,6 +459,20 @@ __global__ void k_smooth_c(const DevP *__restrict__ Ps, int L, int bsel, int xse
         if (i >= v.Nx) continue;
         const int k = i + v.Nx * row;
         double z;
+        if (mode == 2) {
+            // a further application of the preconditioner right after a red-black one:
+            // the residual of every red node is then zero, so black z = r / D with the
+            // full-stencil residual, and red z = -(sum a_rb z_b) / D
+            if (color) {
+                z = (v.b[k] - stencil_apply<double>(v.A, v.x, k, i, j, l, v.Nx, v.Ny, v.Nz)) / v.D[k];
+                v.x[k] += z;
+                v.r[k] = z;
+            } else {
+                z = -offdiag_apply<double>(v.A, v.r, k, i, j, l, v.Nx, v.Ny, v.Nz) / v.D[k];
+                v.x[k] += z;
+            }
+            continue;
+        }
         if (color) {
             const double s = offdiag_apply_div<double>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
             z = (src[k] - s) / v.D[k];
@@ -616,6 +630,7 @@ __global__ void __launch_bounds__(SMALL_TPB) k_vcycle_small(const DevP *__restri
 }
 
 int g_small_nodes = 2048;           // levels at or below this size run in the cluster kernel
+int g_l0_sweeps = 2;                // red-black applications per smoothing step on the finest level
 static int g_cluster = 0;           // CTAs per cluster of the small-level kernel (set on first use)
 
 // cluster size of the small-level kernel (16 CTAs when the device allows non-portable
@@ -625,6 +640,7 @@ static void small_init() {
         const char *e = std::getenv("SEMISIM_B200_CLUSTER");
         g_cluster = (e && std::atoi(e) == 8) ? 8 : 16;
         if (const char *s = std::getenv("SEMISIM_B200_SMALL")) g_small_nodes = std::atoi(s);
+        if (const char *s = std::getenv("SEMISIM_B200_L0SWEEPS")) g_l0_sweeps = std::atoi(s) > 1 ? 2 : 1;
         if (cudaFuncSetAttribute(k_vcycle_small, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
             g_cluster = 8;
         cudaGetLastError();
@@ -677,6 +693,10 @@ void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg
     for (int L = 0; L < Ls; L++) {
         SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 1, gate);
         SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 0, gate);
+        if (L == 0 && g_l0_sweeps > 1) {     // second application on the finest level
+            SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 1, gate);
+            SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
+        }
         const dim3 gr((mg.maxNx[L] + 31) / 32, c.ninst, mg.maxRows[L + 1]);
         SS_LAUNCH(PF_RESID_RESTRICT, mg.maxN[L + 1], k_resid_restrict2, gr, dim3(32, 4), c.st, c.dP, L, bsel, xsel, wsel, gate);
     }
@@ -686,6 +706,10 @@ void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg
         SS_LAUNCH(PF_LEVEL_RESID, mg.maxN[L], k_level_resid, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, gate);
         SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 1, gate);
         SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 0, gate);
+        if (L == 0 && g_l0_sweeps > 1) {
+            SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 1, gate);
+            SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
+        }
     }
 }
 

@@ -92,6 +92,19 @@ void b200x_apply_bc(void) {
     sync(d);
 }
 void b200x_rebuild_np(void) { rebuild_np(*dev()); sync(*dev()); }
+// charge-neutral start state at the contact voltages now set (init_eq + boundary values +
+// carriers + face mobility), without the Newton solve of an equilibrium
+void b200x_init_state(void) {
+    Inst &d = *dev();
+    launch_init_eq(make_ctx(d));
+    double Va[NC_MAX];
+    for (int c = 0; c < d.n_cons; c++) Va[c] = d.cons[c].V;
+    set_vrange(d, Va);
+    apply_bc(d, Va);
+    rebuild_np(d);
+    upd_mob(d);
+    sync(d);
+}
 void b200x_upd_mob(void) { upd_mob(*dev()); sync(*dev()); }
 void b200x_clamp_qf(void) { clamp_qf(*dev()); sync(*dev()); }
 
