@@ -223,6 +223,22 @@ int api3b_use(int h);
 int api3b_current(void);
 int api3b_free(int h);
 
+/* No counterpart in the reference (its solves are FP64 only).  Linear-solve precision of
+   the current instance, kept across api3_init:
+     0  FP64 throughout (the reference's arithmetic);
+     1  refined: the Krylov iterations and the multigrid hierarchy of every linear solve run
+        in FP32 (FP32 copy of the operator, FP32 vectors, dot products summed in FP64)
+        inside FP64 iterative refinement: x and r = b - A x stay FP64 with the FP64
+        operator, and the solve stops on the reference's FP64 rule.  Continuity solves
+        (BiCGSTAB) refine explicitly; the Newton-Poisson corrections (PCG) are refined by
+        the Newton loop's FP64 residual (PCG tolerances below 1e-5 stay FP64).  A refinement
+        that stops gaining hands the solve to the FP64 solver;
+    -1  the library default (SEMISIM_B200_PRECISION=mixed at api3_init selects 1, else 0).
+   api3b_set_precision returns the previous setting; api3b_get_precision the mode in
+   effect (0 or 1). */
+int api3b_set_precision(int mode);
+int api3b_get_precision(void);
+
 /* No counterpart in the reference.  For callers that cannot allocate device memory
    (their memory belongs to another allocator, or a cudaMalloc / cudaFree on their path is
    not acceptable): r = b - A x for a 7-point stencil A (7 arrays of N = Nx*Ny*Nz doubles:

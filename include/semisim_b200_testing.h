@@ -46,11 +46,15 @@ int b200x_bicgstab(int maxit, double rtol, double atol, int qsign, const double 
 int b200x_pcg(int maxit, double rtol, double *sol);
 /* floating-block balance of a continuity solution (in place) */
 int b200x_float_fix(int hole, double *sol);
+/* refinement steps and FP64 take-overs of the instance's refined continuity solves */
+void b200x_ir_stats(long long *steps, long long *fallbacks);
 /* device memory of the instance (bytes) */
 long long b200x_device_bytes(void);
 /* CUDA device of the solver (before its first solve); 1 = done */
 int b200x_set_device(int dev);
-/* microseconds per launch of one kernel over `reps` back-to-back launches */
+/* microseconds per launch of one kernel over `reps` back-to-back launches (0-10 FP64
+   linear algebra, 11-16 the FP32 twins and the FP64 refinement update, 20 continuity
+   assembly, 21 Poisson build) */
 double b200x_bench(int which, int reps);
 /* CUDA-event timer on the instance's stream: op 0 start, op 1 stop -> elapsed ms */
 double b200x_stream_timer(int op);

@@ -50,6 +50,7 @@ HOOKS = {
     "b200x_prof_name": (ctypes.c_char_p, [_I]),
     "b200x_prof_detail": (_I, [_I, _IP, _DP, _DP, _DP]),
     "b200x_launches": (ctypes.c_ulonglong, []),
+    "b200x_ir_stats": (None, [ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
 }
 # state arrays reachable through b200x_set / b200x_get
 ST_PHI, ST_PHIN, ST_PHIP, ST_N, ST_P, ST_MU0N, ST_MU0P, ST_SOL, ST_RHS, ST_SC, ST_DSC = range(11)

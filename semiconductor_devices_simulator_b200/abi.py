@@ -118,6 +118,9 @@ EXTRA = {
     "api3b_use": (_I, [_I]),
     "api3b_current": (_I, []),
     "api3b_free": (_I, [_I]),
+    # linear-solve precision of the current instance (0 FP64, 1 FP32 refined in FP64)
+    "api3b_set_precision": (_I, [_I]),
+    "api3b_get_precision": (_I, []),
 }
 
 

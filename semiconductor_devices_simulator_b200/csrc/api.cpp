@@ -14,6 +14,7 @@
 #include <mutex>
 #include <vector>
 
+#include "prof.h"
 #include "solver_ctx.h"
 
 using namespace ss;
@@ -111,9 +112,11 @@ extern "C" {
 // ------------------------------------------------------------------ set-up
 void api3_init(void) {                                      // semiconductor_3d.c:4570-4597
     Gpu keep = g_dev.g;                                     // device buffers are reused when the size allows
+    const int prec = g_dev.precision;                       // so is the instance's solver precision
     g_dev.g = Gpu();
     g_dev = Inst();
     g_dev.g = keep;
+    g_dev.precision = prec;
     g_dev.g.ready = keep.ready;
     Inst &d = g_dev;
     const char *e = env_get("SEMISIM_PCGRTOL"); d.pcg_rtol = e ? std::atof(e) : 1e-3;
@@ -131,6 +134,11 @@ void api3_init(void) {                                      // semiconductor_3d.
     if (const char *m = env_get("SEMISIM_QFM")) g_knobs.qf_margin = std::atof(m);
     if (const char *m = env_get("SEMISIM_B200_CHECK")) { const int q = std::atoi(m); if (q >= 1 && q <= 64) g_knobs.check_every = q; }
     if (const char *m = env_get("SEMISIM_B200_GRAPHS")) g_use_graphs = std::atoi(m) != 0;
+    if (const char *m = env_get("SEMISIM_B200_PDL")) g_pdl = std::atoi(m) != 0;
+    if (const char *m = env_get("SEMISIM_B200_PRECISION"))
+        g_precision_default = (!std::strcmp(m, "mixed") || !std::strcmp(m, "refined") || !std::strcmp(m, "1")) ? 1 : 0;
+    if (const char *m = env_get("SEMISIM_B200_IR_FACTOR")) { const double q = std::atof(m); if (q > 0. && q <= 1.) g_ir_factor = q; }
+    if (const char *m = env_get("SEMISIM_B200_IR_RTOL")) { const double q = std::atof(m); if (q > 0. && q < 1.) g_ir_rtol_min = q; }
     g_n_trap_species = 0;
 }
 
@@ -694,6 +702,18 @@ int api3b_current(void) {
         if (g_reg[q].get() == t_cur) return (int)q + 1;
     return -1;
 }
+// precision of the current instance's linear solves: 0 FP64 throughout (the reference's
+// arithmetic), 1 FP32 Krylov / multigrid inner solves refined in FP64 to the same FP64
+// stop rule, -1 the library default (SEMISIM_B200_PRECISION=mixed selects 1).  Returns
+// the previous setting.
+int api3b_set_precision(int mode) {
+    Inst &d = g_dev;
+    const int old = d.precision;
+    d.precision = mode < -1 ? -1 : (mode > 1 ? 1 : mode);
+    return old;
+}
+// precision in effect on the current instance (0 FP64, 1 refined FP32)
+int api3b_get_precision(void) { return use_mixed(g_dev); }
 int api3b_free(int h) {
     std::lock_guard<std::mutex> lk(g_reg_mu);
     if (h < 1 || h > (int)g_reg.size() || !g_reg[h - 1]) return 0;

@@ -10,6 +10,15 @@ namespace ss {
 
 #define SS_GRID_LOOP(k, N) for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < (N); k += gridDim.x * blockDim.x)
 
+// Programmatic dependent launch: let the next kernel of the stream start its launch now,
+// then wait until the kernels this one depends on have completed and their writes are
+// visible.  Every kernel launched with SS_LAUNCH_PDL calls this before touching memory;
+// without that launch attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 template <int NV>
 __device__ __forceinline__ void warp_sum(double (&v)[NV]) {
 #pragma unroll

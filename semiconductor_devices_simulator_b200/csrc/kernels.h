@@ -7,9 +7,13 @@
 namespace ss {
 
 // instantiated device-looped Krylov graphs of one instance (kernels_la.cu)
+// kinds: 0 PCG, 1 BiCGSTAB with the multigrid preconditioner, 2 BiCGSTAB with the
+// smoother alone (all FP64); 3 FP32 PCG; 4 one FP64 refinement step around an FP32
+// multigrid BiCGSTAB
+constexpr int LOOP_KINDS = 5;
 struct LoopGraphs {
-    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
-    int kernels[3] = {0, 0, 0};
+    cudaGraphExec_t exec[LOOP_KINDS] = {};
+    int kernels[LOOP_KINDS] = {};
     int failed = 0;
 };
 
@@ -46,20 +50,8 @@ void launch_extrap(const Ctx &c, double r, int s1, int s2);     // history selec
 void launch_region_mark(const Ctx &c, int con1, int type, double dV, int *mark, int *changed);
 void launch_floating_blocks(const Ctx &c, int hole, int *nblocks);
 
-// ---- linear algebra (kernels_la.cu)
-void launch_absmax(const Ctx &c, const double *x, int slot);                   // res[slot]
-void launch_axpy(const Ctx &c, double *y, const double *x, double a, const double *z);  // y = x + a z
-void launch_fill(const Ctx &c, double *y, double v);
-void launch_copy(const Ctx &c, double *y, const double *x);
-
-template <class T> struct MGCtx;
+// ---- linear algebra (kernels_la.cu; drivers declared in solver_ctx.h)
 int mg_levels(int Nx, int Ny, int Nz, int dims[][6]);
-
-// multigrid set-up and the Krylov solvers (FP64 plain path)
-void mg_setup(const Ctx &c, int qsign);
-void pcg_solve(const Ctx &c, const double *b, double *x, int maxit, double rtol, int *its);
-void bicgstab_solve(const Ctx &c, const double *b, double *x, int maxit, double rtol, double atol, int *its,
-                    double *rn_out, double *r0_out, int mg_on);
 
 // ---- Anderson (kernels_aa.cu)
 void launch_aa_step(const Ctx &c, int M, int have, int pos, int nfill, double *const *x, double *const *g,

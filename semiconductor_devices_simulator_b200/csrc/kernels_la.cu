@@ -3,6 +3,13 @@
 // prolongation, Petrov-Galerkin coarse operators, red-black D-ILU smoother, dense
 // coarsest level) and device-resident PCG / BiCGSTAB.
 //
+// Every multigrid and Krylov kernel is a template over the element type T of the
+// vectors and matrices it streams.  T = double is the plain path (the reference's FP64
+// arithmetic).  T = float is the inner solver of the refined path: an FP32 copy of the
+// level-0 system, an FP32 hierarchy and FP32 Krylov vectors (dot products accumulated in
+// FP64), driven by FP64 iterative refinement (FP64 residual b - A x with the FP64
+// operator, FP32 correction) to the reference's own FP64 stop rule.
+//
 // The reference smooths with a chunked natural-order D-ILU(0) (semiconductor_3d.c:
 // 1923-1972), a sequential recurrence.  Here the smoother is D-ILU(0) in red-black
 // order: red nodes (i+j+l even) have only black neighbours, so the forward sweep is a
@@ -16,6 +23,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -37,96 +45,137 @@ static inline dim3 grid_n(const Ctx &c, int n) {
     return dim3(b, c.ninst);
 }
 
-// vector selectors of the level-0 Krylov vectors
-__device__ __forceinline__ double *vsel(const DevP &P, int s) {
-    if (s < 8) return P.wk[s];
-    switch (s) {
-    case V_RHS: return P.rhs;
-    case V_SOL: return P.sol;
-    case V_F: return P.F;
-    case V_TR: return P.tr;
-    case V_PHI: return P.phi;
-    default: return P.dsc;
+// ------------------------------------------------------------------ precision traits
+// where the level-0 system, the Krylov vectors, the hierarchy and the Krylov record of
+// each precision live in an instance's parameter record
+template <class T> struct PT;
+template <> struct PT<double> {
+    static __device__ __forceinline__ double *wk(const DevP &P, int s) { return P.wk[s]; }
+    static __device__ __forceinline__ double *sol(const DevP &P) { return P.sol; }
+    static __device__ __forceinline__ double *rhs(const DevP &P) { return P.rhs; }
+    static __device__ __forceinline__ double *const *A0(const DevP &P) { return P.A; }
+    static __device__ __forceinline__ const double *w0(const DevP &P) { return P.dsc; }
+    static __device__ __forceinline__ const LevelT<double> &lev(const DevP &P, int L) { return P.lev[L]; }
+    static __device__ __forceinline__ KrylovS *ks(const DevP &P) { return P.ks; }
+};
+template <> struct PT<float> {
+    static __device__ __forceinline__ float *wk(const DevP &P, int s) { return P.wk32[s]; }
+    static __device__ __forceinline__ float *sol(const DevP &P) { return P.sol32; }
+    static __device__ __forceinline__ float *rhs(const DevP &P) { return P.rhs32; }
+    static __device__ __forceinline__ float *const *A0(const DevP &P) { return P.A32; }
+    static __device__ __forceinline__ const float *w0(const DevP &P) { return P.dsc32; }
+    static __device__ __forceinline__ const LevelT<float> &lev(const DevP &P, int L) { return P.levf[L]; }
+    static __device__ __forceinline__ KrylovS *ks(const DevP &P) { return P.ksi; }
+};
+
+// vector selectors of the level-0 vectors (0-7 Krylov work vectors; the FP32 side has
+// the work vectors, rhs and sol only)
+template <class T>
+__device__ __forceinline__ T *vsel(const DevP &P, int s) {
+    if (s < 8) return PT<T>::wk(P, s);
+    if constexpr (std::is_same<T, double>::value) {
+        switch (s) {
+        case V_RHS: return P.rhs;
+        case V_SOL: return P.sol;
+        case V_F: return P.F;
+        case V_TR: return P.tr;
+        case V_PHI: return P.phi;
+        default: return P.dsc;
+        }
+    } else {
+        return s == V_RHS ? P.rhs32 : P.sol32;
     }
 }
 
 // y = A x on a level (7-point, boundary terms skipped as in semiconductor_3d.c:1975-1993)
 template <class T>
-__device__ __forceinline__ double stencil_apply(T *const *A, const T *x, int k, int i, int j, int l, int Nx, int Ny,
-                                                int Nz) {
+__device__ __forceinline__ T stencil_apply(T *const *A, const T *x, int k, int i, int j, int l, int Nx, int Ny, int Nz) {
     const int NxNy = Nx * Ny;
-    double s = (double)A[0][k] * (double)x[k];
-    if (i > 0) s += (double)A[1][k] * (double)x[k - 1];
-    if (i < Nx - 1) s += (double)A[2][k] * (double)x[k + 1];
-    if (j > 0) s += (double)A[3][k] * (double)x[k - Nx];
-    if (j < Ny - 1) s += (double)A[4][k] * (double)x[k + Nx];
-    if (l > 0) s += (double)A[5][k] * (double)x[k - NxNy];
-    if (l < Nz - 1) s += (double)A[6][k] * (double)x[k + NxNy];
+    T s = A[0][k] * x[k];
+    if (i > 0) s += A[1][k] * x[k - 1];
+    if (i < Nx - 1) s += A[2][k] * x[k + 1];
+    if (j > 0) s += A[3][k] * x[k - Nx];
+    if (j < Ny - 1) s += A[4][k] * x[k + Nx];
+    if (l > 0) s += A[5][k] * x[k - NxNy];
+    if (l < Nz - 1) s += A[6][k] * x[k + NxNy];
     return s;
 }
 // sum over the off-diagonal couplings only
 template <class T>
-__device__ __forceinline__ double offdiag_apply(T *const *A, const T *x, int k, int i, int j, int l, int Nx, int Ny,
-                                                int Nz) {
+__device__ __forceinline__ T offdiag_apply(T *const *A, const T *x, int k, int i, int j, int l, int Nx, int Ny, int Nz) {
     const int NxNy = Nx * Ny;
-    double s = 0.0;
-    if (i > 0) s += (double)A[1][k] * (double)x[k - 1];
-    if (i < Nx - 1) s += (double)A[2][k] * (double)x[k + 1];
-    if (j > 0) s += (double)A[3][k] * (double)x[k - Nx];
-    if (j < Ny - 1) s += (double)A[4][k] * (double)x[k + Nx];
-    if (l > 0) s += (double)A[5][k] * (double)x[k - NxNy];
-    if (l < Nz - 1) s += (double)A[6][k] * (double)x[k + NxNy];
+    T s = 0;
+    if (i > 0) s += A[1][k] * x[k - 1];
+    if (i < Nx - 1) s += A[2][k] * x[k + 1];
+    if (j > 0) s += A[3][k] * x[k - Nx];
+    if (j < Ny - 1) s += A[4][k] * x[k + Nx];
+    if (l > 0) s += A[5][k] * x[k - NxNy];
+    if (l < Nz - 1) s += A[6][k] * x[k + NxNy];
     return s;
 }
 // sum of a_kj x_j / D_j over the neighbours (forward sweep of the black rows)
 template <class T>
-__device__ __forceinline__ double offdiag_apply_div(T *const *A, const T *x, const T *D, int k, int i, int j, int l,
-                                                    int Nx, int Ny, int Nz) {
+__device__ __forceinline__ T offdiag_apply_div(T *const *A, const T *x, const T *D, int k, int i, int j, int l, int Nx,
+                                               int Ny, int Nz) {
     const int NxNy = Nx * Ny;
-    double s = 0.0;
-    if (i > 0) s += (double)A[1][k] * (double)x[k - 1] / (double)D[k - 1];
-    if (i < Nx - 1) s += (double)A[2][k] * (double)x[k + 1] / (double)D[k + 1];
-    if (j > 0) s += (double)A[3][k] * (double)x[k - Nx] / (double)D[k - Nx];
-    if (j < Ny - 1) s += (double)A[4][k] * (double)x[k + Nx] / (double)D[k + Nx];
-    if (l > 0) s += (double)A[5][k] * (double)x[k - NxNy] / (double)D[k - NxNy];
-    if (l < Nz - 1) s += (double)A[6][k] * (double)x[k + NxNy] / (double)D[k + NxNy];
+    T s = 0;
+    if (i > 0) s += A[1][k] * x[k - 1] / D[k - 1];
+    if (i < Nx - 1) s += A[2][k] * x[k + 1] / D[k + 1];
+    if (j > 0) s += A[3][k] * x[k - Nx] / D[k - Nx];
+    if (j < Ny - 1) s += A[4][k] * x[k + Nx] / D[k + Nx];
+    if (l > 0) s += A[5][k] * x[k - NxNy] / D[k - NxNy];
+    if (l < Nz - 1) s += A[6][k] * x[k + NxNy] / D[k + NxNy];
     return s;
 }
 
 // ------------------------------------------------------------------ multigrid levels
 // level accessors: level 0 reads the instance's system arrays and the caller's vectors
+template <class T>
 struct LevView {
-    double *A[7];
-    double *D, *x, *b, *r, *pw, *ph;
+    T *A[7];
+    T *D, *x, *b, *r, *pw;
+    double *ph;
     int Nx, Ny, Nz, N, cx, cy, cz, last;
 };
-__device__ __forceinline__ LevView levview(const DevP &P, int L, int bsel, int xsel) {
-    const LevelT<double> &lv = P.lev[L];
-    LevView v;
+template <class T>
+__device__ __forceinline__ LevView<T> levview(const DevP &P, int L, int bsel, int xsel) {
+    const LevelT<T> &lv = PT<T>::lev(P, L);
+    LevView<T> v;
 #pragma unroll
-    for (int q = 0; q < 7; q++) v.A[q] = L == 0 ? P.A[q] : lv.A[q];
+    for (int q = 0; q < 7; q++) v.A[q] = lv.A[q];
     v.D = lv.D; v.r = lv.r; v.pw = lv.pw; v.ph = lv.ph;
-    v.x = L == 0 ? vsel(P, xsel) : lv.x;
-    v.b = L == 0 ? vsel(P, bsel) : lv.b;
+    v.x = L == 0 ? vsel<T>(P, xsel) : lv.x;
+    v.b = L == 0 ? vsel<T>(P, bsel) : lv.b;
     v.Nx = lv.Nx; v.Ny = lv.Ny; v.Nz = lv.Nz; v.N = lv.N;
     v.cx = lv.cx; v.cy = lv.cy; v.cz = lv.cz; v.last = lv.last;
     return v;
 }
-__device__ __forceinline__ bool ks_running(const DevP &P) { return P.ks->active != 0; }
+template <class T>
+__device__ __forceinline__ bool ks_running(const DevP &P) { return PT<T>::ks(P)->active != 0; }
+// gate 0: always run; 1: only while the instance's Krylov loop (of precision T) is
+// active; 2: also not after a half-step exit
+template <class T>
+__device__ __forceinline__ bool gated_off(const DevP &P, int gate) {
+    if (!gate) return false;
+    const KrylovS *s = PT<T>::ks(P);
+    return !s->active || (gate == 2 && s->half);
+}
 
 // red-black D-ILU pivots: red D = a_kk; black D = a_kk - sum a_kr a_rk / a_rr, guarded
 // as the reference guards its ILU pivots (semiconductor_3d.c:1937-1938)
+template <class T>
 __global__ void k_ilu_diag(const DevP *__restrict__ Ps, int L) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     if (L > 0 && L >= P.nlev - 1) return;
-    const LevView v = levview(P, L, 0, 0);
+    const LevView<T> v = levview<T>(P, L, 0, 0);
     SS_GRID_LOOP(k, v.N) {
         const Node a = unidx(k, v.Nx, v.Ny);
-        const double c = v.A[0][k];
-        double d = c;
+        const T c = v.A[0][k];
+        T d = c;
         if ((a.i + a.j + a.l) & 1) {
             const int NxNy = v.Nx * v.Ny;
-            double s = 0.0;
+            T s = 0;
             if (a.i > 0) s += v.A[1][k] * v.A[2][k - 1] / v.A[0][k - 1];
             if (a.i < v.Nx - 1) s += v.A[2][k] * v.A[1][k + 1] / v.A[0][k + 1];
             if (a.j > 0) s += v.A[3][k] * v.A[4][k - v.Nx] / v.A[0][k - v.Nx];
@@ -134,49 +183,17 @@ __global__ void k_ilu_diag(const DevP *__restrict__ Ps, int L) {
             if (a.l > 0) s += v.A[5][k] * v.A[6][k - NxNy] / v.A[0][k - NxNy];
             if (a.l < v.Nz - 1) s += v.A[6][k] * v.A[5][k + NxNy] / v.A[0][k + NxNy];
             d = c - s;
-            if (!(d > 1e-8 * fabs(c))) d = c;
+            if (!(d > T(1e-8) * fabs(c))) d = c;
         }
-        if (!(d != 0.0)) d = 1.0;
+        if (!(d != T(0))) d = 1;
         v.D[k] = d;
-    }
-}
-
-// pre-smoothing from x = 0: black rows then red rows of the two triangular sweeps
-// mode 0: x = M^-1 b (from zero).  mode 1: post-smoothing, z = M^-1 r with r the level's
-// residual array, x += z (the black z is parked in r for the red sweep).
-__global__ void k_smooth_black(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int mode, int gate) {
-    const DevP &P = Ps[blockIdx.y];
-    if ((L > 0 && L >= P.nlev - 1) || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
-    const LevView v = levview(P, L, bsel, xsel);
-    const double *src = mode ? v.r : v.b;
-    SS_GRID_LOOP(k, v.N) {
-        const Node a = unidx(k, v.Nx, v.Ny);
-        if (!((a.i + a.j + a.l) & 1)) continue;
-        const double s = offdiag_apply_div<double>(v.A, src, v.D, k, a.i, a.j, a.l, v.Nx, v.Ny, v.Nz);
-        const double z = (src[k] - s) / v.D[k];
-        if (mode) { v.x[k] += z; v.r[k] = z; }
-        else v.x[k] = z;
-    }
-}
-__global__ void k_smooth_red(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int mode, int gate) {
-    const DevP &P = Ps[blockIdx.y];
-    if ((L > 0 && L >= P.nlev - 1) || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
-    const LevView v = levview(P, L, bsel, xsel);
-    const double *src = mode ? v.r : v.b;
-    const double *zb = mode ? v.r : v.x;
-    SS_GRID_LOOP(k, v.N) {
-        const Node a = unidx(k, v.Nx, v.Ny);
-        if ((a.i + a.j + a.l) & 1) continue;
-        const double s = offdiag_apply<double>(v.A, zb, k, a.i, a.j, a.l, v.Nx, v.Ny, v.Nz);
-        const double z = (src[k] - s) / v.D[k];
-        if (mode) v.x[k] += z;
-        else v.x[k] = z;
     }
 }
 
 // coarse aggregate (I,J,L) -> fine index range (AGG_RANGE, semiconductor_3d.c:1996-1999)
 struct Agg { int i0, i1, j0, j1, l0, l1; };
-__device__ __forceinline__ Agg agg_range(const LevView &f, int I, int J, int K) {
+template <class V>
+__device__ __forceinline__ Agg agg_range(const V &f, int I, int J, int K) {
     Agg g;
     g.i0 = f.cx ? 2 * I : I; g.i1 = f.cx ? 2 * I + 1 : I; if (g.i1 > f.Nx - 1) g.i1 = f.Nx - 1;
     g.j0 = f.cy ? 2 * J : J; g.j1 = f.cy ? 2 * J + 1 : J; if (g.j1 > f.Ny - 1) g.j1 = f.Ny - 1;
@@ -184,76 +201,43 @@ __device__ __forceinline__ Agg agg_range(const LevView &f, int I, int J, int K) 
     return g;
 }
 
-// residual b - A x of the fine level summed over every aggregate (restriction), with
-// the level-0 row weights w (semiconductor_3d.c:2028-2037 applied to 1984-1991)
-__global__ void k_resid_restrict(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int wsel, int gate) {
-    const DevP &P = Ps[blockIdx.y];
-    if (L >= P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
-    const LevView f = levview(P, L, bsel, xsel);
-    const LevelT<double> &cl = P.lev[L + 1];
-    const double *w = (L == 0 && wsel) ? P.dsc : nullptr;
-    SS_GRID_LOOP(K, cl.N) {
-        const Node c = unidx(K, cl.Nx, cl.Ny);
-        const Agg g = agg_range(f, c.i, c.j, c.l);
-        double s = 0.0;
-        for (int l = g.l0; l <= g.l1; l++)
-            for (int j = g.j0; j <= g.j1; j++)
-                for (int i = g.i0; i <= g.i1; i++) {
-                    const int k = i + f.Nx * (j + f.Ny * l);
-                    const double r = f.b[k] - stencil_apply<double>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
-                    s += w ? w[k] * r : r;
-                }
-        cl.b[K] = s;
-    }
-}
-
-// x += alpha pw P xc (semiconductor_3d.c:2038-2048), then nothing else: the residual
-// needs every prolonged neighbour and is a separate pass
+// x += alpha pw P xc (semiconductor_3d.c:2038-2048); the residual that follows needs
+// every prolonged neighbour and is a separate pass
+template <class T>
 __global__ void k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha, int gate) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (L >= P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
-    const LevView f = levview(P, L, bsel, xsel);
-    const LevelT<double> &cl = P.lev[L + 1];
+    if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
+    const LevView<T> f = levview<T>(P, L, bsel, xsel);
+    const LevelT<T> &cl = PT<T>::lev(P, L + 1);
+    const T al = (T)alpha;
     SS_GRID_LOOP(k, f.N) {
         const Node a = unidx(k, f.Nx, f.Ny);
         const int I = f.cx ? a.i >> 1 : a.i, J = f.cy ? a.j >> 1 : a.j, K = f.cz ? a.l >> 1 : a.l;
-        f.x[k] += alpha * f.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+        f.x[k] += al * f.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
     }
 }
+template <class T>
 __global__ void k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (L >= P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
-    const LevView f = levview(P, L, bsel, xsel);
+    if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
+    const LevView<T> f = levview<T>(P, L, bsel, xsel);
     SS_GRID_LOOP(k, f.N) {
         const Node a = unidx(k, f.Nx, f.Ny);
-        f.r[k] = f.b[k] - stencil_apply<double>(f.A, f.x, k, a.i, a.j, a.l, f.Nx, f.Ny, f.Nz);
-    }
-}
-
-// coarsest level: x = M^-1 b with the dense inverse formed at set-up (one block per instance)
-__global__ void k_coarse_solve(const DevP *__restrict__ Ps, int L, int gate) {
-    const DevP &P = Ps[blockIdx.y];
-    if (L != P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
-    const LevelT<double> &v = P.lev[L];
-    const int n = v.N;
-    __shared__ double sb[COARSE_MAX];
-    double *b = v.b, *x = v.x;
-    if (L == 0) return;                    // a single-level hierarchy is not built
-    for (int q = threadIdx.x; q < n; q += blockDim.x) sb[q] = b[q];
-    __syncthreads();
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-        double s = 0.0;
-        for (int q = 0; q < n; q++) s += v.D[r * n + q] * sb[q];
-        x[r] = s;
+        f.r[k] = f.b[k] - stencil_apply<T>(f.A, f.x, k, a.i, a.j, a.l, f.Nx, f.Ny, f.Nz);
     }
 }
 
 // coarsest level set-up: dense matrix of the stencil, Gauss-Jordan inverse with partial
-// pivoting (tiny pivots guarded as semiconductor_3d.c:2066 does)
+// pivoting (tiny pivots guarded as semiconductor_3d.c:2066 does), formed in FP64 and
+// stored in T
+template <class T>
 __global__ void k_coarse_setup(const DevP *__restrict__ Ps, int L) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     if (L != P.nlev - 1 || L == 0) return;
-    const LevelT<double> &v = P.lev[L];
+    const LevelT<T> &v = PT<T>::lev(P, L);
     const int n = v.N;
     __shared__ double M[COARSE_MAX][COARSE_MAX + 1];
     __shared__ int perm[COARSE_MAX];
@@ -315,7 +299,7 @@ __global__ void k_coarse_setup(const DevP *__restrict__ Ps, int L) {
     }
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, q = e % n;
-        v.D[r * n + q] = M[r][q];
+        v.D[r * n + q] = (T)M[r][q];
     }
 }
 
@@ -325,18 +309,20 @@ __device__ __forceinline__ double ph0(const DevP &P, int k, int qsign) {
     if (fl_kind(f) != K_SEMI || fl_fix(f)) return PH_NONE;
     return qsign > 0 ? P.phin[k] / P.VTref : -P.phip[k] / P.VTref;
 }
+template <class T>
 __global__ void k_mg_weights(const DevP *__restrict__ Ps, int L, int qsign) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     if (L >= P.nlev - 1) return;
-    const LevView f = levview(P, L, 0, 0);
-    const LevelT<double> &cl = P.lev[L + 1];
+    const LevView<T> f = levview<T>(P, L, 0, 0);
+    const LevelT<T> &cl = PT<T>::lev(P, L + 1);
     SS_GRID_LOOP(K, cl.N) {
         const Node c = unidx(K, cl.Nx, cl.Ny);
         const Agg g = agg_range(f, c.i, c.j, c.l);
         if (qsign == 0) {
             for (int l = g.l0; l <= g.l1; l++)
                 for (int j = g.j0; j <= g.j1; j++)
-                    for (int i = g.i0; i <= g.i1; i++) f.pw[i + f.Nx * (j + f.Ny * l)] = 1.0;
+                    for (int i = g.i0; i <= g.i1; i++) f.pw[i + f.Nx * (j + f.Ny * l)] = 1;
             continue;
         }
         double mx = PH_NONE;
@@ -354,18 +340,20 @@ __global__ void k_mg_weights(const DevP *__restrict__ Ps, int L, int qsign) {
                     const int k = i + f.Nx * (j + f.Ny * l);
                     const double p = L == 0 ? ph0(P, k, qsign) : f.ph[k];
                     const double e = (p <= 0.5 * PH_NONE) ? -800.0 : p - mx;
-                    f.pw[k] = e < -700.0 ? 0.0 : exp(e);
+                    f.pw[k] = (T)(e < -700.0 ? 0.0 : exp(e));
                 }
     }
 }
 
-// Petrov-Galerkin coarse operator P^T W A P (semiconductor_3d.c:2003-2027)
+// Petrov-Galerkin coarse operator P^T W A P (semiconductor_3d.c:2003-2027), summed in FP64
+template <class T>
 __global__ void k_galerkin(const DevP *__restrict__ Ps, int L, int wsel) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     if (L >= P.nlev - 1) return;
-    const LevView f = levview(P, L, 0, 0);
-    const LevelT<double> &cl = P.lev[L + 1];
-    const double *w = (L == 0 && wsel) ? P.dsc : nullptr;
+    const LevView<T> f = levview<T>(P, L, 0, 0);
+    const LevelT<T> &cl = PT<T>::lev(P, L + 1);
+    const T *w = (L == 0 && wsel) ? PT<T>::w0(P) : nullptr;
     const int NxNy = f.Nx * f.Ny;
     SS_GRID_LOOP(K, cl.N) {
         const Node c = unidx(K, cl.Nx, cl.Ny);
@@ -375,26 +363,38 @@ __global__ void k_galerkin(const DevP *__restrict__ Ps, int L, int wsel) {
             for (int j = g.j0; j <= g.j1; j++)
                 for (int i = g.i0; i <= g.i1; i++) {
                     const int k = i + f.Nx * (j + f.Ny * l);
-                    const double wk = w ? w[k] : 1.0;
+                    const double wk = w ? (double)w[k] : 1.0;
                     double a;
-                    cc += wk * f.A[0][k] * f.pw[k];
-                    if (i > 0) { a = wk * f.A[1][k] * f.pw[k - 1]; if (i - 1 >= g.i0) cc += a; else xm += a; }
-                    if (i < f.Nx - 1) { a = wk * f.A[2][k] * f.pw[k + 1]; if (i + 1 <= g.i1) cc += a; else xp += a; }
-                    if (j > 0) { a = wk * f.A[3][k] * f.pw[k - f.Nx]; if (j - 1 >= g.j0) cc += a; else ym += a; }
-                    if (j < f.Ny - 1) { a = wk * f.A[4][k] * f.pw[k + f.Nx]; if (j + 1 <= g.j1) cc += a; else yp += a; }
-                    if (l > 0) { a = wk * f.A[5][k] * f.pw[k - NxNy]; if (l - 1 >= g.l0) cc += a; else zm += a; }
-                    if (l < f.Nz - 1) { a = wk * f.A[6][k] * f.pw[k + NxNy]; if (l + 1 <= g.l1) cc += a; else zp += a; }
+                    cc += wk * (double)f.A[0][k] * (double)f.pw[k];
+                    if (i > 0) { a = wk * (double)f.A[1][k] * (double)f.pw[k - 1]; if (i - 1 >= g.i0) cc += a; else xm += a; }
+                    if (i < f.Nx - 1) { a = wk * (double)f.A[2][k] * (double)f.pw[k + 1]; if (i + 1 <= g.i1) cc += a; else xp += a; }
+                    if (j > 0) { a = wk * (double)f.A[3][k] * (double)f.pw[k - f.Nx]; if (j - 1 >= g.j0) cc += a; else ym += a; }
+                    if (j < f.Ny - 1) { a = wk * (double)f.A[4][k] * (double)f.pw[k + f.Nx]; if (j + 1 <= g.j1) cc += a; else yp += a; }
+                    if (l > 0) { a = wk * (double)f.A[5][k] * (double)f.pw[k - NxNy]; if (l - 1 >= g.l0) cc += a; else zm += a; }
+                    if (l < f.Nz - 1) { a = wk * (double)f.A[6][k] * (double)f.pw[k + NxNy]; if (l + 1 <= g.l1) cc += a; else zp += a; }
                 }
         if (cc == 0. && xm == 0. && xp == 0. && ym == 0. && yp == 0. && zm == 0. && zp == 0.) cc = 1.;
-        cl.A[0][K] = cc; cl.A[1][K] = xm; cl.A[2][K] = xp; cl.A[3][K] = ym;
-        cl.A[4][K] = yp; cl.A[5][K] = zm; cl.A[6][K] = zp;
+        cl.A[0][K] = (T)cc; cl.A[1][K] = (T)xm; cl.A[2][K] = (T)xp; cl.A[3][K] = (T)ym;
+        cl.A[4][K] = (T)yp; cl.A[5][K] = (T)zm; cl.A[6][K] = (T)zp;
     }
 }
 
-// ------------------------------------------------------------------ vector kernels
-__global__ void k_absmax(const DevP *__restrict__ Ps, int xsel, int slot) {
+// FP32 copy of the level-0 operator and its row weights (start of a refined solve)
+__global__ void k_to32(const DevP *__restrict__ Ps, int wsel) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    const double *x = vsel(P, xsel);
+    SS_GRID_LOOP(k, P.N) {
+#pragma unroll
+        for (int q = 0; q < 7; q++) P.A32[q][k] = (float)P.A[q][k];
+        if (wsel) P.dsc32[k] = (float)P.dsc[k];
+    }
+}
+
+// ------------------------------------------------------------------ vector kernels (FP64)
+__global__ void k_absmax(const DevP *__restrict__ Ps, int xsel, int slot) {
+    pdl_entry();
+    const DevP &P = Ps[blockIdx.y];
+    const double *x = vsel<double>(P, xsel);
     double m = 0.0;
     SS_GRID_LOOP(k, P.N) {
         const double a = fabs(x[k]);
@@ -404,82 +404,96 @@ __global__ void k_absmax(const DevP *__restrict__ Ps, int xsel, int slot) {
 }
 // y = x + a z  (selectors)
 __global__ void k_axpy(const DevP *__restrict__ Ps, int ysel, int xsel, double a, int zsel) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    double *y = vsel(P, ysel);
-    const double *x = vsel(P, xsel), *z = vsel(P, zsel);
+    double *y = vsel<double>(P, ysel);
+    const double *x = vsel<double>(P, xsel), *z = vsel<double>(P, zsel);
     SS_GRID_LOOP(k, P.N) y[k] = x[k] + a * z[k];
 }
 __global__ void k_fill(const DevP *__restrict__ Ps, int ysel, double v) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    double *y = vsel(P, ysel);
+    double *y = vsel<double>(P, ysel);
     SS_GRID_LOOP(k, P.N) y[k] = v;
 }
 __global__ void k_copy(const DevP *__restrict__ Ps, int ysel, int xsel) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    double *y = vsel(P, ysel);
-    const double *x = vsel(P, xsel);
+    double *y = vsel<double>(P, ysel);
+    const double *x = vsel<double>(P, xsel);
     SS_GRID_LOOP(k, P.N) y[k] = x[k];
 }
 
-void launch_absmax_sel(const Ctx &c, int xsel, int slot) { SS_LAUNCH(PF_VEC, c.maxN, k_absmax, grid_nodes(c), TPB, c.st, c.dP, xsel, slot); }
+void launch_absmax_sel(const Ctx &c, int xsel, int slot) { SS_LAUNCH_PDL(PF_VEC, c.maxN, k_absmax, grid_nodes(c), TPB, c.st, c.dP, xsel, slot); }
 void launch_axpy_sel(const Ctx &c, int ysel, int xsel, double a, int zsel) {
-    SS_LAUNCH(PF_VEC, c.maxN, k_axpy, grid_nodes(c), TPB, c.st, c.dP, ysel, xsel, a, zsel);
+    SS_LAUNCH_PDL(PF_VEC, c.maxN, k_axpy, grid_nodes(c), TPB, c.st, c.dP, ysel, xsel, a, zsel);
 }
-void launch_fill_sel(const Ctx &c, int ysel, double v) { SS_LAUNCH(PF_VEC, c.maxN, k_fill, grid_nodes(c), TPB, c.st, c.dP, ysel, v); }
-void launch_copy_sel(const Ctx &c, int ysel, int xsel) { SS_LAUNCH(PF_VEC, c.maxN, k_copy, grid_nodes(c), TPB, c.st, c.dP, ysel, xsel); }
+void launch_fill_sel(const Ctx &c, int ysel, double v) { SS_LAUNCH_PDL(PF_VEC, c.maxN, k_fill, grid_nodes(c), TPB, c.st, c.dP, ysel, v); }
+void launch_copy_sel(const Ctx &c, int ysel, int xsel) { SS_LAUNCH_PDL(PF_VEC, c.maxN, k_copy, grid_nodes(c), TPB, c.st, c.dP, ysel, xsel); }
 
-// ------------------------------------------------------------------ multigrid driver
-void mg_setup(const Ctx &c, const MGHost &mg, int qsign) {
+// ------------------------------------------------------------------ multigrid set-up
+// hierarchy of the system now in A: Slotboom weights, Galerkin products, smoother
+// pivots, coarsest inverse.  T = float first copies the level-0 operator to FP32.
+template <class T>
+static void mg_setup_t(const Ctx &c, const MGHost &mg, int qsign) {
+    if (std::is_same<T, float>::value)
+        SS_LAUNCH_PDL(PF_CONVERT32, c.maxN, k_to32, grid_nodes(c), TPB, c.st, c.dP, qsign != 0);
     for (int L = 0; L < mg.maxlev - 1; L++) {
         const int nc = mg.maxN[L + 1];
-        SS_LAUNCH(PF_WEIGHTS, nc, k_mg_weights, grid_n(c, nc), TPB, c.st, c.dP, L, qsign);
-        SS_LAUNCH(PF_GALERKIN, nc, k_galerkin, grid_n(c, nc), TPB, c.st, c.dP, L, qsign != 0);
-        SS_LAUNCH(PF_ILU_DIAG, mg.maxN[L], k_ilu_diag, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L);
+        SS_LAUNCH_PDL(pf<T>(PF_WEIGHTS), nc, k_mg_weights<T>, grid_n(c, nc), TPB, c.st, c.dP, L, qsign);
+        SS_LAUNCH_PDL(pf<T>(PF_GALERKIN), nc, k_galerkin<T>, grid_n(c, nc), TPB, c.st, c.dP, L, qsign != 0);
+        SS_LAUNCH_PDL(pf<T>(PF_ILU_DIAG), mg.maxN[L], k_ilu_diag<T>, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L);
     }
-    for (int L = 1; L < mg.maxlev; L++) SS_LAUNCH(PF_COARSE_SETUP, COARSE_MAX, k_coarse_setup, dim3(1, c.ninst), TPB, c.st, c.dP, L);
+    for (int L = 1; L < mg.maxlev; L++)
+        SS_LAUNCH_PDL(pf<T>(PF_COARSE_SETUP), COARSE_MAX, k_coarse_setup<T>, dim3(1, c.ninst), TPB, c.st, c.dP, L);
 }
+void mg_setup(const Ctx &c, const MGHost &mg, int qsign) { mg_setup_t<double>(c, mg, qsign); }
 
+// ------------------------------------------------------------------ V-cycle
 // one V(1,1) cycle x = M^-1 b on the level-0 vectors (bsel -> xsel); mg_on = 0 applies
-// the level-0 smoother alone (the reference's ILU-only fallback).  gate: 0 always run,
-// 1 only while the instance's Krylov loop is active, 2 also not after a half-step exit.
+// the level-0 smoother alone (the reference's ILU-only fallback).
 // ---- fine levels: one kernel per pass, all SMs
 // Smoother half sweep over the nodes of one colour only: thread t of a row (j,l) takes
 // i = 2t + ((j + l + colour) & 1), so every lane does work (colour 1 = black, 0 = red).
+// mode 0: pre-smoothing from x = 0, x = M^-1 b.  mode 1: post-smoothing, z = M^-1 r
+// with r the level's residual array, x += z (the black z is parked in r for the red
+// sweep).  mode 2: a further application right after a red-black one.
+template <class T>
 __global__ void k_smooth_c(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int mode, int color, int gate) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if ((L > 0 && L >= P.nlev - 1) || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
-    const LevView v = levview(P, L, bsel, xsel);
+    if ((L > 0 && L >= P.nlev - 1) || gated_off<T>(P, gate)) return;
+    const LevView<T> v = levview<T>(P, L, bsel, xsel);
     const int hx = (v.Nx + 1) >> 1, rows = v.Ny * v.Nz;
-    const double *src = mode ? v.r : v.b;
-    const double *zb = mode ? v.r : v.x;
+    const T *src = mode ? v.r : v.b;
+    const T *zb = mode ? v.r : v.x;
     SS_GRID_LOOP(t, hx * rows) {
         const int row = t / hx, ti = t - row * hx;
         const int l = row / v.Ny, j = row - l * v.Ny;
         const int i = 2 * ti + ((j + l + color) & 1);
         if (i >= v.Nx) continue;
         const int k = i + v.Nx * row;
-        double z;
+        T z;
         if (mode == 2) {
-            // a further application of the preconditioner right after a red-black one:
-            // the residual of every red node is then zero, so black z = r / D with the
-            // full-stencil residual, and red z = -(sum a_rb z_b) / D
+            // the residual of every red node is zero after a red-black application, so
+            // black z = r / D with the full-stencil residual, and red z = -(sum a_rb z_b) / D
             if (color) {
-                z = (v.b[k] - stencil_apply<double>(v.A, v.x, k, i, j, l, v.Nx, v.Ny, v.Nz)) / v.D[k];
+                z = (v.b[k] - stencil_apply<T>(v.A, v.x, k, i, j, l, v.Nx, v.Ny, v.Nz)) / v.D[k];
                 v.x[k] += z;
                 v.r[k] = z;
             } else {
-                z = -offdiag_apply<double>(v.A, v.r, k, i, j, l, v.Nx, v.Ny, v.Nz) / v.D[k];
+                z = -offdiag_apply<T>(v.A, v.r, k, i, j, l, v.Nx, v.Ny, v.Nz) / v.D[k];
                 v.x[k] += z;
             }
             continue;
         }
         if (color) {
-            const double s = offdiag_apply_div<double>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
+            const T s = offdiag_apply_div<T>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
             z = (src[k] - s) / v.D[k];
             if (mode) { v.x[k] += z; v.r[k] = z; }
             else v.x[k] = z;
         } else {
-            const double s = offdiag_apply<double>(v.A, zb, k, i, j, l, v.Nx, v.Ny, v.Nz);
+            const T s = offdiag_apply<T>(v.A, zb, k, i, j, l, v.Nx, v.Ny, v.Nz);
             z = (src[k] - s) / v.D[k];
             if (mode) v.x[k] += z;
             else v.x[k] = z;
@@ -492,13 +506,15 @@ __global__ void k_smooth_c(const DevP *__restrict__ Ps, int L, int bsel, int xse
 // row blockIdx.z; pairs along x meet through a shuffle, the four parities through
 // shared memory.  One thread per fine node (the restriction of semiconductor_3d.c:
 // 2028-2037 applied to the residual of 1984-1991).
+template <class T>
 __global__ void __launch_bounds__(128) k_resid_restrict2(const DevP *__restrict__ Ps, int L, int bsel, int xsel,
                                                          int wsel, int gate) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (L >= P.nlev - 1 || (gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
-    const LevView f = levview(P, L, bsel, xsel);
-    const LevelT<double> &cl = P.lev[L + 1];
-    const double *w = (L == 0 && wsel) ? P.dsc : nullptr;
+    if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
+    const LevView<T> f = levview<T>(P, L, bsel, xsel);
+    const LevelT<T> &cl = PT<T>::lev(P, L + 1);
+    const T *w = (L == 0 && wsel) ? PT<T>::w0(P) : nullptr;
     const int R = blockIdx.z;                         // coarse row J + Cy*Lc
     const bool rowok = R < cl.Ny * cl.Nz;
     const int Lc = rowok ? R / cl.Ny : 0, Jc = rowok ? R - Lc * cl.Ny : 0;
@@ -506,17 +522,17 @@ __global__ void __launch_bounds__(128) k_resid_restrict2(const DevP *__restrict_
     const int i = blockIdx.x * 32 + threadIdx.x;
     const int j = f.cy ? 2 * Jc + dj : Jc, l = f.cz ? 2 * Lc + dl : Lc;
     const bool ok = rowok && i < f.Nx && j < f.Ny && l < f.Nz && (f.cy || dj == 0) && (f.cz || dl == 0);
-    double val = 0.0;
+    T val = 0;
     if (ok) {
         const int k = i + f.Nx * (j + f.Ny * l);
-        const double r = f.b[k] - stencil_apply<double>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
+        const T r = f.b[k] - stencil_apply<T>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
         val = w ? w[k] * r : r;
     }
-    __shared__ double sh[4][32];
+    __shared__ T sh[4][32];
     sh[threadIdx.y][threadIdx.x] = val;
     __syncthreads();
     if (threadIdx.y == 0) {
-        double s = sh[0][threadIdx.x] + sh[1][threadIdx.x] + sh[2][threadIdx.x] + sh[3][threadIdx.x];
+        T s = sh[0][threadIdx.x] + sh[1][threadIdx.x] + sh[2][threadIdx.x] + sh[3][threadIdx.x];
         if (f.cx) {
             s += __shfl_down_sync(0xffffffffu, s, 1);
             if (rowok && !(threadIdx.x & 1) && i < f.Nx) cl.b[(i >> 1) + cl.Nx * R] = s;
@@ -536,9 +552,10 @@ __device__ __forceinline__ int cl_first() {
 __device__ __forceinline__ int cl_stride() { return (int)cg::this_cluster().num_blocks() * blockDim.x; }
 __device__ __forceinline__ void cl_sync() { cg::this_cluster().sync(); }
 
-__device__ __forceinline__ void cta_smooth(const LevView &v, int color, int mode) {
-    const double *src = mode ? v.r : v.b;
-    const double *zb = mode ? v.r : v.x;
+template <class T>
+__device__ __forceinline__ void cta_smooth(const LevView<T> &v, int color, int mode) {
+    const T *src = mode ? v.r : v.b;
+    const T *zb = mode ? v.r : v.x;
     const int hx = (v.Nx + 1) >> 1, rows = v.Ny * v.Nz;
     for (int t = cl_first(); t < hx * rows; t += cl_stride()) {
         const int row = t / hx, ti = t - row * hx;
@@ -547,36 +564,38 @@ __device__ __forceinline__ void cta_smooth(const LevView &v, int color, int mode
         if (i >= v.Nx) continue;
         const int k = i + v.Nx * row;
         if (color) {
-            const double s = offdiag_apply_div<double>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
-            const double z = (src[k] - s) / v.D[k];
+            const T s = offdiag_apply_div<T>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
+            const T z = (src[k] - s) / v.D[k];
             if (mode) { v.x[k] += z; v.r[k] = z; }
             else v.x[k] = z;
         } else {
-            const double s = offdiag_apply<double>(v.A, zb, k, i, j, l, v.Nx, v.Ny, v.Nz);
-            const double z = (src[k] - s) / v.D[k];
+            const T s = offdiag_apply<T>(v.A, zb, k, i, j, l, v.Nx, v.Ny, v.Nz);
+            const T z = (src[k] - s) / v.D[k];
             if (mode) v.x[k] += z;
             else v.x[k] = z;
         }
     }
     cl_sync();
 }
-__device__ __forceinline__ void cta_resid_restrict(const LevView &f, const LevelT<double> &cl, const double *w) {
+template <class T>
+__device__ __forceinline__ void cta_resid_restrict(const LevView<T> &f, const LevelT<T> &cl, const T *w) {
     for (int K = cl_first(); K < cl.N; K += cl_stride()) {
         const Node c = unidx(K, cl.Nx, cl.Ny);
         const Agg g = agg_range(f, c.i, c.j, c.l);
-        double s = 0.0;
+        T s = 0;
         for (int l = g.l0; l <= g.l1; l++)
             for (int j = g.j0; j <= g.j1; j++)
                 for (int i = g.i0; i <= g.i1; i++) {
                     const int k = i + f.Nx * (j + f.Ny * l);
-                    const double r = f.b[k] - stencil_apply<double>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
+                    const T r = f.b[k] - stencil_apply<T>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
                     s += w ? w[k] * r : r;
                 }
         cl.b[K] = s;
     }
     cl_sync();
 }
-__device__ __forceinline__ void cta_prolong(const LevView &f, const LevelT<double> &cl, double alpha) {
+template <class T>
+__device__ __forceinline__ void cta_prolong(const LevView<T> &f, const LevelT<T> &cl, T alpha) {
     for (int k = cl_first(); k < f.N; k += cl_stride()) {
         const Node a = unidx(k, f.Nx, f.Ny);
         const int I = f.cx ? a.i >> 1 : a.i, J = f.cy ? a.j >> 1 : a.j, K = f.cz ? a.l >> 1 : a.l;
@@ -584,17 +603,19 @@ __device__ __forceinline__ void cta_prolong(const LevView &f, const LevelT<doubl
     }
     cl_sync();
 }
-__device__ __forceinline__ void cta_resid(const LevView &f) {
+template <class T>
+__device__ __forceinline__ void cta_resid(const LevView<T> &f) {
     for (int k = cl_first(); k < f.N; k += cl_stride()) {
         const Node a = unidx(k, f.Nx, f.Ny);
-        f.r[k] = f.b[k] - stencil_apply<double>(f.A, f.x, k, a.i, a.j, a.l, f.Nx, f.Ny, f.Nz);
+        f.r[k] = f.b[k] - stencil_apply<T>(f.A, f.x, k, a.i, a.j, a.l, f.Nx, f.Ny, f.Nz);
     }
     cl_sync();
 }
-__device__ __forceinline__ void cta_dense(const LevelT<double> &v) {
+template <class T>
+__device__ __forceinline__ void cta_dense(const LevelT<T> &v) {
     const int n = v.N;
     for (int r = cl_first(); r < n; r += cl_stride()) {
-        double s = 0.0;
+        T s = 0;
         for (int q = 0; q < n; q++) s += v.D[r * n + q] * v.b[q];
         v.x[r] = s;
     }
@@ -602,30 +623,32 @@ __device__ __forceinline__ void cta_dense(const LevelT<double> &v) {
 }
 
 constexpr int SMALL_TPB = 1024;
+template <class T>
 __global__ void __launch_bounds__(SMALL_TPB) k_vcycle_small(const DevP *__restrict__ Ps, int Ls, int bsel, int xsel,
                                                             int wsel, double alpha, int gate) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if ((gate && !ks_running(P)) || (gate == 2 && P.ks->half)) return;
+    if (gated_off<T>(P, gate)) return;
     const int nl = P.nlev;
     if (nl == 1) {                                 // a single level: the smoother alone
-        const LevView v = levview(P, 0, bsel, xsel);
-        cta_smooth(v, 1, 0);
-        cta_smooth(v, 0, 0);
+        const LevView<T> v = levview<T>(P, 0, bsel, xsel);
+        cta_smooth<T>(v, 1, 0);
+        cta_smooth<T>(v, 0, 0);
         return;
     }
     for (int L = Ls; L < nl - 1; L++) {
-        const LevView v = levview(P, L, bsel, xsel);
-        cta_smooth(v, 1, 0);
-        cta_smooth(v, 0, 0);
-        cta_resid_restrict(v, P.lev[L + 1], (L == 0 && wsel) ? P.dsc : nullptr);
+        const LevView<T> v = levview<T>(P, L, bsel, xsel);
+        cta_smooth<T>(v, 1, 0);
+        cta_smooth<T>(v, 0, 0);
+        cta_resid_restrict<T>(v, PT<T>::lev(P, L + 1), (L == 0 && wsel) ? PT<T>::w0(P) : nullptr);
     }
-    cta_dense(P.lev[nl - 1]);
+    cta_dense<T>(PT<T>::lev(P, nl - 1));
     for (int L = nl - 2; L >= Ls; L--) {
-        const LevView v = levview(P, L, bsel, xsel);
-        cta_prolong(v, P.lev[L + 1], alpha);
-        cta_resid(v);
-        cta_smooth(v, 1, 1);
-        cta_smooth(v, 0, 1);
+        const LevView<T> v = levview<T>(P, L, bsel, xsel);
+        cta_prolong<T>(v, PT<T>::lev(P, L + 1), (T)alpha);
+        cta_resid<T>(v);
+        cta_smooth<T>(v, 1, 1);
+        cta_smooth<T>(v, 0, 1);
     }
 }
 
@@ -633,153 +656,146 @@ int g_small_nodes = 2048;           // levels at or below this size run in the c
 int g_l0_sweeps = 2;                // red-black applications per smoothing step on the finest level
 static int g_cluster = 0;           // CTAs per cluster of the small-level kernel (set on first use)
 
+template <class T>
+static bool cluster16_ok() {
+    if (cudaFuncSetAttribute(k_vcycle_small<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    cudaLaunchConfig_t q = {};
+    q.gridDim = dim3(16, 1);
+    q.blockDim = dim3(SMALL_TPB);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 16; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+    q.attrs = at;
+    q.numAttrs = 1;
+    int ncl = 0;
+    const bool ok = cudaOccupancyMaxActiveClusters(&ncl, k_vcycle_small<T>, &q) == cudaSuccess && ncl >= 1;
+    cudaGetLastError();
+    return ok;
+}
+
 // cluster size of the small-level kernel (16 CTAs when the device allows non-portable
 // clusters of 16, else 8) and the size split, read once (SEMISIM_B200_CLUSTER / _SMALL)
 static void small_init() {
     if (!g_cluster) {
         const char *e = std::getenv("SEMISIM_B200_CLUSTER");
-        g_cluster = (e && std::atoi(e) == 8) ? 8 : 16;
+        int cl = (e && std::atoi(e) == 8) ? 8 : 16;
         if (const char *s = std::getenv("SEMISIM_B200_SMALL")) g_small_nodes = std::atoi(s);
         if (const char *s = std::getenv("SEMISIM_B200_L0SWEEPS")) g_l0_sweeps = std::atoi(s) > 1 ? 2 : 1;
-        if (cudaFuncSetAttribute(k_vcycle_small, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
-            g_cluster = 8;
-        cudaGetLastError();
-        cudaLaunchConfig_t q = {};
-        q.gridDim = dim3(g_cluster, 1);
-        q.blockDim = dim3(SMALL_TPB);
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = g_cluster; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-        q.attrs = at;
-        q.numAttrs = 1;
-        int ncl = 0;
-        if (cudaOccupancyMaxActiveClusters(&ncl, k_vcycle_small, &q) != cudaSuccess || ncl < 1) g_cluster = 8;
-        cudaGetLastError();
+        const bool ok64 = cluster16_ok<double>(), ok32 = cluster16_ok<float>();
+        if (!ok64 || !ok32) cl = 8;
+        g_cluster = cl;
     }
 }
 
 // launch the small-level V-cycle as clusters of g_cluster CTAs, one cluster per instance
+template <class T>
 static void launch_small(const Ctx &c, int nodes, int Ls, int bsel, int xsel, int wsel, double alpha, int gate) {
     small_init();
     g_launches++;
     t_launches++;
-    if (g_prof_on) prof_begin(PF_COARSE, c.st);
+    if (g_prof_on) prof_begin(pf<T>(PF_COARSE), c.st);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(g_cluster, c.ninst);
     cfg.blockDim = dim3(SMALL_TPB);
     cfg.stream = c.st;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = g_cluster; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_vcycle_small, c.dP, Ls, bsel, xsel, wsel, alpha, gate);
-    if (g_prof_on) prof_end(PF_COARSE, c.st, nodes);
+    cfg.numAttrs = g_pdl ? 2 : 1;
+    cudaLaunchKernelEx(&cfg, k_vcycle_small<T>, c.dP, Ls, bsel, xsel, wsel, alpha, gate);
+    if (g_prof_on) prof_end(pf<T>(PF_COARSE), c.st, nodes);
 }
 
 static inline dim3 grid_half(const Ctx &c, int L, const MGHost &mg) {
     return grid_n(c, ((mg.maxNx[L] + 1) / 2) * (mg.maxN[L] / (mg.maxNx[L] > 0 ? mg.maxNx[L] : 1)));
 }
-
-void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
-    if (!mg_on) {
-        SS_LAUNCH(PF_SMOOTH_B, c.maxN, k_smooth_c, grid_half(c, 0, mg), TPB, c.st, c.dP, 0, bsel, xsel, 0, 1, gate);
-        SS_LAUNCH(PF_SMOOTH_R, c.maxN, k_smooth_c, grid_half(c, 0, mg), TPB, c.st, c.dP, 0, bsel, xsel, 0, 0, gate);
-        return;
-    }
+static int small_split(const MGHost &mg) {
     small_init();
     int Ls = 0;
     while (Ls < mg.maxlev - 1 && mg.maxN[Ls] > g_small_nodes) Ls++;
+    return Ls;
+}
+
+template <class T>
+static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
+    const int SB = pf<T>(PF_SMOOTH_B), SR = pf<T>(PF_SMOOTH_R);
+    if (!mg_on) {
+        SS_LAUNCH_PDL(SB, c.maxN, k_smooth_c<T>, grid_half(c, 0, mg), TPB, c.st, c.dP, 0, bsel, xsel, 0, 1, gate);
+        SS_LAUNCH_PDL(SR, c.maxN, k_smooth_c<T>, grid_half(c, 0, mg), TPB, c.st, c.dP, 0, bsel, xsel, 0, 0, gate);
+        return;
+    }
+    const int Ls = small_split(mg);
     for (int L = 0; L < Ls; L++) {
-        SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 1, gate);
-        SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 0, gate);
+        SS_LAUNCH_PDL(SB, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 1, gate);
+        SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 0, gate);
         if (L == 0 && g_l0_sweeps > 1) {     // second application on the finest level
-            SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 1, gate);
-            SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
+            SS_LAUNCH_PDL(SB, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 1, gate);
+            SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
         }
         const dim3 gr((mg.maxNx[L] + 31) / 32, c.ninst, mg.maxRows[L + 1]);
-        SS_LAUNCH(PF_RESID_RESTRICT, mg.maxN[L + 1], k_resid_restrict2, gr, dim3(32, 4), c.st, c.dP, L, bsel, xsel, wsel, gate);
+        SS_LAUNCH_PDL(pf<T>(PF_RESID_RESTRICT), mg.maxN[L + 1], k_resid_restrict2<T>, gr, dim3(32, 4), c.st, c.dP, L, bsel,
+                  xsel, wsel, gate);
     }
-    launch_small(c, mg.maxN[Ls], Ls, bsel, xsel, wsel, mg.alpha, gate);
+    launch_small<T>(c, mg.maxN[Ls], Ls, bsel, xsel, wsel, mg.alpha, gate);
     for (int L = Ls - 1; L >= 0; L--) {
-        SS_LAUNCH(PF_PROLONG, mg.maxN[L], k_prolong, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, mg.alpha, gate);
-        SS_LAUNCH(PF_LEVEL_RESID, mg.maxN[L], k_level_resid, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel, gate);
-        SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 1, gate);
-        SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 0, gate);
+        SS_LAUNCH_PDL(pf<T>(PF_PROLONG), mg.maxN[L], k_prolong<T>, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel,
+                  mg.alpha, gate);
+        SS_LAUNCH_PDL(pf<T>(PF_LEVEL_RESID), mg.maxN[L], k_level_resid<T>, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel,
+                  xsel, gate);
+        SS_LAUNCH_PDL(SB, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 1, gate);
+        SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 0, gate);
         if (L == 0 && g_l0_sweeps > 1) {
-            SS_LAUNCH(PF_SMOOTH_B, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 1, gate);
-            SS_LAUNCH(PF_SMOOTH_R, mg.maxN[L], k_smooth_c, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
+            SS_LAUNCH_PDL(SB, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 1, gate);
+            SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
         }
     }
 }
-
-__global__ void k_bicg_v(const DevP *__restrict__ Ps);
-__global__ void k_bicg_x(const DevP *__restrict__ Ps);
-__global__ void k_bicg_rho(const DevP *__restrict__ Ps);
-
-// Time `reps` launches of one kernel of the solve path on the instance's present state
-// (test hook for per-kernel roofline numbers; it overwrites work vectors).  Returns
-// microseconds per launch.
-double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
-    KrylovS ks0{};
-    ks0.active = 1;
-    ks0.maxit = 1 << 30;
-    cudaMemcpy(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice);
-    small_init();
-    int Ls = 0;
-    while (Ls < mg.maxlev - 1 && mg.maxN[Ls] > g_small_nodes) Ls++;
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    auto one = [&]() {
-        switch (which) {
-        case 0: k_bicg_v<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
-        case 1: k_smooth_c<<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 1, 0); break;
-        case 2: k_smooth_c<<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 0, 0); break;
-        case 3: k_resid_restrict2<<<dim3((mg.maxNx[0] + 31) / 32, c.ninst, mg.maxRows[1]), dim3(32, 4), 0, c.st>>>(
-                    c.dP, 0, 2, 4, 1, 0); break;
-        case 4: k_level_resid<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
-        case 5: k_prolong<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 1.0, 0); break;
-        case 6: k_bicg_x<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
-        case 7: launch_small(c, mg.maxN[Ls], Ls, 2, 4, 1, 1.0, 0); break;
-        case 8: vcycle(c, mg, 2, 4, 1, 1, 0); break;
-        case 9: k_copy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 5, 6); break;
-        case 10: k_bicg_rho<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
-        default: break;
-        }
-    };
-    for (int r = 0; r < 3; r++) one();
-    cudaEventRecord(a, c.st);
-    for (int r = 0; r < reps; r++) one();
-    cudaEventRecord(b, c.st);
-    cudaEventSynchronize(b);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    return 1e3 * ms / reps;
+void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
+    vcycle_t<double>(c, mg, bsel, xsel, wsel, mg_on, gate);
 }
 
 // ------------------------------------------------------------------ PCG (semiconductor_3d.c:2182-2210)
-// r = b - A x; z = M r; rz = r.z
+// r = b - A x
+template <class T>
 __global__ void k_pcg_init_r(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    const double *b = P.rhs, *x = P.sol;
-    double *r = P.wk[0];
+    const T *b = PT<T>::rhs(P), *x = PT<T>::sol(P);
+    T *r = PT<T>::wk(P, 0);
+    T *const *A = PT<T>::A0(P);
     SS_GRID_LOOP(k, P.N) {
         const Node a = unidx(k, P.Nx, P.Ny);
-        r[k] = b[k] - stencil_apply<double>(P.A, x, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+        r[k] = b[k] - stencil_apply<T>(A, x, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+    }
+}
+// FP32 start of a PCG solve from x = 0: b = r = (float) rhs
+__global__ void k_pcg32_start(const DevP *__restrict__ Ps) {
+    pdl_entry();
+    const DevP &P = Ps[blockIdx.y];
+    SS_GRID_LOOP(k, P.N) {
+        const float b = (float)P.rhs[k];
+        P.rhs32[k] = b;
+        P.wk32[0][k] = b;
+        P.sol32[k] = 0.f;
     }
 }
 // rz = r.z; mode 0 initial (rz0), mode 1 iteration end (stop test, beta)
+template <class T>
 __global__ void k_pcg_rz(const DevP *__restrict__ Ps, int mode) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (mode && !ks_running(P)) return;
-    const double *r = P.wk[0], *z = P.wk[1];
+    if (mode && !ks_running<T>(P)) return;
+    const T *r = PT<T>::wk(P, 0), *z = PT<T>::wk(P, 1);
     double acc[1] = {0.0};
-    SS_GRID_LOOP(k, P.N) acc[0] += r[k] * z[k];
+    SS_GRID_LOOP(k, P.N) acc[0] += (double)r[k] * (double)z[k];
     if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
-        KrylovS &s = *P.ks;
+        KrylovS &s = *PT<T>::ks(P);
         const double rz = acc[0];
         if (!mode) {
             s.rz = s.rz0 = rz; s.it = 0; s.status = 0;
@@ -793,29 +809,34 @@ __global__ void k_pcg_rz(const DevP *__restrict__ Ps, int mode) {
     }
 }
 // p = z (init) or p = z + be p
+template <class T>
 __global__ void k_pcg_p(const DevP *__restrict__ Ps, int init) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P)) return;
-    const double be = init ? 0.0 : P.ks->be;
-    double *p = P.wk[2];
-    const double *z = P.wk[1];
-    SS_GRID_LOOP(k, P.N) p[k] = z[k] + (init ? 0.0 : be * p[k]);
+    if (!ks_running<T>(P)) return;
+    const T be = init ? T(0) : (T)PT<T>::ks(P)->be;
+    T *p = PT<T>::wk(P, 2);
+    const T *z = PT<T>::wk(P, 1);
+    SS_GRID_LOOP(k, P.N) p[k] = z[k] + (init ? T(0) : be * p[k]);
 }
 // q = A p; pq = p.q; al = rz / pq
+template <class T>
 __global__ void k_pcg_q(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P)) return;
-    const double *p = P.wk[2];
-    double *q = P.wk[3];
+    if (!ks_running<T>(P)) return;
+    const T *p = PT<T>::wk(P, 2);
+    T *q = PT<T>::wk(P, 3);
+    T *const *A = PT<T>::A0(P);
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) {
         const Node a = unidx(k, P.Nx, P.Ny);
-        const double v = stencil_apply<double>(P.A, p, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+        const T v = stencil_apply<T>(A, p, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
         q[k] = v;
-        acc[0] += p[k] * v;
+        acc[0] += (double)p[k] * (double)v;
     }
     if (grid_sum<1>(acc, P.part, P.ticket + 5)) {
-        KrylovS &s = *P.ks;
+        KrylovS &s = *PT<T>::ks(P);
         s.it++;
         const double pq = acc[0];
         if (!(pq > 0.0)) { s.active = 0; s.status = 2; s.al = 0.0; }
@@ -823,144 +844,38 @@ __global__ void k_pcg_q(const DevP *__restrict__ Ps) {
     }
 }
 // x += al p; r -= al q
+template <class T>
 __global__ void k_pcg_xr(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P)) return;
-    const double al = P.ks->al;
-    double *x = P.sol, *r = P.wk[0];
-    const double *p = P.wk[2], *q = P.wk[3];
+    if (!ks_running<T>(P)) return;
+    const T al = (T)PT<T>::ks(P)->al;
+    T *x = PT<T>::sol(P), *r = PT<T>::wk(P, 0);
+    const T *p = PT<T>::wk(P, 2), *q = PT<T>::wk(P, 3);
     SS_GRID_LOOP(k, P.N) { x[k] += al * p[k]; r[k] -= al * q[k]; }
+}
+// sol = (double) sol32 (end of an FP32 solve whose result is the whole solution)
+__global__ void k_sol_from32(const DevP *__restrict__ Ps) {
+    pdl_entry();
+    const DevP &P = Ps[blockIdx.y];
+    SS_GRID_LOOP(k, P.N) P.sol[k] = (double)P.sol32[k];
 }
 
 // one PCG iteration (every kernel gated on the instance's active word)
+template <class T>
 static void pcg_body(const Ctx &c, const MGHost &mg) {
-    SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_pcg_q, grid_nodes(c), TPB, c.st, c.dP);
-    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_xr, grid_nodes(c), TPB, c.st, c.dP);
-    vcycle(c, mg, 0, 1, 0, 1, 1);
-    SS_LAUNCH(PF_KRY_DOT, c.maxN, k_pcg_rz, grid_nodes(c), TPB, c.st, c.dP, 1);
-    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_p, grid_nodes(c), TPB, c.st, c.dP, 0);
-}
-static void bicg_body(const Ctx &c, const MGHost &mg, int mg_on);
-
-// ------------------------------------------------------------------ device-looped solves
-// A Krylov solve runs as one CUDA graph: a conditional WHILE node whose body is one
-// iteration; the body's last kernel sets the loop condition from the instances' active
-// words, so the iteration loop runs on the device with no host round trip.
-__global__ void k_loop_cond(const DevP *__restrict__ Ps, int ninst, cudaGraphConditionalHandle h, int body) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    unsigned any = 0;
-    for (int i = 0; i < ninst; i++) {
-        KrylovS *s = Ps[i].ks;
-        if (body) s->body_runs++;
-        any |= s->active ? 1u : 0u;
-    }
-    cudaGraphSetConditional(h, any);
-}
-
-static bool g_graph_warned = false;
-#define GCK(x)                                                                                     \
-    do {                                                                                           \
-        if ((x) != cudaSuccess) {                                                                  \
-            if (!g_graph_warned)                                                                   \
-                std::fprintf(stderr, "semisim-b200: graph build failed (%s), iterating from the host\n", \
-                             cudaGetErrorString(cudaGetLastError()));                              \
-            g_graph_warned = true;                                                                 \
-            if (g) cudaGraphDestroy(g);                                                            \
-            return nullptr;                                                                        \
-        }                                                                                          \
-    } while (0)
-
-// kind 0: PCG; 1: BiCGSTAB with the multigrid preconditioner; 2: BiCGSTAB, smoother only
-static cudaGraphExec_t build_loop(const Ctx &c, const MGHost &mg, int kind, int *nkern) {
-    cudaGraph_t g = nullptr;
-    GCK(cudaGraphCreate(&g, 0));
-    cudaGraphConditionalHandle h;
-    GCK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    const DevP *dp = c.dP;
-    int ninst = c.ninst, body0 = 0;
-    void *args[] = {(void *)&dp, (void *)&ninst, (void *)&h, (void *)&body0};
-    cudaKernelNodeParams kp = {};
-    kp.func = (void *)k_loop_cond;
-    kp.gridDim = dim3(1);
-    kp.blockDim = dim3(32);
-    kp.kernelParams = args;
-    cudaGraphNode_t n0, cn;
-    GCK(cudaGraphAddKernelNode(&n0, g, nullptr, 0, &kp));
-    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    GCK(cudaGraphAddNode(&cn, g, &n0, 1, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    GCK(cudaStreamBeginCaptureToGraph(c.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    const unsigned long long l0 = t_launches;
-    if (kind == 0) pcg_body(c, mg);
-    else bicg_body(c, mg, kind == 1);
-    k_loop_cond<<<1, 32, 0, c.st>>>(c.dP, c.ninst, h, 1);
-    const unsigned long long nb = t_launches - l0;
-    *nkern = int(nb) + 1;
-    g_launches -= nb;                                  // counted per executed body instead
-    t_launches = l0;
-    cudaGraph_t out = nullptr;
-    GCK(cudaStreamEndCapture(c.st, &out));
-    cudaGraphExec_t ex = nullptr;
-    GCK(cudaGraphInstantiate(&ex, g, 0));
-    cudaGraphDestroy(g);
-    return ex;
-}
-
-bool g_use_graphs = true;
-
-// run the iteration loop of `kind` to completion; returns the final Krylov record
-static KrylovS run_loop(const Ctx &c, const MGHost &mg, int kind, int maxit, int check_every) {
-    KrylovS hs{};
-    LoopGraphs *lg = c.lg;
-    if (lg && g_use_graphs && !g_prof_on && !lg->failed) {
-        if (!lg->exec[kind]) {
-            lg->exec[kind] = build_loop(c, mg, kind, &lg->kernels[kind]);
-            if (!lg->exec[kind]) lg->failed = 1;
-        }
-        if (lg->exec[kind]) {
-            cudaGraphLaunch(lg->exec[kind], c.st);
-            cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
-            cudaStreamSynchronize(c.st);
-            const unsigned long long ran = 1ull + (unsigned long long)lg->kernels[kind] * (unsigned long long)hs.body_runs;
-            g_launches += ran;
-            t_launches += ran;
-            return hs;
-        }
-    }
-    for (int it = 0; it < maxit + 1;) {
-        for (int q = 0; q < check_every && it < maxit + 1; q++, it++) {
-            if (kind == 0) pcg_body(c, mg);
-            else bicg_body(c, mg, kind == 1);
-        }
-        cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
-        cudaStreamSynchronize(c.st);
-        if (!hs.active) break;
-    }
-    return hs;
-}
-
-int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every) {
-    KrylovS ks0{};
-    ks0.active = 1;
-    ks0.maxit = maxit;
-    ks0.rtol = rtol;
-    cudaMemcpyAsync(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
-    mg_setup(c, mg, 0);
-    SS_LAUNCH(PF_KRY_INIT, c.maxN, k_pcg_init_r, grid_nodes(c), TPB, c.st, c.dP);
-    vcycle(c, mg, 0, 1, 0, 1, 0);                  // z = M r
-    SS_LAUNCH(PF_KRY_DOT, c.maxN, k_pcg_rz, grid_nodes(c), TPB, c.st, c.dP, 0);
-    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_pcg_p, grid_nodes(c), TPB, c.st, c.dP, 1);
-    const KrylovS hs = run_loop(c, mg, 0, maxit, check_every);
-    return hs.it;
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_SPMV_DOT), c.maxN, k_pcg_q<T>, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_UPDATE), c.maxN, k_pcg_xr<T>, grid_nodes(c), TPB, c.st, c.dP);
+    vcycle_t<T>(c, mg, 0, 1, 0, 1, 1);
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_DOT), c.maxN, k_pcg_rz<T>, grid_nodes(c), TPB, c.st, c.dP, 1);
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_UPDATE), c.maxN, k_pcg_p<T>, grid_nodes(c), TPB, c.st, c.dP, 0);
 }
 
 // ------------------------------------------------------------------ BiCGSTAB (semiconductor_3d.c:2216-2320)
 // work vectors: 0 r, 1 rh, 2 p, 3 v, 4 ph, 5 sh, 6 t, 7 x0 (start backup)
 // r = b - A x; rh = r; p = v = 0; rr = r.r; fl = sum (sum|A x| + |b|)^2; tgt
 __global__ void k_bicg_init(const DevP *__restrict__ Ps, double rtol, double atol) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     const double *b = P.rhs, *x = P.sol;
     double *r = P.wk[0], *rh = P.wk[1], *p = P.wk[2], *v = P.wk[3];
@@ -992,14 +907,16 @@ __global__ void k_bicg_init(const DevP *__restrict__ Ps, double rtol, double ato
     }
 }
 // rho1 = rh.r; restart on breakdown; be
+template <class T>
 __global__ void k_bicg_rho(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P)) return;
-    const double *r = P.wk[0], *rh = P.wk[1];
+    if (!ks_running<T>(P)) return;
+    const T *r = PT<T>::wk(P, 0), *rh = PT<T>::wk(P, 1);
     double acc[1] = {0.0};
-    SS_GRID_LOOP(k, P.N) acc[0] += rh[k] * r[k];
+    SS_GRID_LOOP(k, P.N) acc[0] += (double)rh[k] * (double)r[k];
     if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
-        KrylovS &s = *P.ks;
+        KrylovS &s = *PT<T>::ks(P);
         if (s.it >= s.maxit) { s.active = 0; s.status = 3; return; }
         s.it++;
         double rho1 = acc[0];
@@ -1015,97 +932,109 @@ __global__ void k_bicg_rho(const DevP *__restrict__ Ps) {
     }
 }
 // p = r + be (p - om v); on a restart rh = r, p = r, v = 0
+template <class T>
 __global__ void k_bicg_p(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P)) return;
-    const KrylovS &s = *P.ks;
-    const double be = s.be, om = s.om;
+    if (!ks_running<T>(P)) return;
+    const KrylovS &s = *PT<T>::ks(P);
+    const T be = (T)s.be, om = (T)s.om;
     const int restart = s.pad0;
-    double *p = P.wk[2], *v = P.wk[3], *rh = P.wk[1];
-    const double *r = P.wk[0];
+    T *p = PT<T>::wk(P, 2), *v = PT<T>::wk(P, 3), *rh = PT<T>::wk(P, 1);
+    const T *r = PT<T>::wk(P, 0);
     SS_GRID_LOOP(k, P.N) {
-        if (restart) { rh[k] = r[k]; p[k] = r[k]; v[k] = 0.0; }
+        if (restart) { rh[k] = r[k]; p[k] = r[k]; v[k] = 0; }
         else p[k] = r[k] + be * (p[k] - om * v[k]);
     }
 }
 // v = A ph; rv = rh.v; al
+template <class T>
 __global__ void k_bicg_v(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P)) return;
-    const double *ph = P.wk[4], *rh = P.wk[1];
-    double *v = P.wk[3];
+    if (!ks_running<T>(P)) return;
+    const T *ph = PT<T>::wk(P, 4), *rh = PT<T>::wk(P, 1);
+    T *v = PT<T>::wk(P, 3);
+    T *const *A = PT<T>::A0(P);
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) {
         const Node a = unidx(k, P.Nx, P.Ny);
-        const double t = stencil_apply<double>(P.A, ph, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+        const T t = stencil_apply<T>(A, ph, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
         v[k] = t;
-        acc[0] += rh[k] * t;
+        acc[0] += (double)rh[k] * (double)t;
     }
     if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
-        KrylovS &s = *P.ks;
+        KrylovS &s = *PT<T>::ks(P);
         if (fabs(acc[0]) < 1e-300) { s.active = 0; s.status = 2; return; }
         s.rv = acc[0];
         s.al = s.rho1 / acc[0];
     }
 }
 // r -= al v; ss = r.r; half-step exit test
+template <class T>
 __global__ void k_bicg_s(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P)) return;
-    const double al = P.ks->al;
-    double *r = P.wk[0];
-    const double *v = P.wk[3];
+    if (!ks_running<T>(P)) return;
+    const T al = (T)PT<T>::ks(P)->al;
+    T *r = PT<T>::wk(P, 0);
+    const T *v = PT<T>::wk(P, 3);
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) {
-        const double t = r[k] - al * v[k];
+        const T t = r[k] - al * v[k];
         r[k] = t;
-        acc[0] += t * t;
+        acc[0] += (double)t * (double)t;
     }
     if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
-        KrylovS &s = *P.ks;
+        KrylovS &s = *PT<T>::ks(P);
         s.ss = acc[0];
         if (sqrt(acc[0]) <= s.tgt) { s.half = 1; s.rr = acc[0]; }
     }
 }
 // t = A sh; tt = t.t; ts = t.r; om
+template <class T>
 __global__ void k_bicg_t(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P) || P.ks->half) return;
-    const double *sh = P.wk[5], *r = P.wk[0];
-    double *t = P.wk[6];
+    if (!ks_running<T>(P) || PT<T>::ks(P)->half) return;
+    const T *sh = PT<T>::wk(P, 5), *r = PT<T>::wk(P, 0);
+    T *t = PT<T>::wk(P, 6);
+    T *const *A = PT<T>::A0(P);
     double acc[2] = {0.0, 0.0};
     SS_GRID_LOOP(k, P.N) {
         const Node a = unidx(k, P.Nx, P.Ny);
-        const double q = stencil_apply<double>(P.A, sh, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
+        const T q = stencil_apply<T>(A, sh, k, a.i, a.j, a.l, P.Nx, P.Ny, P.Nz);
         t[k] = q;
-        acc[0] += q * q;
-        acc[1] += q * r[k];
+        acc[0] += (double)q * (double)q;
+        acc[1] += (double)q * (double)r[k];
     }
     if (grid_sum<2>(acc, P.part, P.ticket + 4)) {
-        KrylovS &s = *P.ks;
+        KrylovS &s = *PT<T>::ks(P);
         s.tt = acc[0]; s.ts = acc[1];
         s.om = acc[0] > 0.0 ? acc[1] / acc[0] : 0.0;
     }
 }
 // x += al ph + om sh; r -= om t; rr = r.r; stop tests (or the half-step x update)
+template <class T>
 __global__ void k_bicg_x(const DevP *__restrict__ Ps) {
+    pdl_entry();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running(P)) return;
-    const KrylovS &s0 = *P.ks;
-    const double al = s0.al, om = s0.om;
+    if (!ks_running<T>(P)) return;
+    const KrylovS &s0 = *PT<T>::ks(P);
+    const T al = (T)s0.al, om = (T)s0.om;
     const int half = s0.half;
-    double *x = P.sol, *r = P.wk[0];
-    const double *ph = P.wk[4], *sh = P.wk[5], *t = P.wk[6];
+    T *x = PT<T>::sol(P), *r = PT<T>::wk(P, 0);
+    const T *ph = PT<T>::wk(P, 4), *sh = PT<T>::wk(P, 5), *t = PT<T>::wk(P, 6);
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) {
         if (half) { x[k] += al * ph[k]; continue; }
         x[k] += al * ph[k] + om * sh[k];
-        const double q = r[k] - om * t[k];
+        const T q = r[k] - om * t[k];
         r[k] = q;
-        acc[0] += q * q;
+        acc[0] += (double)q * (double)q;
     }
     if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
-        KrylovS &s = *P.ks;
+        KrylovS &s = *PT<T>::ks(P);
         if (half) { s.active = 0; s.status = 1; return; }
         s.rr = acc[0];
         const double rn = sqrt(acc[0]);
@@ -1116,38 +1045,433 @@ __global__ void k_bicg_x(const DevP *__restrict__ Ps) {
     }
 }
 
-// One BiCGSTAB solve of P.A sol = rhs from the present sol.  Returns the iterations;
-// rn / r0 the final and initial residual norms.
 // one BiCGSTAB iteration (the continuity systems use the Slotboom-weighted hierarchy)
+template <class T>
 static void bicg_body(const Ctx &c, const MGHost &mg, int mg_on) {
-    SS_LAUNCH(PF_KRY_DOT, c.maxN, k_bicg_rho, grid_nodes(c), TPB, c.st, c.dP);
-    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_p, grid_nodes(c), TPB, c.st, c.dP);
-    vcycle(c, mg, 2, 4, 1, mg_on, 1);            // ph = M p
-    SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_bicg_v, grid_nodes(c), TPB, c.st, c.dP);
-    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_s, grid_nodes(c), TPB, c.st, c.dP);
-    vcycle(c, mg, 0, 5, 1, mg_on, 2);            // sh = M r
-    SS_LAUNCH(PF_KRY_SPMV_DOT, c.maxN, k_bicg_t, grid_nodes(c), TPB, c.st, c.dP);
-    SS_LAUNCH(PF_KRY_UPDATE, c.maxN, k_bicg_x, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_DOT), c.maxN, k_bicg_rho<T>, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_UPDATE), c.maxN, k_bicg_p<T>, grid_nodes(c), TPB, c.st, c.dP);
+    vcycle_t<T>(c, mg, 2, 4, 1, mg_on, 1);          // ph = M p
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_SPMV_DOT), c.maxN, k_bicg_v<T>, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_UPDATE), c.maxN, k_bicg_s<T>, grid_nodes(c), TPB, c.st, c.dP);
+    vcycle_t<T>(c, mg, 0, 5, 1, mg_on, 2);          // sh = M r
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_SPMV_DOT), c.maxN, k_bicg_t<T>, grid_nodes(c), TPB, c.st, c.dP);
+    SS_LAUNCH_PDL(pf<T>(PF_KRY_UPDATE), c.maxN, k_bicg_x<T>, grid_nodes(c), TPB, c.st, c.dP);
+}
+
+// ------------------------------------------------------------------ FP64 iterative refinement
+// The refined continuity solve keeps x (sol) and the residual r = b - A x (wk[0]) in
+// FP64 with the FP64 operator; each step solves A d = r in FP32 (the FP32 copy of A and
+// the FP32 hierarchy, BiCGSTAB from d = 0 to a relative target) and applies x += d,
+// r -= A d in FP64.  The stop rule is the reference's, evaluated on the FP64 residual:
+// |r| <= max(rtol |r0|, atol sqrt(sum_k (sum_j |a_kj x_j| + |b_k|)^2)).
+//
+// start: r = b - A x, r0, the rounding floor and the target (outer record P.ks);
+// rhs32 = (float) r
+__global__ void k_ir_init(const DevP *__restrict__ Ps) {
+    pdl_entry();
+    const DevP &P = Ps[blockIdx.y];
+    const double *b = P.rhs, *x = P.sol;
+    double *r = P.wk[0];
+    const int NxNy = P.Nx * P.Ny;
+    double acc[2] = {0.0, 0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const Node a = unidx(k, P.Nx, P.Ny);
+        const int i = a.i, j = a.j, l = a.l;
+        double s = P.A[0][k] * x[k], fl = fabs(P.A[0][k] * x[k]) + fabs(b[k]), t;
+        if (i > 0) { t = P.A[1][k] * x[k - 1]; s += t; fl += fabs(t); }
+        if (i < P.Nx - 1) { t = P.A[2][k] * x[k + 1]; s += t; fl += fabs(t); }
+        if (j > 0) { t = P.A[3][k] * x[k - P.Nx]; s += t; fl += fabs(t); }
+        if (j < P.Ny - 1) { t = P.A[4][k] * x[k + P.Nx]; s += t; fl += fabs(t); }
+        if (l > 0) { t = P.A[5][k] * x[k - NxNy]; s += t; fl += fabs(t); }
+        if (l < P.Nz - 1) { t = P.A[6][k] * x[k + NxNy]; s += t; fl += fabs(t); }
+        const double rk = b[k] - s;
+        r[k] = rk;
+        P.rhs32[k] = (float)rk;
+        acc[0] += rk * rk;
+        acc[1] += fl * fl;
+    }
+    if (grid_sum<2>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        s.rr = acc[0]; s.fl = acc[1];
+        s.r0 = sqrt(acc[0]);
+        s.tgt = fmax(s.rtol * s.r0, s.atol * sqrt(acc[1]));
+        s.rbest = s.r0; s.stall = 0; s.it = 0; s.half = 0;
+        if (!(s.r0 > s.tgt)) { s.active = 0; s.status = 1; }
+        else { s.active = 1; s.status = 0; }
+    }
+}
+// inner start: d = 0, r = rh = rhs32, p = v = 0; inner target
+// max(rtol_in |r_in|, factor * outer target) with rtol_in = ksi.rtol, factor = ksi.atol
+__global__ void k_ir_inner_init(const DevP *__restrict__ Ps) {
+    pdl_entry();
+    const DevP &P = Ps[blockIdx.y];
+    const KrylovS &so = *P.ks;
+    if (!so.active) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) { P.ksi->active = 0; P.ksi->body_runs = 0; }
+        return;
+    }
+    float *r = P.wk32[0], *rh = P.wk32[1], *p = P.wk32[2], *v = P.wk32[3], *x = P.sol32;
+    const float *b = P.rhs32;
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const float bk = b[k];
+        r[k] = bk; rh[k] = bk; p[k] = 0.f; v[k] = 0.f; x[k] = 0.f;
+        acc[0] += (double)bk * (double)bk;
+    }
+    if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ksi;
+        s.rr = acc[0];
+        s.r0 = sqrt(acc[0]);
+        s.tgt = fmax(s.rtol * s.r0, s.atol * so.tgt);
+        s.rho = s.al = s.om = 1.0; s.rbest = s.r0; s.stall = 0; s.it = 0; s.half = 0; s.body_runs = 0;
+        s.maxit = so.maxit - so.it;
+        s.status = 0;
+        s.active = (s.r0 > s.tgt && s.maxit > 0) ? 1 : 0;
+    }
+}
+// x += d; r -= A d (FP64 operator); rhs32 = (float) r; the outer stop test.  A step
+// that does not halve the residual ends the refinement with status 4 (the FP64 solver
+// takes over from the host).
+__global__ void k_ir_update(const DevP *__restrict__ Ps) {
+    pdl_entry();
+    const DevP &P = Ps[blockIdx.y];
+    if (!P.ks->active) return;
+    const float *d = P.sol32;
+    double *x = P.sol, *r = P.wk[0];
+    const int NxNy = P.Nx * P.Ny;
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const Node a = unidx(k, P.Nx, P.Ny);
+        const int i = a.i, j = a.j, l = a.l;
+        const double dk = (double)d[k];
+        double s = P.A[0][k] * dk;
+        if (i > 0) s += P.A[1][k] * (double)d[k - 1];
+        if (i < P.Nx - 1) s += P.A[2][k] * (double)d[k + 1];
+        if (j > 0) s += P.A[3][k] * (double)d[k - P.Nx];
+        if (j < P.Ny - 1) s += P.A[4][k] * (double)d[k + P.Nx];
+        if (l > 0) s += P.A[5][k] * (double)d[k - NxNy];
+        if (l < P.Nz - 1) s += P.A[6][k] * (double)d[k + NxNy];
+        x[k] += dk;
+        const double rk = r[k] - s;
+        r[k] = rk;
+        P.rhs32[k] = (float)rk;
+        acc[0] += rk * rk;
+    }
+    if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
+        KrylovS &s = *P.ks;
+        s.it += P.ksi->it;
+        s.body_runs++;                                // refinement steps of this solve
+        s.rr = acc[0];
+        const double rn = sqrt(acc[0]);
+        if (rn <= s.tgt) { s.active = 0; s.status = 1; }
+        else if (!(rn < 0.5 * s.rbest)) { s.active = 0; s.status = 4; }
+        else if (s.it >= s.maxit) { s.active = 0; s.status = 3; }
+        else s.rbest = rn;
+    }
+}
+
+// ------------------------------------------------------------------ device-looped solves
+// A Krylov solve runs as one CUDA graph: a conditional WHILE node whose body is one
+// iteration; the body's last kernel sets the loop condition from the instances' active
+// words, so the iteration loop runs on the device with no host round trip.
+__global__ void k_loop_cond(const DevP *__restrict__ Ps, int ninst, cudaGraphConditionalHandle h, int body, int inner) {
+    pdl_entry();
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned any = 0;
+    for (int i = 0; i < ninst; i++) {
+        KrylovS *s = inner ? Ps[i].ksi : Ps[i].ks;
+        if (body) s->body_runs++;
+        any |= s->active ? 1u : 0u;
+    }
+    cudaGraphSetConditional(h, any);
+}
+
+static bool g_graph_warned = false;
+#define GCK(x)                                                                                     \
+    do {                                                                                           \
+        if ((x) != cudaSuccess) {                                                                  \
+            if (!g_graph_warned)                                                                   \
+                std::fprintf(stderr, "semisim-b200: graph build failed (%s), iterating from the host\n", \
+                             cudaGetErrorString(cudaGetLastError()));                              \
+            g_graph_warned = true;                                                                 \
+            if (g) cudaGraphDestroy(g);                                                            \
+            return nullptr;                                                                        \
+        }                                                                                          \
+    } while (0)
+
+static void loop_body(const Ctx &c, const MGHost &mg, int kind) {
+    switch (kind) {
+    case 0: pcg_body<double>(c, mg); break;
+    case 1: bicg_body<double>(c, mg, 1); break;
+    case 2: bicg_body<double>(c, mg, 0); break;
+    case 3: pcg_body<float>(c, mg); break;
+    default: bicg_body<float>(c, mg, 1); break;
+    }
+}
+
+// the graph of `kind` (LoopGraphs); *nkern = kernels of one body pass, *nfix = kernels
+// outside the loop
+static cudaGraphExec_t build_loop(const Ctx &c, const MGHost &mg, int kind, int *nkern, int *nfix) {
+    cudaGraph_t g = nullptr;
+    GCK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    GCK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    const DevP *dp = c.dP;
+    const int inner = kind >= 3 ? 1 : 0;
+    int ninst = c.ninst, body0 = 0;
+    const int nblk = c.nodes_blocks();
+    void *args[] = {(void *)&dp, (void *)&ninst, (void *)&h, (void *)&body0, (void *)&inner};
+    void *args1[] = {(void *)&dp};
+    cudaKernelNodeParams kp = {};
+    cudaGraphNode_t n_init = nullptr, n0, cn, n_upd;
+    int fixed = 1;
+    if (kind == 4) {                                  // refinement step: inner start
+        kp.func = (void *)k_ir_inner_init;
+        kp.gridDim = dim3(nblk, c.ninst);
+        kp.blockDim = dim3(TPB);
+        kp.kernelParams = args1;
+        GCK(cudaGraphAddKernelNode(&n_init, g, nullptr, 0, &kp));
+        fixed++;
+    }
+    kp = {};
+    kp.func = (void *)k_loop_cond;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = args;
+    GCK(cudaGraphAddKernelNode(&n0, g, n_init ? &n_init : nullptr, n_init ? 1 : 0, &kp));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    GCK(cudaGraphAddNode(&cn, g, &n0, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    GCK(cudaStreamBeginCaptureToGraph(c.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const unsigned long long l0 = t_launches;
+    loop_body(c, mg, kind);
+    launch_pdl(k_loop_cond, dim3(1), dim3(32), c.st, c.dP, c.ninst, h, 1, inner);
+    const unsigned long long nb = t_launches - l0;
+    *nkern = int(nb) + 1;
+    g_launches -= nb;                                  // counted per executed body instead
+    t_launches = l0;
+    cudaGraph_t out = nullptr;
+    GCK(cudaStreamEndCapture(c.st, &out));
+    if (kind == 4) {                                  // refinement step: FP64 update
+        kp = {};
+        kp.func = (void *)k_ir_update;
+        kp.gridDim = dim3(nblk, c.ninst);
+        kp.blockDim = dim3(TPB);
+        kp.kernelParams = args1;
+        GCK(cudaGraphAddKernelNode(&n_upd, g, &cn, 1, &kp));
+        fixed++;
+    }
+    *nfix = fixed;
+    cudaGraphExec_t ex = nullptr;
+    GCK(cudaGraphInstantiate(&ex, g, 0));
+    cudaGraphDestroy(g);
+    return ex;
+}
+
+bool g_use_graphs = true;
+
+static KrylovS read_ks(const Ctx &c, const KrylovS *src) {
+    KrylovS hs{};
+    cudaMemcpyAsync(&hs, src, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
+    cudaStreamSynchronize(c.st);
+    return hs;
+}
+
+// Run the iteration loop of `kind` to completion (kind 4: one refinement step); returns
+// the loop's Krylov record (the inner one for the FP32 kinds)
+static KrylovS run_loop(const Ctx &c, const MGHost &mg, int kind, int maxit, int check_every) {
+    const KrylovS *rec = kind >= 3 ? c.h.ksi : c.h.ks;
+    LoopGraphs *lg = c.lg;
+    if (lg && g_use_graphs && !g_prof_on && !lg->failed) {
+        if (!lg->exec[kind]) {
+            int nfix = 1;
+            lg->exec[kind] = build_loop(c, mg, kind, &lg->kernels[kind], &nfix);
+            if (!lg->exec[kind]) lg->failed = 1;
+            else lg->kernels[kind] |= nfix << 16;
+        }
+        if (lg->exec[kind]) {
+            cudaGraphLaunch(lg->exec[kind], c.st);
+            const KrylovS hs = read_ks(c, rec);
+            const unsigned long long body = (unsigned long long)(lg->kernels[kind] & 0xffff);
+            const unsigned long long ran = (unsigned long long)(lg->kernels[kind] >> 16) + body * hs.body_runs;
+            g_launches += ran;
+            t_launches += ran;
+            return hs;
+        }
+    }
+    if (kind == 4) SS_LAUNCH_PDL(PF_KRY_INIT32, c.maxN, k_ir_inner_init, grid_nodes(c), TPB, c.st, c.dP);
+    KrylovS hs{};
+    for (int it = 0; it < maxit + 1;) {
+        if (kind == 4 && it == 0) {
+            hs = read_ks(c, rec);
+            if (!hs.active) break;
+        }
+        for (int q = 0; q < check_every && it < maxit + 1; q++, it++) loop_body(c, mg, kind);
+        hs = read_ks(c, rec);
+        if (!hs.active) break;
+    }
+    if (kind == 4) SS_LAUNCH_PDL(PF_REFINE, c.maxN, k_ir_update, grid_nodes(c), TPB, c.st, c.dP);
+    return hs;
+}
+
+// ------------------------------------------------------------------ solver drivers
+// refinement statistics of the calling thread's solves (steps, FP64 take-overs)
+thread_local long long t_ir_steps = 0, t_ir_fallbacks = 0;
+double g_ir_factor = 0.7;      // inner target as a fraction of the outer target
+double g_ir_rtol_min = 1e-5;   // smallest relative reduction asked of one FP32 solve
+
+// PCG of the Poisson Newton system from sol = 0 (the reference's stop rule r.z <=
+// rtol^2 r0.z0).  mixed: FP32 vectors and hierarchy (the Newton loop's FP64 residual
+// refines it); rtol below 1e-5 and FP32 failures use the FP64 solver.
+int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every, int mixed) {
+    KrylovS ks0{};
+    ks0.active = 1;
+    ks0.maxit = maxit;
+    ks0.rtol = rtol;
+    if (mixed && rtol >= 1e-5) {
+        cudaMemcpyAsync(c.h.ksi, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
+        mg_setup_t<float>(c, mg, 0);
+        SS_LAUNCH_PDL(PF_KRY_INIT32, c.maxN, k_pcg32_start, grid_nodes(c), TPB, c.st, c.dP);
+        vcycle_t<float>(c, mg, 0, 1, 0, 1, 0);
+        SS_LAUNCH_PDL(PF_KRY_DOT32, c.maxN, k_pcg_rz<float>, grid_nodes(c), TPB, c.st, c.dP, 0);
+        SS_LAUNCH_PDL(PF_KRY_UPDATE32, c.maxN, k_pcg_p<float>, grid_nodes(c), TPB, c.st, c.dP, 1);
+        const KrylovS hs = run_loop(c, mg, 3, maxit, check_every);
+        if (hs.status == 1) {
+            SS_LAUNCH_PDL(PF_VEC, c.maxN, k_sol_from32, grid_nodes(c), TPB, c.st, c.dP);
+            return hs.it;
+        }
+        t_ir_fallbacks++;
+        launch_fill_sel(c, V_SOL, 0.0);
+        return hs.it + pcg_solve(c, mg, maxit, rtol, check_every, 0);
+    }
+    cudaMemcpyAsync(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
+    mg_setup_t<double>(c, mg, 0);
+    SS_LAUNCH_PDL(PF_KRY_INIT, c.maxN, k_pcg_init_r<double>, grid_nodes(c), TPB, c.st, c.dP);
+    vcycle_t<double>(c, mg, 0, 1, 0, 1, 0);                  // z = M r
+    SS_LAUNCH_PDL(PF_KRY_DOT, c.maxN, k_pcg_rz<double>, grid_nodes(c), TPB, c.st, c.dP, 0);
+    SS_LAUNCH_PDL(PF_KRY_UPDATE, c.maxN, k_pcg_p<double>, grid_nodes(c), TPB, c.st, c.dP, 1);
+    const KrylovS hs = run_loop(c, mg, 0, maxit, check_every);
+    return hs.it;
+}
+
+// FP64-refined BiCGSTAB with FP32 inner solves (multigrid preconditioner).  A stalled
+// refinement hands the solve to the FP64 solver with the same target.
+static int bicgstab_refined(const Ctx &c, const MGHost &mg, int maxit, double rtol, double atol, int check_every,
+                            double *rn, double *r0, int qsign) {
+    KrylovS ko{}, ki{};
+    ko.maxit = maxit;
+    ko.rtol = rtol;
+    ko.atol = atol;
+    ki.rtol = g_ir_rtol_min;
+    ki.atol = g_ir_factor;
+    cudaMemcpyAsync(c.h.ks, &ko, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
+    cudaMemcpyAsync(c.h.ksi, &ki, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
+    launch_copy_sel(c, 7, V_SOL);                   // start backup
+    mg_setup_t<float>(c, mg, qsign);
+    SS_LAUNCH_PDL(PF_REFINE, c.maxN, k_ir_init, grid_nodes(c), TPB, c.st, c.dP);
+    KrylovS hs{};
+    for (int step = 0; step < 16; step++) {
+        run_loop(c, mg, 4, maxit, check_every);
+        hs = read_ks(c, c.h.ks);
+        t_ir_steps++;
+        if (!hs.active) break;
+    }
+    *r0 = hs.r0;
+    if (hs.status == 1 || hs.status == 3) {
+        *rn = sqrt(hs.rr);
+        return hs.it;
+    }
+    // the refinement stalled: FP64 BiCGSTAB to the same target, from the better of
+    // the start and the refined iterate
+    t_ir_fallbacks++;
+    double rcur = sqrt(hs.rr);
+    if (!(rcur <= hs.r0)) {
+        launch_copy_sel(c, V_SOL, 7);
+        rcur = hs.r0;
+    }
+    const double rt = rcur > 0.0 ? hs.tgt / rcur : rtol;
+    double rn2 = 0, r02 = 0;
+    const int its = bicgstab_core(c, mg, maxit, rt, atol, 1, check_every, &rn2, &r02, qsign, 0);
+    *rn = rn2;
+    return hs.it + its;
 }
 
 // One BiCGSTAB solve of P.A sol = rhs from the present sol.  Returns the iterations;
-// rn / r0 the final and initial residual norms.
+// rn / r0 the final and initial residual norms.  mixed: FP64-refined FP32 solve (with
+// the multigrid preconditioner only; the smoother-only retry stays FP64).
 int bicgstab_core(const Ctx &c, const MGHost &mg, int maxit, double rtol, double atol, int mg_on, int check_every,
-                  double *rn, double *r0, int qsign) {
+                  double *rn, double *r0, int qsign, int mixed) {
+    if (mixed && mg_on && mg.maxlev > 1) return bicgstab_refined(c, mg, maxit, rtol, atol, check_every, rn, r0, qsign);
     KrylovS ks0{};
     ks0.maxit = maxit;
     ks0.rtol = rtol;
     ks0.atol = atol;
     cudaMemcpyAsync(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice, c.st);
-    if (mg_on) mg_setup(c, mg, qsign);
+    if (mg_on) mg_setup_t<double>(c, mg, qsign);
     else {
-        SS_LAUNCH(PF_ILU_DIAG, c.maxN, k_ilu_diag, grid_nodes(c), TPB, c.st, c.dP, 0);
+        SS_LAUNCH_PDL(PF_ILU_DIAG, c.maxN, k_ilu_diag<double>, grid_nodes(c), TPB, c.st, c.dP, 0);
     }
-    SS_LAUNCH(PF_KRY_INIT, c.maxN, k_bicg_init, grid_nodes(c), TPB, c.st, c.dP, rtol, atol);
+    SS_LAUNCH_PDL(PF_KRY_INIT, c.maxN, k_bicg_init, grid_nodes(c), TPB, c.st, c.dP, rtol, atol);
     const KrylovS hs = run_loop(c, mg, mg_on ? 1 : 2, maxit, check_every);
     *rn = sqrt(hs.rr);
     *r0 = hs.r0;
     return hs.it;
+}
+
+// ------------------------------------------------------------------ kernel timing hook
+// Time `reps` launches of one kernel of the solve path on the instance's present state
+// (test hook for per-kernel roofline numbers; it overwrites work vectors).  Returns
+// microseconds per launch.  0-10 FP64, 11-16 the FP32 twins.
+double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
+    KrylovS ks0{};
+    ks0.active = 1;
+    ks0.maxit = 1 << 30;
+    cudaMemcpy(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice);
+    cudaMemcpy(c.h.ksi, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice);
+    const int Ls = small_split(mg);
+    if (which >= 11) {
+        mg_setup_t<float>(c, mg, 1);
+        cudaStreamSynchronize(c.st);
+    }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const dim3 grr((mg.maxNx[0] + 31) / 32, c.ninst, mg.maxRows[1]);
+    auto one = [&]() {
+        switch (which) {
+        case 0: k_bicg_v<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        case 1: k_smooth_c<double><<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 1, 0); break;
+        case 2: k_smooth_c<double><<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 0, 0); break;
+        case 3: k_resid_restrict2<double><<<grr, dim3(32, 4), 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
+        case 4: k_level_resid<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
+        case 5: k_prolong<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 1.0, 0); break;
+        case 6: k_bicg_x<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        case 7: launch_small<double>(c, mg.maxN[Ls], Ls, 2, 4, 1, 1.0, 0); break;
+        case 8: vcycle_t<double>(c, mg, 2, 4, 1, 1, 0); break;
+        case 9: k_copy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 5, 6); break;
+        case 10: k_bicg_rho<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        case 11: k_bicg_v<float><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        case 12: k_smooth_c<float><<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 1, 0); break;
+        case 13: k_smooth_c<float><<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 0, 0); break;
+        case 14: k_resid_restrict2<float><<<grr, dim3(32, 4), 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
+        case 15: vcycle_t<float>(c, mg, 2, 4, 1, 1, 0); break;
+        case 16: k_ir_update<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        default: break;
+        }
+    };
+    for (int r = 0; r < 3; r++) one();
+    cudaEventRecord(a, c.st);
+    for (int r = 0; r < reps; r++) one();
+    cudaEventRecord(b, c.st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return 1e3 * ms / reps;
 }
 
 }  // namespace ss

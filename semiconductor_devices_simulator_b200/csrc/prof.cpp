@@ -39,14 +39,53 @@ const double kProfBytesPerNode[PF_NPROF] = {
     24.0,   // PF_VEC
     24.0,   // PF_CCL
     120.0,  // PF_DISPLAY
+    23.0,   // PF_SMOOTH_B32 (FP32 words: half the FP64 figures)
+    19.0,   // PF_SMOOTH_R32
+    40.0,   // PF_RESID_RESTRICT32
+    12.5,   // PF_PROLONG32
+    40.0,   // PF_LEVEL_RESID32
+    4.0,    // PF_COARSE32
+    40.0,   // PF_GALERKIN32
+    12.0,   // PF_WEIGHTS32
+    32.0,   // PF_ILU_DIAG32
+    4.0,    // PF_COARSE_SETUP32
+    40.0,   // PF_KRY_SPMV_DOT32
+    24.0,   // PF_KRY_UPDATE32
+    8.0,    // PF_KRY_DOT32
+    24.0,   // PF_KRY_INIT32: rhs read; r, rh, p, v, x written
+    92.0,   // PF_REFINE: FP64 A 56 + x, r read and written 32, FP32 correction 4 (FP64 start: 96)
+    96.0,   // PF_CONVERT32: A and row weights 64 read, 32 written
 };
+int pf_f32(int id) {
+    switch (id) {
+    case PF_SMOOTH_B: return PF_SMOOTH_B32;
+    case PF_SMOOTH_R: return PF_SMOOTH_R32;
+    case PF_RESID_RESTRICT: return PF_RESID_RESTRICT32;
+    case PF_PROLONG: return PF_PROLONG32;
+    case PF_LEVEL_RESID: return PF_LEVEL_RESID32;
+    case PF_COARSE: return PF_COARSE32;
+    case PF_GALERKIN: return PF_GALERKIN32;
+    case PF_WEIGHTS: return PF_WEIGHTS32;
+    case PF_ILU_DIAG: return PF_ILU_DIAG32;
+    case PF_COARSE_SETUP: return PF_COARSE_SETUP32;
+    case PF_KRY_SPMV_DOT: return PF_KRY_SPMV_DOT32;
+    case PF_KRY_UPDATE: return PF_KRY_UPDATE32;
+    case PF_KRY_DOT: return PF_KRY_DOT32;
+    case PF_KRY_INIT: return PF_KRY_INIT32;
+    default: return id;
+    }
+}
 const char *kProfName[PF_NPROF] = {
     "poisson_eval", "rebuild_np", "upd_mob", "cont_assemble", "cont_update", "smooth_black", "smooth_red",
     "resid_restrict", "prolong", "level_resid", "coarse_solve", "galerkin", "mg_weights", "ilu_diag",
     "coarse_setup", "krylov_spmv_dot", "krylov_update", "krylov_dot", "krylov_init", "terminal_currents",
-    "anderson", "boundary", "vector", "labelling", "display"};
+    "anderson", "boundary", "vector", "labelling", "display", "smooth_black_f32", "smooth_red_f32",
+    "resid_restrict_f32", "prolong_f32", "level_resid_f32", "coarse_solve_f32", "galerkin_f32", "mg_weights_f32",
+    "ilu_diag_f32", "coarse_setup_f32", "krylov_spmv_dot_f32", "krylov_update_f32", "krylov_dot_f32",
+    "krylov_init_f32", "refine_f64", "convert_f32"};
 
 bool g_prof_on = false;
+bool g_pdl = true;
 std::atomic<unsigned long long> g_launches{0};
 thread_local unsigned long long t_launches = 0;
 

@@ -59,7 +59,8 @@ struct LevelT {
     T *A[7];                     // c, xm, xp, ym, yp, zm, zp
     T *D;                        // red-black D-ILU pivots (or the dense inverse on the last level)
     T *x, *b, *r;
-    double *pw, *ph;             // prolongation weights (to the parent), reference level / VT
+    T *pw;                       // prolongation weights (to the parent)
+    double *ph;                  // reference level / VT of the Slotboom weights (set-up only)
 };
 
 // per-instance Krylov scalars (device resident; written by the reduction finalisers)
@@ -107,6 +108,10 @@ struct DevP {
     int *ffint;                   // floating-block flags / counts / roots: 16 + 1024
     double *res;                  // scalar results (64)
     KrylovS *ks;
+    // FP32 copy of the level-0 system and the FP32 Krylov vectors of the refined solves
+    float *A32[7], *dsc32, *rhs32, *sol32;
+    float *wk32[8];
+    KrylovS *ksi;                 // Krylov record of the FP32 inner solve
     // multigrid (FP64 and FP32 hierarchies)
     LevelT<double> *lev;          // device array of nlev levels
     LevelT<float> *levf;

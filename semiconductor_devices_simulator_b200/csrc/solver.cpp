@@ -46,6 +46,10 @@ int select_device(int dev) {
     return 1;
 }
 
+int g_precision_default = 0;
+
+int use_mixed(const Inst &d) { return (d.precision < 0 ? g_precision_default : d.precision) == 1 ? 1 : 0; }
+
 Ctx make_ctx(Inst &d) {
     if (g_device >= 0) cudaSetDevice(g_device);
     Ctx c;
@@ -78,7 +82,8 @@ struct Carver {
 };
 
 // Lay out every device array of an instance in one block (two passes: size, then place).
-static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &levs, int nlev, const int dims[][6]) {
+static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &levs, std::vector<LevelT<float>> &levsf,
+                  int nlev, const int dims[][6]) {
     const size_t N = d.N;
     P.flags = cv.take<uint32_t>(N);
     P.Nd = cv.take<double>(N); P.Na = cv.take<double>(N); P.Nf = cv.take<double>(N);
@@ -112,16 +117,25 @@ static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &lev
     P.ffint = cv.take<int>(16 + 1024);
     P.res = cv.take<double>(R_TOTAL);
     P.ks = cv.take<KrylovS>(1);
+    P.ksi = cv.take<KrylovS>(1);
+    for (int q = 0; q < 7; q++) P.A32[q] = cv.take<float>(N);
+    P.dsc32 = cv.take<float>(N); P.rhs32 = cv.take<float>(N); P.sol32 = cv.take<float>(N);
+    for (int q = 0; q < 8; q++) P.wk32[q] = cv.take<float>(N);
     P.lev = cv.take<LevelT<double>>(MAXLEV);
-    P.levf = nullptr;
+    P.levf = cv.take<LevelT<float>>(MAXLEV);
     P.ccl = cv.take<int>(N); P.cclaux = cv.take<int>(N);
     levs.assign(nlev, LevelT<double>{});
-    for (int L = 0; L < nlev; L++) {
-        LevelT<double> &v = levs[L];
+    levsf.assign(nlev, LevelT<float>{});
+    // the FP64 hierarchy (plain solves) and its FP32 twin (inner solves of the refined path)
+    auto shape = [&](auto &v, int L) {
         v.Nx = dims[L][0]; v.Ny = dims[L][1]; v.Nz = dims[L][2];
         v.N = v.Nx * v.Ny * v.Nz;
         v.cx = dims[L][3]; v.cy = dims[L][4]; v.cz = dims[L][5];
         v.last = L == nlev - 1;
+    };
+    for (int L = 0; L < nlev; L++) {
+        LevelT<double> &v = levs[L];
+        shape(v, L);
         const size_t n = (size_t)v.N;
         if (L == 0) {
             for (int q = 0; q < 7; q++) v.A[q] = P.A[q];
@@ -134,6 +148,22 @@ static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &lev
         v.r = cv.take<double>(n);
         v.pw = cv.take<double>(n);
         v.ph = cv.take<double>(n);
+    }
+    for (int L = 0; L < nlev; L++) {
+        LevelT<float> &v = levsf[L];
+        shape(v, L);
+        const size_t n = (size_t)v.N;
+        if (L == 0) {
+            for (int q = 0; q < 7; q++) v.A[q] = P.A32[q];
+            v.x = nullptr; v.b = nullptr;
+        } else {
+            for (int q = 0; q < 7; q++) v.A[q] = cv.take<float>(n);
+            v.x = cv.take<float>(n); v.b = cv.take<float>(n);
+        }
+        v.D = cv.take<float>(v.last && L > 0 ? n * n : n);
+        v.r = cv.take<float>(n);
+        v.pw = cv.take<float>(n);
+        v.ph = levs[L].ph;              // set-up scratch, shared with the FP64 twin
     }
 }
 
@@ -188,7 +218,8 @@ static int gpu_alloc(Inst &d) {
     Carver cv;
     DevP P{};
     std::vector<LevelT<double>> levs;
-    carve(d, cv, P, levs, nl, dims);              // sizing pass
+    std::vector<LevelT<float>> levsf;
+    carve(d, cv, P, levs, levsf, nl, dims);       // sizing pass
     const size_t bytes = cv.off;
     void *blk = nullptr;
     CK(cudaMalloc(&blk, bytes));
@@ -196,7 +227,7 @@ static int gpu_alloc(Inst &d) {
     Carver cv2;
     cv2.base = static_cast<char *>(blk);
     P = DevP{};
-    carve(d, cv2, P, levs, nl, dims);
+    carve(d, cv2, P, levs, levsf, nl, dims);
     P.Nx = d.Nx; P.Ny = d.Ny; P.Nz = d.Nz; P.N = (int)d.N; P.nlev = nl;
     d.g.block = blk;
     d.g.bytes = bytes;
@@ -209,6 +240,7 @@ static int gpu_alloc(Inst &d) {
     CK(cudaMalloc(&d.g.scratch, sizeof(double) * (d.N > 0 ? d.N : 1)));
     CK(cudaMalloc(&d.g.flag, sizeof(int) * 16));
     CK(cudaMemcpy(P.lev, levs.data(), sizeof(LevelT<double>) * nl, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.levf, levsf.data(), sizeof(LevelT<float>) * nl, cudaMemcpyHostToDevice));
     MGHost &mg = d.g.mg;
     mg.maxlev = mg.minlev = nl;
     for (int L = 0; L < nl; L++) {
@@ -494,7 +526,8 @@ static int poisson_newton(Inst &d, const double *Va, double ntol, int maxit) {
         const double f0 = read_res(d, R_PNORM);
         if (!(f0 > 0.)) return f0 == 0.;
         launch_fill_sel(c, V_SOL, 0.0);
-        const int its = pcg_solve(c, d.g.mg, d.max_iter_p > 0 ? d.max_iter_p : 2000, d.pcg_rtol, g_knobs.check_every);
+        const int its = pcg_solve(c, d.g.mg, d.max_iter_p > 0 ? d.max_iter_p : 2000, d.pcg_rtol, g_knobs.check_every,
+                                  use_mixed(d));
         d.pcg_its += its;
         launch_absmax_sel(c, V_SOL, R_DMAX);
         const double dm = read_res(d, R_DMAX);
@@ -532,7 +565,11 @@ static int solve_cont(Inst &d, int hole, double lo, double hi, double *dmax) {
     const int maxit = d.max_iter_c > 0 ? d.max_iter_c : 1000;
     launch_copy_sel(c, 7, V_SOL);                        // x0 backup
     double rn = 0, r0 = 0;
-    int its = bicgstab_core(c, d.g.mg, maxit, d.bicg_rtol, atol, 1, g_knobs.check_every, &rn, &r0, hole ? -1 : 1);
+    const long long s0 = t_ir_steps, f0 = t_ir_fallbacks;
+    int its = bicgstab_core(c, d.g.mg, maxit, d.bicg_rtol, atol, 1, g_knobs.check_every, &rn, &r0, hole ? -1 : 1,
+                            use_mixed(d));
+    d.ir_steps += t_ir_steps - s0;
+    d.ir_fallbacks += t_ir_fallbacks - f0;
     if (!(rn <= std::fmax(r0, 1e-300)) && d.g.mg.maxlev > 1) {
         if (d.verbose) std::fprintf(stderr, "semisim-b200: MG-BiCGSTAB diverged (%.2e > %.2e), retry ILU\n", rn, r0);
         launch_copy_sel(c, V_SOL, 7);

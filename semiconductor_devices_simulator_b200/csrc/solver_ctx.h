@@ -79,6 +79,8 @@ struct Inst {
     double Ve1[NC_MAX] = {0}, Ve2[NC_MAX] = {0};
     int e_n = 0;
     int aa_m = 0, aa_n = 0, aa_pos = 0, aa_have = 0;
+    int precision = -1;               // linear solves: 0 FP64, 1 FP32 refined in FP64, -1 library default
+    long long ir_steps = 0, ir_fallbacks = 0;
     // ---- derived by prepare (host copies)
     std::vector<uint32_t> flags;
     std::vector<double> bgn, robA, mu0n, mu0p;
@@ -127,14 +129,19 @@ void rebuild_np(Inst &d);
 void upd_mob(Inst &d);
 void terminal_currents(Inst &d, double *I, double *S);
 Ctx make_ctx(Inst &d);
+int use_mixed(const Inst &d);       // precision of the instance's linear solves (1 = refined FP32)
+extern int g_precision_default;
 void gpu_free(Inst &d);
 
 // linear-algebra drivers (kernels_la.cu)
 void mg_setup(const Ctx &c, const MGHost &mg, int qsign);
 void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate);
-int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every);
+// mixed = 1: FP32 inner solves (FP32 hierarchy and Krylov vectors) refined in FP64
+int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every, int mixed = 0);
 int bicgstab_core(const Ctx &c, const MGHost &mg, int maxit, double rtol, double atol, int mg_on, int check_every,
-                  double *rn, double *r0, int qsign);
+                  double *rn, double *r0, int qsign, int mixed = 0);
+extern thread_local long long t_ir_steps, t_ir_fallbacks;   // refinement steps / FP64 take-overs
+extern double g_ir_factor, g_ir_rtol_min;
 void launch_absmax_sel(const Ctx &c, int xsel, int slot);
 void launch_axpy_sel(const Ctx &c, int ysel, int xsel, double a, int zsel);
 void launch_fill_sel(const Ctx &c, int ysel, double v);

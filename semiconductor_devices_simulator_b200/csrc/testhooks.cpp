@@ -172,7 +172,7 @@ int b200x_bicgstab(int maxit, double rtol, double atol, int qsign, const double 
     Ctx c = make_ctx(d);
     if (x0) cudaMemcpyAsync(d.g.h.sol, x0, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
     else launch_fill_sel(c, V_SOL, 1.0);
-    const int its = bicgstab_core(c, d.g.mg, maxit, rtol, atol, 1, 1, rn, r0, qsign);
+    const int its = bicgstab_core(c, d.g.mg, maxit, rtol, atol, 1, 1, rn, r0, qsign, use_mixed(d));
     if (sol) cudaMemcpyAsync(sol, d.g.h.sol, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
     sync(d);
     return its;
@@ -182,7 +182,7 @@ int b200x_pcg(int maxit, double rtol, double *sol) {
     Inst &d = *dev();
     Ctx c = make_ctx(d);
     launch_fill_sel(c, V_SOL, 0.0);
-    const int its = pcg_solve(c, d.g.mg, maxit, rtol, 1);
+    const int its = pcg_solve(c, d.g.mg, maxit, rtol, 1, use_mixed(d));
     if (sol) cudaMemcpyAsync(sol, d.g.h.sol, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
     sync(d);
     return its;
@@ -223,6 +223,13 @@ double b200x_bench(int which, int reps) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return 1e3 * ms / reps;
+}
+
+// refinement steps and FP64 take-overs of the instance's refined continuity solves
+void b200x_ir_stats(long long *steps, long long *fallbacks) {
+    Inst &d = *dev();
+    *steps = d.ir_steps;
+    *fallbacks = d.ir_fallbacks;
 }
 
 // select the CUDA device of the solver (before its first solve); 1 = done

@@ -2,8 +2,9 @@
 
 Every device kernel runs through the library's b200x_* hooks on the same seeded state
 the golden vectors were dumped at (tests/golden/*.npz, from the reference core), and on
-top of that against the numpy restatement (oracle/restate.py).  FP64 throughout; the
-tolerances are stated per quantity.
+top of that against the numpy restatement (oracle/restate.py).  FP64 throughout, except
+the refined linear solves (FP32 inner solves refined in FP64), which are held to the
+reference's FP64 stop rule; the tolerances are stated per quantity.
 """
 import os
 import sys
@@ -203,3 +204,69 @@ def test_pcg_solves_poisson(lib, name):
     res = np.linalg.norm(g["pois_F"] - R.matvec(A, dims, sol))
     assert its < 100
     assert res <= 1e-5 * np.linalg.norm(g["pois_F"]), (res, its)
+
+
+@pytest.fixture
+def refined(lib):
+    old = lib.api3b_set_precision(1)
+    yield
+    lib.api3b_set_precision(old)
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("hole", [0, 1])
+@pytest.mark.parametrize("rtol", [1e-4, 1e-10])
+def test_refined_bicgstab_meets_fp64_stop_rule(lib, refined, name, hole, rtol):
+    """FP32 Krylov / multigrid inner solves refined in FP64: the FP64 residual of the
+    result meets the reference's FP64 rule ||b - A x|| <= max(rtol ||r0||, atol floor),
+    also far below FP32 round-off (rtol 1e-10)."""
+    g, w = setup(lib, name)
+    N = w.N
+    t = "p" if hole else "n"
+    load_state(lib, g, "pert_")
+    lib.b200x_cont_assemble(hole, None, None, None, None)
+    sol = np.zeros(N); rn = np.zeros(1); r0 = np.zeros(1)
+    atol = 2e-14
+    s0, f0 = ir_stats(lib)
+    its = lib.b200x_bicgstab(1000, rtol, atol, -1 if hole else 1, None, dptr(sol), dptr(rn), dptr(r0))
+    A, b = g[f"cont{t}_A"], g[f"cont{t}_rhs"]
+    dims = tuple(int(v) for v in g["dims"])
+    res = np.linalg.norm(b - R.matvec(A, dims, sol))
+    r00 = np.linalg.norm(b - R.matvec(A, dims, np.ones(N)))
+    tgt = max(rtol * r00, atol * R.bicg_floor(A, dims, b, np.ones(N)))
+    assert its < 400
+    assert res <= 1.5 * tgt + 1e-300, (res, tgt, its)
+    close(r0[0], r00, 1e-9, what="initial residual")
+
+
+def ir_stats(lib):
+    from ctypes import c_longlong, byref
+    a, b = c_longlong(0), c_longlong(0)
+    lib.b200x_ir_stats(byref(a), byref(b))
+    return a.value, b.value
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_refined_pcg_matches_fp64(lib, refined, name):
+    """FP32 PCG (the Newton-Poisson correction; the Newton loop's FP64 residual refines
+    it) reaches the same relative stop rule as the FP64 solve, and its correction agrees
+    with the FP64 one to that tolerance."""
+    g, w = setup(lib, name)
+    N = w.N
+    load_state(lib, g, "pert_")
+    F = np.zeros(N)
+    lib.b200x_poisson(dptr(np.ascontiguousarray(g["pert_phi"])), dptr(F), None, None)
+    sol32 = np.zeros(N)
+    its32 = lib.b200x_pcg(2000, 1e-5, dptr(sol32))
+    lib.api3b_set_precision(0)
+    sol64 = np.zeros(N)
+    its64 = lib.b200x_pcg(2000, 1e-5, dptr(sol64))
+    lib.api3b_set_precision(1)
+    A = g["pois_A"]
+    dims = tuple(int(v) for v in g["dims"])
+    nF = np.linalg.norm(g["pois_F"])
+    res32 = np.linalg.norm(g["pois_F"] - R.matvec(A, dims, sol32))
+    res64 = np.linalg.norm(g["pois_F"] - R.matvec(A, dims, sol64))
+    assert its32 <= its64 + 3, (its32, its64)
+    assert res32 <= 1e-3 * nF and res64 <= 1e-3 * nF, (res32, res64, nF)
+    assert np.abs(sol32 - sol64).max() <= 1e-3 * np.abs(sol64).max()

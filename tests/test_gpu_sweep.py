@@ -67,14 +67,24 @@ def check_currents(I, rI, rF):
     assert not bad.any(), f"currents differ: worst {err[bad].max():.3e} vs tol {tol[bad].min():.3e}\n{I}\n{rI}"
 
 
+@pytest.fixture(params=[0, 1], ids=["fp64", "refined"])
+def prec(request, lib):
+    """Linear-solve precision of the instance: 0 FP64 throughout, 1 FP32 inner solves
+    refined in FP64 to the same stop rule."""
+    old = lib.api3b_set_precision(request.param)
+    yield request.param
+    lib.api3b_set_precision(old)
+
+
 @pytest.mark.parametrize("name", NAMES)
-def test_small_sweeps_tight_match_reference(lib, name, monkeypatch):
+def test_small_sweeps_tight_match_reference(lib, name, prec, monkeypatch):
     """Both codes converged to the discrete solution (inner solves to round-off, Gummel
     tolerance 1e-12 V): every target holds on every node and terminal."""
     g = golden(name)
     for k, v in MG.TIGHT_ENV.items():
         monkeypatch.setenv(k, v)                 # read by api3_init, as the reference reads them
     w, mat, bias = MG.build(lib, name)
+    assert lib.api3b_get_precision() == prec
     lib.api3_set_solver(*MG.TIGHT_SOLVER)
     s = w.sweeps[0]
     ok0, V, I, F, conv, psi, n, p = sweep_fields(lib, w, s)
@@ -85,7 +95,7 @@ def test_small_sweeps_tight_match_reference(lib, name, monkeypatch):
 
 
 @pytest.mark.parametrize("name", NAMES)
-def test_small_sweeps_default_match_reference(lib, name):
+def test_small_sweeps_default_match_reference(lib, name, prec):
     """Production tolerances (the GUI's solver tuple).  The reference then converges
     the quasi-Fermi level of a carrier only where it is >= 1e-3 of the local charge
     scale (its Gummel weight, semiconductor_3d.c:3136-3144), and its terminal currents
@@ -93,6 +103,7 @@ def test_small_sweeps_default_match_reference(lib, name):
     differ by the reference's own distance to its converged value."""
     g = golden(name)
     w, mat, bias = MG.build(lib, name)
+    assert lib.api3b_get_precision() == prec
     s = w.sweeps[0]
     ok0, V, I, F, conv, psi, n, p = sweep_fields(lib, w, s)
     assert ok0 and conv.all()
