@@ -11,7 +11,10 @@ A step is the workload's two Id-Vg sweeps (24 resolved bias points each after th
 which api3_solve solves) through the library's C ABI (api3_set_contact_V + api3_resolve
 per point, the way main.py's run_sweep drives it), the two sweeps solved concurrently by
 two solver instances (api3b_new / api3b_use), each on its own host thread and CUDA
-stream.  Bias points/s = converged points / time of the step (the slower stream's
+stream.  The solver runs refined (FP32 Krylov / multigrid inner solves inside FP64
+iterative refinement, api3b_set_precision(1)); the plain FP64 GPU path is timed on the
+same steps beside it, and the refined currents are compared with the FP64 ones and with
+the reference core's.  Bias points/s = converged points / time of the step (the slower stream's
 CUDA-event time);
 device set-up and the equilibrium + ramp to the first point (api3_solve) are outside
 the timed region, as the metric defines.  `value` reads only the terminal currents per
@@ -40,7 +43,7 @@ sys.path.insert(0, ROOT)
 
 from semiconductor_devices_simulator_b200 import abi, devices as D  # noqa: E402
 
-METRIC = "I-V bias points/s (n-MOSFET Id-Vg sweep, FP64 solve, dI/I<=1e-4)"
+METRIC = "I-V bias points/s on 1 B200 (refined+batched+learned vs plain FP64), dI/I<=1e-4"
 UNIT = "bias points/s"
 
 
@@ -51,6 +54,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--mesh", default="120,80,60")
+    ap.add_argument("--precision", default="refined", choices=["refined", "fp64"],
+                    help="linear solves: FP32 refined in FP64 (default) or FP64 throughout")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bounded CPU-baseline sample (s)")
     ap.add_argument("--no-profile", action="store_true")
@@ -67,6 +73,7 @@ def run_probe(a):
     mesh = tuple(int(v) for v in a.mesh.split(","))
     lib = S.load()
     w = build(lib, mesh)
+    lib.api3b_set_precision(1 if a.precision == "refined" else 0)
     s = w.sweeps[1]
     for cid, vv in D.bias_vector(w, s, 0.6).items():
         lib.api3_set_contact_V(cid, vv)
@@ -77,6 +84,7 @@ def run_probe(a):
     rn, r0 = np.zeros(1), np.zeros(1)
     its = lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
     print(json.dumps({"probe": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]} electron continuity", "nodes": w.N,
+                      "precision": a.precision,
                       "bicgstab_its": its, "r0": r0[0], "rn": rn[0],
                       "launches": int(lib.b200x_launches() - l0)}))
 
@@ -168,9 +176,10 @@ def build(lib, mesh):
     return D.nmosfet(lib, n=mesh)
 
 
-def sweep_points(lib, w, s, fields=False, npts=None):
+def sweep_points(lib, w, s, fields=False, npts=None, out=None):
     """Timed part of one step: every point of the sweep after the first (or the next
-    npts); the first point is the one api3_solve already solved."""
+    npts); the first point is the one api3_solve already solved.  `out` collects the
+    terminal currents and round-off floors of every point."""
     nc = lib.api3_get_ncon()
     V = s["V"][1:] if npts is None else s["V"][1:1 + npts]
     conv = 0
@@ -179,12 +188,19 @@ def sweep_points(lib, w, s, fields=False, npts=None):
         for cid, vv in D.bias_vector(w, s, v).items():
             lib.api3_set_contact_V(cid, vv)
         conv += int(lib.api3_resolve())
-        for c in range(nc):
-            lib.api3_get_contact_I(c)
+        I = [lib.api3_get_contact_I(c) for c in range(nc)]
+        if out is not None:
+            out.append((I, [lib.api3_get_contact_Ifloor(c) for c in range(nc)]))
         if fields:
             for q, which in enumerate((0, 1, 2)):
                 lib.api3_bulk_copy(which, abi.dptr(bufs[q]))
     return len(V), conv
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a kernel class on
+# the default 120x80x60 mesh, from one ncu capture (profiles/vcycle_f32_kernels_nmosfet_120x80x60.md:
+# the launch mix of one V-cycle weighted by its level-0/1/2 passes)
+NCU_TRAFFIC = {"smooth_black_f32": 10.9e6}
 
 
 def peaks():
@@ -210,10 +226,13 @@ def cpu_baseline(mesh, seconds):
     D.start_sweep(ref, w, s)
     t0 = time.perf_counter()
     n = 0
+    cur = []
+    nc = ref.api3_get_ncon()
     for v in s["V"][1:]:
         for cid, vv in D.bias_vector(w, s, v).items():
             ref.api3_set_contact_V(cid, vv)
         ref.api3_resolve()
+        cur.append(([ref.api3_get_contact_I(c) for c in range(nc)], [ref.api3_get_contact_Ifloor(c) for c in range(nc)]))
         n += 1
         if time.perf_counter() - t0 > seconds:
             break
@@ -221,17 +240,19 @@ def cpu_baseline(mesh, seconds):
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": f"first {n} resolves of the Vd=1.0 V Id-Vg sweep, {mesh[0]}x{mesh[1]}x{mesh[2]} mesh, "
                       f"reference core semiconductor_3d.c built from source (-O3 -fopenmp), {cores} threads, "
-                      f"{dt:.1f} s"}
+                      f"{dt:.1f} s"}, cur
 
 
 class Sweeper:
     """One solver instance on its own host thread and CUDA stream, solving one sweep."""
 
-    def __init__(self, lib, mesh, sweep_index, dev):
+    def __init__(self, lib, mesh, sweep_index, dev, precision):
         self.lib, self.mesh, self.si = lib, mesh, sweep_index
         self.h = lib.api3b_new()
         self.dev = dev
         self.w = None
+        self.precision = precision
+        self.cur = []
 
     def _use(self):
         self.lib.api3b_use(self.h)
@@ -239,6 +260,7 @@ class Sweeper:
 
     def prepare(self):
         self._use()
+        self.lib.api3b_set_precision(self.precision)
         if self.w is None:
             self.w = build(self.lib, self.mesh)
             self.lib.api3_set_verbose(0)
@@ -248,7 +270,8 @@ class Sweeper:
         self._use()
         self.lib.b200x_stream_timer(0)
         t0 = time.perf_counter()
-        self.npts, self.conv = sweep_points(self.lib, self.w, self.w.sweeps[self.si], fields=fields)
+        self.cur = []
+        self.npts, self.conv = sweep_points(self.lib, self.w, self.w.sweeps[self.si], fields=fields, out=self.cur)
         self.dev_s = self.lib.b200x_stream_timer(1) / 1e3
         self.wall = time.perf_counter() - t0
 
@@ -261,26 +284,40 @@ def concurrent(workers, fn):
         t.join()
 
 
+def rel_dI(cur, ref):
+    """Largest |I - I_ref| / |I_ref| over the points both lists hold, on terminals whose
+    reference current is above its own round-off floor (and above 1e-30 A)."""
+    worst = 0.0
+    for (I, _), (Ir, Fr) in zip(cur, ref):
+        for x, y, f in zip(I, Ir, Fr):
+            if abs(y) > max(f, 1e-30):
+                worst = max(worst, abs(x - y) / abs(y))
+    return worst
+
+
 def run_b200(a, dist):
     import semiconductor_devices_simulator_b200 as S
     mesh = tuple(int(v) for v in a.mesh.split(","))
     lib = S.load()
     lib.b200x_set_device(dist.local)
     nsw = 2                                   # the two drain biases of the workload
-    workers = [Sweeper(lib, mesh, (q + dist.rank) % nsw, dist.local) for q in range(nsw)]
-    w = None
+    prec = 1 if a.precision == "refined" else 0
 
-    def step(i, fields=False, timed=True):
+    def make(p):
+        return [Sweeper(lib, mesh, (q + dist.rank) % nsw, dist.local, p) for q in range(nsw)]
+    workers = make(prec)
+
+    def step(ws, fields=False):
         """Both sweeps, concurrently (one instance, thread and stream each)."""
-        concurrent(workers, lambda s: s.prepare())
+        concurrent(ws, lambda s: s.prepare())
         dist.barrier()
         t0 = time.perf_counter()
-        concurrent(workers, lambda s: s.run(fields))
+        concurrent(ws, lambda s: s.run(fields))
         wall = time.perf_counter() - t0
-        return (sum(s.npts for s in workers), sum(s.conv for s in workers), max(s.dev_s for s in workers), wall)
+        return (sum(s.npts for s in ws), sum(s.conv for s in ws), max(s.dev_s for s in ws), wall)
 
     for i in range(a.warmup):
-        step(i)
+        step(workers)
     w = workers[0].w
     clocks = Clocks(dist.local)
     clocks.start()
@@ -288,15 +325,16 @@ def run_b200(a, dist):
     tot_pts = tot_conv = 0
     tot_dev = tot_wall = 0.0
     for i in range(a.steps):
-        npts, conv, dev_s, wall = step(a.warmup + i)
+        npts, conv, dev_s, wall = step(workers)
         tot_pts += npts; tot_conv += conv; tot_dev += dev_s; tot_wall += wall
     launches = int(lib.b200x_launches() - l0)
     clk = clocks.stop()
+    cur = {s.si: list(s.cur) for s in workers}
     # e2e: the same steps with every point's psi, n, p copied to host buffers
     e_pts = 0
     e_wall = 0.0
     for i in range(0 if a.no_e2e else a.steps):
-        npts, conv, dev_s, wall = step(a.warmup + i, fields=True)
+        npts, conv, dev_s, wall = step(workers, fields=True)
         e_pts += npts; e_wall += wall
     if a.no_e2e:
         e_pts, e_wall = tot_pts, tot_wall
@@ -314,6 +352,18 @@ def run_b200(a, dist):
             lib.b200x_prof_read(k, abi.dptr(ms), abi.dptr(cnt), abi.dptr(by))
             rows.append((lib.b200x_prof_name(k).decode(), float(ms[0]), int(cnt[0]), float(by[0])))
         prof = rows
+    # the plain FP64 GPU path on the same steps (own instances, one warm-up step)
+    f64 = None
+    if prec == 1 and not a.no_fp64:
+        w64 = make(0)
+        step(w64)
+        f_pts = 0
+        f_dev = 0.0
+        for i in range(a.steps):
+            npts, conv, dev_s, wall = step(w64)
+            f_pts += npts; f_dev += dev_s
+        cur64 = {s.si: list(s.cur) for s in w64}
+        f64 = (dist.sum(f_pts), dist.max(f_dev), max(rel_dI(cur[k], cur64[k]) for k in cur))
     T = dist.max(tot_dev)
     pts_all = dist.sum(tot_pts)
     e_T = dist.max(e_wall)
@@ -327,8 +377,9 @@ def run_b200(a, dist):
             tot_ms = sum(r[1] for r in prof) or 1.0
             top = max(prof, key=lambda r: r[1])
             ach = top[3] / (top[1] / 1e3) / 1e9 if top[1] > 0 else 0.0
+            traffic = NCU_TRAFFIC.get(top[0]) if mesh == (120, 80, 60) else None
             roof = {"bound": "hbm", "kernel": top[0], "achieved": round(ach, 1), "peak": hbm,
-                    "peak_kind": pk_kind, "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": None,
+                    "peak_kind": pk_kind, "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": traffic,
                     "launches": top[2], "avg_launch_us": round(1e3 * top[1] / max(top[2], 1), 2),
                     "bytes_per_launch": round(top[3] / max(top[2], 1))}
             kernels = {r[0]: {"ms": round(r[1], 2), "share": round(r[1] / tot_ms, 4), "launches": r[2],
@@ -337,14 +388,17 @@ def run_b200(a, dist):
         h2d = 8 * 4 * len(w.contacts)                              # contact voltages per point
         d2h = 3 * 8 * w.N + 16 * len(w.contacts)                   # psi, n, p + currents per point
         npts_step = (len(w.sweeps[0]["V"]) - 1) * nsw
+        value = pts_all / T
         out = {
-            "metric": METRIC, "value": round(pts_all / T, 4), "unit": UNIT, "n_gpus": dist.world,
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * T / a.steps, 2),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner solves refined in f64 (f64 residuals, physics, currents)" if prec else "f64",
             "data": "synthetic (device built from the workload definition)",
             "config": {"workload": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]}_idvg",
                        "nodes": w.N, "points_per_step": npts_step, "drain_biases_V": [0.05, 1.0],
                        "gate_sweep_V": [0.0, 1.2, 0.05], "models": 4, "solver": list(D.GUI_SOLVER),
+                       "precision": a.precision,
                        "parallelism": f"replicas{dist.world}, {nsw} concurrent sweeps per GPU (instance + stream each)",
                        "l2": "state of 576k nodes (~0.5 GB) exceeds the 126 MB L2; no flush"},
             "converged_points": tot_conv, "wall_s": round(tot_wall, 3),
@@ -355,8 +409,16 @@ def run_b200(a, dist):
             "kernels": kernels,
             "clocks": clk,
         }
+        if f64:
+            out["plain_fp64"] = {"value": round(f64[0] / f64[1], 4), "unit": UNIT,
+                                 "speedup": round(value / (f64[0] / f64[1]), 3),
+                                 "max_rel_dI_vs_fp64": f64[2]}
         if dist.world == 1 and not a.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_baseline(mesh, a.cpu_seconds)
+            cb = cpu_baseline(mesh, a.cpu_seconds)
+            if cb:
+                cb, rcur = cb
+                out["cpu_baseline"] = cb
+                out["max_rel_dI_vs_reference"] = rel_dI(cur[1], rcur)
     return out
 
 

@@ -440,8 +440,8 @@ static void mg_setup_t(const Ctx &c, const MGHost &mg, int qsign) {
         SS_LAUNCH_PDL(PF_CONVERT32, c.maxN, k_to32, grid_nodes(c), TPB, c.st, c.dP, qsign != 0);
     for (int L = 0; L < mg.maxlev - 1; L++) {
         const int nc = mg.maxN[L + 1];
-        SS_LAUNCH_PDL(pf<T>(PF_WEIGHTS), nc, k_mg_weights<T>, grid_n(c, nc), TPB, c.st, c.dP, L, qsign);
-        SS_LAUNCH_PDL(pf<T>(PF_GALERKIN), nc, k_galerkin<T>, grid_n(c, nc), TPB, c.st, c.dP, L, qsign != 0);
+        SS_LAUNCH_PDL(pf<T>(PF_WEIGHTS), mg.maxN[L], k_mg_weights<T>, grid_n(c, nc), TPB, c.st, c.dP, L, qsign);
+        SS_LAUNCH_PDL(pf<T>(PF_GALERKIN), mg.maxN[L], k_galerkin<T>, grid_n(c, nc), TPB, c.st, c.dP, L, qsign != 0);
         SS_LAUNCH_PDL(pf<T>(PF_ILU_DIAG), mg.maxN[L], k_ilu_diag<T>, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L);
     }
     for (int L = 1; L < mg.maxlev; L++)
@@ -739,7 +739,7 @@ static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wse
             SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
         }
         const dim3 gr((mg.maxNx[L] + 31) / 32, c.ninst, mg.maxRows[L + 1]);
-        SS_LAUNCH_PDL(pf<T>(PF_RESID_RESTRICT), mg.maxN[L + 1], k_resid_restrict2<T>, gr, dim3(32, 4), c.st, c.dP, L, bsel,
+        SS_LAUNCH_PDL(pf<T>(PF_RESID_RESTRICT), mg.maxN[L], k_resid_restrict2<T>, gr, dim3(32, 4), c.st, c.dP, L, bsel,
                   xsel, wsel, gate);
     }
     launch_small<T>(c, mg.maxN[Ls], Ls, bsel, xsel, wsel, mg.alpha, gate);
