@@ -100,49 +100,22 @@ __device__ __forceinline__ T stencil_apply(T *const *A, const T *x, int k, int i
     if (l < Nz - 1) s += A[6][k] * x[k + NxNy];
     return s;
 }
-// sum over the off-diagonal couplings only
-template <class T>
-__device__ __forceinline__ T offdiag_apply(T *const *A, const T *x, int k, int i, int j, int l, int Nx, int Ny, int Nz) {
-    const int NxNy = Nx * Ny;
-    T s = 0;
-    if (i > 0) s += A[1][k] * x[k - 1];
-    if (i < Nx - 1) s += A[2][k] * x[k + 1];
-    if (j > 0) s += A[3][k] * x[k - Nx];
-    if (j < Ny - 1) s += A[4][k] * x[k + Nx];
-    if (l > 0) s += A[5][k] * x[k - NxNy];
-    if (l < Nz - 1) s += A[6][k] * x[k + NxNy];
-    return s;
-}
-// sum of a_kj x_j / D_j over the neighbours (forward sweep of the black rows)
-template <class T>
-__device__ __forceinline__ T offdiag_apply_div(T *const *A, const T *x, const T *D, int k, int i, int j, int l, int Nx,
-                                               int Ny, int Nz) {
-    const int NxNy = Nx * Ny;
-    T s = 0;
-    if (i > 0) s += A[1][k] * x[k - 1] / D[k - 1];
-    if (i < Nx - 1) s += A[2][k] * x[k + 1] / D[k + 1];
-    if (j > 0) s += A[3][k] * x[k - Nx] / D[k - Nx];
-    if (j < Ny - 1) s += A[4][k] * x[k + Nx] / D[k + Nx];
-    if (l > 0) s += A[5][k] * x[k - NxNy] / D[k - NxNy];
-    if (l < Nz - 1) s += A[6][k] * x[k + NxNy] / D[k + NxNy];
-    return s;
-}
-
 // ------------------------------------------------------------------ multigrid levels
 // level accessors: level 0 reads the instance's system arrays and the caller's vectors
 template <class T>
 struct LevView {
-    T *A[7];
-    T *D, *x, *b, *r, *pw;
+    const T *A;                  // coupling q of node k at A[q * ap + k] (q: c, xm, xp, ym, yp, zm, zp)
+    T *D, *x, *b, *r, *pw;       // D: reciprocal smoother pivots
     double *ph;
-    int Nx, Ny, Nz, N, cx, cy, cz, last;
+    int ap, Nx, Ny, Nz, N, cx, cy, cz, last;
+    __device__ __forceinline__ T a(int q, int k) const { return A[q * ap + k]; }
 };
 template <class T>
 __device__ __forceinline__ LevView<T> levview(const DevP &P, int L, int bsel, int xsel) {
     const LevelT<T> &lv = PT<T>::lev(P, L);
     LevView<T> v;
-#pragma unroll
-    for (int q = 0; q < 7; q++) v.A[q] = lv.A[q];
+    v.A = lv.A[0];
+    v.ap = lv.apitch;
     v.D = lv.D; v.r = lv.r; v.pw = lv.pw; v.ph = lv.ph;
     v.x = L == 0 ? vsel<T>(P, xsel) : lv.x;
     v.b = L == 0 ? vsel<T>(P, bsel) : lv.b;
@@ -150,6 +123,47 @@ __device__ __forceinline__ LevView<T> levview(const DevP &P, int L, int bsel, in
     v.cx = lv.cx; v.cy = lv.cy; v.cz = lv.cz; v.last = lv.last;
     return v;
 }
+// y = A x at node k = (i, j, l) of a level
+template <class T>
+__device__ __forceinline__ T lv_apply(const LevView<T> &v, const T *x, int k, int i, int j, int l) {
+    const int NxNy = v.Nx * v.Ny;
+    T s = v.a(0, k) * x[k];
+    if (i > 0) s += v.a(1, k) * x[k - 1];
+    if (i < v.Nx - 1) s += v.a(2, k) * x[k + 1];
+    if (j > 0) s += v.a(3, k) * x[k - v.Nx];
+    if (j < v.Ny - 1) s += v.a(4, k) * x[k + v.Nx];
+    if (l > 0) s += v.a(5, k) * x[k - NxNy];
+    if (l < v.Nz - 1) s += v.a(6, k) * x[k + NxNy];
+    return s;
+}
+// sum over the off-diagonal couplings only
+template <class T>
+__device__ __forceinline__ T lv_offdiag(const LevView<T> &v, const T *x, int k, int i, int j, int l) {
+    const int NxNy = v.Nx * v.Ny;
+    T s = 0;
+    if (i > 0) s += v.a(1, k) * x[k - 1];
+    if (i < v.Nx - 1) s += v.a(2, k) * x[k + 1];
+    if (j > 0) s += v.a(3, k) * x[k - v.Nx];
+    if (j < v.Ny - 1) s += v.a(4, k) * x[k + v.Nx];
+    if (l > 0) s += v.a(5, k) * x[k - NxNy];
+    if (l < v.Nz - 1) s += v.a(6, k) * x[k + NxNy];
+    return s;
+}
+// sum of a_kj x_j / D_j over the neighbours (forward sweep of the black rows), with the
+// reciprocal pivots
+template <class T>
+__device__ __forceinline__ T lv_offdiag_scaled(const LevView<T> &v, const T *x, int k, int i, int j, int l) {
+    const int NxNy = v.Nx * v.Ny;
+    T s = 0;
+    if (i > 0) s += v.a(1, k) * (x[k - 1] * v.D[k - 1]);
+    if (i < v.Nx - 1) s += v.a(2, k) * (x[k + 1] * v.D[k + 1]);
+    if (j > 0) s += v.a(3, k) * (x[k - v.Nx] * v.D[k - v.Nx]);
+    if (j < v.Ny - 1) s += v.a(4, k) * (x[k + v.Nx] * v.D[k + v.Nx]);
+    if (l > 0) s += v.a(5, k) * (x[k - NxNy] * v.D[k - NxNy]);
+    if (l < v.Nz - 1) s += v.a(6, k) * (x[k + NxNy] * v.D[k + NxNy]);
+    return s;
+}
+
 template <class T>
 __device__ __forceinline__ bool ks_running(const DevP &P) { return PT<T>::ks(P)->active != 0; }
 // gate 0: always run; 1: only while the instance's Krylov loop (of precision T) is
@@ -171,22 +185,22 @@ __global__ void k_ilu_diag(const DevP *__restrict__ Ps, int L) {
     const LevView<T> v = levview<T>(P, L, 0, 0);
     SS_GRID_LOOP(k, v.N) {
         const Node a = unidx(k, v.Nx, v.Ny);
-        const T c = v.A[0][k];
+        const T c = v.a(0, k);
         T d = c;
         if ((a.i + a.j + a.l) & 1) {
             const int NxNy = v.Nx * v.Ny;
             T s = 0;
-            if (a.i > 0) s += v.A[1][k] * v.A[2][k - 1] / v.A[0][k - 1];
-            if (a.i < v.Nx - 1) s += v.A[2][k] * v.A[1][k + 1] / v.A[0][k + 1];
-            if (a.j > 0) s += v.A[3][k] * v.A[4][k - v.Nx] / v.A[0][k - v.Nx];
-            if (a.j < v.Ny - 1) s += v.A[4][k] * v.A[3][k + v.Nx] / v.A[0][k + v.Nx];
-            if (a.l > 0) s += v.A[5][k] * v.A[6][k - NxNy] / v.A[0][k - NxNy];
-            if (a.l < v.Nz - 1) s += v.A[6][k] * v.A[5][k + NxNy] / v.A[0][k + NxNy];
+            if (a.i > 0) s += v.a(1, k) * v.a(2, k - 1) / v.a(0, k - 1);
+            if (a.i < v.Nx - 1) s += v.a(2, k) * v.a(1, k + 1) / v.a(0, k + 1);
+            if (a.j > 0) s += v.a(3, k) * v.a(4, k - v.Nx) / v.a(0, k - v.Nx);
+            if (a.j < v.Ny - 1) s += v.a(4, k) * v.a(3, k + v.Nx) / v.a(0, k + v.Nx);
+            if (a.l > 0) s += v.a(5, k) * v.a(6, k - NxNy) / v.a(0, k - NxNy);
+            if (a.l < v.Nz - 1) s += v.a(6, k) * v.a(5, k + NxNy) / v.a(0, k + NxNy);
             d = c - s;
             if (!(d > T(1e-8) * fabs(c))) d = c;
         }
         if (!(d != T(0))) d = 1;
-        v.D[k] = d;
+        v.D[k] = T(1) / d;                     // the smoothers multiply by the reciprocal
     }
 }
 
@@ -201,31 +215,46 @@ __device__ __forceinline__ Agg agg_range(const V &f, int I, int J, int K) {
     return g;
 }
 
+// Row-blocked launch shape of the level passes: block (32, 4), threadIdx.x along x (the
+// x index, or the half-row index of a colour), threadIdx.y + 4 blockIdx.z the grid row
+// j + Ny l, so no thread divides its linear index.
+constexpr int ROWS_PER_BLOCK = 4;
+#define SS_ROW_LOOP(row, rows) \
+    for (int row = blockIdx.z * ROWS_PER_BLOCK + threadIdx.y; row < (rows); row += gridDim.z * ROWS_PER_BLOCK)
+
 // x += alpha pw P xc (semiconductor_3d.c:2038-2048); the residual that follows needs
 // every prolonged neighbour and is a separate pass
 template <class T>
-__global__ void k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha, int gate) {
+__global__ void __launch_bounds__(128) k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha,
+                                                 int gate) {
     pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
     const LevView<T> f = levview<T>(P, L, bsel, xsel);
     const LevelT<T> &cl = PT<T>::lev(P, L + 1);
     const T al = (T)alpha;
-    SS_GRID_LOOP(k, f.N) {
-        const Node a = unidx(k, f.Nx, f.Ny);
-        const int I = f.cx ? a.i >> 1 : a.i, J = f.cy ? a.j >> 1 : a.j, K = f.cz ? a.l >> 1 : a.l;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    if (i >= f.Nx) return;
+    const int I = f.cx ? i >> 1 : i;
+    SS_ROW_LOOP(row, f.Ny * f.Nz) {
+        const int l = row / f.Ny, j = row - l * f.Ny;
+        const int J = f.cy ? j >> 1 : j, K = f.cz ? l >> 1 : l;
+        const int k = i + f.Nx * row;
         f.x[k] += al * f.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
     }
 }
 template <class T>
-__global__ void k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
+__global__ void __launch_bounds__(128) k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
     pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
     const LevView<T> f = levview<T>(P, L, bsel, xsel);
-    SS_GRID_LOOP(k, f.N) {
-        const Node a = unidx(k, f.Nx, f.Ny);
-        f.r[k] = f.b[k] - stencil_apply<T>(f.A, f.x, k, a.i, a.j, a.l, f.Nx, f.Ny, f.Nz);
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    if (i >= f.Nx) return;
+    SS_ROW_LOOP(row, f.Ny * f.Nz) {
+        const int l = row / f.Ny, j = row - l * f.Ny;
+        const int k = i + f.Nx * row;
+        f.r[k] = f.b[k] - lv_apply<T>(f, f.x, k, i, j, l);
     }
 }
 
@@ -365,13 +394,13 @@ __global__ void k_galerkin(const DevP *__restrict__ Ps, int L, int wsel) {
                     const int k = i + f.Nx * (j + f.Ny * l);
                     const double wk = w ? (double)w[k] : 1.0;
                     double a;
-                    cc += wk * (double)f.A[0][k] * (double)f.pw[k];
-                    if (i > 0) { a = wk * (double)f.A[1][k] * (double)f.pw[k - 1]; if (i - 1 >= g.i0) cc += a; else xm += a; }
-                    if (i < f.Nx - 1) { a = wk * (double)f.A[2][k] * (double)f.pw[k + 1]; if (i + 1 <= g.i1) cc += a; else xp += a; }
-                    if (j > 0) { a = wk * (double)f.A[3][k] * (double)f.pw[k - f.Nx]; if (j - 1 >= g.j0) cc += a; else ym += a; }
-                    if (j < f.Ny - 1) { a = wk * (double)f.A[4][k] * (double)f.pw[k + f.Nx]; if (j + 1 <= g.j1) cc += a; else yp += a; }
-                    if (l > 0) { a = wk * (double)f.A[5][k] * (double)f.pw[k - NxNy]; if (l - 1 >= g.l0) cc += a; else zm += a; }
-                    if (l < f.Nz - 1) { a = wk * (double)f.A[6][k] * (double)f.pw[k + NxNy]; if (l + 1 <= g.l1) cc += a; else zp += a; }
+                    cc += wk * (double)f.a(0, k) * (double)f.pw[k];
+                    if (i > 0) { a = wk * (double)f.a(1, k) * (double)f.pw[k - 1]; if (i - 1 >= g.i0) cc += a; else xm += a; }
+                    if (i < f.Nx - 1) { a = wk * (double)f.a(2, k) * (double)f.pw[k + 1]; if (i + 1 <= g.i1) cc += a; else xp += a; }
+                    if (j > 0) { a = wk * (double)f.a(3, k) * (double)f.pw[k - f.Nx]; if (j - 1 >= g.j0) cc += a; else ym += a; }
+                    if (j < f.Ny - 1) { a = wk * (double)f.a(4, k) * (double)f.pw[k + f.Nx]; if (j + 1 <= g.j1) cc += a; else yp += a; }
+                    if (l > 0) { a = wk * (double)f.a(5, k) * (double)f.pw[k - NxNy]; if (l - 1 >= g.l0) cc += a; else zm += a; }
+                    if (l < f.Nz - 1) { a = wk * (double)f.a(6, k) * (double)f.pw[k + NxNy]; if (l + 1 <= g.l1) cc += a; else zp += a; }
                 }
         if (cc == 0. && xm == 0. && xp == 0. && ym == 0. && yp == 0. && zm == 0. && zp == 0.) cc = 1.;
         cl.A[0][K] = (T)cc; cl.A[1][K] = (T)xm; cl.A[2][K] = (T)xp; cl.A[3][K] = (T)ym;
@@ -453,52 +482,62 @@ void mg_setup(const Ctx &c, const MGHost &mg, int qsign) { mg_setup_t<double>(c,
 // one V(1,1) cycle x = M^-1 b on the level-0 vectors (bsel -> xsel); mg_on = 0 applies
 // the level-0 smoother alone (the reference's ILU-only fallback).
 // ---- fine levels: one kernel per pass, all SMs
-// Smoother half sweep over the nodes of one colour only: thread t of a row (j,l) takes
-// i = 2t + ((j + l + colour) & 1), so every lane does work (colour 1 = black, 0 = red).
-// mode 0: pre-smoothing from x = 0, x = M^-1 b.  mode 1: post-smoothing, z = M^-1 r
-// with r the level's residual array, x += z (the black z is parked in r for the red
-// sweep).  mode 2: a further application right after a red-black one.
+// Smoother update of node k = (i, j, l) in a half sweep over one colour (1 = black,
+// 0 = red), with D the reciprocal pivots.  mode 0: pre-smoothing from x = 0,
+// x = M^-1 b.  mode 1: post-smoothing, z = M^-1 r with r the level's residual array,
+// x += z (the black z is parked in r for the red sweep).  mode 2: a further application
+// right after a red-black one: the residual of every red node is then zero, so black
+// z = r / D with the full-stencil residual, and red z = -(sum a_rb z_b) / D.
 template <class T>
-__global__ void k_smooth_c(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int mode, int color, int gate) {
+__device__ __forceinline__ void smooth_node(const LevView<T> &v, int k, int i, int j, int l, int mode, int color) {
+    if (mode == 2) {
+        if (color) {
+            const T z = (v.b[k] - lv_apply<T>(v, v.x, k, i, j, l)) * v.D[k];
+            v.x[k] += z;
+            v.r[k] = z;
+        } else {
+            v.x[k] -= lv_offdiag<T>(v, v.r, k, i, j, l) * v.D[k];
+        }
+        return;
+    }
+    const T *src = mode ? v.r : v.b;
+    if (color) {
+        const T z = (src[k] - lv_offdiag_scaled<T>(v, src, k, i, j, l)) * v.D[k];
+        if (mode) { v.x[k] += z; v.r[k] = z; }
+        else v.x[k] = z;
+    } else {
+        const T z = (src[k] - lv_offdiag<T>(v, mode ? v.r : v.x, k, i, j, l)) * v.D[k];
+        if (mode) v.x[k] += z;
+        else v.x[k] = z;
+    }
+}
+// Half sweep over the nodes of one colour: thread ti of row (j, l) takes
+// i = 2 ti + ((j + l + colour) & 1), so every lane does work.
+template <class T, int MODE, int COLOR>
+__global__ void __launch_bounds__(128) k_smooth_cm(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
+    constexpr int mode = MODE, color = COLOR;
     pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     if ((L > 0 && L >= P.nlev - 1) || gated_off<T>(P, gate)) return;
     const LevView<T> v = levview<T>(P, L, bsel, xsel);
-    const int hx = (v.Nx + 1) >> 1, rows = v.Ny * v.Nz;
-    const T *src = mode ? v.r : v.b;
-    const T *zb = mode ? v.r : v.x;
-    SS_GRID_LOOP(t, hx * rows) {
-        const int row = t / hx, ti = t - row * hx;
+    const int ti = blockIdx.x * 32 + threadIdx.x;
+    if (2 * ti >= v.Nx) return;
+    SS_ROW_LOOP(row, v.Ny * v.Nz) {
         const int l = row / v.Ny, j = row - l * v.Ny;
         const int i = 2 * ti + ((j + l + color) & 1);
         if (i >= v.Nx) continue;
-        const int k = i + v.Nx * row;
-        T z;
-        if (mode == 2) {
-            // the residual of every red node is zero after a red-black application, so
-            // black z = r / D with the full-stencil residual, and red z = -(sum a_rb z_b) / D
-            if (color) {
-                z = (v.b[k] - stencil_apply<T>(v.A, v.x, k, i, j, l, v.Nx, v.Ny, v.Nz)) / v.D[k];
-                v.x[k] += z;
-                v.r[k] = z;
-            } else {
-                z = -offdiag_apply<T>(v.A, v.r, k, i, j, l, v.Nx, v.Ny, v.Nz) / v.D[k];
-                v.x[k] += z;
-            }
-            continue;
-        }
-        if (color) {
-            const T s = offdiag_apply_div<T>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
-            z = (src[k] - s) / v.D[k];
-            if (mode) { v.x[k] += z; v.r[k] = z; }
-            else v.x[k] = z;
-        } else {
-            const T s = offdiag_apply<T>(v.A, zb, k, i, j, l, v.Nx, v.Ny, v.Nz);
-            z = (src[k] - s) / v.D[k];
-            if (mode) v.x[k] += z;
-            else v.x[k] = z;
-        }
+        smooth_node<T>(v, i + v.Nx * row, i, j, l, mode, color);
     }
+}
+// the half sweep of (mode, colour), one kernel instance per pair
+template <class T>
+using SmoothFn = void (*)(const DevP *, int, int, int, int);
+template <class T>
+static SmoothFn<T> smooth_fn(int mode, int color) {
+    static const SmoothFn<T> tab[3][2] = {{k_smooth_cm<T, 0, 0>, k_smooth_cm<T, 0, 1>},
+                                          {k_smooth_cm<T, 1, 0>, k_smooth_cm<T, 1, 1>},
+                                          {k_smooth_cm<T, 2, 0>, k_smooth_cm<T, 2, 1>}};
+    return tab[mode][color];
 }
 
 // Weighted residual of every fine node summed into its 2x2x2 aggregate.  Block (32, 4):
@@ -525,7 +564,7 @@ __global__ void __launch_bounds__(128) k_resid_restrict2(const DevP *__restrict_
     T val = 0;
     if (ok) {
         const int k = i + f.Nx * (j + f.Ny * l);
-        const T r = f.b[k] - stencil_apply<T>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
+        const T r = f.b[k] - lv_apply<T>(f, f.x, k, i, j, l);
         val = w ? w[k] * r : r;
     }
     __shared__ T sh[4][32];
@@ -554,26 +593,13 @@ __device__ __forceinline__ void cl_sync() { cg::this_cluster().sync(); }
 
 template <class T>
 __device__ __forceinline__ void cta_smooth(const LevView<T> &v, int color, int mode) {
-    const T *src = mode ? v.r : v.b;
-    const T *zb = mode ? v.r : v.x;
     const int hx = (v.Nx + 1) >> 1, rows = v.Ny * v.Nz;
     for (int t = cl_first(); t < hx * rows; t += cl_stride()) {
         const int row = t / hx, ti = t - row * hx;
         const int l = row / v.Ny, j = row - l * v.Ny;
         const int i = 2 * ti + ((j + l + color) & 1);
         if (i >= v.Nx) continue;
-        const int k = i + v.Nx * row;
-        if (color) {
-            const T s = offdiag_apply_div<T>(v.A, src, v.D, k, i, j, l, v.Nx, v.Ny, v.Nz);
-            const T z = (src[k] - s) / v.D[k];
-            if (mode) { v.x[k] += z; v.r[k] = z; }
-            else v.x[k] = z;
-        } else {
-            const T s = offdiag_apply<T>(v.A, zb, k, i, j, l, v.Nx, v.Ny, v.Nz);
-            const T z = (src[k] - s) / v.D[k];
-            if (mode) v.x[k] += z;
-            else v.x[k] = z;
-        }
+        smooth_node<T>(v, i + v.Nx * row, i, j, l, mode, color);
     }
     cl_sync();
 }
@@ -587,7 +613,7 @@ __device__ __forceinline__ void cta_resid_restrict(const LevView<T> &f, const Le
             for (int j = g.j0; j <= g.j1; j++)
                 for (int i = g.i0; i <= g.i1; i++) {
                     const int k = i + f.Nx * (j + f.Ny * l);
-                    const T r = f.b[k] - stencil_apply<T>(f.A, f.x, k, i, j, l, f.Nx, f.Ny, f.Nz);
+                    const T r = f.b[k] - lv_apply<T>(f, f.x, k, i, j, l);
                     s += w ? w[k] * r : r;
                 }
         cl.b[K] = s;
@@ -607,7 +633,7 @@ template <class T>
 __device__ __forceinline__ void cta_resid(const LevView<T> &f) {
     for (int k = cl_first(); k < f.N; k += cl_stride()) {
         const Node a = unidx(k, f.Nx, f.Ny);
-        f.r[k] = f.b[k] - stencil_apply<T>(f.A, f.x, k, a.i, a.j, a.l, f.Nx, f.Ny, f.Nz);
+        f.r[k] = f.b[k] - lv_apply<T>(f, f.x, k, a.i, a.j, a.l);
     }
     cl_sync();
 }
@@ -712,9 +738,15 @@ static void launch_small(const Ctx &c, int nodes, int Ls, int bsel, int xsel, in
     if (g_prof_on) prof_end(pf<T>(PF_COARSE), c.st, nodes);
 }
 
-static inline dim3 grid_half(const Ctx &c, int L, const MGHost &mg) {
-    return grid_n(c, ((mg.maxNx[L] + 1) / 2) * (mg.maxN[L] / (mg.maxNx[L] > 0 ? mg.maxNx[L] : 1)));
+// row-blocked grids (block (32, ROWS_PER_BLOCK)): x extent `nx`, all rows of level L
+static inline dim3 grid_rows(const Ctx &c, int L, const MGHost &mg, int nx) {
+    int gz = (mg.maxRows[L] + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK;
+    if (gz > 65535) gz = 65535;
+    return dim3((nx + 31) / 32, c.ninst, gz > 0 ? gz : 1);
 }
+static inline dim3 grid_half(const Ctx &c, int L, const MGHost &mg) { return grid_rows(c, L, mg, (mg.maxNx[L] + 1) / 2); }
+static inline dim3 grid_full(const Ctx &c, int L, const MGHost &mg) { return grid_rows(c, L, mg, mg.maxNx[L]); }
+static const dim3 ROW_BLOCK(32, ROWS_PER_BLOCK);
 static int small_split(const MGHost &mg) {
     small_init();
     int Ls = 0;
@@ -726,17 +758,17 @@ template <class T>
 static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
     const int SB = pf<T>(PF_SMOOTH_B), SR = pf<T>(PF_SMOOTH_R);
     if (!mg_on) {
-        SS_LAUNCH_PDL(SB, c.maxN, k_smooth_c<T>, grid_half(c, 0, mg), TPB, c.st, c.dP, 0, bsel, xsel, 0, 1, gate);
-        SS_LAUNCH_PDL(SR, c.maxN, k_smooth_c<T>, grid_half(c, 0, mg), TPB, c.st, c.dP, 0, bsel, xsel, 0, 0, gate);
+        SS_LAUNCH_PDL(SB, c.maxN, smooth_fn<T>(0, 1), grid_half(c, 0, mg), ROW_BLOCK, c.st, c.dP, 0, bsel, xsel, gate);
+        SS_LAUNCH_PDL(SR, c.maxN, smooth_fn<T>(0, 0), grid_half(c, 0, mg), ROW_BLOCK, c.st, c.dP, 0, bsel, xsel, gate);
         return;
     }
     const int Ls = small_split(mg);
     for (int L = 0; L < Ls; L++) {
-        SS_LAUNCH_PDL(SB, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 1, gate);
-        SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 0, 0, gate);
+        SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(0, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
+        SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(0, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         if (L == 0 && g_l0_sweeps > 1) {     // second application on the finest level
-            SS_LAUNCH_PDL(SB, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 1, gate);
-            SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
+            SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(2, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
+            SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(2, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         }
         const dim3 gr((mg.maxNx[L] + 31) / 32, c.ninst, mg.maxRows[L + 1]);
         SS_LAUNCH_PDL(pf<T>(PF_RESID_RESTRICT), mg.maxN[L], k_resid_restrict2<T>, gr, dim3(32, 4), c.st, c.dP, L, bsel,
@@ -744,15 +776,15 @@ static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wse
     }
     launch_small<T>(c, mg.maxN[Ls], Ls, bsel, xsel, wsel, mg.alpha, gate);
     for (int L = Ls - 1; L >= 0; L--) {
-        SS_LAUNCH_PDL(pf<T>(PF_PROLONG), mg.maxN[L], k_prolong<T>, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel, xsel,
+        SS_LAUNCH_PDL(pf<T>(PF_PROLONG), mg.maxN[L], k_prolong<T>, grid_full(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel,
                   mg.alpha, gate);
-        SS_LAUNCH_PDL(pf<T>(PF_LEVEL_RESID), mg.maxN[L], k_level_resid<T>, grid_n(c, mg.maxN[L]), TPB, c.st, c.dP, L, bsel,
+        SS_LAUNCH_PDL(pf<T>(PF_LEVEL_RESID), mg.maxN[L], k_level_resid<T>, grid_full(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel,
                   xsel, gate);
-        SS_LAUNCH_PDL(SB, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 1, gate);
-        SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 1, 0, gate);
+        SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(1, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
+        SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(1, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         if (L == 0 && g_l0_sweeps > 1) {
-            SS_LAUNCH_PDL(SB, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 1, gate);
-            SS_LAUNCH_PDL(SR, mg.maxN[L], k_smooth_c<T>, grid_half(c, L, mg), TPB, c.st, c.dP, L, bsel, xsel, 2, 0, gate);
+            SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(2, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
+            SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(2, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         }
     }
 }
@@ -1443,19 +1475,19 @@ double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
     auto one = [&]() {
         switch (which) {
         case 0: k_bicg_v<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
-        case 1: k_smooth_c<double><<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 1, 0); break;
-        case 2: k_smooth_c<double><<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 0, 0); break;
+        case 1: k_smooth_cm<double, 0, 1><<<grid_half(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
+        case 2: k_smooth_cm<double, 0, 0><<<grid_half(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
         case 3: k_resid_restrict2<double><<<grr, dim3(32, 4), 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
-        case 4: k_level_resid<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
-        case 5: k_prolong<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 1.0, 0); break;
+        case 4: k_level_resid<double><<<grid_full(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
+        case 5: k_prolong<double><<<grid_full(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 1.0, 0); break;
         case 6: k_bicg_x<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
         case 7: launch_small<double>(c, mg.maxN[Ls], Ls, 2, 4, 1, 1.0, 0); break;
         case 8: vcycle_t<double>(c, mg, 2, 4, 1, 1, 0); break;
         case 9: k_copy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 5, 6); break;
         case 10: k_bicg_rho<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
         case 11: k_bicg_v<float><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
-        case 12: k_smooth_c<float><<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 1, 0); break;
-        case 13: k_smooth_c<float><<<grid_half(c, 0, mg), TPB, 0, c.st>>>(c.dP, 0, 2, 4, 0, 0, 0); break;
+        case 12: k_smooth_cm<float, 0, 1><<<grid_half(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
+        case 13: k_smooth_cm<float, 0, 0><<<grid_half(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
         case 14: k_resid_restrict2<float><<<grr, dim3(32, 4), 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
         case 15: vcycle_t<float>(c, mg, 2, 4, 1, 1, 0); break;
         case 16: k_ir_update<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;

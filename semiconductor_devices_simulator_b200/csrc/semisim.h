@@ -56,8 +56,9 @@ template <class T>
 struct LevelT {
     int Nx, Ny, Nz, N;
     int cx, cy, cz, last;        // coarsened along x/y/z; last = coarsest (dense) level
+    int apitch, pad_;            // A[q] = A[0] + q * apitch (the seven arrays are laid out back to back)
     T *A[7];                     // c, xm, xp, ym, yp, zm, zp
-    T *D;                        // red-black D-ILU pivots (or the dense inverse on the last level)
+    T *D;                        // reciprocal red-black D-ILU pivots (or the dense inverse on the last level)
     T *x, *b, *r;
     T *pw;                       // prolongation weights (to the parent)
     double *ph;                  // reference level / VT of the Slotboom weights (set-up only)

@@ -130,6 +130,7 @@ static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &lev
     auto shape = [&](auto &v, int L) {
         v.Nx = dims[L][0]; v.Ny = dims[L][1]; v.Nz = dims[L][2];
         v.N = v.Nx * v.Ny * v.Nz;
+        v.apitch = int(align_up((size_t)v.N * sizeof(*v.A[0])) / sizeof(*v.A[0]));
         v.cx = dims[L][3]; v.cy = dims[L][4]; v.cz = dims[L][5];
         v.last = L == nlev - 1;
     };
@@ -239,6 +240,14 @@ static int gpu_alloc(Inst &d) {
     CK(cudaMallocHost(&d.g.pin, sizeof(double) * 256));
     CK(cudaMalloc(&d.g.scratch, sizeof(double) * (d.N > 0 ? d.N : 1)));
     CK(cudaMalloc(&d.g.flag, sizeof(int) * 16));
+    for (int L = 0; L < nl; L++)                     // the kernels address A[q] as A[0] + q * apitch
+        for (int q = 1; q < 7; q++)
+            if (levs[L].A[q] != levs[L].A[0] + (size_t)q * levs[L].apitch ||
+                levsf[L].A[q] != levsf[L].A[0] + (size_t)q * levsf[L].apitch) {
+                std::fprintf(stderr, "semisim-b200: level %d coupling arrays are not evenly spaced\n", L);
+                gpu_free(d);
+                return 0;
+            }
     CK(cudaMemcpy(P.lev, levs.data(), sizeof(LevelT<double>) * nl, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(P.levf, levsf.data(), sizeof(LevelT<float>) * nl, cudaMemcpyHostToDevice));
     MGHost &mg = d.g.mg;
