@@ -678,9 +678,134 @@ __global__ void __launch_bounds__(SMALL_TPB) k_vcycle_small(const DevP *__restri
     }
 }
 
+// ---- small levels, shared-memory resident: one CTA per instance loads the couplings,
+// pivots and weights of every level from Ls down (and b of level Ls) into shared memory,
+// runs the rest of the V-cycle there with block barriers between passes, and writes x of
+// level Ls back.  Layout per level: A (7 N, pitch N), D, pw, x, b, r; the coarsest level
+// keeps its dense inverse (N x N), x and b.
+__host__ __device__ inline size_t al16(size_t b) { return (b + 15) & ~size_t(15); }
+template <class T>
+__host__ __device__ inline size_t smem_level_bytes(int N, bool last) {
+    if (last) return al16((size_t)N * N * sizeof(T)) + 2 * al16((size_t)N * sizeof(T));
+    return al16(7 * (size_t)N * sizeof(T)) + 5 * al16((size_t)N * sizeof(T));
+}
+template <class T>
+__device__ LevView<T> smem_view(const DevP &P, int L, int Ls, unsigned char *base) {
+    size_t off = 0;
+    for (int q = Ls; q < L; q++) off += smem_level_bytes<T>(PT<T>::lev(P, q).N, false);
+    const LevelT<T> &g = PT<T>::lev(P, L);
+    const int N = g.N;
+    const size_t nb = al16((size_t)N * sizeof(T));
+    unsigned char *p = base + off;
+    LevView<T> v;
+    v.ap = N;
+    v.Nx = g.Nx; v.Ny = g.Ny; v.Nz = g.Nz; v.N = N;
+    v.cx = g.cx; v.cy = g.cy; v.cz = g.cz; v.last = g.last;
+    v.ph = nullptr;
+    if (g.last) {
+        v.A = nullptr; v.r = nullptr; v.pw = nullptr;
+        v.D = reinterpret_cast<T *>(p); p += al16((size_t)N * N * sizeof(T));
+        v.x = reinterpret_cast<T *>(p); p += nb;
+        v.b = reinterpret_cast<T *>(p);
+    } else {
+        v.A = reinterpret_cast<T *>(p); p += al16(7 * (size_t)N * sizeof(T));
+        v.D = reinterpret_cast<T *>(p); p += nb;
+        v.pw = reinterpret_cast<T *>(p); p += nb;
+        v.x = reinterpret_cast<T *>(p); p += nb;
+        v.b = reinterpret_cast<T *>(p); p += nb;
+        v.r = reinterpret_cast<T *>(p);
+    }
+    return v;
+}
+template <class T>
+__device__ __forceinline__ void blk_copy(T *dst, const T *src, int n) {
+    for (int q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[q];
+}
+template <class T>
+__device__ __forceinline__ void blk_smooth(const LevView<T> &v, int color, int mode) {
+    const int hx = (v.Nx + 1) >> 1, rows = v.Ny * v.Nz;
+    for (int t = threadIdx.x; t < hx * rows; t += blockDim.x) {
+        const int row = t / hx, ti = t - row * hx;
+        const int l = row / v.Ny, j = row - l * v.Ny;
+        const int i = 2 * ti + ((j + l + color) & 1);
+        if (i >= v.Nx) continue;
+        smooth_node<T>(v, i + v.Nx * row, i, j, l, mode, color);
+    }
+    __syncthreads();
+}
+template <class T>
+__global__ void __launch_bounds__(SMALL_TPB) k_vcycle_smem(const DevP *__restrict__ Ps, int Ls, double alpha,
+                                                           int gate) {
+    pdl_entry();
+    const DevP &P = Ps[blockIdx.y];
+    if (gated_off<T>(P, gate)) return;
+    extern __shared__ __align__(16) unsigned char sraw[];
+    const int nl = P.nlev;
+    for (int L = Ls; L < nl; L++) {               // stage the levels
+        const LevelT<T> &g = PT<T>::lev(P, L);
+        const LevView<T> v = smem_view<T>(P, L, Ls, sraw);
+        if (g.last) {
+            blk_copy<T>(v.D, g.D, g.N * g.N);
+        } else {
+            for (int q = 0; q < 7; q++) blk_copy<T>(const_cast<T *>(v.A) + q * g.N, g.A[q], g.N);
+            blk_copy<T>(v.D, g.D, g.N);
+            blk_copy<T>(v.pw, g.pw, g.N);
+        }
+        if (L == Ls) blk_copy<T>(v.b, g.b, g.N);
+    }
+    __syncthreads();
+    for (int L = Ls; L < nl - 1; L++) {
+        const LevView<T> v = smem_view<T>(P, L, Ls, sraw), cv = smem_view<T>(P, L + 1, Ls, sraw);
+        blk_smooth<T>(v, 1, 0);
+        blk_smooth<T>(v, 0, 0);
+        for (int K = threadIdx.x; K < cv.N; K += blockDim.x) {   // residual summed into the aggregates
+            const Node c = unidx(K, cv.Nx, cv.Ny);
+            const Agg g = agg_range(v, c.i, c.j, c.l);
+            T sum = 0;
+            for (int l = g.l0; l <= g.l1; l++)
+                for (int j = g.j0; j <= g.j1; j++)
+                    for (int i = g.i0; i <= g.i1; i++) {
+                        const int k = i + v.Nx * (j + v.Ny * l);
+                        sum += v.b[k] - lv_apply<T>(v, v.x, k, i, j, l);
+                    }
+            cv.b[K] = sum;
+        }
+        __syncthreads();
+    }
+    {                                             // coarsest level: x = D^-1 b (dense inverse)
+        const LevView<T> v = smem_view<T>(P, nl - 1, Ls, sraw);
+        for (int r = threadIdx.x; r < v.N; r += blockDim.x) {
+            T sum = 0;
+            for (int q = 0; q < v.N; q++) sum += v.D[r * v.N + q] * v.b[q];
+            v.x[r] = sum;
+        }
+        __syncthreads();
+    }
+    const T al = (T)alpha;
+    for (int L = nl - 2; L >= Ls; L--) {
+        const LevView<T> v = smem_view<T>(P, L, Ls, sraw), cv = smem_view<T>(P, L + 1, Ls, sraw);
+        for (int k = threadIdx.x; k < v.N; k += blockDim.x) {
+            const Node a = unidx(k, v.Nx, v.Ny);
+            const int I = v.cx ? a.i >> 1 : a.i, J = v.cy ? a.j >> 1 : a.j, K = v.cz ? a.l >> 1 : a.l;
+            v.x[k] += al * v.pw[k] * cv.x[I + cv.Nx * (J + cv.Ny * K)];
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < v.N; k += blockDim.x) {
+            const Node a = unidx(k, v.Nx, v.Ny);
+            v.r[k] = v.b[k] - lv_apply<T>(v, v.x, k, a.i, a.j, a.l);
+        }
+        __syncthreads();
+        blk_smooth<T>(v, 1, 1);
+        blk_smooth<T>(v, 0, 1);
+    }
+    const LevView<T> v = smem_view<T>(P, Ls, Ls, sraw);
+    blk_copy<T>(PT<T>::lev(P, Ls).x, v.x, v.N);
+}
+
 int g_small_nodes = 2048;           // levels at or below this size run in the cluster kernel
 int g_l0_sweeps = 2;                // red-black applications per smoothing step on the finest level
 static int g_cluster = 0;           // CTAs per cluster of the small-level kernel (set on first use)
+static size_t g_smem_max = 0;       // dynamic shared memory of the shared-memory small-level kernel (0: off)
 
 template <class T>
 static bool cluster16_ok() {
@@ -713,6 +838,19 @@ static void small_init() {
         const bool ok64 = cluster16_ok<double>(), ok32 = cluster16_ok<float>();
         if (!ok64 || !ok32) cl = 8;
         g_cluster = cl;
+        int dev = 0, optin = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        g_smem_max = optin > 0 ? (size_t)optin : 0;
+        const char *sm = std::getenv("SEMISIM_B200_SMEM");
+        if (sm && std::atoi(sm) == 0) g_smem_max = 0;
+        if (g_smem_max &&
+            (cudaFuncSetAttribute(k_vcycle_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_smem_max) !=
+                 cudaSuccess ||
+             cudaFuncSetAttribute(k_vcycle_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_smem_max) !=
+                 cudaSuccess))
+            g_smem_max = 0;
+        cudaGetLastError();
     }
 }
 
@@ -753,6 +891,45 @@ static int small_split(const MGHost &mg) {
     while (Ls < mg.maxlev - 1 && mg.maxN[Ls] > g_small_nodes) Ls++;
     return Ls;
 }
+// shared-memory bytes of levels Ls.. of the shared-memory small-level kernel
+template <class T>
+static size_t smem_bytes(const MGHost &mg, int Ls) {
+    size_t b = 0;
+    for (int L = Ls; L < mg.maxlev; L++) b += smem_level_bytes<T>(mg.maxN[L], L == mg.maxlev - 1);
+    return b;
+}
+// where the per-level kernels stop: the shared-memory kernel takes the levels from the
+// first one at or below g_small_nodes whose data fits (never level 0); *smem = its bytes,
+// 0 when the cluster kernel takes the small levels instead
+template <class T>
+static int small_plan(const MGHost &mg, size_t *smem) {
+    int Ls = small_split(mg);
+    *smem = 0;
+    if (!g_smem_max || mg.maxlev < 2) return Ls;
+    int L = Ls < 1 ? 1 : Ls;
+    while (L < mg.maxlev - 1 && smem_bytes<T>(mg, L) > g_smem_max) L++;
+    if (smem_bytes<T>(mg, L) > g_smem_max) return Ls;
+    *smem = smem_bytes<T>(mg, L);
+    return L;
+}
+template <class T>
+static void launch_smem(const Ctx &c, int nodes, int Ls, double alpha, int gate, size_t bytes) {
+    g_launches++;
+    t_launches++;
+    if (g_prof_on) prof_begin(pf<T>(PF_COARSE), c.st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1, c.ninst);
+    cfg.blockDim = dim3(SMALL_TPB);
+    cfg.dynamicSmemBytes = bytes;
+    cfg.stream = c.st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = g_pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k_vcycle_smem<T>, c.dP, Ls, alpha, gate);
+    if (g_prof_on) prof_end(pf<T>(PF_COARSE), c.st, nodes);
+}
 
 template <class T>
 static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate) {
@@ -762,7 +939,8 @@ static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wse
         SS_LAUNCH_PDL(SR, c.maxN, smooth_fn<T>(0, 0), grid_half(c, 0, mg), ROW_BLOCK, c.st, c.dP, 0, bsel, xsel, gate);
         return;
     }
-    const int Ls = small_split(mg);
+    size_t smem = 0;
+    const int Ls = small_plan<T>(mg, &smem);
     for (int L = 0; L < Ls; L++) {
         SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(0, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(0, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
@@ -774,7 +952,8 @@ static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wse
         SS_LAUNCH_PDL(pf<T>(PF_RESID_RESTRICT), mg.maxN[L], k_resid_restrict2<T>, gr, dim3(32, 4), c.st, c.dP, L, bsel,
                   xsel, wsel, gate);
     }
-    launch_small<T>(c, mg.maxN[Ls], Ls, bsel, xsel, wsel, mg.alpha, gate);
+    if (smem) launch_smem<T>(c, mg.maxN[Ls], Ls, mg.alpha, gate, smem);
+    else launch_small<T>(c, mg.maxN[Ls], Ls, bsel, xsel, wsel, mg.alpha, gate);
     for (int L = Ls - 1; L >= 0; L--) {
         SS_LAUNCH_PDL(pf<T>(PF_PROLONG), mg.maxN[L], k_prolong<T>, grid_full(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel,
                   mg.alpha, gate);
@@ -1463,7 +1642,8 @@ double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
     ks0.maxit = 1 << 30;
     cudaMemcpy(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice);
     cudaMemcpy(c.h.ksi, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice);
-    const int Ls = small_split(mg);
+    size_t sm64 = 0, sm32 = 0;
+    const int Ls64 = small_plan<double>(mg, &sm64), Ls32 = small_plan<float>(mg, &sm32);
     if (which >= 11) {
         mg_setup_t<float>(c, mg, 1);
         cudaStreamSynchronize(c.st);
@@ -1481,7 +1661,10 @@ double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
         case 4: k_level_resid<double><<<grid_full(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
         case 5: k_prolong<double><<<grid_full(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 1.0, 0); break;
         case 6: k_bicg_x<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
-        case 7: launch_small<double>(c, mg.maxN[Ls], Ls, 2, 4, 1, 1.0, 0); break;
+        case 7:
+            if (sm64) launch_smem<double>(c, mg.maxN[Ls64], Ls64, 1.0, 0, sm64);
+            else launch_small<double>(c, mg.maxN[Ls64], Ls64, 2, 4, 1, 1.0, 0);
+            break;
         case 8: vcycle_t<double>(c, mg, 2, 4, 1, 1, 0); break;
         case 9: k_copy<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP, 5, 6); break;
         case 10: k_bicg_rho<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
@@ -1491,6 +1674,10 @@ double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
         case 14: k_resid_restrict2<float><<<grr, dim3(32, 4), 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
         case 15: vcycle_t<float>(c, mg, 2, 4, 1, 1, 0); break;
         case 16: k_ir_update<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
+        case 17:
+            if (sm32) launch_smem<float>(c, mg.maxN[Ls32], Ls32, 1.0, 0, sm32);
+            else launch_small<float>(c, mg.maxN[Ls32], Ls32, 2, 4, 1, 1.0, 0);
+            break;
         default: break;
         }
     };
