@@ -239,6 +239,24 @@ int api3b_free(int h);
 int api3b_set_precision(int mode);
 int api3b_get_precision(void);
 
+/* No counterpart in the reference (it has no learned component).  Learned sweep predictor
+   of the current instance: a per-node MLP (48 features -> 3 x 128 SiLU -> 3, BF16 weights,
+   FP32 accumulation) corrects the sweep predictor's linear extrapolation
+   x1 + s (x1 - x0) of (psi, phi_n, phi_p) at the first continuation step of a new bias
+   point.  It only changes the Gummel loop's starting point: the loop still stops on the
+   same tolerances, and a seeded step that fails is redone from the linear guess.
+     api3b_seed_set_model: load api3b_seed_nparam() FP32 parameters (W1 [128][48], b1 [128],
+        W2 [128][128], b2, W3 [128][128], b3, W4 [8][128] with rows 3-7 zero, b4 [8]) into the
+        instance (after its first solve) and enable the seed; 1 = done, 0 = wrong size /
+        no device memory yet.
+     api3b_seed_enable: 1 on, 0 off (linear guess only); returns the previous setting.
+        api3_init switches the seed off (the model stays loaded for api3b_seed_enable(1)).
+     api3b_seed_stats: seeded predictor steps and seeded steps redone from the linear guess. */
+int api3b_seed_set_model(const float *params, int n);
+int api3b_seed_enable(int on);
+void api3b_seed_stats(long long *used, long long *fallbacks);
+int api3b_seed_nparam(void);
+
 /* No counterpart in the reference.  For callers that cannot allocate device memory
    (their memory belongs to another allocator, or a cudaMalloc / cudaFree on their path is
    not acceptable): r = b - A x for a 7-point stencil A (7 arrays of N = Nx*Ny*Nz doubles:

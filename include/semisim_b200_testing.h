@@ -18,7 +18,8 @@ int b200x_prepare(void);
 /* per node: kind, contact id + 1, gate id + 1, Robin area (m^2) */
 int b200x_masks(int *kind, int *con, int *gate, double *robA);
 /* device state arrays: 0 psi, 1 phi_n, 2 phi_p, 3 n, 4 p, 5/6 low-field mobility n/p,
-   7 sol, 8 rhs, 9 sc, 10 dsc, 16..21 face mobility (n x,y,z; p x,y,z) */
+   7 sol, 8 rhs, 9 sc, 10 dsc, 16..21 face mobility (n x,y,z; p x,y,z), 22..24 sweep history
+   h1 (psi, phi_n, phi_p now), 25..27 e2 (one step back) */
 int b200x_set(int which, const double *in);
 int b200x_get(int which, double *out);
 double b200x_vlo(void);
@@ -46,6 +47,11 @@ int b200x_bicgstab(int maxit, double rtol, double atol, int qsign, const double 
 int b200x_pcg(int maxit, double rtol, double *sol);
 /* floating-block balance of a continuity solution (in place) */
 int b200x_float_fix(int hole, double *sol);
+/* learned predictor on the present history arrays (22-24 h1, 25-27 e2 of b200x_set /
+   b200x_get): psi, phi_n, phi_p = h1 + s (h1 - e2) + VT * MLP; 1 = done */
+int b200x_seed_run(double s, const double *dv4);
+/* thermal voltage of the reference material (0 before prepare) */
+double b200x_vtref(void);
 /* refinement steps and FP64 take-overs of the instance's refined continuity solves */
 void b200x_ir_stats(long long *steps, long long *fallbacks);
 /* device memory of the instance (bytes) */

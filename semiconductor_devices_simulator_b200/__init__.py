@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libsemisim_b200.so")
 
 _I, _D, _LL = ctypes.c_int, ctypes.c_double, ctypes.c_longlong
 _DP, _IP = ctypes.POINTER(_D), ctypes.POINTER(_I)
+_VP = ctypes.c_void_p
 HOOKS = {
     "b200x_prepare": (_I, []),
     "b200x_masks": (_I, [_IP, _IP, _IP, _DP]),
@@ -51,10 +52,20 @@ HOOKS = {
     "b200x_prof_detail": (_I, [_I, _IP, _DP, _DP, _DP]),
     "b200x_launches": (ctypes.c_ulonglong, []),
     "b200x_ir_stats": (None, [ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
+    "b200x_seed_run": (_I, [_D, _DP]),
+    "b200x_vtref": (_D, []),
+    # training kernels of the learned predictor (device pointers as integers)
+    "b200m_seed_features": (_I, [_VP] * 6 + [_D, _DP, _VP, _VP]),
+    "b200m_mlp_pack": (_I, [_VP, _VP, _VP, _VP]),
+    "b200m_mlp_forward": (_I, [_VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "b200m_mlp_backward": (_I, [_VP, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "b200m_mlp_adam": (_I, [_VP, _VP, _VP, _VP, ctypes.c_float, _I, _VP, _VP, _VP]),
+    "b200m_mlp_sizes": (_I, [_IP, _IP, _IP]),
 }
 # state arrays reachable through b200x_set / b200x_get
 ST_PHI, ST_PHIN, ST_PHIP, ST_N, ST_P, ST_MU0N, ST_MU0P, ST_SOL, ST_RHS, ST_SC, ST_DSC = range(11)
 ST_FMU = 16
+ST_H1, ST_E2 = 22, 25                 # sweep history: solution now (h1) and one step back (e2)
 
 _lib = None
 

@@ -121,6 +121,11 @@ EXTRA = {
     # linear-solve precision of the current instance (0 FP64, 1 FP32 refined in FP64)
     "api3b_set_precision": (_I, [_I]),
     "api3b_get_precision": (_I, []),
+    # learned sweep predictor of the current instance
+    "api3b_seed_set_model": (_I, [ctypes.POINTER(ctypes.c_float), _I]),
+    "api3b_seed_enable": (_I, [_I]),
+    "api3b_seed_stats": (None, [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+    "api3b_seed_nparam": (_I, []),
 }
 
 

@@ -198,6 +198,7 @@ void gpu_free(Inst &d) {
     if (d.g.pin) cudaFreeHost(d.g.pin);
     if (d.g.scratch) cudaFree(d.g.scratch);
     if (d.g.flag) cudaFree(d.g.flag);
+    if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();
 }
@@ -774,7 +775,7 @@ static int cont_path(Inst &d) {
             if (r >= -2. && r <= 3. && std::fabs(r) > 1e-12 && err <= 1e-9 + 1e-6 * span) rx = r;
         }
     }
-    int first = 1;
+    int first = 1, noseed = 0;
     double t = 0., tp = -1., dt = span > 0. ? std::fmin(1., 0.1 / span) : 1.;
     int ok_all = 0, its = 0, steps = 0;
     double res = 0.;
@@ -784,8 +785,15 @@ static int cont_path(Inst &d) {
         const double tn = std::fmin(1., t + dt);
         for (int q = 0; q < nc; q++) Va[q] = Vf[q] + tn * (Vt[q] - Vf[q]);
         set_vrange(d, Va);
+        int seeded = 0;
         if (tp >= 0.) {
             launch_extrap(c, (tn - t) / (t - tp), 0, 1);
+        } else if (rx != 0. && !noseed && seed_available(d)) {
+            // learned correction of the sweep predictor's linear guess
+            double dvs[4] = {0., 0., 0., 0.};
+            for (int q = 0; q < nc && q < 4; q++) dvs[q] = Va[q] - Vf[q];
+            launch_mlp_seed(d, tn * rx, dvs);
+            seeded = 1;
         } else if (rx != 0.) {
             launch_extrap(c, tn * rx, 0, 2);
         } else {
@@ -795,14 +803,21 @@ static int cont_path(Inst &d) {
                 region_shift(d, dV);
             }
         }
-        if (first) {
-            for (int a = 0; a < 3; a++) copy_dev(d, d.g.h.e2[a], d.g.h.h1[a]);
-            first = 0;
-        }
         clamp_qf(d);
         apply_bc(d, Va);
         rebuild_np(d);
         const int ok = gummel(d, Va, maxg, gtol, &its, &res);
+        if (!ok && seeded) {                       // redo the step from the linear guess
+            d.seed_fallbacks++;
+            noseed = 1;
+            if (d.verbose) std::fprintf(stderr, "semisim-b200: learned seed failed, linear guess\n");
+            continue;
+        }
+        if (seeded) d.seed_used++;
+        if (first) {                               // the path's start (h1 until the first accepted step)
+            for (int a = 0; a < 3; a++) copy_dev(d, d.g.h.e2[a], d.g.h.h1[a]);
+            first = 0;
+        }
         d.conv_iter = its;
         d.conv_res = res;
         if (d.verbose)

@@ -46,6 +46,8 @@ struct Gpu {
     double *pin = nullptr;       // pinned host scratch (results)
     double *scratch = nullptr;   // device scratch (bulk output)
     int *flag = nullptr;         // device int scratch
+    void *seedw = nullptr;       // learned predictor: BF16 weight pack, then FP32 biases and parameters
+    float *seedb = nullptr;
 };
 
 struct TrapSpec { int type, ref; double E, sn, sp; };   // deep-level species (stored, not solved)
@@ -81,6 +83,8 @@ struct Inst {
     int aa_m = 0, aa_n = 0, aa_pos = 0, aa_have = 0;
     int precision = -1;               // linear solves: 0 FP64, 1 FP32 refined in FP64, -1 library default
     long long ir_steps = 0, ir_fallbacks = 0;
+    int seed_on = 0;                  // learned sweep predictor enabled (needs a loaded model)
+    long long seed_used = 0, seed_fallbacks = 0;
     // ---- derived by prepare (host copies)
     std::vector<uint32_t> flags;
     std::vector<double> bgn, robA, mu0n, mu0p;
@@ -129,7 +133,9 @@ void rebuild_np(Inst &d);
 void upd_mob(Inst &d);
 void terminal_currents(Inst &d, double *I, double *S);
 Ctx make_ctx(Inst &d);
-int use_mixed(const Inst &d);       // precision of the instance's linear solves (1 = refined FP32)
+int use_mixed(const Inst &d);
+int seed_available(const Inst &d);                       // learned.cu
+void launch_mlp_seed(Inst &d, double s, const double *dv);       // precision of the instance's linear solves (1 = refined FP32)
 extern int g_precision_default;
 void gpu_free(Inst &d);
 

@@ -27,6 +27,8 @@ double *arr(Inst &d, int which) {
     case 7: return P.sol; case 8: return P.rhs; case 9: return P.sc; case 10: return P.dsc;
     }
     if (which >= 16 && which < 22) return P.fmu[which - 16];
+    if (which >= 22 && which < 25) return P.h1[which - 22];
+    if (which >= 25 && which < 28) return P.e2[which - 25];
     return nullptr;
 }
 void dump7(Inst &d, double *const *A, size_t n, double *A7) {
@@ -223,6 +225,22 @@ double b200x_bench(int which, int reps) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return 1e3 * ms / reps;
+}
+
+// thermal voltage of the reference material (the unit of the learned predictor's
+// outputs); 0 before the device is prepared
+double b200x_vtref(void) { return dev()->g.ready ? dev()->g.h.VTref : 0.0; }
+
+// learned predictor on the present history: psi, phi_n, phi_p = h1 + s (h1 - e2) +
+// VT * MLP (the step voltages dv: 4 values, volts); 1 = done (a model must be loaded)
+int b200x_seed_run(double s, const double *dv4) {
+    Inst &d = *dev();
+    if (!d.g.ready || !d.g.seedw) return 0;
+    double dv[4] = {0., 0., 0., 0.};
+    for (int q = 0; q < 4; q++) dv[q] = dv4 ? dv4[q] : 0.;
+    launch_mlp_seed(d, s, dv);
+    sync(d);
+    return cudaGetLastError() == cudaSuccess ? 1 : 0;
 }
 
 // refinement steps and FP64 take-overs of the instance's refined continuity solves
