@@ -57,6 +57,11 @@ def parse():
     ap.add_argument("--precision", default="refined", choices=["refined", "fp64"],
                     help="linear solves: FP32 refined in FP64 (default) or FP64 throughout")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison steps")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor step")
+    ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "diodes64"],
+                    help="nmosfet: the Id-Vg workload (default); diodes64: the 64 pn-diode variants batch")
+    ap.add_argument("--workers", type=int, default=0, help="diodes64: concurrent host threads (0: one per variant)")
+    ap.add_argument("--variants", type=int, default=0, help="diodes64: only the first n variants (0: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bounded CPU-baseline sample (s)")
     ap.add_argument("--no-profile", action="store_true")
@@ -270,8 +275,10 @@ class Sweeper:
         self._use()
         self.lib.b200x_stream_timer(0)
         t0 = time.perf_counter()
+        g0 = self.lib.api3_get_stat(3)
         self.cur = []
         self.npts, self.conv = sweep_points(self.lib, self.w, self.w.sweeps[self.si], fields=fields, out=self.cur)
+        self.gummel = self.lib.api3_get_stat(3) - g0
         self.dev_s = self.lib.b200x_stream_timer(1) / 1e3
         self.wall = time.perf_counter() - t0
 
@@ -284,15 +291,64 @@ def concurrent(workers, fn):
         t.join()
 
 
-def rel_dI(cur, ref):
+def rel_dI(cur, ref, on=1e-30):
     """Largest |I - I_ref| / |I_ref| over the points both lists hold, on terminals whose
-    reference current is above its own round-off floor (and above 1e-30 A)."""
+    reference current is above its own round-off floor and above `on` amperes."""
     worst = 0.0
     for (I, _), (Ir, Fr) in zip(cur, ref):
         for x, y, f in zip(I, Ir, Fr):
-            if abs(y) > max(f, 1e-30):
+            if abs(y) > max(f, on):
                 worst = max(worst, abs(x - y) / abs(y))
     return worst
+
+
+def learned_step(a, lib, workers, step, cur, gummel_per_step, dist):
+    """Train the learned predictor on the workload device's own sweeps at gate voltages
+    shifted by half a step (both drain biases), then run one step of the workload with
+    it.  Returns the measured block (seed error, Gummel iterations, points/s)."""
+    import torch
+    from semiconductor_devices_simulator_b200 import learned as LR
+    s0 = workers[0]
+    s0._use()
+    t0 = time.perf_counter()
+    feats, targs = [], []
+    for sw in s0.w.sweeps:
+        s2 = dict(sw)
+        s2["V"] = np.round(sw["V"] + 0.5 * (sw["V"][1] - sw["V"][0]), 12)
+        Vs, Xs, ok = LR.collect(lib, s0.w, s2)
+        f, t = LR.pair_data(lib, torch, Vs, Xs, per_pair=131072)
+        feats.append(f)
+        targs.append(t)
+    t_data = time.perf_counter() - t0
+    tr = LR.Trainer(lib, torch, batch=16384, seed=0)
+    tr.fit(torch.cat(feats), torch.cat(targs), steps=6000, lr=1e-3, lr_end=1e-4)
+    params = tr.params()
+    for s in workers:                           # the workload's own points, as a held-out set
+        s._use()
+        s.prepare()
+        LR.load(lib, params)
+        lib.api3b_seed_enable(1)
+    dist.barrier()
+    t1 = time.perf_counter()
+    concurrent(workers, lambda s: s.run(False))
+    wall = time.perf_counter() - t1
+    dev = max(s.dev_s for s in workers)
+    pts = sum(s.npts for s in workers)
+    used = []
+    for s in workers:
+        s._use()
+        used.append(LR.stats(lib))
+        lib.api3b_seed_enable(0)
+    curl = {s.si: list(s.cur) for s in workers}
+    return {"points_per_s": round(pts / dev, 4), "unit": UNIT,
+            "gummel_iterations_per_step": {"linear_guess": gummel_per_step,
+                                           "learned_guess": sum(s.gummel for s in workers)},
+            "seeded_steps": int(sum(u[0] for u in used)), "fallbacks": int(sum(u[1] for u in used)),
+            "max_rel_dI_vs_linear_on_state": max(rel_dI(curl[k], cur[k], on=1e-9) for k in cur),
+            "train": {"rows": int(sum(f.shape[0] for f in feats)), "steps": 6000, "seconds": round(tr.seconds, 2),
+                      "data_seconds": round(t_data, 1)},
+            "note": "not in `value`: at this 0.05 V step the Gummel iteration count is set by the loop's "
+                    "convergence tail, not by the starting guess"}
 
 
 def run_b200(a, dist):
@@ -352,18 +408,32 @@ def run_b200(a, dist):
             lib.b200x_prof_read(k, abi.dptr(ms), abi.dptr(cnt), abi.dptr(by))
             rows.append((lib.b200x_prof_name(k).decode(), float(ms[0]), int(cnt[0]), float(by[0])))
         prof = rows
-    # the plain FP64 GPU path on the same steps (own instances, one warm-up step)
+    gummel = sum(s.gummel for s in workers)
+    # the FP64 GPU path on the same steps (own instances, one warm-up step): batched (both
+    # sweeps at once, as above) and plain (one sweep after the other, one instance at a time)
     f64 = None
     if prec == 1 and not a.no_fp64:
         w64 = make(0)
         step(w64)
-        f_pts = 0
-        f_dev = 0.0
+        f_pts = s_pts = 0
+        f_dev = s_dev = 0.0
         for i in range(a.steps):
             npts, conv, dev_s, wall = step(w64)
             f_pts += npts; f_dev += dev_s
         cur64 = {s.si: list(s.cur) for s in w64}
-        f64 = (dist.sum(f_pts), dist.max(f_dev), max(rel_dI(cur[k], cur64[k]) for k in cur))
+        for i in range(a.steps):
+            for s in w64:
+                s.prepare()
+                dist.barrier()
+                s.run(False)
+                s_pts += s.npts; s_dev += s.dev_s
+        f64 = (dist.sum(f_pts), dist.max(f_dev), max(rel_dI(cur[k], cur64[k]) for k in cur),
+               dist.sum(s_pts), dist.max(s_dev), max(rel_dI(cur[k], cur64[k], on=1e-9) for k in cur))
+    # the learned predictor: trained (untimed) on this device's own solutions at gate
+    # voltages half a step off the workload's, then one step of the workload seeded by it
+    learned = None
+    if not a.no_learned:
+        learned = learned_step(a, lib, workers, step, cur, gummel / max(a.steps, 1), dist)
     T = dist.max(tot_dev)
     pts_all = dist.sum(tot_pts)
     e_T = dist.max(e_wall)
@@ -410,9 +480,16 @@ def run_b200(a, dist):
             "clocks": clk,
         }
         if f64:
-            out["plain_fp64"] = {"value": round(f64[0] / f64[1], 4), "unit": UNIT,
-                                 "speedup": round(value / (f64[0] / f64[1]), 3),
-                                 "max_rel_dI_vs_fp64": f64[2]}
+            out["plain_fp64"] = {"value": round(f64[3] / f64[4], 4), "unit": UNIT,
+                                 "what": "FP64 solves, one sweep at a time (no concurrent instances), linear guess",
+                                 "speedup": round(value / (f64[3] / f64[4]), 3)}
+            out["fp64_batched"] = {"value": round(f64[0] / f64[1], 4), "unit": UNIT,
+                                   "speedup": round(value / (f64[0] / f64[1]), 3)}
+            out["max_rel_dI_vs_fp64"] = {"all_points": f64[2], "on_state_Id_gt_1nA": f64[5],
+                                         "note": "both at the workload's default tolerances; terminals above "
+                                                 "their round-off floor"}
+        if learned:
+            out["learned_seed"] = learned
         if dist.world == 1 and not a.no_cpu_baseline:
             cb = cpu_baseline(mesh, a.cpu_seconds)
             if cb:
@@ -459,12 +536,91 @@ def run_reference(a, dist):
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_batch(a, dist):
+    """The batching workload: the 64 pn-diode variants (node counts 32^3..72^3, doping
+    log-uniform in 1e15..1e18 cm^-3, junction depth 0.2..0.8 um, recorded seed), each swept
+    0..0.7 V in 25 mV steps, one solver instance (own CUDA stream) per variant and
+    `workers` host threads driving them at once (0: one per variant).  Untimed: device
+    set-up, equilibrium and the first point of every sweep; timed (wall clock, max over
+    ranks): the remaining 28 points of every sweep.  Ranks take every world-th variant."""
+    import queue
+    import semiconductor_devices_simulator_b200 as S
+    lib = S.load()
+    lib.b200x_set_device(dist.local)
+    prec = 1 if a.precision == "refined" else 0
+    var = D.diode_variants(64)[dist.rank::dist.world][:a.variants or None]
+    hs = [lib.api3b_new() for _ in var]
+    ws = [None] * len(var)
+
+    def setup(q):
+        lib.api3b_use(hs[q])
+        lib.b200x_set_device(dist.local)
+        lib.api3b_set_precision(prec)
+        ws[q] = D.diode_variant(lib, var[q])
+        ok = D.start_sweep(lib, ws[q], ws[q].sweeps[0])
+        lib.api3b_use(0)
+        return ok
+
+    def pool(fn, n, W):
+        jobs = queue.Queue()
+        for q in range(n):
+            jobs.put(q)
+        res = [None] * n
+
+        def loop():
+            while True:
+                try:
+                    q = jobs.get_nowait()
+                except queue.Empty:
+                    return
+                res[q] = fn(q)
+        th = [threading.Thread(target=loop) for _ in range(W)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        return res
+
+    W = a.workers or len(var)
+    pool(setup, len(var), W)
+
+    def run(q):
+        lib.api3b_use(hs[q])
+        n, c = sweep_points(lib, ws[q], ws[q].sweeps[0])
+        lib.api3b_use(0)
+        return n, c
+    dist.barrier()
+    t0 = time.perf_counter()
+    res = pool(run, len(var), W)
+    wall = time.perf_counter() - t0
+    pts = sum(r[0] for r in res)
+    conv = sum(r[1] for r in res)
+    T = dist.max(wall)
+    pts_all = dist.sum(pts)
+    nodes = [int(np.prod(v["n"])) for v in var]
+    for h in hs:
+        lib.api3b_free(h)
+    if dist.rank != 0:
+        return None
+    return {"metric": "I-V bias points/s (64 pn-diode variants, one instance and stream each)",
+            "value": round(pts_all / T, 3), "unit": UNIT, "n_gpus": dist.world, "higher_is_better": True,
+            "scaling": "weak" if dist.world > 1 else "strong", "wall_s": round(T, 3), "points": int(pts_all),
+            "converged_points": conv, "dtype": "f32 inner solves refined in f64" if prec else "f64",
+            "config": {"workload": "pn_diode_variants_64", "variants": len(var), "workers": W,
+                       "nodes_min": min(nodes), "nodes_max": max(nodes), "nodes_total": sum(nodes),
+                       "sweep_V": [0.0, 0.7, 0.025], "precision": a.precision,
+                       "timing": "wall clock around all sweeps (host control included)"}}
+
+
 def main():
     a = parse()
     if a.probe:
         return run_probe(a)
     dist = Dist()
-    out = run_reference(a, dist) if a.impl == "reference" else run_b200(a, dist)
+    if a.workload == "diodes64" and a.impl != "reference":
+        out = run_batch(a, dist)
+    else:
+        out = run_reference(a, dist) if a.impl == "reference" else run_b200(a, dist)
     if dist.rank == 0 and out is not None:
         print(json.dumps(out))
     dist.close()

@@ -215,6 +215,15 @@ static int gpu_alloc(Inst &d) {
         g_device = e ? std::atoi(e) : 0;
     }
     CK(cudaSetDevice(g_device));
+    static bool sync_set = false;             // host wait mode, once per process (SEMISIM_B200_SYNC)
+    if (!sync_set) {
+        sync_set = true;
+        if (const char *m = std::getenv("SEMISIM_B200_SYNC")) {
+            const unsigned fl = !std::strcmp(m, "blocking") ? cudaDeviceScheduleBlockingSync
+                                : !std::strcmp(m, "yield") ? cudaDeviceScheduleYield : cudaDeviceScheduleSpin;
+            if (cudaSetDeviceFlags(fl) != cudaSuccess) cudaGetLastError();   // an active context keeps its mode
+        }
+    }
     int dims[MAXLEV][6];
     const int nl = mg_levels(d.Nx, d.Ny, d.Nz, dims);
     Carver cv;
