@@ -58,6 +58,7 @@ def parse():
                     help="linear solves: FP32 refined in FP64 (default) or FP64 throughout")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison steps")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor step")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuner)")
     ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "diodes64"],
                     help="nmosfet: the Id-Vg workload (default); diodes64: the 64 pn-diode variants batch")
     ap.add_argument("--workers", type=int, default=0, help="diodes64: concurrent host threads (0: one per variant)")
@@ -384,6 +385,15 @@ def run_b200(a, dist):
         wall = time.perf_counter() - t0
         return (sum(s.npts for s in ws), sum(s.conv for s in ws), max(s.dev_s for s in ws), wall)
 
+    tune = None
+    if not a.no_autotune:                     # launch shapes, one instance at a time (untimed)
+        for s in workers:
+            s.prepare()
+            us = lib.api3b_autotune(2)
+        r, g, sm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib.api3b_tune_get(ctypes.byref(r), ctypes.byref(g), ctypes.byref(sm))
+        tune = {"rows_per_block": r.value, "grid_cap": g.value, "small_level_nodes": sm.value or 2048,
+                "vcycle_us": round(us, 2)}
     for i in range(a.warmup):
         step(workers)
     w = workers[0].w
@@ -480,7 +490,7 @@ def run_b200(a, dist):
             "config": {"workload": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]}_idvg",
                        "nodes": w.N, "points_per_step": npts_step, "drain_biases_V": [0.05, 1.0],
                        "gate_sweep_V": [0.0, 1.2, 0.05], "models": 4, "solver": list(D.GUI_SOLVER),
-                       "precision": a.precision,
+                       "precision": a.precision, "launch_shapes": tune,
                        "parallelism": f"replicas{dist.world}, {nsw} concurrent sweeps per GPU (instance + stream each)",
                        "l2": "state of 576k nodes (~0.5 GB) exceeds the 126 MB L2; no flush"},
             "converged_points": tot_conv, "wall_s": round(tot_wall, 3),

@@ -257,6 +257,18 @@ int api3b_seed_enable(int on);
 void api3b_seed_stats(long long *used, long long *fallbacks);
 int api3b_seed_nparam(void);
 
+/* No counterpart in the reference.  Launch-shape autotuner of the current instance: rows
+   per block of the row-blocked multigrid passes, blocks of the grid-stride node kernels,
+   and the level size where the small-level kernel takes over, chosen by timing V-cycles of
+   the instance's own hierarchy (in the precision its solves use) on the GPU.
+     mode 0: default shapes; 1: tune now; 2: reuse the shapes cached for this mesh shape
+     and precision, tuning when there are none.  Call after the instance's first solve,
+     with no other GPU work of the process running.  Returns the chosen V-cycle time in
+     microseconds (0 for mode 0, -1 before the first solve).
+   api3b_tune_get: the shapes in use; returns 1 when they came from the tuner. */
+double api3b_autotune(int mode);
+int api3b_tune_get(int *rpb, int *grid_cap, int *small_nodes);
+
 /* No counterpart in the reference.  For callers that cannot allocate device memory
    (their memory belongs to another allocator, or a cudaMalloc / cudaFree on their path is
    not acceptable): r = b - A x for a 7-point stencil A (7 arrays of N = Nx*Ny*Nz doubles:

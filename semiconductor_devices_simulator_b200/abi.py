@@ -126,6 +126,9 @@ EXTRA = {
     "api3b_seed_enable": (_I, [_I]),
     "api3b_seed_stats": (None, [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "api3b_seed_nparam": (_I, []),
+    # launch-shape autotuner of the current instance
+    "api3b_autotune": (_D, [_I]),
+    "api3b_tune_get": (_I, [ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
 }
 
 

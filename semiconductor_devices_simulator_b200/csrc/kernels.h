@@ -26,7 +26,9 @@ struct Ctx {
     int ninst = 1;
     int maxN = 0;
     cudaStream_t st = 0;
-    int grid_cap = 148 * 8;
+    int grid_cap = 148 * 8;     // blocks of the grid-stride node kernels (<= RED_MAX_BLOCKS)
+    int rpb = 4;                // rows per block of the row-blocked level passes (block 32 x rpb)
+    int small_nodes = 0;        // levels at or below this size go to the small-level kernel (0: default)
     int nodes_blocks() const;
 };
 

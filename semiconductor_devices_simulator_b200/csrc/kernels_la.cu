@@ -215,17 +215,16 @@ __device__ __forceinline__ Agg agg_range(const V &f, int I, int J, int K) {
     return g;
 }
 
-// Row-blocked launch shape of the level passes: block (32, 4), threadIdx.x along x (the
-// x index, or the half-row index of a colour), threadIdx.y + 4 blockIdx.z the grid row
-// j + Ny l, so no thread divides its linear index.
-constexpr int ROWS_PER_BLOCK = 4;
+// Row-blocked launch shape of the level passes: block (32, rpb), threadIdx.x along x (the
+// x index, or the half-row index of a colour), threadIdx.y + rpb blockIdx.z the grid row
+// j + Ny l, so no thread divides its linear index (rpb: Ctx, set by the autotuner).
 #define SS_ROW_LOOP(row, rows) \
-    for (int row = blockIdx.z * ROWS_PER_BLOCK + threadIdx.y; row < (rows); row += gridDim.z * ROWS_PER_BLOCK)
+    for (int row = blockIdx.z * blockDim.y + threadIdx.y; row < (rows); row += gridDim.z * blockDim.y)
 
 // x += alpha pw P xc (semiconductor_3d.c:2038-2048); the residual that follows needs
 // every prolonged neighbour and is a separate pass
 template <class T>
-__global__ void __launch_bounds__(128) k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha,
+__global__ void __launch_bounds__(256) k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha,
                                                  int gate) {
     pdl_entry();
     const DevP &P = Ps[blockIdx.y];
@@ -244,7 +243,7 @@ __global__ void __launch_bounds__(128) k_prolong(const DevP *__restrict__ Ps, in
     }
 }
 template <class T>
-__global__ void __launch_bounds__(128) k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
+__global__ void __launch_bounds__(256) k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
     pdl_entry();
     const DevP &P = Ps[blockIdx.y];
     if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
@@ -514,7 +513,7 @@ __device__ __forceinline__ void smooth_node(const LevView<T> &v, int k, int i, i
 // Half sweep over the nodes of one colour: thread ti of row (j, l) takes
 // i = 2 ti + ((j + l + colour) & 1), so every lane does work.
 template <class T, int MODE, int COLOR>
-__global__ void __launch_bounds__(128) k_smooth_cm(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
+__global__ void __launch_bounds__(256) k_smooth_cm(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
     constexpr int mode = MODE, color = COLOR;
     pdl_entry();
     const DevP &P = Ps[blockIdx.y];
@@ -876,19 +875,20 @@ static void launch_small(const Ctx &c, int nodes, int Ls, int bsel, int xsel, in
     if (g_prof_on) prof_end(pf<T>(PF_COARSE), c.st, nodes);
 }
 
-// row-blocked grids (block (32, ROWS_PER_BLOCK)): x extent `nx`, all rows of level L
+// row-blocked grids (block (32, c.rpb)): x extent `nx`, all rows of level L
 static inline dim3 grid_rows(const Ctx &c, int L, const MGHost &mg, int nx) {
-    int gz = (mg.maxRows[L] + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK;
+    int gz = (mg.maxRows[L] + c.rpb - 1) / c.rpb;
     if (gz > 65535) gz = 65535;
     return dim3((nx + 31) / 32, c.ninst, gz > 0 ? gz : 1);
 }
 static inline dim3 grid_half(const Ctx &c, int L, const MGHost &mg) { return grid_rows(c, L, mg, (mg.maxNx[L] + 1) / 2); }
 static inline dim3 grid_full(const Ctx &c, int L, const MGHost &mg) { return grid_rows(c, L, mg, mg.maxNx[L]); }
-static const dim3 ROW_BLOCK(32, ROWS_PER_BLOCK);
-static int small_split(const MGHost &mg) {
+#define ROW_BLOCK dim3(32, c.rpb)
+static int small_split(const Ctx &c, const MGHost &mg) {
     small_init();
+    const int lim = c.small_nodes > 0 ? c.small_nodes : g_small_nodes;
     int Ls = 0;
-    while (Ls < mg.maxlev - 1 && mg.maxN[Ls] > g_small_nodes) Ls++;
+    while (Ls < mg.maxlev - 1 && mg.maxN[Ls] > lim) Ls++;
     return Ls;
 }
 // shared-memory bytes of levels Ls.. of the shared-memory small-level kernel
@@ -902,8 +902,8 @@ static size_t smem_bytes(const MGHost &mg, int Ls) {
 // first one at or below g_small_nodes whose data fits (never level 0); *smem = its bytes,
 // 0 when the cluster kernel takes the small levels instead
 template <class T>
-static int small_plan(const MGHost &mg, size_t *smem) {
-    int Ls = small_split(mg);
+static int small_plan(const Ctx &c, const MGHost &mg, size_t *smem) {
+    int Ls = small_split(c, mg);
     *smem = 0;
     if (!g_smem_max || mg.maxlev < 2) return Ls;
     int L = Ls < 1 ? 1 : Ls;
@@ -940,7 +940,7 @@ static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wse
         return;
     }
     size_t smem = 0;
-    const int Ls = small_plan<T>(mg, &smem);
+    const int Ls = small_plan<T>(c, mg, &smem);
     for (int L = 0; L < Ls; L++) {
         SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(0, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(0, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
@@ -1643,7 +1643,7 @@ double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
     cudaMemcpy(c.h.ks, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice);
     cudaMemcpy(c.h.ksi, &ks0, sizeof(KrylovS), cudaMemcpyHostToDevice);
     size_t sm64 = 0, sm32 = 0;
-    const int Ls64 = small_plan<double>(mg, &sm64), Ls32 = small_plan<float>(mg, &sm32);
+    const int Ls64 = small_plan<double>(c, mg, &sm64), Ls32 = small_plan<float>(c, mg, &sm32);
     if (which >= 11) {
         mg_setup_t<float>(c, mg, 1);
         cudaStreamSynchronize(c.st);

@@ -59,6 +59,9 @@ Ctx make_ctx(Inst &d) {
     c.maxN = (int)d.N;
     c.st = d.g.st;
     c.lg = &d.g.lg;
+    c.rpb = d.tune.rpb;
+    c.grid_cap = d.tune.grid_cap;
+    c.small_nodes = d.tune.small_nodes;
     return c;
 }
 

@@ -52,6 +52,15 @@ struct Gpu {
 
 struct TrapSpec { int type, ref; double E, sn, sp; };   // deep-level species (stored, not solved)
 
+// launch shapes of an instance's linear-algebra kernels (picked by api3b_autotune)
+struct Tune {
+    int rpb = 4;                  // rows per block of the row-blocked level passes
+    int grid_cap = 148 * 8;       // blocks of the grid-stride node kernels
+    int small_nodes = 0;          // size at which the small-level kernel takes over (0: default)
+    int tuned = 0;
+    double us = 0.0;              // V-cycle time of the chosen shapes (microseconds)
+};
+
 struct Inst {
     // ---- configuration (the reference's Dev, semiconductor_3d.c:234-364)
     int Nx = 0, Ny = 0, Nz = 0;
@@ -83,6 +92,7 @@ struct Inst {
     int aa_m = 0, aa_n = 0, aa_pos = 0, aa_have = 0;
     int precision = -1;               // linear solves: 0 FP64, 1 FP32 refined in FP64, -1 library default
     long long ir_steps = 0, ir_fallbacks = 0;
+    Tune tune;
     int seed_on = 0;                  // learned sweep predictor enabled (needs a loaded model)
     long long seed_used = 0, seed_fallbacks = 0;
     // ---- derived by prepare (host copies)

@@ -189,3 +189,28 @@ def test_pn_diode_40cubed_matches_reference(lib, monkeypatch):
     g0, r0 = out["gpu", 0], out["ref", 0]
     check_currents(g0[2], r0[2], np.maximum(r0[3], 2.0 * np.abs(r0[2] - r1[2])))
     assert np.abs(g0[5] - r0[5]).max() <= PSI_TOL
+
+
+@pytest.mark.parametrize("name", ["mos_small"])
+def test_autotuned_shapes_keep_parity(lib, name):
+    """Launch shapes picked by the autotuner (after the first solve) change no answer: the
+    sweep still matches the reference within its error bar."""
+    import ctypes
+    g = golden(name)
+    w, mat, bias = MG.build(lib, name)
+    lib.api3b_set_precision(1)
+    s = w.sweeps[0]
+    try:
+        assert D.start_sweep(lib, w, s)
+        us = lib.api3b_autotune(1)
+        r, gc, sm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        assert lib.api3b_tune_get(ctypes.byref(r), ctypes.byref(gc), ctypes.byref(sm)) == 1
+        assert us > 0.0 and r.value in (2, 4, 8) and gc.value in (592, 1184, 1776) and sm.value in (0, 1024, 2048, 4096, 8192)
+        ok0, V, I, F, conv, psi, n, p = sweep_fields(lib, w, s)
+        assert ok0 and conv.all()
+        own = 2.0 * np.abs(g["sw0_I"] - g["swt0_I"])
+        check_currents(I, g["sw0_I"], np.maximum(g["sw0_Iflr"], own))
+        assert np.abs(psi - g["sw0_psi"]).max() <= PSI_TOL
+    finally:
+        lib.api3b_autotune(0)
+        lib.api3b_set_precision(-1)
