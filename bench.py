@@ -390,10 +390,10 @@ def run_b200(a, dist):
         for s in workers:
             s.prepare()
             us = lib.api3b_autotune(2)
-        r, g, sm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        lib.api3b_tune_get(ctypes.byref(r), ctypes.byref(g), ctypes.byref(sm))
-        tune = {"rows_per_block": r.value, "grid_cap": g.value, "small_level_nodes": sm.value or 2048,
-                "vcycle_us": round(us, 2)}
+        r, g, sm, zc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib.api3b_tune_get(ctypes.byref(r), ctypes.byref(g), ctypes.byref(sm), ctypes.byref(zc))
+        tune = {"rows_per_block": r.value, "row_blocks_max": zc.value, "grid_cap": g.value,
+                "small_level_nodes": sm.value or 2048, "vcycle_us": round(us, 2)}
     for i in range(a.warmup):
         step(workers)
     w = workers[0].w

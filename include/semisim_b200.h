@@ -265,9 +265,10 @@ int api3b_seed_nparam(void);
      and precision, tuning when there are none.  Call after the instance's first solve,
      with no other GPU work of the process running.  Returns the chosen V-cycle time in
      microseconds (0 for mode 0, -1 before the first solve).
-   api3b_tune_get: the shapes in use; returns 1 when they came from the tuner. */
+   api3b_tune_get: the shapes in use (zcap: most row blocks per pass; may be null); returns
+   1 when they came from the tuner. */
 double api3b_autotune(int mode);
-int api3b_tune_get(int *rpb, int *grid_cap, int *small_nodes);
+int api3b_tune_get(int *rpb, int *grid_cap, int *small_nodes, int *zcap);
 
 /* No counterpart in the reference.  For callers that cannot allocate device memory
    (their memory belongs to another allocator, or a cudaMalloc / cudaFree on their path is

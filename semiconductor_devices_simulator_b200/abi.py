@@ -128,7 +128,7 @@ EXTRA = {
     "api3b_seed_nparam": (_I, []),
     # launch-shape autotuner of the current instance
     "api3b_autotune": (_D, [_I]),
-    "api3b_tune_get": (_I, [ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "api3b_tune_get": (_I, [ctypes.POINTER(_I)] * 4),
 }
 
 

@@ -803,6 +803,7 @@ __global__ void __launch_bounds__(SMALL_TPB) k_vcycle_smem(const DevP *__restric
 
 int g_small_nodes = 2048;           // levels at or below this size run in the cluster kernel
 int g_l0_sweeps = 2;                // red-black applications per smoothing step on the finest level
+int g_deep_levels = 1;              // levels (from the finest) that get the second application
 static int g_cluster = 0;           // CTAs per cluster of the small-level kernel (set on first use)
 static size_t g_smem_max = 0;       // dynamic shared memory of the shared-memory small-level kernel (0: off)
 
@@ -834,6 +835,7 @@ static void small_init() {
         int cl = (e && std::atoi(e) == 8) ? 8 : 16;
         if (const char *s = std::getenv("SEMISIM_B200_SMALL")) g_small_nodes = std::atoi(s);
         if (const char *s = std::getenv("SEMISIM_B200_L0SWEEPS")) g_l0_sweeps = std::atoi(s) > 1 ? 2 : 1;
+        if (const char *s = std::getenv("SEMISIM_B200_DEEP")) g_deep_levels = std::atoi(s) < 1 ? 1 : std::atoi(s);
         const bool ok64 = cluster16_ok<double>(), ok32 = cluster16_ok<float>();
         if (!ok64 || !ok32) cl = 8;
         g_cluster = cl;
@@ -878,6 +880,7 @@ static void launch_small(const Ctx &c, int nodes, int Ls, int bsel, int xsel, in
 // row-blocked grids (block (32, c.rpb)): x extent `nx`, all rows of level L
 static inline dim3 grid_rows(const Ctx &c, int L, const MGHost &mg, int nx) {
     int gz = (mg.maxRows[L] + c.rpb - 1) / c.rpb;
+    if (gz > c.zcap) gz = c.zcap;
     if (gz > 65535) gz = 65535;
     return dim3((nx + 31) / 32, c.ninst, gz > 0 ? gz : 1);
 }
@@ -944,7 +947,7 @@ static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wse
     for (int L = 0; L < Ls; L++) {
         SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(0, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(0, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
-        if (L == 0 && g_l0_sweeps > 1) {     // second application on the finest level
+        if (L < g_deep_levels && g_l0_sweeps > 1) {     // second application (finest levels)
             SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(2, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
             SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(2, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         }
@@ -961,7 +964,7 @@ static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wse
                   xsel, gate);
         SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(1, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(1, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
-        if (L == 0 && g_l0_sweeps > 1) {
+        if (L < g_deep_levels && g_l0_sweeps > 1) {
             SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(2, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
             SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(2, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         }

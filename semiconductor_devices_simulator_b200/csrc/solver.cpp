@@ -62,6 +62,7 @@ Ctx make_ctx(Inst &d) {
     c.rpb = d.tune.rpb;
     c.grid_cap = d.tune.grid_cap;
     c.small_nodes = d.tune.small_nodes;
+    c.zcap = d.tune.zcap;
     return c;
 }
 

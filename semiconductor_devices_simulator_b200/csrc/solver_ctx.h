@@ -57,6 +57,7 @@ struct Tune {
     int rpb = 4;                  // rows per block of the row-blocked level passes
     int grid_cap = 148 * 8;       // blocks of the grid-stride node kernels
     int small_nodes = 0;          // size at which the small-level kernel takes over (0: default)
+    int zcap = 65535;             // most row blocks of one row-blocked pass
     int tuned = 0;
     double us = 0.0;              // V-cycle time of the chosen shapes (microseconds)
 };

@@ -203,8 +203,9 @@ def test_autotuned_shapes_keep_parity(lib, name):
     try:
         assert D.start_sweep(lib, w, s)
         us = lib.api3b_autotune(1)
-        r, gc, sm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        assert lib.api3b_tune_get(ctypes.byref(r), ctypes.byref(gc), ctypes.byref(sm)) == 1
+        r, gc, sm, zc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        assert lib.api3b_tune_get(ctypes.byref(r), ctypes.byref(gc), ctypes.byref(sm), ctypes.byref(zc)) == 1
+        assert zc.value in (65535, 296, 148)
         assert us > 0.0 and r.value in (2, 4, 8) and gc.value in (592, 1184, 1776) and sm.value in (0, 1024, 2048, 4096, 8192)
         ok0, V, I, F, conv, psi, n, p = sweep_fields(lib, w, s)
         assert ok0 and conv.all()
