@@ -74,7 +74,8 @@ def parse():
 
 
 def run_probe(a):
-    """Few-launch case for ncu: the workload's device, one electron continuity system."""
+    """Few-launch case for ncu: the workload's device, one electron continuity system
+    (multigrid set-up and `ITS` BiCGSTAB iterations), then one learned-seed pass."""
     import semiconductor_devices_simulator_b200 as S
     mesh = tuple(int(v) for v in a.mesh.split(","))
     lib = S.load()
@@ -89,8 +90,14 @@ def run_probe(a):
     lib.b200x_cont_assemble(0, None, None, None, None)
     rn, r0 = np.zeros(1), np.zeros(1)
     its = lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
+    # one pass of the learned predictor's seed kernel (untrained weights) on the same device
+    from semiconductor_devices_simulator_b200 import learned as LR
+    LR.load(lib, LR.init_params(lib.api3b_seed_nparam(), seed=0, out_scale=1.0))
+    lib.api3b_seed_enable(0)
+    dv = np.array([0.0, 0.0, 0.05, 0.0])
+    seed_ok = lib.b200x_seed_run(1.0, abi.dptr(dv))
     print(json.dumps({"probe": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]} electron continuity", "nodes": w.N,
-                      "precision": a.precision,
+                      "precision": a.precision, "seed_kernel": seed_ok,
                       "bicgstab_its": its, "r0": r0[0], "rn": rn[0],
                       "launches": int(lib.b200x_launches() - l0)}))
 

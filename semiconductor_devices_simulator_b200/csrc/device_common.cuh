@@ -18,6 +18,12 @@ __device__ __forceinline__ void pdl_entry() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     asm volatile("griddepcontrol.wait;" ::: "memory");
 }
+// The two halves, for kernels that first read set-up data (instance and level records,
+// array pointers, sizes: written only by host copies, never by a kernel) and only then
+// wait: those loads overlap the previous kernel's tail.  Every path calls pdl_wait()
+// before it reads kernel-written memory and before it returns.
+__device__ __forceinline__ void pdl_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 template <int NV>
 __device__ __forceinline__ void warp_sum(double (&v)[NV]) {

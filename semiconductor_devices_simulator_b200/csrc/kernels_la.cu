@@ -226,11 +226,13 @@ __device__ __forceinline__ Agg agg_range(const V &f, int I, int J, int K) {
 template <class T>
 __global__ void __launch_bounds__(256) k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha,
                                                  int gate) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
     const LevView<T> f = levview<T>(P, L, bsel, xsel);
-    const LevelT<T> &cl = PT<T>::lev(P, L + 1);
+    const LevelT<T> cl = PT<T>::lev(P, L + 1 < MAXLEV ? L + 1 : L);
+    const int nl = P.nlev;
+    pdl_wait();
+    if (L >= nl - 1 || gated_off<T>(P, gate)) return;
     const T al = (T)alpha;
     const int i = blockIdx.x * 32 + threadIdx.x;
     if (i >= f.Nx) return;
@@ -244,10 +246,12 @@ __global__ void __launch_bounds__(256) k_prolong(const DevP *__restrict__ Ps, in
 }
 template <class T>
 __global__ void __launch_bounds__(256) k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
     const LevView<T> f = levview<T>(P, L, bsel, xsel);
+    const int nl = P.nlev;
+    pdl_wait();
+    if (L >= nl - 1 || gated_off<T>(P, gate)) return;
     const int i = blockIdx.x * 32 + threadIdx.x;
     if (i >= f.Nx) return;
     SS_ROW_LOOP(row, f.Ny * f.Nz) {
@@ -515,10 +519,12 @@ __device__ __forceinline__ void smooth_node(const LevView<T> &v, int k, int i, i
 template <class T, int MODE, int COLOR>
 __global__ void __launch_bounds__(256) k_smooth_cm(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
     constexpr int mode = MODE, color = COLOR;
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if ((L > 0 && L >= P.nlev - 1) || gated_off<T>(P, gate)) return;
     const LevView<T> v = levview<T>(P, L, bsel, xsel);
+    const int nl = P.nlev;
+    pdl_wait();
+    if ((L > 0 && L >= nl - 1) || gated_off<T>(P, gate)) return;
     const int ti = blockIdx.x * 32 + threadIdx.x;
     if (2 * ti >= v.Nx) return;
     SS_ROW_LOOP(row, v.Ny * v.Nz) {
@@ -547,12 +553,14 @@ static SmoothFn<T> smooth_fn(int mode, int color) {
 template <class T>
 __global__ void __launch_bounds__(128) k_resid_restrict2(const DevP *__restrict__ Ps, int L, int bsel, int xsel,
                                                          int wsel, int gate) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (L >= P.nlev - 1 || gated_off<T>(P, gate)) return;
     const LevView<T> f = levview<T>(P, L, bsel, xsel);
-    const LevelT<T> &cl = PT<T>::lev(P, L + 1);
+    const LevelT<T> cl = PT<T>::lev(P, L + 1 < MAXLEV ? L + 1 : L);
     const T *w = (L == 0 && wsel) ? PT<T>::w0(P) : nullptr;
+    const int nl = P.nlev;
+    pdl_wait();
+    if (L >= nl - 1 || gated_off<T>(P, gate)) return;
     const int R = blockIdx.z;                         // coarse row J + Cy*Lc
     const bool rowok = R < cl.Ny * cl.Nz;
     const int Lc = rowok ? R / cl.Ny : 0, Jc = rowok ? R - Lc * cl.Ny : 0;
@@ -1002,10 +1010,11 @@ __global__ void k_pcg32_start(const DevP *__restrict__ Ps) {
 // rz = r.z; mode 0 initial (rz0), mode 1 iteration end (stop test, beta)
 template <class T>
 __global__ void k_pcg_rz(const DevP *__restrict__ Ps, int mode) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (mode && !ks_running<T>(P)) return;
     const T *r = PT<T>::wk(P, 0), *z = PT<T>::wk(P, 1);
+    pdl_wait();
+    if (mode && !ks_running<T>(P)) return;
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) acc[0] += (double)r[k] * (double)z[k];
     if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
@@ -1025,23 +1034,25 @@ __global__ void k_pcg_rz(const DevP *__restrict__ Ps, int mode) {
 // p = z (init) or p = z + be p
 template <class T>
 __global__ void k_pcg_p(const DevP *__restrict__ Ps, int init) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running<T>(P)) return;
-    const T be = init ? T(0) : (T)PT<T>::ks(P)->be;
     T *p = PT<T>::wk(P, 2);
     const T *z = PT<T>::wk(P, 1);
+    pdl_wait();
+    if (!ks_running<T>(P)) return;
+    const T be = init ? T(0) : (T)PT<T>::ks(P)->be;
     SS_GRID_LOOP(k, P.N) p[k] = z[k] + (init ? T(0) : be * p[k]);
 }
 // q = A p; pq = p.q; al = rz / pq
 template <class T>
 __global__ void k_pcg_q(const DevP *__restrict__ Ps) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running<T>(P)) return;
     const T *p = PT<T>::wk(P, 2);
     T *q = PT<T>::wk(P, 3);
     T *const *A = PT<T>::A0(P);
+    pdl_wait();
+    if (!ks_running<T>(P)) return;
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) {
         const Node a = unidx(k, P.Nx, P.Ny);
@@ -1060,12 +1071,13 @@ __global__ void k_pcg_q(const DevP *__restrict__ Ps) {
 // x += al p; r -= al q
 template <class T>
 __global__ void k_pcg_xr(const DevP *__restrict__ Ps) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running<T>(P)) return;
-    const T al = (T)PT<T>::ks(P)->al;
     T *x = PT<T>::sol(P), *r = PT<T>::wk(P, 0);
     const T *p = PT<T>::wk(P, 2), *q = PT<T>::wk(P, 3);
+    pdl_wait();
+    if (!ks_running<T>(P)) return;
+    const T al = (T)PT<T>::ks(P)->al;
     SS_GRID_LOOP(k, P.N) { x[k] += al * p[k]; r[k] -= al * q[k]; }
 }
 // sol = (double) sol32 (end of an FP32 solve whose result is the whole solution)
@@ -1123,10 +1135,11 @@ __global__ void k_bicg_init(const DevP *__restrict__ Ps, double rtol, double ato
 // rho1 = rh.r; restart on breakdown; be
 template <class T>
 __global__ void k_bicg_rho(const DevP *__restrict__ Ps) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running<T>(P)) return;
     const T *r = PT<T>::wk(P, 0), *rh = PT<T>::wk(P, 1);
+    pdl_wait();
+    if (!ks_running<T>(P)) return;
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) acc[0] += (double)rh[k] * (double)r[k];
     if (grid_sum<1>(acc, P.part, P.ticket + 4)) {
@@ -1148,14 +1161,15 @@ __global__ void k_bicg_rho(const DevP *__restrict__ Ps) {
 // p = r + be (p - om v); on a restart rh = r, p = r, v = 0
 template <class T>
 __global__ void k_bicg_p(const DevP *__restrict__ Ps) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
+    T *p = PT<T>::wk(P, 2), *v = PT<T>::wk(P, 3), *rh = PT<T>::wk(P, 1);
+    const T *r = PT<T>::wk(P, 0);
+    pdl_wait();
     if (!ks_running<T>(P)) return;
     const KrylovS &s = *PT<T>::ks(P);
     const T be = (T)s.be, om = (T)s.om;
     const int restart = s.pad0;
-    T *p = PT<T>::wk(P, 2), *v = PT<T>::wk(P, 3), *rh = PT<T>::wk(P, 1);
-    const T *r = PT<T>::wk(P, 0);
     SS_GRID_LOOP(k, P.N) {
         if (restart) { rh[k] = r[k]; p[k] = r[k]; v[k] = 0; }
         else p[k] = r[k] + be * (p[k] - om * v[k]);
@@ -1164,12 +1178,13 @@ __global__ void k_bicg_p(const DevP *__restrict__ Ps) {
 // v = A ph; rv = rh.v; al
 template <class T>
 __global__ void k_bicg_v(const DevP *__restrict__ Ps) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running<T>(P)) return;
     const T *ph = PT<T>::wk(P, 4), *rh = PT<T>::wk(P, 1);
     T *v = PT<T>::wk(P, 3);
     T *const *A = PT<T>::A0(P);
+    pdl_wait();
+    if (!ks_running<T>(P)) return;
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) {
         const Node a = unidx(k, P.Nx, P.Ny);
@@ -1187,12 +1202,13 @@ __global__ void k_bicg_v(const DevP *__restrict__ Ps) {
 // r -= al v; ss = r.r; half-step exit test
 template <class T>
 __global__ void k_bicg_s(const DevP *__restrict__ Ps) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running<T>(P)) return;
-    const T al = (T)PT<T>::ks(P)->al;
     T *r = PT<T>::wk(P, 0);
     const T *v = PT<T>::wk(P, 3);
+    pdl_wait();
+    if (!ks_running<T>(P)) return;
+    const T al = (T)PT<T>::ks(P)->al;
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) {
         const T t = r[k] - al * v[k];
@@ -1208,12 +1224,13 @@ __global__ void k_bicg_s(const DevP *__restrict__ Ps) {
 // t = A sh; tt = t.t; ts = t.r; om
 template <class T>
 __global__ void k_bicg_t(const DevP *__restrict__ Ps) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (!ks_running<T>(P) || PT<T>::ks(P)->half) return;
     const T *sh = PT<T>::wk(P, 5), *r = PT<T>::wk(P, 0);
     T *t = PT<T>::wk(P, 6);
     T *const *A = PT<T>::A0(P);
+    pdl_wait();
+    if (!ks_running<T>(P) || PT<T>::ks(P)->half) return;
     double acc[2] = {0.0, 0.0};
     SS_GRID_LOOP(k, P.N) {
         const Node a = unidx(k, P.Nx, P.Ny);
@@ -1231,14 +1248,15 @@ __global__ void k_bicg_t(const DevP *__restrict__ Ps) {
 // x += al ph + om sh; r -= om t; rr = r.r; stop tests (or the half-step x update)
 template <class T>
 __global__ void k_bicg_x(const DevP *__restrict__ Ps) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
+    T *x = PT<T>::sol(P), *r = PT<T>::wk(P, 0);
+    const T *ph = PT<T>::wk(P, 4), *sh = PT<T>::wk(P, 5), *t = PT<T>::wk(P, 6);
+    pdl_wait();
     if (!ks_running<T>(P)) return;
     const KrylovS &s0 = *PT<T>::ks(P);
     const T al = (T)s0.al, om = (T)s0.om;
     const int half = s0.half;
-    T *x = PT<T>::sol(P), *r = PT<T>::wk(P, 0);
-    const T *ph = PT<T>::wk(P, 4), *sh = PT<T>::wk(P, 5), *t = PT<T>::wk(P, 6);
     double acc[1] = {0.0};
     SS_GRID_LOOP(k, P.N) {
         if (half) { x[k] += al * ph[k]; continue; }
