@@ -743,14 +743,18 @@ __device__ __forceinline__ void blk_smooth(const LevView<T> &v, int color, int m
 template <class T>
 __global__ void __launch_bounds__(SMALL_TPB) k_vcycle_smem(const DevP *__restrict__ Ps, int Ls, double alpha,
                                                            int gate) {
-    pdl_entry();
+    pdl_launch();
     const DevP &P = Ps[blockIdx.y];
-    if (gated_off<T>(P, gate)) return;
     extern __shared__ __align__(16) unsigned char sraw[];
+    __shared__ LevView<T> sv[MAXLEV];             // the levels' views into shared memory
     const int nl = P.nlev;
+    if (threadIdx.x < nl - Ls) sv[threadIdx.x] = smem_view<T>(P, Ls + threadIdx.x, Ls, sraw);
+    pdl_wait();
+    if (gated_off<T>(P, gate)) return;
+    __syncthreads();
     for (int L = Ls; L < nl; L++) {               // stage the levels
         const LevelT<T> &g = PT<T>::lev(P, L);
-        const LevView<T> v = smem_view<T>(P, L, Ls, sraw);
+        const LevView<T> v = sv[L - Ls];
         if (g.last) {
             blk_copy<T>(v.D, g.D, g.N * g.N);
         } else {
@@ -762,25 +766,35 @@ __global__ void __launch_bounds__(SMALL_TPB) k_vcycle_smem(const DevP *__restric
     }
     __syncthreads();
     for (int L = Ls; L < nl - 1; L++) {
-        const LevView<T> v = smem_view<T>(P, L, Ls, sraw), cv = smem_view<T>(P, L + 1, Ls, sraw);
+        const LevView<T> v = sv[L - Ls], cv = sv[L + 1 - Ls];
         blk_smooth<T>(v, 1, 0);
         blk_smooth<T>(v, 0, 0);
-        for (int K = threadIdx.x; K < cv.N; K += blockDim.x) {   // residual summed into the aggregates
-            const Node c = unidx(K, cv.Nx, cv.Ny);
-            const Agg g = agg_range(v, c.i, c.j, c.l);
-            T sum = 0;
-            for (int l = g.l0; l <= g.l1; l++)
-                for (int j = g.j0; j <= g.j1; j++)
-                    for (int i = g.i0; i <= g.i1; i++) {
-                        const int k = i + v.Nx * (j + v.Ny * l);
-                        sum += v.b[k] - lv_apply<T>(v, v.x, k, i, j, l);
-                    }
-            cv.b[K] = sum;
+        // residual summed into the aggregates: 8 lanes per coarse node, lane bits (di, dj, dl)
+        // pick the fine node (the same summation order for every aggregate)
+        const int nK = ((cv.N + 3) >> 2) << 5;       // 8 lanes x coarse nodes, whole warps
+        for (int t = threadIdx.x; t < nK; t += blockDim.x) {
+            const int K = t >> 3, sub = t & 7;
+            T val = 0;
+            if (K < cv.N) {
+                const Node c = unidx(K, cv.Nx, cv.Ny);
+                const int di = sub & 1, dj = (sub >> 1) & 1, dl = sub >> 2;
+                const int i = v.cx ? 2 * c.i + di : c.i, j = v.cy ? 2 * c.j + dj : c.j, l = v.cz ? 2 * c.l + dl : c.l;
+                const bool ok = i < v.Nx && j < v.Ny && l < v.Nz && (v.cx || di == 0) && (v.cy || dj == 0) &&
+                                (v.cz || dl == 0);
+                if (ok) {
+                    const int k = i + v.Nx * (j + v.Ny * l);
+                    val = v.b[k] - lv_apply<T>(v, v.x, k, i, j, l);
+                }
+            }
+            val += __shfl_xor_sync(0xffffffffu, val, 1);
+            val += __shfl_xor_sync(0xffffffffu, val, 2);
+            val += __shfl_xor_sync(0xffffffffu, val, 4);
+            if (sub == 0 && K < cv.N) cv.b[K] = val;
         }
         __syncthreads();
     }
     {                                             // coarsest level: x = D^-1 b (dense inverse)
-        const LevView<T> v = smem_view<T>(P, nl - 1, Ls, sraw);
+        const LevView<T> v = sv[nl - 1 - Ls];
         for (int r = threadIdx.x; r < v.N; r += blockDim.x) {
             T sum = 0;
             for (int q = 0; q < v.N; q++) sum += v.D[r * v.N + q] * v.b[q];
@@ -790,7 +804,7 @@ __global__ void __launch_bounds__(SMALL_TPB) k_vcycle_smem(const DevP *__restric
     }
     const T al = (T)alpha;
     for (int L = nl - 2; L >= Ls; L--) {
-        const LevView<T> v = smem_view<T>(P, L, Ls, sraw), cv = smem_view<T>(P, L + 1, Ls, sraw);
+        const LevView<T> v = sv[L - Ls], cv = sv[L + 1 - Ls];
         for (int k = threadIdx.x; k < v.N; k += blockDim.x) {
             const Node a = unidx(k, v.Nx, v.Ny);
             const int I = v.cx ? a.i >> 1 : a.i, J = v.cy ? a.j >> 1 : a.j, K = v.cz ? a.l >> 1 : a.l;
@@ -805,7 +819,7 @@ __global__ void __launch_bounds__(SMALL_TPB) k_vcycle_smem(const DevP *__restric
         blk_smooth<T>(v, 1, 1);
         blk_smooth<T>(v, 0, 1);
     }
-    const LevView<T> v = smem_view<T>(P, Ls, Ls, sraw);
+    const LevView<T> v = sv[0];
     blk_copy<T>(PT<T>::lev(P, Ls).x, v.x, v.N);
 }
 
@@ -850,7 +864,7 @@ static void small_init() {
         int dev = 0, optin = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        g_smem_max = optin > 0 ? (size_t)optin : 0;
+        g_smem_max = optin > 8192 ? (size_t)optin - 8192 : 0;     // room for the static shared arrays
         const char *sm = std::getenv("SEMISIM_B200_SMEM");
         if (sm && std::atoi(sm) == 0) g_smem_max = 0;
         if (g_smem_max &&
