@@ -96,8 +96,12 @@ def run_probe(a):
     lib.api3b_seed_enable(0)
     dv = np.array([0.0, 0.0, 0.05, 0.0])
     seed_ok = lib.b200x_seed_run(1.0, abi.dptr(dv))
+    lib.b200x_stream_timer(0)
+    for _ in range(10):
+        lib.b200x_seed_run(1.0, abi.dptr(dv))
+    seed_ms = lib.b200x_stream_timer(1) / 10
     print(json.dumps({"probe": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]} electron continuity", "nodes": w.N,
-                      "precision": a.precision, "seed_kernel": seed_ok,
+                      "precision": a.precision, "seed_kernel": seed_ok, "seed_ms": round(seed_ms, 4),
                       "bicgstab_its": its, "r0": r0[0], "rn": rn[0],
                       "launches": int(lib.b200x_launches() - l0)}))
 

@@ -54,9 +54,11 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
     return *reinterpret_cast<const uint32_t *>(&v);
 }
 __device__ __forceinline__ uint32_t ld32(const bf16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
-__device__ __forceinline__ float silu(float z) { return z / (1.f + expf(-z)); }
+// SiLU and its derivative with the fast exponential and division intrinsics (relative
+// error ~1e-6, far below the BF16 rounding of the activations they feed)
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.f / (1.f + expf(-z));
+    const float s = __fdividef(1.f, 1.f + __expf(-z));
     return s * (1.f + z * (1.f - s));
 }
 
@@ -184,31 +186,30 @@ __device__ __forceinline__ void out_mma(float (&o)[4], const uint32_t (&a)[8][4]
     }
 }
 
-// ------------------------------------------------------------------ fused seed
-// x_next = x1 + s (x1 - x0) + VT * MLP(features) for psi, phi_n, phi_p of every node,
-// 64 nodes per CTA pass (4 warps x 16), x1 = h1 and x0 = e2 of the instance
-constexpr int SEED_TPB = 128, SEED_ROWS = 64;
-__global__ void __launch_bounds__(SEED_TPB) k_mlp_seed(const DevP *__restrict__ Ps, const bf16 *__restrict__ Wb,
-                                                        const float *__restrict__ bias, SeedIn in) {
+// ------------------------------------------------------------------ seed
+// x_next = x1 + s (x1 - x0) + VT * MLP(X) for psi, phi_n, phi_p of every node; X the
+// node features (k_seed_features), 128 nodes per CTA pass (8 warps x 16 rows), x1 = h1 and
+// x0 = e2 of the instance
+constexpr int SEED_TPB = 128, SEED_ROWS = 64;            // training kernels
+constexpr int INF_TPB = 256, INF_ROWS = 128;             // inference
+__global__ void __launch_bounds__(INF_TPB) k_mlp_seed(const DevP *__restrict__ Ps, const bf16 *__restrict__ Wb,
+                                                       const float *__restrict__ bias, SeedIn in,
+                                                       const bf16 *__restrict__ X) {
     const DevP &P = Ps[blockIdx.y];
     extern __shared__ __align__(16) unsigned char smraw[];
     MlpSmem &s = *reinterpret_cast<MlpSmem *>(smraw);
     bf16 *Xs = reinterpret_cast<bf16 *>(smraw + sizeof(MlpSmem));
     load_weights(s, Wb, bias);
     const int w = threadIdx.x >> 5, g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
-    double *dst[3] = {P.phi, P.phin, P.phip};
     const double VT = P.VTref;
-    for (int base = blockIdx.x * SEED_ROWS; base < P.N; base += gridDim.x * SEED_ROWS) {
+    const int N = P.N;
+    for (int base = blockIdx.x * INF_ROWS; base < N; base += gridDim.x * INF_ROWS) {
         __syncthreads();                           // weights staged / previous tile consumed
-        if (threadIdx.x < SEED_ROWS) {
-            const int k = base + threadIdx.x;
-            float f[MI];
-            if (k < P.N) node_features(P, in, k, f);
-            else
-                for (int q = 0; q < MI; q++) f[q] = 0.f;
-            bf16 *xr = Xs + threadIdx.x * P1;
-            for (int q = 0; q < MI; q += 2)
-                *reinterpret_cast<__nv_bfloat162 *>(xr + q) = __floats2bfloat162_rn(f[q], f[q + 1]);
+        for (int e = threadIdx.x; e < INF_ROWS * MI / 2; e += blockDim.x) {
+            const int r = e / (MI / 2), q = 2 * (e % (MI / 2));
+            const int row = base + r;
+            const uint32_t v = row < N ? ld32(X + (size_t)row * MI + q) : 0u;
+            *reinterpret_cast<uint32_t *>(Xs + r * P1 + q) = v;
         }
         __syncthreads();
         uint32_t a0[3][4], a[8][4];
@@ -226,13 +227,17 @@ __global__ void __launch_bounds__(SEED_TPB) k_mlp_seed(const DevP *__restrict__ 
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int k = base + 16 * w + g + 8 * h;
-                if (k >= P.N) continue;
+                if (k >= N) continue;
 #pragma unroll
                 for (int e = 0; e < 2; e++) {
                     const int c = 2 * t + e;
                     if (c >= MOUT) continue;
-                    const double x1 = in.x1[c][k], x0 = in.x0[c][k];
-                    dst[c][k] = x1 + (double)in.s * (x1 - x0) + VT * (double)o[2 * h + e];
+                    // channel pointers by select (no dynamically indexed arrays: no local memory)
+                    const double *X1 = c == 0 ? in.x1[0] : (c == 1 ? in.x1[1] : in.x1[2]);
+                    const double *X0 = c == 0 ? in.x0[0] : (c == 1 ? in.x0[1] : in.x0[2]);
+                    double *D = c == 0 ? P.phi : (c == 1 ? P.phin : P.phip);
+                    const double x1 = X1[k], x0 = X0[k];
+                    D[k] = x1 + (double)in.s * (x1 - x0) + VT * (double)o[2 * h + e];
                 }
             }
         }
@@ -485,10 +490,11 @@ __global__ void k_mlp_pack(const float *P, bf16 *Wb, float *bias) {
 }
 
 static size_t seed_smem() { return sizeof(MlpSmem) + (size_t)SEED_ROWS * P1 * sizeof(bf16); }
+static size_t inf_smem() { return sizeof(MlpSmem) + (size_t)INF_ROWS * P1 * sizeof(bf16); }
 static bool g_mlp_attr = false;
 static void mlp_attrs() {
     if (g_mlp_attr) return;
-    cudaFuncSetAttribute(k_mlp_seed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seed_smem());
+    cudaFuncSetAttribute(k_mlp_seed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inf_smem());
     cudaFuncSetAttribute(k_mlp_train_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seed_smem());
     cudaFuncSetAttribute(k_mlp_train_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmemT));
     g_mlp_attr = true;
@@ -497,7 +503,8 @@ static void mlp_attrs() {
 // ------------------------------------------------------------------ solver side
 int seed_available(const Inst &d) { return d.seed_on && d.g.seedw != nullptr; }
 
-// x = x1 + s (x1 - x0) + VT * MLP for the sweep predictor step (h1 = x1, e2 = x0)
+// x = x1 + s (x1 - x0) + VT * MLP for the sweep predictor step (h1 = x1, e2 = x0): the
+// features into the instance's feature buffer, then the network and the seed write
 void launch_mlp_seed(Inst &d, double s, const double *dv) {
     mlp_attrs();
     Ctx c = make_ctx(d);
@@ -505,13 +512,15 @@ void launch_mlp_seed(Inst &d, double s, const double *dv) {
     for (int a = 0; a < 3; a++) { in.x1[a] = d.g.h.h1[a]; in.x0[a] = d.g.h.e2[a]; }
     in.s = (float)s;
     for (int q = 0; q < 4; q++) in.dv[q] = (float)dv[q];
-    int nb = (int)((d.N + SEED_ROWS - 1) / SEED_ROWS);
+    bf16 *X = reinterpret_cast<bf16 *>(d.g.seedx);
+    int nb = (int)((d.N + INF_ROWS - 1) / INF_ROWS);
     if (nb > 296) nb = 296;
-    g_launches++;
-    t_launches++;
+    g_launches += 2;
+    t_launches += 2;
     if (g_prof_on) prof_begin(PF_SEED, c.st);
-    k_mlp_seed<<<dim3(nb, 1), SEED_TPB, seed_smem(), c.st>>>(c.dP, (const bf16 *)d.g.seedw, (const float *)d.g.seedb,
-                                                             in);
+    k_seed_features<<<dim3(c.nodes_blocks(), 1), TPB, 0, c.st>>>(c.dP, in, X);
+    k_mlp_seed<<<dim3(nb, 1), INF_TPB, inf_smem(), c.st>>>(c.dP, (const bf16 *)d.g.seedw, (const float *)d.g.seedb,
+                                                           in, X);
     if (g_prof_on) prof_end(PF_SEED, c.st, (double)d.N);
 }
 
@@ -530,11 +539,14 @@ int api3b_seed_set_model(const float *params, int n) {
     Inst &d = *b200_global_dev();
     if (n != NPARAM || !params || !d.g.ready) return 0;
     Ctx c = make_ctx(d);
-    if (!d.g.seedw) {
+    if (!d.g.seedw) {                              // weights, biases, parameters, node features
         void *p = nullptr;
-        if (cudaMalloc(&p, NWB * sizeof(bf16) + (NBIAS + NPARAM) * sizeof(float)) != cudaSuccess) return 0;
+        const size_t wb = NWB * sizeof(bf16) + (NBIAS + NPARAM) * sizeof(float);
+        const size_t xo = (wb + 255) & ~size_t(255);
+        if (cudaMalloc(&p, xo + d.N * MI * sizeof(bf16)) != cudaSuccess) return 0;
         d.g.seedw = p;
         d.g.seedb = reinterpret_cast<float *>(reinterpret_cast<char *>(p) + NWB * sizeof(bf16));
+        d.g.seedx = reinterpret_cast<char *>(p) + xo;
     }
     float *P = d.g.seedb + NBIAS;
     cudaMemcpyAsync(P, params, NPARAM * sizeof(float), cudaMemcpyHostToDevice, c.st);

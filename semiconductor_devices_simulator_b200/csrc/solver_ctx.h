@@ -48,6 +48,7 @@ struct Gpu {
     int *flag = nullptr;         // device int scratch
     void *seedw = nullptr;       // learned predictor: BF16 weight pack, then FP32 biases and parameters
     float *seedb = nullptr;
+    void *seedx = nullptr;       // its node features (N x 48 BF16), in the same allocation
 };
 
 struct TrapSpec { int type, ref; double E, sn, sp; };   // deep-level species (stored, not solved)
