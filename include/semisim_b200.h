@@ -268,6 +268,19 @@ int api3b_seed_nparam(void);
    api3b_tune_get: the shapes in use (zcap: most row blocks per pass; may be null); returns
    1 when they came from the tuner. */
 double api3b_autotune(int mode);
+
+/* No counterpart in the reference (its callers that multiply solves - main.py's cap_matrix
+   C-V perturbations, main.py:4034-4087, and solve_floating's secant, main.py:3575-3636 -
+   restore a state and call api3_resolve once per bias vector).  Solves n bias vectors V
+   (n x ncon volts) from the current instance's solved state, each independently, on up to
+   `workers` worker instances at once (<= 0: min(n, 8)), each with its own device memory,
+   CUDA stream and host thread.  Outputs per vector: terminal currents I (n x ncon), floors
+   Iflr and converged flags conv (both may be null).  The current instance is unchanged.
+   Returns the number of converged solves, -1 without a solution or on a device error.
+   api3b_resolve_batch_free releases the current instance's workers (they are kept for
+   later calls; api3b_free does not release them). */
+int api3b_resolve_batch(int n, const double *V, double *I, double *Iflr, int *conv, int workers);
+int api3b_resolve_batch_free(void);
 int api3b_tune_get(int *rpb, int *grid_cap, int *small_nodes, int *zcap);
 
 /* No counterpart in the reference.  For callers that cannot allocate device memory

@@ -128,6 +128,9 @@ EXTRA = {
     "api3b_seed_nparam": (_I, []),
     # launch-shape autotuner of the current instance
     "api3b_autotune": (_D, [_I]),
+    # batched resolve of several bias vectors from the current solved state
+    "api3b_resolve_batch": (_I, [_I, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_I), _I]),
+    "api3b_resolve_batch_free": (_I, []),
     "api3b_tune_get": (_I, [ctypes.POINTER(_I)] * 4),
 }
 

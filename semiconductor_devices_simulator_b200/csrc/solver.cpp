@@ -473,6 +473,8 @@ int prepare(Inst &d) {
     CK(cudaStreamSynchronize(st));
     d.g.mg.alpha = g_knobs.mg_alpha;
     d.dirty = 0;
+    static std::atomic<unsigned long long> gen{0};
+    d.upload_gen = ++gen;
     return 1;
 }
 

@@ -95,6 +95,9 @@ struct Inst {
     int precision = -1;               // linear solves: 0 FP64, 1 FP32 refined in FP64, -1 library default
     long long ir_steps = 0, ir_fallbacks = 0;
     Tune tune;
+    unsigned long long upload_gen = 0;      // set-up upload this instance's device holds (prepare)
+    const Inst *clone_src = nullptr;        // batched-resolve worker: the instance and upload
+    unsigned long long clone_gen = 0;       //   generation its set-up was copied from
     int seed_on = 0;                  // learned sweep predictor enabled (needs a loaded model)
     long long seed_used = 0, seed_fallbacks = 0;
     // ---- derived by prepare (host copies)

@@ -270,3 +270,47 @@ def test_diode_variant_matches_reference(lib):
     assert g[0] and g[4].all() and r[4].all()
     check_currents(g[2], r[2], r[3])
     assert np.abs(g[5] - r[5]).max() <= PSI_TOL
+
+
+def test_resolve_batch_matches_sequential_resolves(lib):
+    """Six bias vectors around an operating point of the small MOSFET (gate and drain
+    perturbed both ways), solved at once by api3b_resolve_batch, give the currents of six
+    sequential api3_resolve calls from the restored state (api3_set_state), to 1e-10."""
+    import ctypes
+    w, mat, bias = MG.build(lib, "mos_small")
+    s = dict(w.sweeps[0])
+    s["V"] = s["V"][:4]
+    assert D.start_sweep(lib, w, s)
+    D.run_sweep(lib, w, s)
+    nc = lib.api3_get_ncon()
+    base = np.array([lib.api3_get_contact_Vsolved(c) for c in range(nc)])
+    N = w.N
+    st = [np.zeros(N) for _ in range(3)]
+    assert lib.api3_get_state(*(abi.dptr(a) for a in st))
+    g, d = w.contacts["gate"], w.contacts["drain"]
+    Vs = []
+    for cid, dv in ((g, 0.01), (g, -0.01), (d, 0.02), (d, -0.02), (g, 0.03), (d, 0.05)):
+        v = base.copy()
+        v[cid] += dv
+        Vs.append(v)
+    Vs = np.ascontiguousarray(Vs)
+    Ib = np.zeros((len(Vs), nc))
+    conv = np.zeros(len(Vs), np.int32)
+    try:
+        nok = lib.api3b_resolve_batch(len(Vs), abi.dptr(Vs), abi.dptr(Ib), None,
+                                      conv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), 3)
+        assert nok == len(Vs) and conv.all()
+        # the source instance was not moved
+        assert np.allclose([lib.api3_get_contact_Vsolved(c) for c in range(nc)], base)
+        Iseq = np.zeros_like(Ib)
+        for j, v in enumerate(Vs):
+            for c in range(nc):
+                lib.api3_set_contact_V(c, float(base[c]))
+            assert lib.api3_set_state(*(abi.dptr(a) for a in st))
+            for c in range(nc):
+                lib.api3_set_contact_V(c, float(v[c]))
+            assert lib.api3_resolve()
+            Iseq[j] = [lib.api3_get_contact_I(c) for c in range(nc)]
+        np.testing.assert_allclose(Ib, Iseq, rtol=1e-10, atol=1e-30)
+    finally:
+        lib.api3b_resolve_batch_free()
