@@ -1,7 +1,8 @@
 // Autotuner of the linear-algebra launch shapes of one solver instance: rows per block of
 // the row-blocked level passes (block 32 x rpb) and the most row blocks of a pass (more rows
-// per thread beyond it), the block count of the grid-stride node kernels, and the level
-// size at which the small-level kernel takes over.  It times
+// per thread beyond it), coarse rows per block of the residual + restriction pass, the
+// block count of the grid-stride node kernels, and the level size at which the small-level
+// kernel takes over.  It times
 // V-cycles of the instance's own multigrid hierarchy (the precision its solves use) on
 // the GPU with CUDA events and keeps the fastest shapes, one parameter at a time.  Results
 // are cached per mesh shape and precision for the process, so instances of the same
@@ -65,22 +66,24 @@ double api3b_autotune(int mode) {
     Tune best = Tune();
     best.us = time_vcycle(d, best, mixed, reps);
     const int small_c[] = {1024, 2048, 4096, 8192};
-    const int rpb_c[] = {2, 4, 8};
+    const int rpb_c[] = {2, 4, 8, 16, 32};
+    const int rq_c[] = {1, 2, 4, 8};
     const int cap_c[] = {148 * 4, 148 * 8, 148 * 12};
     const int zcap_c[] = {65535, 148 * 2, 148};
-    for (int pass = 0; pass < 4; pass++) {
-        const int *cand = pass == 0 ? small_c : (pass == 1 ? rpb_c : (pass == 2 ? cap_c : zcap_c));
-        const int nc = pass == 0 ? 4 : 3;
+    for (int pass = 0; pass < 5; pass++) {
+        const int *cand = pass == 0 ? small_c : (pass == 1 ? rpb_c : (pass == 2 ? cap_c : (pass == 3 ? zcap_c : rq_c)));
+        const int nc = pass == 0 || pass == 4 ? 4 : (pass == 1 ? 5 : 3);
         for (int q = 0; q < nc; q++) {
             Tune t = best;
             if (pass == 0) t.small_nodes = cand[q];
             else if (pass == 1) t.rpb = cand[q];
             else if (pass == 2) t.grid_cap = cand[q];
-            else t.zcap = cand[q];
+            else if (pass == 3) t.zcap = cand[q];
+            else t.rq = cand[q];
             const double us = time_vcycle(d, t, mixed, reps);
             if (d.verbose)
-                std::fprintf(stderr, "semisim-b200: autotune rpb %d cap %d small %d zcap %d: %.2f us\n", t.rpb,
-                             t.grid_cap, t.small_nodes, t.zcap, us);
+                std::fprintf(stderr, "semisim-b200: autotune rpb %d cap %d small %d zcap %d rq %d: %.2f us\n", t.rpb,
+                             t.grid_cap, t.small_nodes, t.zcap, t.rq, us);
             if (us < 0.97 * best.us) {       // keep a change only when it clearly wins
                 best = t;
                 best.us = us;
@@ -95,7 +98,7 @@ double api3b_autotune(int mode) {
 }
 
 // the current instance's launch shapes: rows per block, grid cap, small-level size, most
-// row blocks per pass
+// row blocks per pass (the restriction's coarse rows per block are not reported)
 int api3b_tune_get(int *rpb, int *grid_cap, int *small_nodes, int *zcap) {
     Inst &d = *b200_global_dev();
     *rpb = d.tune.rpb;

@@ -29,6 +29,7 @@ struct Ctx {
     int grid_cap = 148 * 8;     // blocks of the grid-stride node kernels (<= RED_MAX_BLOCKS)
     int rpb = 4;                // rows per block of the row-blocked level passes (block 32 x rpb)
     int zcap = 65535;           // most row blocks of one pass (more rows per thread beyond it)
+    int rq = 1;                 // coarse rows per block of the residual + restriction pass
     int small_nodes = 0;        // levels at or below this size go to the small-level kernel (0: default)
     int nodes_blocks() const;
 };

@@ -224,7 +224,7 @@ __device__ __forceinline__ Agg agg_range(const V &f, int I, int J, int K) {
 // x += alpha pw P xc (semiconductor_3d.c:2038-2048); the residual that follows needs
 // every prolonged neighbour and is a separate pass
 template <class T>
-__global__ void __launch_bounds__(256) k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha,
+__global__ void __launch_bounds__(1024) k_prolong(const DevP *__restrict__ Ps, int L, int bsel, int xsel, double alpha,
                                                  int gate) {
     pdl_launch();
     const DevP &P = Ps[blockIdx.y];
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(256) k_prolong(const DevP *__restrict__ Ps, in
     }
 }
 template <class T>
-__global__ void __launch_bounds__(256) k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
+__global__ void __launch_bounds__(1024) k_level_resid(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
     pdl_launch();
     const DevP &P = Ps[blockIdx.y];
     const LevView<T> f = levview<T>(P, L, bsel, xsel);
@@ -517,7 +517,7 @@ __device__ __forceinline__ void smooth_node(const LevView<T> &v, int k, int i, i
 // Half sweep over the nodes of one colour: thread ti of row (j, l) takes
 // i = 2 ti + ((j + l + colour) & 1), so every lane does work.
 template <class T, int MODE, int COLOR>
-__global__ void __launch_bounds__(256) k_smooth_cm(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
+__global__ void __launch_bounds__(1024) k_smooth_cm(const DevP *__restrict__ Ps, int L, int bsel, int xsel, int gate) {
     constexpr int mode = MODE, color = COLOR;
     pdl_launch();
     const DevP &P = Ps[blockIdx.y];
@@ -545,14 +545,14 @@ static SmoothFn<T> smooth_fn(int mode, int color) {
     return tab[mode][color];
 }
 
-// Weighted residual of every fine node summed into its 2x2x2 aggregate.  Block (32, 4):
-// threadIdx.x runs along fine x, threadIdx.y picks the (j, l) parity inside the coarse
-// row blockIdx.z; pairs along x meet through a shuffle, the four parities through
-// shared memory.  One thread per fine node (the restriction of semiconductor_3d.c:
+// Weighted residual of every fine node summed into its 2x2x2 aggregate.  Block (32, 4 Q):
+// threadIdx.x runs along fine x, threadIdx.y picks one of Q coarse rows and the (j, l)
+// parity inside it; pairs along x meet through a shuffle, the four parities through
+// shared memory; the blocks loop over the coarse rows.  One thread per fine node (the restriction of semiconductor_3d.c:
 // 2028-2037 applied to the residual of 1984-1991).
 template <class T>
-__global__ void __launch_bounds__(128) k_resid_restrict2(const DevP *__restrict__ Ps, int L, int bsel, int xsel,
-                                                         int wsel, int gate) {
+__global__ void __launch_bounds__(1024) k_resid_restrict2(const DevP *__restrict__ Ps, int L, int bsel, int xsel,
+                                                          int wsel, int gate) {
     pdl_launch();
     const DevP &P = Ps[blockIdx.y];
     const LevView<T> f = levview<T>(P, L, bsel, xsel);
@@ -561,30 +561,37 @@ __global__ void __launch_bounds__(128) k_resid_restrict2(const DevP *__restrict_
     const int nl = P.nlev;
     pdl_wait();
     if (L >= nl - 1 || gated_off<T>(P, gate)) return;
-    const int R = blockIdx.z;                         // coarse row J + Cy*Lc
-    const bool rowok = R < cl.Ny * cl.Nz;
-    const int Lc = rowok ? R / cl.Ny : 0, Jc = rowok ? R - Lc * cl.Ny : 0;
-    const int dj = threadIdx.y & 1, dl = threadIdx.y >> 1;
+    // block (32, 4 Q): Q coarse rows per pass, threadIdx.y = 4 q + (j, l) parity
+    const int Q = blockDim.y >> 2, q = threadIdx.y >> 2, par = threadIdx.y & 3;
+    const int dj = par & 1, dl = par >> 1;
+    const int rows = cl.Ny * cl.Nz;
     const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = f.cy ? 2 * Jc + dj : Jc, l = f.cz ? 2 * Lc + dl : Lc;
-    const bool ok = rowok && i < f.Nx && j < f.Ny && l < f.Nz && (f.cy || dj == 0) && (f.cz || dl == 0);
-    T val = 0;
-    if (ok) {
-        const int k = i + f.Nx * (j + f.Ny * l);
-        const T r = f.b[k] - lv_apply<T>(f, f.x, k, i, j, l);
-        val = w ? w[k] * r : r;
-    }
-    __shared__ T sh[4][32];
-    sh[threadIdx.y][threadIdx.x] = val;
-    __syncthreads();
-    if (threadIdx.y == 0) {
-        T s = sh[0][threadIdx.x] + sh[1][threadIdx.x] + sh[2][threadIdx.x] + sh[3][threadIdx.x];
-        if (f.cx) {
-            s += __shfl_down_sync(0xffffffffu, s, 1);
-            if (rowok && !(threadIdx.x & 1) && i < f.Nx) cl.b[(i >> 1) + cl.Nx * R] = s;
-        } else if (rowok && i < f.Nx) {
-            cl.b[i + cl.Nx * R] = s;
+    __shared__ T sh[32][32];
+    for (int R0 = blockIdx.z * Q; R0 < rows; R0 += gridDim.z * Q) {
+        const int R = R0 + q;                         // coarse row J + Cy*Lc
+        const bool rowok = R < rows;
+        const int Lc = rowok ? R / cl.Ny : 0, Jc = rowok ? R - Lc * cl.Ny : 0;
+        const int j = f.cy ? 2 * Jc + dj : Jc, l = f.cz ? 2 * Lc + dl : Lc;
+        const bool ok = rowok && i < f.Nx && j < f.Ny && l < f.Nz && (f.cy || dj == 0) && (f.cz || dl == 0);
+        T val = 0;
+        if (ok) {
+            const int k = i + f.Nx * (j + f.Ny * l);
+            const T r = f.b[k] - lv_apply<T>(f, f.x, k, i, j, l);
+            val = w ? w[k] * r : r;
         }
+        sh[threadIdx.y][threadIdx.x] = val;
+        __syncthreads();
+        if (par == 0) {
+            T s = sh[4 * q][threadIdx.x] + sh[4 * q + 1][threadIdx.x] + sh[4 * q + 2][threadIdx.x] +
+                  sh[4 * q + 3][threadIdx.x];
+            if (f.cx) {
+                s += __shfl_down_sync(0xffffffffu, s, 1);
+                if (rowok && !(threadIdx.x & 1) && i < f.Nx) cl.b[(i >> 1) + cl.Nx * R] = s;
+            } else if (rowok && i < f.Nx) {
+                cl.b[i + cl.Nx * R] = s;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -908,6 +915,13 @@ static inline dim3 grid_rows(const Ctx &c, int L, const MGHost &mg, int nx) {
 }
 static inline dim3 grid_half(const Ctx &c, int L, const MGHost &mg) { return grid_rows(c, L, mg, (mg.maxNx[L] + 1) / 2); }
 static inline dim3 grid_full(const Ctx &c, int L, const MGHost &mg) { return grid_rows(c, L, mg, mg.maxNx[L]); }
+// residual + restriction from level L: block (32, 4 rq), grid over the coarse rows
+static inline dim3 block_rr(const Ctx &c) { return dim3(32, 4 * c.rq); }
+static inline dim3 grid_rr(const Ctx &c, int L, const MGHost &mg) {
+    int gz = (mg.maxRows[L + 1] + c.rq - 1) / c.rq;
+    if (gz > 65535) gz = 65535;
+    return dim3((mg.maxNx[L] + 31) / 32, c.ninst, gz > 0 ? gz : 1);
+}
 #define ROW_BLOCK dim3(32, c.rpb)
 static int small_split(const Ctx &c, const MGHost &mg) {
     small_init();
@@ -973,8 +987,7 @@ static void vcycle_t(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wse
             SS_LAUNCH_PDL(SB, mg.maxN[L], smooth_fn<T>(2, 1), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
             SS_LAUNCH_PDL(SR, mg.maxN[L], smooth_fn<T>(2, 0), grid_half(c, L, mg), ROW_BLOCK, c.st, c.dP, L, bsel, xsel, gate);
         }
-        const dim3 gr((mg.maxNx[L] + 31) / 32, c.ninst, mg.maxRows[L + 1]);
-        SS_LAUNCH_PDL(pf<T>(PF_RESID_RESTRICT), mg.maxN[L], k_resid_restrict2<T>, gr, dim3(32, 4), c.st, c.dP, L, bsel,
+        SS_LAUNCH_PDL(pf<T>(PF_RESID_RESTRICT), mg.maxN[L], k_resid_restrict2<T>, grid_rr(c, L, mg), block_rr(c), c.st, c.dP, L, bsel,
                   xsel, wsel, gate);
     }
     if (smem) launch_smem<T>(c, mg.maxN[Ls], Ls, mg.alpha, gate, smem);
@@ -1686,13 +1699,13 @@ double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    const dim3 grr((mg.maxNx[0] + 31) / 32, c.ninst, mg.maxRows[1]);
+    const dim3 grr = grid_rr(c, 0, mg), brr = block_rr(c);
     auto one = [&]() {
         switch (which) {
         case 0: k_bicg_v<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
         case 1: k_smooth_cm<double, 0, 1><<<grid_half(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
         case 2: k_smooth_cm<double, 0, 0><<<grid_half(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
-        case 3: k_resid_restrict2<double><<<grr, dim3(32, 4), 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
+        case 3: k_resid_restrict2<double><<<grr, brr, 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
         case 4: k_level_resid<double><<<grid_full(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
         case 5: k_prolong<double><<<grid_full(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 1.0, 0); break;
         case 6: k_bicg_x<double><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
@@ -1706,7 +1719,7 @@ double bench_la_kernel(const Ctx &c, const MGHost &mg, int which, int reps) {
         case 11: k_bicg_v<float><<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
         case 12: k_smooth_cm<float, 0, 1><<<grid_half(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
         case 13: k_smooth_cm<float, 0, 0><<<grid_half(c, 0, mg), ROW_BLOCK, 0, c.st>>>(c.dP, 0, 2, 4, 0); break;
-        case 14: k_resid_restrict2<float><<<grr, dim3(32, 4), 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
+        case 14: k_resid_restrict2<float><<<grr, brr, 0, c.st>>>(c.dP, 0, 2, 4, 1, 0); break;
         case 15: vcycle_t<float>(c, mg, 2, 4, 1, 1, 0); break;
         case 16: k_ir_update<<<grid_nodes(c), TPB, 0, c.st>>>(c.dP); break;
         case 17:

@@ -63,6 +63,7 @@ Ctx make_ctx(Inst &d) {
     c.grid_cap = d.tune.grid_cap;
     c.small_nodes = d.tune.small_nodes;
     c.zcap = d.tune.zcap;
+    c.rq = d.tune.rq;
     return c;
 }
 

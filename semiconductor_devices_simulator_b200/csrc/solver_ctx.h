@@ -59,6 +59,7 @@ struct Tune {
     int grid_cap = 148 * 8;       // blocks of the grid-stride node kernels
     int small_nodes = 0;          // size at which the small-level kernel takes over (0: default)
     int zcap = 65535;             // most row blocks of one row-blocked pass
+    int rq = 1;                   // coarse rows per residual + restriction block
     int tuned = 0;
     double us = 0.0;              // V-cycle time of the chosen shapes (microseconds)
 };

@@ -206,7 +206,7 @@ def test_autotuned_shapes_keep_parity(lib, name):
         r, gc, sm, zc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         assert lib.api3b_tune_get(ctypes.byref(r), ctypes.byref(gc), ctypes.byref(sm), ctypes.byref(zc)) == 1
         assert zc.value in (65535, 296, 148)
-        assert us > 0.0 and r.value in (2, 4, 8) and gc.value in (592, 1184, 1776) and sm.value in (0, 1024, 2048, 4096, 8192)
+        assert us > 0.0 and r.value in (2, 4, 8, 16, 32) and gc.value in (592, 1184, 1776) and sm.value in (0, 1024, 2048, 4096, 8192)
         ok0, V, I, F, conv, psi, n, p = sweep_fields(lib, w, s)
         assert ok0 and conv.all()
         own = 2.0 * np.abs(g["sw0_I"] - g["swt0_I"])
