@@ -518,7 +518,7 @@ __global__ void k_node_val(const DevP *__restrict__ Ps, int which, double *out) 
         case 26: v = kd == K_SEMI ? niK(P, m, k) : 0.0; break;
         case 27: v = 0.0; break;                                 // gate tunnelling J: not built
         case 28: case 29: v = kd == K_SEMI ? 0.0 : nan; break;   // quantum potentials: not built
-        case 30: v = kd == K_SEMI ? 1.0 : nan; break;            // interface distance: not built
+        case 30: v = kd == K_SEMI ? P.qd[k] : nan; break;        // distance to the nearest wall
         case 31: case 32: v = kd == K_SEMI ? 0.0 : nan; break;   // traps: not built
         case 33: v = 0.0; break;                                 // impact ionisation: not built
         case 34: v = kd == K_SEMI ? 0.0 : nan; break;            // Coulomb N_C: not built

@@ -81,6 +81,7 @@ struct DevP {
     const double *xs, *ys, *zs, *Lx, *Ly, *Lz;
     const uint32_t *flags;
     const double *Nd, *Na, *Nf, *bgn, *robA;
+    const double *qd;             // distance to the nearest insulator / gate wall (display)
     const MatD *mats;
     const ConD *cons;
     const int *cnode;             // contact-node list (semiconductor nodes of carrier contacts)

@@ -92,7 +92,7 @@ static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &lev
     const size_t N = d.N;
     P.flags = cv.take<uint32_t>(N);
     P.Nd = cv.take<double>(N); P.Na = cv.take<double>(N); P.Nf = cv.take<double>(N);
-    P.bgn = cv.take<double>(N); P.robA = cv.take<double>(N);
+    P.bgn = cv.take<double>(N); P.robA = cv.take<double>(N); P.qd = cv.take<double>(N);
     P.xs = cv.take<double>(d.Nx); P.ys = cv.take<double>(d.Ny); P.zs = cv.take<double>(d.Nz);
     P.Lx = cv.take<double>(d.Nx); P.Ly = cv.take<double>(d.Ny); P.Lz = cv.take<double>(d.Nz);
     P.mats = cv.take<MatD>(NM_MAX);
@@ -360,6 +360,47 @@ static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
 
 // prepare (semiconductor_3d.c:1638-1775): node kinds, contact and gate masks, Robin gate
 // areas, contact areas, band-gap narrowing; uploaded to the device with the geometry.
+// Distance of every node to the nearest wall along the mesh axes (the interface distance
+// semiconductor_3d.c:1100-1145 reports for display): scanning each mesh line both ways, a
+// wall is the midpoint to an insulator neighbour, or the domain face of the node's gate
+// contact; a metal node or the domain edge without such a gate ends the run.  1 m where no
+// wall is in sight.
+static void wall_distance(const Inst &d, const std::vector<unsigned char> &kind, const std::vector<int> &gate,
+                          std::vector<double> &qd) {
+    const int n3[3] = {d.Nx, d.Ny, d.Nz};
+    const std::vector<double> *cs[3] = {&d.xs, &d.ys, &d.zs};
+    const size_t st3[3] = {1, (size_t)d.Nx, (size_t)d.Nx * d.Ny};
+    qd.assign(d.N, 1.0);
+    for (int ax = 0; ax < 3; ax++) {
+        const int n = n3[ax];
+        const std::vector<double> &c = *cs[ax];
+        const size_t st = st3[ax];
+        for (size_t k0 = 0; k0 < d.N; k0++) {
+            if ((k0 / st) % (size_t)n != 0) continue;          // a line starts at index 0 along ax
+            for (int side = 0; side < 2; side++) {               // 0: walls below, 1: walls above
+                double w = 0.;
+                bool have = false;
+                for (int t = 0; t < n; t++) {
+                    const int q = side ? n - 1 - t : t;
+                    const size_t k = k0 + (size_t)q * st;
+                    if (kind[k] != K_SEMI) { have = false; continue; }
+                    const int qp = side ? q + 1 : q - 1;
+                    if (qp < 0 || qp >= n) {
+                        have = false;
+                        const int g = gate[k];
+                        if (g && d.cons[g - 1].face == 2 * ax + side) { w = c[q]; have = true; }
+                    } else {
+                        const unsigned char kb = kind[k0 + (size_t)qp * st];
+                        if (kb == K_INS) { w = 0.5 * (c[q] + c[qp]); have = true; }
+                        else if (kb != K_SEMI) have = false;
+                    }
+                    if (have) qd[k] = std::fmin(qd[k], std::fabs(c[q] - w));
+                }
+            }
+        }
+    }
+}
+
 int prepare(Inst &d) {
     if (!d.allocated || d.n_mats < 1) return 0;
     if (!d.dirty && d.g.ready) return 1;       // set-up unchanged since the last upload
@@ -436,6 +477,8 @@ int prepare(Inst &d) {
             d.mu0p[k] = mobility_low(m, Nt, 1);
         }
     }
+    std::vector<double> qd;
+    wall_distance(d, kind, gate, qd);
     if (!gpu_alloc(d)) return 0;
     // upload
     DevP &P = d.g.h;
@@ -460,6 +503,7 @@ int prepare(Inst &d) {
     CK(cudaMemcpyAsync((void *)P.Nf, d.Nf.data(), N * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync((void *)P.bgn, d.bgn.data(), N * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync((void *)P.robA, d.robA.data(), N * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)P.qd, qd.data(), N * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(P.mu0n, d.mu0n.data(), N * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(P.mu0p, d.mu0p.data(), N * 8, cudaMemcpyHostToDevice, st));
     if (!d.cnode.empty())
