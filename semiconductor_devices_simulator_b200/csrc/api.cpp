@@ -421,33 +421,8 @@ void api3_iv_sweep2(int cid, double Vs, double Ve, int Npts, double *Varr, doubl
 // ------------------------------------------------------------------ getters
 double api3_get_Emax(void) {                                // semiconductor_3d.c:4981-5001
     Inst &d = g_dev;
-    if (!d.allocated) return 0.;
-    const std::vector<double> *phi = node_vals(d, 0);
-    if (!phi) return 0.;
-    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
-    double Em = 0.;
-    for (int l = 0; l < Nz; l++)
-        for (int j = 0; j < Ny; j++)
-            for (int i = 0; i < Nx; i++) {
-                const size_t k = (size_t)l * Nx * Ny + (size_t)j * Nx + i;
-                if (kind_of(d, k) != K_SEMI) continue;
-                double g2 = 0.;
-                const int idx[3] = {i, j, l}, nn[3] = {Nx, Ny, Nz};
-                const size_t st[3] = {1, (size_t)Nx, (size_t)Nx * Ny};
-                const std::vector<double> *cs[3] = {&d.xs, &d.ys, &d.zs};
-                for (int ax = 0; ax < 3; ax++) {
-                    const int q = idx[ax];
-                    const bool a = q > 0, b = q < nn[ax] - 1;
-                    const std::vector<double> &c = *cs[ax];
-                    double g = 0.;
-                    if (a && b) g = ((*phi)[k + st[ax]] - (*phi)[k - st[ax]]) / (c[q + 1] - c[q - 1]);
-                    else if (b) g = ((*phi)[k + st[ax]] - (*phi)[k]) / (c[q + 1] - c[q]);
-                    else if (a) g = ((*phi)[k] - (*phi)[k - st[ax]]) / (c[q] - c[q - 1]);
-                    g2 += g * g;
-                }
-                if (g2 > Em) Em = g2;
-            }
-    return std::sqrt(Em);
+    if (!d.allocated || !d.have_solution || !d.g.ready) return 0.;
+    return out_emax(d);
 }
 int api3_get_Nx(void) { return g_dev.Nx; }
 int api3_get_Ny(void) { return g_dev.Ny; }
@@ -530,18 +505,8 @@ void api3_bulk_copy(int which, double *out) {
 void api3_carrier_sums(double *out) {                       // semiconductor_3d.c:5137-5147
     Inst &d = g_dev;
     out[0] = out[1] = 0.;
-    if (!d.allocated) return;
-    const std::vector<double> *n = node_vals(d, 1);
-    const std::vector<double> *p = node_vals(d, 2);
-    if (!n || !p) return;
-    double sn = 0., sp = 0.;
-    for (size_t k = 0; k < d.N; k++) {
-        if (kind_of(d, k) != K_SEMI) continue;
-        const int l = int(k / ((size_t)d.Nx * d.Ny)), rem = int(k - (size_t)l * d.Nx * d.Ny);
-        const double v = d.Lx[rem % d.Nx] * d.Ly[rem / d.Nx] * d.Lz[l];
-        sn += (*n)[k] * v; sp += (*p)[k] * v;
-    }
-    out[0] = sn; out[1] = sp;
+    if (!d.allocated || !d.have_solution || !d.g.ready) return;
+    out_carrier_sums(d, out);
 }
 
 // terminal partition for the quasi-static charges (semiconductor_3d.c:5192-5246)
@@ -552,6 +517,7 @@ int api3_charge_partition(const int *cterm) {
     if (!n || !p) return -1;
     const size_t N = d.N;
     g_qown.assign(N, -1);
+    d.g.qown_ok = false;
     for (int c = 0; c < NC_MAX; c++) g_qct[c] = c < d.n_cons ? cterm[c] : -1;
     auto qtype = [&](size_t k) { return (*n)[k] >= (*p)[k] ? 1 : -1; };
     std::vector<size_t> qu;
@@ -597,36 +563,37 @@ int api3_charge_partition(const int *cterm) {
 int api3_terminal_charges(int nt, double *Qt) {             // semiconductor_3d.c:5248-5282
     Inst &d = g_dev;
     const size_t N = d.N;
-    if (!d.allocated || !d.have_solution || g_qown.size() != N || nt <= 0 || !Qt) return 0;
-    const std::vector<double> *phi = node_vals(d, 0);
-    if (!phi) return 0;
-    for (int t = 0; t <= nt; t++) Qt[t] = 0.;
-    size_t nb[6]; double cf[6], hh[6];
-    for (size_t k = 0; k < N; k++) {
-        const int t = g_qown[k];
+    if (!d.allocated || !d.have_solution || !d.g.ready || g_qown.size() != N || nt <= 0 || !Qt) return 0;
+    // owners only take the contacts' terminal ids: number the ones inside [0, nt) densely
+    // (at most NC_MAX), the others count as no terminal, like -1
+    int slot[NC_MAX], ids[NC_MAX], m = 0, gate_slot[NC_MAX];
+    for (int c = 0; c < NC_MAX; c++) {
+        const int t = g_qct[c];
+        slot[c] = -1;
         if (t < 0 || t >= nt) continue;
-        const int m = qnbrs(d, k, nb, cf, hh);
-        for (int e = 0; e < m; e++) {
-            const size_t b = nb[e];
-            const int tb = g_qown[b];
-            if (tb == t) continue;
-            const double f = cf[e] * ((*phi)[k] - (*phi)[b]);
-            Qt[t] += f;
-            if (tb < 0 || tb >= nt) Qt[nt] += f;
+        for (int q = 0; q < m; q++) if (ids[q] == t) slot[c] = q;
+        if (slot[c] < 0) { ids[m] = t; slot[c] = m++; }
+    }
+    for (int c = 0; c < NC_MAX; c++) gate_slot[c] = slot[c];
+    if (!d.g.qown_ok || d.g.qown_nt != nt) {                // the partition's owners, once per nt
+        std::vector<int> own(N);
+        for (size_t k = 0; k < N; k++) {
+            const int t = g_qown[k];
+            int q = -1;
+            for (int r = 0; r < m && t >= 0; r++) if (ids[r] == t) { q = r; break; }
+            own[k] = q;
         }
+        if (!d.g.qown && cudaMalloc(&d.g.qown, N * sizeof(int)) != cudaSuccess) { d.g.qown = nullptr; return 0; }
+        cudaMemcpyAsync(d.g.qown, own.data(), N * sizeof(int), cudaMemcpyHostToDevice, d.g.st);
+        cudaStreamSynchronize(d.g.st);
+        d.g.qown_ok = true;
+        d.g.qown_nt = nt;
     }
-    for (size_t k = 0; k < N; k++) {
-        if (d.robA.empty() || d.robA[k] == 0.0) continue;
-        const int c = fl_gate(d.flags[k]) - 1;
-        if (c < 0) continue;
-        const Contact &cn = d.cons[c];
-        const double Cox = EPS_OX / (cn.tox > 0. ? cn.tox : 10e-9);
-        const double pm = cn.phi_m > 0. ? cn.phi_m : d.Cref;
-        const double f = d.robA[k] * Cox * ((*phi)[k] - (cn.V + d.Cref - pm));
-        const int t = g_qown[k], tg = g_qct[c];
-        if (t >= 0 && t < nt) Qt[t] += f;
-        if (tg >= 0 && tg < nt) Qt[tg] -= f;
-    }
+    double acc[NC_MAX + 1];
+    if (!out_terminal_charges(d, d.g.qown, m, gate_slot, acc)) return 0;
+    for (int t = 0; t <= nt; t++) Qt[t] = 0.;
+    for (int q = 0; q < m; q++) Qt[ids[q]] = acc[q];
+    Qt[nt] = acc[m];
     return 1;
 }
 int api3_face_J(int ax, int carrier, double *out) {
@@ -645,36 +612,13 @@ int api3_charge_owner(int *out) {
 }
 double api3_ins_field_max(double *pos) {                    // semiconductor_3d.c:5308-5339
     Inst &d = g_dev;
-    double best = 0.;
     if (pos) pos[0] = pos[1] = pos[2] = nanv();
-    if (!d.allocated || !d.have_solution) return nanv();
-    const std::vector<double> *phi = node_vals(d, 0);
-    if (!phi) return nanv();
-    size_t kbest = (size_t)-1;
-    size_t nb[6]; double cf[6], hh[6];
-    for (size_t k = 0; k < d.N; k++) {
-        if (kind_of(d, k) == K_SEMI) continue;
-        const int m = qnbrs(d, k, nb, cf, hh);
-        for (int e = 0; e < m; e++) {
-            const size_t b = nb[e];
-            if (b < k || kind_of(d, b) == K_SEMI) continue;
-            if (kind_of(d, k) != K_INS && kind_of(d, b) != K_INS) continue;
-            const double F = std::fabs((*phi)[b] - (*phi)[k]) / hh[e];
-            if (F > best) { best = F; kbest = kind_of(d, k) == K_INS ? k : b; }
-        }
-    }
-    for (size_t k = 0; k < d.N; k++) {
-        if (d.robA.empty() || d.robA[k] == 0.0) continue;
-        const int c = fl_gate(d.flags[k]) - 1;
-        if (c < 0) continue;
-        const Contact &cn = d.cons[c];
-        const double tox = cn.tox > 0. ? cn.tox : 10e-9;
-        const double pm = cn.phi_m > 0. ? cn.phi_m : d.Cref;
-        const double F = std::fabs((*phi)[k] - (cn.V + d.Cref - pm)) / tox;
-        if (F > best) { best = F; kbest = k; }
-    }
-    if (pos && kbest != (size_t)-1) {
-        const int l = int(kbest / ((size_t)d.Nx * d.Ny)), rem = int(kbest - (size_t)l * d.Nx * d.Ny);
+    if (!d.allocated || !d.have_solution || !d.g.ready) return nanv();
+    long long kb = -1;
+    const double best = out_ins_field(d, &kb);
+    if (pos && kb >= 0) {
+        const size_t k = (size_t)kb;
+        const int l = int(k / ((size_t)d.Nx * d.Ny)), rem = int(k - (size_t)l * d.Nx * d.Ny);
         pos[0] = d.xs[rem % d.Nx]; pos[1] = d.ys[rem / d.Nx]; pos[2] = d.zs[l];
     }
     return best;

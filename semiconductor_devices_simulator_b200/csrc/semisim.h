@@ -132,6 +132,7 @@ enum ResSlot {
     R_I = 8,         // terminal currents I[NC_MAX] at 8..39
     R_S = 40,        // scales S[NC_MAX] at 40..71 (res has 128 doubles)
     R_IN = 72,       // electron components at 72..103
+    R_OUT = 104,     // per-point output reductions at 104..110
     R_TOTAL = 128
 };
 

@@ -203,6 +203,7 @@ void gpu_free(Inst &d) {
     if (d.g.pin) cudaFreeHost(d.g.pin);
     if (d.g.scratch) cudaFree(d.g.scratch);
     if (d.g.flag) cudaFree(d.g.flag);
+    if (d.g.qown) cudaFree(d.g.qown);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();

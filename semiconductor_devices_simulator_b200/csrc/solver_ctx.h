@@ -46,6 +46,9 @@ struct Gpu {
     double *pin = nullptr;       // pinned host scratch (results)
     double *scratch = nullptr;   // device scratch (bulk output)
     int *flag = nullptr;         // device int scratch
+    int *qown = nullptr;         // charge-partition owners (N, dense terminal slots), uploaded on first use
+    bool qown_ok = false;
+    int qown_nt = 0;             // the terminal count they were numbered for
     void *seedw = nullptr;       // learned predictor: BF16 weight pack, then FP32 biases and parameters
     float *seedb = nullptr;
     void *seedx = nullptr;       // its node features (N x 48 BF16), in the same allocation
@@ -151,8 +154,13 @@ void terminal_currents(Inst &d, double *I, double *S);
 Ctx make_ctx(Inst &d);
 int use_mixed(const Inst &d);
 int seed_available(const Inst &d);                       // learned.cu
-void launch_mlp_seed(Inst &d, double s, const double *dv);       // precision of the instance's linear solves (1 = refined FP32)
-extern int g_precision_default;
+void launch_mlp_seed(Inst &d, double s, const double *dv);
+extern int g_precision_default;                          // precision of new instances (1 = refined FP32)
+// per-point output reductions on the device (outputs.cu)
+double out_emax(Inst &d);
+void out_carrier_sums(Inst &d, double *out);
+double out_ins_field(Inst &d, long long *node);
+int out_terminal_charges(Inst &d, const int *owner_dev, int nt, const int *gate_term, double *out);
 void gpu_free(Inst &d);
 
 // linear-algebra drivers (kernels_la.cu)

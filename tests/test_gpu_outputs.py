@@ -119,3 +119,66 @@ def test_per_point_outputs_match_reference(lib, name, monkeypatch):
     if not np.abs(g["Qt"] - r["Qt"]).max() <= 1e-6 * qs + 1e-300:
         bad.append(f"terminal charges {g['Qt']} vs {r['Qt']}")
     assert not bad, name + "\n" + "\n".join(bad)
+
+
+def scalar_outputs(L, N, nc):
+    o = {"Emax": L.api3_get_Emax()}
+    cs = np.zeros(2)
+    L.api3_carrier_sums(dptr(cs))
+    o["sums"] = cs
+    cterm = np.arange(nc, dtype=np.int32)
+    o["meet"] = L.api3_charge_partition(iptr(cterm))
+    own = np.zeros(N, np.int32)
+    assert L.api3_charge_owner(iptr(own)) == 1
+    o["own"] = own
+    for nt in (nc, nc + 2, max(nc - 1, 1)):
+        Qt = np.zeros(nt + 1)
+        assert L.api3_terminal_charges(nt, dptr(Qt)) == 1
+        o[f"Qt{nt}"] = Qt
+    pos = np.zeros(3)
+    o["Fins"] = L.api3_ins_field_max(dptr(pos))
+    o["Fpos"] = pos
+    return o
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_output_reductions_on_one_state(lib, name, monkeypatch):
+    """The device reductions behind api3_get_Emax, api3_carrier_sums, api3_terminal_charges
+    and api3_ins_field_max against the reference core's scans of the same state: this
+    library's solution is installed in the reference with api3_set_state, so both evaluate
+    identical potentials.  Emax and the insulator field (differences and quotients of the
+    same doubles) agree to round-off and the field's position exactly (ties resolve to the
+    reference's scan order); the sums differ only by summation order; terminal counts above,
+    at and below the number of terminals are covered."""
+    for k, v in MG.TIGHT_ENV.items():
+        monkeypatch.setenv(k, v)
+    ref = reference_lib()
+    ref.api3_set_threads(os.cpu_count() or 1)
+    states = []
+    for L in (lib, ref):
+        w, mat, bias = MG.build(L, name)
+        L.api3_set_solver(*MG.TIGHT_SOLVER)
+        for cid, v in bias.items():
+            L.api3_set_contact_V(cid, v)
+        assert L.api3_solve()
+        states.append(w)
+    N, nc = states[0].N, lib.api3_get_ncon()
+    phi, phin, phip = np.zeros(N), np.zeros(N), np.zeros(N)
+    assert lib.api3_get_state(dptr(phi), dptr(phin), dptr(phip)) == 1
+    assert ref.api3_set_state(dptr(phi), dptr(phin), dptr(phip)) == 1
+    g, r = scalar_outputs(lib, N, nc), scalar_outputs(ref, N, nc)
+    bad = []
+    for key, tol in (("Emax", 1e-13), ("Fins", 1e-14)):
+        if not abs(g[key] - r[key]) <= tol * abs(r[key]):
+            bad.append(f"{key}: {g[key]!r} vs {r[key]!r}")
+    if not np.array_equal(g["Fpos"], r["Fpos"], equal_nan=True):
+        bad.append(f"field position {g['Fpos']} vs {r['Fpos']}")
+    if not np.allclose(g["sums"], r["sums"], rtol=1e-12, atol=0):
+        bad.append(f"carrier sums {g['sums']} vs {r['sums']}")
+    if g["meet"] != r["meet"] or not np.array_equal(g["own"], r["own"]):
+        bad.append("charge partition differs")
+    for key in [k for k in r if k.startswith("Qt")]:
+        qs = np.abs(r[key]).max()
+        if not np.abs(g[key] - r[key]).max() <= 1e-10 * qs:
+            bad.append(f"{key}: {g[key]} vs {r[key]}")
+    assert not bad, name + "\n" + "\n".join(bad)
