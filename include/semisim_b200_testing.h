@@ -17,6 +17,10 @@ extern "C" {
 int b200x_prepare(void);
 /* per node: kind, contact id + 1, gate id + 1, Robin area (m^2) */
 int b200x_masks(int *kind, int *con, int *gate, double *robA);
+/* the incomplete-ionisation constants of the prepared device, 4 per node (two donor
+   sites, the acceptor, the neutral majority density); returns 4, or 0 when every dopant
+   is fully ionised (semiconductor_3d.c:1472-1510) */
+int b200x_ion(double *out);
 /* device state arrays: 0 psi, 1 phi_n, 2 phi_p, 3 n, 4 p, 5/6 low-field mobility n/p,
    7 sol, 8 rhs, 9 sc, 10 dsc, 16..21 face mobility (n x,y,z; p x,y,z), 22..24 sweep history
    h1 (psi, phi_n, phi_p now), 25..27 e2 (one step back) */

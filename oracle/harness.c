@@ -202,6 +202,14 @@ double hx_bicg_floor(const double *b, const double *x){
     return sqrt(fl);
 }
 
+/* incomplete-ionisation constants of the prepared device (ION_W per node), 0 when every
+   dopant is ionised */
+int hx_ion(double *out){
+    if(!gdev.ion) return 0;
+    if(out) memcpy(out,gdev.ion,ION_W*NN(&gdev)*sizeof(double));
+    return ION_W;
+}
+
 /* ---- scalar physics (semiconductor_3d.c:646-697) */
 double hx_B(double x){ return B(x); }
 double hx_mob_low(int mi, double N, int hole){ return mob_low(&gdev.mats[mi],N,hole); }
@@ -218,7 +226,9 @@ int hx_mat(int mi, double *out){
                 m->mu_n_max,m->mu_p_max,m->mu_n_min,m->mu_p_min,m->Nref_n,m->Nref_p,m->alpha_n,m->alpha_p,
                 m->mt_min,m->mt_max_n,m->mt_max_p,m->mt_Nref,m->mt_alpha,(double)m->mas_on,
                 m->vsat_n,m->vsat_p,m->beta_n,m->beta_p,m->tau_n0,m->tau_p0,m->Cn,m->Cp,m->Brad,m->tau_Nref,
-                m->bgn_E,m->bgn_N,m->bgn_C,m->lnc,m->lnv,(double)m->insulator,m->ani_n,m->ani_p};
+                m->bgn_E,m->bgn_N,m->bgn_C,m->lnc,m->lnv,(double)m->insulator,m->ani_n,m->ani_p,
+                (double)m->ion_on,m->ion_w[0],m->ion_w[1],m->ion_Ed[0],m->ion_Ed[1],m->ion_ad[0],m->ion_ad[1],
+                m->ion_gd,m->ion_Ea,m->ion_aa,m->ion_ga};
     memcpy(out,v,sizeof v);
     return (int)(sizeof v/sizeof v[0]);
 }

@@ -29,7 +29,9 @@ MAT_FIELDS = ["T", "VT", "Eg", "chi", "eps_r", "Nc", "Nv", "ni",
               "mu_n_max", "mu_p_max", "mu_n_min", "mu_p_min", "Nref_n", "Nref_p", "alpha_n", "alpha_p",
               "mt_min", "mt_max_n", "mt_max_p", "mt_Nref", "mt_alpha", "mas_on",
               "vsat_n", "vsat_p", "beta_n", "beta_p", "tau_n0", "tau_p0", "Cn", "Cp", "Brad", "tau_Nref",
-              "bgn_E", "bgn_N", "bgn_C", "lnc", "lnv", "insulator", "ani_n", "ani_p"]
+              "bgn_E", "bgn_N", "bgn_C", "lnc", "lnv", "insulator", "ani_n", "ani_p",
+              "ion_on", "ion_w0", "ion_w1", "ion_Ed0", "ion_Ed1", "ion_ad0", "ion_ad1",
+              "ion_gd", "ion_Ea", "ion_aa", "ion_ga"]
 MF = {n: i for i, n in enumerate(MAT_FIELDS)}
 
 
@@ -85,6 +87,111 @@ def pK(dev, psi, qp):
     """semiconductor_3d.c:742-744"""
     with np.errstate(over="ignore", invalid="ignore"):
         return np.exp(clampe(lnvK(dev) + (qp - psi) / matp(dev, "VT")))
+
+
+# ------------------------------------------------------------------ incomplete ionisation
+def _ion_fields(dev):
+    return dev["mats"].shape[1] > MF["ion_ga"]
+
+
+def ion_consts(dev):
+    """Per-node ionisation constants (semiconductor_3d.c:1472-1510): N_c/g_D e^(-dE_s/kT)
+    of the two donor sites, N_v/g_A e^(-dE_A/kT), dE = dE0 - alpha N^(1/3) clamped at 0,
+    and the neutral majority density |n - p| at the neutral potential; None when models
+    bit 9 is off or no semiconductor material has level data."""
+    if not (dev["models"] & 512) or not _ion_fields(dev):
+        return None
+    mats = dev["mats"]
+    if not np.any((mats[:, MF["ion_on"]] != 0) & (mats[:, MF["insulator"]] == 0)):
+        return None
+    N = len(dev["Nd"])
+    x = np.zeros((N, 4))
+    on = (dev["kind"] == K_SEMI) & (matp(dev, "ion_on") != 0)
+    VT = matp(dev, "VT")
+    Nd, Na = dev["Nd"], dev["Na"]
+    cd = np.cbrt(Nd)
+    for s_ in range(2):
+        E = np.maximum(matp(dev, f"ion_Ed{s_}") - matp(dev, f"ion_ad{s_}") * cd, 0.0)
+        x[:, s_] = np.where(on & (Nd > 0), matp(dev, "Nc") / matp(dev, "ion_gd") * np.exp(-E / VT), 0.0)
+    E = np.maximum(matp(dev, "ion_Ea") - matp(dev, "ion_aa") * np.cbrt(Na), 0.0)
+    x[:, 2] = np.where(on & (Na > 0), matp(dev, "Nv") / matp(dev, "ion_ga") * np.exp(-E / VT), 0.0)
+    d2 = dict(dev)
+    d2["ion"] = x
+    io = ion_node(d2)
+    psi = neutral_psi(d2, 0.0)
+    n, p = nK(d2, psi, 0.0), pK(d2, psi, 0.0)
+    x[:, 3] = np.where(io, np.abs(n - p), 0.0)
+    return x
+
+
+def ion_node(dev):
+    """semiconductor_3d.c:755-757"""
+    x = dev.get("ion")
+    if x is None:
+        return np.zeros(len(dev["Nd"]), bool)
+    return ((x[:, 0] > 0) & (dev["Nd"] > 0)) | ((x[:, 2] > 0) & (dev["Na"] > 0))
+
+
+def ion_eval(dev, n, p):
+    """Ionised donor / acceptor densities and their psi-derivatives at fixed quasi-Fermi
+    potentials (semiconductor_3d.c:758-777); fully ionised where no constants apply."""
+    Nd, Na = dev["Nd"], dev["Na"]
+    x = dev.get("ion")
+    if x is None:
+        z = np.zeros_like(Nd)
+        return Nd.copy(), z, Na.copy(), z.copy()
+    VT = matp(dev, "VT")
+    e = dev["bgn"]
+    w0, w1 = matp(dev, "ion_w0"), matp(dev, "ion_w1")
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        ne = np.where(e != 0, n * np.exp(-e), n)
+        don = (Nd > 0) & (x[:, 0] > 0)
+        a = ne / np.where(don, x[:, 0], 1.0)
+        f = w0 / (1 + a)
+        df = -w0 * a / ((1 + a) * (1 + a))
+        two = don & (w1 > 0) & (x[:, 1] > 0)
+        b = ne / np.where(two, x[:, 1], 1.0)
+        f = np.where(two, f + w1 / (1 + b), f)
+        df = np.where(two, df - w1 * b / ((1 + b) * (1 + b)), df)
+        Np = np.where(don, Nd * f, Nd)
+        dNp = np.where(don, Nd * df / VT, 0.0)
+        pe = np.where(e != 0, p * np.exp(-e), p)
+        acc = (Na > 0) & (x[:, 2] > 0)
+        c = pe / np.where(acc, x[:, 2], 1.0)
+        Nm = np.where(acc, Na / (1 + c), Na)
+        dNm = np.where(acc, Na * c / ((1 + c) * (1 + c) * VT), 0.0)
+    return Np, dNp, Nm, dNm
+
+
+def neutral_psi(dev, V):
+    """Neutral potential with both quasi-Fermi levels at V (semiconductor_3d.c:1782-1805):
+    closed form, then on incompletely ionised nodes the safeguarded Newton on
+    p - n + N_D+ - N_A- + Nf = 0 (no traps in scope), each node stopping on its own."""
+    VT = matp(dev, "VT")
+    D = dev["Nd"] - dev["Na"]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        psi = V + VT * (np.arcsinh(D / (2.0 * niK(dev))) - 0.5 * (lncK(dev) - lnvK(dev)))
+    act = ion_node(dev).copy()
+    if not act.any():
+        return psi
+    Eg = matp(dev, "Eg")
+    lo, hi = psi - Eg - 1.0, psi + Eg + 1.0
+    for _ in range(200):
+        if not act.any():
+            break
+        n, p = nK(dev, psi, V), pK(dev, psi, V)
+        Np, dNp, Nm, dNm = ion_eval(dev, n, p)
+        g = p - n + Np - Nm + dev["Nf"]
+        dg = -(n + p) / VT + dNp - dNm
+        lo = np.where(act & (g > 0), psi, lo)
+        hi = np.where(act & ~(g > 0), psi, hi)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            nx = np.where(dg < 0, psi - g / dg, 0.5 * (lo + hi))
+        nx = np.where((nx > lo) & (nx < hi), nx, 0.5 * (lo + hi))
+        done = np.abs(nx - psi) < 1e-13 * (1.0 + np.abs(psi))
+        psi = np.where(act, nx, psi)
+        act = act & ~done
+    return psi
 
 
 def tauf(dev):
@@ -204,8 +311,9 @@ def poisson_eval(dev, phi, g=None):
     n = nK(dev, phi, dev["phin"])
     p = pK(dev, phi, dev["phip"])
     VT = matp(dev, "VT")
-    F += np.where(semi, g.vol * Q * (p - n + dev["Nd"] - dev["Na"] + dev["Nf"]), g.vol * Q * dev["Nf"])
-    dg += np.where(semi, g.vol * Q * (n + p) / VT, 0.0)
+    Np, dNp, Nm, dNm = ion_eval(dev, n, p)          # the doping itself where fully ionised
+    F += np.where(semi, g.vol * Q * (p - n + Np - Nm + dev["Nf"]), g.vol * Q * dev["Nf"])
+    dg += np.where(semi, g.vol * Q * ((n + p) / VT - dNp + dNm), 0.0)
     A = np.vstack([dg[None, :], off])
     sc = dg.copy()
     F[isdir] = 0.0

@@ -23,6 +23,7 @@ _VP = ctypes.c_void_p
 HOOKS = {
     "b200x_prepare": (_I, []),
     "b200x_masks": (_I, [_IP, _IP, _IP, _DP]),
+    "b200x_ion": (_I, [_DP]),
     "b200x_set": (_I, [_I, _DP]),
     "b200x_get": (_I, [_I, _DP]),
     "b200x_vlo": (_D, []),

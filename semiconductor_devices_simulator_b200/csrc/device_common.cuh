@@ -168,6 +168,45 @@ __device__ __forceinline__ double nK(const DevP &P, const MatD &m, int k, double
 __device__ __forceinline__ double pK(const DevP &P, const MatD &m, int k, double psi, double qp) {
     return exp(clampe(lnvK(P, m, k) + (qp - psi) / m.VT));
 }
+// Incomplete ionisation (semiconductor_3d.c:749-786): P.ion holds per node N_c/g_D e^(-dE/kT)
+// of the two donor sites, N_v/g_A e^(-dE_A/kT) (m^-3; 0 = fully ionised) and the node's
+// majority density when neutral.  ion_eval gives the ionised donor and acceptor densities at
+// carrier densities n, p and their psi-derivatives at fixed quasi-Fermi potentials.
+__device__ __forceinline__ bool ion_node(const DevP &P, int k) {
+    if (!P.ion) return false;
+    const double *x = P.ion + (size_t)ION_W * k;
+    return (x[0] > 0.0 && P.Nd[k] > 0.0) || (x[2] > 0.0 && P.Na[k] > 0.0);
+}
+__device__ __forceinline__ void ion_eval(const DevP &P, const MatD &m, int k, double n, double p, double &Np,
+                                         double &dNp, double &Nm, double &dNm) {
+    const double Nd = P.Nd[k], Na = P.Na[k];
+    Np = Nd; Nm = Na; dNp = dNm = 0.0;
+    if (!P.ion) return;
+    const double *x = P.ion + (size_t)ION_W * k;
+    const double VT = m.VT, e = bgn_of(P, k);
+    if (Nd > 0.0 && x[0] > 0.0) {
+        const double ne = e != 0.0 ? n * exp(-e) : n;
+        const double a = ne / x[0];
+        double f = m.ion_w[0] / (1.0 + a), df = -m.ion_w[0] * a / ((1.0 + a) * (1.0 + a));
+        if (m.ion_w[1] > 0.0 && x[1] > 0.0) {
+            const double b = ne / x[1];
+            f += m.ion_w[1] / (1.0 + b);
+            df -= m.ion_w[1] * b / ((1.0 + b) * (1.0 + b));
+        }
+        Np = Nd * f; dNp = Nd * df / VT;
+    }
+    if (Na > 0.0 && x[2] > 0.0) {
+        const double pe = e != 0.0 ? p * exp(-e) : p;
+        const double c = pe / x[2];
+        Nm = Na / (1.0 + c); dNm = Na * c / ((1.0 + c) * (1.0 + c) * VT);
+    }
+}
+// the doping scale of the quasi-neutral tests: |Nd - Na|, or the neutral majority density
+__device__ __forceinline__ double dnet_ion(const DevP &P, int k) {
+    if (!ion_node(P, k)) return fabs(P.Nd[k] - P.Na[k]);
+    return P.ion[(size_t)ION_W * k + 3];
+}
+
 // SRH lifetime doping factor (semiconductor_3d.c:787-791)
 __device__ __forceinline__ double tauf(const DevP &P, const MatD &m, int k) {
     if (!(P.models & 2) || !(m.tau_Nref > 0.)) return 1.0;

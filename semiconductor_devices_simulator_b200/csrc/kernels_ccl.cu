@@ -24,7 +24,7 @@ __device__ __forceinline__ bool ff_maj(const DevP &P, int k, int hole) {
     if (fl_kind(f) != K_SEMI || fl_con(f)) return false;
     const double s = P.sc[k], c = s * P.sol[k];
     const double oth = hole ? P.n[k] : P.p[k];
-    const double hd = 0.5 * fabs(P.Nd[k] - P.Na[k]);
+    const double hd = 0.5 * dnet_ion(P, k);
     const MatD &m = P.mats[fl_mat(f)];
     return c >= oth && c >= hd && s >= hd && c > 10.0 * niK(P, m, k);
 }

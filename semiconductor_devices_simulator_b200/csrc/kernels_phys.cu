@@ -62,8 +62,15 @@ __global__ void k_poisson(const DevP *__restrict__ Ps, int src, int build) {
         const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
         if (fl_kind(f) == K_SEMI) {
             const double n = nK(P, m, k, pk, P.phin[k]), p = pK(P, m, k, pk, P.phip[k]);
-            fk += vol * Q * (p - n + P.Nd[k] - P.Na[k] + P.Nf[k]);
-            dg += vol * Q * (n + p) / m.VT;
+            if (ion_node(P, k)) {                 // incompletely ionised dopants
+                double Np, dNp, Nm, dNm;
+                ion_eval(P, m, k, n, p, Np, dNp, Nm, dNm);
+                fk += vol * Q * (p - n + Np - Nm + P.Nf[k]);
+                dg += vol * Q * ((n + p) / m.VT - dNp + dNm);
+            } else {
+                fk += vol * Q * (p - n + P.Nd[k] - P.Na[k] + P.Nf[k]);
+                dg += vol * Q * (n + p) / m.VT;
+            }
         } else {
             fk += vol * Q * P.Nf[k];
         }
@@ -248,11 +255,42 @@ void launch_cont_update(const Ctx &c, int hole, double lo, double hi) {
 }
 
 // ------------------------------------------------------------------ boundary values
-// neutral potential with both quasi-Fermi levels at V, closed form (semiconductor_3d.c:1787-1790)
-__device__ __forceinline__ double neutral_psi(const DevP &P, const MatD &m, int k, double V) {
-    const double D = P.Nd[k] - P.Na[k];
-    return V + m.VT * (asinh(D / (2.0 * niK(P, m, k))) - 0.5 * (lncK(P, m, k) - lnvK(P, m, k)));
+// neutral potential with both quasi-Fermi levels at V (semiconductor_3d.c:1782-1805): the
+// closed form, and with incompletely ionised dopants a safeguarded Newton on
+// p - n + N_D+ - N_A- + Nf = 0 (decreasing in psi) from it, at most 200 steps
+__device__ double neutral_psi(const DevP &P, const MatD &m, int k, double V) {
+    const double D = P.Nd[k] - P.Na[k], VT = m.VT;
+    double psi = V + VT * (asinh(D / (2.0 * niK(P, m, k))) - 0.5 * (lncK(P, m, k) - lnvK(P, m, k)));
+    if (!ion_node(P, k)) return psi;
+    double lo = psi - m.Eg - 1.0, hi = psi + m.Eg + 1.0;
+    for (int it = 0; it < 200; it++) {
+        const double n = nK(P, m, k, psi, V), p = pK(P, m, k, psi, V);
+        double Np, dNp, Nm, dNm;
+        ion_eval(P, m, k, n, p, Np, dNp, Nm, dNm);
+        const double g = p - n + Np - Nm + P.Nf[k], dg = -(n + p) / VT + dNp - dNm;
+        if (g > 0.0) lo = psi; else hi = psi;
+        double nx = dg < 0.0 ? psi - g / dg : 0.5 * (lo + hi);
+        if (!(nx > lo && nx < hi)) nx = 0.5 * (lo + hi);
+        if (fabs(nx - psi) < 1e-13 * (1.0 + fabs(psi))) { psi = nx; break; }
+        psi = nx;
+    }
+    return psi;
 }
+
+// the neutral majority density of every incompletely ionised node, slot 3 of its
+// ionisation constants (semiconductor_3d.c:1502-1508)
+__global__ void k_ion_neutral(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    if (!P.ion) return;
+    SS_GRID_LOOP(k, P.N) {
+        if (!ion_node(P, k)) continue;
+        const MatD &m = P.mats[fl_mat(P.flags[k])];
+        const double ps = neutral_psi(P, m, k, 0.0);
+        const double n = nK(P, m, k, ps, 0.0), p = pK(P, m, k, ps, 0.0);
+        P.ion[(size_t)ION_W * k + 3] = fabs(n - p);
+    }
+}
+void launch_ion_neutral(const Ctx &c) { SS_LAUNCH(PF_BC, c.maxN, k_ion_neutral, grid_of(c), TPB, c.st, c.dP); }
 
 // Dirichlet values of every contact node at the stage voltages (semiconductor_3d.c:1806-1829)
 __global__ void k_apply_bc(const DevP *__restrict__ Ps) {
@@ -396,7 +434,7 @@ __global__ void k_predictor(const DevP *__restrict__ Ps) {
         const double ps = P.phi[k];
         P.xk[k] = ps;
         if (fl_kind(f) != K_SEMI || fl_con(f)) continue;
-        const double n = P.n[k], p = P.p[k], D = fabs(P.Nd[k] - P.Na[k]);
+        const double n = P.n[k], p = P.p[k], D = dnet_ion(P, k);
         const double den = fmax(n + p, D);
         if (!(den > 0.0)) continue;
         P.phi[k] = ps + (n * P.dqn[k] + p * P.dqp[k]) / den;
@@ -522,7 +560,13 @@ __global__ void k_node_val(const DevP *__restrict__ Ps, int which, double *out) 
         case 31: case 32: v = kd == K_SEMI ? 0.0 : nan; break;   // traps: not built
         case 33: v = 0.0; break;                                 // impact ionisation: not built
         case 34: v = kd == K_SEMI ? 0.0 : nan; break;            // Coulomb N_C: not built
-        case 35: v = kd == K_SEMI ? P.Nd[k] - P.Na[k] : 0.0; break;
+        case 35: {                                  // ionised net doping N_D+ - N_A-
+            if (kd != K_SEMI) { v = 0.0; break; }
+            double Np, dNp, Nm, dNm;
+            ion_eval(P, m, k, P.n[k], P.p[k], Np, dNp, Nm, dNm);
+            v = Np - Nm;
+            break;
+        }
         default: v = 0.0;
         }
         out[k] = v;

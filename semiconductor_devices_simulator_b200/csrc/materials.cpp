@@ -98,7 +98,12 @@ void material_init(Material &m, int id, double T) {
         set_lowfield(m, {0.095, 0.0124, 0.0040, 0.00159, 1.94e23, 1.76e25, 0.61, 0.34, -0.5, -2.40, -2.15, 0., 0.});
         set_sat(m, {2.2e5, 1.6e5, 1.2, 1.});
         set_recomb(m, {1e-6, 1e-7, 5e-44, 2e-44, 1.5e-18});
-        m.ii_on = 1; m.lb_on = 1; m.lbc_on = 1; m.ion_on = 1;
+        m.ii_on = 1; m.lb_on = 1; m.lbc_on = 1;
+        // nitrogen on the hexagonal and cubic sites (1:1), aluminium acceptors
+        // (semiconductor_3d.c:553-555)
+        m.ion_on = 1; m.ion_w[0] = m.ion_w[1] = 0.5;
+        m.ion_Ed[0] = 0.0709; m.ion_ad[0] = 3.38e-10; m.ion_Ed[1] = 0.1237; m.ion_ad[1] = 4.65e-10; m.ion_gd = 2.;
+        m.ion_Ea = 0.225; m.ion_aa = 3.2e-10; m.ion_ga = 4.;
         m.ani_n = 1. / 0.83; m.ani_p = 1. / 1.15;
         break;
     case 5:     // GaN

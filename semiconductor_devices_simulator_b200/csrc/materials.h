@@ -21,8 +21,13 @@ struct Material {
     double tau_n0 = 0, tau_p0 = 0, Cn = 0, Cp = 0, Brad = 0, tau_Nref = 0;
     double bgn_E = 0, bgn_N = 1, bgn_C = 0;
     double ani_n = 0, ani_p = 0;
+    // incomplete ionisation (models bit 9): donors on up to two lattice sites with weights
+    // ion_w, level depth dE = ion_Ed - ion_ad N^(1/3) (eV, eV m; clamped at 0) below Ec and
+    // degeneracy ion_gd; acceptors one level ion_Ea - ion_aa N^(1/3) above Ev, degeneracy ion_ga
+    int ion_on = 0;
+    double ion_w[2] = {0, 0}, ion_Ed[2] = {0, 0}, ion_ad[2] = {0, 0}, ion_gd = 1, ion_Ea = 0, ion_aa = 0, ion_ga = 1;
     // models outside this library's scope that the material would switch on
-    int lb_on = 0, lbc_on = 0, ion_on = 0, ii_on = 0;
+    int lb_on = 0, lbc_on = 0, ii_on = 0;
     double lnc = 0, lnv = 0;      // effective ln Nc / ln Nv in the common gauge (mat_prepare)
 };
 

@@ -24,6 +24,7 @@ constexpr int TPB = 256;            // threads per block of the node kernels
 constexpr int RED_MAX_BLOCKS = 2048; // grid cap of reducing kernels (partials per instance)
 constexpr int RED_NV = 16;          // doubles per block partial record
 constexpr int COARSE_MAX = 64;      // unknowns of the coarsest multigrid level
+constexpr int ION_W = 4;            // doubles per node of the ionisation constants
 
 // per-node flag word: kind(2) | contact+1 (6) | gate+1 (6) | material (4) | car_fix (1)
 __host__ __device__ inline int fl_kind(uint32_t f) { return int(f & 3u); }
@@ -42,6 +43,7 @@ struct MatD {
     double tau_n0, tau_p0, Cn, Cp, Brad, tau_Nref;
     double vsat_n, vsat_p, beta_n, beta_p, ani_n, ani_p;
     double chi, Eg;
+    double ion_w[2];             // donor site weights of incomplete ionisation
     int insulator, pad;
 };
 
@@ -82,6 +84,7 @@ struct DevP {
     const uint32_t *flags;
     const double *Nd, *Na, *Nf, *bgn, *robA;
     const double *qd;             // distance to the nearest insulator / gate wall (display)
+    double *ion;                  // incomplete ionisation, ION_W per node (null: every dopant ionised)
     const MatD *mats;
     const ConD *cons;
     const int *cnode;             // contact-node list (semiconductor nodes of carrier contacts)

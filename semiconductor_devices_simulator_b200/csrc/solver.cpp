@@ -204,6 +204,7 @@ void gpu_free(Inst &d) {
     if (d.g.scratch) cudaFree(d.g.scratch);
     if (d.g.flag) cudaFree(d.g.flag);
     if (d.g.qown) cudaFree(d.g.qown);
+    if (d.g.ion) cudaFree(d.g.ion);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();
@@ -350,7 +351,6 @@ static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
         if (m.insulator) continue;
         if ((d.models & 16) && m.lb_on && (any_ins || any_gate) && used(mi)) why = "surface mobility (models bit 4)";
         if ((d.models & 256) && m.ii_on && used(mi)) why = "impact ionisation (models bit 8)";
-        if ((d.models & 512) && m.ion_on && used(mi)) why = "incomplete ionisation (models bit 9)";
     }
     if (why) {
         std::fprintf(stderr, "semisim-b200: %s is not supported by this solver library\n", why);
@@ -480,12 +480,46 @@ int prepare(Inst &d) {
     }
     std::vector<double> qd;
     wall_distance(d, kind, gate, qd);
+    // incomplete ionisation (semiconductor_3d.c:1472-1510): per node the constants
+    // N_c/g_D e^(-dE_s/kT) of the two donor sites and N_v/g_A e^(-dE_A/kT), the level depths
+    // falling with the node's own dopant density; the neutral majority density (slot 3)
+    // follows on the device
+    bool want_ion = false;
+    std::vector<double> ionx;
+    if (d.models & 512)
+        for (int q = 0; q < d.n_mats; q++) if (d.mats[q].ion_on && !d.mats[q].insulator) want_ion = true;
+    if (want_ion) {
+        ionx.assign((size_t)ION_W * N, 0.0);
+        for (size_t k = 0; k < N; k++) {
+            if (kind[k] != K_SEMI) continue;
+            const Material &m = d.mats[d.mat_idx[k]];
+            if (!m.ion_on) continue;
+            double *x = ionx.data() + (size_t)ION_W * k;
+            if (d.Nd[k] > 0.) {
+                const double c = std::cbrt(d.Nd[k]);
+                for (int s_ = 0; s_ < 2; s_++) {
+                    const double E = std::fmax(m.ion_Ed[s_] - m.ion_ad[s_] * c, 0.);
+                    x[s_] = m.Nc / m.ion_gd * std::exp(-E / m.VT);
+                }
+            }
+            if (d.Na[k] > 0.) {
+                const double E = std::fmax(m.ion_Ea - m.ion_aa * std::cbrt(d.Na[k]), 0.);
+                x[2] = m.Nv / m.ion_ga * std::exp(-E / m.VT);
+            }
+        }
+    }
     if (!gpu_alloc(d)) return 0;
+    if (want_ion && !d.g.ion && cudaMalloc(&d.g.ion, (size_t)ION_W * N * sizeof(double)) != cudaSuccess) {
+        d.g.ion = nullptr;
+        std::fprintf(stderr, "semisim-b200: out of device memory for the ionisation constants\n");
+        return 0;
+    }
     // upload
     DevP &P = d.g.h;
     P.models = d.models; P.caxis = d.caxis; P.ncon = d.n_cons; P.ref_mat = d.ref_mat;
     P.VTref = d.mats[d.ref_mat].VT; P.Cref = d.Cref;
     P.ncnode = (int)d.cnode.size();
+    P.ion = want_ion ? d.g.ion : nullptr;
     MatD md[NM_MAX];
     std::memset(md, 0, sizeof md);
     for (int i = 0; i < d.n_mats; i++) {
@@ -495,6 +529,7 @@ int prepare(Inst &d) {
         o.tau_n0 = m.tau_n0; o.tau_p0 = m.tau_p0; o.Cn = m.Cn; o.Cp = m.Cp; o.Brad = m.Brad; o.tau_Nref = m.tau_Nref;
         o.vsat_n = m.vsat_n; o.vsat_p = m.vsat_p; o.beta_n = m.beta_n; o.beta_p = m.beta_p;
         o.ani_n = m.ani_n; o.ani_p = m.ani_p; o.chi = m.chi; o.Eg = m.Eg; o.insulator = m.insulator;
+        o.ion_w[0] = m.ion_on ? m.ion_w[0] : 0.; o.ion_w[1] = m.ion_on ? m.ion_w[1] : 0.;
     }
     cudaStream_t st = d.g.st;
     CK(cudaMemcpyAsync((void *)P.mats, md, sizeof md, cudaMemcpyHostToDevice, st));
@@ -515,7 +550,10 @@ int prepare(Inst &d) {
     CK(cudaMemcpyAsync((void *)P.Lx, d.Lx.data(), d.Nx * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync((void *)P.Ly, d.Ly.data(), d.Ny * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync((void *)P.Lz, d.Lz.data(), d.Nz * 8, cudaMemcpyHostToDevice, st));
+    if (want_ion)
+        CK(cudaMemcpyAsync(d.g.ion, ionx.data(), ionx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(d.g.d, &P, sizeof(DevP), cudaMemcpyHostToDevice, st));
+    if (want_ion) launch_ion_neutral(make_ctx(d));
     CK(cudaStreamSynchronize(st));
     d.g.mg.alpha = g_knobs.mg_alpha;
     d.dirty = 0;

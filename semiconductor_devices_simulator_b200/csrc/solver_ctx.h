@@ -46,6 +46,7 @@ struct Gpu {
     double *pin = nullptr;       // pinned host scratch (results)
     double *scratch = nullptr;   // device scratch (bulk output)
     int *flag = nullptr;         // device int scratch
+    double *ion = nullptr;       // incomplete-ionisation constants (ION_W x N), when a material needs them
     int *qown = nullptr;         // charge-partition owners (N, dense terminal slots), uploaded on first use
     bool qown_ok = false;
     int qown_nt = 0;             // the terminal count they were numbered for

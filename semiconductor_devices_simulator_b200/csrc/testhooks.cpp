@@ -67,6 +67,16 @@ int b200x_masks(int *kind, int *con, int *gate, double *robA) {
     }
     return 1;
 }
+// the device's incomplete-ionisation constants (ION_W x N); 0 when every dopant is ionised
+int b200x_ion(double *out) {
+    Inst &d = *dev();
+    if (!d.g.ready || !d.g.h.ion) return 0;
+    if (out) {
+        cudaMemcpyAsync(out, d.g.h.ion, (size_t)ION_W * d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
+        sync(d);
+    }
+    return ION_W;
+}
 int b200x_set(int which, const double *in) {
     Inst &d = *dev();
     double *a = arr(d, which);

@@ -25,7 +25,7 @@ import numpy as np
 
 from .abi import dptr, iptr
 
-SI, SIO2 = 0, 8                     # material ids of semiconductor_3d.c:430, :560
+SI, SIC, SIO2 = 0, 4, 8             # material ids of semiconductor_3d.c:431, :513, :600
 GUI_SOLVER = (2000, 1000, 500, 1e-8, 1e-6, 1.0, 1.0)   # main.py:3286 default tuple
 
 
@@ -58,8 +58,9 @@ def _grid(lib, xs, ys, zs):
 
 def pn_diode(lib, n=(40, 40, 40), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj=0.5e-6,
              mobility=(1350.0, 480.0), tau=1e-7, models=0, solver=GUI_SOLVER, vmax=0.6,
-             dv=0.05):
-    """Abrupt Si pn diode; the anode (x = 0, p side) is swept 0..vmax."""
+             dv=0.05, material=None):
+    """Abrupt pn diode (silicon unless `material` names another reference material id);
+    the anode (x = 0, p side) is swept 0..vmax."""
     lib.api3_init()
     xs = np.linspace(0.0, L[0], n[0])
     ys = np.linspace(0.0, L[1], n[1])
@@ -67,7 +68,7 @@ def pn_diode(lib, n=(40, 40, 40), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj=0.5
     _grid(lib, xs, ys, zs)
     lib.api3_set_solver(*solver)
     lib.api3_set_models(models)
-    si = lib.api3_add_material(SI, 300.0)
+    si = lib.api3_add_material(SI if material is None else material, 300.0)
     if mobility is not None:
         if not lib.api3_set_mat_mobility(si, mobility[0] * 1e-4, mobility[1] * 1e-4):
             raise RuntimeError("api3_set_mat_mobility failed")

@@ -10,6 +10,9 @@ semiconductor_3d.c #included, plus dump hooks) on small seeded devices and write
                 narrowing, tau(N), velocity saturation)
   moscap_small  Si / SiO2 stack 8x10x4 with a metal gate electrode on the oxide and a
                 Schottky back contact (insulator and metal node kinds)
+  sic_small     4H-SiC pn diode 14x5x4 (p+ 1e18 / n 1e16 cm^-3), models 519: band-gap
+                narrowing, tau(N), velocity saturation and incomplete ionisation of the
+                nitrogen donors and aluminium acceptors; anode swept 0..2.8 V
 
 Each file holds the prepared device (masks, geometry, materials, contacts), a
 converged state and, at a perturbed state, the outputs of the per-node kernels
@@ -50,7 +53,7 @@ HX = {
     "hx_mg_setup": (_I, [_I]), "hx_mg_level": (_I, [_I, _IP, _DP, _DP, _DP]),
     "hx_mg_matvec": (_I, [_I, _DP, _DP]), "hx_mg_restrict": (_I, [_I, _DP, _DP]),
     "hx_mg_prolong": (_I, [_I, _DP, _DP]), "hx_bicg_floor": (_D, [_DP, _DP]),
-    "hx_B": (_D, [_D]), "hx_mat": (_I, [_I, _DP]),
+    "hx_B": (_D, [_D]), "hx_mat": (_I, [_I, _DP]), "hx_ion": (_I, [_DP]),
 }
 W_PHI, W_PHIN, W_PHIP, W_N, W_P, W_MUN, W_MUP, W_BGN, W_EPS, W_ND, W_NA, W_NF = range(12)
 
@@ -92,11 +95,17 @@ def device_record(lib, w):
     zs = np.array([lib.api3_get_zs(i) for i in range(Nz)])
     # material index per node: recovered from eps and the Nd/Na layout is not unique,
     # so the builders' material ids are passed explicitly
-    return dict(dims=np.array(w.shape), xs=xs, ys=ys, zs=zs, kind=kind, con=con, gate=gate,
-                rob_k=rk[:nrob], rob_A=rA[:nrob], rob_c=rc[:nrob], con_A=area,
-                mats=np.array(mats), Cref=lib.hx_cref(),
-                Nd=get(lib, W_ND, N), Na=get(lib, W_NA, N), Nf=get(lib, W_NF, N),
-                bgn=get(lib, W_BGN, N), eps=get(lib, W_EPS, N))
+    rec = dict(dims=np.array(w.shape), xs=xs, ys=ys, zs=zs, kind=kind, con=con, gate=gate,
+               rob_k=rk[:nrob], rob_A=rA[:nrob], rob_c=rc[:nrob], con_A=area,
+               mats=np.array(mats), Cref=lib.hx_cref(),
+               Nd=get(lib, W_ND, N), Na=get(lib, W_NA, N), Nf=get(lib, W_NF, N),
+               bgn=get(lib, W_BGN, N), eps=get(lib, W_EPS, N))
+    nw = lib.hx_ion(None)
+    if nw:                                   # incomplete-ionisation constants, (N, 4)
+        ion = np.zeros(nw * N)
+        lib.hx_ion(dptr(ion))
+        rec["ion"] = ion.reshape(N, nw)
+    return rec
 
 
 def state(lib, N):
@@ -226,6 +235,11 @@ def build(lib, name):
         w = D.nmosfet(lib, n=(16, 12, 6), models=7, vds=(0.5,), vg_max=1.0, dvg=0.25)
         mat = np.zeros(w.N, np.int32)
         bias = {w.contacts["gate"]: 0.8, w.contacts["drain"]: 0.5}
+    elif name == "sic_small":
+        w = D.pn_diode(lib, n=(14, 5, 4), NA=1e18, ND=1e16, material=D.SIC, mobility=None, tau=None,
+                       models=519, vmax=2.8, dv=0.4)
+        mat = np.zeros(w.N, np.int32)
+        bias = {w.contacts["anode"]: 2.6, w.contacts["cathode"]: 0.0}
     elif name == "moscap_small":
         w = moscap(lib)
         mat = w.info.pop("mat")
@@ -257,7 +271,7 @@ def moscap(lib, n=(8, 10, 4)):
                       [{"fixed": {"back": 0.0}, "swept": "gate", "V": V}], {"mat": mat.ravel()})
 
 
-def main(names=("diode_small", "mos_small", "moscap_small")):
+def main(names=("diode_small", "mos_small", "moscap_small", "sic_small")):
     lib = load_harness()
     lib.api3_set_threads(1)          # fixed thread count: the chunked ILU depends on it
     for name in names:
@@ -283,4 +297,4 @@ def main(names=("diode_small", "mos_small", "moscap_small")):
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("diode_small", "mos_small", "moscap_small"))
+    main(tuple(sys.argv[1:]) or ("diode_small", "mos_small", "moscap_small", "sic_small"))

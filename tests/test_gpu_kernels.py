@@ -21,7 +21,7 @@ import semiconductor_devices_simulator_b200 as S  # noqa: E402
 from semiconductor_devices_simulator_b200.abi import dptr, iptr  # noqa: E402
 
 pytestmark = pytest.mark.gpu
-NAMES = ["diode_small", "mos_small", "moscap_small"]
+NAMES = ["diode_small", "mos_small", "moscap_small", "sic_small"]
 
 
 def golden(name):
@@ -270,3 +270,19 @@ def test_refined_pcg_matches_fp64(lib, refined, name):
     assert its32 <= its64 + 3, (its32, its64)
     assert res32 <= 1e-3 * nF and res64 <= 1e-3 * nF, (res32, res64, nF)
     assert np.abs(sol32 - sol64).max() <= 1e-3 * np.abs(sol64).max()
+
+
+def test_ionisation_constants(lib):
+    """The device's incomplete-ionisation constants of the 4H-SiC diode (level constants
+    of the nitrogen sites and the aluminium acceptor from the host, the neutral majority
+    density from the device's Newton on the neutrality condition) against the reference's."""
+    g, w = setup(lib, "sic_small")
+    N = w.N
+    assert lib.b200x_ion(None) == 4
+    x = np.zeros(4 * N)
+    assert lib.b200x_ion(dptr(x)) == 4
+    x = x.reshape(N, 4)
+    close(x[:, :3], g["ion"][:, :3], 1e-14, what="level constants")
+    close(x[:, 3], g["ion"][:, 3], 1e-11, what="neutral majority density")
+    g2, w2 = setup(lib, "diode_small")
+    assert lib.b200x_ion(None) == 0

@@ -28,7 +28,7 @@ from semiconductor_devices_simulator_b200 import abi  # noqa: E402
 from semiconductor_devices_simulator_b200.abi import dptr, iptr  # noqa: E402
 
 pytestmark = pytest.mark.gpu
-NAMES = ["diode_small", "mos_small", "moscap_small"]
+NAMES = ["diode_small", "mos_small", "moscap_small", "sic_small"]
 
 
 @pytest.fixture(scope="module")

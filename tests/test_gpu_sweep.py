@@ -22,7 +22,7 @@ import semiconductor_devices_simulator_b200 as S  # noqa: E402
 from semiconductor_devices_simulator_b200 import abi, devices as D  # noqa: E402
 
 pytestmark = pytest.mark.gpu
-NAMES = ["diode_small", "mos_small", "moscap_small"]
+NAMES = ["diode_small", "mos_small", "moscap_small", "sic_small"]
 PSI_TOL = 1e-6
 NP_RTOL, NP_FLOOR = 1e-6, 1e9
 I_RTOL = 1e-4

@@ -8,7 +8,7 @@ import pytest
 from oracle import restate as R
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ["diode_small", "mos_small", "moscap_small"]
+NAMES = ["diode_small", "mos_small", "moscap_small", "sic_small"]
 
 
 def load(name):
@@ -122,3 +122,21 @@ def test_multigrid_hierarchy(name):
         close(R.restrict(dims, cf, g[f"mg{L}_r"], w), g[f"mg{L}_rc"], rtol=1e-10, atol=1e-14 * np.abs(g[f"mg{L}_rc"]).max())
         xf = R.prolong_add(dims, cf, g[f"mg{L}_pw"], g[f"mg{L}_xc"], np.zeros(int(np.prod(dims))))
         close(xf, g[f"mg{L}_xf"], rtol=1e-14)
+
+
+def test_ionisation_constants():
+    """The incomplete-ionisation constants (two nitrogen donor sites, the aluminium
+    acceptor, the neutral majority density) restated from the material's level data
+    against the reference's own (4H-SiC diode, models bit 9)."""
+    g = load("sic_small")
+    d = dev_at(g, "pert_")
+    x = R.ion_consts(d)
+    assert x is not None and "ion" in g
+    close(x[:, :3], g["ion"][:, :3], rtol=1e-14)
+    close(x[:, 3], g["ion"][:, 3], rtol=1e-12)
+    # the ionised fraction of 1e18 cm^-3 aluminium at 300 K is a few per cent
+    n, p = d["n"], d["p"]
+    Np, dNp, Nm, dNm = R.ion_eval(d, n, p)
+    acc = (d["Na"] > 0) & (d["kind"] == 0)
+    assert 0.01 < np.median(Nm[acc] / d["Na"][acc]) < 0.2
+    assert np.all(dNp <= 0) and np.all(dNm >= 0)
