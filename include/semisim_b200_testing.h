@@ -21,6 +21,14 @@ int b200x_masks(int *kind, int *con, int *gate, double *robA);
    sites, the acceptor, the neutral majority density); returns 4, or 0 when every dopant
    is fully ionised (semiconductor_3d.c:1472-1510) */
 int b200x_ion(double *out);
+/* metal contacts (models bit 6): te_update at the contacts' voltages (returns 0 without
+   metal contacts), and the entry / column records: cnt[0] entries, cnt[1] column nodes;
+   emission terms te_K / te_G (2 per entry), column exchange terms tc_K / tc_G and
+   image-force lowering tc_I (2 per column node), per-node band lowering qcn / qcp (N);
+   null arrays are skipped (semiconductor_3d.c:3390-3571) */
+int b200x_te_update(void);
+int b200x_set_qc(const double *qcn, const double *qcp);   /* install an image-force band (N each) */
+int b200x_te(int *cnt, double *teK, double *teG, double *tcK, double *tcG, double *tcI, double *qcn, double *qcp);
 /* device state arrays: 0 psi, 1 phi_n, 2 phi_p, 3 n, 4 p, 5/6 low-field mobility n/p,
    7 sol, 8 rhs, 9 sc, 10 dsc, 16..21 face mobility (n x,y,z; p x,y,z), 22..24 sweep history
    h1 (psi, phi_n, phi_p now), 25..27 e2 (one step back) */

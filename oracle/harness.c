@@ -210,6 +210,32 @@ int hx_ion(double *out){
     return ION_W;
 }
 
+/* metal contacts: te_update at the contacts' stage voltages, and the entry / column
+   records (counts in cnt[2] = n_te, n_tc; arrays may be NULL) */
+void hx_te_update(void){
+    double Va[NC_MAX];
+    for(int c=0;c<gdev.n_cons;c++) Va[c]=gdev.cons[c].V;
+    te_update(&gdev,Va);
+}
+/* install an image-force band (qcn, qcp; N each) as te_update would have left it */
+void hx_set_qc(const double *qcn, const double *qcp){
+    size_t N=NN(&gdev);
+    memcpy(gdev.qcn,qcn,N*sizeof(double)); memcpy(gdev.qcp,qcp,N*sizeof(double));
+    if(gdev.imgn) memcpy(gdev.imgn,qcn,N*sizeof(double));
+    if(gdev.imgp) memcpy(gdev.imgp,qcp,N*sizeof(double));
+}
+int hx_te(int *cnt, double *teK, double *teG, double *tcK, double *tcG, double *tcI, double *qcn, double *qcp){
+    cnt[0]=gdev.n_te; cnt[1]=gdev.n_tc;
+    if(teK) memcpy(teK,gdev.te_K,2*gdev.n_te*sizeof(double));
+    if(teG) memcpy(teG,gdev.te_G,2*gdev.n_te*sizeof(double));
+    if(tcK) memcpy(tcK,gdev.tc_K,2*gdev.n_tc*sizeof(double));
+    if(tcG) memcpy(tcG,gdev.tc_G,2*gdev.n_tc*sizeof(double));
+    if(tcI) memcpy(tcI,gdev.tc_I,2*gdev.n_tc*sizeof(double));
+    if(qcn) memcpy(qcn,gdev.qcn,NN(&gdev)*sizeof(double));
+    if(qcp) memcpy(qcp,gdev.qcp,NN(&gdev)*sizeof(double));
+    return gdev.n_te;
+}
+
 /* ---- scalar physics (semiconductor_3d.c:646-697) */
 double hx_B(double x){ return B(x); }
 double hx_mob_low(int mi, double N, int hole){ return mob_low(&gdev.mats[mi],N,hole); }

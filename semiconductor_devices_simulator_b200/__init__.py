@@ -24,6 +24,9 @@ HOOKS = {
     "b200x_prepare": (_I, []),
     "b200x_masks": (_I, [_IP, _IP, _IP, _DP]),
     "b200x_ion": (_I, [_DP]),
+    "b200x_te_update": (_I, []),
+    "b200x_set_qc": (_I, [_DP, _DP]),
+    "b200x_te": (_I, [_IP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "b200x_set": (_I, [_I, _DP]),
     "b200x_get": (_I, [_I, _DP]),
     "b200x_vlo": (_D, []),

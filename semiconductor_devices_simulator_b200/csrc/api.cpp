@@ -132,6 +132,7 @@ void api3_init(void) {                                      // semiconductor_3d.
     if (const char *m = env_get("SEMISIM_GROW")) { const double gg = std::atof(m); if (gg >= 1. && gg <= 4.) g_knobs.grow_slow = gg; }
     if (const char *m = env_get("SEMISIM_CATOL")) g_knobs.cont_atol = std::atof(m);
     if (const char *m = env_get("SEMISIM_QFM")) g_knobs.qf_margin = std::atof(m);
+    if (const char *m = env_get("SEMISIM_TECOLVS")) g_knobs.te_colvs = std::atoi(m);
     if (const char *m = env_get("SEMISIM_B200_CHECK")) { const int q = std::atoi(m); if (q >= 1 && q <= 64) g_knobs.check_every = q; }
     if (const char *m = env_get("SEMISIM_B200_GRAPHS")) g_use_graphs = std::atoi(m) != 0;
     if (const char *m = env_get("SEMISIM_B200_PDL")) g_pdl = std::atoi(m) != 0;
@@ -529,7 +530,8 @@ int api3_charge_partition(const int *cterm) {
         if (c < 0 || c >= d.n_cons) continue;
         const int t = cterm[c];
         g_qown[k] = t;
-        if (t >= 0 && d.cons[c].bc == 0 && (kind_of(d, k) == K_SEMI || kind_of(d, k) == K_METAL)) qu.push_back(k);
+        if (t >= 0 && d.cons[c].bc == 0 && !d.cons[c].te && (kind_of(d, k) == K_SEMI || kind_of(d, k) == K_METAL))
+            qu.push_back(k);
     }
     size_t nb[6]; double cf[6], hh[6];
     while (qh < qu.size()) {

@@ -159,9 +159,14 @@ __device__ __forceinline__ bool nbr(const DevP &P, const Node &a, int k, int dir
 }
 
 __device__ __forceinline__ double bgn_of(const DevP &P, int k) { return P.bgn ? P.bgn[k] : 0.0; }
-__device__ __forceinline__ double lncK(const DevP &P, const MatD &m, int k) { return m.lnc + bgn_of(P, k); }
-__device__ __forceinline__ double lnvK(const DevP &P, const MatD &m, int k) { return m.lnv + bgn_of(P, k); }
-__device__ __forceinline__ double niK(const DevP &P, const MatD &m, int k) { return m.ni * exp(bgn_of(P, k)); }
+// image-force band lowering near metal contacts (0 elsewhere; semiconductor_3d.c:736-738)
+__device__ __forceinline__ double qcn_of(const DevP &P, int k) { return P.qcn ? P.qcn[k] : 0.0; }
+__device__ __forceinline__ double qcp_of(const DevP &P, int k) { return P.qcp ? P.qcp[k] : 0.0; }
+__device__ __forceinline__ double lncK(const DevP &P, const MatD &m, int k) { return m.lnc + bgn_of(P, k) + qcn_of(P, k); }
+__device__ __forceinline__ double lnvK(const DevP &P, const MatD &m, int k) { return m.lnv + bgn_of(P, k) + qcp_of(P, k); }
+__device__ __forceinline__ double niK(const DevP &P, const MatD &m, int k) {
+    return m.ni * exp(bgn_of(P, k) + 0.5 * (qcn_of(P, k) + qcp_of(P, k)));
+}
 __device__ __forceinline__ double nK(const DevP &P, const MatD &m, int k, double psi, double qn) {
     return exp(clampe(lncK(P, m, k) + (psi - qn) / m.VT));
 }
@@ -183,8 +188,9 @@ __device__ __forceinline__ void ion_eval(const DevP &P, const MatD &m, int k, do
     Np = Nd; Nm = Na; dNp = dNm = 0.0;
     if (!P.ion) return;
     const double *x = P.ion + (size_t)ION_W * k;
-    const double VT = m.VT, e = bgn_of(P, k);
+    const double VT = m.VT;
     if (Nd > 0.0 && x[0] > 0.0) {
+        const double e = bgn_of(P, k) + qcn_of(P, k);
         const double ne = e != 0.0 ? n * exp(-e) : n;
         const double a = ne / x[0];
         double f = m.ion_w[0] / (1.0 + a), df = -m.ion_w[0] * a / ((1.0 + a) * (1.0 + a));
@@ -196,6 +202,7 @@ __device__ __forceinline__ void ion_eval(const DevP &P, const MatD &m, int k, do
         Np = Nd * f; dNp = Nd * df / VT;
     }
     if (Na > 0.0 && x[2] > 0.0) {
+        const double e = bgn_of(P, k) + qcp_of(P, k);
         const double pe = e != 0.0 ? p * exp(-e) : p;
         const double c = pe / x[2];
         Nm = Na / (1.0 + c); dNm = Na * c / ((1.0 + c) * (1.0 + c) * VT);

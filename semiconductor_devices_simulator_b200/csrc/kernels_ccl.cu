@@ -134,8 +134,10 @@ __global__ void k_ff_recomb(const DevP *__restrict__ Ps, int hole, const double 
         double R, dRn, dRp;
         recomb(m, niK(P, m, k), tauf(P, m, k), hole ? oth : c, hole ? c : oth, R, dRn, dRp);
         const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
-        atomicAdd(G + b, vol * R);
-        atomicAdd(dG + b, vol * (hole ? dRp : dRn) * c);
+        double g = vol * R, dg = vol * (hole ? dRp : dRn) * c;
+        if (P.tk) { g += P.tk[k] * c - P.tg[k]; dg += P.tk[k] * c; }   // metal-contact exchange
+        atomicAdd(G + b, g);
+        atomicAdd(dG + b, dg);
     }
 }
 __global__ void k_ff_apply(const DevP *__restrict__ Ps, const double *scale) {

@@ -140,12 +140,28 @@ __global__ void k_upd_mob(const DevP *__restrict__ Ps) {
                 if (m.ani_n > 0.0) mn *= m.ani_n;
                 if (m.ani_p > 0.0) mp *= m.ani_p;
             }
+            // velocity saturation, tapered off across the barrier region of a metal contact
+            // (te_vsat_w, semiconductor_3d.c:810-824)
+            double wv = 0.0;
             if (sat) {
+                wv = 1.0;
+                if (P.te_vw) {
+                    auto node_w = [&](int kk) {
+                        const double w = P.te_vw[kk];
+                        if (w >= 1.0) return 1.0;
+                        const double c2 = P.te_ax[kk] == ax ? 1.0 : 0.0;
+                        return 1.0 - (1.0 - w) * c2;
+                    };
+                    wv = 0.5 * (node_w(k) + node_w(kp));
+                }
+            }
+            if (wv > 0.0) {
                 const double dps = P.phi[kp] - P.phi[k];
                 const double Fn = heat_field(P.phin[kp] - P.phin[k], dps, h);
                 const double Fp = heat_field(P.phip[kp] - P.phip[k], dps, h);
-                mn = mob_hf(mn, Fn, m.vsat_n, m.beta_n);
-                mp = mob_hf(mp, Fp, m.vsat_p, m.beta_p);
+                const double sn = mob_hf(mn, Fn, m.vsat_n, m.beta_n), sp = mob_hf(mp, Fp, m.vsat_p, m.beta_p);
+                mn += wv * (sn - mn);
+                mp += wv * (sp - mp);
             }
             P.fmu[ax][k] = mn; P.fmu[3 + ax][k] = mp;
         }
@@ -205,6 +221,7 @@ __global__ void k_cont_assemble(const DevP *__restrict__ Ps, int hole) {
         const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
         dg += vol * dR;
         b += vol * (dR * car[k] - R);
+        if (P.tk) { dg += P.tk[k]; b += P.tg[k]; }   // metal-contact exchange: sink tk c - tg
         const double w = 1.0 / (dg * sk);
         P.A[0][k] = 1.0;
 #pragma unroll
@@ -293,7 +310,7 @@ __global__ void k_ion_neutral(const DevP *__restrict__ Ps) {
 void launch_ion_neutral(const Ctx &c) { SS_LAUNCH(PF_BC, c.maxN, k_ion_neutral, grid_of(c), TPB, c.st, c.dP); }
 
 // Dirichlet values of every contact node at the stage voltages (semiconductor_3d.c:1806-1829)
-__global__ void k_apply_bc(const DevP *__restrict__ Ps) {
+__global__ void k_apply_bc(const DevP *__restrict__ Ps, int have_solution) {
     const DevP &P = Ps[blockIdx.y];
     SS_GRID_LOOP(k, P.N) {
         const uint32_t f = P.flags[k];
@@ -310,6 +327,11 @@ __global__ void k_apply_bc(const DevP *__restrict__ Ps) {
         if (cn.bc == 1) {
             const double pm = cn.phi_m > 0.0 ? cn.phi_m : P.Cref;
             P.phi[k] = V + P.Cref - pm;
+            if (cn.te && have_solution) {          // metal contact: the carriers are unknowns
+                P.n[k] = nK(P, m, k, P.phi[k], P.phin[k]);
+                P.p[k] = pK(P, m, k, P.phi[k], P.phip[k]);
+                continue;
+            }
         } else {
             P.phi[k] = neutral_psi(P, m, k, V);
         }
@@ -318,7 +340,9 @@ __global__ void k_apply_bc(const DevP *__restrict__ Ps) {
         P.p[k] = pK(P, m, k, P.phi[k], V);
     }
 }
-void launch_apply_bc(const Ctx &c, int) { SS_LAUNCH(PF_BC, c.maxN, k_apply_bc, grid_of(c), TPB, c.st, c.dP); }
+void launch_apply_bc(const Ctx &c, int have_solution) {
+    SS_LAUNCH(PF_BC, c.maxN, k_apply_bc, grid_of(c), TPB, c.st, c.dP, have_solution);
+}
 
 // local charge-neutral equilibrium start (semiconductor_3d.c:1831-1845)
 __global__ void k_init_eq(const DevP *__restrict__ Ps) {
@@ -381,7 +405,7 @@ __global__ void k_currents(const DevP *__restrict__ Ps) {
         double v[3] = {0.0, 0.0, 0.0};
         for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < P.ncnode; q += gridDim.x * blockDim.x) {
             const int k = P.cnode[q];
-            if (fl_con(P.flags[k]) != c + 1) continue;
+            if (fl_con(P.flags[k]) != c + 1 || P.cons[c].te) continue;   // metal contacts: te_currents
             const Node a = unidx(k, P.Nx, P.Ny);
             for (int dir = 0; dir < 6; dir++) {
                 int kb; double h, ar;
@@ -554,7 +578,7 @@ __global__ void k_node_val(const DevP *__restrict__ Ps, int which, double *out) 
             break;
         }
         case 26: v = kd == K_SEMI ? niK(P, m, k) : 0.0; break;
-        case 27: v = 0.0; break;                                 // gate tunnelling J: not built
+        case 27: v = kd == K_SEMI && P.tg ? P.tg[k] : 0.0; break;   // exchange source of the last continuity solve
         case 28: case 29: v = kd == K_SEMI ? 0.0 : nan; break;   // quantum potentials: not built
         case 30: v = kd == K_SEMI ? P.qd[k] : nan; break;        // distance to the nearest wall
         case 31: case 32: v = kd == K_SEMI ? 0.0 : nan; break;   // traps: not built

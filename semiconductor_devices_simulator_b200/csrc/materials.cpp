@@ -137,6 +137,15 @@ void material_init(Material &m, int id, double T) {
         material_init(m, 0, T);
         return;
     }
+    // Richardson constants and tunnelling masses (semiconductor_3d.c:461, 483, 494, 512, 524,
+    // 569, 585, 597, 601-614)
+    static const double te_tab[14][4] = {
+        {1.12e6, 3.2e5, 0.26, 0.39},  {1.43e6, 4.1e5, 0.12, 0.28}, {8.16e4, 7.44e5, 0.067, 0.45},
+        {9.6e4, 7.2e5, 0.08, 0.60},   {1.46e6, 9.6e5, 0.33, 0.80}, {2.64e5, 9.6e5, 0.22, 0.80},
+        {1.08e5, 6.6e5, 0.092, 0.50}, {3.0e5, 9.6e5, 0.25, 1.0},   {0., 0., 0.42, 0.33},
+        {0., 0., 0.35, 0.35},         {0., 0., 0.18, 0.20},        {0., 0., 0.50, 0.50},
+        {0., 0., 1., 1.},             {0., 0., 1., 1.}};
+    m.rich_n = te_tab[id][0]; m.rich_p = te_tab[id][1]; m.mtun_e = te_tab[id][2]; m.mtun_h = te_tab[id][3];
     if (m.insulator) {
         // insulators carry no mobility / recombination data; keep the defaults neutral
         m.mt_min = m.mt_max_n = m.mt_max_p = m.mt_Nref = m.mt_alpha = 0.;

@@ -56,6 +56,7 @@ const double kProfBytesPerNode[PF_NPROF] = {
     92.0,   // PF_REFINE: FP64 A 56 + x, r read and written 32, FP32 correction 4 (FP64 start: 96)
     96.0,   // PF_CONVERT32: A and row weights 64 read, 32 written
     112.0,  // PF_SEED: x1, x0 of 3 fields at the node (neighbours from cache), flags, doping; 3 fields written
+    64.0,   // PF_METAL: column node state, exchange slots and the per-node results
 };
 int pf_f32(int id) {
     switch (id) {
@@ -83,7 +84,7 @@ const char *kProfName[PF_NPROF] = {
     "anderson", "boundary", "vector", "labelling", "display", "smooth_black_f32", "smooth_red_f32",
     "resid_restrict_f32", "prolong_f32", "level_resid_f32", "coarse_solve_f32", "galerkin_f32", "mg_weights_f32",
     "ilu_diag_f32", "coarse_setup_f32", "krylov_spmv_dot_f32", "krylov_update_f32", "krylov_dot_f32",
-    "krylov_init_f32", "refine_f64", "convert_f32", "learned_seed"};
+    "krylov_init_f32", "refine_f64", "convert_f32", "learned_seed", "metal_contacts"};
 
 bool g_prof_on = false;
 bool g_pdl = true;

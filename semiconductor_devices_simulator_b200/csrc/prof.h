@@ -20,6 +20,7 @@ enum ProfId {
     PF_GALERKIN32, PF_WEIGHTS32, PF_ILU_DIAG32, PF_COARSE_SETUP32, PF_KRY_SPMV_DOT32, PF_KRY_UPDATE32,
     PF_KRY_DOT32, PF_KRY_INIT32, PF_REFINE, PF_CONVERT32,
     PF_SEED,                     // learned sweep predictor (features + MLP + seed write)
+    PF_METAL,                    // metal-contact exchange (per column node)
     PF_NPROF
 };
 // kernel class of the FP32 twin of an FP64 linear-algebra class

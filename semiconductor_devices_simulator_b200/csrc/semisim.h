@@ -44,13 +44,15 @@ struct MatD {
     double vsat_n, vsat_p, beta_n, beta_p, ani_n, ani_p;
     double chi, Eg;
     double ion_w[2];             // donor site weights of incomplete ionisation
+    double T, Nc, Nv;            // temperature and band densities of states (metal contacts)
+    double rich_n, rich_p, mtun_e, mtun_h;   // Richardson constants, tunnelling masses
     int insulator, pad;
 };
 
 // contact constants the kernels need
 struct ConD {
     double V, phi_m, tox, qox;   // applied voltage of the stage, work function, oxide
-    int bc, pad;
+    int bc, te;                  // boundary type; thermionic-emission metal contact (models bit 6)
 };
 
 // one multigrid level of scalar type T (7-point stencil, 2x2x2 aggregation)
@@ -85,6 +87,13 @@ struct DevP {
     const double *Nd, *Na, *Nf, *bgn, *robA;
     const double *qd;             // distance to the nearest insulator / gate wall (display)
     double *ion;                  // incomplete ionisation, ION_W per node (null: every dopant ionised)
+    // thermionic-emission metal contacts (null without them): image-force band lowering of
+    // electrons / holes (units of VT, the reference's qcn / qcp), the continuity sink and
+    // source of the metal exchange (tk c - tg), and the velocity-saturation weight near a
+    // contact with the axis of its normal
+    double *qcn, *qcp, *tk, *tg;
+    const float *te_vw;
+    const signed char *te_ax;
     const MatD *mats;
     const ConD *cons;
     const int *cnode;             // contact-node list (semiconductor nodes of carrier contacts)
@@ -122,6 +131,25 @@ struct DevP {
     LevelT<float> *levf;
     int *ccl;                     // labels for connected-component work
     int *cclaux;
+};
+
+// Thermionic-emission metal contacts (models bit 6, semiconductor_3d.c:3390-3571): the
+// entries are the semiconductor nodes of metal face contacts, each with its column of
+// nodes along the inward normal (at most TE_COL deep); `touched` lists every column node
+// once with its column entries in ascending order (CSR), so gathers add in entry order.
+constexpr double TE_COL = 60e-9;
+constexpr int TE_NE = 64;          // Simpson intervals of the tunnelling energy integral
+constexpr int TE_NNMAX = 256;      // column nodes the tunnelling integral looks at
+struct TeD {
+    int n_te, n_tc, n_touch, models;
+    const int *te_k, *te_c, *te_c0, *te_cn;
+    const double *te_A;
+    double *te_K, *te_G;           // 2 per entry: thermionic-emission coefficients (n, p)
+    const int *tc_k;
+    const double *tc_s;            // distance of a column node from the interface
+    double *tc_K, *tc_G, *tc_I;    // 2 per column node: exchange terms, image-force lowering
+    const int *tn_k, *tn_ptr, *tn_q;
+    int ce0[NC_MAX], ce1[NC_MAX];  // entry range of every contact
 };
 
 // slots of DevP::res

@@ -205,6 +205,7 @@ void gpu_free(Inst &d) {
     if (d.g.flag) cudaFree(d.g.flag);
     if (d.g.qown) cudaFree(d.g.qown);
     if (d.g.ion) cudaFree(d.g.ion);
+    if (d.g.teblock) cudaFree(d.g.teblock);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();
@@ -343,9 +344,6 @@ static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
     if (d.n_trap_entries > 0) why = "deep-level traps";
     if ((d.models & 8) && (any_ins || any_gate)) why = "quantum confinement (models bit 3)";
     if ((d.models & 32) && any_ins) why = "gate tunnelling (models bit 5)";
-    if (d.models & 64)
-        for (int c = 0; c < d.n_cons; c++)
-            if (d.cons[c].bc == 1 && d.cons[c].face <= 5) why = "thermionic-emission metal contacts (models bit 6)";
     for (int mi = 0; mi < d.n_mats; mi++) {
         const Material &m = d.mats[mi];
         if (m.insulator) continue;
@@ -402,6 +400,143 @@ static void wall_distance(const Inst &d, const std::vector<unsigned char> &kind,
     }
 }
 
+// Thermionic-emission metal contacts (semiconductor_3d.c:1376-1416, 1723-1768): one entry
+// per semiconductor node of a metal face contact with its column along the inward normal
+// (semiconductor nodes of no contact, until TE_COL deep), the velocity-saturation weight
+// of the column nodes (0 in the first half of the column, rising to 1 at its end) and,
+// per column node, its column entries in ascending order.
+struct TeHost {
+    std::vector<int> te_k, te_c, te_c0, te_cn, tc_k, tn_k, tn_ptr, tn_q;
+    std::vector<double> te_A, tc_s;
+    std::vector<float> vw;
+    std::vector<signed char> ax;
+    int ce0[NC_MAX], ce1[NC_MAX];
+};
+static void te_build(Inst &d, const std::vector<unsigned char> &kind, const std::vector<int> &con, TeHost &H) {
+    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
+    const size_t N = d.N;
+    for (int c = 0; c < NC_MAX; c++) H.ce0[c] = H.ce1[c] = 0;
+    for (int c = 0; c < d.n_cons; c++) {
+        const Contact &cn = d.cons[c];
+        H.ce0[c] = H.ce1[c] = (int)H.te_k.size();
+        if (!cn.te) continue;
+        const int dir = cn.face ^ 1;                       // inward normal of the face
+        for_con_nodes(d, cn, [&](int, int, int, size_t k, double area) {
+            if (con[k] != c + 1 || kind[k] != K_SEMI || !(area > 0.)) return;
+            H.te_k.push_back((int)k); H.te_A.push_back(area); H.te_c.push_back(c);
+            H.te_c0.push_back((int)H.tc_k.size());
+            H.tc_k.push_back((int)k); H.tc_s.push_back(0.);
+            int cnt = 1;
+            double s_ = 0.;
+            size_t cur = k;
+            for (int guard = 0; guard < 100000; guard++) {
+                const int l = int(cur / ((size_t)Nx * Ny)), rem = int(cur - (size_t)l * Nx * Ny);
+                const int j = rem / Nx, i = rem % Nx;
+                long long kn = -1;
+                double h = 0.;
+                switch (dir) {
+                case 0: if (i > 0) { kn = (long long)cur - 1; h = d.xs[i] - d.xs[i - 1]; } break;
+                case 1: if (i < Nx - 1) { kn = (long long)cur + 1; h = d.xs[i + 1] - d.xs[i]; } break;
+                case 2: if (j > 0) { kn = (long long)cur - Nx; h = d.ys[j] - d.ys[j - 1]; } break;
+                case 3: if (j < Ny - 1) { kn = (long long)cur + Nx; h = d.ys[j + 1] - d.ys[j]; } break;
+                case 4: if (l > 0) { kn = (long long)cur - (long long)Nx * Ny; h = d.zs[l] - d.zs[l - 1]; } break;
+                default: if (l < Nz - 1) { kn = (long long)cur + (long long)Nx * Ny; h = d.zs[l + 1] - d.zs[l]; } break;
+                }
+                if (kn < 0 || kind[kn] != K_SEMI || con[kn]) break;
+                s_ += h;
+                H.tc_k.push_back((int)kn); H.tc_s.push_back(s_);
+                cnt++;
+                if (s_ >= TE_COL) break;
+                cur = (size_t)kn;
+            }
+            H.te_cn.push_back(cnt);
+        });
+        H.ce1[c] = (int)H.te_k.size();
+    }
+    // velocity-saturation weight of the column nodes (semiconductor_3d.c:1750-1764)
+    H.vw.assign(N, 1.f);
+    H.ax.assign(N, 0);
+    for (size_t t = 0; t < H.te_k.size(); t++) {
+        const int a = d.cons[H.te_c[t]].face / 2;
+        for (int q = H.te_c0[t]; q < H.te_c0[t] + H.te_cn[t]; q++) {
+            const double s_ = H.tc_s[q];
+            double w;
+            if (g_knobs.te_colvs) w = s_ <= 0.5 * TE_COL ? 0. : (s_ >= TE_COL ? 1. : (s_ - 0.5 * TE_COL) / (0.5 * TE_COL));
+            else w = s_ > 0. ? 1. : 0.;
+            const int k = H.tc_k[q];
+            if ((float)w < H.vw[k]) { H.vw[k] = (float)w; H.ax[k] = (signed char)a; }
+        }
+    }
+    // column entries of every column node, ascending
+    std::vector<int> slot(N, -1);
+    std::vector<std::vector<int>> lists;
+    for (int q = 0; q < (int)H.tc_k.size(); q++) {
+        const int k = H.tc_k[q];
+        if (slot[k] < 0) { slot[k] = (int)lists.size(); lists.emplace_back(); H.tn_k.push_back(k); }
+        lists[slot[k]].push_back(q);
+    }
+    H.tn_ptr.assign(1, 0);
+    for (auto &L : lists) {
+        for (int q : L) H.tn_q.push_back(q);
+        H.tn_ptr.push_back((int)H.tn_q.size());
+    }
+}
+
+// device copy of the metal-contact data; the per-node band lowering and sink / source
+// start at zero (the reference resets them at prepare)
+static int te_upload(Inst &d, const TeHost &H, DevP &P, cudaStream_t st) {
+    if (d.g.teblock) { cudaFree(d.g.teblock); d.g.teblock = nullptr; }
+    d.g.te_on = false;
+    P.qcn = P.qcp = P.tk = P.tg = nullptr;
+    P.te_vw = nullptr;
+    P.te_ax = nullptr;
+    const size_t N = d.N, nte = H.te_k.size(), ntc = H.tc_k.size(), ntn = H.tn_k.size();
+    if (nte == 0) return 1;
+    size_t off = 0;
+    auto room = [&](size_t bytes) { const size_t o = off; off += align_up(bytes > 0 ? bytes : 1); return o; };
+    const size_t o_qcn = room(N * 8), o_qcp = room(N * 8), o_tk = room(N * 8), o_tg = room(N * 8);
+    const size_t o_vw = room(N * 4), o_ax = room(N);
+    const size_t o_tek = room(nte * 4), o_tec = room(nte * 4), o_tec0 = room(nte * 4), o_tecn = room(nte * 4);
+    const size_t o_teA = room(nte * 8), o_teK = room(nte * 16), o_teG = room(nte * 16);
+    const size_t o_tck = room(ntc * 4), o_tcs = room(ntc * 8), o_tcK = room(ntc * 16), o_tcG = room(ntc * 16),
+                 o_tcI = room(ntc * 16);
+    const size_t o_tnk = room(ntn * 4), o_tnp = room((ntn + 1) * 4), o_tnq = room(ntc * 4);
+    char *b = nullptr;
+    if (cudaMalloc(&b, off) != cudaSuccess) {
+        std::fprintf(stderr, "semisim-b200: out of device memory for the metal contacts\n");
+        return 0;
+    }
+    d.g.teblock = b;
+    CK(cudaMemsetAsync(b, 0, off, st));
+    TeD &T = d.g.te;
+    T = TeD{};
+    T.n_te = (int)nte; T.n_tc = (int)ntc; T.n_touch = (int)ntn; T.models = d.models;
+    T.te_k = (int *)(b + o_tek); T.te_c = (int *)(b + o_tec); T.te_c0 = (int *)(b + o_tec0); T.te_cn = (int *)(b + o_tecn);
+    T.te_A = (double *)(b + o_teA); T.te_K = (double *)(b + o_teK); T.te_G = (double *)(b + o_teG);
+    T.tc_k = (int *)(b + o_tck); T.tc_s = (double *)(b + o_tcs);
+    T.tc_K = (double *)(b + o_tcK); T.tc_G = (double *)(b + o_tcG); T.tc_I = (double *)(b + o_tcI);
+    T.tn_k = (int *)(b + o_tnk); T.tn_ptr = (int *)(b + o_tnp); T.tn_q = (int *)(b + o_tnq);
+    for (int c = 0; c < NC_MAX; c++) { T.ce0[c] = H.ce0[c]; T.ce1[c] = H.ce1[c]; }
+    bool ok = true;
+    auto up = [&](const void *dst, const void *src, size_t bytes) {
+        if (bytes && cudaMemcpyAsync((void *)dst, src, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) ok = false;
+    };
+    up(T.te_k, H.te_k.data(), nte * 4); up(T.te_c, H.te_c.data(), nte * 4);
+    up(T.te_c0, H.te_c0.data(), nte * 4); up(T.te_cn, H.te_cn.data(), nte * 4);
+    up(T.te_A, H.te_A.data(), nte * 8);
+    up(T.tc_k, H.tc_k.data(), ntc * 4); up(T.tc_s, H.tc_s.data(), ntc * 8);
+    up(T.tn_k, H.tn_k.data(), ntn * 4); up(T.tn_ptr, H.tn_ptr.data(), (ntn + 1) * 4);
+    up(T.tn_q, H.tn_q.data(), ntc * 4);
+    up(b + o_vw, H.vw.data(), N * 4); up(b + o_ax, H.ax.data(), N);
+    P.qcn = (double *)(b + o_qcn); P.qcp = (double *)(b + o_qcp);
+    P.tk = (double *)(b + o_tk); P.tg = (double *)(b + o_tg);
+    P.te_vw = (const float *)(b + o_vw);
+    P.te_ax = (const signed char *)(b + o_ax);
+    if (!ok) return 0;
+    d.g.te_on = true;
+    return 1;
+}
+
 int prepare(Inst &d) {
     if (!d.allocated || d.n_mats < 1) return 0;
     if (!d.dirty && d.g.ready) return 1;       // set-up unchanged since the last upload
@@ -418,6 +553,8 @@ int prepare(Inst &d) {
         d.bgn[k] = (!m.insulator && (d.models & 1)) ? bgn_half(m, d.Nd[k] + d.Na[k]) : 0.;
     }
     int nrob = 0;
+    for (int c = 0; c < d.n_cons; c++)                  // metal face contacts (semiconductor_3d.c:1655)
+        d.cons[c].te = (d.models & 64) && d.cons[c].bc == 1 && d.cons[c].face <= 5;
     for (int c = 0; c < d.n_cons; c++) {
         Contact &cn = d.cons[c];
         cn.A = 0.;
@@ -468,7 +605,9 @@ int prepare(Inst &d) {
     d.mu0n.assign(N, 0.0);
     d.mu0p.assign(N, 0.0);
     for (size_t k = 0; k < N; k++) {
-        const bool fix = con[k] != 0;          // no thermionic-emission contacts: every contact node is fixed
+        // carrier densities are fixed on contact nodes, except the semiconductor nodes of a
+        // thermionic-emission contact (car_fix, semiconductor_3d.c:796-799)
+        const bool fix = con[k] != 0 && !(d.cons[con[k] - 1].te && kind[k] == K_SEMI);
         d.flags[k] = make_flags(kind[k], con[k], gate[k], d.mat_idx[k], fix);
         if (con[k] && kind[k] == K_SEMI) d.cnode.push_back((int)k);
         if (kind[k] == K_SEMI) {
@@ -508,6 +647,8 @@ int prepare(Inst &d) {
             }
         }
     }
+    TeHost teh;
+    te_build(d, kind, con, teh);
     if (!gpu_alloc(d)) return 0;
     if (want_ion && !d.g.ion && cudaMalloc(&d.g.ion, (size_t)ION_W * N * sizeof(double)) != cudaSuccess) {
         d.g.ion = nullptr;
@@ -520,6 +661,7 @@ int prepare(Inst &d) {
     P.VTref = d.mats[d.ref_mat].VT; P.Cref = d.Cref;
     P.ncnode = (int)d.cnode.size();
     P.ion = want_ion ? d.g.ion : nullptr;
+    if (!te_upload(d, teh, P, d.g.st)) return 0;
     MatD md[NM_MAX];
     std::memset(md, 0, sizeof md);
     for (int i = 0; i < d.n_mats; i++) {
@@ -530,6 +672,8 @@ int prepare(Inst &d) {
         o.vsat_n = m.vsat_n; o.vsat_p = m.vsat_p; o.beta_n = m.beta_n; o.beta_p = m.beta_p;
         o.ani_n = m.ani_n; o.ani_p = m.ani_p; o.chi = m.chi; o.Eg = m.Eg; o.insulator = m.insulator;
         o.ion_w[0] = m.ion_on ? m.ion_w[0] : 0.; o.ion_w[1] = m.ion_on ? m.ion_w[1] : 0.;
+        o.T = m.T; o.Nc = m.Nc; o.Nv = m.Nv;
+        o.rich_n = m.rich_n; o.rich_p = m.rich_p; o.mtun_e = m.mtun_e; o.mtun_h = m.mtun_h;
     }
     cudaStream_t st = d.g.st;
     CK(cudaMemcpyAsync((void *)P.mats, md, sizeof md, cudaMemcpyHostToDevice, st));
@@ -567,7 +711,7 @@ void upload_voltages(Inst &d, const double *Va) {
     std::memset(cd, 0, sizeof cd);
     for (int c = 0; c < d.n_cons; c++) {
         cd[c].V = Va[c]; cd[c].phi_m = d.cons[c].phi_m; cd[c].tox = d.cons[c].tox;
-        cd[c].qox = d.cons[c].qox; cd[c].bc = d.cons[c].bc;
+        cd[c].qox = d.cons[c].qox; cd[c].bc = d.cons[c].bc; cd[c].te = d.cons[c].te;
     }
     cudaMemcpyAsync((void *)d.g.h.cons, cd, sizeof(ConD) * (d.n_cons > 0 ? d.n_cons : 1), cudaMemcpyHostToDevice,
                     d.g.st);
@@ -604,6 +748,7 @@ void terminal_currents(Inst &d, double *I, double *S) {
     Ctx c = make_ctx(d);
     const int nc = d.n_cons;
     launch_currents(c);
+    te_currents(d);
     cudaMemcpyAsync(d.g.pin, d.g.h.res, sizeof(double) * R_TOTAL, cudaMemcpyDeviceToHost, d.g.st);
     cudaStreamSynchronize(d.g.st);
     for (int q = 0; q < nc; q++) {
@@ -668,6 +813,7 @@ int float_fix(Inst &d, int hole);   // kernels_ccl.cu
 // floating-block balance -> update (semiconductor_3d.c:2216-2232, 3580-3594)
 static int solve_cont(Inst &d, int hole, double lo, double hi, double *dmax) {
     Ctx c = make_ctx(d);
+    te_scatter(d, hole);                                 // metal-contact sink / source of this carrier
     launch_cont_assemble(c, hole);
     launch_fill_sel(c, V_SOL, 1.0);
     const double atol = g_knobs.cont_atol * d.cont_atol_f;
@@ -717,8 +863,7 @@ static void aa_step(Inst &d) {                      // semiconductor_3d.c:3709-3
 
 // ------------------------------------------------------------------ Gummel
 // One Gummel solve at fixed terminal voltages (semiconductor_3d.c:3781-3930; the
-// impact-ionisation and metal-contact branches belong to models this library does not
-// build)
+// impact-ionisation branch belongs to a model this library does not build)
 static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters, double *res) {
     Ctx c = make_ctx(d);
     const int nc = d.n_cons;
@@ -729,8 +874,9 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
     apply_bc(d, Va);
     aa_reset(d);
     poisson_newton(d, Va, std::fmax(nt0, 1e-6), 100);
-    int it, conv = 0, it_mark = 0;
+    int it, conv = 0, it_mark = 0, stall = 0, ntight = 0, loose = 0;
     double dpsi = 1., dq = 1., best = 1e300, prev = 1., best_mark = 1e300;
+    const int n_te = d.g.te_on ? d.g.te.n_te : 0;
     for (it = 1; it <= maxit; it++) {
         if (g_stop.load()) break;
         const double t0 = wtime();
@@ -739,6 +885,7 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
         copy_dev(d, d.g.h.qp0, d.g.h.phip);
         rebuild_np(d);
         upd_mob(d);
+        te_update(d);
         const double t1 = wtime();
         d.t_mob += t1 - t0;
         double dn = 0., dp = 0.;
@@ -749,10 +896,13 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
         dq = std::fmax(dn, dp);
         terminal_currents(d, I, S);
         d.t_cur += wtime() - t2;
-        int icv = haveI;
+        int icv = haveI, icl = haveI;                     // icl: stable to 1e-4 (metal-contact noise floor)
         if (haveI)
-            for (int q = 0; q < nc; q++)
+            for (int q = 0; q < nc; q++) {
                 if (std::fabs(I[q] - Iold[q]) > std::fmax(itol * std::fabs(I[q]), 3e-14 * S[q])) icv = 0;
+                if (std::fabs(I[q] - Iold[q]) > std::fmax(std::fmax(itol, 1e-4) * std::fabs(I[q]), 3e-14 * S[q])) icl = 0;
+            }
+        loose = icl ? loose + 1 : 0;
         std::memcpy(Iold, I, sizeof(double) * nc);
         haveI = 1;
         launch_predictor(c);                               // xk = psi; neutral-region predictor
@@ -771,6 +921,30 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
             copy_dev(d, d.g.h.phi, d.g.h.xk);
             conv = 1;
             break;
+        }
+        // metal contacts: potentials converged but a terminal current keeps moving (a trace
+        // carrier left at the BiCGSTAB tolerance): tighten that tolerance (it stays tight
+        // for this device), then the residual floor, then accept at the 1e-4 noise floor
+        // (semiconductor_3d.c:3875-3904)
+        if (n_te > 0 && r <= 1e3 * gtol && !icv && haveI) {
+            if (++stall >= 3 + 3 * ntight) {
+                int did = 0;
+                if (d.bicg_rtol > 1.01e-10) { d.bicg_rtol = std::fmax(d.bicg_rtol * 1e-2, 1e-10); did = 1; }
+                else if (d.cont_atol_f > 1e-6) { d.cont_atol_f *= 1e-3; did = 1; }
+                if (did) {
+                    stall = 0; ntight++; best_mark = 1e300; it_mark = it;
+                    if (d.verbose)
+                        std::fprintf(stderr, "semisim-b200: terminal current not settling - continuity tolerance %.0e, floor %.0e\n",
+                                     d.bicg_rtol, g_knobs.cont_atol * d.cont_atol_f);
+                } else if (loose >= 8) {
+                    copy_dev(d, d.g.h.phi, d.g.h.xk);
+                    conv = 1;
+                    if (d.verbose) std::fprintf(stderr, "semisim-b200: accepted at the metal-contact noise floor (res %.2e)\n", r);
+                    break;
+                }
+            }
+        } else {
+            stall = 0;
         }
         prev = r;
         if (r < 0.5 * best_mark) { best_mark = r; it_mark = it; }

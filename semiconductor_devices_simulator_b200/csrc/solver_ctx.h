@@ -29,6 +29,7 @@ struct Contact {
     double V = 0, phi_m = 0, tox = 10e-9, qox = 0;
     double Vprev = 0, I = 0, A = 0, In = 0, Iflr = 0, Iraw = 0;
     int snl = 0;                 // gate stack layers (tunnelling, not built)
+    int te = 0;                  // thermionic-emission metal contact (set by prepare)
 };
 
 struct Gpu {
@@ -47,6 +48,9 @@ struct Gpu {
     double *scratch = nullptr;   // device scratch (bulk output)
     int *flag = nullptr;         // device int scratch
     double *ion = nullptr;       // incomplete-ionisation constants (ION_W x N), when a material needs them
+    void *teblock = nullptr;     // metal-contact entries, columns and per-node arrays (one allocation)
+    TeD te{};
+    bool te_on = false;
     int *qown = nullptr;         // charge-partition owners (N, dense terminal slots), uploaded on first use
     bool qown_ok = false;
     int qown_nt = 0;             // the terminal count they were numbered for
@@ -130,6 +134,7 @@ struct Knobs {
     double grow_slow = 2.2;
     double cont_atol = 2e-14;
     double qf_margin = 0.0;
+    int te_colvs = 1;            // metal contacts: velocity saturation tapered over the column (0: first edge only)
     int check_every = 1;        // Krylov iterations queued between status reads
 };
 extern Knobs g_knobs;
@@ -157,6 +162,10 @@ int use_mixed(const Inst &d);
 int seed_available(const Inst &d);                       // learned.cu
 void launch_mlp_seed(Inst &d, double s, const double *dv);
 extern int g_precision_default;                          // precision of new instances (1 = refined FP32)
+// thermionic-emission metal contacts (metal.cu)
+void te_update(Inst &d);
+void te_scatter(Inst &d, int hole);
+void te_currents(Inst &d);
 // per-point output reductions on the device (outputs.cu)
 double out_emax(Inst &d);
 void out_carrier_sums(Inst &d, double *out);

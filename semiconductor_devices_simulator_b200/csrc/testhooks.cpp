@@ -67,6 +67,42 @@ int b200x_masks(int *kind, int *con, int *gate, double *robA) {
     }
     return 1;
 }
+// metal contacts: the exchange update at the contacts' voltages, and the entry / column
+// records (the entry node's own column slot holds its emission terms here; the reference
+// keeps them only in te_K / te_G)
+int b200x_te_update(void) {
+    Inst &d = *dev();
+    if (!d.g.ready || !d.g.te_on) return 0;
+    double Va[NC_MAX];
+    for (int c = 0; c < d.n_cons; c++) Va[c] = d.cons[c].V;
+    upload_voltages(d, Va);
+    te_update(d);
+    sync(d);
+    return 1;
+}
+int b200x_set_qc(const double *qcn, const double *qcp) {
+    Inst &d = *dev();
+    if (!d.g.ready || !d.g.te_on) return 0;
+    cudaMemcpyAsync(d.g.h.qcn, qcn, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
+    cudaMemcpyAsync(d.g.h.qcp, qcp, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
+    sync(d);
+    return 1;
+}
+int b200x_te(int *cnt, double *teK, double *teG, double *tcK, double *tcG, double *tcI, double *qcn, double *qcp) {
+    Inst &d = *dev();
+    cnt[0] = cnt[1] = 0;
+    if (!d.g.ready || !d.g.te_on) return 0;
+    const TeD &T = d.g.te;
+    cnt[0] = T.n_te; cnt[1] = T.n_tc;
+    auto cp = [&](double *dst, const double *src, size_t n) {
+        if (dst) cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToHost, d.g.st);
+    };
+    cp(teK, T.te_K, 2 * (size_t)T.n_te); cp(teG, T.te_G, 2 * (size_t)T.n_te);
+    cp(tcK, T.tc_K, 2 * (size_t)T.n_tc); cp(tcG, T.tc_G, 2 * (size_t)T.n_tc); cp(tcI, T.tc_I, 2 * (size_t)T.n_tc);
+    cp(qcn, d.g.h.qcn, d.N); cp(qcp, d.g.h.qcp, d.N);
+    sync(d);
+    return T.n_te;
+}
 // the device's incomplete-ionisation constants (ION_W x N); 0 when every dopant is ionised
 int b200x_ion(double *out) {
     Inst &d = *dev();

@@ -87,6 +87,31 @@ def pn_diode(lib, n=(40, 40, 40), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj=0.5
                     {"NA_cm3": NA, "ND_cm3": ND, "xj_m": xj, "models": models, "L_m": L})
 
 
+def schottky_diode(lib, n=(40, 3, 3), L=1e-6, ND=1e16, phi_m=4.8, models=7 | 64, h0=2e-9,
+                   solver=GUI_SOLVER, V=None):
+    """n-Si Schottky diode: a metal face contact (bc 1, work function phi_m eV) on x = 0
+    over uniform donors ND (cm^-3), ohmic cathode on x = L, mesh graded from h0 at the
+    metal; `models` 7 | 64 switches on thermionic emission with image-force lowering, | 128
+    barrier tunnelling.  The metal (anode) is swept over V (default 0..0.4 V)."""
+    lib.api3_init()
+    xs = graded_axis(L, n[0], h0)
+    ys = np.linspace(0.0, 0.2e-6, n[1])
+    zs = np.linspace(0.0, 0.2e-6, n[2])
+    _grid(lib, xs, ys, zs)
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    si = lib.api3_add_material(SI, 300.0)
+    lib.api3_set_region(0, 0, 0, n[0] - 1, n[1] - 1, n[2] - 1, si, ND * 1e6, 0.0)
+    lib.api3_clear_contacts()
+    ca = lib.api3_add_contact_ex(0, 0, n[1] - 1, 0, n[2] - 1, 0, 0, 1, 0.0, phi_m, 0.0, 0.0)
+    cc = lib.api3_add_contact_ex(1, 0, n[1] - 1, 0, n[2] - 1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    if V is None:
+        V = np.round(np.linspace(0.0, 0.4, 9), 12)
+    return Workload("schottky", n, {"anode": ca, "cathode": cc},
+                    [{"fixed": {"cathode": 0.0}, "swept": "anode", "V": np.asarray(V, float)}],
+                    {"ND_cm3": ND, "phi_m": phi_m, "models": models})
+
+
 def graded_axis(L, n, h0):
     """n coordinates on [0, L] whose spacing grows geometrically from h0 at 0."""
     if n < 3:
