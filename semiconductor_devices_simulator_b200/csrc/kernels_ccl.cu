@@ -136,6 +136,7 @@ __global__ void k_ff_recomb(const DevP *__restrict__ Ps, int hole, const double 
         const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
         double g = vol * R, dg = vol * (hole ? dRp : dRn) * c;
         if (P.tk) { g += P.tk[k] * c - P.tg[k]; dg += P.tk[k] * c; }   // metal-contact exchange
+        if (P.gii) g -= P.gii[k];                                        // impact-ionisation pairs
         atomicAdd(G + b, g);
         atomicAdd(dG + b, dg);
     }

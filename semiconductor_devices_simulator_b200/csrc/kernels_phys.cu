@@ -120,10 +120,39 @@ void launch_rebuild_np(const Ctx &c) { SS_LAUNCH(PF_REBUILD, c.maxN, k_rebuild_n
 
 // Face mobility of the edge k -> k+e_ax from the node low-field mobilities, with
 // Caughey-Thomas saturation driven by the harmonic-mean field when models bit 2 is set
-// (semiconductor_3d.c:2962-3006; the surface-mobility branches are not built).
+// (semiconductor_3d.c:2962-3006), and Lombardi surface scattering near insulator / gate walls
+// when models bit 4 is set (the Coulomb term of 4H-SiC is not built).
+// potential gradient along ax taken inside the semiconductor (one-sided at an interface,
+// semiconductor_3d.c:2909-2917)
+__device__ __forceinline__ double grad_semi(const DevP &P, const Node &a, int k, int ax) {
+    int km = 0, kp = 0;
+    double hm = 1.0, hp = 1.0, ar;
+    const bool lo = nbr(P, a, k, 2 * ax, km, hm, ar) && fl_kind(P.flags[km]) == K_SEMI;
+    const bool hi = nbr(P, a, k, 2 * ax + 1, kp, hp, ar) && fl_kind(P.flags[kp]) == K_SEMI;
+    if (lo && hi) return (P.phi[kp] - P.phi[km]) / (hm + hp);
+    if (hi) return (P.phi[kp] - P.phi[k]) / hp;
+    if (lo) return (P.phi[k] - P.phi[km]) / hm;
+    return 0.0;
+}
+// squared field normal to axis ax (semiconductor_3d.c:2918-2921)
+__device__ __forceinline__ double fnorm2(const DevP &P, const Node &a, int k, int ax) {
+    const double g1 = grad_semi(P, a, k, (ax + 1) % 3), g2 = grad_semi(P, a, k, (ax + 2) % 3);
+    return g1 * g1 + g2 * g2;
+}
+// Lombardi: 1/mu = 1/mu_b + D (1/mu_ac + 1/mu_sr), cm units inside (semiconductor_3d.c:2924-2933)
+__device__ __forceinline__ double lombardi(const MatD &m, double mub, double Fv, double Nt, double Dw, int hole) {
+    double F = Fv * 1e-2;
+    if (F < 1.0) F = 1.0;                          // V/cm
+    double N = Nt * 1e-6;
+    if (N < 1.0) N = 1.0;                          // cm^-3
+    const double Bc = m.lbB[hole], Cc = m.lbC[hole], Lc = m.lbL[hole], Dc = m.lbD[hole], Ec = m.lbE[hole];
+    const double muac = Bc / F + Cc * pow(N, Lc) / (cbrt(F) * (m.T / 300.0));
+    const double musr = Ec > 0.0 ? 1.0 / (F * F / Dc + F * F * F / Ec) : Dc / (F * F);
+    return 1.0 / (1.0 / mub + Dw * 1e4 * (1.0 / muac + 1.0 / musr));
+}
 __global__ void k_upd_mob(const DevP *__restrict__ Ps) {
     const DevP &P = Ps[blockIdx.y];
-    const bool sat = (P.models & 4) != 0;
+    const bool sat = (P.models & 4) != 0, lb = (P.models & 16) != 0;
     SS_GRID_LOOP(k, P.N) {
         const uint32_t f = P.flags[k];
         const Node a = unidx(k, P.Nx, P.Ny);
@@ -139,6 +168,17 @@ __global__ void k_upd_mob(const DevP *__restrict__ Ps) {
             if (ax == P.caxis) {
                 if (m.ani_n > 0.0) mn *= m.ani_n;
                 if (m.ani_p > 0.0) mp *= m.ani_p;
+            }
+            if (lb && m.lb_on) {
+                const double Dw = exp(-0.5 * (P.qd[k] + P.qd[kp]) / 1e-8);
+                if (Dw > 1e-8) {
+                    Node b = a;
+                    if (ax == 0) b.i++; else if (ax == 1) b.j++; else b.l++;
+                    const double F = sqrt(0.5 * (fnorm2(P, a, k, ax) + fnorm2(P, b, kp, ax)));
+                    const double Nt = 0.5 * (P.Nd[k] + P.Na[k] + P.Nd[kp] + P.Na[kp]);
+                    if (m.lb_on & 1) mn = lombardi(m, mn, F, Nt, Dw, 0);
+                    if (m.lb_on & 2) mp = lombardi(m, mp, F, Nt, Dw, 1);
+                }
             }
             // velocity saturation, tapered off across the barrier region of a metal contact
             // (te_vsat_w, semiconductor_3d.c:810-824)
@@ -222,6 +262,7 @@ __global__ void k_cont_assemble(const DevP *__restrict__ Ps, int hole) {
         dg += vol * dR;
         b += vol * (dR * car[k] - R);
         if (P.tk) { dg += P.tk[k]; b += P.tg[k]; }   // metal-contact exchange: sink tk c - tg
+        if (P.gii) b += P.gii[k];                   // impact ionisation (pairs)
         const double w = 1.0 / (dg * sk);
         P.A[0][k] = 1.0;
 #pragma unroll
@@ -448,6 +489,61 @@ void launch_currents(const Ctx &c) {
     SS_LAUNCH(PF_CURRENTS, c.h.ncnode, k_currents, dim3(nb, c.ninst), TPB, c.st, c.dP);
 }
 
+// ------------------------------------------------------------------ impact ionisation
+// alpha(F) = g a exp(-(g b / F)^m), (a, b) below / above E0 (semiconductor_3d.c:4478-4485)
+__device__ __forceinline__ double ii_alpha(const MatD &m, double F, int c) {
+    if (!(F > 1e5)) return 0.0;                    // below 1 kV/cm: nothing
+    const int r = F >= m.ii_E0[c];
+    double x = m.ii_g * m.ii_b[c][r] / F;
+    if (m.ii_m[c] != 1.0) x = pow(x, m.ii_m[c]);
+    if (x > 700.0) return 0.0;
+    return m.ii_g * m.ii_a[c][r] * exp(-x);
+}
+// pair generation G = (alpha_n(F_n) |J_n| + alpha_p(F_p) |J_p|) / q over the control volume,
+// F the field along each carrier's node current density (semiconductor_3d.c:4486-4523), and
+// the total generation -> res[R_GII]
+__global__ void k_ii_update(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const uint32_t f = P.flags[k];
+        double gk = 0.0;
+        const MatD &m = P.mats[fl_mat(f)];
+        if (fl_kind(f) == K_SEMI && !fl_fix(f) && m.ii_on) {
+            const Node a = unidx(k, P.Nx, P.Ny);
+            double Jn[3], Jp[3], E[3];
+#pragma unroll
+            for (int ax = 0; ax < 3; ax++) {
+                double sn = 0.0, sp = 0.0, h, ar, jn, jp, s1, s2;
+                int cnt = 0, kb;
+                if (nbr(P, a, k, 2 * ax, kb, h, ar) && fl_kind(P.flags[kb]) == K_SEMI) {
+                    face_flux(P, kb, k, ax, h, ar, jn, jp, s1, s2); sn += jn / ar; sp += jp / ar; cnt++;
+                }
+                if (nbr(P, a, k, 2 * ax + 1, kb, h, ar) && fl_kind(P.flags[kb]) == K_SEMI) {
+                    face_flux(P, k, kb, ax, h, ar, jn, jp, s1, s2); sn += jn / ar; sp += jp / ar; cnt++;
+                }
+                Jn[ax] = cnt ? sn / cnt : 0.0;
+                Jp[ax] = cnt ? sp / cnt : 0.0;
+                E[ax] = -grad_semi(P, a, k, ax);
+            }
+            const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
+            double G = 0.0;
+            for (int c = 0; c < 2; c++) {
+                const double *J = c ? Jp : Jn;
+                const double jj = sqrt(J[0] * J[0] + J[1] * J[1] + J[2] * J[2]);
+                if (!(jj > 0.0)) continue;
+                const double F = fabs(E[0] * J[0] + E[1] * J[1] + E[2] * J[2]) / jj;
+                G += ii_alpha(m, F, c) * jj;
+            }
+            gk = G / Q * vol;
+        }
+        P.gii[k] = gk;
+        acc[0] += gk;
+    }
+    if (grid_sum<1>(acc, P.part, P.ticket + 9)) P.res[R_GII] = acc[0];
+}
+void launch_ii_update(const Ctx &c) { SS_LAUNCH(PF_DISPLAY, c.maxN, k_ii_update, grid_of(c), TPB, c.st, c.dP); }
+
 // ------------------------------------------------------------------ Gummel helpers
 // xk = psi; neutral-region psi predictor from the quasi-Fermi changes
 // (semiconductor_3d.c:3853-3859)
@@ -582,7 +678,12 @@ __global__ void k_node_val(const DevP *__restrict__ Ps, int which, double *out) 
         case 28: case 29: v = kd == K_SEMI ? 0.0 : nan; break;   // quantum potentials: not built
         case 30: v = kd == K_SEMI ? P.qd[k] : nan; break;        // distance to the nearest wall
         case 31: case 32: v = kd == K_SEMI ? 0.0 : nan; break;   // traps: not built
-        case 33: v = 0.0; break;                                 // impact ionisation: not built
+        case 33: {                                  // impact-ionisation generation (m^-3 s^-1)
+            if (kd != K_SEMI || !P.gii) { v = 0.0; break; }
+            const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
+            v = vol > 0.0 ? P.gii[k] / vol : 0.0;
+            break;
+        }
         case 34: v = kd == K_SEMI ? 0.0 : nan; break;            // Coulomb N_C: not built
         case 35: {                                  // ionised net doping N_D+ - N_A-
             if (kd != K_SEMI) { v = 0.0; break; }

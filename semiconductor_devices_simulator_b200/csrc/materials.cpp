@@ -36,6 +36,15 @@ void set_sat(Material &m, const Sat &s) {
     m.vsat_n = s.vsat_n; m.vsat_p = s.vsat_p; m.beta_n = s.beta_n; m.beta_p = s.beta_p;
 }
 
+// impact-ionisation coefficients: electrons (a, b) below / above E0, holes likewise
+struct Ii { double an0, bn0, an1, bn1, E0n, mn, ap0, bp0, ap1, bp1, E0p, mp, hw; };
+void set_ii(Material &m, const Ii &v) {
+    m.ii_on = 1;
+    m.ii_a[0][0] = v.an0; m.ii_b[0][0] = v.bn0; m.ii_a[0][1] = v.an1; m.ii_b[0][1] = v.bn1; m.ii_E0[0] = v.E0n; m.ii_m[0] = v.mn;
+    m.ii_a[1][0] = v.ap0; m.ii_b[1][0] = v.bp0; m.ii_a[1][1] = v.ap1; m.ii_b[1][1] = v.bp1; m.ii_E0[1] = v.E0p; m.ii_m[1] = v.mp;
+    m.ii_hw = v.hw;
+}
+
 // Semiconductor band data: Eg(T) Varshni, affinity, permittivity, Nc/Nv at 300 K with
 // power-law temperature exponents.
 struct Band { double E0, a, b, chi, eps_r, Nc300, Nc_exp, Nv300, Nv_exp; };
@@ -71,7 +80,12 @@ void material_init(Material &m, int id, double T) {
         set_recomb(m, {1e-5, 1e-5, 2.8e-43, 9.9e-44, 4.73e-21});
         m.tau_Nref = 1e22;
         m.bgn_E = 6.92e-3; m.bgn_N = 1.3e23; m.bgn_C = 0.5;
-        m.lb_on = 3; m.ii_on = 1;
+        // Lombardi as parameterised in Sentaurus (semiconductor_3d.c:462-465)
+        m.lb_on = 3;
+        m.lbB[0] = 4.75e7; m.lbC[0] = 580.; m.lbL[0] = 0.125; m.lbD[0] = 5.82e14;
+        m.lbB[1] = 9.925e6; m.lbC[1] = 2947.; m.lbL[1] = 0.0317; m.lbD[1] = 2.0546e14;
+        // van Overstraeten - de Man (semiconductor_3d.c:466-472)
+        set_ii(m, {7.03e7, 1.231e8, 7.03e7, 1.231e8, 4e7, 1., 1.582e8, 2.036e8, 6.71e7, 1.693e8, 4e7, 1., 0.063});
         break;
     }
     case 1:     // Ge
@@ -85,7 +99,7 @@ void material_init(Material &m, int id, double T) {
         set_lowfield(m, {0.94, 0.040, 0.050, 0.0020, 6.0e22, 2.75e23, 0.394, 0.394, 0., -2.1, -2.1, 3.0, 0.});
         set_sat(m, {7.7e4, 7.7e4, 1., 1.});
         set_recomb(m, {1e-9, 1e-9, 1e-43, 1e-43, 1.5e-16});
-        m.ii_on = 1;
+        set_ii(m, {2.99e7, 6.848e7, 2.99e7, 6.848e7, 1e30, 1.6, 2.215e7, 6.57e7, 2.215e7, 6.57e7, 1e30, 1.75, 0.});   // :498-500
         break;
     case 3:     // InP
         set_band(m, {1.4236, 3.63e-4, 162., 4.38, 12.5, 5.7e23, 1.5, 1.1e25, 1.5});
@@ -98,7 +112,9 @@ void material_init(Material &m, int id, double T) {
         set_lowfield(m, {0.095, 0.0124, 0.0040, 0.00159, 1.94e23, 1.76e25, 0.61, 0.34, -0.5, -2.40, -2.15, 0., 0.});
         set_sat(m, {2.2e5, 1.6e5, 1.2, 1.});
         set_recomb(m, {1e-6, 1e-7, 5e-44, 2e-44, 1.5e-18});
-        m.ii_on = 1; m.lb_on = 1; m.lbc_on = 1;
+        m.lb_on = 1; m.lbc_on = 1;                  // electrons, with Coulomb scattering (semiconductor_3d.c:545-548)
+        m.lbB[0] = 1e6; m.lbC[0] = 1.077e4; m.lbL[0] = 0.0284; m.lbD[0] = 1.7e13; m.lbE[0] = 1.7e29;
+        set_ii(m, {1.76e10, 3.30e9, 1.76e10, 3.30e9, 1e30, 1., 3.41e10, 2.50e9, 3.41e10, 2.50e9, 1e30, 1., 0.});   // :528-530
         // nitrogen on the hexagonal and cubic sites (1:1), aluminium acceptors
         // (semiconductor_3d.c:553-555)
         m.ion_on = 1; m.ion_w[0] = m.ion_w[1] = 0.5;
@@ -111,7 +127,7 @@ void material_init(Material &m, int id, double T) {
         set_lowfield(m, {0.120, 0.0030, 0.0055, 0.00030, 1.00e23, 3.00e23, 1.0, 2.0, -1.02, -3.84, -3.84, 0., 0.});
         set_sat(m, {2.5e5, 2e5, 1., 1.});
         set_recomb(m, {1e-8, 1e-8, 1e-43, 1e-43, 1.1e-16});
-        m.ii_on = 1;
+        set_ii(m, {2.11e11, 3.689e9, 2.11e11, 3.689e9, 1e30, 1., 4.39e8, 1.8e9, 4.39e8, 1.8e9, 1e30, 1., 0.});   // :572-574
         break;
     case 6:     // Al0.3Ga0.7As
         set_band(m, {1.882, 5.58e-4, 295., 3.827, 12.24, 7.2e23, 1.5, 1.05e25, 1.5});
@@ -151,6 +167,7 @@ void material_init(Material &m, int id, double T) {
         m.mt_min = m.mt_max_n = m.mt_max_p = m.mt_Nref = m.mt_alpha = 0.;
     }
     m.ni = m.insulator ? 0. : std::sqrt(m.Nc * m.Nv) * std::exp(-m.Eg / (2. * m.VT));
+    m.ii_g = m.ii_hw > 0. ? std::tanh(m.ii_hw / (2. * KB * 300. / Q)) / std::tanh(m.ii_hw / (2. * m.VT)) : 1.;
 }
 
 // Low-field mobility: Masetti (mas_on) or Arora / Caughey-Thomas (semiconductor_3d.c:646-662)

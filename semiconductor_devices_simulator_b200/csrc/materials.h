@@ -29,8 +29,19 @@ struct Material {
     // metal contacts (models bits 6, 7): Richardson constants A** (A m^-2 K^-2) and the
     // tunnelling effective masses (units of m0) of electrons and holes
     double rich_n = 0, rich_p = 0, mtun_e = 0, mtun_h = 0;
+    // impact ionisation (models bit 8), Chynoweth law per carrier c (0 n, 1 p):
+    // alpha(F) = g a exp(-(g b / F)^m) with (a, b) below / above the field E0, temperature
+    // factor g = tanh(hw / 2kT0) / tanh(hw / 2kT) from the optical-phonon energy hw
+    int ii_on = 0;
+    double ii_a[2][2] = {{0, 0}, {0, 0}}, ii_b[2][2] = {{0, 0}, {0, 0}}, ii_E0[2] = {0, 0}, ii_m[2] = {1, 1};
+    double ii_hw = 0, ii_g = 1;
+    // Lombardi surface mobility (models bit 4): lb_on bit 0 electrons, bit 1 holes;
+    // 1/mu = 1/mu_b + D (1/mu_ac + 1/mu_sr), mu_ac = B/F + C N^L / (F^(1/3) T/300),
+    // mu_sr = D/F^2 (or 1/(F^2/D + F^3/E) with the roughness term E), cm units [0] n, [1] p
+    int lb_on = 0;
+    double lbB[2] = {0, 0}, lbC[2] = {0, 0}, lbL[2] = {0, 0}, lbD[2] = {0, 0}, lbE[2] = {0, 0};
     // models outside this library's scope that the material would switch on
-    int lb_on = 0, lbc_on = 0, ii_on = 0;
+    int lbc_on = 0;
     double lnc = 0, lnv = 0;      // effective ln Nc / ln Nv in the common gauge (mat_prepare)
 };
 

@@ -46,7 +46,9 @@ struct MatD {
     double ion_w[2];             // donor site weights of incomplete ionisation
     double T, Nc, Nv;            // temperature and band densities of states (metal contacts)
     double rich_n, rich_p, mtun_e, mtun_h;   // Richardson constants, tunnelling masses
-    int insulator, pad;
+    double ii_a[2][2], ii_b[2][2], ii_E0[2], ii_m[2], ii_g;   // impact ionisation (models bit 8)
+    double lbB[2], lbC[2], lbL[2], lbD[2], lbE[2];           // Lombardi surface mobility (models bit 4)
+    int insulator, ii_on, lb_on, pad;
 };
 
 // contact constants the kernels need
@@ -92,6 +94,7 @@ struct DevP {
     // source of the metal exchange (tk c - tg), and the velocity-saturation weight near a
     // contact with the axis of its normal
     double *qcn, *qcp, *tk, *tg;
+    double *gii;                  // impact-ionisation pair generation of the node (1/s; null: models bit 8 off)
     const float *te_vw;
     const signed char *te_ax;
     const MatD *mats;
@@ -164,6 +167,7 @@ enum ResSlot {
     R_S = 40,        // scales S[NC_MAX] at 40..71 (res has 128 doubles)
     R_IN = 72,       // electron components at 72..103
     R_OUT = 104,     // per-point output reductions at 104..110
+    R_GII = 111,     // total impact-ionisation generation
     R_TOTAL = 128
 };
 

@@ -205,6 +205,7 @@ void gpu_free(Inst &d) {
     if (d.g.flag) cudaFree(d.g.flag);
     if (d.g.qown) cudaFree(d.g.qown);
     if (d.g.ion) cudaFree(d.g.ion);
+    if (d.g.gii) cudaFree(d.g.gii);
     if (d.g.teblock) cudaFree(d.g.teblock);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
@@ -347,8 +348,8 @@ static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
     for (int mi = 0; mi < d.n_mats; mi++) {
         const Material &m = d.mats[mi];
         if (m.insulator) continue;
-        if ((d.models & 16) && m.lb_on && (any_ins || any_gate) && used(mi)) why = "surface mobility (models bit 4)";
-        if ((d.models & 256) && m.ii_on && used(mi)) why = "impact ionisation (models bit 8)";
+        if ((d.models & 16) && m.lbc_on && (m.lb_on & 1) && (any_ins || any_gate) && used(mi))
+            why = "Coulomb scattering on interface charge (models bit 4, 4H-SiC)";
     }
     if (why) {
         std::fprintf(stderr, "semisim-b200: %s is not supported by this solver library\n", why);
@@ -650,6 +651,11 @@ int prepare(Inst &d) {
     TeHost teh;
     te_build(d, kind, con, teh);
     if (!gpu_alloc(d)) return 0;
+    if ((d.models & 256) && !d.g.gii && cudaMalloc(&d.g.gii, N * sizeof(double)) != cudaSuccess) {
+        d.g.gii = nullptr;
+        std::fprintf(stderr, "semisim-b200: out of device memory for the impact-ionisation generation\n");
+        return 0;
+    }
     if (want_ion && !d.g.ion && cudaMalloc(&d.g.ion, (size_t)ION_W * N * sizeof(double)) != cudaSuccess) {
         d.g.ion = nullptr;
         std::fprintf(stderr, "semisim-b200: out of device memory for the ionisation constants\n");
@@ -661,6 +667,8 @@ int prepare(Inst &d) {
     P.VTref = d.mats[d.ref_mat].VT; P.Cref = d.Cref;
     P.ncnode = (int)d.cnode.size();
     P.ion = want_ion ? d.g.ion : nullptr;
+    P.gii = (d.models & 256) ? d.g.gii : nullptr;
+    if (P.gii) CK(cudaMemsetAsync(P.gii, 0, N * sizeof(double), d.g.st));
     if (!te_upload(d, teh, P, d.g.st)) return 0;
     MatD md[NM_MAX];
     std::memset(md, 0, sizeof md);
@@ -674,6 +682,17 @@ int prepare(Inst &d) {
         o.ion_w[0] = m.ion_on ? m.ion_w[0] : 0.; o.ion_w[1] = m.ion_on ? m.ion_w[1] : 0.;
         o.T = m.T; o.Nc = m.Nc; o.Nv = m.Nv;
         o.rich_n = m.rich_n; o.rich_p = m.rich_p; o.mtun_e = m.mtun_e; o.mtun_h = m.mtun_h;
+        o.ii_on = m.ii_on;
+        for (int c = 0; c < 2; c++) {
+            o.ii_a[c][0] = m.ii_a[c][0]; o.ii_a[c][1] = m.ii_a[c][1];
+            o.ii_b[c][0] = m.ii_b[c][0]; o.ii_b[c][1] = m.ii_b[c][1];
+            o.ii_E0[c] = m.ii_E0[c]; o.ii_m[c] = m.ii_m[c];
+        }
+        o.ii_g = m.ii_g;
+        o.lb_on = m.lb_on;
+        for (int c = 0; c < 2; c++) {
+            o.lbB[c] = m.lbB[c]; o.lbC[c] = m.lbC[c]; o.lbL[c] = m.lbL[c]; o.lbD[c] = m.lbD[c]; o.lbE[c] = m.lbE[c];
+        }
     }
     cudaStream_t st = d.g.st;
     CK(cudaMemcpyAsync((void *)P.mats, md, sizeof md, cudaMemcpyHostToDevice, st));
@@ -877,6 +896,16 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
     int it, conv = 0, it_mark = 0, stall = 0, ntight = 0, loose = 0;
     double dpsi = 1., dq = 1., best = 1e300, prev = 1., best_mark = 1e300;
     const int n_te = d.g.te_on ? d.g.te.n_te : 0;
+    // impact ionisation: the multiplication converges slowly near breakdown; track the total
+    // generation Gs and accept only when its change and the extrapolated remainder of the
+    // series are below tol_ii Gs; the continuity solves run tighter meanwhile
+    // (semiconductor_3d.c:3788-3799, 3815-3831)
+    const int iion = (d.models & 256) != 0 && d.g.h.gii;
+    const double tol_ii = std::fmax(itol, 1e-4);
+    double Gs_old = -1., dG_old = 0., ii_rel = 1., ii_best = 1e300, Erem = 0.;
+    const double brtol0 = d.bicg_rtol;
+    if (iion && d.bicg_rtol > 1e-8) d.bicg_rtol = 1e-8;
+    d.ii_err = 0.;
     for (it = 1; it <= maxit; it++) {
         if (g_stop.load()) break;
         const double t0 = wtime();
@@ -886,6 +915,27 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
         rebuild_np(d);
         upd_mob(d);
         te_update(d);
+        int iiok = 1;
+        if (iion) {
+            launch_ii_update(c);
+            const double Gs = read_res(d, R_GII);
+            if (Gs > 0.) {
+                if (Gs_old < 0.) { iiok = 0; Erem = Gs; }
+                else {
+                    const double dG = std::fabs(Gs - Gs_old);
+                    double rho = dG_old > 0. ? dG / dG_old : 0.;
+                    if (rho > 0.99) rho = 0.99;
+                    Erem = dG + dG * rho / (1. - rho);
+                    iiok = dG <= tol_ii * Gs && Erem <= tol_ii * Gs;
+                    dG_old = dG;
+                }
+                ii_rel = Erem / Gs;
+                Gs_old = Gs;
+            } else {
+                Erem = 0.;
+                ii_rel = 0.;
+            }
+        }
         const double t1 = wtime();
         d.t_mob += t1 - t0;
         double dn = 0., dp = 0.;
@@ -902,6 +952,11 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
                 if (std::fabs(I[q] - Iold[q]) > std::fmax(itol * std::fabs(I[q]), 3e-14 * S[q])) icv = 0;
                 if (std::fabs(I[q] - Iold[q]) > std::fmax(std::fmax(itol, 1e-4) * std::fabs(I[q]), 3e-14 * S[q])) icl = 0;
             }
+        if (iion && !iiok) {                              // generation below the current resolution
+            double Sm = 0.;
+            for (int q = 0; q < nc; q++) if (S[q] > Sm) Sm = S[q];
+            if (Q * Erem <= 3e-14 * Sm) iiok = 1;
+        }
         loose = icl ? loose + 1 : 0;
         std::memcpy(Iold, I, sizeof(double) * nc);
         haveI = 1;
@@ -917,7 +972,7 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
         if (dpsi != dpsi || dq != dq) break;
         const double r = std::fmax(dpsi, dq);
         g_prog[1] = it; g_prog[2] = r; g_prog[5] = (double)(d.gummel_its + it);
-        if (dq < gtol && dpsi < gtol && icv) {            // accept psi_k with its carriers
+        if (dq < gtol && dpsi < gtol && icv && iiok) {    // accept psi_k with its carriers
             copy_dev(d, d.g.h.phi, d.g.h.xk);
             conv = 1;
             break;
@@ -936,7 +991,7 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
                     if (d.verbose)
                         std::fprintf(stderr, "semisim-b200: terminal current not settling - continuity tolerance %.0e, floor %.0e\n",
                                      d.bicg_rtol, g_knobs.cont_atol * d.cont_atol_f);
-                } else if (loose >= 8) {
+                } else if (loose >= 8 && iiok) {
                     copy_dev(d, d.g.h.phi, d.g.h.xk);
                     conv = 1;
                     if (d.verbose) std::fprintf(stderr, "semisim-b200: accepted at the metal-contact noise floor (res %.2e)\n", r);
@@ -948,7 +1003,8 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
         }
         prev = r;
         if (r < 0.5 * best_mark) { best_mark = r; it_mark = it; }
-        if (it - it_mark > 20 && r <= 1e3 * gtol && icv) {
+        if (iion && ii_rel < 0.5 * ii_best) { ii_best = ii_rel; it_mark = it; }   // slow multiplication is progress
+        if (it - it_mark > 20 && r <= 1e3 * gtol && icv && iiok) {
             copy_dev(d, d.g.h.phi, d.g.h.xk);
             conv = 1;
             if (d.verbose) std::fprintf(stderr, "semisim-b200: accepted at noise floor (res %.2e)\n", r);
@@ -963,6 +1019,8 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
     }
     if (it > maxit) it = maxit;
     cudaStreamSynchronize(d.g.st);
+    if (iion && brtol0 > 1e-8 && d.bicg_rtol == 1e-8) d.bicg_rtol = brtol0;   // (a metal-contact tightening stays)
+    if (iion) d.ii_err = Q * Erem;
     d.gummel_its += it;
     *iters = it;
     *res = std::fmax(dpsi, dq);
@@ -1168,7 +1226,7 @@ int run_continuation(Inst &d) {
         const double fo = F - fl[q];
         if (d.cons[q].bc != 2 && ncar > 1 && fo < fv) { Iv = -(ks - I[q]); fv = fo; }
         d.cons[q].I = Iv;
-        d.cons[q].Iflr = fv * scl;
+        d.cons[q].Iflr = fv * scl + (ok_all ? d.ii_err : 0.);   // (a failed point keeps its partial-state floor)
         d.cons[q].Iraw = I[q];
     }
     return ok_all;

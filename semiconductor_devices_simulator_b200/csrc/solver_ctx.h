@@ -48,6 +48,7 @@ struct Gpu {
     double *scratch = nullptr;   // device scratch (bulk output)
     int *flag = nullptr;         // device int scratch
     double *ion = nullptr;       // incomplete-ionisation constants (ION_W x N), when a material needs them
+    double *gii = nullptr;       // impact-ionisation generation (N), with models bit 8
     void *teblock = nullptr;     // metal-contact entries, columns and per-node arrays (one allocation)
     TeD te{};
     bool te_on = false;
@@ -93,6 +94,7 @@ struct Inst {
     double vlo = 0, vhi = 0;
     long long pcg_its = 0, bicg_its = 0, newton_its = 0, gummel_its = 0;
     double t_pois = 0, t_cont = 0, t_mob = 0, t_cur = 0, t_aa = 0, t_mg = 0;
+    double ii_err = 0;           // impact ionisation: estimated remaining change of the generated current (A)
     double pcg_rtol = 1e-3, ntol_fac = 0.1, bicg_rtol = 1e-4, cont_atol_f = 1;
     int nthreads = 1, caxis = 1, models = 7;
     int n_trap_entries = 0;
