@@ -47,6 +47,8 @@ int clone_into(Inst &w, Inst &src) {
     if (src.g.te_on && w.g.te_on) {            // the image-force band of the source's last iteration
         cudaMemcpyAsync(w.g.h.qcn, src.g.h.qcn, bytes, cudaMemcpyDeviceToDevice, w.g.st);
         cudaMemcpyAsync(w.g.h.qcp, src.g.h.qcp, bytes, cudaMemcpyDeviceToDevice, w.g.st);
+        cudaMemcpyAsync(w.g.h.imgn, src.g.h.imgn, bytes, cudaMemcpyDeviceToDevice, w.g.st);
+        cudaMemcpyAsync(w.g.h.imgp, src.g.h.imgp, bytes, cudaMemcpyDeviceToDevice, w.g.st);
     }
     double Va[NC_MAX];
     for (int c = 0; c < w.n_cons; c++) { Va[c] = src.cons[c].Vprev; w.cons[c].Vprev = Va[c]; }

@@ -675,7 +675,13 @@ __global__ void k_node_val(const DevP *__restrict__ Ps, int which, double *out) 
         }
         case 26: v = kd == K_SEMI ? niK(P, m, k) : 0.0; break;
         case 27: v = kd == K_SEMI && P.tg ? P.tg[k] : 0.0; break;   // exchange source of the last continuity solve
-        case 28: case 29: v = kd == K_SEMI ? 0.0 : nan; break;   // quantum potentials: not built
+        case 28: case 29: {                         // quantum potentials (eV): the MLDA part of qcn / qcp
+            if (kd != K_SEMI) { v = nan; break; }
+            const double qc = which == 28 ? qcn_of(P, k) : qcp_of(P, k);
+            const double *img = which == 28 ? P.imgn : P.imgp;
+            v = -(qc - (img ? img[k] : 0.0)) * m.VT;
+            break;
+        }
         case 30: v = kd == K_SEMI ? P.qd[k] : nan; break;        // distance to the nearest wall
         case 31: case 32: v = kd == K_SEMI ? 0.0 : nan; break;   // traps: not built
         case 33: {                                  // impact-ionisation generation (m^-3 s^-1)

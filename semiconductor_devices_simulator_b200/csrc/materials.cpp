@@ -80,6 +80,9 @@ void material_init(Material &m, int id, double T) {
         set_recomb(m, {1e-5, 1e-5, 2.8e-43, 9.9e-44, 4.73e-21});
         m.tau_Nref = 1e22;
         m.bgn_E = 6.92e-3; m.bgn_N = 1.3e23; m.bgn_C = 0.5;
+        // MLDA: the 2 Delta-2 valleys (m_l 0.916, 1/3) and the 4 Delta-4 valleys (0.19);
+        // heavy (0.29, 0.84) and light (0.20) holes (semiconductor_3d.c:457)
+        m.mq_e1 = 0.916; m.mq_e2 = 0.19; m.wq_e1 = 1. / 3.; m.mq_h1 = 0.29; m.mq_h2 = 0.20; m.wq_h1 = 0.84;
         // Lombardi as parameterised in Sentaurus (semiconductor_3d.c:462-465)
         m.lb_on = 3;
         m.lbB[0] = 4.75e7; m.lbC[0] = 580.; m.lbL[0] = 0.125; m.lbD[0] = 5.82e14;
@@ -162,6 +165,11 @@ void material_init(Material &m, int id, double T) {
         {0., 0., 0.35, 0.35},         {0., 0., 0.18, 0.20},        {0., 0., 0.50, 0.50},
         {0., 0., 1., 1.},             {0., 0., 1., 1.}};
     m.rich_n = te_tab[id][0]; m.rich_p = te_tab[id][1]; m.mtun_e = te_tab[id][2]; m.mtun_h = te_tab[id][3];
+    if (!m.insulator && !(m.mq_e1 > 0.) && id < 8) {    // generic single confinement masses (:619-624)
+        static const double me[8] = {0.916, 0.082, 0.067, 0.08, 0.37, 0.20, 0.09, 0.23};
+        static const double mh[8] = {0.29, 0.28, 0.50, 0.60, 1.00, 1.00, 0.55, 1.00};
+        m.mq_e1 = m.mq_e2 = me[id]; m.wq_e1 = 1.; m.mq_h1 = m.mq_h2 = mh[id]; m.wq_h1 = 1.;
+    }
     if (m.insulator) {
         // insulators carry no mobility / recombination data; keep the defaults neutral
         m.mt_min = m.mt_max_n = m.mt_max_p = m.mt_Nref = m.mt_alpha = 0.;

@@ -26,6 +26,9 @@ struct Material {
     // degeneracy ion_gd; acceptors one level ion_Ea - ion_aa N^(1/3) above Ev, degeneracy ion_ga
     int ion_on = 0;
     double ion_w[2] = {0, 0}, ion_Ed[2] = {0, 0}, ion_ad[2] = {0, 0}, ion_gd = 1, ion_Ea = 0, ion_aa = 0, ion_ga = 1;
+    // MLDA quantum confinement (models bit 3): confinement masses (units of m0) of two
+    // electron / hole populations with the weight of the first
+    double mq_e1 = 0, mq_e2 = 0, wq_e1 = 1, mq_h1 = 0, mq_h2 = 0, wq_h1 = 1;
     // metal contacts (models bits 6, 7): Richardson constants A** (A m^-2 K^-2) and the
     // tunnelling effective masses (units of m0) of electrons and holes
     double rich_n = 0, rich_p = 0, mtun_e = 0, mtun_h = 0;

@@ -64,8 +64,9 @@ __global__ void k_te_img(const DevP *__restrict__ Ps, TeD T) {
     }
 }
 
-// band lowering of every column node: the largest of its columns (te_apply_img,
-// semiconductor_3d.c:3448-3462)
+// band lowering of every column node: the largest of its columns replaces the node's
+// previous image-force part of qcn / qcp, in the reference's order of operations
+// (te_apply_img, semiconductor_3d.c:3448-3462)
 __global__ void k_te_apply(const DevP *__restrict__ Ps, TeD T) {
     const DevP &P = Ps[0];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -77,8 +78,10 @@ __global__ void k_te_apply(const DevP *__restrict__ Ps, TeD T) {
         if (T.tc_I[2 * q + 1] > mp) mp = T.tc_I[2 * q + 1];
     }
     const int k = T.tn_k[i];
-    P.qcn[k] = mn;
-    P.qcp[k] = mp;
+    P.qcn[k] = (P.qcn[k] - P.imgn[k]) + mn;
+    P.qcp[k] = (P.qcp[k] - P.imgp[k]) + mp;
+    P.imgn[k] = mn;
+    P.imgp[k] = mp;
 }
 
 __device__ __forceinline__ double softplus(double x) { return x > 35.0 ? x + log1p(exp(-x)) : log1p(exp(x)); }

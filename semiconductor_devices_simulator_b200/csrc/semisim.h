@@ -89,11 +89,12 @@ struct DevP {
     const double *Nd, *Na, *Nf, *bgn, *robA;
     const double *qd;             // distance to the nearest insulator / gate wall (display)
     double *ion;                  // incomplete ionisation, ION_W per node (null: every dopant ionised)
-    // thermionic-emission metal contacts (null without them): image-force band lowering of
-    // electrons / holes (units of VT, the reference's qcn / qcp), the continuity sink and
-    // source of the metal exchange (tk c - tg), and the velocity-saturation weight near a
-    // contact with the axis of its normal
+    // band corrections of electrons / holes in units of VT (the reference's qcn / qcp: MLDA
+    // confinement plus the image-force lowering at metal contacts; null without either);
+    // metal contacts (null without them): the continuity sink and source of the exchange
+    // (tk c - tg), and the velocity-saturation weight near a contact with the axis of its normal
     double *qcn, *qcp, *tk, *tg;
+    double *imgn, *imgp;          // the image-force part of qcn / qcp (metal contacts)
     double *gii;                  // impact-ionisation pair generation of the node (1/s; null: models bit 8 off)
     const float *te_vw;
     const signed char *te_ax;

@@ -207,6 +207,7 @@ void gpu_free(Inst &d) {
     if (d.g.ion) cudaFree(d.g.ion);
     if (d.g.gii) cudaFree(d.g.gii);
     if (d.g.teblock) cudaFree(d.g.teblock);
+    if (d.g.qc) cudaFree(d.g.qc);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();
@@ -343,7 +344,6 @@ static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
     };
     const char *why = nullptr;
     if (d.n_trap_entries > 0) why = "deep-level traps";
-    if ((d.models & 8) && (any_ins || any_gate)) why = "quantum confinement (models bit 3)";
     if ((d.models & 32) && any_ins) why = "gate tunnelling (models bit 5)";
     for (int mi = 0; mi < d.n_mats; mi++) {
         const Material &m = d.mats[mi];
@@ -365,12 +365,43 @@ static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
 // wall is the midpoint to an insulator neighbour, or the domain face of the node's gate
 // contact; a metal node or the domain edge without such a gate ends the run.  1 m where no
 // wall is in sight.
+// MLDA factor of one population averaged over a cell z in [a, b] from a hard wall:
+// 1 - exp(-(z/lambda)^2) (semiconductor_3d.c:1072-1080)
+static double mlda_pop(double a, double b, double lam) {
+    const double u = a / lam, v = b / lam;
+    if (v < 0.05) {                                       // series: no cancellation
+        const double dd = v - u;
+        if (dd < 1e-12) return u * u;
+        return ((v * v * v - u * u * u) / 3. - (std::pow(v, 5) - std::pow(u, 5)) / 10. +
+                (std::pow(v, 7) - std::pow(u, 7)) / 42.) / dd;
+    }
+    if (v - u < 1e-9 * v) return 1. - std::exp(-u * u);
+    return 1. - 0.5 * std::sqrt(3.14159265358979323846) * (std::erf(v) - std::erf(u)) / (v - u);
+}
+// two populations, lambda = hbar / sqrt(2 m kT) (semiconductor_3d.c:1081-1088)
+static double mlda_factor(const Material &m, double a, double b, int hole) {
+    const double HBAR_ = 1.054571817e-34, M0_ = 9.1093837015e-31;
+    const double kT = KB * m.T, m1 = hole ? m.mq_h1 : m.mq_e1, m2 = hole ? m.mq_h2 : m.mq_e2,
+                 w = hole ? m.wq_h1 : m.wq_e1;
+    if (!(m1 > 0.)) return 1.;
+    if (a < 0.) a = 0.;
+    if (b < a) b = a;
+    double f = w * mlda_pop(a, b, HBAR_ / std::sqrt(2. * m1 * M0_ * kT));
+    if (w < 1. && m2 > 0.) f += (1. - w) * mlda_pop(a, b, HBAR_ / std::sqrt(2. * m2 * M0_ * kT));
+    return f;
+}
+
+// With qc (models bit 3) also the MLDA band corrections qcn / qcp: the sum over the walls
+// within 40 nm of the log of the cell-averaged factor, clamped at -60
+// (semiconductor_3d.c:1090-1145).
 static void wall_distance(const Inst &d, const std::vector<unsigned char> &kind, const std::vector<int> &gate,
-                          std::vector<double> &qd) {
+                          std::vector<double> &qd, bool qc, std::vector<double> &qcn, std::vector<double> &qcp) {
     const int n3[3] = {d.Nx, d.Ny, d.Nz};
     const std::vector<double> *cs[3] = {&d.xs, &d.ys, &d.zs};
     const size_t st3[3] = {1, (size_t)d.Nx, (size_t)d.Nx * d.Ny};
     qd.assign(d.N, 1.0);
+    qcn.assign(qc ? d.N : 0, 0.0);
+    qcp.assign(qc ? d.N : 0, 0.0);
     for (int ax = 0; ax < 3; ax++) {
         const int n = n3[ax];
         const std::vector<double> &c = *cs[ax];
@@ -394,10 +425,25 @@ static void wall_distance(const Inst &d, const std::vector<unsigned char> &kind,
                         if (kb == K_INS) { w = 0.5 * (c[q] + c[qp]); have = true; }
                         else if (kb != K_SEMI) have = false;
                     }
-                    if (have) qd[k] = std::fmin(qd[k], std::fabs(c[q] - w));
+                    if (!have) continue;
+                    const double lo = q > 0 ? 0.5 * (c[q - 1] + c[q]) : c[q];
+                    const double hi = q < n - 1 ? 0.5 * (c[q] + c[q + 1]) : c[q];
+                    double za = side ? w - hi : lo - w;
+                    const double zb = side ? w - lo : hi - w, zn = std::fabs(c[q] - w);
+                    if (za < 0.) za = 0.;
+                    if (zn < qd[k]) qd[k] = zn;
+                    if (qc && za < 40e-9) {
+                        const Material &m = d.mats[d.mat_idx[k]];
+                        qcn[k] += std::log(std::fmax(mlda_factor(m, za, zb, 0), 1e-30));
+                        qcp[k] += std::log(std::fmax(mlda_factor(m, za, zb, 1), 1e-30));
+                    }
                 }
             }
         }
+    }
+    for (size_t k = 0; k < qcn.size(); k++) {            // keep the exponents sane
+        if (qcn[k] < -60.) qcn[k] = -60.;
+        if (qcp[k] < -60.) qcp[k] = -60.;
     }
 }
 
@@ -488,14 +534,14 @@ static void te_build(Inst &d, const std::vector<unsigned char> &kind, const std:
 static int te_upload(Inst &d, const TeHost &H, DevP &P, cudaStream_t st) {
     if (d.g.teblock) { cudaFree(d.g.teblock); d.g.teblock = nullptr; }
     d.g.te_on = false;
-    P.qcn = P.qcp = P.tk = P.tg = nullptr;
+    P.tk = P.tg = P.imgn = P.imgp = nullptr;
     P.te_vw = nullptr;
     P.te_ax = nullptr;
     const size_t N = d.N, nte = H.te_k.size(), ntc = H.tc_k.size(), ntn = H.tn_k.size();
     if (nte == 0) return 1;
     size_t off = 0;
     auto room = [&](size_t bytes) { const size_t o = off; off += align_up(bytes > 0 ? bytes : 1); return o; };
-    const size_t o_qcn = room(N * 8), o_qcp = room(N * 8), o_tk = room(N * 8), o_tg = room(N * 8);
+    const size_t o_imgn = room(N * 8), o_imgp = room(N * 8), o_tk = room(N * 8), o_tg = room(N * 8);
     const size_t o_vw = room(N * 4), o_ax = room(N);
     const size_t o_tek = room(nte * 4), o_tec = room(nte * 4), o_tec0 = room(nte * 4), o_tecn = room(nte * 4);
     const size_t o_teA = room(nte * 8), o_teK = room(nte * 16), o_teG = room(nte * 16);
@@ -514,6 +560,7 @@ static int te_upload(Inst &d, const TeHost &H, DevP &P, cudaStream_t st) {
     T.n_te = (int)nte; T.n_tc = (int)ntc; T.n_touch = (int)ntn; T.models = d.models;
     T.te_k = (int *)(b + o_tek); T.te_c = (int *)(b + o_tec); T.te_c0 = (int *)(b + o_tec0); T.te_cn = (int *)(b + o_tecn);
     T.te_A = (double *)(b + o_teA); T.te_K = (double *)(b + o_teK); T.te_G = (double *)(b + o_teG);
+
     T.tc_k = (int *)(b + o_tck); T.tc_s = (double *)(b + o_tcs);
     T.tc_K = (double *)(b + o_tcK); T.tc_G = (double *)(b + o_tcG); T.tc_I = (double *)(b + o_tcI);
     T.tn_k = (int *)(b + o_tnk); T.tn_ptr = (int *)(b + o_tnp); T.tn_q = (int *)(b + o_tnq);
@@ -529,8 +576,8 @@ static int te_upload(Inst &d, const TeHost &H, DevP &P, cudaStream_t st) {
     up(T.tn_k, H.tn_k.data(), ntn * 4); up(T.tn_ptr, H.tn_ptr.data(), (ntn + 1) * 4);
     up(T.tn_q, H.tn_q.data(), ntc * 4);
     up(b + o_vw, H.vw.data(), N * 4); up(b + o_ax, H.ax.data(), N);
-    P.qcn = (double *)(b + o_qcn); P.qcp = (double *)(b + o_qcp);
     P.tk = (double *)(b + o_tk); P.tg = (double *)(b + o_tg);
+    P.imgn = (double *)(b + o_imgn); P.imgp = (double *)(b + o_imgp);
     P.te_vw = (const float *)(b + o_vw);
     P.te_ax = (const signed char *)(b + o_ax);
     if (!ok) return 0;
@@ -618,8 +665,9 @@ int prepare(Inst &d) {
             d.mu0p[k] = mobility_low(m, Nt, 1);
         }
     }
-    std::vector<double> qd;
-    wall_distance(d, kind, gate, qd);
+    std::vector<double> qd, qcn0, qcp0;
+    const bool qc_on = (d.models & 8) != 0;
+    wall_distance(d, kind, gate, qd, qc_on, qcn0, qcp0);
     // incomplete ionisation (semiconductor_3d.c:1472-1510): per node the constants
     // N_c/g_D e^(-dE_s/kT) of the two donor sites and N_v/g_A e^(-dE_A/kT), the level depths
     // falling with the node's own dopant density; the neutral majority density (slot 3)
@@ -670,6 +718,23 @@ int prepare(Inst &d) {
     P.gii = (d.models & 256) ? d.g.gii : nullptr;
     if (P.gii) CK(cudaMemsetAsync(P.gii, 0, N * sizeof(double), d.g.st));
     if (!te_upload(d, teh, P, d.g.st)) return 0;
+    // band corrections: the MLDA part from the wall scan (zero without models bit 3); the
+    // metal contacts add their image-force lowering on the device
+    P.qcn = P.qcp = nullptr;
+    if (qc_on || d.g.te_on) {
+        if (!d.g.qc && cudaMalloc(&d.g.qc, 2 * N * sizeof(double)) != cudaSuccess) {
+            d.g.qc = nullptr;
+            std::fprintf(stderr, "semisim-b200: out of device memory for the band corrections\n");
+            return 0;
+        }
+        P.qcn = d.g.qc; P.qcp = d.g.qc + N;
+        if (qc_on) {
+            CK(cudaMemcpyAsync(P.qcn, qcn0.data(), N * 8, cudaMemcpyHostToDevice, d.g.st));
+            CK(cudaMemcpyAsync(P.qcp, qcp0.data(), N * 8, cudaMemcpyHostToDevice, d.g.st));
+        } else {
+            CK(cudaMemsetAsync(d.g.qc, 0, 2 * N * sizeof(double), d.g.st));
+        }
+    }
     MatD md[NM_MAX];
     std::memset(md, 0, sizeof md);
     for (int i = 0; i < d.n_mats; i++) {

@@ -49,6 +49,7 @@ struct Gpu {
     int *flag = nullptr;         // device int scratch
     double *ion = nullptr;       // incomplete-ionisation constants (ION_W x N), when a material needs them
     double *gii = nullptr;       // impact-ionisation generation (N), with models bit 8
+    double *qc = nullptr;        // band corrections qcn, qcp (2 N), with MLDA or metal contacts
     void *teblock = nullptr;     // metal-contact entries, columns and per-node arrays (one allocation)
     TeD te{};
     bool te_on = false;

@@ -85,6 +85,8 @@ int b200x_set_qc(const double *qcn, const double *qcp) {
     if (!d.g.ready || !d.g.te_on) return 0;
     cudaMemcpyAsync(d.g.h.qcn, qcn, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
     cudaMemcpyAsync(d.g.h.qcp, qcp, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
+    cudaMemcpyAsync(d.g.h.imgn, qcn, d.N * 8, cudaMemcpyHostToDevice, d.g.st);   // no MLDA part
+    cudaMemcpyAsync(d.g.h.imgp, qcp, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
     sync(d);
     return 1;
 }

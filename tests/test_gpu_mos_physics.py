@@ -1,10 +1,16 @@
-"""Lombardi surface mobility (models bit 4: acoustic-phonon and surface-roughness scattering
-near an insulator or gate wall, weighted by D = exp(-d / 10 nm)) against the reference core
-run live: the small n-MOSFET (oxide Robin face gate) swept in Vg at Vd = 0.5 V with models 7
-| 16.  Converged tightly: drain current within 1e-6 relative (or the floor), psi within
-1e-6 V, the display mobility maps (bulk_copy 10, 11) within 1e-9 of their peak; at the
-production tolerances the current within the reference's own distance to its converged
-value or 1e-4."""
+"""Nanoscale MOS physics against the reference core run live on the small n-MOSFET (oxide
+Robin face gate) swept in Vg at Vd = 0.5 V:
+
+* Lombardi surface mobility (models bit 4: acoustic-phonon and surface-roughness scattering
+  near an insulator or gate wall, weighted by D = exp(-d / 10 nm));
+* MLDA quantum confinement (models bit 3: the carrier densities in front of the wall fall
+  off as 1 - exp(-(z/lambda)^2), applied as band corrections qcn / qcp);
+* both together.
+
+Converged tightly: drain current within 1e-6 relative (or the floor), psi within 1e-6 V,
+the display mobility maps (bulk_copy 10, 11) and quantum potentials (28, 29) within 1e-9 of
+their peak; at the production tolerances the current within the reference's own distance
+to its converged value or 1e-4."""
 import ctypes
 import os
 import sys
@@ -53,31 +59,37 @@ def run(L, models, tight, monkeypatch):
     V, I, F, conv = D.run_sweep(L, w, s)
     d = w.contacts["drain"]
     return (ok0, I[:, d], F[:, d], conv, D.field(L, 0, w.shape).ravel(),
-            D.field(L, 10, w.shape).ravel(), D.field(L, 11, w.shape).ravel())
+            D.field(L, 10, w.shape).ravel(), D.field(L, 11, w.shape).ravel(),
+            D.field(L, 28, w.shape).ravel(), D.field(L, 29, w.shape).ravel())
 
 
+@pytest.mark.parametrize("models", [7 | 16, 7 | 8, 7 | 8 | 16], ids=["lombardi", "mlda", "mlda_lombardi"])
 @pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "refined"])
-def test_lombardi_mosfet_matches_reference(lib, prec, monkeypatch):
+def test_mos_physics_matches_reference(lib, prec, models, monkeypatch):
     ref = reference_lib()
     old = lib.api3b_set_precision(prec)
     try:
-        g1 = run(lib, 7 | 16, 1, monkeypatch)
-        g0 = run(lib, 7 | 16, 0, monkeypatch)
+        g1 = run(lib, models, 1, monkeypatch)
+        g0 = run(lib, models, 0, monkeypatch)
         plain = run(lib, 7, 1, monkeypatch)
     finally:
         lib.api3b_set_precision(old)
-    r1 = run(ref, 7 | 16, 1, monkeypatch)
-    r0 = run(ref, 7 | 16, 0, monkeypatch)
+    r1 = run(ref, models, 1, monkeypatch)
+    r0 = run(ref, models, 0, monkeypatch)
     for o in (g1, g0, r1, r0, plain):
         assert o[0] and o[3].all()
-    # surface scattering lowers the on-state drain current
-    assert abs(g1[1][-1]) < 0.95 * abs(plain[1][-1])
+    # surface scattering and confinement both lower the on-state drain current
+    assert abs(g1[1][-1]) < 0.97 * abs(plain[1][-1])
     tol = np.maximum(1e-6 * np.abs(r1[1]), r1[2])
     assert (np.abs(g1[1] - r1[1]) <= tol).all(), f"tight currents\n{g1[1]}\n{r1[1]}"
     assert np.abs(g1[4] - r1[4]).max() <= 1e-6
-    for q in (5, 6):
+    for q in (5, 6, 7, 8):
         a, b = g1[q], r1[q]
-        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max(), "display mobility"
+        assert np.array_equal(np.isnan(a), np.isnan(b))
+        m = ~np.isnan(b)
+        assert np.abs(a[m] - b[m]).max() <= 1e-9 * max(np.abs(b[m]).max(), 1e-300), f"display map {q}"
+    if models & 8:
+        assert np.nanmax(np.abs(g1[7])) > 1e-3                  # a quantum potential of meV and more
     own = 2.0 * np.abs(r0[1] - r1[1])
     tol0 = np.maximum(np.maximum(1e-4 * np.abs(r0[1]), r0[2]), own)
     assert (np.abs(g0[1] - r0[1]) <= tol0).all(), f"default currents\n{g0[1]}\n{r0[1]}"
