@@ -28,6 +28,12 @@ int b200x_ion(double *out);
    null arrays are skipped (semiconductor_3d.c:3390-3571) */
 int b200x_te_update(void);
 int b200x_set_qc(const double *qcn, const double *qcp);   /* install an image-force band (N each) */
+/* gate tunnelling (models bit 5): tun_update at the contacts' voltages (0 without paths), and
+   the records: cnt[0] paths, cnt[1] column nodes; injection tp_G (2 per path), escape rates
+   col_K (2 per column node), path and column node indices; null arrays are skipped
+   (semiconductor_3d.c:3326-3371) */
+int b200x_tun_update(void);
+int b200x_tun(int *cnt, double *tpG, double *colK, long long *tpk, long long *colk);
 int b200x_te(int *cnt, double *teK, double *teG, double *tcK, double *tcG, double *tcI, double *qcn, double *qcp);
 /* device state arrays: 0 psi, 1 phi_n, 2 phi_p, 3 n, 4 p, 5/6 low-field mobility n/p,
    7 sol, 8 rhs, 9 sc, 10 dsc, 16..21 face mobility (n x,y,z; p x,y,z), 22..24 sweep history

@@ -217,6 +217,21 @@ void hx_te_update(void){
     for(int c=0;c<gdev.n_cons;c++) Va[c]=gdev.cons[c].V;
     te_update(&gdev,Va);
 }
+/* gate tunnelling: tun_update at the contacts' stage voltages, and the path / column
+   records (counts in cnt[2] = n_tp, n_col; arrays may be NULL) */
+void hx_tun_update(void){
+    double Va[NC_MAX];
+    for(int c=0;c<gdev.n_cons;c++) Va[c]=gdev.cons[c].V;
+    tun_update(&gdev,Va);
+}
+int hx_tun(int *cnt, double *tpG, double *colK, long *tpk, long *colk){
+    cnt[0]=gdev.n_tp; cnt[1]=gdev.n_col;
+    if(tpG) memcpy(tpG,gdev.tp_G,2*gdev.n_tp*sizeof(double));
+    if(colK) memcpy(colK,gdev.col_K,2*gdev.n_col*sizeof(double));
+    if(tpk) for(int p=0;p<gdev.n_tp;p++) tpk[p]=(long)gdev.tp_k[p];
+    if(colk) for(int q=0;q<gdev.n_col;q++) colk[q]=(long)gdev.col_k[q];
+    return gdev.n_tp;
+}
 /* install an image-force band (qcn, qcp; N each) as te_update would have left it */
 void hx_set_qc(const double *qcn, const double *qcp){
     size_t N=NN(&gdev);

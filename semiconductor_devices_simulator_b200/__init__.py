@@ -26,6 +26,8 @@ HOOKS = {
     "b200x_ion": (_I, [_DP]),
     "b200x_te_update": (_I, []),
     "b200x_set_qc": (_I, [_DP, _DP]),
+    "b200x_tun_update": (_I, []),
+    "b200x_tun": (_I, [_IP, _DP, _DP, ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
     "b200x_te": (_I, [_IP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "b200x_set": (_I, [_I, _DP]),
     "b200x_get": (_I, [_I, _DP]),

@@ -304,7 +304,8 @@ int api3_set_gate_stack(int cid, int nl, const int *mat, const double *t) {
     Inst &d = g_dev;
     if (cid < 0 || cid >= d.n_cons || nl < 0 || nl > 6) return 0;
     for (int i = 0; i < nl; i++) if (mat[i] < 0 || mat[i] >= d.n_mats || !(t[i] > 0.)) return 0;
-    d.cons[cid].snl = nl;             // the stack only matters to gate tunnelling (not built)
+    d.cons[cid].snl = nl;             // Robin-gate layer stack of gate tunnelling (semiconductor_3d.c:4776-4787)
+    for (int i = 0; i < nl; i++) { d.cons[cid].smat[i] = mat[i]; d.cons[cid].st[i] = t[i]; }
     mark_changed(d);
     return 1;
 }
@@ -340,17 +341,50 @@ int api3_set_con_nodes(int cid, int n, const int *nodes, const double *areas) {
     return 1;
 }
 void api3_set_walls(const double *) {}                     // graph meshes only
-int api3_get_ntp(int) { return 0; }                          // gate tunnelling is not built
-double api3_tun_eval(int, int, const int *, const double *, double, double, double, double, double, double *out) {
-    if (out) for (int i = 0; i < 4; i++) out[i] = nanv();
-    return nanv();
+int api3_get_ntp(int cid) {                                  // semiconductor_3d.c:4844-4847
+    Inst &d = g_dev;
+    if (cid < 0) {
+        int n = 0;
+        for (int c = 0; c < d.n_cons; c++) n += d.cons[c].ntp;
+        return n;
+    }
+    return cid < d.n_cons ? d.cons[cid].ntp : 0;
 }
-double api3_mlda_factor(int, double, double, int) { return nanv(); }
-double api3_coulomb_inv(int, double, double, double, double) { return nanv(); }
-int api3_set_surface_mobility(int mi, double, double, double) {
-    return (mi >= 0 && mi < g_dev.n_mats) ? 1 : 0;
+double api3_tun_eval(int smat, int nl, const int *mat, const double *t, double psi, double phin, double phip,
+                     double Vg, double pm, double *out) {      // semiconductor_3d.c:4855-4868
+    Inst &d = g_dev;
+    if (smat < 0 || smat >= d.n_mats || nl < 1 || nl > 6) return 0.;
+    for (int i = 0; i < nl; i++) if (mat[i] < 0 || mat[i] >= d.n_mats) return 0.;
+    mat_prepare(d);
+    MatD md[NM_MAX];
+    for (int i = 0; i < d.n_mats; i++) mat_to_dev(d.mats[i], md[i]);
+    return tun_eval_host(md, smat, nl, mat, t, psi, phin, phip, Vg, pm, d.Cref, out);
 }
-double api3_lombardi(int, double, double, double, double, int) { return nanv(); }
+double api3_mlda_factor(int mi, double a, double b, int hole) {   // semiconductor_3d.c:4869-4872
+    if (mi < 0 || mi >= g_dev.n_mats) return 1.;
+    return mlda_factor_host(g_dev.mats[mi], a, b, hole);
+}
+double api3_coulomb_inv(int mi, double F, double n, double NC, double NA) {   // semiconductor_3d.c:4878-4881
+    if (mi < 0 || mi >= g_dev.n_mats || !g_dev.mats[mi].lbc_on) return nanv();
+    return coulomb_inv(g_dev.mats[mi], F, n, NC, NA);
+}
+int api3_set_surface_mobility(int mi, double delta, double eta, double mu1) {   // semiconductor_3d.c:4885-4893
+    Inst &d = g_dev;
+    if (mi < 0 || mi >= d.n_mats) return 0;
+    Material &m = d.mats[mi];
+    if (delta > 0.) m.lbD[0] = delta;
+    if (eta > 0.) m.lbE[0] = eta;
+    if (mu1 > 0.) m.lbc_mu1 = mu1;
+    mark_changed(d);
+    d.have_solution = 0;
+    return 1;
+}
+double api3_lombardi(int mi, double mub, double F, double Nt, double Dw, int hole) {   // semiconductor_3d.c:4894-4897
+    if (mi < 0 || mi >= g_dev.n_mats) return mub;
+    MatD md;
+    mat_to_dev(g_dev.mats[mi], md);
+    return lombardi_host(md, mub, F, Nt, Dw, hole);
+}
 void api3_set_contact_V(int cid, double V) { if (cid >= 0 && cid < g_dev.n_cons) g_dev.cons[cid].V = V; }
 int api3_get_ncon(void) { return g_dev.n_cons; }
 double api3_get_contact_I(int cid) { return (cid >= 0 && cid < g_dev.n_cons) ? g_dev.cons[cid].I : 0.; }

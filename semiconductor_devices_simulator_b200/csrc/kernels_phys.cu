@@ -7,6 +7,7 @@
 #include <cstdio>
 
 #include "device_common.cuh"
+#include "physics_hd.cuh"
 #include "prof.h"
 #include "kernels.h"
 
@@ -139,17 +140,7 @@ __device__ __forceinline__ double fnorm2(const DevP &P, const Node &a, int k, in
     const double g1 = grad_semi(P, a, k, (ax + 1) % 3), g2 = grad_semi(P, a, k, (ax + 2) % 3);
     return g1 * g1 + g2 * g2;
 }
-// Lombardi: 1/mu = 1/mu_b + D (1/mu_ac + 1/mu_sr), cm units inside (semiconductor_3d.c:2924-2933)
-__device__ __forceinline__ double lombardi(const MatD &m, double mub, double Fv, double Nt, double Dw, int hole) {
-    double F = Fv * 1e-2;
-    if (F < 1.0) F = 1.0;                          // V/cm
-    double N = Nt * 1e-6;
-    if (N < 1.0) N = 1.0;                          // cm^-3
-    const double Bc = m.lbB[hole], Cc = m.lbC[hole], Lc = m.lbL[hole], Dc = m.lbD[hole], Ec = m.lbE[hole];
-    const double muac = Bc / F + Cc * pow(N, Lc) / (cbrt(F) * (m.T / 300.0));
-    const double musr = Ec > 0.0 ? 1.0 / (F * F / Dc + F * F * F / Ec) : Dc / (F * F);
-    return 1.0 / (1.0 / mub + Dw * 1e4 * (1.0 / muac + 1.0 / musr));
-}
+
 __global__ void k_upd_mob(const DevP *__restrict__ Ps) {
     const DevP &P = Ps[blockIdx.y];
     const bool sat = (P.models & 4) != 0, lb = (P.models & 16) != 0;
@@ -674,7 +665,7 @@ __global__ void k_node_val(const DevP *__restrict__ Ps, int which, double *out) 
             break;
         }
         case 26: v = kd == K_SEMI ? niK(P, m, k) : 0.0; break;
-        case 27: v = kd == K_SEMI && P.tg ? P.tg[k] : 0.0; break;   // exchange source of the last continuity solve
+        case 27: v = kd == K_SEMI && P.tg ? P.tg[k] : 0.0; break;   // gate tunnelling J (none: 0 after a solve)
         case 28: case 29: {                         // quantum potentials (eV): the MLDA part of qcn / qcp
             if (kd != K_SEMI) { v = nan; break; }
             const double qc = which == 28 ? qcn_of(P, k) : qcp_of(P, k);

@@ -83,6 +83,7 @@ void material_init(Material &m, int id, double T) {
         // MLDA: the 2 Delta-2 valleys (m_l 0.916, 1/3) and the 4 Delta-4 valleys (0.19);
         // heavy (0.29, 0.84) and light (0.20) holes (semiconductor_3d.c:457)
         m.mq_e1 = 0.916; m.mq_e2 = 0.19; m.wq_e1 = 1. / 3.; m.mq_h1 = 0.29; m.mq_h2 = 0.20; m.wq_h1 = 0.84;
+        m.ms_e = 0.50; m.ms_h = 0.50;
         // Lombardi as parameterised in Sentaurus (semiconductor_3d.c:462-465)
         m.lb_on = 3;
         m.lbB[0] = 4.75e7; m.lbC[0] = 580.; m.lbL[0] = 0.125; m.lbD[0] = 5.82e14;
@@ -116,6 +117,7 @@ void material_init(Material &m, int id, double T) {
         set_sat(m, {2.2e5, 1.6e5, 1.2, 1.});
         set_recomb(m, {1e-6, 1e-7, 5e-44, 2e-44, 1.5e-18});
         m.lb_on = 1; m.lbc_on = 1;                  // electrons, with Coulomb scattering (semiconductor_3d.c:545-548)
+        m.lbc_mu1 = 40.; m.lbc_nu = 1.5; m.lbc_N0 = 1e11; m.lbc_e1 = 1.; m.lbc_e2 = 0.5; m.lbc_E0 = 2e5; m.lbc_gam = 2.;
         m.lbB[0] = 1e6; m.lbC[0] = 1.077e4; m.lbL[0] = 0.0284; m.lbD[0] = 1.7e13; m.lbE[0] = 1.7e29;
         set_ii(m, {1.76e10, 3.30e9, 1.76e10, 3.30e9, 1e30, 1., 3.41e10, 2.50e9, 3.41e10, 2.50e9, 1e30, 1., 0.});   // :528-530
         // nitrogen on the hexagonal and cubic sites (1:1), aluminium acceptors
@@ -169,6 +171,7 @@ void material_init(Material &m, int id, double T) {
         static const double me[8] = {0.916, 0.082, 0.067, 0.08, 0.37, 0.20, 0.09, 0.23};
         static const double mh[8] = {0.29, 0.28, 0.50, 0.60, 1.00, 1.00, 0.55, 1.00};
         m.mq_e1 = m.mq_e2 = me[id]; m.wq_e1 = 1.; m.mq_h1 = m.mq_h2 = mh[id]; m.wq_h1 = 1.;
+        m.ms_e = me[id] < 0.5 ? me[id] : 0.5; m.ms_h = 0.5;
     }
     if (m.insulator) {
         // insulators carry no mobility / recombination data; keep the defaults neutral
@@ -196,6 +199,27 @@ double mobility_low(const Material &m, double Ntot, int hole) {
     const double alpha = (hole ? m.alpha_p : m.alpha_n) * std::pow(tr, m.mt_alpha);
     if (mumax < mumin) mumax = mumin;
     return mumin + (mumax - mumin) / (1. + std::pow(Ntot / Nref, alpha));
+}
+
+// n_trans (cm^-3) of the Coulomb term against the acceptor doping (cm^-3): log-log
+// interpolation of four points, clamped (semiconductor_3d.c:2937-2944)
+static double ntrans_sic(double NA) {
+    static const double a[4] = {1e15, 1e16, 5e16, 5e17}, t[4] = {2.8e16, 8e16, 2.5e17, 1.55e18};
+    if (!(NA > a[0])) return t[0];
+    if (NA >= a[3]) return t[3];
+    int q = 0;
+    while (NA > a[q + 1]) q++;
+    return t[q] * std::pow(t[q + 1] / t[q], std::log(NA / a[q]) / std::log(a[q + 1] / a[q]));
+}
+// 1/mu_C (cm^2/Vs)^-1 of electrons at density n (m^-3) in a normal field Fv (V/m) near an
+// interface holding NC charges per m^2, acceptor doping NA (m^-3) (semiconductor_3d.c:2948-2955)
+double coulomb_inv(const Material &m, double Fv, double n, double NC, double NA) {
+    const double F = Fv * 1e-2, r = NC * 1e-4 / m.lbc_N0;
+    if (!(r > 0.) || !(F > 0.)) return 0.;
+    const double f = 1. - std::exp(-std::pow(F / m.lbc_E0, m.lbc_gam));
+    if (!(f > 0.)) return 0.;
+    const double s = std::pow(n * 1e-6 / (ntrans_sic(NA * 1e-6) * std::pow(r, m.lbc_e1)), m.lbc_nu);
+    return std::pow(r, m.lbc_e2) * f / (m.lbc_mu1 * (m.T / 300.) * (1. + s));
 }
 
 // Half the band-gap narrowing in units of VT, Klaassen form (semiconductor_3d.c:839-843)

@@ -29,6 +29,8 @@ struct Material {
     // MLDA quantum confinement (models bit 3): confinement masses (units of m0) of two
     // electron / hole populations with the weight of the first
     double mq_e1 = 0, mq_e2 = 0, wq_e1 = 1, mq_h1 = 0, mq_h2 = 0, wq_h1 = 1;
+    // gate tunnelling (models bit 5): supply (density-of-states) masses of the carriers
+    double ms_e = 0, ms_h = 0;
     // metal contacts (models bits 6, 7): Richardson constants A** (A m^-2 K^-2) and the
     // tunnelling effective masses (units of m0) of electrons and holes
     double rich_n = 0, rich_p = 0, mtun_e = 0, mtun_h = 0;
@@ -43,13 +45,16 @@ struct Material {
     // mu_sr = D/F^2 (or 1/(F^2/D + F^3/E) with the roughness term E), cm units [0] n, [1] p
     int lb_on = 0;
     double lbB[2] = {0, 0}, lbC[2] = {0, 0}, lbL[2] = {0, 0}, lbD[2] = {0, 0}, lbE[2] = {0, 0};
-    // models outside this library's scope that the material would switch on
+    // Coulomb scattering of electrons on interface charge (4H-SiC; the solver does not build
+    // it, api3_coulomb_inv evaluates it): mu1 (cm^2/Vs), nu, N0 (cm^-2), e1, e2, E0 (V/cm), gamma
     int lbc_on = 0;
+    double lbc_mu1 = 0, lbc_nu = 0, lbc_N0 = 1, lbc_e1 = 0, lbc_e2 = 0, lbc_E0 = 1, lbc_gam = 1;
     double lnc = 0, lnv = 0;      // effective ln Nc / ln Nv in the common gauge (mat_prepare)
 };
 
 void material_init(Material &m, int id, double T);
 double mobility_low(const Material &m, double Ntot, int hole);
 double bgn_half(const Material &m, double N);
+double coulomb_inv(const Material &m, double Fv, double n, double NC, double NA);
 
 }  // namespace ss

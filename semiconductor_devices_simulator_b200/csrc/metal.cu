@@ -11,16 +11,16 @@
 // One thread per contact entry computes the image-force lowering of its column, its
 // emission coefficients and its tunnelling terms (the entry owns its column's slots, so
 // nothing races); gathers over the column nodes (CSR, ascending entry order) give the
-// per-node band lowering and continuity sink / source in the reference's summation order.
+// per-node band lowering, and the exchange gather of tunnel.cu the continuity sink / source,
+// in the reference's summation order.
 #include "device_common.cuh"
+#include "physics_hd.cuh"
 #include "prof.h"
 #include "solver_ctx.h"
 
 namespace ss {
 
 constexpr double PI_D = 3.14159265358979323846;
-constexpr double HBAR = 1.054571817e-34;
-constexpr double M0 = 9.1093837015e-31;
 
 // image-force lowering along the column of entry t (te_img, semiconductor_3d.c:3422-3445):
 // the interface field F sets dphi = sqrt(qF / 4 pi eps) (at most 1 V) and the barrier
@@ -82,19 +82,6 @@ __global__ void k_te_apply(const DevP *__restrict__ Ps, TeD T) {
     P.qcp[k] = (P.qcp[k] - P.imgp[k]) + mp;
     P.imgn[k] = mn;
     P.imgp[k] = mp;
-}
-
-__device__ __forceinline__ double softplus(double x) { return x > 35.0 ? x + log1p(exp(-x)) : log1p(exp(x)); }
-// 2 int kappa dx over a layer of length L whose barrier above the carrier energy runs
-// linearly from u0 to u1 (eV), kappa = sqrt(2 m q u) / hbar (semiconductor_3d.c:3261-3268)
-__device__ __forceinline__ double wkb_seg(double mt, double L, double u0, double u1) {
-    const double a = u0 > 0.0 ? u0 : 0.0, b = u1 > 0.0 ? u1 : 0.0;
-    if (a == 0.0 && b == 0.0) return 0.0;
-    const double c = 2.0 * sqrt(2.0 * mt * M0 * Q) / HBAR, du = u1 - u0;
-    double I;
-    if (fabs(du) < 1e-9 * (a + b)) I = L * sqrt(0.5 * (a + b));
-    else I = L * (2.0 / 3.0) * (b * sqrt(b) - a * sqrt(a)) / du;
-    return c * I;
 }
 
 // exchange with the metal at entry t (te_one, semiconductor_3d.c:3467-3533): emission
@@ -172,23 +159,6 @@ __global__ void __launch_bounds__(64) k_te_one(const DevP *__restrict__ Ps, TeD 
     }
 }
 
-// continuity sink / source of carrier `hole` at every column node (te_scatter,
-// semiconductor_3d.c:3544-3553): the sum of its column slots in entry order
-__global__ void k_te_scatter(const DevP *__restrict__ Ps, TeD T, int hole) {
-    const DevP &P = Ps[0];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= T.n_touch) return;
-    double K = 0.0, G = 0.0;
-    for (int e = T.tn_ptr[i]; e < T.tn_ptr[i + 1]; e++) {
-        const int q = T.tn_q[e];
-        K += T.tc_K[2 * q + hole];
-        G += T.tc_G[2 * q + hole];
-    }
-    const int k = T.tn_k[i];
-    P.tk[k] = K;
-    P.tg[k] = G;
-}
-
 // terminal current of the metal contacts (te_currents, semiconductor_3d.c:3555-3571), added
 // to the face-flux currents of the other contacts: one block, each contact's entries summed
 // by the block in a fixed order
@@ -243,13 +213,6 @@ void te_update(Inst &d) {
     SS_LAUNCH(PF_METAL, T.n_tc, k_te_img, blocks(T.n_te, 128), 128, c.st, c.dP, T);
     SS_LAUNCH(PF_METAL, T.n_tc, k_te_apply, blocks(T.n_touch, 128), 128, c.st, c.dP, T);
     SS_LAUNCH(PF_METAL, T.n_tc, k_te_one, blocks(T.n_te, 64), 64, c.st, c.dP, T);
-}
-// before each continuity assembly
-void te_scatter(Inst &d, int hole) {
-    if (!d.g.te_on) return;
-    Ctx c = make_ctx(d);
-    const TeD &T = d.g.te;
-    SS_LAUNCH(PF_METAL, T.n_tc, k_te_scatter, blocks(T.n_touch, 128), 128, c.st, c.dP, T, hole);
 }
 // after the face-flux terminal currents
 void te_currents(Inst &d) {

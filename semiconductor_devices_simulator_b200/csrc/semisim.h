@@ -46,6 +46,7 @@ struct MatD {
     double ion_w[2];             // donor site weights of incomplete ionisation
     double T, Nc, Nv;            // temperature and band densities of states (metal contacts)
     double rich_n, rich_p, mtun_e, mtun_h;   // Richardson constants, tunnelling masses
+    double ms_e, ms_h;                       // supply masses of gate tunnelling
     double ii_a[2][2], ii_b[2][2], ii_E0[2], ii_m[2], ii_g;   // impact ionisation (models bit 8)
     double lbB[2], lbC[2], lbL[2], lbD[2], lbE[2];           // Lombardi surface mobility (models bit 4)
     int insulator, ii_on, lb_on, pad;
@@ -154,6 +155,27 @@ struct TeD {
     double *tc_K, *tc_G, *tc_I;    // 2 per column node: exchange terms, image-force lowering
     const int *tn_k, *tn_ptr, *tn_q;
     int ce0[NC_MAX], ce1[NC_MAX];  // entry range of every contact
+};
+
+// Gate tunnelling (models bit 5, semiconductor_3d.c:3146-3388): one path per semiconductor
+// node facing an insulator that ends on a gate metal within 30 nm (plus one per Robin-gate
+// node with a layer stack), its layers (material, thickness; at most 6) and its supply
+// column of semiconductor nodes inward from the interface (5 nm deep).
+struct TunD {
+    int n_tp, n_col;
+    const int *tp_k, *tp_c, *tp_nl, *tp_m, *tp_c0, *tp_cn;   // tp_m: 6 per path
+    const double *tp_t, *tp_A;                               // tp_t: 6 per path
+    double *tp_G;                  // 2 per path: injection from the gate (electrons, holes; 1/s)
+    const int *col_k;
+    const double *col_l, *col_h;   // cell length along the path axis, spacing to the next node
+    double *col_K;                 // 2 per column node: escape rate per unit density
+};
+// gather of the continuity sink / source per node, in the reference's order: gate
+// tunnelling column terms, gate injection, then the metal-contact terms
+struct ScD {
+    int n;
+    const int *k, *pk, *pg, *pe;   // nodes; CSR pointers into qk (tunnel column entries),
+    const int *qk, *qg, *qe;       // qg (paths of the node) and qe (metal-contact column entries)
 };
 
 // slots of DevP::res

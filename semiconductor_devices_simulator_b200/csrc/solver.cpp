@@ -10,6 +10,7 @@
 #include <cstring>
 
 #include "solver_ctx.h"
+#include "physics_hd.cuh"
 
 namespace ss {
 
@@ -208,6 +209,8 @@ void gpu_free(Inst &d) {
     if (d.g.gii) cudaFree(d.g.gii);
     if (d.g.teblock) cudaFree(d.g.teblock);
     if (d.g.qc) cudaFree(d.g.qc);
+    if (d.g.xchg) cudaFree(d.g.xchg);
+    if (d.g.tunblock) cudaFree(d.g.tunblock);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();
@@ -319,7 +322,7 @@ static void for_con_nodes(const Inst &d, const Contact &cn, F body) {
 }
 
 // Material band offsets in the common gauge (mat_prepare, semiconductor_3d.c:631-642)
-static void mat_prepare(Inst &d) {
+void mat_prepare(Inst &d) {
     d.ref_mat = 0;
     for (int i = 0; i < d.n_mats; i++)
         if (!d.mats[i].insulator) { d.ref_mat = i; break; }
@@ -330,6 +333,30 @@ static void mat_prepare(Inst &d) {
         if (m.insulator) { m.lnc = m.lnv = -1e300; continue; }
         m.lnc = std::log(m.Nc) + (m.chi - d.Cref) / m.VT;
         m.lnv = std::log(m.Nv) + (d.Cref - m.chi - m.Eg) / m.VT;
+    }
+}
+
+// device record of a material (the constants the kernels and the tunnelling arithmetic read)
+void mat_to_dev(const Material &m, MatD &o) {
+    std::memset(&o, 0, sizeof o);
+    o.VT = m.VT; o.lnc = m.lnc; o.lnv = m.lnv; o.ni = m.ni; o.eps = m.eps_r * EPS0;
+    o.tau_n0 = m.tau_n0; o.tau_p0 = m.tau_p0; o.Cn = m.Cn; o.Cp = m.Cp; o.Brad = m.Brad; o.tau_Nref = m.tau_Nref;
+    o.vsat_n = m.vsat_n; o.vsat_p = m.vsat_p; o.beta_n = m.beta_n; o.beta_p = m.beta_p;
+    o.ani_n = m.ani_n; o.ani_p = m.ani_p; o.chi = m.chi; o.Eg = m.Eg; o.insulator = m.insulator;
+    o.ion_w[0] = m.ion_on ? m.ion_w[0] : 0.; o.ion_w[1] = m.ion_on ? m.ion_w[1] : 0.;
+    o.T = m.T; o.Nc = m.Nc; o.Nv = m.Nv;
+    o.rich_n = m.rich_n; o.rich_p = m.rich_p; o.mtun_e = m.mtun_e; o.mtun_h = m.mtun_h;
+    o.ms_e = m.ms_e; o.ms_h = m.ms_h;
+    o.ii_on = m.ii_on;
+    for (int c = 0; c < 2; c++) {
+        o.ii_a[c][0] = m.ii_a[c][0]; o.ii_a[c][1] = m.ii_a[c][1];
+        o.ii_b[c][0] = m.ii_b[c][0]; o.ii_b[c][1] = m.ii_b[c][1];
+        o.ii_E0[c] = m.ii_E0[c]; o.ii_m[c] = m.ii_m[c];
+    }
+    o.ii_g = m.ii_g;
+    o.lb_on = m.lb_on;
+    for (int c = 0; c < 2; c++) {
+        o.lbB[c] = m.lbB[c]; o.lbC[c] = m.lbC[c]; o.lbL[c] = m.lbL[c]; o.lbD[c] = m.lbD[c]; o.lbE[c] = m.lbE[c];
     }
 }
 
@@ -344,7 +371,6 @@ static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
     };
     const char *why = nullptr;
     if (d.n_trap_entries > 0) why = "deep-level traps";
-    if ((d.models & 32) && any_ins) why = "gate tunnelling (models bit 5)";
     for (int mi = 0; mi < d.n_mats; mi++) {
         const Material &m = d.mats[mi];
         if (m.insulator) continue;
@@ -379,7 +405,7 @@ static double mlda_pop(double a, double b, double lam) {
     return 1. - 0.5 * std::sqrt(3.14159265358979323846) * (std::erf(v) - std::erf(u)) / (v - u);
 }
 // two populations, lambda = hbar / sqrt(2 m kT) (semiconductor_3d.c:1081-1088)
-static double mlda_factor(const Material &m, double a, double b, int hole) {
+double mlda_factor_host(const Material &m, double a, double b, int hole) {
     const double HBAR_ = 1.054571817e-34, M0_ = 9.1093837015e-31;
     const double kT = KB * m.T, m1 = hole ? m.mq_h1 : m.mq_e1, m2 = hole ? m.mq_h2 : m.mq_e2,
                  w = hole ? m.wq_h1 : m.wq_e1;
@@ -434,8 +460,8 @@ static void wall_distance(const Inst &d, const std::vector<unsigned char> &kind,
                     if (zn < qd[k]) qd[k] = zn;
                     if (qc && za < 40e-9) {
                         const Material &m = d.mats[d.mat_idx[k]];
-                        qcn[k] += std::log(std::fmax(mlda_factor(m, za, zb, 0), 1e-30));
-                        qcp[k] += std::log(std::fmax(mlda_factor(m, za, zb, 1), 1e-30));
+                        qcn[k] += std::log(std::fmax(mlda_factor_host(m, za, zb, 0), 1e-30));
+                        qcp[k] += std::log(std::fmax(mlda_factor_host(m, za, zb, 1), 1e-30));
                     }
                 }
             }
@@ -529,6 +555,176 @@ static void te_build(Inst &d, const std::vector<unsigned char> &kind, const std:
     }
 }
 
+// Gate-tunnelling paths (tun_build, semiconductor_3d.c:1146-1247): from every semiconductor
+// node of no contact with an insulator neighbour of no contact, straight through the
+// insulator; the path counts if it ends on the metal of a Dirichlet gate within TUN_LMAX.
+// Layers: the semiconductor half cell, then one per run of equal insulator material, the
+// last ending on the metal node.  A Robin gate adds one path per gate node with the
+// contact's stack.  Each path has its supply column inward from the interface.
+struct TunHost {
+    std::vector<int> tp_k, tp_c, tp_nl, tp_m, tp_c0, tp_cn, col_k;
+    std::vector<double> tp_t, tp_A, col_l, col_h;
+};
+static void tun_build(Inst &d, const std::vector<unsigned char> &kind, const std::vector<int> &con,
+                      const std::vector<int> &rob_k, const std::vector<double> &rob_A, const std::vector<int> &rob_c,
+                      TunHost &H) {
+    for (int c = 0; c < d.n_cons; c++) d.cons[c].ntp = 0;
+    if (!(d.models & 32)) return;
+    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
+    auto nb = [&](size_t k, int dir, size_t &kn, double &h, double &ar) {
+        const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny), j = rem / Nx, i = rem % Nx;
+        switch (dir) {
+        case 0: if (i == 0) return false; kn = k - 1; h = d.xs[i] - d.xs[i - 1]; ar = d.Ly[j] * d.Lz[l]; return true;
+        case 1: if (i == Nx - 1) return false; kn = k + 1; h = d.xs[i + 1] - d.xs[i]; ar = d.Ly[j] * d.Lz[l]; return true;
+        case 2: if (j == 0) return false; kn = k - Nx; h = d.ys[j] - d.ys[j - 1]; ar = d.Lx[i] * d.Lz[l]; return true;
+        case 3: if (j == Ny - 1) return false; kn = k + Nx; h = d.ys[j + 1] - d.ys[j]; ar = d.Lx[i] * d.Lz[l]; return true;
+        case 4: if (l == 0) return false; kn = k - (size_t)Nx * Ny; h = d.zs[l] - d.zs[l - 1]; ar = d.Lx[i] * d.Ly[j]; return true;
+        default: if (l == Nz - 1) return false; kn = k + (size_t)Nx * Ny; h = d.zs[l + 1] - d.zs[l]; ar = d.Lx[i] * d.Ly[j]; return true;
+        }
+    };
+    auto push = [&](size_t k, double A, int c, int dir, int nl, const int *m, const double *t) {
+        H.tp_k.push_back((int)k); H.tp_A.push_back(A); H.tp_c.push_back(c); H.tp_nl.push_back(nl);
+        for (int i = 0; i < 6; i++) { H.tp_m.push_back(i < nl ? m[i] : 0); H.tp_t.push_back(i < nl ? t[i] : 0.); }
+        H.tp_c0.push_back((int)H.col_k.size());
+        int cnt = 0;
+        if (dir >= 0) {                                    // supply column, inward (direction dir^1)
+            size_t cur = k;
+            double depth = 0.;
+            const int in = dir ^ 1, ax = dir / 2;
+            for (;;) {
+                const int l = int(cur / ((size_t)Nx * Ny)), rem = int(cur - (size_t)l * Nx * Ny);
+                const double L = ax == 0 ? d.Lx[rem % Nx] : (ax == 1 ? d.Ly[rem / Nx] : d.Lz[l]);
+                size_t kn = 0;
+                double h = 0., ar;
+                bool more = nb(cur, in, kn, h, ar);
+                if (!more || kind[kn] != K_SEMI || con[kn]) more = false;
+                H.col_k.push_back((int)cur); H.col_l.push_back(L); H.col_h.push_back(more ? h : 0.);
+                cnt++;
+                depth += L;
+                if (!more || depth >= TUN_COL) break;
+                cur = kn;
+            }
+        }
+        H.tp_cn.push_back(cnt);
+        d.cons[c].ntp++;
+    };
+    for (int l = 0; l < Nz; l++)
+        for (int j = 0; j < Ny; j++)
+            for (int i = 0; i < Nx; i++) {
+                const size_t k = (size_t)l * Nx * Ny + (size_t)j * Nx + i;
+                if (kind[k] != K_SEMI || con[k]) continue;
+                for (int dir = 0; dir < 6; dir++) {
+                    size_t kb;
+                    double h, ar;
+                    if (!nb(k, dir, kb, h, ar) || kind[kb] != K_INS || con[kb]) continue;
+                    int m[6];
+                    double t[6];
+                    int nl = 1, ok = 0;
+                    m[0] = d.mat_idx[k]; t[0] = 0.5 * h;     // semiconductor half cell
+                    double tins = 0., hin = h;
+                    size_t cur = kb;
+                    for (int guard = 0; guard < 100000; guard++) {
+                        size_t kn;
+                        double h2, ar2;
+                        if (!nb(cur, dir, kn, h2, ar2)) break;   // domain edge
+                        const int mi = d.mat_idx[cur];
+                        const bool end = kind[kn] == K_METAL && con[kn] && d.cons[con[kn] - 1].bc == 2;
+                        const double seg = 0.5 * hin + (end ? h2 : 0.5 * h2);
+                        if (nl > 1 && m[nl - 1] == mi) t[nl - 1] += seg;
+                        else {
+                            if (nl >= 6) break;
+                            m[nl] = mi; t[nl] = seg; nl++;
+                        }
+                        tins += seg;
+                        if (tins > TUN_LMAX) break;
+                        if (end) { ok = con[kn]; break; }
+                        if (kind[kn] != K_INS || con[kn]) break;
+                        cur = kn; hin = h2;
+                    }
+                    if (ok) push(k, ar, ok - 1, dir, nl, m, t);
+                }
+            }
+    for (size_t r = 0; r < rob_k.size(); r++) {
+        const Contact &cn = d.cons[rob_c[r]];
+        if (cn.snl < 1) continue;
+        push((size_t)rob_k[r], rob_A[r], rob_c[r], cn.face, cn.snl, cn.smat, cn.st);
+    }
+}
+
+// the per-node gather of the continuity sink / source: tunnelling column entries, paths
+// ending at the node, metal-contact column entries, each list in ascending order
+struct ScHost {
+    std::vector<int> k, pk, pg, pe, qk, qg, qe;
+};
+static void sc_build(size_t N, const TunHost &U, const std::vector<int> &tc_k, ScHost &H) {
+    std::vector<int> slot(N, -1);
+    std::vector<std::vector<int>> lk, lg, le;
+    auto at = [&](int k) {
+        if (slot[k] < 0) { slot[k] = (int)H.k.size(); H.k.push_back(k); lk.emplace_back(); lg.emplace_back(); le.emplace_back(); }
+        return slot[k];
+    };
+    for (int q = 0; q < (int)U.col_k.size(); q++) lk[at(U.col_k[q])].push_back(q);
+    for (int p = 0; p < (int)U.tp_k.size(); p++) lg[at(U.tp_k[p])].push_back(p);
+    for (int q = 0; q < (int)tc_k.size(); q++) le[at(tc_k[q])].push_back(q);
+    H.pk.assign(1, 0); H.pg.assign(1, 0); H.pe.assign(1, 0);
+    for (size_t i = 0; i < H.k.size(); i++) {
+        for (int q : lk[i]) H.qk.push_back(q);
+        for (int p : lg[i]) H.qg.push_back(p);
+        for (int q : le[i]) H.qe.push_back(q);
+        H.pk.push_back((int)H.qk.size()); H.pg.push_back((int)H.qg.size()); H.pe.push_back((int)H.qe.size());
+    }
+}
+
+// device copy of the tunnelling paths and the exchange gather (one allocation)
+static int tun_upload(Inst &d, const TunHost &U, const ScHost &G, cudaStream_t st) {
+    if (d.g.tunblock) { cudaFree(d.g.tunblock); d.g.tunblock = nullptr; }
+    d.g.tun_on = false;
+    d.g.tun = TunD{};
+    d.g.sc = ScD{};
+    const size_t np = U.tp_k.size(), nc = U.col_k.size(), ns = G.k.size();
+    if (ns == 0) return 1;
+    size_t off = 0;
+    auto room = [&](size_t bytes) { const size_t o = off; off += align_up(bytes > 0 ? bytes : 1); return o; };
+    const size_t o_tpk = room(np * 4), o_tpc = room(np * 4), o_tpnl = room(np * 4), o_tpm = room(np * 24),
+                 o_tpc0 = room(np * 4), o_tpcn = room(np * 4), o_tpt = room(np * 48), o_tpA = room(np * 8),
+                 o_tpG = room(np * 16), o_colk = room(nc * 4), o_coll = room(nc * 8), o_colh = room(nc * 8),
+                 o_colK = room(nc * 16);
+    const size_t o_sk = room(ns * 4), o_spk = room((ns + 1) * 4), o_spg = room((ns + 1) * 4), o_spe = room((ns + 1) * 4),
+                 o_sqk = room(G.qk.size() * 4), o_sqg = room(G.qg.size() * 4), o_sqe = room(G.qe.size() * 4);
+    char *b = nullptr;
+    if (cudaMalloc(&b, off) != cudaSuccess) {
+        std::fprintf(stderr, "semisim-b200: out of device memory for the gate-tunnelling paths\n");
+        return 0;
+    }
+    d.g.tunblock = b;
+    bool ok = cudaMemsetAsync(b, 0, off, st) == cudaSuccess;
+    auto up = [&](size_t o, const void *src, size_t bytes) {
+        if (bytes && cudaMemcpyAsync(b + o, src, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) ok = false;
+    };
+    up(o_tpk, U.tp_k.data(), np * 4); up(o_tpc, U.tp_c.data(), np * 4); up(o_tpnl, U.tp_nl.data(), np * 4);
+    up(o_tpm, U.tp_m.data(), np * 24); up(o_tpc0, U.tp_c0.data(), np * 4); up(o_tpcn, U.tp_cn.data(), np * 4);
+    up(o_tpt, U.tp_t.data(), np * 48); up(o_tpA, U.tp_A.data(), np * 8);
+    up(o_colk, U.col_k.data(), nc * 4); up(o_coll, U.col_l.data(), nc * 8); up(o_colh, U.col_h.data(), nc * 8);
+    up(o_sk, G.k.data(), ns * 4); up(o_spk, G.pk.data(), (ns + 1) * 4); up(o_spg, G.pg.data(), (ns + 1) * 4);
+    up(o_spe, G.pe.data(), (ns + 1) * 4); up(o_sqk, G.qk.data(), G.qk.size() * 4);
+    up(o_sqg, G.qg.data(), G.qg.size() * 4); up(o_sqe, G.qe.data(), G.qe.size() * 4);
+    TunD &T = d.g.tun;
+    T.n_tp = (int)np; T.n_col = (int)nc;
+    T.tp_k = (const int *)(b + o_tpk); T.tp_c = (const int *)(b + o_tpc); T.tp_nl = (const int *)(b + o_tpnl);
+    T.tp_m = (const int *)(b + o_tpm); T.tp_c0 = (const int *)(b + o_tpc0); T.tp_cn = (const int *)(b + o_tpcn);
+    T.tp_t = (const double *)(b + o_tpt); T.tp_A = (const double *)(b + o_tpA); T.tp_G = (double *)(b + o_tpG);
+    T.col_k = (const int *)(b + o_colk); T.col_l = (const double *)(b + o_coll); T.col_h = (const double *)(b + o_colh);
+    T.col_K = (double *)(b + o_colK);
+    ScD &S = d.g.sc;
+    S.n = (int)ns;
+    S.k = (const int *)(b + o_sk); S.pk = (const int *)(b + o_spk); S.pg = (const int *)(b + o_spg);
+    S.pe = (const int *)(b + o_spe); S.qk = (const int *)(b + o_sqk); S.qg = (const int *)(b + o_sqg);
+    S.qe = (const int *)(b + o_sqe);
+    if (!ok) return 0;
+    d.g.tun_on = np > 0;
+    return 1;
+}
+
 // device copy of the metal-contact data; the per-node band lowering and sink / source
 // start at zero (the reference resets them at prepare)
 static int te_upload(Inst &d, const TeHost &H, DevP &P, cudaStream_t st) {
@@ -541,7 +737,7 @@ static int te_upload(Inst &d, const TeHost &H, DevP &P, cudaStream_t st) {
     if (nte == 0) return 1;
     size_t off = 0;
     auto room = [&](size_t bytes) { const size_t o = off; off += align_up(bytes > 0 ? bytes : 1); return o; };
-    const size_t o_imgn = room(N * 8), o_imgp = room(N * 8), o_tk = room(N * 8), o_tg = room(N * 8);
+    const size_t o_imgn = room(N * 8), o_imgp = room(N * 8);
     const size_t o_vw = room(N * 4), o_ax = room(N);
     const size_t o_tek = room(nte * 4), o_tec = room(nte * 4), o_tec0 = room(nte * 4), o_tecn = room(nte * 4);
     const size_t o_teA = room(nte * 8), o_teK = room(nte * 16), o_teG = room(nte * 16);
@@ -576,7 +772,6 @@ static int te_upload(Inst &d, const TeHost &H, DevP &P, cudaStream_t st) {
     up(T.tn_k, H.tn_k.data(), ntn * 4); up(T.tn_ptr, H.tn_ptr.data(), (ntn + 1) * 4);
     up(T.tn_q, H.tn_q.data(), ntc * 4);
     up(b + o_vw, H.vw.data(), N * 4); up(b + o_ax, H.ax.data(), N);
-    P.tk = (double *)(b + o_tk); P.tg = (double *)(b + o_tg);
     P.imgn = (double *)(b + o_imgn); P.imgp = (double *)(b + o_imgp);
     P.te_vw = (const float *)(b + o_vw);
     P.te_ax = (const signed char *)(b + o_ax);
@@ -619,12 +814,15 @@ int prepare(Inst &d) {
     }
     d.robA.assign(N, 0.0);
     d.n_rob = 0;
+    std::vector<int> rob_k, rob_c;                      // the Robin list in the reference's order
+    std::vector<double> rob_A;
     for (int c = 0; c < d.n_cons; c++) {
         const Contact &cn = d.cons[c];
         if (cn.bc != 2 || cn.face > 5) continue;
         for_con_nodes(d, cn, [&](int, int, int, size_t k, double area) {
             if (gate[k] == c + 1 && !con[k] && d.n_rob < nrob && d.robA[k] == 0.0) {
                 d.robA[k] = area; d.n_rob++;
+                rob_k.push_back((int)k); rob_A.push_back(area); rob_c.push_back(c);
             }
         });
     }
@@ -698,6 +896,10 @@ int prepare(Inst &d) {
     }
     TeHost teh;
     te_build(d, kind, con, teh);
+    TunHost tuh;
+    tun_build(d, kind, con, rob_k, rob_A, rob_c, tuh);
+    ScHost sch;
+    sc_build(N, tuh, teh.tc_k, sch);
     if (!gpu_alloc(d)) return 0;
     if ((d.models & 256) && !d.g.gii && cudaMalloc(&d.g.gii, N * sizeof(double)) != cudaSuccess) {
         d.g.gii = nullptr;
@@ -718,6 +920,18 @@ int prepare(Inst &d) {
     P.gii = (d.models & 256) ? d.g.gii : nullptr;
     if (P.gii) CK(cudaMemsetAsync(P.gii, 0, N * sizeof(double), d.g.st));
     if (!te_upload(d, teh, P, d.g.st)) return 0;
+    if (!tun_upload(d, tuh, sch, d.g.st)) return 0;
+    // continuity sink / source of the exchange with gate and metal contacts (zero elsewhere)
+    P.tk = P.tg = nullptr;
+    if (d.g.te_on || d.g.tun_on) {
+        if (!d.g.xchg && cudaMalloc(&d.g.xchg, 2 * N * sizeof(double)) != cudaSuccess) {
+            d.g.xchg = nullptr;
+            std::fprintf(stderr, "semisim-b200: out of device memory for the exchange terms\n");
+            return 0;
+        }
+        CK(cudaMemsetAsync(d.g.xchg, 0, 2 * N * sizeof(double), d.g.st));
+        P.tk = d.g.xchg; P.tg = d.g.xchg + N;
+    }
     // band corrections: the MLDA part from the wall scan (zero without models bit 3); the
     // metal contacts add their image-force lowering on the device
     P.qcn = P.qcp = nullptr;
@@ -737,28 +951,7 @@ int prepare(Inst &d) {
     }
     MatD md[NM_MAX];
     std::memset(md, 0, sizeof md);
-    for (int i = 0; i < d.n_mats; i++) {
-        const Material &m = d.mats[i];
-        MatD &o = md[i];
-        o.VT = m.VT; o.lnc = m.lnc; o.lnv = m.lnv; o.ni = m.ni; o.eps = m.eps_r * EPS0;
-        o.tau_n0 = m.tau_n0; o.tau_p0 = m.tau_p0; o.Cn = m.Cn; o.Cp = m.Cp; o.Brad = m.Brad; o.tau_Nref = m.tau_Nref;
-        o.vsat_n = m.vsat_n; o.vsat_p = m.vsat_p; o.beta_n = m.beta_n; o.beta_p = m.beta_p;
-        o.ani_n = m.ani_n; o.ani_p = m.ani_p; o.chi = m.chi; o.Eg = m.Eg; o.insulator = m.insulator;
-        o.ion_w[0] = m.ion_on ? m.ion_w[0] : 0.; o.ion_w[1] = m.ion_on ? m.ion_w[1] : 0.;
-        o.T = m.T; o.Nc = m.Nc; o.Nv = m.Nv;
-        o.rich_n = m.rich_n; o.rich_p = m.rich_p; o.mtun_e = m.mtun_e; o.mtun_h = m.mtun_h;
-        o.ii_on = m.ii_on;
-        for (int c = 0; c < 2; c++) {
-            o.ii_a[c][0] = m.ii_a[c][0]; o.ii_a[c][1] = m.ii_a[c][1];
-            o.ii_b[c][0] = m.ii_b[c][0]; o.ii_b[c][1] = m.ii_b[c][1];
-            o.ii_E0[c] = m.ii_E0[c]; o.ii_m[c] = m.ii_m[c];
-        }
-        o.ii_g = m.ii_g;
-        o.lb_on = m.lb_on;
-        for (int c = 0; c < 2; c++) {
-            o.lbB[c] = m.lbB[c]; o.lbC[c] = m.lbC[c]; o.lbL[c] = m.lbL[c]; o.lbD[c] = m.lbD[c]; o.lbE[c] = m.lbE[c];
-        }
-    }
+    for (int i = 0; i < d.n_mats; i++) mat_to_dev(d.mats[i], md[i]);
     cudaStream_t st = d.g.st;
     CK(cudaMemcpyAsync((void *)P.mats, md, sizeof md, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync((void *)P.flags, d.flags.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
@@ -807,7 +1000,7 @@ void set_vrange(Inst &d, const double *Va) {   // semiconductor_3d.c:3660-3668
     int any = 0;
     double lo = 0., hi = 0.;
     for (int c = 0; c < d.n_cons; c++) {
-        if (d.cons[c].bc == 2) continue;       // a gate without tunnelling is no carrier terminal
+        if (d.cons[c].bc == 2 && !d.cons[c].ntp) continue;   // a tunnelling gate is a carrier terminal
         if (!any) { lo = hi = Va[c]; any = 1; }
         else { if (Va[c] < lo) lo = Va[c]; if (Va[c] > hi) hi = Va[c]; }
     }
@@ -832,6 +1025,7 @@ void terminal_currents(Inst &d, double *I, double *S) {
     Ctx c = make_ctx(d);
     const int nc = d.n_cons;
     launch_currents(c);
+    tun_currents(d);
     te_currents(d);
     cudaMemcpyAsync(d.g.pin, d.g.h.res, sizeof(double) * R_TOTAL, cudaMemcpyDeviceToHost, d.g.st);
     cudaStreamSynchronize(d.g.st);
@@ -897,7 +1091,7 @@ int float_fix(Inst &d, int hole);   // kernels_ccl.cu
 // floating-block balance -> update (semiconductor_3d.c:2216-2232, 3580-3594)
 static int solve_cont(Inst &d, int hole, double lo, double hi, double *dmax) {
     Ctx c = make_ctx(d);
-    te_scatter(d, hole);                                 // metal-contact sink / source of this carrier
+    exchange_scatter(d, hole);                           // gate / metal-contact sink and source of this carrier
     launch_cont_assemble(c, hole);
     launch_fill_sel(c, V_SOL, 1.0);
     const double atol = g_knobs.cont_atol * d.cont_atol_f;
@@ -979,6 +1173,7 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
         copy_dev(d, d.g.h.qp0, d.g.h.phip);
         rebuild_np(d);
         upd_mob(d);
+        tun_update(d);
         te_update(d);
         int iiok = 1;
         if (iion) {
@@ -1301,6 +1496,13 @@ void finish_point(Inst &d) {
     Ctx c = make_ctx(d);
     launch_upd_J(c);
     launch_mob_display(c);
+    // the display update leaves the sink / source arrays holding the gate-tunnelling current
+    // density at the interface nodes (A/m^2), as upd_J does (semiconductor_3d.c:3648-3657)
+    if (d.g.h.tk) {
+        cudaMemsetAsync(d.g.h.tk, 0, d.N * sizeof(double), d.g.st);
+        cudaMemsetAsync(d.g.h.tg, 0, d.N * sizeof(double), d.g.st);
+        tun_display(d);
+    }
     cudaStreamSynchronize(d.g.st);
     for (auto &v : d.cache_ok) v = 0;
 }

@@ -28,7 +28,8 @@ struct Contact {
     int face = 0, i0 = 0, i1 = 0, j0 = 0, j1 = 0, k0 = 0, k1 = 0, bc = 0;
     double V = 0, phi_m = 0, tox = 10e-9, qox = 0;
     double Vprev = 0, I = 0, A = 0, In = 0, Iflr = 0, Iraw = 0;
-    int snl = 0;                 // gate stack layers (tunnelling, not built)
+    int snl = 0, smat[6] = {0}, ntp = 0;   // Robin-gate layer stack for tunnelling; paths of the contact
+    double st[6] = {0};
     int te = 0;                  // thermionic-emission metal contact (set by prepare)
 };
 
@@ -50,7 +51,12 @@ struct Gpu {
     double *ion = nullptr;       // incomplete-ionisation constants (ION_W x N), when a material needs them
     double *gii = nullptr;       // impact-ionisation generation (N), with models bit 8
     double *qc = nullptr;        // band corrections qcn, qcp (2 N), with MLDA or metal contacts
+    double *xchg = nullptr;      // continuity sink / source tk, tg (2 N), with gate tunnelling or metal contacts
     void *teblock = nullptr;     // metal-contact entries, columns and per-node arrays (one allocation)
+    void *tunblock = nullptr;    // gate-tunnelling paths and columns, and the exchange gather
+    TunD tun{};
+    ScD sc{};
+    bool tun_on = false;
     TeD te{};
     bool te_on = false;
     int *qown = nullptr;         // charge-partition owners (N, dense terminal slots), uploaded on first use
@@ -165,10 +171,19 @@ int use_mixed(const Inst &d);
 int seed_available(const Inst &d);                       // learned.cu
 void launch_mlp_seed(Inst &d, double s, const double *dv);
 extern int g_precision_default;                          // precision of new instances (1 = refined FP32)
-// thermionic-emission metal contacts (metal.cu)
+// thermionic-emission metal contacts (metal.cu) and gate tunnelling (tunnel.cu)
 void te_update(Inst &d);
-void te_scatter(Inst &d, int hole);
 void te_currents(Inst &d);
+void tun_update(Inst &d);
+void tun_currents(Inst &d);
+void tun_display(Inst &d);
+void exchange_scatter(Inst &d, int hole);   // continuity sink / source of both
+void mat_to_dev(const Material &m, MatD &o);
+void mat_prepare(Inst &d);                 // gauge Cref and the effective band densities
+double tun_eval_host(const MatD *mats, int smat, int nl, const int *mat, const double *t, double psi, double phin,
+                     double phip, double Vg, double pm, double Cref, double *out);
+double lombardi_host(const MatD &m, double mub, double F, double Nt, double Dw, int hole);
+double mlda_factor_host(const Material &m, double a, double b, int hole);
 // per-point output reductions on the device (outputs.cu)
 double out_emax(Inst &d);
 void out_carrier_sums(Inst &d, double *out);

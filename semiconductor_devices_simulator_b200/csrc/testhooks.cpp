@@ -80,6 +80,33 @@ int b200x_te_update(void) {
     sync(d);
     return 1;
 }
+// gate tunnelling: the path update at the contacts' voltages, and the path / column records
+int b200x_tun_update(void) {
+    Inst &d = *dev();
+    if (!d.g.ready || !d.g.tun_on) return 0;
+    double Va[NC_MAX];
+    for (int c = 0; c < d.n_cons; c++) Va[c] = d.cons[c].V;
+    upload_voltages(d, Va);
+    tun_update(d);
+    sync(d);
+    return 1;
+}
+int b200x_tun(int *cnt, double *tpG, double *colK, long long *tpk, long long *colk) {
+    Inst &d = *dev();
+    cnt[0] = cnt[1] = 0;
+    if (!d.g.ready || !d.g.tun_on) return 0;
+    const TunD &T = d.g.tun;
+    cnt[0] = T.n_tp; cnt[1] = T.n_col;
+    if (tpG) cudaMemcpyAsync(tpG, T.tp_G, 2 * (size_t)T.n_tp * 8, cudaMemcpyDeviceToHost, d.g.st);
+    if (colK) cudaMemcpyAsync(colK, T.col_K, 2 * (size_t)T.n_col * 8, cudaMemcpyDeviceToHost, d.g.st);
+    std::vector<int> a((size_t)T.n_tp), b((size_t)T.n_col);
+    cudaMemcpyAsync(a.data(), T.tp_k, a.size() * 4, cudaMemcpyDeviceToHost, d.g.st);
+    cudaMemcpyAsync(b.data(), T.col_k, b.size() * 4, cudaMemcpyDeviceToHost, d.g.st);
+    sync(d);
+    if (tpk) for (size_t p = 0; p < a.size(); p++) tpk[p] = a[p];
+    if (colk) for (size_t q = 0; q < b.size(); q++) colk[q] = b[q];
+    return T.n_tp;
+}
 int b200x_set_qc(const double *qcn, const double *qcp) {
     Inst &d = *dev();
     if (!d.g.ready || !d.g.te_on) return 0;
