@@ -156,15 +156,23 @@ int api3_trap_species(int type, int ref, double E, double sn, double sp) {
     t.type = type < 0 ? -1 : (type > 0 ? 1 : 0); t.ref = ref < 0 || ref > 2 ? 2 : ref; t.E = E; t.sn = sn; t.sp = sp;
     return g_n_trap_species++;
 }
-int api3_trap_add(int sid, int n, const int *nodes, const double *dens) {
+int api3_trap_add(int sid, int n, const int *nodes, const double *dens) {   // semiconductor_3d.c:4629-4644
     Inst &d = g_dev;
     if (sid < 0 || sid >= g_n_trap_species || n <= 0) return 0;
-    for (int q = 0; q < n; q++)
-        if (dens[q] > 0. && nodes[q] >= 0) d.n_trap_entries++;
+    for (int q = 0; q < n; q++) {
+        if (!(dens[q] > 0.)) continue;
+        d.trq_k.push_back(nodes[q]); d.trq_s.push_back(sid); d.trq_N.push_back(dens[q]);
+    }
     mark_changed(d);
     return 1;
 }
-void api3_traps_clear(void) { g_dev.n_trap_entries = 0; g_n_trap_species = 0; mark_changed(g_dev); }
+void api3_traps_clear(void) {                                  // semiconductor_3d.c:4645
+    Inst &d = g_dev;
+    d.trq_k.clear(); d.trq_s.clear(); d.trq_N.clear();
+    d.n_tr = 0;
+    g_n_trap_species = 0;
+    mark_changed(d);
+}
 int api3_charge_add(int n, const int *nodes, const double *rho) {
     Inst &d = g_dev;
     if (!d.allocated) return 0;
@@ -175,7 +183,7 @@ int api3_charge_add(int n, const int *nodes, const double *rho) {
     mark_changed(d);
     return 1;
 }
-int api3_n_trap_entries(void) { return 0; }
+int api3_n_trap_entries(void) { return g_dev.n_tr; }
 void api3_set_models(int flags) { g_dev.models = flags; g_dev.have_solution = 0; g_dev.dirty = 1; }
 void api3_set_caxis(int ax) { g_dev.caxis = (ax >= 0 && ax <= 2) ? ax : -1; g_dev.have_solution = 0; g_dev.dirty = 1; }
 int api3_get_caxis(void) { return g_dev.caxis; }
@@ -366,7 +374,9 @@ double api3_mlda_factor(int mi, double a, double b, int hole) {   // semiconduct
 }
 double api3_coulomb_inv(int mi, double F, double n, double NC, double NA) {   // semiconductor_3d.c:4878-4881
     if (mi < 0 || mi >= g_dev.n_mats || !g_dev.mats[mi].lbc_on) return nanv();
-    return coulomb_inv(g_dev.mats[mi], F, n, NC, NA);
+    MatD md;
+    mat_to_dev(g_dev.mats[mi], md);
+    return coulomb_inv_host(md, F, n, NC, NA);
 }
 int api3_set_surface_mobility(int mi, double delta, double eta, double mu1) {   // semiconductor_3d.c:4885-4893
     Inst &d = g_dev;

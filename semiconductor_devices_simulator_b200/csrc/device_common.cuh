@@ -233,6 +233,68 @@ __device__ __forceinline__ void recomb(const MatD &m, double ni, double tf, doub
     dRp = dsp + m.Cp * np_ + Au * n + m.Brad * n;
 }
 
+// Shockley-Read-Hall statistics of the trap entries of node k at densities n, p
+// (semiconductor_3d.c:368-400): recombination R with dR/dn, dR/dp, and the trapped charge
+// rho (elementary charges per m^3) with d rho / d psi at fixed quasi-Fermi levels; the
+// occupancy f = (cn n + cp p1) / (cn (n + n1) + cp (p + p1)) with n1, p1 at the local band
+// edges, so the equilibrium is exact
+__device__ __forceinline__ bool trap_node(const DevP &P, int k) { return P.tr_rp && P.tr_rp[k] < P.tr_rp[k + 1]; }
+__device__ __forceinline__ void trap_levels(const TrapD &s, const MatD &m, double ni, double &n1, double &p1) {
+    const double VT = m.VT;
+    if (s.ref == 0) { n1 = m.Nc * exp(-s.E / VT); p1 = ni * ni / n1; }
+    else if (s.ref == 1) { p1 = m.Nv * exp(-s.E / VT); n1 = ni * ni / p1; }
+    else { n1 = ni * exp(s.E / VT); p1 = ni * exp(-s.E / VT); }
+}
+__device__ __forceinline__ void trap_eval(const DevP &P, const MatD &m, int k, double n, double p, double &R,
+                                          double &dRn, double &dRp, double &rho, double &drho) {
+    R = dRn = dRp = rho = drho = 0.0;
+    if (!trap_node(P, k)) return;
+    const double VT = m.VT, ni = niK(P, m, k), ni2 = ni * ni;
+    for (int q = P.tr_rp[k]; q < P.tr_rp[k + 1]; q++) {
+        const TrapD &s = P.tsp[P.tr_s[q]];
+        double n1, p1;
+        trap_levels(s, m, ni, n1, p1);
+        const double cn = P.tr_cn[q], cp = P.tr_cp[q], Nt = P.tr_N[q];
+        const double den = cn * (n + n1) + cp * (p + p1) + 1e-300, np_ = n * p - ni2, A = Nt * cn * cp;
+        R += A * np_ / den;
+        dRn += A * (p * den - np_ * cn) / (den * den);
+        dRp += A * (n * den - np_ * cp) / (den * den);
+        if (s.type) {
+            const double num = cn * n + cp * p1, f = num / den;
+            const double df = (cn * n * den - num * (cn * n - cp * p)) / (VT * den * den);   // df/dpsi >= 0
+            rho += s.type < 0 ? -Nt * f : Nt * (1.0 - f);
+            drho -= Nt * df;
+        }
+    }
+}
+// charged trap states of node k (m^-3, all signs counted): occupied acceptors plus empty
+// donors - the scattering centres of the trapped charge (trap_abs, semiconductor_3d.c:402-420)
+__device__ __forceinline__ double trap_abs(const DevP &P, const MatD &m, int k, double n, double p) {
+    if (!trap_node(P, k)) return 0.0;
+    const double ni = niK(P, m, k);
+    double sum = 0.0;
+    for (int q = P.tr_rp[k]; q < P.tr_rp[k + 1]; q++) {
+        const TrapD &s = P.tsp[P.tr_s[q]];
+        if (!s.type) continue;
+        double n1, p1;
+        trap_levels(s, m, ni, n1, p1);
+        const double cn = P.tr_cn[q], cp = P.tr_cp[q], Nt = P.tr_N[q];
+        const double f = (cn * n + cp * p1) / (cn * (n + n1) + cp * (p + p1) + 1e-300);
+        sum += s.type < 0 ? Nt * f : Nt * (1.0 - f);
+    }
+    return sum;
+}
+// band-to-band recombination plus the traps of the node (recombKnp, semiconductor_3d.c:823-837)
+__device__ __forceinline__ void recombK(const DevP &P, const MatD &m, int k, double n, double p, double &R,
+                                        double &dRn, double &dRp) {
+    recomb(m, niK(P, m, k), tauf(P, m, k), n, p, R, dRn, dRp);
+    if (trap_node(P, k)) {
+        double r, a, b, c, e;
+        trap_eval(P, m, k, n, p, r, a, b, c, e);
+        R += r; dRn += a; dRp += b;
+    }
+}
+
 // Caughey-Thomas velocity saturation (semiconductor_3d.c:664-668)
 __device__ __forceinline__ double mob_hf(double mu0, double E, double vsat, double beta) {
     const double r = mu0 * fabs(E) / vsat;

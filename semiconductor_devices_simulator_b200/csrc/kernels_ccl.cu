@@ -132,7 +132,7 @@ __global__ void k_ff_recomb(const DevP *__restrict__ Ps, int hole, const double 
         const double c = lam[b] * P.sc[k] * P.sol[k];
         const double oth = hole ? P.n[k] : P.p[k];
         double R, dRn, dRp;
-        recomb(m, niK(P, m, k), tauf(P, m, k), hole ? oth : c, hole ? c : oth, R, dRn, dRp);
+        recombK(P, m, k, hole ? oth : c, hole ? c : oth, R, dRn, dRp);
         const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
         double g = vol * R, dg = vol * (hole ? dRp : dRn) * c;
         if (P.tk) { g += P.tk[k] * c - P.tg[k]; dg += P.tk[k] * c; }   // metal-contact exchange

@@ -72,6 +72,12 @@ __global__ void k_poisson(const DevP *__restrict__ Ps, int src, int build) {
                 fk += vol * Q * (p - n + P.Nd[k] - P.Na[k] + P.Nf[k]);
                 dg += vol * Q * (n + p) / m.VT;
             }
+            if (trap_node(P, k)) {                    // charge in deep traps
+                double r, a, b, rho, drho;
+                trap_eval(P, m, k, n, p, r, a, b, rho, drho);
+                fk += vol * Q * rho;
+                dg -= vol * Q * drho;
+            }
         } else {
             fk += vol * Q * P.Nf[k];
         }
@@ -167,8 +173,17 @@ __global__ void k_upd_mob(const DevP *__restrict__ Ps) {
                     if (ax == 0) b.i++; else if (ax == 1) b.j++; else b.l++;
                     const double F = sqrt(0.5 * (fnorm2(P, a, k, ax) + fnorm2(P, b, kp, ax)));
                     const double Nt = 0.5 * (P.Nd[k] + P.Na[k] + P.Nd[kp] + P.Na[kp]);
-                    if (m.lb_on & 1) mn = lombardi(m, mn, F, Nt, Dw, 0);
-                    if (m.lb_on & 2) mp = lombardi(m, mp, F, Nt, Dw, 1);
+                    double ic = 0.0;
+                    if (P.if_NC && m.lbc_on) {          // Coulomb scattering, n from the reference levels
+                        const double nn = 0.5 * (nK(P, m, k, P.phi[k], P.phin[k]) +
+                                                 nK(P, P.mats[fl_mat(P.flags[kp])], kp, P.phi[kp], P.phin[kp]));
+                        const int ea = P.qi[k], eb = P.qi[kp];
+                        const double NC = ea >= 0 && eb >= 0 ? 0.5 * (P.if_NC[ea] + P.if_NC[eb])
+                                        : (ea >= 0 ? P.if_NC[ea] : (eb >= 0 ? P.if_NC[eb] : 0.0));
+                        ic = coul_inv(m, F, nn, NC, 0.5 * (P.Na[k] + P.Na[kp]));
+                    }
+                    if (m.lb_on & 1) mn = lombardi(m, mn, F, Nt, Dw, 0, ic);
+                    if (m.lb_on & 2) mp = lombardi(m, mp, F, Nt, Dw, 1, 0.0);
                 }
             }
             // velocity saturation, tapered off across the barrier region of a metal contact
@@ -198,7 +213,30 @@ __global__ void k_upd_mob(const DevP *__restrict__ Ps) {
         }
     }
 }
-void launch_upd_mob(const Ctx &c) { SS_LAUNCH(PF_UPDMOB, c.maxN, k_upd_mob, grid_of(c), TPB, c.st, c.dP); }
+// N_C of every Coulomb interface entry: fixed charge plus the charged trap states of the
+// node at the reference quasi-Fermi potentials, per interface area (coul_update,
+// semiconductor_3d.c:1624-1636)
+__global__ void k_coul_update(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[blockIdx.y];
+    SS_GRID_LOOP(e, P.n_if) {
+        const int k = P.if_k[e];
+        const double A = P.if_A[e];
+        if (!(A > 0.0)) { P.if_NC[e] = 0.0; continue; }
+        double Qt = 0.0;
+        if (trap_node(P, k)) {
+            const MatD &m = P.mats[fl_mat(P.flags[k])];
+            const Node a = unidx(k, P.Nx, P.Ny);
+            Qt = trap_abs(P, m, k, nK(P, m, k, P.phi[k], P.phin[k]), pK(P, m, k, P.phi[k], P.phip[k])) *
+                 (P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l]);
+        }
+        P.if_NC[e] = (P.if_Qf[e] + Qt) / A;
+    }
+}
+void launch_upd_mob(const Ctx &c) {
+    if (c.h.if_NC && (c.h.models & 16))
+        SS_LAUNCH(PF_UPDMOB, c.h.n_if, k_coul_update, dim3(c.nodes_blocks(), c.ninst), TPB, c.st, c.dP);
+    SS_LAUNCH(PF_UPDMOB, c.maxN, k_upd_mob, grid_of(c), TPB, c.st, c.dP);
+}
 
 // ------------------------------------------------------------------ continuity
 // Scaled Scharfetter-Gummel row for u = c/s (semiconductor_3d.c:3067-3106):
@@ -246,7 +284,7 @@ __global__ void k_cont_assemble(const DevP *__restrict__ Ps, int hole) {
             else off[dir] = -nb * fmax(car[kb], NFLOOR);
         }
         double R, dRn, dRp;
-        recomb(m, niK(P, m, k), tauf(P, m, k), P.n[k], P.p[k], R, dRn, dRp);
+        recombK(P, m, k, P.n[k], P.p[k], R, dRn, dRp);
         double dR = hole ? dRp : dRn;
         if (dR < 0.0) dR = 0.0;
         const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
@@ -305,18 +343,25 @@ void launch_cont_update(const Ctx &c, int hole, double lo, double hi) {
 
 // ------------------------------------------------------------------ boundary values
 // neutral potential with both quasi-Fermi levels at V (semiconductor_3d.c:1782-1805): the
-// closed form, and with incompletely ionised dopants a safeguarded Newton on
-// p - n + N_D+ - N_A- + Nf = 0 (decreasing in psi) from it, at most 200 steps
+// closed form, and with deep traps or incompletely ionised dopants a safeguarded Newton on
+// p - n + N_D+ - N_A- + Nf + trapped charge = 0 (decreasing in psi) from it, at most 200 steps
 __device__ double neutral_psi(const DevP &P, const MatD &m, int k, double V) {
     const double D = P.Nd[k] - P.Na[k], VT = m.VT;
     double psi = V + VT * (asinh(D / (2.0 * niK(P, m, k))) - 0.5 * (lncK(P, m, k) - lnvK(P, m, k)));
-    if (!ion_node(P, k)) return psi;
+    const bool io = ion_node(P, k);
+    if (!trap_node(P, k) && !io) return psi;
     double lo = psi - m.Eg - 1.0, hi = psi + m.Eg + 1.0;
     for (int it = 0; it < 200; it++) {
         const double n = nK(P, m, k, psi, V), p = pK(P, m, k, psi, V);
-        double Np, dNp, Nm, dNm;
-        ion_eval(P, m, k, n, p, Np, dNp, Nm, dNm);
-        const double g = p - n + Np - Nm + P.Nf[k], dg = -(n + p) / VT + dNp - dNm;
+        double a, b, c, r, dr;
+        trap_eval(P, m, k, n, p, a, b, c, r, dr);
+        double g = p - n + D + P.Nf[k] + r, dg = -(n + p) / VT + dr;
+        if (io) {                                    // incompletely ionised dopants
+            double Np, dNp, Nm, dNm;
+            ion_eval(P, m, k, n, p, Np, dNp, Nm, dNm);
+            g = p - n + Np - Nm + P.Nf[k] + r;
+            dg = -(n + p) / VT + dr + dNp - dNm;
+        }
         if (g > 0.0) lo = psi; else hi = psi;
         double nx = dg < 0.0 ? psi - g / dg : 0.5 * (lo + hi);
         if (!(nx > lo && nx < hi)) nx = 0.5 * (lo + hi);
@@ -587,7 +632,7 @@ __global__ void k_upd_J(const DevP *__restrict__ Ps) {
         }
         const MatD &m = P.mats[fl_mat(f)];
         double R, x, y;
-        recomb(m, niK(P, m, k), tauf(P, m, k), P.n[k], P.p[k], R, x, y);
+        recombK(P, m, k, P.n[k], P.p[k], R, x, y);
         P.Rt[k] = R;
     }
 }
@@ -674,14 +719,27 @@ __global__ void k_node_val(const DevP *__restrict__ Ps, int which, double *out) 
             break;
         }
         case 30: v = kd == K_SEMI ? P.qd[k] : nan; break;        // distance to the nearest wall
-        case 31: case 32: v = kd == K_SEMI ? 0.0 : nan; break;   // traps: not built
+        case 31: case 32: {                         // trapped charge (q/m^3) / total trap density (m^-3)
+            if (kd != K_SEMI) { v = nan; break; }
+            if (!trap_node(P, k)) { v = 0.0; break; }
+            if (which == 32) {
+                double sN = 0.0;
+                for (int e = P.tr_rp[k]; e < P.tr_rp[k + 1]; e++) sN += P.tr_N[e];
+                v = sN;
+            } else {
+                double r, a, b, rho, drho;
+                trap_eval(P, m, k, P.n[k], P.p[k], r, a, b, rho, drho);
+                v = rho;
+            }
+            break;
+        }
         case 33: {                                  // impact-ionisation generation (m^-3 s^-1)
             if (kd != K_SEMI || !P.gii) { v = 0.0; break; }
             const double vol = P.Lx[a.i] * P.Ly[a.j] * P.Lz[a.l];
             v = vol > 0.0 ? P.gii[k] / vol : 0.0;
             break;
         }
-        case 34: v = kd == K_SEMI ? 0.0 : nan; break;            // Coulomb N_C: not built
+        case 34: v = kd == K_SEMI ? (P.if_NC && P.qi[k] >= 0 ? P.if_NC[P.qi[k]] : 0.0) : nan; break;   // N_C (m^-2)
         case 35: {                                  // ionised net doping N_D+ - N_A-
             if (kd != K_SEMI) { v = 0.0; break; }
             double Np, dNp, Nm, dNm;

@@ -201,27 +201,6 @@ double mobility_low(const Material &m, double Ntot, int hole) {
     return mumin + (mumax - mumin) / (1. + std::pow(Ntot / Nref, alpha));
 }
 
-// n_trans (cm^-3) of the Coulomb term against the acceptor doping (cm^-3): log-log
-// interpolation of four points, clamped (semiconductor_3d.c:2937-2944)
-static double ntrans_sic(double NA) {
-    static const double a[4] = {1e15, 1e16, 5e16, 5e17}, t[4] = {2.8e16, 8e16, 2.5e17, 1.55e18};
-    if (!(NA > a[0])) return t[0];
-    if (NA >= a[3]) return t[3];
-    int q = 0;
-    while (NA > a[q + 1]) q++;
-    return t[q] * std::pow(t[q + 1] / t[q], std::log(NA / a[q]) / std::log(a[q + 1] / a[q]));
-}
-// 1/mu_C (cm^2/Vs)^-1 of electrons at density n (m^-3) in a normal field Fv (V/m) near an
-// interface holding NC charges per m^2, acceptor doping NA (m^-3) (semiconductor_3d.c:2948-2955)
-double coulomb_inv(const Material &m, double Fv, double n, double NC, double NA) {
-    const double F = Fv * 1e-2, r = NC * 1e-4 / m.lbc_N0;
-    if (!(r > 0.) || !(F > 0.)) return 0.;
-    const double f = 1. - std::exp(-std::pow(F / m.lbc_E0, m.lbc_gam));
-    if (!(f > 0.)) return 0.;
-    const double s = std::pow(n * 1e-6 / (ntrans_sic(NA * 1e-6) * std::pow(r, m.lbc_e1)), m.lbc_nu);
-    return std::pow(r, m.lbc_e2) * f / (m.lbc_mu1 * (m.T / 300.) * (1. + s));
-}
-
 // Half the band-gap narrowing in units of VT, Klaassen form (semiconductor_3d.c:839-843)
 double bgn_half(const Material &m, double N) {
     if (!(m.bgn_E > 0.) || N < 1.) return 0.;

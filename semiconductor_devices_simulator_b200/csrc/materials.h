@@ -45,8 +45,8 @@ struct Material {
     // mu_sr = D/F^2 (or 1/(F^2/D + F^3/E) with the roughness term E), cm units [0] n, [1] p
     int lb_on = 0;
     double lbB[2] = {0, 0}, lbC[2] = {0, 0}, lbL[2] = {0, 0}, lbD[2] = {0, 0}, lbE[2] = {0, 0};
-    // Coulomb scattering of electrons on interface charge (4H-SiC; the solver does not build
-    // it, api3_coulomb_inv evaluates it): mu1 (cm^2/Vs), nu, N0 (cm^-2), e1, e2, E0 (V/cm), gamma
+    // Coulomb scattering of electrons on interface charge (4H-SiC, in the Lombardi sum):
+    // mu1 (cm^2/Vs), nu, N0 (cm^-2), e1, e2, E0 (V/cm), gamma
     int lbc_on = 0;
     double lbc_mu1 = 0, lbc_nu = 0, lbc_N0 = 1, lbc_e1 = 0, lbc_e2 = 0, lbc_E0 = 1, lbc_gam = 1;
     double lnc = 0, lnv = 0;      // effective ln Nc / ln Nv in the common gauge (mat_prepare)
@@ -55,6 +55,5 @@ struct Material {
 void material_init(Material &m, int id, double T);
 double mobility_low(const Material &m, double Ntot, int hole);
 double bgn_half(const Material &m, double N);
-double coulomb_inv(const Material &m, double Fv, double n, double NC, double NA);
 
 }  // namespace ss

@@ -116,8 +116,9 @@ SS_HD void tun_flux(const MatD &ms, const TPath &P, double Ecp, double Evp, doub
     F[3] = ch * tun_int(P, Evp, EFm, kT, 1);
 }
 
-// Lombardi: 1/mu = 1/mu_b + D (1/mu_ac + 1/mu_sr), cm units inside
-SS_HD double lombardi(const MatD &m, double mub, double Fv, double Nt, double Dw, int hole) {
+// Lombardi: 1/mu = 1/mu_b + D (1/mu_ac + 1/mu_sr + invC), cm units inside; invC the 1/mu of
+// further surface terms (Coulomb), (cm^2/Vs)^-1
+SS_HD double lombardi(const MatD &m, double mub, double Fv, double Nt, double Dw, int hole, double invC) {
     double F = Fv * 1e-2;
     if (F < 1.0) F = 1.0;                          // V/cm
     double N = Nt * 1e-6;
@@ -125,7 +126,29 @@ SS_HD double lombardi(const MatD &m, double mub, double Fv, double Nt, double Dw
     const double Bc = m.lbB[hole], Cc = m.lbC[hole], Lc = m.lbL[hole], Dc = m.lbD[hole], Ec = m.lbE[hole];
     const double muac = Bc / F + Cc * pow(N, Lc) / (cbrt(F) * (m.T / 300.0));
     const double musr = Ec > 0.0 ? 1.0 / (F * F / Dc + F * F * F / Ec) : Dc / (F * F);
-    return 1.0 / (1.0 / mub + Dw * 1e4 * (1.0 / muac + 1.0 / musr));
+    return 1.0 / (1.0 / mub + Dw * 1e4 * (1.0 / muac + 1.0 / musr + invC));
+}
+
+// n_trans (cm^-3) of the Coulomb term against the acceptor doping (cm^-3): log-log
+// interpolation of four points, clamped (semiconductor_3d.c:2937-2944)
+SS_HD double ntrans_sic(double NA) {
+    const double a[4] = {1e15, 1e16, 5e16, 5e17}, t[4] = {2.8e16, 8e16, 2.5e17, 1.55e18};
+    if (!(NA > a[0])) return t[0];
+    if (NA >= a[3]) return t[3];
+    int q = 0;
+    while (NA > a[q + 1]) q++;
+    return t[q] * pow(t[q + 1] / t[q], log(NA / a[q]) / log(a[q + 1] / a[q]));
+}
+// 1/mu_C (cm^2/Vs)^-1 of electrons at density n (m^-3) in a normal field Fv (V/m) near an
+// interface holding NC charges per m^2, acceptor doping NA (m^-3); 0 without interface
+// charge or normal field (semiconductor_3d.c:2948-2955)
+SS_HD double coul_inv(const MatD &m, double Fv, double n, double NC, double NA) {
+    const double F = Fv * 1e-2, r = NC * 1e-4 / m.lbc_N0;
+    if (!(r > 0.0) || !(F > 0.0)) return 0.0;
+    const double f = 1.0 - exp(-pow(F / m.lbc_E0, m.lbc_gam));
+    if (!(f > 0.0)) return 0.0;
+    const double s = pow(n * 1e-6 / (ntrans_sic(NA * 1e-6) * pow(r, m.lbc_e1)), m.lbc_nu);
+    return pow(r, m.lbc_e2) * f / (m.lbc_mu1 * (m.T / 300.0) * (1.0 + s));
 }
 
 }  // namespace ss

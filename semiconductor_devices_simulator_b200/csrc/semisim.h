@@ -49,7 +49,8 @@ struct MatD {
     double ms_e, ms_h;                       // supply masses of gate tunnelling
     double ii_a[2][2], ii_b[2][2], ii_E0[2], ii_m[2], ii_g;   // impact ionisation (models bit 8)
     double lbB[2], lbC[2], lbL[2], lbD[2], lbE[2];           // Lombardi surface mobility (models bit 4)
-    int insulator, ii_on, lb_on, pad;
+    double lbc_mu1, lbc_nu, lbc_N0, lbc_e1, lbc_e2, lbc_E0, lbc_gam;   // its Coulomb term (4H-SiC)
+    int insulator, ii_on, lb_on, lbc_on;
 };
 
 // contact constants the kernels need
@@ -97,6 +98,18 @@ struct DevP {
     double *qcn, *qcp, *tk, *tg;
     double *imgn, *imgp;          // the image-force part of qcn / qcp (metal contacts)
     double *gii;                  // impact-ionisation pair generation of the node (1/s; null: models bit 8 off)
+    // deep-level traps (null without them): per node the range tr_rp[k]..tr_rp[k+1] of its
+    // entries - species, density (m^-3), capture coefficients cn, cp (m^3/s)
+    const int *tr_rp, *tr_s;
+    const double *tr_N, *tr_cn, *tr_cp;
+    const struct TrapD *tsp;      // species: type (-1 acceptor, 1 donor, 0 neutral), level reference, energy
+    // Coulomb scattering on interface charge (models bit 4 with a Coulomb material; null
+    // without): per node its nearest interface entry (-1: none within reach); per entry its
+    // node, dual-face area, fixed charge (elementary charges) and N_C (m^-2)
+    const int *qi, *if_k;
+    const double *if_A, *if_Qf;
+    double *if_NC;
+    int n_if, pad_if;
     const float *te_vw;
     const signed char *te_ax;
     const MatD *mats;
@@ -136,6 +149,13 @@ struct DevP {
     LevelT<float> *levf;
     int *ccl;                     // labels for connected-component work
     int *cclaux;
+};
+
+// a deep-level species: type -1 acceptor / +1 donor / 0 neutral; E (eV) below Ec (ref 0),
+// above Ev (ref 1) or above the intrinsic level (ref 2)
+struct TrapD {
+    int type, ref;
+    double E;
 };
 
 // Thermionic-emission metal contacts (models bit 6, semiconductor_3d.c:3390-3571): the

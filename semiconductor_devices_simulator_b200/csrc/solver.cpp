@@ -211,6 +211,8 @@ void gpu_free(Inst &d) {
     if (d.g.qc) cudaFree(d.g.qc);
     if (d.g.xchg) cudaFree(d.g.xchg);
     if (d.g.tunblock) cudaFree(d.g.tunblock);
+    if (d.g.trblock) cudaFree(d.g.trblock);
+    if (d.g.coblock) cudaFree(d.g.coblock);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();
@@ -355,33 +357,12 @@ void mat_to_dev(const Material &m, MatD &o) {
     }
     o.ii_g = m.ii_g;
     o.lb_on = m.lb_on;
+    o.lbc_on = m.lbc_on;
+    o.lbc_mu1 = m.lbc_mu1; o.lbc_nu = m.lbc_nu; o.lbc_N0 = m.lbc_N0; o.lbc_e1 = m.lbc_e1; o.lbc_e2 = m.lbc_e2;
+    o.lbc_E0 = m.lbc_E0; o.lbc_gam = m.lbc_gam;
     for (int c = 0; c < 2; c++) {
         o.lbB[c] = m.lbB[c]; o.lbC[c] = m.lbC[c]; o.lbL[c] = m.lbL[c]; o.lbD[c] = m.lbD[c]; o.lbE[c] = m.lbE[c];
     }
-}
-
-// Reject inputs that need models this library does not build.
-static int check_scope(const Inst &d, const std::vector<unsigned char> &kind) {
-    bool any_ins = false, any_gate = false;
-    for (size_t k = 0; k < d.N; k++) if (kind[k] == K_INS) { any_ins = true; break; }
-    for (int c = 0; c < d.n_cons; c++) if (d.cons[c].bc == 2) any_gate = true;
-    auto used = [&](int mi) {
-        for (size_t k = 0; k < d.N; k++) if (d.mat_idx[k] == mi && kind[k] == K_SEMI) return true;
-        return false;
-    };
-    const char *why = nullptr;
-    if (d.n_trap_entries > 0) why = "deep-level traps";
-    for (int mi = 0; mi < d.n_mats; mi++) {
-        const Material &m = d.mats[mi];
-        if (m.insulator) continue;
-        if ((d.models & 16) && m.lbc_on && (m.lb_on & 1) && (any_ins || any_gate) && used(mi))
-            why = "Coulomb scattering on interface charge (models bit 4, 4H-SiC)";
-    }
-    if (why) {
-        std::fprintf(stderr, "semisim-b200: %s is not supported by this solver library\n", why);
-        return 0;
-    }
-    return 1;
 }
 
 // prepare (semiconductor_3d.c:1638-1775): node kinds, contact and gate masks, Robin gate
@@ -675,6 +656,220 @@ static void sc_build(size_t N, const TunHost &U, const std::vector<int> &tc_k, S
     }
 }
 
+// Deep-level traps (traps_build, semiconductor_3d.c:1428-1468): the requests compiled into
+// per-node lists (semiconductor nodes only), entries of one species on one node summed in
+// the order of their first request; capture coefficients sigma v_th with
+// v_th = sqrt(3 kT / m*) from the node material's tunnelling masses.  Uploaded with the
+// species table into one allocation.
+static int traps_upload(Inst &d, const std::vector<unsigned char> &kind, DevP &P, cudaStream_t st) {
+    if (d.g.trblock) { cudaFree(d.g.trblock); d.g.trblock = nullptr; }
+    P.tr_rp = P.tr_s = nullptr;
+    P.tr_N = P.tr_cn = P.tr_cp = nullptr;
+    P.tsp = nullptr;
+    d.n_tr = 0;
+    if (d.trq_k.empty()) return 1;
+    const size_t N = d.N;
+    std::vector<int> rp(N + 1, 0);
+    for (size_t q = 0; q < d.trq_k.size(); q++) {
+        const size_t k = (size_t)(unsigned)d.trq_k[q];
+        if (k < N && kind[k] == K_SEMI) rp[k + 1]++;
+    }
+    for (size_t k = 0; k < N; k++) rp[k + 1] += rp[k];
+    std::vector<int> fill(rp), ts(rp[N] > 0 ? rp[N] : 1);
+    std::vector<double> tN(ts.size());
+    for (size_t q = 0; q < d.trq_k.size(); q++) {
+        const size_t k = (size_t)(unsigned)d.trq_k[q];
+        if (k >= N || kind[k] != K_SEMI) continue;
+        const int sid = d.trq_s[q];
+        int w = -1;
+        for (int e = rp[k]; e < fill[k]; e++) if (ts[e] == sid) { w = e; break; }
+        if (w >= 0) { tN[w] += d.trq_N[q]; continue; }
+        w = fill[k]++;
+        ts[w] = sid; tN[w] = d.trq_N[q];
+    }
+    int o = 0;                                            // compact the merged duplicates
+    for (size_t k = 0; k < N; k++) {
+        const int a = rp[k], b = fill[k];
+        rp[k] = o;
+        for (int e = a; e < b; e++) { ts[o] = ts[e]; tN[o] = tN[e]; o++; }
+    }
+    rp[N] = o;
+    d.n_tr = o;
+    if (o == 0) return 1;
+    std::vector<double> tcn(o), tcp(o);
+    const double M0_ = 9.1093837015e-31;
+    for (size_t k = 0; k < N; k++) {
+        if (rp[k] == rp[k + 1]) continue;
+        const Material &m = d.mats[d.mat_idx[k]];
+        const double me = m.mtun_e > 0. ? m.mtun_e : 0.3, mh = m.mtun_h > 0. ? m.mtun_h : 0.5;
+        const double vn = std::sqrt(3. * KB * m.T / (me * M0_)), vp = std::sqrt(3. * KB * m.T / (mh * M0_));
+        for (int e = rp[k]; e < rp[k + 1]; e++) {
+            const TrapSpec &sp = d.tsp[ts[e]];
+            tcn[e] = sp.sn * vn; tcp[e] = sp.sp * vp;
+        }
+    }
+    std::vector<TrapD> tab(d.n_tsp > 0 ? d.n_tsp : 1);
+    for (int q = 0; q < d.n_tsp; q++) { tab[q].type = d.tsp[q].type; tab[q].ref = d.tsp[q].ref; tab[q].E = d.tsp[q].E; }
+    size_t off = 0;
+    auto room = [&](size_t bytes) { const size_t x = off; off += align_up(bytes > 0 ? bytes : 1); return x; };
+    const size_t o_rp = room((N + 1) * 4), o_s = room((size_t)o * 4), o_N = room((size_t)o * 8),
+                 o_cn = room((size_t)o * 8), o_cp = room((size_t)o * 8), o_tab = room(tab.size() * sizeof(TrapD));
+    char *b = nullptr;
+    if (cudaMalloc(&b, off) != cudaSuccess) {
+        std::fprintf(stderr, "semisim-b200: out of device memory for the traps\n");
+        return 0;
+    }
+    d.g.trblock = b;
+    bool ok = true;
+    auto up = [&](size_t x, const void *src, size_t bytes) {
+        if (bytes && cudaMemcpyAsync(b + x, src, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) ok = false;
+    };
+    up(o_rp, rp.data(), (N + 1) * 4); up(o_s, ts.data(), (size_t)o * 4); up(o_N, tN.data(), (size_t)o * 8);
+    up(o_cn, tcn.data(), (size_t)o * 8); up(o_cp, tcp.data(), (size_t)o * 8); up(o_tab, tab.data(), tab.size() * sizeof(TrapD));
+    P.tr_rp = (const int *)(b + o_rp); P.tr_s = (const int *)(b + o_s);
+    P.tr_N = (const double *)(b + o_N); P.tr_cn = (const double *)(b + o_cn); P.tr_cp = (const double *)(b + o_cp);
+    P.tsp = (const TrapD *)(b + o_tab);
+    if (!ok) return 0;
+    if (d.verbose) std::fprintf(stderr, "semisim-b200: %d trap entries (%d species) on the mesh\n", d.n_tr, d.n_tsp);
+    return 1;
+}
+
+// Coulomb scattering on interface charge (coul_build, semiconductor_3d.c:1540-1623; models
+// bit 4 with a material whose electrons have the Coulomb term): the interface entries are
+// the semiconductor nodes of such a material, of no contact, next to an insulator node or
+// under a face gate; an entry's area is its dual faces to insulator nodes (plus a Robin
+// gate's area), its fixed charge the node's own |Nf| and its insulator neighbours' shared
+// by area (plus the gate's oxide charge).  Every node of a Coulomb material then takes the
+// nearest entry with an area within 150 nm, found by a breadth-first search from the entries.
+static int coul_upload(Inst &d, const std::vector<unsigned char> &kind, const std::vector<int> &con,
+                       const std::vector<int> &gate, const std::vector<int> &rob_k, const std::vector<double> &rob_A,
+                       const std::vector<int> &rob_c, DevP &P, cudaStream_t st) {
+    if (d.g.coblock) { cudaFree(d.g.coblock); d.g.coblock = nullptr; }
+    P.qi = P.if_k = nullptr;
+    P.if_A = P.if_Qf = nullptr;
+    P.if_NC = nullptr;
+    P.n_if = 0;
+    if (!(d.models & 16)) return 1;
+    bool any = false;
+    for (int q = 0; q < d.n_mats; q++) if (d.mats[q].lbc_on && (d.mats[q].lb_on & 1)) any = true;
+    if (!any) return 1;
+    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
+    const size_t N = d.N;
+    auto nbrs = [&](size_t k, size_t *kb, double *ar) {
+        const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny), j = rem / Nx, i = rem % Nx;
+        int c = 0;
+        if (i > 0) { kb[c] = k - 1; ar[c++] = d.Ly[j] * d.Lz[l]; }
+        if (i < Nx - 1) { kb[c] = k + 1; ar[c++] = d.Ly[j] * d.Lz[l]; }
+        if (j > 0) { kb[c] = k - Nx; ar[c++] = d.Lx[i] * d.Lz[l]; }
+        if (j < Ny - 1) { kb[c] = k + Nx; ar[c++] = d.Lx[i] * d.Lz[l]; }
+        if (l > 0) { kb[c] = k - (size_t)Nx * Ny; ar[c++] = d.Lx[i] * d.Ly[j]; }
+        if (l < Nz - 1) { kb[c] = k + (size_t)Nx * Ny; ar[c++] = d.Lx[i] * d.Ly[j]; }
+        return c;
+    };
+    auto xyz = [&](size_t k, double *pq) {
+        const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny);
+        pq[0] = d.xs[rem % Nx]; pq[1] = d.ys[rem / Nx]; pq[2] = d.zs[l];
+    };
+    auto vol = [&](size_t k) {
+        const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny);
+        return d.Lx[rem % Nx] * d.Ly[rem / Nx] * d.Lz[l];
+    };
+    auto d2 = [](const double *a, const double *b) {
+        const double x = a[0] - b[0], y = a[1] - b[1], z = a[2] - b[2];
+        return x * x + y * y + z * z;
+    };
+    std::vector<int> qi(N, -1), ik;
+    size_t kb[6], kb2[6];
+    double ar[6], ar2[6];
+    for (size_t k = 0; k < N; k++) {
+        if (kind[k] != K_SEMI || con[k] || !d.mats[d.mat_idx[k]].lbc_on) continue;
+        bool is = gate[k] != 0;
+        if (!is) {
+            const int c = nbrs(k, kb, ar);
+            for (int q = 0; q < c; q++) if (kind[kb[q]] == K_INS) { is = true; break; }
+        }
+        if (is) { qi[k] = (int)ik.size(); ik.push_back((int)k); }
+    }
+    const int cnt = (int)ik.size();
+    if (!cnt) return 1;
+    std::vector<double> iA(cnt, 0.), iQ(cnt, 0.);
+    for (int e = 0; e < cnt; e++) {
+        const size_t k = (size_t)ik[e];
+        const int c = nbrs(k, kb, ar);
+        double A = 0., Qf = std::fabs(d.Nf[k]) * vol(k);
+        for (int q = 0; q < c; q++) {
+            const size_t ko = kb[q];
+            if (kind[ko] != K_INS) continue;
+            A += ar[q];
+            if (d.Nf[ko] != 0.) {
+                const int c2 = nbrs(ko, kb2, ar2);
+                double As = 0.;
+                for (int q2 = 0; q2 < c2; q2++) if (kind[kb2[q2]] == K_SEMI) As += ar2[q2];
+                if (As > 0.) Qf += std::fabs(d.Nf[ko]) * vol(ko) * ar[q] / As;
+            }
+        }
+        iA[e] = A; iQ[e] = Qf;
+    }
+    for (size_t r = 0; r < rob_k.size(); r++) {
+        const int e = qi[rob_k[r]];
+        if (e < 0) continue;
+        iA[e] += rob_A[r];
+        iQ[e] += std::fabs(d.cons[rob_c[r]].qox) / Q * rob_A[r];
+    }
+    // breadth-first search from the entries with an area (a ring of N slots)
+    std::vector<size_t> qu(N);
+    std::vector<char> inq(N, 0);
+    size_t head = 0, tail = 0, used = 0;
+    for (int e = 0; e < cnt; e++) {
+        const size_t k = (size_t)ik[e];
+        if (iA[e] > 0.) { qu[tail] = k; tail = (tail + 1) % N; used++; inq[k] = 1; }
+        else qi[k] = -1;
+    }
+    const double R2 = 150e-9 * 150e-9;
+    while (used) {
+        const size_t u = qu[head];
+        head = (head + 1) % N; used--; inq[u] = 0;
+        const int lab = qi[u];
+        if (lab < 0) continue;
+        double pl[3], pv[3], pc[3];
+        xyz((size_t)ik[lab], pl);
+        const int c = nbrs(u, kb, ar);
+        for (int q = 0; q < c; q++) {
+            const size_t v = kb[q];
+            if (kind[v] != K_SEMI || !d.mats[d.mat_idx[v]].lbc_on) continue;
+            xyz(v, pv);
+            const double r2 = d2(pv, pl);
+            if (r2 > R2) continue;
+            const int cur = qi[v];
+            if (cur == lab) continue;
+            if (cur >= 0) { xyz((size_t)ik[cur], pc); if (r2 >= d2(pv, pc)) continue; }
+            qi[v] = lab;
+            if (!inq[v]) { qu[tail] = v; tail = (tail + 1) % N; used++; inq[v] = 1; }
+        }
+    }
+    size_t off = 0;
+    auto room = [&](size_t bytes) { const size_t x = off; off += align_up(bytes > 0 ? bytes : 1); return x; };
+    const size_t o_qi = room(N * 4), o_ik = room((size_t)cnt * 4), o_A = room((size_t)cnt * 8),
+                 o_Q = room((size_t)cnt * 8), o_NC = room((size_t)cnt * 8);
+    char *b = nullptr;
+    if (cudaMalloc(&b, off) != cudaSuccess) {
+        std::fprintf(stderr, "semisim-b200: out of device memory for the interface entries\n");
+        return 0;
+    }
+    d.g.coblock = b;
+    bool ok = cudaMemsetAsync(b, 0, off, st) == cudaSuccess;
+    auto up = [&](size_t x, const void *src, size_t bytes) {
+        if (bytes && cudaMemcpyAsync(b + x, src, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) ok = false;
+    };
+    up(o_qi, qi.data(), N * 4); up(o_ik, ik.data(), (size_t)cnt * 4);
+    up(o_A, iA.data(), (size_t)cnt * 8); up(o_Q, iQ.data(), (size_t)cnt * 8);
+    P.qi = (const int *)(b + o_qi); P.if_k = (const int *)(b + o_ik);
+    P.if_A = (const double *)(b + o_A); P.if_Qf = (const double *)(b + o_Q); P.if_NC = (double *)(b + o_NC);
+    P.n_if = cnt;
+    if (d.verbose) std::fprintf(stderr, "semisim-b200: %d interface nodes for Coulomb scattering\n", cnt);
+    return ok ? 1 : 0;
+}
+
 // device copy of the tunnelling paths and the exchange gather (one allocation)
 static int tun_upload(Inst &d, const TunHost &U, const ScHost &G, cudaStream_t st) {
     if (d.g.tunblock) { cudaFree(d.g.tunblock); d.g.tunblock = nullptr; }
@@ -844,7 +1039,6 @@ int prepare(Inst &d) {
         });
         cn.A = A;
     }
-    if (!check_scope(d, kind)) return 0;
     // flags, contact-node list, low-field mobility
     d.flags.assign(N, 0);
     d.cnode.clear();
@@ -921,6 +1115,8 @@ int prepare(Inst &d) {
     if (P.gii) CK(cudaMemsetAsync(P.gii, 0, N * sizeof(double), d.g.st));
     if (!te_upload(d, teh, P, d.g.st)) return 0;
     if (!tun_upload(d, tuh, sch, d.g.st)) return 0;
+    if (!traps_upload(d, kind, P, d.g.st)) return 0;
+    if (!coul_upload(d, kind, con, gate, rob_k, rob_A, rob_c, P, d.g.st)) return 0;
     // continuity sink / source of the exchange with gate and metal contacts (zero elsewhere)
     P.tk = P.tg = nullptr;
     if (d.g.te_on || d.g.tun_on) {

@@ -52,6 +52,8 @@ struct Gpu {
     double *gii = nullptr;       // impact-ionisation generation (N), with models bit 8
     double *qc = nullptr;        // band corrections qcn, qcp (2 N), with MLDA or metal contacts
     double *xchg = nullptr;      // continuity sink / source tk, tg (2 N), with gate tunnelling or metal contacts
+    void *trblock = nullptr;     // deep-level trap entries (CSR per node) and species
+    void *coblock = nullptr;     // Coulomb interface entries and every node's nearest one
     void *teblock = nullptr;     // metal-contact entries, columns and per-node arrays (one allocation)
     void *tunblock = nullptr;    // gate-tunnelling paths and columns, and the exchange gather
     TunD tun{};
@@ -67,7 +69,7 @@ struct Gpu {
     void *seedx = nullptr;       // its node features (N x 48 BF16), in the same allocation
 };
 
-struct TrapSpec { int type, ref; double E, sn, sp; };   // deep-level species (stored, not solved)
+struct TrapSpec { int type, ref; double E, sn, sp; };   // deep-level species (api3_trap_species)
 
 // launch shapes of an instance's linear-algebra kernels (picked by api3b_autotune)
 struct Tune {
@@ -104,7 +106,9 @@ struct Inst {
     double ii_err = 0;           // impact ionisation: estimated remaining change of the generated current (A)
     double pcg_rtol = 1e-3, ntol_fac = 0.1, bicg_rtol = 1e-4, cont_atol_f = 1;
     int nthreads = 1, caxis = 1, models = 7;
-    int n_trap_entries = 0;
+    std::vector<int> trq_k, trq_s;        // trap requests (api3_trap_add): node, species, density
+    std::vector<double> trq_N;
+    int n_tr = 0;                         // compiled trap entries of the last prepare
     double Cref = 0;
     int ref_mat = 0;
     double Ve1[NC_MAX] = {0}, Ve2[NC_MAX] = {0};
@@ -183,6 +187,7 @@ void mat_prepare(Inst &d);                 // gauge Cref and the effective band 
 double tun_eval_host(const MatD *mats, int smat, int nl, const int *mat, const double *t, double psi, double phin,
                      double phip, double Vg, double pm, double Cref, double *out);
 double lombardi_host(const MatD &m, double mub, double F, double Nt, double Dw, int hole);
+double coulomb_inv_host(const MatD &m, double F, double n, double NC, double NA);
 double mlda_factor_host(const Material &m, double a, double b, int hole);
 // per-point output reductions on the device (outputs.cu)
 double out_emax(Inst &d);

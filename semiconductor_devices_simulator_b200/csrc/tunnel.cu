@@ -198,7 +198,8 @@ double tun_eval_host(const MatD *mats, int smat, int nl, const int *mat, const d
     return Q * ((F[0] - F[1]) - (F[2] - F[3]));
 }
 double lombardi_host(const MatD &m, double mub, double F, double Nt, double Dw, int hole) {
-    return lombardi(m, mub, F, Nt, Dw, hole);
+    return lombardi(m, mub, F, Nt, Dw, hole, 0.0);
 }
+double coulomb_inv_host(const MatD &m, double F, double n, double NC, double NA) { return coul_inv(m, F, n, NC, NA); }
 
 }  // namespace ss

@@ -142,11 +142,12 @@ def _gauss_sd(xs, ys, x0, x1, peak, sigma):
 
 def nmosfet(lib, n=(120, 80, 60), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e17,
             Nsd=1e20, sigma=20e-9, sd_len=100e-9, tox=2e-9, phi_m=4.6, models=4,
-            solver=GUI_SOLVER, vds=(0.05, 1.0), vg_max=1.2, dvg=0.05, h0=0.5e-9):
+            solver=GUI_SOLVER, vds=(0.05, 1.0), vg_max=1.2, dvg=0.05, h0=0.5e-9, material=None, Nox=0.0):
     """n-MOSFET: x along the channel, y into the substrate (y = 0 the gate surface),
     z across the width.  Contacts: source / drain ohmic on the surface over the n+
-    windows, gate as a Robin face gate (oxide tox) over the channel, body ohmic on
-    the back face."""
+    windows, gate as a Robin face gate (oxide tox, fixed oxide charge Nox per m^2) over the
+    channel, body ohmic on the back face.  Silicon unless `material` names another
+    reference material id."""
     lib.api3_init()
     xs = np.linspace(0.0, Lx, n[0])
     ys = graded_axis(Ly, n[1], h0)
@@ -154,7 +155,7 @@ def nmosfet(lib, n=(120, 80, 60), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e17,
     _grid(lib, xs, ys, zs)
     lib.api3_set_solver(*solver)
     lib.api3_set_models(models)
-    si = lib.api3_add_material(SI, 300.0)
+    si = lib.api3_add_material(SI if material is None else material, 300.0)
     Nd2 = _gauss_sd(xs, ys, 0.0, sd_len, Nsd, sigma) + _gauss_sd(xs, ys, Lx - sd_len, Lx, Nsd, sigma)
     Nd = np.ascontiguousarray(np.broadcast_to(Nd2[None, :, :], (n[2], n[1], n[0])).ravel() * 1e6)
     Na = np.full(Nd.shape, Nbody * 1e6)
@@ -169,7 +170,7 @@ def nmosfet(lib, n=(120, 80, 60), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e17,
     nz = n[2] - 1
     cs = lib.api3_add_contact_ex(2, 0, iS1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
     cd = lib.api3_add_contact_ex(2, iD0, n[0] - 1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
-    cg = lib.api3_add_contact_ex(2, iG0, iG1, 0, nz, 0, 0, 2, 0.0, phi_m, tox, 0.0)
+    cg = lib.api3_add_contact_ex(2, iG0, iG1, 0, nz, 0, 0, 2, 0.0, phi_m, tox, Nox)
     cb = lib.api3_add_contact_ex(3, 0, n[0] - 1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
     npts = int(round(vg_max / dvg)) + 1
     V = np.round(np.linspace(0.0, vg_max, npts), 12)
