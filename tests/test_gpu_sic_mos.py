@@ -5,8 +5,10 @@ of acceptor traps on the surface nodes; without and with incomplete ionisation (
 The small n-MOSFET geometry in 4H-SiC with a 20 nm oxide, gate swept 0..6 V at Vd = 0.5 V.
 
 Converged tightly: drain current within 1e-6 relative or the floor, psi within 1e-6 V, the
-interface-charge, display-mobility and trapped-charge maps (bulk_copy 34, 10, 31) within
-1e-9 of their peaks."""
+interface-charge and trapped-charge maps (bulk_copy 34, 31) within 1e-9 of their peaks, the
+display electron mobility (bulk_copy 10) within 1e-6: through the Coulomb term it depends on
+the channel electron density, which the tight solve converges to that level (measured
+2e-7)."""
 import ctypes
 import os
 import sys
@@ -74,8 +76,8 @@ def test_sic_channel_matches_reference(lib, prec, models, monkeypatch):
     tol = np.maximum(1e-6 * np.abs(r[1]), r[2])
     assert (np.abs(g[1] - r[1]) <= tol).all(), f"currents\n{g[1]}\n{r[1]}"
     assert np.abs(g[4] - r[4]).max() <= 1e-6
-    for q in (5, 6, 7):
+    for q, rt in ((5, 1e-9), (6, 1e-6), (7, 1e-9)):
         a, b = g[q], r[q]
         assert np.array_equal(np.isnan(a), np.isnan(b))
         m = ~np.isnan(b)
-        assert np.abs(a[m] - b[m]).max() <= 1e-9 * np.abs(b[m]).max(), f"map {q}"
+        assert np.abs(a[m] - b[m]).max() <= rt * np.abs(b[m]).max(), f"map {q}"
