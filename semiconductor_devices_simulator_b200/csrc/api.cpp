@@ -59,7 +59,8 @@ const std::vector<double> *node_vals(Inst &d, int which) {
     if (d.cache.size() < 36) { d.cache.assign(36, {}); d.cache_ok.assign(36, 0); }
     if (!d.cache_ok[which]) {
         Ctx c = make_ctx(d);
-        launch_node_val(c, which, d.g.scratch);
+        if (d.unstr && which >= 20 && which <= 25) launch_node_Jc_g(c, which, d.g.scratch);   // least squares
+        else launch_node_val(c, which, d.g.scratch);
         d.cache[which].resize(d.N);
         cudaMemcpyAsync(d.cache[which].data(), d.g.scratch, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
         cudaStreamSynchronize(d.g.st);
@@ -80,6 +81,17 @@ int con_of(const Inst &d, size_t k) { return fl_con(d.flags[k]); }
 
 // neighbours with their Poisson coupling eps A / h and spacing (semiconductor_3d.c:5166-5186)
 int qnbrs(const Inst &d, size_t k, size_t *nb, double *cf, double *hh) {
+    if (d.unstr) {                                  // the graph's edges, in CSR order (at most 64)
+        const GraphHost &G = d.ggh;
+        const double ek = d.mats[d.mat_idx[k]].eps_r * EPS0;
+        int m = 0;
+        for (int e = G.rp[k]; e < G.rp[k + 1] && m < 64; e++) {
+            const size_t kb = (size_t)G.cj[e];
+            const double eb = d.mats[d.mat_idx[kb]].eps_r * EPS0;
+            nb[m] = kb; cf[m] = (2. * ek * eb / (ek + eb)) * G.ar[e] / G.h[e]; hh[m] = G.h[e]; m++;
+        }
+        return m;
+    }
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny), j = rem / Nx, i = rem % Nx;
     int m = 0;
@@ -127,6 +139,8 @@ void api3_init(void) {                                      // semiconductor_3d.
     d.caxis = 1;
     const char *v = env_get("SEMISIM_VERBOSE"); d.verbose = v ? std::atoi(v) : 0;
     const char *a = env_get("SEMISIM_MGA"); if (a) g_knobs.mg_alpha = std::atof(a);
+    if (const char *m = env_get("SEMISIM_GPASS")) g_knobs.gpass = std::atoi(m);
+    if (const char *m = env_get("SEMISIM_GBETA")) g_knobs.gbeta = std::atof(m);
     if (const char *m = env_get("SEMISIM_AAM")) { int q = std::atoi(m); g_knobs.aa_depth = q < 0 ? 0 : (q > AA_MAX ? AA_MAX : q); }
     if (const char *m = env_get("SEMISIM_PRED")) g_knobs.pred_on = std::atoi(m) != 0;
     if (const char *m = env_get("SEMISIM_GROW")) { const double gg = std::atof(m); if (gg >= 1. && gg <= 4.) g_knobs.grow_slow = gg; }
@@ -225,6 +239,8 @@ int api3_set_grid_coords(int Nx, int Ny, int Nz, const double *xs, const double 
     if (Nx < 2 || Ny < 2 || Nz < 2) return 0;
     const size_t N = (size_t)Nx * Ny * Nz;
     if (N > 2000000000ULL) return 0;
+    d.unstr = 0;
+    d.ggh = GraphHost();
     d.Nx = Nx; d.Ny = Ny; d.Nz = Nz; d.N = N;
     d.xs.assign(xs, xs + Nx); d.ys.assign(ys, ys + Ny); d.zs.assign(zs, zs + Nz);
     d.Lx.resize(Nx); d.Ly.resize(Ny); d.Lz.resize(Nz);
@@ -317,12 +333,54 @@ int api3_set_gate_stack(int cid, int nl, const int *mat, const double *t) {
     mark_changed(d);
     return 1;
 }
-int api3_set_mesh_graph(int, int, const int *, const int *, const double *, const double *, const double *,
-                        const double *) {
-    std::fprintf(stderr, "semisim-b200: unstructured (prism) meshes are not supported by this solver library\n");
-    return 0;
+// a device on a general box-method mesh (semiconductor_3d.c:4788-4805, alloc_dev_graph
+// :981-1041): N nodes, E directed edges as a symmetric CSR graph, per edge its length and
+// dual face area, per node its control volume and position.  Nx = N, Ny = Nz = 1 with the
+// volume in Lx, so the node-wise parts of the solver apply unchanged.  Returns 0 for a bad
+// graph (not symmetric, self edges, non-positive lengths or volumes).
+int api3_set_mesh_graph(int N, int E, const int *rp, const int *cj, const double *h, const double *ar,
+                        const double *vol, const double *pos) {
+    Inst &d = g_dev;
+    if (N < 2 || E < 1 || !rp || !cj || !h || !ar || !vol || !pos || rp[0] != 0 || rp[N] != E) return 0;
+    for (int k = 0; k < N; k++) {
+        if (rp[k + 1] < rp[k] || !(vol[k] > 0.)) return 0;
+        for (int e = rp[k]; e < rp[k + 1]; e++)
+            if (cj[e] < 0 || cj[e] >= N || cj[e] == k || !(h[e] > 0.) || !(ar[e] >= 0.)) return 0;
+    }
+    GraphHost G;
+    G.rp.assign(rp, rp + N + 1); G.cj.assign(cj, cj + E);
+    G.h.assign(h, h + E); G.ar.assign(ar, ar + E);
+    G.vol.assign(vol, vol + N); G.pos.assign(pos, pos + 3 * (size_t)N);
+    G.rev.assign(E, -1); G.ue.assign(E, -1);
+    for (int k = 0; k < N; k++)
+        for (int e = rp[k]; e < rp[k + 1]; e++) {       // reverse entries and undirected ids
+            const int j = cj[e];
+            int r = -1;
+            for (int t = rp[j]; t < rp[j + 1]; t++) if (cj[t] == k) { r = t; break; }
+            if (r < 0) return 0;
+            G.rev[e] = r;
+            if (k < j) G.ue[e] = G.nue++;
+        }
+    for (int k = 0; k < N; k++)
+        for (int e = rp[k]; e < rp[k + 1]; e++) if (cj[e] < k) G.ue[e] = G.ue[G.rev[e]];
+    G.wall.assign(6 * (size_t)N, 1.);
+    d.unstr = 1;
+    d.ggh = std::move(G);
+    d.Nx = N; d.Ny = 1; d.Nz = 1; d.N = (size_t)N;
+    d.xs.assign(N, 0.); d.Lx.assign(vol, vol + N);
+    for (int k = 0; k < N; k++) d.xs[k] = pos[3 * k];
+    d.ys.assign(1, 0.); d.zs.assign(1, 0.); d.Ly.assign(1, 1.); d.Lz.assign(1, 1.);
+    d.mat_idx.assign(N, 0);
+    d.Nd.assign(N, 0.0); d.Na.assign(N, 0.0); d.Nf.assign(N, 0.0);
+    d.flags.assign(N, 0);
+    d.allocated = 1; d.have_solution = 0; d.dirty = 1;
+    d.aa_m = AA_MAX;
+    invalidate(d);
+    // the continuity solves of a general mesh stop at 1e-6 unless SEMISIM_BRTOL says otherwise
+    if (!env_get("SEMISIM_BRTOL")) d.bicg_rtol = 1e-6;
+    return 1;
 }
-int api3_is_graph(void) { return 0; }
+int api3_is_graph(void) { return g_dev.unstr; }
 void api3_set_node_data(const int *mat, const double *Nd, const double *Na, const double *Nf) {
     Inst &d = g_dev;
     if (!d.allocated) return;
@@ -348,7 +406,15 @@ int api3_set_con_nodes(int cid, int n, const int *nodes, const double *areas) {
     mark_changed(d);
     return 1;
 }
-void api3_set_walls(const double *) {}                     // graph meshes only
+// the interface walls of a graph device: per node two walls, each the node's distance to it
+// and the range a..b of its cell measured from it; a distance >= 0.5 m is no wall
+// (semiconductor_3d.c:4835-4841)
+void api3_set_walls(const double *w) {
+    Inst &d = g_dev;
+    if (!d.allocated || !d.unstr || !w) return;
+    d.ggh.wall.assign(w, w + 6 * d.N);
+    mark_changed(d);
+}
 int api3_get_ntp(int cid) {                                  // semiconductor_3d.c:4844-4847
     Inst &d = g_dev;
     if (cid < 0) {
@@ -577,7 +643,7 @@ int api3_charge_partition(const int *cterm) {
         if (t >= 0 && d.cons[c].bc == 0 && !d.cons[c].te && (kind_of(d, k) == K_SEMI || kind_of(d, k) == K_METAL))
             qu.push_back(k);
     }
-    size_t nb[6]; double cf[6], hh[6];
+    size_t nb[64]; double cf[64], hh[64];
     while (qh < qu.size()) {
         const size_t k = qu[qh++];
         const int t = g_qown[k];
@@ -645,6 +711,7 @@ int api3_terminal_charges(int nt, double *Qt) {             // semiconductor_3d.
 int api3_face_J(int ax, int carrier, double *out) {
     Inst &d = g_dev;
     if (!d.allocated || !d.have_solution || !out || ax < 0 || ax > 2 || !d.g.ready) return 0;
+    if (d.unstr) return 0;                          // faces of a graph mesh have no axis (as the reference)
     launch_face_J(make_ctx(d), ax, carrier, d.g.scratch);
     cudaMemcpyAsync(out, d.g.scratch, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
     cudaStreamSynchronize(d.g.st);
@@ -665,7 +732,8 @@ double api3_ins_field_max(double *pos) {                    // semiconductor_3d.
     if (pos && kb >= 0) {
         const size_t k = (size_t)kb;
         const int l = int(k / ((size_t)d.Nx * d.Ny)), rem = int(k - (size_t)l * d.Nx * d.Ny);
-        pos[0] = d.xs[rem % d.Nx]; pos[1] = d.ys[rem / d.Nx]; pos[2] = d.zs[l];
+        if (d.unstr) { pos[0] = d.ggh.pos[3 * k]; pos[1] = d.ggh.pos[3 * k + 1]; pos[2] = d.ggh.pos[3 * k + 2]; }
+        else { pos[0] = d.xs[rem % d.Nx]; pos[1] = d.ys[rem / d.Nx]; pos[2] = d.zs[l]; }
     }
     return best;
 }

@@ -51,6 +51,8 @@ void launch_mob_display(const Ctx &c);
 void launch_node_val(const Ctx &c, int which, double *out);
 void launch_ion_neutral(const Ctx &c);
 void launch_ii_update(const Ctx &c);
+void launch_region_seed(const Ctx &c, int c1, int *mark);
+void launch_region_shift(const Ctx &c, int c1, double dV, const int *mark);
 void launch_face_J(const Ctx &c, int ax, int carrier, double *out);
 void launch_extrap(const Ctx &c, double r, int s1, int s2);     // history selectors 0 h1, 1 h2, 2 e2
 void launch_region_mark(const Ctx &c, int con1, int type, double dV, int *mark, int *changed);

@@ -159,6 +159,7 @@ int float_fix(Inst &d, int hole) {
     SS_LAUNCH(PF_CCL, d.N, k_ff_init, g, TPB, c.st, c.dP, hole);
     int h = 1, cycles = 0;
     const int maxcyc = d.Nx + d.Ny + d.Nz + 8;
+    if (d.unstr) { ff_label_g(d, changed); h = 0; }           // labels over the graph's edges, anchors
     while (h && cycles < maxcyc) {
         cudaMemsetAsync(changed, 0, sizeof(int), c.st);
         for (int ax = 0; ax < 3; ax++) {
@@ -170,7 +171,7 @@ int float_fix(Inst &d, int hole) {
         cudaStreamSynchronize(c.st);
         cycles++;
     }
-    SS_LAUNCH(PF_CCL, d.N, k_ff_anchor, g, TPB, c.st, c.dP);
+    if (!d.unstr) SS_LAUNCH(PF_CCL, d.N, k_ff_anchor, g, TPB, c.st, c.dP);
     cudaMemsetAsync(count, 0, sizeof(int), c.st);
     SS_LAUNCH(PF_CCL, d.N, k_ff_roots, g, TPB, c.st, c.dP, count, roots);
     int nb = 0;
@@ -181,7 +182,8 @@ int float_fix(Inst &d, int hole) {
     double *Aout = g_ffbuf, *Bin = g_ffbuf + FF_MAX_BLOCKS, *lam = g_ffbuf + 2 * FF_MAX_BLOCKS;
     double *G = g_ffbuf + 3 * FF_MAX_BLOCKS, *dG = g_ffbuf + 4 * FF_MAX_BLOCKS;
     cudaMemsetAsync(Aout, 0, sizeof(double) * 2 * FF_MAX_BLOCKS, c.st);
-    SS_LAUNCH(PF_CCL, d.N, k_ff_boundary, g, TPB, c.st, c.dP, hole, Aout, Bin);
+    if (d.unstr) ff_boundary_g(d, hole, Aout, Bin);
+    else SS_LAUNCH(PF_CCL, d.N, k_ff_boundary, g, TPB, c.st, c.dP, hole, Aout, Bin);
     std::vector<double> hA(nb), hB(nb), sl(nb, 0.0), hl(nb), hG(nb), hdG(nb);
     std::vector<int> act(nb, 1);
     cudaMemcpyAsync(hA.data(), Aout, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.st);

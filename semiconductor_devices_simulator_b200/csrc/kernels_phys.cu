@@ -850,6 +850,13 @@ __global__ void k_region_shift(const DevP *__restrict__ Ps, int c1, double dV, c
         P.phi[k] += dV; P.phin[k] += dV; P.phip[k] += dV;
     }
 }
+// the seed and the shift of a region, for the graph-mesh growth between them
+void launch_region_seed(const Ctx &c, int c1, int *mark) {
+    SS_LAUNCH(PF_CCL, c.maxN, k_region_seed, grid_of(c), TPB, c.st, c.dP, c1, mark);
+}
+void launch_region_shift(const Ctx &c, int c1, double dV, const int *mark) {
+    SS_LAUNCH(PF_CCL, c.maxN, k_region_shift, grid_of(c), TPB, c.st, c.dP, c1, dV, mark);
+}
 void launch_region_mark(const Ctx &c, int c1, int type, double dV, int *mark, int *changed) {
     SS_LAUNCH(PF_CCL, c.maxN, k_region_seed, grid_of(c), TPB, c.st, c.dP, c1, mark);
     int h_changed = 1, cycles = 0;

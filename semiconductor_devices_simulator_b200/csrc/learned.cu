@@ -501,7 +501,7 @@ static void mlp_attrs() {
 }
 
 // ------------------------------------------------------------------ solver side
-int seed_available(const Inst &d) { return d.seed_on && d.g.seedw != nullptr; }
+int seed_available(const Inst &d) { return d.seed_on && d.g.seedw != nullptr && !d.unstr; }
 
 // x = x1 + s (x1 - x0) + VT * MLP for the sweep predictor step (h1 = x1, e2 = x0): the
 // features into the instance's feature buffer, then the network and the seed write

@@ -22,6 +22,20 @@ __device__ __forceinline__ bool edge(const DevP &P, int k, const Node &a, int di
     return true;
 }
 
+// the same for either mesh: neighbour idx of node k (the six directions of the tensor grid,
+// or the ELL slots of a graph in CSR order), with its coupling and spacing
+__device__ __forceinline__ int nslots(const DevP &P) { return P.gD ? P.gD : 6; }
+__device__ __forceinline__ bool edge_any(const DevP &P, int k, const Node &a, int idx, int &kb, double &cf, double &h) {
+    if (!P.gD) return edge(P, k, a, idx, kb, cf, h);
+    const size_t e = (size_t)idx * P.N + k;
+    kb = P.gcol[e];
+    if (kb < 0) return false;
+    h = P.gh[e];
+    const double ek = P.mats[fl_mat(P.flags[k])].eps, eb = P.mats[fl_mat(P.flags[kb])].eps;
+    cf = (2.0 * ek * eb / (ek + eb)) * P.ga[e] / h;
+    return true;
+}
+
 // Grid-wide arg-max of (v, idx): the largest v, the smallest idx among equal v (what a
 // sequential scan in idx order with a strict comparison keeps).  idx < 2^53, so it travels
 // exactly through the double partials; NO_IDX marks an empty candidate.  Thread 0 of the
@@ -141,15 +155,16 @@ __global__ void k_out_insfield(const DevP *__restrict__ Ps, int mode) {
         if (mode == 0) {
             if (fl_kind(fk) == K_SEMI) continue;
             const Node a = unidx(k, P.Nx, P.Ny);
-            for (int dir = 0; dir < 6; dir++) {
+            const int ns = nslots(P);
+            for (int dir = 0; dir < ns; dir++) {
                 int b;
-                double h, ar;
-                if (!nbr(P, a, k, dir, b, h, ar) || b < k) continue;
+                double h, cf;
+                if (!edge_any(P, k, a, dir, b, cf, h) || b < k) continue;
                 const int kb = fl_kind(P.flags[b]);
                 if (kb == K_SEMI) continue;
                 if (fl_kind(fk) != K_INS && kb != K_INS) continue;
                 const double F = fabs(P.phi[b] - P.phi[k]) / h;
-                if (F > best) { best = F; key = 6LL * k + dir; }   // this thread's scan order
+                if (F > best) { best = F; key = (long long)ns * k + dir; }   // this thread's scan order
             }
         } else {
             if (P.robA[k] == 0.0) continue;
@@ -166,11 +181,12 @@ __global__ void k_out_insfield(const DevP *__restrict__ Ps, int mode) {
         long long at = -1;
         if (key != NO_IDX) {
             if (mode == 0) {
-                const int k = int(key / 6), dir = int(key - 6LL * (key / 6));
+                const int ns = nslots(P);
+                const int k = int(key / ns), dir = int(key - (long long)ns * (key / ns));
                 const Node a = unidx(k, P.Nx, P.Ny);
-                int b;
-                double h, ar;
-                nbr(P, a, k, dir, b, h, ar);
+                int b = k;
+                double h, cf;
+                edge_any(P, k, a, dir, b, cf, h);
                 at = fl_kind(P.flags[k]) == K_INS ? k : b;
             } else {
                 at = key;
@@ -203,10 +219,11 @@ __global__ void __launch_bounds__(OUT_TPB) k_out_qterm(const DevP *__restrict__ 
         const int t = owner[k];
         if (t >= 0 && t < nt) {
             const Node a = unidx(k, P.Nx, P.Ny);
-            for (int dir = 0; dir < 6; dir++) {
+            const int ns = nslots(P);
+            for (int dir = 0; dir < ns; dir++) {
                 int b;
                 double cf, h;
-                if (!edge(P, k, a, dir, b, cf, h)) continue;
+                if (!edge_any(P, k, a, dir, b, cf, h)) continue;
                 const int tb = owner[b];
                 if (tb == t) continue;
                 const double f = cf * (P.phi[k] - P.phi[b]);
@@ -265,7 +282,8 @@ static void read(Inst &d, int slot, int n, double *v) {
 
 double out_emax(Inst &d) {
     Ctx c = make_ctx(d);
-    SS_LAUNCH(PF_DISPLAY, d.N, k_out_emax, dim3(out_blocks(d), 1), OUT_TPB, c.st, c.dP);
+    if (d.unstr) launch_emax_g(c);                  // least-squares gradients of a graph mesh
+    else SS_LAUNCH(PF_DISPLAY, d.N, k_out_emax, dim3(out_blocks(d), 1), OUT_TPB, c.st, c.dP);
     double v;
     read(d, R_OUT, 1, &v);
     return std::sqrt(v);

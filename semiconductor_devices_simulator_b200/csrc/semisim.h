@@ -81,6 +81,20 @@ struct KrylovS {
     int half, pad0, maxit, body_runs;
 };
 
+// one level of the aggregation multigrid of a general (graph) mesh: the level's matrix in
+// ELL (slot s of node k at s*N + k; the diagonal apart), its D-ILU(0) pivot reciprocals in
+// a multicolour order, and towards the next level the aggregate of every node, the member
+// lists of the aggregates and, per ELL entry, the coarse ELL entry it sums into (-1 inside
+// an aggregate)
+struct GLev {
+    int N, D;
+    const int *col, *rev, *color;
+    double *val, *diag, *dil;
+    const int *agg, *mrp, *mem, *emap;   // null at the coarsest level
+    double *pw, *ph, *x, *b, *r;
+    double *inv;                         // coarsest level: dense inverse (N x N), or null (ILU sweeps)
+};
+
 // everything a kernel needs about one instance
 struct DevP {
     int Nx, Ny, Nz, N;
@@ -110,6 +124,15 @@ struct DevP {
     const double *if_A, *if_Qf;
     double *if_NC;
     int n_if, pad_if;
+    // general (graph) mesh, null on a tensor mesh: ELL layout with gD slots per node, slot s
+    // of node k at s*N + k - neighbour (-1 past the degree), undirected edge id, slot of the
+    // reverse edge, edge length, dual face area, matrix off-diagonal; node positions (3 per
+    // node), least-squares gradient matrices (6 per node), colours of the D-ILU order and
+    // its reciprocal pivots; edge mobilities per undirected edge
+    int gD, nUE;
+    const int *gcol, *gue, *grev;
+    const double *gh, *ga, *gpos, *glsq;
+    double *gval, *gmu_n, *gmu_p, *gdil;
     const float *te_vw;
     const signed char *te_ax;
     const MatD *mats;

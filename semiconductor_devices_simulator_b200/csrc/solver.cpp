@@ -3,6 +3,7 @@
 // the floating-block balance, the Gummel loop with Anderson mixing and the adaptive
 // continuation with the sweep predictor.  The control logic follows the reference
 // routine named beside each function; all O(N) work runs in the CUDA kernels.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -213,6 +214,8 @@ void gpu_free(Inst &d) {
     if (d.g.tunblock) cudaFree(d.g.tunblock);
     if (d.g.trblock) cudaFree(d.g.trblock);
     if (d.g.coblock) cudaFree(d.g.coblock);
+    if (d.g.gblock) cudaFree(d.g.gblock);
+    if (d.g.gmgblock) cudaFree(d.g.gmgblock);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();
@@ -293,7 +296,8 @@ template <class F>
 static void for_con_nodes(const Inst &d, const Contact &cn, F body) {
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int cid = int(&cn - d.cons);
-    if (cid >= 0 && cid < NC_MAX && !d.cnodes[cid].empty()) {
+    if (d.unstr || (cid >= 0 && cid < NC_MAX && !d.cnodes[cid].empty())) {   // node lists (graph: only those)
+        if (cid < 0 || cid >= NC_MAX) return;
         for (size_t q = 0; q < d.cnodes[cid].size(); q++) {
             const size_t k = (size_t)d.cnodes[cid][q];
             const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny);
@@ -452,6 +456,114 @@ static void wall_distance(const Inst &d, const std::vector<unsigned char> &kind,
         if (qcn[k] < -60.) qcn[k] = -60.;
         if (qcp[k] < -60.) qcp[k] = -60.;
     }
+}
+
+// interface distance and MLDA corrections of a graph device from the walls the host gave
+// (two per node: the node's distance, the range a..b of its cell; distance >= 0.5 m: none)
+// (walls_graph, semiconductor_3d.c:1252-1271)
+static void walls_graph(const Inst &d, const std::vector<unsigned char> &kind, std::vector<double> &qd, bool qc,
+                        std::vector<double> &qcn, std::vector<double> &qcp) {
+    const size_t N = d.N;
+    qd.assign(N, 1.0);
+    qcn.assign(qc ? N : 0, 0.0);
+    qcp.assign(qc ? N : 0, 0.0);
+    for (size_t k = 0; k < N; k++) {
+        if (kind[k] != K_SEMI) continue;
+        const Material &m = d.mats[d.mat_idx[k]];
+        for (int w = 0; w < 2; w++) {
+            const double *g = d.ggh.wall.data() + 6 * k + 3 * w;
+            if (!(g[0] < 0.5)) continue;
+            if (g[0] < qd[k]) qd[k] = g[0];
+            if (qc && g[1] < 40e-9) {
+                qcn[k] += std::log(std::fmax(mlda_factor_host(m, g[1], g[2], 0), 1e-30));
+                qcp[k] += std::log(std::fmax(mlda_factor_host(m, g[1], g[2], 1), 1e-30));
+            }
+        }
+        if (qc) {
+            if (qcn[k] < -60.) qcn[k] = -60.;
+            if (qcp[k] < -60.) qcp[k] = -60.;
+        }
+    }
+}
+
+// device arrays of a graph device: the CSR graph packed as ELL (gD slots per node, slot s of
+// node k at s*N + k), the least-squares gradient matrices of the semiconductor nodes (g_lsq_setup,
+// semiconductor_3d.c:2682-2700), room for the edge mobilities, matrix off-diagonals and
+// pivots, and the aggregation multigrid hierarchy
+static int graph_upload(Inst &d, const std::vector<unsigned char> &kind, DevP &P, cudaStream_t st) {
+    if (d.g.gblock) { cudaFree(d.g.gblock); d.g.gblock = nullptr; }
+    gmg_free(d);
+    P.gD = 0; P.nUE = 0;
+    P.gcol = P.gue = P.grev = nullptr;
+    P.gh = P.ga = P.gpos = P.glsq = nullptr;
+    P.gval = P.gmu_n = P.gmu_p = P.gdil = nullptr;
+    if (!d.unstr) return 1;
+    GraphHost &G = d.ggh;
+    const int N = (int)d.N;
+    int D = 0;
+    for (int k = 0; k < N; k++) D = std::max(D, G.rp[k + 1] - G.rp[k]);
+    G.D = D;
+    std::vector<int> col((size_t)D * N, -1), ue((size_t)D * N, 0), rv((size_t)D * N, 0), slot(G.cj.size());
+    std::vector<double> h((size_t)D * N, 1.0), ar((size_t)D * N, 0.0);
+    for (int k = 0; k < N; k++)
+        for (int e = G.rp[k]; e < G.rp[k + 1]; e++) slot[e] = e - G.rp[k];
+    for (int k = 0; k < N; k++)
+        for (int e = G.rp[k]; e < G.rp[k + 1]; e++) {
+            const size_t q = (size_t)slot[e] * N + k;
+            col[q] = G.cj[e]; ue[q] = G.ue[e]; rv[q] = slot[G.rev[e]]; h[q] = G.h[e]; ar[q] = G.ar[e];
+        }
+    std::vector<double> lsq(6 * (size_t)N, 0.0);
+    for (int k = 0; k < N; k++) {
+        double m[6] = {0, 0, 0, 0, 0, 0};
+        double *o = lsq.data() + 6 * (size_t)k;
+        if (kind[k] == K_SEMI)
+            for (int e = G.rp[k]; e < G.rp[k + 1]; e++) {
+                const int b = G.cj[e];
+                if (kind[b] != K_SEMI) continue;
+                const double dx = G.pos[3 * b] - G.pos[3 * k], dy = G.pos[3 * b + 1] - G.pos[3 * k + 1],
+                             dz = G.pos[3 * b + 2] - G.pos[3 * k + 2];
+                const double w = 1. / (dx * dx + dy * dy + dz * dz + 1e-40);
+                m[0] += w * dx * dx; m[1] += w * dx * dy; m[2] += w * dx * dz;
+                m[3] += w * dy * dy; m[4] += w * dy * dz; m[5] += w * dz * dz;
+            }
+        const double tr = m[0] + m[3] + m[5], eps = 1e-6 * tr + 1e-30;
+        m[0] += eps; m[3] += eps; m[5] += eps;
+        const double a = m[0], b = m[1], c = m[2], dd = m[3], e = m[4], f = m[5];
+        const double A = dd * f - e * e, B = -(b * f - c * e), Cc = b * e - c * dd, Dq = a * f - c * c,
+                     E = -(a * e - b * c), F = a * dd - b * b;
+        const double det = a * A + b * B + Cc * c;
+        if (!(std::fabs(det) > 0.)) continue;
+        o[0] = A / det; o[1] = B / det; o[2] = Cc / det; o[3] = Dq / det; o[4] = E / det; o[5] = F / det;
+    }
+    const size_t DN = (size_t)D * N, nue = G.nue > 0 ? (size_t)G.nue : 1;
+    size_t off = 0;
+    auto room = [&](size_t bytes) { const size_t x = off; off += align_up(bytes > 0 ? bytes : 1); return x; };
+    const size_t o_col = room(DN * 4), o_ue = room(DN * 4), o_rv = room(DN * 4), o_h = room(DN * 8), o_ar = room(DN * 8),
+                 o_val = room(DN * 8),
+                 o_pos = room(3 * (size_t)N * 8), o_lsq = room(6 * (size_t)N * 8), o_mun = room(nue * 8),
+                 o_mup = room(nue * 8), o_dil = room((size_t)N * 8);
+    char *b = nullptr;
+    if (cudaMalloc(&b, off) != cudaSuccess) {
+        std::fprintf(stderr, "semisim-b200: out of device memory for the mesh graph\n");
+        return 0;
+    }
+    d.g.gblock = b;
+    bool ok = cudaMemsetAsync(b, 0, off, st) == cudaSuccess;
+    auto up = [&](size_t x, const void *src, size_t bytes) {
+        if (bytes && cudaMemcpyAsync(b + x, src, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) ok = false;
+    };
+    up(o_col, col.data(), DN * 4); up(o_ue, ue.data(), DN * 4); up(o_rv, rv.data(), DN * 4);
+    up(o_h, h.data(), DN * 8); up(o_ar, ar.data(), DN * 8);
+    up(o_pos, G.pos.data(), 3 * (size_t)N * 8);
+    up(o_lsq, lsq.data(), 6 * (size_t)N * 8);
+    P.gD = D; P.nUE = G.nue;
+    P.gcol = (const int *)(b + o_col); P.gue = (const int *)(b + o_ue); P.grev = (const int *)(b + o_rv);
+    P.gh = (const double *)(b + o_h); P.ga = (const double *)(b + o_ar); P.gpos = (const double *)(b + o_pos);
+    P.glsq = (const double *)(b + o_lsq);
+    P.gval = (double *)(b + o_val); P.gmu_n = (double *)(b + o_mun); P.gmu_p = (double *)(b + o_mup);
+    P.gdil = (double *)(b + o_dil);
+    if (cudaStreamSynchronize(st) != cudaSuccess) ok = false;
+    return ok && gmg_build(d, st) ? 1 : 0;
 }
 
 // Thermionic-emission metal contacts (semiconductor_3d.c:1376-1416, 1723-1768): one entry
@@ -1026,6 +1138,18 @@ int prepare(Inst &d) {
         Contact &cn = d.cons[c];
         if (cn.face <= 5) continue;
         double A = 0.;
+        if (d.unstr) {
+            const GraphHost &G = d.ggh;
+            for_con_nodes(d, cn, [&](int, int, int, size_t k, double) {
+                if (con[k] != c + 1) return;
+                for (int e = G.rp[k]; e < G.rp[k + 1]; e++) {
+                    const int kb = G.cj[e];
+                    if (kind[kb] == K_SEMI && con[kb] != c + 1) A += G.ar[e];
+                }
+            });
+            cn.A = A;
+            continue;
+        }
         for_con_nodes(d, cn, [&](int i, int j, int l, size_t k, double) {
             if (con[k] != c + 1) return;
             const int Nx = d.Nx, Ny = d.Ny;
@@ -1059,7 +1183,22 @@ int prepare(Inst &d) {
     }
     std::vector<double> qd, qcn0, qcp0;
     const bool qc_on = (d.models & 8) != 0;
-    wall_distance(d, kind, gate, qd, qc_on, qcn0, qcp0);
+    if (d.unstr) {
+        // models that touch neighbours through the tensor geometry have no graph variant here
+        const char *why = nullptr;
+        if (d.models & 16) why = "surface mobility (models bit 4)";
+        if (d.models & 32) why = "gate tunnelling (models bit 5)";
+        if (d.models & 256) why = "impact ionisation (models bit 8)";
+        for (int c = 0; c < d.n_cons; c++)
+            if ((d.models & 64) && d.cons[c].bc == 1 && d.cons[c].face <= 5) why = "metal contacts (models bit 6)";
+        if (why) {
+            std::fprintf(stderr, "semisim-b200: %s on a general (prism) mesh is not supported by this solver library\n", why);
+            return 0;
+        }
+        walls_graph(d, kind, qd, qc_on, qcn0, qcp0);
+    } else {
+        wall_distance(d, kind, gate, qd, qc_on, qcn0, qcp0);
+    }
     // incomplete ionisation (semiconductor_3d.c:1472-1510): per node the constants
     // N_c/g_D e^(-dE_s/kT) of the two donor sites and N_v/g_A e^(-dE_A/kT), the level depths
     // falling with the node's own dopant density; the neutral majority density (slot 3)
@@ -1089,9 +1228,15 @@ int prepare(Inst &d) {
         }
     }
     TeHost teh;
-    te_build(d, kind, con, teh);
     TunHost tuh;
-    tun_build(d, kind, con, rob_k, rob_A, rob_c, tuh);
+    if (!d.unstr) {
+        te_build(d, kind, con, teh);
+        tun_build(d, kind, con, rob_k, rob_A, rob_c, tuh);
+    } else {
+        teh.vw.assign(N, 1.f); teh.ax.assign(N, 0);
+        for (int c = 0; c < NC_MAX; c++) teh.ce0[c] = teh.ce1[c] = 0;
+        for (int c = 0; c < d.n_cons; c++) d.cons[c].ntp = 0;
+    }
     ScHost sch;
     sc_build(N, tuh, teh.tc_k, sch);
     if (!gpu_alloc(d)) return 0;
@@ -1117,6 +1262,7 @@ int prepare(Inst &d) {
     if (!tun_upload(d, tuh, sch, d.g.st)) return 0;
     if (!traps_upload(d, kind, P, d.g.st)) return 0;
     if (!coul_upload(d, kind, con, gate, rob_k, rob_A, rob_c, P, d.g.st)) return 0;
+    if (!graph_upload(d, kind, P, d.g.st)) return 0;
     // continuity sink / source of the exchange with gate and metal contacts (zero elsewhere)
     P.tk = P.tg = nullptr;
     if (d.g.te_on || d.g.tun_on) {
@@ -1215,12 +1361,16 @@ void clamp_qf(Inst &d) {
     launch_clamp_qf(make_ctx(d), d.vlo - g_knobs.qf_margin, d.vhi + g_knobs.qf_margin);
 }
 void rebuild_np(Inst &d) { launch_rebuild_np(make_ctx(d)); }
-void upd_mob(Inst &d) { launch_upd_mob(make_ctx(d)); }
+void upd_mob(Inst &d) {
+    if (d.unstr) launch_upd_mob_g(make_ctx(d));
+    else launch_upd_mob(make_ctx(d));
+}
 
 void terminal_currents(Inst &d, double *I, double *S) {
     Ctx c = make_ctx(d);
     const int nc = d.n_cons;
-    launch_currents(c);
+    if (d.unstr) launch_currents_g(c);
+    else launch_currents(c);
     tun_currents(d);
     te_currents(d);
     cudaMemcpyAsync(d.g.pin, d.g.h.res, sizeof(double) * R_TOTAL, cudaMemcpyDeviceToHost, d.g.st);
@@ -1250,12 +1400,14 @@ static int poisson_newton(Inst &d, const double *Va, double ntol, int maxit) {
     upload_voltages(d, Va);
     for (int it = 0; it < maxit; it++) {
         d.newton_its++;
-        launch_poisson(c, nullptr, 1, nullptr);
+        if (d.unstr) launch_poisson_g(c, nullptr, 1);
+        else launch_poisson(c, nullptr, 1, nullptr);
         const double f0 = read_res(d, R_PNORM);
         if (!(f0 > 0.)) return f0 == 0.;
         launch_fill_sel(c, V_SOL, 0.0);
-        const int its = pcg_solve(c, d.g.mg, d.max_iter_p > 0 ? d.max_iter_p : 2000, d.pcg_rtol, g_knobs.check_every,
-                                  use_mixed(d));
+        const int maxp = d.max_iter_p > 0 ? d.max_iter_p : 2000;
+        const int its = d.unstr ? pcg_graph(d, maxp, d.pcg_rtol)
+                                : pcg_solve(c, d.g.mg, maxp, d.pcg_rtol, g_knobs.check_every, use_mixed(d));
         d.pcg_its += its;
         launch_absmax_sel(c, V_SOL, R_DMAX);
         const double dm = read_res(d, R_DMAX);
@@ -1267,7 +1419,8 @@ static int poisson_newton(Inst &d, const double *Va, double ntol, int maxit) {
         double lam = 1.;
         for (int ls = 0; ls < 40; ls++) {
             launch_axpy_sel(c, V_TR, V_PHI, lam, V_SOL);    // trial psi + lam dx
-            launch_poisson(c, d.g.h.tr, 0, nullptr);
+            if (d.unstr) launch_poisson_g(c, d.g.h.tr, 0);
+            else launch_poisson(c, d.g.h.tr, 0, nullptr);
             const double f1 = read_res(d, R_PNORM);
             if (f1 <= (1. - 1e-4 * lam) * f0) break;
             lam *= 0.5;
@@ -1288,21 +1441,25 @@ int float_fix(Inst &d, int hole);   // kernels_ccl.cu
 static int solve_cont(Inst &d, int hole, double lo, double hi, double *dmax) {
     Ctx c = make_ctx(d);
     exchange_scatter(d, hole);                           // gate / metal-contact sink and source of this carrier
-    launch_cont_assemble(c, hole);
+    if (d.unstr) launch_cont_assemble_g(c, hole);
+    else launch_cont_assemble(c, hole);
     launch_fill_sel(c, V_SOL, 1.0);
     const double atol = g_knobs.cont_atol * d.cont_atol_f;
     const int maxit = d.max_iter_c > 0 ? d.max_iter_c : 1000;
     launch_copy_sel(c, 7, V_SOL);                        // x0 backup
     double rn = 0, r0 = 0;
     const long long s0 = t_ir_steps, f0 = t_ir_fallbacks;
-    int its = bicgstab_core(c, d.g.mg, maxit, d.bicg_rtol, atol, 1, g_knobs.check_every, &rn, &r0, hole ? -1 : 1,
-                            use_mixed(d));
+    int its = d.unstr ? bicg_graph(d, maxit, d.bicg_rtol, atol, &rn, &r0, hole ? -1 : 1, false)
+                      : bicgstab_core(c, d.g.mg, maxit, d.bicg_rtol, atol, 1, g_knobs.check_every, &rn, &r0,
+                                      hole ? -1 : 1, use_mixed(d));
     d.ir_steps += t_ir_steps - s0;
     d.ir_fallbacks += t_ir_fallbacks - f0;
-    if (!(rn <= std::fmax(r0, 1e-300)) && d.g.mg.maxlev > 1) {
+    if (!(rn <= std::fmax(r0, 1e-300)) && (d.unstr ? gmg_levels(d) > 1 : d.g.mg.maxlev > 1)) {
         if (d.verbose) std::fprintf(stderr, "semisim-b200: MG-BiCGSTAB diverged (%.2e > %.2e), retry ILU\n", rn, r0);
         launch_copy_sel(c, V_SOL, 7);
-        its += bicgstab_core(c, d.g.mg, 4 * maxit, d.bicg_rtol, atol, 0, g_knobs.check_every, &rn, &r0, hole ? -1 : 1);
+        its += d.unstr ? bicg_graph(d, 4 * maxit, d.bicg_rtol, atol, &rn, &r0, hole ? -1 : 1, true)
+                       : bicgstab_core(c, d.g.mg, 4 * maxit, d.bicg_rtol, atol, 0, g_knobs.check_every, &rn, &r0,
+                                       hole ? -1 : 1);
     }
     d.bicg_its += its;
     if (!(rn <= std::fmax(r0, 1e-300)) || !std::isfinite(rn)) {
@@ -1499,7 +1656,8 @@ static void region_shift(Inst &d, const double *dV) {      // semiconductor_3d.c
             }
         }
         if (!type) continue;
-        launch_region_mark(c, q + 1, type, dV[q], mark, d.g.flag);
+        if (d.unstr) launch_region_mark_g(d, q + 1, type, dV[q], mark, d.g.flag);
+        else launch_region_mark(c, q + 1, type, dV[q], mark, d.g.flag);
     }
 }
 
@@ -1690,8 +1848,13 @@ int run_continuation(Inst &d) {
 
 void finish_point(Inst &d) {
     Ctx c = make_ctx(d);
-    launch_upd_J(c);
-    launch_mob_display(c);
+    if (d.unstr) {
+        launch_upd_J_g(c);
+        launch_mob_display_g(c);
+    } else {
+        launch_upd_J(c);
+        launch_mob_display(c);
+    }
     // the display update leaves the sink / source arrays holding the gate-tunnelling current
     // density at the interface nodes (A/m^2), as upd_J does (semiconductor_3d.c:3648-3657)
     if (d.g.h.tk) {

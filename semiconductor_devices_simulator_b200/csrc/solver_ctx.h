@@ -33,6 +33,23 @@ struct Contact {
     int te = 0;                  // thermionic-emission metal contact (set by prepare)
 };
 
+// a device on a general box-method mesh (api3_set_mesh_graph): the symmetric CSR graph with
+// per directed edge its length and dual face area, per node its volume, position and walls
+// (api3_set_walls), and the derived reverse entries, undirected edge ids and colouring
+struct GraphHost {
+    std::vector<int> rp, cj, rev, ue;
+    std::vector<double> h, ar, vol, pos, wall;
+    int nue = 0, D = 0;
+};
+
+// a level of the graph multigrid on the host: the device view and its colour classes
+struct GLevHost {
+    GLev dv{};
+    int ncolor = 0;
+    std::vector<int> cptr;       // colour q: cnodes[cptr[q] .. cptr[q+1])
+    int *cnodes = nullptr;       // device
+};
+
 struct Gpu {
     bool ready = false;
     int dev = 0;
@@ -52,6 +69,9 @@ struct Gpu {
     double *gii = nullptr;       // impact-ionisation generation (N), with models bit 8
     double *qc = nullptr;        // band corrections qcn, qcp (2 N), with MLDA or metal contacts
     double *xchg = nullptr;      // continuity sink / source tk, tg (2 N), with gate tunnelling or metal contacts
+    void *gblock = nullptr;      // graph-mesh arrays (ELL edges, colours, gradients, edge mobilities)
+    void *gmgblock = nullptr;    // graph multigrid levels (one allocation)
+    std::vector<GLevHost> glev;  // graph multigrid hierarchy, level 0 = the mesh
     void *trblock = nullptr;     // deep-level trap entries (CSR per node) and species
     void *coblock = nullptr;     // Coulomb interface entries and every node's nearest one
     void *teblock = nullptr;     // metal-contact entries, columns and per-node arrays (one allocation)
@@ -109,6 +129,8 @@ struct Inst {
     std::vector<int> trq_k, trq_s;        // trap requests (api3_trap_add): node, species, density
     std::vector<double> trq_N;
     int n_tr = 0;                         // compiled trap entries of the last prepare
+    int unstr = 0;                        // a general (graph) mesh instead of the tensor grid
+    GraphHost ggh;
     double Cref = 0;
     int ref_mat = 0;
     double Ve1[NC_MAX] = {0}, Ve2[NC_MAX] = {0};
@@ -142,6 +164,8 @@ struct Inst {
 // global knobs (the reference's static tunables, read by api3_init)
 struct Knobs {
     double mg_alpha = 1.0;
+    int gpass = 3;               // graph multigrid: rounds of pairwise matching per level
+    double gbeta = 0.5;          //   and the strength threshold of a match
     int aa_depth = AA_MAX;
     int pred_on = 1;
     double grow_slow = 2.2;
@@ -175,6 +199,27 @@ int use_mixed(const Inst &d);
 int seed_available(const Inst &d);                       // learned.cu
 void launch_mlp_seed(Inst &d, double s, const double *dv);
 extern int g_precision_default;                          // precision of new instances (1 = refined FP32)
+// general (graph) meshes (graph.cu)
+void launch_poisson_g(const Ctx &c, const double *phi_sel, int build);
+void launch_upd_mob_g(const Ctx &c);
+void launch_cont_assemble_g(const Ctx &c, int hole);
+void launch_currents_g(const Ctx &c);
+void launch_upd_J_g(const Ctx &c);
+void launch_mob_display_g(const Ctx &c);
+void launch_node_Jc_g(const Ctx &c, int which, double *out);
+void launch_emax_g(const Ctx &c);
+int pcg_graph(Inst &d, int maxit, double rtol);
+int bicg_graph(Inst &d, int maxit, double rtol, double atol, double *rn, double *r0, int qsign, bool ilu_only);
+// aggregation multigrid of a graph mesh (graph_mg.cu)
+int gmg_build(Inst &d, cudaStream_t st);
+void gmg_free(Inst &d);
+void gmg_setup(Inst &d, const Ctx &c, int qsign, const double *w);
+void gmg_apply(Inst &d, const Ctx &c, const double *r, double *z, const double *w, bool ilu_only);
+int gmg_levels(const Inst &d);
+int ff_label_g(Inst &d, int *changed);
+void ff_boundary_g(Inst &d, int hole, double *Aout, double *Bin);
+void region_grow_g(Inst &d, int c1, int type, int *mark, int *changed);
+void launch_region_mark_g(Inst &d, int c1, int type, double dV, int *mark, int *changed);
 // thermionic-emission metal contacts (metal.cu) and gate tunnelling (tunnel.cu)
 void te_update(Inst &d);
 void te_currents(Inst &d);

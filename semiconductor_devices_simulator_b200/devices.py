@@ -112,6 +112,108 @@ def schottky_diode(lib, n=(40, 3, 3), L=1e-6, ND=1e16, phi_m=4.8, models=7 | 64,
                     {"ND_cm3": ND, "phi_m": phi_m, "models": models})
 
 
+def fv_len(c):
+    """Box-method cell lengths of a coordinate axis (half the distance to each neighbour)."""
+    c = np.asarray(c, float)
+    L = np.empty_like(c)
+    L[0] = 0.5 * (c[1] - c[0])
+    L[-1] = 0.5 * (c[-1] - c[-2])
+    L[1:-1] = 0.5 * (c[2:] - c[:-2])
+    return L
+
+
+def tensor_graph(xs, ys, zs, diag=0.0):
+    """A tensor mesh as a general box-method graph (api3_set_mesh_graph): node k = i + Nx (j +
+    Ny l), edges to the six axis neighbours with their spacing and dual face area, control
+    volumes Lx Ly Lz, positions.  diag > 0 adds the two diagonals of every x-y cell face pair
+    (i, j) - (i+1, j+1) and (i+1, j) - (i, j+1) with a dual area of diag times the smaller
+    axis face: a graph that is no tensor product, on which both solvers must still agree.
+    Returns (rp, cj, h, ar, vol, pos) as numpy arrays."""
+    Nx, Ny, Nz = len(xs), len(ys), len(zs)
+    Lx, Ly, Lz = fv_len(xs), fv_len(ys), fv_len(zs)
+    N = Nx * Ny * Nz
+    nb = [[] for _ in range(N)]
+    for l in range(Nz):
+        for j in range(Ny):
+            for i in range(Nx):
+                k = i + Nx * (j + Ny * l)
+                for di, dj, dl in ((-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)):
+                    ii, jj, ll = i + di, j + dj, l + dl
+                    if not (0 <= ii < Nx and 0 <= jj < Ny and 0 <= ll < Nz):
+                        continue
+                    kb = ii + Nx * (jj + Ny * ll)
+                    if di:
+                        h, a = abs(xs[ii] - xs[i]), Ly[j] * Lz[l]
+                    elif dj:
+                        h, a = abs(ys[jj] - ys[j]), Lx[i] * Lz[l]
+                    else:
+                        h, a = abs(zs[ll] - zs[l]), Lx[i] * Ly[j]
+                    nb[k].append((kb, h, a))
+                if diag > 0.0:
+                    for di, dj in ((-1, -1), (1, 1), (-1, 1), (1, -1)):
+                        ii, jj = i + di, j + dj
+                        if not (0 <= ii < Nx and 0 <= jj < Ny):
+                            continue
+                        kb = ii + Nx * (jj + Ny * l)
+                        h = float(np.hypot(xs[ii] - xs[i], ys[jj] - ys[j]))
+                        a = diag * min(Ly[min(j, jj)], Lx[min(i, ii)]) * Lz[l]
+                        nb[k].append((kb, h, a))
+    rp = np.zeros(N + 1, np.int32)
+    for k in range(N):
+        rp[k + 1] = rp[k] + len(nb[k])
+    cj = np.array([b for row in nb for b, _, _ in row], np.int32)
+    h = np.array([x for row in nb for _, x, _ in row], float)
+    ar = np.array([a for row in nb for _, _, a in row], float)
+    vol = np.array([Lx[i] * Ly[j] * Lz[l] for l in range(Nz) for j in range(Ny) for i in range(Nx)])
+    pos = np.array([[xs[i], ys[j], zs[l]] for l in range(Nz) for j in range(Ny) for i in range(Nx)]).ravel()
+    return rp, cj, h, ar, vol, pos
+
+
+def graph_pn_diode(lib, n=(12, 6, 5), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj=0.5e-6, models=7,
+                   solver=GUI_SOLVER, vmax=0.6, dv=0.1, diag=0.0, graph=True):
+    """The abrupt Si pn diode on a general (graph) mesh built from its tensor mesh
+    (tensor_graph, optional diagonal edges), contacts as node lists on the x = 0 and x = L
+    planes with their face areas; graph=False sets up the same diode on the tensor grid."""
+    lib.api3_init()
+    xs = np.linspace(0.0, L[0], n[0]); ys = np.linspace(0.0, L[1], n[1]); zs = np.linspace(0.0, L[2], n[2])
+    Nx, Ny, Nz = n
+    N = Nx * Ny * Nz
+    si = None
+    if graph:
+        rp, cj, h, ar, vol, pos = tensor_graph(xs, ys, zs, diag)
+        si = lib.api3_add_material(SI, 300.0)
+        if not lib.api3_set_mesh_graph(N, len(cj), iptr(rp), iptr(cj), dptr(h), dptr(ar), dptr(vol), dptr(pos)):
+            raise RuntimeError("api3_set_mesh_graph rejected the graph")
+    else:
+        _grid(lib, xs, ys, zs)
+        si = lib.api3_add_material(SI, 300.0)
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    i = np.arange(N) % Nx
+    x = xs[i]
+    Nd = np.where(x >= xj, ND * 1e6, 0.0)
+    Na = np.where(x < xj, NA * 1e6, 0.0)
+    mat = np.full(N, si, np.int32)
+    lib.api3_set_node_data(iptr(mat), dptr(np.ascontiguousarray(Nd)), dptr(np.ascontiguousarray(Na)), None)
+    lib.api3_clear_contacts()
+    ca = lib.api3_add_contact_ex(0, 0, Ny - 1, 0, Nz - 1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cc = lib.api3_add_contact_ex(1, 0, Ny - 1, 0, Nz - 1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    if graph:
+        Ly, Lz = fv_len(ys), fv_len(zs)
+        k = np.arange(N)
+        j, l = (k // Nx) % Ny, k // (Nx * Ny)
+        for cid, plane in ((ca, 0), (cc, Nx - 1)):
+            nodes = np.ascontiguousarray(k[i == plane], np.int32)
+            areas = np.ascontiguousarray(Ly[j[i == plane]] * Lz[l[i == plane]])
+            if not lib.api3_set_con_nodes(cid, len(nodes), iptr(nodes), dptr(areas)):
+                raise RuntimeError("api3_set_con_nodes failed")
+    npts = int(round(vmax / dv)) + 1
+    V = np.round(np.linspace(0.0, vmax, npts), 12)
+    return Workload("graph_pn_diode" if graph else "pn_diode", (N, 1, 1) if graph else n,
+                    {"anode": ca, "cathode": cc}, [{"fixed": {"cathode": 0.0}, "swept": "anode", "V": V}],
+                    {"models": models, "diag": diag})
+
+
 def graded_axis(L, n, h0):
     """n coordinates on [0, L] whose spacing grows geometrically from h0 at 0."""
     if n < 3:

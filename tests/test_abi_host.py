@@ -11,6 +11,7 @@ import pytest
 
 import semiconductor_devices_simulator_b200 as S
 from semiconductor_devices_simulator_b200 import abi, devices as D
+from semiconductor_devices_simulator_b200.abi import dptr, iptr
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -100,3 +101,24 @@ def test_reference_core_and_library_agree_on_setup(lib):
     for mi in range(1):
         assert lib.api3_mat_ni(mi) == ref.api3_mat_ni(mi)
         assert lib.api3_mat_Eg(mi) == ref.api3_mat_Eg(mi)
+
+
+def test_mesh_graph_validation(lib):
+    """api3_set_mesh_graph accepts a symmetric graph and refuses broken ones (no GPU needed);
+    a tensor grid set afterwards leaves graph mode (semiconductor_3d.c:981-1041)."""
+    xs = np.linspace(0, 1e-6, 4)
+    rp, cj, h, ar, vol, pos = D.tensor_graph(xs, xs[:3], xs[:2], diag=0.2)
+    N = len(vol)
+    lib.api3_init()
+    lib.api3_add_material(D.SI, 300.0)
+    args = lambda rp_, cj_, h_: (N, len(cj_), iptr(rp_), iptr(cj_), dptr(h_), dptr(ar), dptr(vol), dptr(pos))
+    assert lib.api3_set_mesh_graph(*args(rp, cj, h)) == 1
+    assert lib.api3_is_graph() == 1 and lib.api3_get_Nx() == N and lib.api3_get_Ny() == 1
+    bad = cj.copy(); bad[0] = 0                       # a self edge
+    assert lib.api3_set_mesh_graph(*args(rp, bad, h)) == 0
+    asym = cj.copy(); asym[0] = (cj[0] + 2) % N if (cj[0] + 2) % N != 0 else 3   # an edge without its reverse
+    assert lib.api3_set_mesh_graph(*args(rp, asym, h)) == 0
+    hz = h.copy(); hz[1] = 0.0
+    assert lib.api3_set_mesh_graph(*args(rp, cj, hz)) == 0
+    assert lib.api3_set_grid_coords(4, 3, 2, dptr(xs), dptr(xs[:3]), dptr(xs[:2])) == 1
+    assert lib.api3_is_graph() == 0
