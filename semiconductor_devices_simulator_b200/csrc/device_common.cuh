@@ -308,4 +308,15 @@ __device__ __forceinline__ double heat_field(double dq, double dps, double h) {
     return 2.0 * a * b / ((a + b) * h);
 }
 
+// impact ionisation coefficient alpha(F) = g a exp(-(g b / F)^m), (a, b) below / above E0
+// (semiconductor_3d.c:4478-4485)
+__device__ __forceinline__ double ii_alpha(const MatD &m, double F, int c) {
+    if (!(F > 1e5)) return 0.0;                    // below 1 kV/cm: nothing
+    const int r = F >= m.ii_E0[c];
+    double x = m.ii_g * m.ii_b[c][r] / F;
+    if (m.ii_m[c] != 1.0) x = pow(x, m.ii_m[c]);
+    if (x > 700.0) return 0.0;
+    return m.ii_g * m.ii_a[c][r] * exp(-x);
+}
+
 }  // namespace ss

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "device_common.cuh"
+#include "physics_hd.cuh"
 #include "prof.h"
 #include "solver_ctx.h"
 
@@ -103,11 +104,33 @@ __device__ __forceinline__ double ani_edge(const DevP &P, int k, int kp, double 
     for (int q = 0; q < 3; q++) { dv[q] = P.gpos[3 * kp + q] - P.gpos[3 * k + q]; L2 += dv[q] * dv[q]; }
     return L2 > 0.0 ? 1.0 + (a - 1.0) * dv[P.caxis] * dv[P.caxis] / L2 : 1.0;
 }
-// edge mobilities, each undirected edge once (upd_mob_ref_g, :4241-4293; no surface model)
+// least-squares potential gradient of the semiconductor nodes within reach of a wall
+// (qd < 0.5 m), zero elsewhere: the Lombardi field of the edges (upd_mob_ref_g, :4244-4250)
+__device__ void g_grad(const DevP &P, const double *fld, int k, double *g);
+__global__ void k_ggrad_g(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[0];
+    SS_GRID_LOOP(k, P.N) {
+        double g[3] = {0.0, 0.0, 0.0};
+        if (fl_kind(P.flags[k]) == K_SEMI && P.qd[k] < 0.5) g_grad(P, P.phi, k, g);
+        for (int q = 0; q < 3; q++) P.ggrad[3 * k + q] = g[q];
+    }
+}
+// weight of velocity saturation of a node next to a metal contact for an edge of unit
+// direction t (te_node_w, semiconductor_3d.c:813-817)
+__device__ __forceinline__ double te_node_w_g(const DevP &P, int k, const double *t) {
+    const double w = P.te_vw[k];
+    if (w >= 1.0) return 1.0;
+    const double c = t[P.te_ax[k]];
+    return 1.0 - (1.0 - w) * c * c;
+}
+// edge mobilities, each undirected edge once (upd_mob_ref_g, semiconductor_3d.c:4241-4293):
+// anisotropy projected on the edge, Lombardi surface scattering from the field normal to
+// the edge (with the Coulomb term of 4H-SiC), Caughey-Thomas saturation tapered next to
+// metal contacts
 __global__ void k_upd_mob_g(const DevP *__restrict__ Ps) {
     const DevP &P = Ps[0];
     const int N = P.N, D = P.gD;
-    const bool sat = (P.models & 4) != 0;
+    const bool sat = (P.models & 4) != 0, lb = (P.models & 16) != 0;
     SS_GRID_LOOP(k, N) {
         const uint32_t f = P.flags[k];
         for (int s = 0; s < D; s++) {
@@ -118,16 +141,43 @@ __global__ void k_upd_mob_g(const DevP *__restrict__ Ps) {
             if (fl_kind(f) != K_SEMI || fl_kind(P.flags[kp]) != K_SEMI) { P.gmu_n[ue] = P.gmu_p[ue] = 0.0; continue; }
             const MatD &m = P.mats[fl_mat(f)];
             const double h = P.gh[e];
+            double t[3];
+            for (int q = 0; q < 3; q++) t[q] = (P.gpos[3 * kp + q] - P.gpos[3 * k + q]) / h;
             double mn = 0.5 * (P.mu0n[k] + P.mu0n[kp]), mp = 0.5 * (P.mu0p[k] + P.mu0p[kp]);
             mn *= ani_edge(P, k, kp, m.ani_n);
             mp *= ani_edge(P, k, kp, m.ani_p);
-            if (sat) {
+            if (lb && m.lb_on) {
+                const double Dw = exp(-0.5 * (P.qd[k] + P.qd[kp]) / 1e-8);
+                if (Dw > 1e-8) {
+                    const double *ga = P.ggrad + 3 * (size_t)k, *gb = P.ggrad + 3 * (size_t)kp;
+                    const double pa = ga[0] * t[0] + ga[1] * t[1] + ga[2] * t[2];
+                    const double pb = gb[0] * t[0] + gb[1] * t[1] + gb[2] * t[2];
+                    const double Fa = ga[0] * ga[0] + ga[1] * ga[1] + ga[2] * ga[2] - pa * pa;
+                    const double Fb = gb[0] * gb[0] + gb[1] * gb[1] + gb[2] * gb[2] - pb * pb;
+                    const double F = sqrt(fmax(0.5 * (Fa + Fb), 0.0));
+                    const double Nt = 0.5 * (P.Nd[k] + P.Na[k] + P.Nd[kp] + P.Na[kp]);
+                    double ic = 0.0;
+                    if (P.if_NC && m.lbc_on) {          // Coulomb scattering, n from the reference levels
+                        const double nn = 0.5 * (nK(P, m, k, P.phi[k], P.phin[k]) +
+                                                 nK(P, P.mats[fl_mat(P.flags[kp])], kp, P.phi[kp], P.phin[kp]));
+                        const int ea = P.qi[k], eb = P.qi[kp];
+                        const double NC = ea >= 0 && eb >= 0 ? 0.5 * (P.if_NC[ea] + P.if_NC[eb])
+                                        : (ea >= 0 ? P.if_NC[ea] : (eb >= 0 ? P.if_NC[eb] : 0.0));
+                        ic = coul_inv(m, F, nn, NC, 0.5 * (P.Na[k] + P.Na[kp]));
+                    }
+                    if (m.lb_on & 1) mn = lombardi(m, mn, F, Nt, Dw, 0, ic);
+                    if (m.lb_on & 2) mp = lombardi(m, mp, F, Nt, Dw, 1, 0.0);
+                }
+            }
+            double wv = 0.0;
+            if (sat) wv = P.te_vw ? 0.5 * (te_node_w_g(P, k, t) + te_node_w_g(P, kp, t)) : 1.0;
+            if (wv > 0.0) {
                 const double dps = P.phi[kp] - P.phi[k];
                 const double Fn = heat_field(P.phin[kp] - P.phin[k], dps, h);
                 const double Fp = heat_field(P.phip[kp] - P.phip[k], dps, h);
                 const double sn = mob_hf(mn, Fn, m.vsat_n, m.beta_n), sp = mob_hf(mp, Fp, m.vsat_p, m.beta_p);
-                mn += 1.0 * (sn - mn);
-                mp += 1.0 * (sp - mp);
+                mn += wv * (sn - mn);
+                mp += wv * (sp - mp);
             }
             P.gmu_n[ue] = mn;
             P.gmu_p[ue] = mp;
@@ -181,6 +231,8 @@ __global__ void k_cont_assemble_g(const DevP *__restrict__ Ps, int hole) {
         const double vol = gvol(P, k);
         dg += vol * dR;
         b += vol * (dR * car[k] - R);
+        if (P.tk) { dg += P.tk[k]; b += P.tg[k]; }   // gate / metal-contact exchange: sink tk c - tg
+        if (P.gii) b += P.gii[k];                   // impact ionisation (pairs)
         const double w = 1.0 / (dg * sk);
         P.A[0][k] = 1.0;
         for (int s = 0; s < D; s++) P.gval[(size_t)s * N + k] *= w;
@@ -213,7 +265,7 @@ __global__ void k_currents_g(const DevP *__restrict__ Ps) {
         double v[3] = {0.0, 0.0, 0.0};
         for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < P.ncnode; q += gridDim.x * blockDim.x) {
             const int k = P.cnode[q];
-            if (fl_con(P.flags[k]) != c + 1) continue;
+            if (fl_con(P.flags[k]) != c + 1 || P.cons[c].te) continue;   // metal contacts: te_currents
             for (int s = 0; s < D; s++) {
                 const size_t e = (size_t)s * N + k;
                 const int kb = P.gcol[e];
@@ -328,29 +380,66 @@ __global__ void k_node_Jc_g(const DevP *__restrict__ Ps, int which, double *out)
         out[k] = fl_kind(P.flags[k]) == K_SEMI ? J[ax] : 0.0;
     }
 }
-// least-squares potential gradient (g_grad, :2702-2714) and the largest field (Emax_g, :4557-4565)
-__global__ void k_emax_g(const DevP *__restrict__ Ps) {
-    const DevP &P = Ps[0];
+// least-squares gradient of a node field over the node's semiconductor neighbours
+// (g_grad, semiconductor_3d.c:2702-2714): g = M^-1 sum_e (f_b - f_k) dr_e / |dr_e|^2
+__device__ void g_grad(const DevP &P, const double *fld, int k, double *g) {
     const int N = P.N, D = P.gD;
-    double mx = 0.0;
-    SS_GRID_LOOP(k, N) {
-        if (fl_kind(P.flags[k]) != K_SEMI) continue;
-        double r[3] = {0, 0, 0};
+    double r[3] = {0, 0, 0};
+    if (fl_kind(P.flags[k]) == K_SEMI)
         for (int s = 0; s < D; s++) {
             const int b = P.gcol[(size_t)s * N + k];
             if (b < 0 || fl_kind(P.flags[b]) != K_SEMI) continue;
             const double dx = P.gpos[3 * b] - P.gpos[3 * k], dy = P.gpos[3 * b + 1] - P.gpos[3 * k + 1],
                          dz = P.gpos[3 * b + 2] - P.gpos[3 * k + 2];
-            const double w = (P.phi[b] - P.phi[k]) / (dx * dx + dy * dy + dz * dz + 1e-40);
+            const double w = (fld[b] - fld[k]) / (dx * dx + dy * dy + dz * dz + 1e-40);
             r[0] += w * dx; r[1] += w * dy; r[2] += w * dz;
         }
-        const double *m = P.glsq + 6 * (size_t)k;
-        const double g0 = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
-        const double g1 = m[1] * r[0] + m[3] * r[1] + m[4] * r[2];
-        const double g2 = m[2] * r[0] + m[4] * r[1] + m[5] * r[2];
-        mx = fmax(mx, g0 * g0 + g1 * g1 + g2 * g2);
+    const double *m = P.glsq + 6 * (size_t)k;
+    g[0] = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
+    g[1] = m[1] * r[0] + m[3] * r[1] + m[4] * r[2];
+    g[2] = m[2] * r[0] + m[4] * r[1] + m[5] * r[2];
+}
+// the largest field (Emax_g, semiconductor_3d.c:4557-4565)
+__global__ void k_emax_g(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[0];
+    double mx = 0.0;
+    SS_GRID_LOOP(k, P.N) {
+        if (fl_kind(P.flags[k]) != K_SEMI) continue;
+        double g[3];
+        g_grad(P, P.phi, k, g);
+        mx = fmax(mx, g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
     }
     if (grid_max(mx, P.part, P.ticket + 8)) P.res[R_OUT] = mx;
+}
+// impact-ionisation pair generation on the graph: node current densities of each carrier
+// and the field by least squares (ii_update, semiconductor_3d.c:4490-4523); total -> res[R_GII]
+__global__ void k_ii_update_g(const DevP *__restrict__ Ps) {
+    const DevP &P = Ps[0];
+    double acc[1] = {0.0};
+    SS_GRID_LOOP(k, P.N) {
+        const uint32_t f = P.flags[k];
+        double gk = 0.0;
+        const MatD &m = P.mats[fl_mat(f)];
+        if (fl_kind(f) == K_SEMI && !fl_fix(f) && m.ii_on) {
+            double Jn[3], Jp[3], g[3], E[3];
+            node_J_g(P, k, 1, Jn);
+            node_J_g(P, k, 2, Jp);
+            g_grad(P, P.phi, k, g);
+            for (int q = 0; q < 3; q++) E[q] = -g[q];
+            double G = 0.0;
+            for (int c = 0; c < 2; c++) {
+                const double *J = c ? Jp : Jn;
+                const double jj = sqrt(J[0] * J[0] + J[1] * J[1] + J[2] * J[2]);
+                if (!(jj > 0.0)) continue;
+                const double F = fabs(E[0] * J[0] + E[1] * J[1] + E[2] * J[2]) / jj;
+                G += ii_alpha(m, F, c) * jj;
+            }
+            gk = G / Q * gvol(P, k);
+        }
+        P.gii[k] = gk;
+        acc[0] += gk;
+    }
+    if (grid_sum<1>(acc, P.part, P.ticket + 9)) P.res[R_GII] = acc[0];
 }
 
 // ------------------------------------------------------------------ linear algebra
@@ -501,7 +590,10 @@ static dim3 gblocks(const Ctx &c) { return dim3(c.nodes_blocks(), 1); }
 void launch_poisson_g(const Ctx &c, const double *phi_sel, int build) {
     SS_LAUNCH(PF_POISSON, c.maxN, k_poisson_g, gblocks(c), TPB, c.st, c.dP, phi_sel ? 1 : 0, build);
 }
-void launch_upd_mob_g(const Ctx &c) { SS_LAUNCH(PF_UPDMOB, c.maxN, k_upd_mob_g, gblocks(c), TPB, c.st, c.dP); }
+void launch_upd_mob_g(const Ctx &c) {
+    if (c.h.models & 16) SS_LAUNCH(PF_UPDMOB, c.maxN, k_ggrad_g, gblocks(c), TPB, c.st, c.dP);
+    SS_LAUNCH(PF_UPDMOB, c.maxN, k_upd_mob_g, gblocks(c), TPB, c.st, c.dP);
+}
 void launch_cont_assemble_g(const Ctx &c, int hole) {
     SS_LAUNCH(PF_CONT_ASM, c.maxN, k_cont_assemble_g, gblocks(c), TPB, c.st, c.dP, hole);
 }
@@ -517,6 +609,7 @@ void launch_node_Jc_g(const Ctx &c, int which, double *out) {
     SS_LAUNCH(PF_DISPLAY, c.maxN, k_node_Jc_g, gblocks(c), TPB, c.st, c.dP, which, out);
 }
 void launch_emax_g(const Ctx &c) { SS_LAUNCH(PF_DISPLAY, c.maxN, k_emax_g, gblocks(c), TPB, c.st, c.dP); }
+void launch_ii_update_g(const Ctx &c) { SS_LAUNCH(PF_DISPLAY, c.maxN, k_ii_update_g, gblocks(c), TPB, c.st, c.dP); }
 
 namespace {
 double rd(Inst &d, int slot) {

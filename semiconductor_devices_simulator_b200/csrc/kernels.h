@@ -38,6 +38,7 @@ struct Ctx {
 void launch_poisson(const Ctx &c, const double *phi, int build, double *F);   // res[R_PNORM]
 void launch_rebuild_np(const Ctx &c);
 void launch_upd_mob(const Ctx &c);
+void launch_coul_update(const Ctx &c);      // Coulomb interface charge (before the edge mobilities)
 void launch_cont_assemble(const Ctx &c, int hole);
 void launch_cont_update(const Ctx &c, int hole, double lo, double hi);          // res[R_DQ]
 void launch_apply_bc(const Ctx &c, int have_solution);
@@ -51,6 +52,7 @@ void launch_mob_display(const Ctx &c);
 void launch_node_val(const Ctx &c, int which, double *out);
 void launch_ion_neutral(const Ctx &c);
 void launch_ii_update(const Ctx &c);
+void launch_ii_update_g(const Ctx &c);   // graph mesh (graph.cu)
 void launch_region_seed(const Ctx &c, int c1, int *mark);
 void launch_region_shift(const Ctx &c, int c1, double dV, const int *mark);
 void launch_face_J(const Ctx &c, int ax, int carrier, double *out);

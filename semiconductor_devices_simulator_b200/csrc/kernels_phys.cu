@@ -232,9 +232,12 @@ __global__ void k_coul_update(const DevP *__restrict__ Ps) {
         P.if_NC[e] = (P.if_Qf[e] + Qt) / A;
     }
 }
-void launch_upd_mob(const Ctx &c) {
+void launch_coul_update(const Ctx &c) {
     if (c.h.if_NC && (c.h.models & 16))
         SS_LAUNCH(PF_UPDMOB, c.h.n_if, k_coul_update, dim3(c.nodes_blocks(), c.ninst), TPB, c.st, c.dP);
+}
+void launch_upd_mob(const Ctx &c) {
+    launch_coul_update(c);
     SS_LAUNCH(PF_UPDMOB, c.maxN, k_upd_mob, grid_of(c), TPB, c.st, c.dP);
 }
 
@@ -526,15 +529,6 @@ void launch_currents(const Ctx &c) {
 }
 
 // ------------------------------------------------------------------ impact ionisation
-// alpha(F) = g a exp(-(g b / F)^m), (a, b) below / above E0 (semiconductor_3d.c:4478-4485)
-__device__ __forceinline__ double ii_alpha(const MatD &m, double F, int c) {
-    if (!(F > 1e5)) return 0.0;                    // below 1 kV/cm: nothing
-    const int r = F >= m.ii_E0[c];
-    double x = m.ii_g * m.ii_b[c][r] / F;
-    if (m.ii_m[c] != 1.0) x = pow(x, m.ii_m[c]);
-    if (x > 700.0) return 0.0;
-    return m.ii_g * m.ii_a[c][r] * exp(-x);
-}
 // pair generation G = (alpha_n(F_n) |J_n| + alpha_p(F_p) |J_p|) / q over the control volume,
 // F the field along each carrier's node current density (semiconductor_3d.c:4486-4523), and
 // the total generation -> res[R_GII]

@@ -133,6 +133,7 @@ struct DevP {
     const int *gcol, *gue, *grev;
     const double *gh, *ga, *gpos, *glsq;
     double *gval, *gmu_n, *gmu_p, *gdil;
+    double *ggrad;               // least-squares potential gradient near walls (3 N, surface mobility)
     const float *te_vw;
     const signed char *te_ax;
     const MatD *mats;

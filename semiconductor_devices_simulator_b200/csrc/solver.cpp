@@ -496,7 +496,7 @@ static int graph_upload(Inst &d, const std::vector<unsigned char> &kind, DevP &P
     P.gD = 0; P.nUE = 0;
     P.gcol = P.gue = P.grev = nullptr;
     P.gh = P.ga = P.gpos = P.glsq = nullptr;
-    P.gval = P.gmu_n = P.gmu_p = P.gdil = nullptr;
+    P.gval = P.gmu_n = P.gmu_p = P.gdil = P.ggrad = nullptr;
     if (!d.unstr) return 1;
     GraphHost &G = d.ggh;
     const int N = (int)d.N;
@@ -541,7 +541,7 @@ static int graph_upload(Inst &d, const std::vector<unsigned char> &kind, DevP &P
     const size_t o_col = room(DN * 4), o_ue = room(DN * 4), o_rv = room(DN * 4), o_h = room(DN * 8), o_ar = room(DN * 8),
                  o_val = room(DN * 8),
                  o_pos = room(3 * (size_t)N * 8), o_lsq = room(6 * (size_t)N * 8), o_mun = room(nue * 8),
-                 o_mup = room(nue * 8), o_dil = room((size_t)N * 8);
+                 o_mup = room(nue * 8), o_dil = room((size_t)N * 8), o_gg = room(3 * (size_t)N * 8);
     char *b = nullptr;
     if (cudaMalloc(&b, off) != cudaSuccess) {
         std::fprintf(stderr, "semisim-b200: out of device memory for the mesh graph\n");
@@ -562,6 +562,7 @@ static int graph_upload(Inst &d, const std::vector<unsigned char> &kind, DevP &P
     P.glsq = (const double *)(b + o_lsq);
     P.gval = (double *)(b + o_val); P.gmu_n = (double *)(b + o_mun); P.gmu_p = (double *)(b + o_mup);
     P.gdil = (double *)(b + o_dil);
+    P.ggrad = (double *)(b + o_gg);
     if (cudaStreamSynchronize(st) != cudaSuccess) ok = false;
     return ok && gmg_build(d, st) ? 1 : 0;
 }
@@ -578,6 +579,25 @@ struct TeHost {
     std::vector<signed char> ax;
     int ce0[NC_MAX], ce1[NC_MAX];
 };
+// graph mesh: the displacement a -> b projected on the unit vector u, and the neighbour of
+// cur best aligned with u (cosine above cmin), not prev (g_proj / g_step,
+// semiconductor_3d.c:1272-1284)
+static double g_proj(const GraphHost &G, size_t a, size_t b, const double *u) {
+    return (G.pos[3 * b] - G.pos[3 * a]) * u[0] + (G.pos[3 * b + 1] - G.pos[3 * a + 1]) * u[1] +
+           (G.pos[3 * b + 2] - G.pos[3 * a + 2]) * u[2];
+}
+static long g_step(const GraphHost &G, size_t cur, long prev, const double *u, double cmin) {
+    long best = -1;
+    double bc = cmin;
+    for (int e = G.rp[cur]; e < G.rp[cur + 1]; e++) {
+        const int b = G.cj[e];
+        if ((long)b == prev) continue;
+        const double c = g_proj(G, cur, (size_t)b, u) / G.h[e];
+        if (c > bc) { bc = c; best = b; }
+    }
+    return best;
+}
+
 static void te_build(Inst &d, const std::vector<unsigned char> &kind, const std::vector<int> &con, TeHost &H) {
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const size_t N = d.N;
@@ -595,6 +615,25 @@ static void te_build(Inst &d, const std::vector<unsigned char> &kind, const std:
             int cnt = 1;
             double s_ = 0.;
             size_t cur = k;
+            if (d.unstr) {                                  // graph: the neighbour best aligned with the normal
+                double v[3] = {0., 0., 0.};
+                v[cn.face / 2] = (cn.face & 1) ? -1. : 1.;
+                long prev = -1;
+                for (int guard = 0; guard < 100000; guard++) {
+                    const long nb = g_step(d.ggh, cur, prev, v, 0.8);
+                    if (nb < 0 || kind[nb] != K_SEMI || con[nb]) break;
+                    const double h = g_proj(d.ggh, cur, (size_t)nb, v);
+                    if (!(h > 0.)) break;
+                    s_ += h;
+                    H.tc_k.push_back((int)nb); H.tc_s.push_back(s_);
+                    cnt++;
+                    if (s_ >= TE_COL) break;
+                    prev = (long)cur;
+                    cur = (size_t)nb;
+                }
+                H.te_cn.push_back(cnt);
+                return;
+            }
             for (int guard = 0; guard < 100000; guard++) {
                 const int l = int(cur / ((size_t)Nx * Ny)), rem = int(cur - (size_t)l * Nx * Ny);
                 const int j = rem / Nx, i = rem % Nx;
@@ -744,6 +783,94 @@ static void tun_build(Inst &d, const std::vector<unsigned char> &kind, const std
     }
 }
 
+// Gate-tunnelling paths on a graph mesh (tun_build_graph / tun_push_g,
+// semiconductor_3d.c:1285-1349): from every semiconductor node of no contact along each edge
+// into an insulator node of no contact, on through the insulator by the neighbour best
+// aligned with that edge, each layer bounded at the midpoints of the projected positions;
+// the path counts if it ends on the metal of a Dirichlet gate within TUN_LMAX.  A Robin
+// gate adds one path per gate node along the face's outward normal.  The supply column
+// runs from the node against the path direction, a node's share half the spacing to each
+// column neighbour (the interface half cell first).
+static void tun_build_graph(Inst &d, const std::vector<unsigned char> &kind, const std::vector<int> &con,
+                            const std::vector<int> &rob_k, const std::vector<double> &rob_A,
+                            const std::vector<int> &rob_c, TunHost &H) {
+    for (int c = 0; c < d.n_cons; c++) d.cons[c].ntp = 0;
+    if (!(d.models & 32)) return;
+    const GraphHost &G = d.ggh;
+    const int N = (int)d.N;
+    auto push = [&](size_t k, double A, int c, const double *u, double hw, int nl, const int *m, const double *t) {
+        H.tp_k.push_back((int)k); H.tp_A.push_back(A); H.tp_c.push_back(c); H.tp_nl.push_back(nl);
+        for (int i = 0; i < TUN_MAXL; i++) { H.tp_m.push_back(i < nl ? m[i] : 0); H.tp_t.push_back(i < nl ? t[i] : 0.); }
+        H.tp_c0.push_back((int)H.col_k.size());
+        const double v[3] = {-u[0], -u[1], -u[2]};
+        size_t cur = k;
+        long prev = -1;
+        double depth = 0., hprev = 2. * hw;
+        int cnt = 0;
+        for (int guard = 0; guard < 10000; guard++) {
+            long nb = g_step(G, cur, prev, v, 0.8);
+            if (nb >= 0 && (kind[nb] != K_SEMI || con[nb])) nb = -1;
+            const double h = nb >= 0 ? g_proj(G, cur, (size_t)nb, v) : 0.;
+            if (nb >= 0 && !(h > 0.)) nb = -1;
+            double L = 0.5 * hprev + (nb >= 0 ? 0.5 * h : 0.5 * hprev);
+            if (!(L > 0.)) L = std::cbrt(d.Lx[cur]);
+            H.col_k.push_back((int)cur); H.col_l.push_back(L); H.col_h.push_back(nb >= 0 ? h : 0.);
+            cnt++;
+            depth += L;
+            if (nb < 0 || depth >= TUN_COL) break;
+            prev = (long)cur;
+            cur = (size_t)nb;
+            hprev = h;
+        }
+        H.tp_cn.push_back(cnt);
+        d.cons[c].ntp++;
+    };
+    for (int k = 0; k < N; k++) {
+        if (kind[k] != K_SEMI || con[k]) continue;
+        for (int e0 = G.rp[k]; e0 < G.rp[k + 1]; e0++) {
+            const int kb = G.cj[e0];
+            if (kind[kb] != K_INS || con[kb]) continue;
+            const double h = G.h[e0];
+            double u[3];
+            for (int q = 0; q < 3; q++) u[q] = (G.pos[3 * kb + q] - G.pos[3 * k + q]) / h;
+            int m[TUN_MAXL];
+            double t[TUN_MAXL];
+            int nl = 1, ok = 0;
+            m[0] = d.mat_idx[k]; t[0] = 0.5 * h;              // semiconductor half cell
+            double s0 = 0.5 * h, scur = g_proj(G, k, kb, u), tins = 0.;
+            size_t cur = kb;
+            long prev = k;
+            for (int guard = 0; guard < 100000; guard++) {
+                const long nb = g_step(G, cur, prev, u, 0.8);
+                if (nb < 0) break;
+                const double snb = g_proj(G, k, (size_t)nb, u);
+                const bool end = kind[nb] == K_METAL && con[nb] && d.cons[con[nb] - 1].bc == 2;
+                const double s1 = end ? snb : 0.5 * (scur + snb), seg = s1 - s0;
+                if (!(seg > 0.)) break;
+                const int mi = d.mat_idx[cur];
+                if (nl > 1 && m[nl - 1] == mi) t[nl - 1] += seg;
+                else {
+                    if (nl >= TUN_MAXL) break;
+                    m[nl] = mi; t[nl] = seg; nl++;
+                }
+                tins += seg;
+                if (tins > TUN_LMAX) break;
+                if (end) { ok = con[nb]; break; }
+                if (kind[nb] != K_INS || con[nb]) break;
+                s0 = s1; scur = snb; prev = (long)cur; cur = (size_t)nb;
+            }
+            if (ok) push((size_t)k, G.ar[e0], ok - 1, u, 0.5 * h, nl, m, t);
+        }
+    }
+    for (size_t r = 0; r < rob_k.size(); r++) {
+        const Contact &cn = d.cons[rob_c[r]];
+        if (cn.snl < 1) continue;
+        double u[3] = {0., 0., 0.};
+        u[cn.face / 2] = (cn.face & 1) ? 1. : -1.;            // outward normal of the face
+        push((size_t)rob_k[r], rob_A[r], rob_c[r], u, 0., cn.snl, cn.smat, cn.st);
+    }
+}
+
 // the per-node gather of the continuity sink / source: tunnelling column entries, paths
 // ending at the node, metal-contact column entries, each list in ascending order
 struct ScHost {
@@ -867,9 +994,14 @@ static int coul_upload(Inst &d, const std::vector<unsigned char> &kind, const st
     if (!any) return 1;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const size_t N = d.N;
-    auto nbrs = [&](size_t k, size_t *kb, double *ar) {
-        const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny), j = rem / Nx, i = rem % Nx;
+    const GraphHost &G = d.ggh;
+    auto nbrs = [&](size_t k, size_t *kb, double *ar) {     // at most 64 (NBR_MAX) on a graph
         int c = 0;
+        if (d.unstr) {
+            for (int e = G.rp[k]; e < G.rp[k + 1] && c < 64; e++) { kb[c] = (size_t)G.cj[e]; ar[c++] = G.ar[e]; }
+            return c;
+        }
+        const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny), j = rem / Nx, i = rem % Nx;
         if (i > 0) { kb[c] = k - 1; ar[c++] = d.Ly[j] * d.Lz[l]; }
         if (i < Nx - 1) { kb[c] = k + 1; ar[c++] = d.Ly[j] * d.Lz[l]; }
         if (j > 0) { kb[c] = k - Nx; ar[c++] = d.Lx[i] * d.Lz[l]; }
@@ -879,6 +1011,7 @@ static int coul_upload(Inst &d, const std::vector<unsigned char> &kind, const st
         return c;
     };
     auto xyz = [&](size_t k, double *pq) {
+        if (d.unstr) { for (int q = 0; q < 3; q++) pq[q] = G.pos[3 * k + q]; return; }
         const int l = int(k / ((size_t)Nx * Ny)), rem = int(k - (size_t)l * Nx * Ny);
         pq[0] = d.xs[rem % Nx]; pq[1] = d.ys[rem / Nx]; pq[2] = d.zs[l];
     };
@@ -891,8 +1024,8 @@ static int coul_upload(Inst &d, const std::vector<unsigned char> &kind, const st
         return x * x + y * y + z * z;
     };
     std::vector<int> qi(N, -1), ik;
-    size_t kb[6], kb2[6];
-    double ar[6], ar2[6];
+    size_t kb[64], kb2[64];
+    double ar[64], ar2[64];
     for (size_t k = 0; k < N; k++) {
         if (kind[k] != K_SEMI || con[k] || !d.mats[d.mat_idx[k]].lbc_on) continue;
         bool is = gate[k] != 0;
@@ -1184,17 +1317,6 @@ int prepare(Inst &d) {
     std::vector<double> qd, qcn0, qcp0;
     const bool qc_on = (d.models & 8) != 0;
     if (d.unstr) {
-        // models that touch neighbours through the tensor geometry have no graph variant here
-        const char *why = nullptr;
-        if (d.models & 16) why = "surface mobility (models bit 4)";
-        if (d.models & 32) why = "gate tunnelling (models bit 5)";
-        if (d.models & 256) why = "impact ionisation (models bit 8)";
-        for (int c = 0; c < d.n_cons; c++)
-            if ((d.models & 64) && d.cons[c].bc == 1 && d.cons[c].face <= 5) why = "metal contacts (models bit 6)";
-        if (why) {
-            std::fprintf(stderr, "semisim-b200: %s on a general (prism) mesh is not supported by this solver library\n", why);
-            return 0;
-        }
         walls_graph(d, kind, qd, qc_on, qcn0, qcp0);
     } else {
         wall_distance(d, kind, gate, qd, qc_on, qcn0, qcp0);
@@ -1229,14 +1351,9 @@ int prepare(Inst &d) {
     }
     TeHost teh;
     TunHost tuh;
-    if (!d.unstr) {
-        te_build(d, kind, con, teh);
-        tun_build(d, kind, con, rob_k, rob_A, rob_c, tuh);
-    } else {
-        teh.vw.assign(N, 1.f); teh.ax.assign(N, 0);
-        for (int c = 0; c < NC_MAX; c++) teh.ce0[c] = teh.ce1[c] = 0;
-        for (int c = 0; c < d.n_cons; c++) d.cons[c].ntp = 0;
-    }
+    te_build(d, kind, con, teh);
+    if (!d.unstr) tun_build(d, kind, con, rob_k, rob_A, rob_c, tuh);
+    else tun_build_graph(d, kind, con, rob_k, rob_A, rob_c, tuh);
     ScHost sch;
     sc_build(N, tuh, teh.tc_k, sch);
     if (!gpu_alloc(d)) return 0;
@@ -1362,8 +1479,13 @@ void clamp_qf(Inst &d) {
 }
 void rebuild_np(Inst &d) { launch_rebuild_np(make_ctx(d)); }
 void upd_mob(Inst &d) {
-    if (d.unstr) launch_upd_mob_g(make_ctx(d));
-    else launch_upd_mob(make_ctx(d));
+    if (d.unstr) {
+        const Ctx c = make_ctx(d);
+        launch_coul_update(c);
+        launch_upd_mob_g(c);
+    } else {
+        launch_upd_mob(make_ctx(d));
+    }
 }
 
 void terminal_currents(Inst &d, double *I, double *S) {
@@ -1530,7 +1652,8 @@ static int gummel(Inst &d, const double *Va, int maxit, double gtol, int *iters,
         te_update(d);
         int iiok = 1;
         if (iion) {
-            launch_ii_update(c);
+            if (d.unstr) launch_ii_update_g(c);
+            else launch_ii_update(c);
             const double Gs = read_res(d, R_GII);
             if (Gs > 0.) {
                 if (Gs_old < 0.) { iiok = 0; Erem = Gs; }

@@ -170,7 +170,7 @@ def tensor_graph(xs, ys, zs, diag=0.0):
 
 
 def graph_pn_diode(lib, n=(12, 6, 5), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj=0.5e-6, models=7,
-                   solver=GUI_SOLVER, vmax=0.6, dv=0.1, diag=0.0, graph=True):
+                   solver=GUI_SOLVER, vmax=0.6, dv=0.1, diag=0.0, graph=True, mobility=None, tau=None):
     """The abrupt Si pn diode on a general (graph) mesh built from its tensor mesh
     (tensor_graph, optional diagonal edges), contacts as node lists on the x = 0 and x = L
     planes with their face areas; graph=False sets up the same diode on the tensor grid."""
@@ -189,6 +189,11 @@ def graph_pn_diode(lib, n=(12, 6, 5), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj
         si = lib.api3_add_material(SI, 300.0)
     lib.api3_set_solver(*solver)
     lib.api3_set_models(models)
+    if mobility is not None:
+        if not lib.api3_set_mat_mobility(si, mobility[0] * 1e-4, mobility[1] * 1e-4):
+            raise RuntimeError("api3_set_mat_mobility failed")
+    if tau is not None:
+        lib.api3_set_mat_tau(si, tau, tau)
     i = np.arange(N) % Nx
     x = xs[i]
     Nd = np.where(x >= xj, ND * 1e6, 0.0)
@@ -212,6 +217,141 @@ def graph_pn_diode(lib, n=(12, 6, 5), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj
     return Workload("graph_pn_diode" if graph else "pn_diode", (N, 1, 1) if graph else n,
                     {"anode": ca, "cathode": cc}, [{"fixed": {"cathode": 0.0}, "swept": "anode", "V": V}],
                     {"models": models, "diag": diag})
+
+
+def graph_schottky_diode(lib, n=(40, 3, 3), L=1e-6, ND=1e16, phi_m=4.8, models=7 | 64, h0=2e-9,
+                         solver=GUI_SOLVER, V=None, diag=0.0):
+    """The n-Si Schottky diode of schottky_diode() on a general (graph) mesh built from its
+    tensor mesh: the metal face contact (bc 1) and the ohmic cathode as node lists on the
+    x = 0 and x = L planes; the metal contact's inward column is walked along the graph."""
+    lib.api3_init()
+    xs = graded_axis(L, n[0], h0)
+    ys = np.linspace(0.0, 0.2e-6, n[1])
+    zs = np.linspace(0.0, 0.2e-6, n[2])
+    Nx, Ny, Nz = n
+    N = Nx * Ny * Nz
+    rp, cj, h, ar, vol, pos = tensor_graph(xs, ys, zs, diag)
+    si = lib.api3_add_material(SI, 300.0)
+    if not lib.api3_set_mesh_graph(N, len(cj), iptr(rp), iptr(cj), dptr(h), dptr(ar), dptr(vol), dptr(pos)):
+        raise RuntimeError("api3_set_mesh_graph rejected the graph")
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    mat = np.full(N, si, np.int32)
+    lib.api3_set_node_data(iptr(mat), dptr(np.full(N, ND * 1e6)), dptr(np.zeros(N)), None)
+    lib.api3_clear_contacts()
+    ca = lib.api3_add_contact_ex(0, 0, Ny - 1, 0, Nz - 1, 0, 0, 1, 0.0, phi_m, 0.0, 0.0)
+    cc = lib.api3_add_contact_ex(1, 0, Ny - 1, 0, Nz - 1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    k = np.arange(N)
+    i, j, l = k % Nx, (k // Nx) % Ny, k // (Nx * Ny)
+    Ly, Lz = fv_len(ys), fv_len(zs)
+    for cid, plane in ((ca, 0), (cc, Nx - 1)):
+        sel = i == plane
+        if not lib.api3_set_con_nodes(cid, int(sel.sum()), iptr(np.ascontiguousarray(k[sel], np.int32)),
+                                      dptr(np.ascontiguousarray(Ly[j[sel]] * Lz[l[sel]]))):
+            raise RuntimeError("api3_set_con_nodes failed")
+    if V is None:
+        V = np.round(np.linspace(0.0, 0.4, 9), 12)
+    return Workload("graph_schottky_diode", (N, 1, 1), {"anode": ca, "cathode": cc},
+                    [{"fixed": {"cathode": 0.0}, "swept": "anode", "V": np.asarray(V, float)}],
+                    {"ND_cm3": ND, "phi_m_eV": phi_m, "models": models, "diag": diag})
+
+
+def graph_moscap(lib, models=7 | 32, solver=GUI_SOLVER, diag=0.0):
+    """A thin-oxide n-Si MOS capacitor on a general (graph) mesh: n-Si (3e17 cm^-3) 40 nm deep
+    under 1.5 nm of SiO2 meshed at 0.5 nm, a metal gate (work function 4.1 eV, a Dirichlet
+    gate on the top plane) and an ohmic back contact as node lists; gate swept 0..1.6 V
+    (accumulation: direct tunnelling of the accumulated electrons through the oxide nodes)."""
+    lib.api3_init()
+    ysi = 40e-9 - graded_axis(40e-9, 24, 0.3e-9)[::-1]
+    ys = np.concatenate([ysi, 40e-9 + np.array([0.5e-9, 1.0e-9, 1.5e-9])])
+    xs = np.linspace(0, 20e-9, 3)
+    zs = np.linspace(0, 20e-9, 3)
+    Nx, Ny, Nz = len(xs), len(ys), len(zs)
+    N = Nx * Ny * Nz
+    rp, cj, h, ar, vol, pos = tensor_graph(xs, ys, zs, diag)
+    si = lib.api3_add_material(SI, 300.0)
+    ox = lib.api3_add_material(SIO2, 300.0)
+    if not lib.api3_set_mesh_graph(N, len(cj), iptr(rp), iptr(cj), dptr(h), dptr(ar), dptr(vol), dptr(pos)):
+        raise RuntimeError("api3_set_mesh_graph rejected the graph")
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    k = np.arange(N)
+    i, j, l = k % Nx, (k // Nx) % Ny, k // (Nx * Ny)
+    oxide = j >= Ny - 3
+    mat = np.where(oxide, ox, si).astype(np.int32)
+    lib.api3_set_node_data(iptr(mat), dptr(np.where(oxide, 0.0, 3e23)), dptr(np.zeros(N)), None)
+    lib.api3_clear_contacts()
+    cb = lib.api3_add_contact_ex(2, 0, 2, 0, 2, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cg = lib.api3_add_contact_ex(3, 0, 2, 0, 2, 0, 0, 2, 0.0, 4.1, 0.0, 0.0)
+    LX, LZ = fv_len(xs), fv_len(zs)
+    for cid, sel in ((cb, j == 0), (cg, j == Ny - 1)):
+        if not lib.api3_set_con_nodes(cid, int(sel.sum()), iptr(np.ascontiguousarray(k[sel], np.int32)),
+                                      dptr(np.ascontiguousarray(LX[i[sel]] * LZ[l[sel]]))):
+            raise RuntimeError("api3_set_con_nodes failed")
+    V = np.round(np.linspace(0.0, 1.6, 9), 12)
+    return Workload("graph_moscap", (N, 1, 1), {"back": cb, "gate": cg},
+                    [{"fixed": {"back": 0.0}, "swept": "gate", "V": V}], {"models": models, "diag": diag})
+
+
+def graph_nmosfet(lib, n=(24, 12, 3), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e17, Nsd=1e20, sigma=20e-9,
+                  sd_len=100e-9, tox=2e-9, phi_m=4.6, models=4 | 8 | 16, solver=GUI_SOLVER, vd=0.05, vg_max=1.0,
+                  dvg=0.25, h0=2e-9, diag=0.0, Nox=0.0, material=None):
+    """The n-MOSFET of nmosfet() on a general (graph) mesh built from its tensor mesh
+    (tensor_graph, optional diagonal edges): contacts as node lists on the y = 0 surface
+    (source, drain, the Robin face gate) and the back face (body), and the interface walls
+    the host supplies on a graph (api3_set_walls): every semiconductor node under the gate
+    has the gate surface as its wall - its distance and its cell's range from it - the
+    walls the tensor path's scan finds for a face gate."""
+    lib.api3_init()
+    xs = np.linspace(0.0, Lx, n[0])
+    ys = graded_axis(Ly, n[1], h0)
+    zs = np.linspace(0.0, Lz, n[2])
+    Nx, Ny, Nz = n
+    N = Nx * Ny * Nz
+    rp, cj, h, ar, vol, pos = tensor_graph(xs, ys, zs, diag)
+    si = lib.api3_add_material(SI if material is None else material, 300.0)
+    if not lib.api3_set_mesh_graph(N, len(cj), iptr(rp), iptr(cj), dptr(h), dptr(ar), dptr(vol), dptr(pos)):
+        raise RuntimeError("api3_set_mesh_graph rejected the graph")
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    k = np.arange(N)
+    i, j, l = k % Nx, (k // Nx) % Ny, k // (Nx * Ny)
+    Nd2 = _gauss_sd(xs, ys, 0.0, sd_len, Nsd, sigma) + _gauss_sd(xs, ys, Lx - sd_len, Lx, Nsd, sigma)
+    Nd = np.ascontiguousarray(Nd2[j, i] * 1e6)
+    Na = np.full(N, Nbody * 1e6)
+    mat = np.full(N, si, np.int32)
+    lib.api3_set_node_data(iptr(mat), dptr(Nd), dptr(Na), dptr(np.zeros(N)))
+    lib.api3_clear_contacts()
+    iS1 = int(np.searchsorted(xs, 0.8 * sd_len, side="right")) - 1
+    iD0 = int(np.searchsorted(xs, Lx - 0.8 * sd_len, side="left"))
+    iG0 = int(np.searchsorted(xs, sd_len - 0.5 * sigma, side="left"))
+    iG1 = int(np.searchsorted(xs, Lx - sd_len + 0.5 * sigma, side="right")) - 1
+    nz = Nz - 1
+    cs = lib.api3_add_contact_ex(2, 0, iS1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cd = lib.api3_add_contact_ex(2, iD0, Nx - 1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cg = lib.api3_add_contact_ex(2, iG0, iG1, 0, nz, 0, 0, 2, 0.0, phi_m, tox, Nox)
+    cb = lib.api3_add_contact_ex(3, 0, Nx - 1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    LX, LZ = fv_len(xs), fv_len(zs)
+    for cid, sel in ((cs, (j == 0) & (i <= iS1)), (cd, (j == 0) & (i >= iD0)),
+                     (cg, (j == 0) & (i >= iG0) & (i <= iG1)), (cb, j == Ny - 1)):
+        nodes = np.ascontiguousarray(k[sel], np.int32)
+        areas = np.ascontiguousarray(LX[i[sel]] * LZ[l[sel]])
+        if not lib.api3_set_con_nodes(cid, len(nodes), iptr(nodes), dptr(areas)):
+            raise RuntimeError("api3_set_con_nodes failed")
+    walls = np.ones((N, 6))
+    under = (i >= iG0) & (i <= iG1)
+    y = ys[j]
+    lo = np.where(j > 0, 0.5 * (ys[np.maximum(j - 1, 0)] + y), y)
+    hi = np.where(j < Ny - 1, 0.5 * (y + ys[np.minimum(j + 1, Ny - 1)]), y)
+    walls[under, 0] = y[under]
+    walls[under, 1] = np.maximum(lo[under], 0.0)
+    walls[under, 2] = hi[under]
+    lib.api3_set_walls(dptr(np.ascontiguousarray(walls.ravel())))
+    npts = int(round(vg_max / dvg)) + 1
+    V = np.round(np.linspace(0.0, vg_max, npts), 12)
+    return Workload("graph_nmosfet", (N, 1, 1), {"source": cs, "drain": cd, "gate": cg, "body": cb},
+                    [{"fixed": {"drain": vd, "source": 0.0, "body": 0.0}, "swept": "gate", "V": V}],
+                    {"models": models, "diag": diag, "tox_m": tox})
 
 
 def graded_axis(L, n, h0):
