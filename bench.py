@@ -22,6 +22,12 @@ point (state resident in HBM); `e2e` also copies psi, n and p of every point to 
 buffers (api3_bulk_copy), the per-point results a caller reads.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload nmosfet|finfet|diodes64]
+
+`--workload finfet`: the tri-gate FinFET Id-Vg family instead (96x96x64 tensor mesh, fin
+10 nm wide x 40 nm tall wrapped by 1.5 nm SiO2 and three gate electrodes driven together,
+gate 0..1.0 V in 0.02 V steps at 5 drain biases, one instance and stream per drain bias),
+with the same refined / FP64 / learned-seed / reference-core measurements.
 
 Multi-GPU (torchrun, one rank per GPU): every rank solves its own sweeps (independent
 devices, no data-path collective): weak scaling, time = max over ranks.
@@ -53,14 +59,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--mesh", default="120,80,60")
+    ap.add_argument("--mesh", default=None, help="Nx,Ny,Nz (default: the workload's mesh)")
     ap.add_argument("--precision", default="refined", choices=["refined", "fp64"],
                     help="linear solves: FP32 refined in FP64 (default) or FP64 throughout")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison steps")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor step")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuner)")
-    ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "diodes64"],
-                    help="nmosfet: the Id-Vg workload (default); diodes64: the 64 pn-diode variants batch")
+    ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "finfet", "diodes64"],
+                    help="nmosfet: the Id-Vg workload (default); finfet: the tri-gate FinFET Id-Vg family "
+                         "(96x96x64, 5 drain biases); diodes64: the 64 pn-diode variants batch")
     ap.add_argument("--workers", type=int, default=0, help="diodes64: concurrent host threads (0: one per variant)")
     ap.add_argument("--variants", type=int, default=0, help="diodes64: only the first n variants (0: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -77,11 +84,11 @@ def run_probe(a):
     """Few-launch case for ncu: the workload's device, one electron continuity system
     (multigrid set-up and `ITS` BiCGSTAB iterations), then one learned-seed pass."""
     import semiconductor_devices_simulator_b200 as S
-    mesh = tuple(int(v) for v in a.mesh.split(","))
+    mesh = mesh_of(a)
     lib = S.load()
     w = build(lib, mesh)
     lib.api3b_set_precision(1 if a.precision == "refined" else 0)
-    s = w.sweeps[1]
+    s = w.sweeps[-1]
     for cid, vv in D.bias_vector(w, s, 0.6).items():
         lib.api3_set_contact_V(cid, vv)
     assert lib.b200x_prepare() == 1
@@ -100,7 +107,7 @@ def run_probe(a):
     for _ in range(10):
         lib.b200x_seed_run(1.0, abi.dptr(dv))
     seed_ms = lib.b200x_stream_timer(1) / 10
-    print(json.dumps({"probe": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]} electron continuity", "nodes": w.N,
+    print(json.dumps({"probe": f"{WL}_{mesh[0]}x{mesh[1]}x{mesh[2]} electron continuity", "nodes": w.N,
                       "precision": a.precision, "seed_kernel": seed_ok, "seed_ms": round(seed_ms, 4),
                       "bicgstab_its": its, "r0": r0[0], "rn": rn[0],
                       "launches": int(lib.b200x_launches() - l0)}))
@@ -200,8 +207,34 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ workload
+# The Id-Vg workloads: the n-MOSFET (120x80x60, gate 0..1.2 V in 0.05 V steps at Vd = 0.05
+# and 1.0 V) and the tri-gate FinFET (96x96x64, fin 10 x 40 nm, gate 0..1.0 V in 0.02 V
+# steps at 5 drain biases).  Each drain bias is one sweep, solved by its own instance.
+WORKLOADS = {
+    "nmosfet": {"mesh": (120, 80, 60), "build": lambda lib, n: D.nmosfet(lib, n=n)},
+    "finfet": {"mesh": (96, 96, 64), "build": lambda lib, n: D.finfet(lib, n=n)},
+}
+WL = "nmosfet"
+
+
 def build(lib, mesh):
-    return D.nmosfet(lib, n=mesh)
+    return WORKLOADS[WL]["build"](lib, mesh)
+
+
+def mesh_of(a):
+    return tuple(int(v) for v in a.mesh.split(",")) if a.mesh else WORKLOADS[WL]["mesh"]
+
+
+def workload_name(mesh):
+    return f"{WL}_{mesh[0]}x{mesh[1]}x{mesh[2]}_idvg"
+
+
+def workload_config(w):
+    s = w.sweeps
+    V = s[0]["V"]
+    return {"drain_biases_V": [float(x["fixed"]["drain"]) for x in s],
+            "gate_sweep_V": [float(V[0]), float(V[-1]), round(float(V[1] - V[0]), 6)],
+            "models": int(w.info.get("models", 0))}
 
 
 def sweep_points(lib, w, s, fields=False, npts=None, out=None):
@@ -242,7 +275,7 @@ def peaks():
 
 def cpu_baseline(mesh, seconds):
     """The reference core (oracle/_ref, built from the reference sources) on this
-    host's cores: the same workload, a bounded sample of the Vd = 1.0 V sweep."""
+    host's cores: the same workload, a bounded sample of its highest-drain-bias sweep."""
     path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_ref.so")
     if not os.path.exists(path):
         return None
@@ -250,7 +283,7 @@ def cpu_baseline(mesh, seconds):
     cores = os.cpu_count() or 1
     ref.api3_set_threads(cores)
     w = build(ref, mesh)
-    s = w.sweeps[1]
+    s = w.sweeps[-1]
     D.start_sweep(ref, w, s)
     t0 = time.perf_counter()
     n = 0
@@ -266,7 +299,8 @@ def cpu_baseline(mesh, seconds):
             break
     dt = time.perf_counter() - t0
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"first {n} resolves of the Vd=1.0 V Id-Vg sweep, {mesh[0]}x{mesh[1]}x{mesh[2]} mesh, "
+            "sample": f"first {n} resolves of the Vd={s['fixed']['drain']} V Id-Vg sweep of {WL}, "
+                      f"{mesh[0]}x{mesh[1]}x{mesh[2]} mesh, "
                       f"reference core semiconductor_3d.c built from source (-O3 -fopenmp), {cores} threads, "
                       f"{dt:.1f} s"}, cur
 
@@ -377,10 +411,10 @@ def learned_step(a, lib, workers, step, cur, gummel_per_step, dist):
 
 def run_b200(a, dist):
     import semiconductor_devices_simulator_b200 as S
-    mesh = tuple(int(v) for v in a.mesh.split(","))
+    mesh = mesh_of(a)
     lib = S.load()
     lib.b200x_set_device(dist.local)
-    nsw = 2                                   # the two drain biases of the workload
+    nsw = 5 if WL == "finfet" else 2          # the drain biases of the workload, one sweep each
     prec = 1 if a.precision == "refined" else 0
 
     def make(p):
@@ -480,7 +514,7 @@ def run_b200(a, dist):
             tot_ms = sum(r[1] for r in prof) or 1.0
             top = max(prof, key=lambda r: r[1])
             ach = top[3] / (top[1] / 1e3) / 1e9 if top[1] > 0 else 0.0
-            traffic = NCU_TRAFFIC.get(top[0]) if mesh == (120, 80, 60) else None
+            traffic = NCU_TRAFFIC.get(top[0]) if (WL, mesh) == ("nmosfet", (120, 80, 60)) else None
             roof = {"bound": "hbm", "kernel": top[0], "achieved": round(ach, 1), "peak": hbm,
                     "peak_kind": pk_kind, "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": traffic,
                     "launches": top[2], "avg_launch_us": round(1e3 * top[1] / max(top[2], 1), 2),
@@ -498,12 +532,13 @@ def run_b200(a, dist):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 inner solves refined in f64 (f64 residuals, physics, currents)" if prec else "f64",
             "data": "synthetic (device built from the workload definition)",
-            "config": {"workload": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]}_idvg",
-                       "nodes": w.N, "points_per_step": npts_step, "drain_biases_V": [0.05, 1.0],
-                       "gate_sweep_V": [0.0, 1.2, 0.05], "models": 4, "solver": list(D.GUI_SOLVER),
-                       "precision": a.precision, "launch_shapes": tune,
-                       "parallelism": f"replicas{dist.world}, {nsw} concurrent sweeps per GPU (instance + stream each)",
-                       "l2": "state of 576k nodes (~0.5 GB) exceeds the 126 MB L2; no flush"},
+            "config": dict({"workload": workload_name(mesh),
+                            "nodes": w.N, "points_per_step": npts_step}, **workload_config(w),
+                           **{"solver": list(D.GUI_SOLVER), "precision": a.precision, "launch_shapes": tune,
+                              "parallelism": f"replicas{dist.world}, {nsw} concurrent sweeps per GPU "
+                                             "(instance + stream each)",
+                              "l2": f"state of {w.N} nodes (~{w.N * 760 / 1e9:.2f} GB) exceeds the 126 MB L2; "
+                                    "no flush"}),
             "converged_points": tot_conv, "wall_s": round(tot_wall, 3),
             "e2e": {"value": round(e_all / e_T, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * npts_step,
                     "d2h_bytes_per_step": d2h * npts_step},
@@ -528,7 +563,7 @@ def run_b200(a, dist):
             if cb:
                 cb, rcur = cb
                 out["cpu_baseline"] = cb
-                out["max_rel_dI_vs_reference"] = rel_dI(cur[1], rcur)
+                out["max_rel_dI_vs_reference"] = rel_dI(cur[nsw - 1], rcur)
     return out
 
 
@@ -537,7 +572,7 @@ def run_reference(a, dist):
     (the first points of one sweep), all host threads."""
     if dist.rank != 0:
         return None
-    mesh = tuple(int(v) for v in a.mesh.split(","))
+    mesh = mesh_of(a)
     path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_ref.so")
     if not os.path.exists(path):
         return {"impl": "reference", "unavailable": "reference core not built (make -C oracle)"}
@@ -562,8 +597,8 @@ def run_reference(a, dist):
             "warmup": a.warmup, "ms_per_step": round(1e3 * tot / a.steps, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
             "data": "synthetic (device built from the workload definition)",
-            "config": {"workload": f"nmosfet_{mesh[0]}x{mesh[1]}x{mesh[2]}_idvg", "nodes": w.N,
-                       "points_per_step": npts, "parallelism": "cpu"},
+            "config": dict({"workload": workload_name(mesh), "nodes": w.N,
+                            "points_per_step": npts, "parallelism": "cpu"}, **workload_config(w)),
             "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": f"first {npts} points of one Id-Vg sweep per step"},
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -647,7 +682,10 @@ def run_batch(a, dist):
 
 
 def main():
+    global WL
     a = parse()
+    if a.workload in WORKLOADS:
+        WL = a.workload
     if a.probe:
         return run_probe(a)
     dist = Dist()

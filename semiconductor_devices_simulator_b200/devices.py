@@ -422,6 +422,65 @@ def nmosfet(lib, n=(120, 80, 60), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e17,
                      "models": models, "Nbody_cm3": Nbody, "Nsd_cm3": Nsd, "sigma_m": sigma})
 
 
+def finfet(lib, n=(96, 96, 64), Lsd=30e-9, Lg=30e-9, W=10e-9, H=40e-9, tox=1.5e-9, tmet=3e-9, tbox=5e-9,
+           Nch=1e17, Nsd=1e20, sigma=3e-9, phi_m=4.6, models=4, solver=GUI_SOLVER,
+           vds=(0.05, 0.25, 0.5, 0.75, 1.0), vg_max=1.0, dvg=0.02):
+    """Tri-gate FinFET-like device on a tensor mesh: an n-channel Si fin W wide and H tall
+    (x along the channel: source extension Lsd, gate Lg, drain extension Lsd) on a buried
+    oxide tbox thick, wrapped on both sides and on top by tox of SiO2 and by gate metal tmet
+    thick over the gate length (three box gate electrodes - left, right, top - driven
+    together); SiO2 spacers fill the rest.  Channel p-type Nch (cm^-3), n+ source / drain
+    Nsd with a Gaussian lateral falloff sigma under the gate edges; ohmic source / drain on
+    the fin's end faces.  Uniform spacing on each axis; a node takes the region holding its
+    position.  Gate swept 0..vg_max in dvg steps at each drain bias of `vds`."""
+    lib.api3_init()
+    Lx = 2 * Lsd + Lg
+    Wt = W + 2 * (tox + tmet)
+    Ht = tbox + H + tox + tmet
+    xs = np.linspace(0.0, Lx, n[0])
+    ys = np.linspace(0.0, Wt, n[1])
+    zs = np.linspace(0.0, Ht, n[2])
+    _grid(lib, xs, ys, zs)
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    si = lib.api3_add_material(SI, 300.0)
+    ox = lib.api3_add_material(SIO2, 300.0)
+    eps = 1e-15
+    y0, y1 = tmet + tox, tmet + tox + W                 # fin faces across
+    z0, z1 = tbox, tbox + H                             # fin bottom / top
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")    # (Nx, Ny, Nz)
+    fin = (Y >= y0 - eps) & (Y <= y1 + eps) & (Z >= z0 - eps) & (Z <= z1 + eps)
+    d = np.where(X < Lsd, 0.0, np.where(X > Lsd + Lg, 0.0, np.minimum(X - Lsd, Lsd + Lg - X)))
+    inside = (X <= Lsd + eps) | (X >= Lsd + Lg - eps)
+    dsd = np.where(inside, 0.0, d)
+    Nd3 = np.where(fin, Nsd * np.exp(-0.5 * (dsd / sigma) ** 2), 0.0)
+    Na3 = np.where(fin, Nch, 0.0)
+    mat3 = np.where(fin, si, ox).astype(np.int32)
+    tr = lambda a: np.ascontiguousarray(np.transpose(a, (2, 1, 0)).ravel())   # to x-fastest order
+    lib.api3_set_node_data(iptr(tr(mat3)), dptr(tr(Nd3) * 1e6), dptr(tr(Na3) * 1e6), None)
+    lib.api3_clear_contacts()
+    idx = lambda c, lo, hi: (int(np.searchsorted(c, lo - eps, side="left")), int(np.searchsorted(c, hi + eps, side="right")) - 1)
+    jf0, jf1 = idx(ys, y0, y1)
+    lf0, lf1 = idx(zs, z0, z1)
+    iG0, iG1 = idx(xs, Lsd, Lsd + Lg)
+    jl1 = int(np.searchsorted(ys, tmet + eps, side="right")) - 1            # left metal: y <= tmet
+    jr0 = int(np.searchsorted(ys, Wt - tmet - eps, side="left"))           # right metal: y >= Wt - tmet
+    lt0 = int(np.searchsorted(zs, Ht - tmet - eps, side="left"))           # top metal: z >= Ht - tmet
+    nx, ny, nz = n[0] - 1, n[1] - 1, n[2] - 1
+    cs = lib.api3_add_contact_ex(0, jf0, jf1, lf0, lf1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cd = lib.api3_add_contact_ex(1, jf0, jf1, lf0, lf1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    gl = lib.api3_add_contact_ex(6, iG0, iG1, 0, jl1, lf0, nz, 2, 0.0, phi_m, 0.0, 0.0)
+    gr = lib.api3_add_contact_ex(6, iG0, iG1, jr0, ny, lf0, nz, 2, 0.0, phi_m, 0.0, 0.0)
+    gt = lib.api3_add_contact_ex(6, iG0, iG1, 0, ny, lt0, nz, 2, 0.0, phi_m, 0.0, 0.0)
+    npts = int(round(vg_max / dvg)) + 1
+    V = np.round(np.linspace(0.0, vg_max, npts), 12)
+    gates = ("gate_l", "gate_r", "gate_t")
+    sweeps = [{"fixed": {"drain": vd, "source": 0.0}, "swept": gates, "V": V} for vd in vds]
+    return Workload("finfet", n, {"source": cs, "drain": cd, "gate_l": gl, "gate_r": gr, "gate_t": gt}, sweeps,
+                    {"fin_nm": (W * 1e9, H * 1e9), "Lg_m": Lg, "tox_m": tox, "phi_m_eV": phi_m, "models": models,
+                     "Nch_cm3": Nch, "Nsd_cm3": Nsd})
+
+
 def diode_variants(count=64, seed=20261203, nmin=32, nmax=72):
     """Parameters of the batched pn-diode family (recorded seed)."""
     rng = np.random.default_rng(seed)
@@ -447,9 +506,12 @@ def diode_variant(lib, v, vmax=0.7, dv=0.025, solver=GUI_SOLVER):
 
 
 def bias_vector(w, sweep, Vswept):
-    """Contact voltages (by contact id) of one sweep point."""
+    """Contact voltages (by contact id) of one sweep point; `swept` names one contact or a
+    tuple of contacts driven together (the three gate electrodes of a tri-gate)."""
     V = {w.contacts[k]: v for k, v in sweep["fixed"].items()}
-    V[w.contacts[sweep["swept"]]] = float(Vswept)
+    sw = sweep["swept"]
+    for k in (sw if isinstance(sw, (tuple, list)) else (sw,)):
+        V[w.contacts[k]] = float(Vswept)
     return V
 
 
