@@ -34,6 +34,11 @@ int b200x_set_qc(const double *qcn, const double *qcp);   /* install an image-fo
    (semiconductor_3d.c:3326-3371) */
 int b200x_tun_update(void);
 int b200x_tun(int *cnt, double *tpG, double *colK, long long *tpk, long long *colk);
+/* graph multigrid hierarchy of a CSR graph, host only (replaces reading the reference's
+   gdev.lev[] after gmg_alloc, semiconductor_3d.c:2475-2512): level L's size, pattern and
+   aggregates; returns the number of levels */
+int b200x_gmg_plan(int N, const int *rp, const int *cj, const double *h, const double *ar, int L,
+                   int *n_out, int *nnz_out, int *rp_out, int *cj_out, int *agg_out);
 int b200x_te(int *cnt, double *teK, double *teG, double *tcK, double *tcG, double *tcI, double *qcn, double *qcp);
 /* device state arrays: 0 psi, 1 phi_n, 2 phi_p, 3 n, 4 p, 5/6 low-field mobility n/p,
    7 sol, 8 rhs, 9 sc, 10 dsc, 16..21 face mobility (n x,y,z; p x,y,z), 22..24 sweep history

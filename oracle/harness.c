@@ -273,3 +273,21 @@ int hx_mat(int mi, double *out){
     memcpy(out,v,sizeof v);
     return (int)(sizeof v/sizeof v[0]);
 }
+
+/* graph multigrid hierarchy built by api3_set_mesh_graph (gmg_alloc,
+   semiconductor_3d.c:2475-2512): level L's node count and pattern size, and when the
+   buffers are given its CSR pattern and (below the coarsest) every node's aggregate.
+   Returns the number of levels (0 without a graph device). */
+int hx_gmg_level(int L, int *n_out, int *nnz_out, int *rp, int *cj, int *agg){
+    if(!gdev.allocated || !gdev.unstr) return 0;
+    int nl=gdev.nlev;
+    if(L<0 || L>=nl) return nl;
+    const Lev *v=&gdev.lev[L];
+    int n=(int)v->N;
+    if(n_out) *n_out=n;
+    if(nnz_out) *nnz_out=v->rp[n];
+    if(rp) for(int i=0;i<=n;i++) rp[i]=v->rp[i];
+    if(cj) for(int e=0;e<v->rp[n];e++) cj[e]=v->cj[e];
+    if(agg && L<nl-1 && v->agg) for(int i=0;i<n;i++) agg[i]=v->agg[i];
+    return nl;
+}

@@ -374,6 +374,32 @@ struct LevelBuild {
     int ncolor = 0, D = 0;
 };
 
+// the levels of a graph (CSR rp / cj, edge lengths h, dual areas ar): patterns, aggregates,
+// member lists and entry maps, down to GMG_COARSE nodes or until the aggregation stalls
+// (gmg_alloc, semiconductor_3d.c:2475-2512); host only
+std::vector<LevelBuild> plan(int N, const std::vector<int> &rp, const std::vector<int> &cj,
+                             const std::vector<double> &h, const std::vector<double> &ar, int passes, double beta) {
+    std::vector<LevelBuild> B(1);
+    B[0].g.N = N;
+    B[0].g.rp = rp;
+    B[0].g.cj = cj;
+    B[0].g.w.resize(cj.size());
+    for (size_t e = 0; e < cj.size(); e++) B[0].g.w[e] = h[e] > 0.0 ? ar[e] / h[e] : 0.0;
+    while ((int)B.size() < MAXLEV) {
+        LevelBuild &f = B.back();
+        if (f.g.N <= GMG_COARSE) break;
+        std::vector<int> agg;
+        const int na = aggregate(f.g, passes, beta, agg);
+        if (na < 1 || (double)na > 0.7 * (double)f.g.N) break;
+        f.agg = agg;
+        members(f.agg, na, f.mrp, f.mem);
+        LevelBuild c;
+        c.g = contract(f.g, f.agg, na, &f.emap);
+        B.push_back(std::move(c));
+    }
+    return B;
+}
+
 }  // namespace
 
 void gmg_free(Inst &d) {
@@ -387,25 +413,7 @@ void gmg_free(Inst &d) {
 int gmg_build(Inst &d, cudaStream_t st) {
     gmg_free(d);
     const GraphHost &G = d.ggh;
-    const int N = (int)d.N;
-    std::vector<LevelBuild> B(1);
-    B[0].g.N = N;
-    B[0].g.rp = G.rp;
-    B[0].g.cj = G.cj;
-    B[0].g.w.resize(G.cj.size());
-    for (size_t e = 0; e < G.cj.size(); e++) B[0].g.w[e] = G.h[e] > 0.0 ? G.ar[e] / G.h[e] : 0.0;
-    while ((int)B.size() < MAXLEV) {
-        LevelBuild &f = B.back();
-        if (f.g.N <= GMG_COARSE) break;
-        std::vector<int> agg;
-        const int na = aggregate(f.g, g_knobs.gpass, g_knobs.gbeta, agg);
-        if (na < 1 || (double)na > 0.7 * (double)f.g.N) break;
-        f.agg = agg;
-        members(f.agg, na, f.mrp, f.mem);
-        LevelBuild c;
-        c.g = contract(f.g, f.agg, na, &f.emap);
-        B.push_back(std::move(c));
-    }
+    std::vector<LevelBuild> B = plan((int)d.N, G.rp, G.cj, G.h, G.ar, g_knobs.gpass, g_knobs.gbeta);
     const int nl = (int)B.size();
     for (auto &b : B) {
         b.ncolor = colour(b.g, b.color);
@@ -628,3 +636,25 @@ void gmg_apply(Inst &d, const Ctx &c, const double *r, double *z, const double *
 int gmg_levels(const Inst &d) { return (int)d.g.glev.size(); }
 
 }  // namespace ss
+
+// Test hook (no GPU needed): the graph multigrid hierarchy of a graph (api3_set_mesh_graph's
+// CSR arrays) with the current pairing knobs.  Level L's node count and pattern size go to
+// n_out / nnz_out; when the buffers are given, its CSR pattern (rp: n + 1, cj: nnz) and, below
+// the coarsest level, every node's aggregate (agg: n).  Returns the number of levels.
+extern "C" int b200x_gmg_plan(int N, const int *rp, const int *cj, const double *h, const double *ar, int L,
+                              int *n_out, int *nnz_out, int *crp, int *ccj, int *agg) {
+    if (N < 1 || !rp || !cj || !h || !ar) return 0;
+    const int E = rp[N];
+    std::vector<int> r(rp, rp + N + 1), c(cj, cj + E);
+    std::vector<double> hh(h, h + E), aa(ar, ar + E);
+    const auto B = ss::plan(N, r, c, hh, aa, ss::g_knobs.gpass, ss::g_knobs.gbeta);
+    const int nl = (int)B.size();
+    if (L < 0 || L >= nl) return nl;
+    const auto &b = B[L];
+    if (n_out) *n_out = b.g.N;
+    if (nnz_out) *nnz_out = (int)b.g.cj.size();
+    if (crp) std::copy(b.g.rp.begin(), b.g.rp.end(), crp);
+    if (ccj) std::copy(b.g.cj.begin(), b.g.cj.end(), ccj);
+    if (agg && L < nl - 1) std::copy(b.agg.begin(), b.agg.end(), agg);
+    return nl;
+}
