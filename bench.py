@@ -563,7 +563,10 @@ def run_b200(a, dist):
             if cb:
                 cb, rcur = cb
                 out["cpu_baseline"] = cb
-                out["max_rel_dI_vs_reference"] = rel_dI(cur[nsw - 1], rcur)
+                out["max_rel_dI_vs_reference"] = {
+                    "all_points": rel_dI(cur[nsw - 1], rcur), "on_state_Id_gt_1nA": rel_dI(cur[nsw - 1], rcur, on=1e-9),
+                    "note": "the reference core's sampled points; off-state currents converge to ~1e-3 in either "
+                            "code at the workload's default tolerances"}
     return out
 
 
