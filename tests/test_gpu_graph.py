@@ -15,8 +15,9 @@ libraries solving the same discrete equations.
   host supplies, Lombardi surface mobility from least-squares gradients), its 4H-SiC
   variant (with the Coulomb interface-charge term), an avalanche diode (impact
   ionisation from least-squares node currents), Schottky diodes (metal contacts with
-  image-force lowering and barrier tunnelling, columns walked along the graph), and gate
-  tunnelling through oxide nodes to a metal gate and through a Robin gate's layer stack."""
+  image-force lowering and barrier tunnelling, columns walked along the graph), gate
+  tunnelling through oxide nodes to a metal gate and through a Robin gate's layer stack,
+  deep traps, and the 4H-SiC MOSFET with surface traps and incomplete ionisation."""
 import ctypes
 import os
 import sys
@@ -147,11 +148,43 @@ def graph_mos_stack(L, s):
     return w
 
 
+def graph_trapped_diode(L, s):
+    """The graph pn diode with a mid-gap acceptor species on the n side (two merged requests)
+    and a donor species 0.3 eV below Ec on the p side."""
+    n = (12, 6, 5)
+    w = D.graph_pn_diode(L, n=n, models=3, solver=s)
+    k = np.arange(w.N)
+    i = k % n[0]
+    sa = L.api3_trap_species(-1, 2, 0.0, 1e-19, 1e-19)
+    sd = L.api3_trap_species(1, 0, 0.3, 2e-20, 5e-20)
+    nn = np.ascontiguousarray(k[i >= n[0] // 2], np.int32)
+    pp = np.ascontiguousarray(k[i < n[0] // 2], np.int32)
+    assert L.api3_trap_add(sa, len(nn), iptr(nn), dptr(np.full(len(nn), 0.6e22))) == 1
+    assert L.api3_trap_add(sa, len(nn), iptr(nn), dptr(np.full(len(nn), 0.4e22))) == 1
+    assert L.api3_trap_add(sd, len(pp), iptr(pp), dptr(np.full(len(pp), 3e22))) == 1
+    return w
+
+
+def graph_sic_traps_incomplete(L, s):
+    """The 4H-SiC graph MOSFET (Coulomb term, 20 nm oxide with fixed charge) with acceptor
+    traps 0.2 eV below Ec on its gate surface and incomplete ionisation of the dopants."""
+    n = (16, 12, 6)
+    w = D.graph_nmosfet(L, n=n, models=7 | 16 | 512, vd=0.5, vg_max=6.0, dvg=1.5, material=D.SIC, Nox=1e16,
+                        tox=20e-9, solver=s)
+    k = np.arange(w.N)
+    surf = np.ascontiguousarray(k[(k // n[0]) % n[1] == 0], np.int32)
+    sid = L.api3_trap_species(-1, 0, 0.2, 1e-19, 1e-19)
+    assert L.api3_trap_add(sid, len(surf), iptr(surf), dptr(np.full(len(surf), 1e24))) == 1
+    return w
+
+
 # physics models on the graph (semiconductor_3d.c:4241-4293 Lombardi / Coulomb / saturation,
 # 1249-1271 walls and MLDA, 4486-4523 impact ionisation, 1285-1349 tunnelling paths, 1376-1416
 # metal-contact columns), each against the reference's graph path
 MODEL_CASES = {
     "tun_moscap": lambda L, s: D.graph_moscap(L, models=1 | 32, solver=s),
+    "traps": graph_trapped_diode,
+    "sic_traps_incomplete": graph_sic_traps_incomplete,
     "tun_mos_stack": graph_mos_stack,
     "mos_lombardi_mlda": lambda L, s: D.graph_nmosfet(L, solver=s),
     "mos_lombardi_mlda_diag": lambda L, s: D.graph_nmosfet(L, solver=s, diag=0.3),
@@ -173,7 +206,7 @@ def model_sweep(L, case, tight):
     ok0 = D.start_sweep(L, w, s)
     psi = []
     V, I, F, conv = D.run_sweep(L, w, s, on_point=lambda q, v: psi.append(D.field(L, 0, w.shape).ravel()))
-    maps = {q: D.field(L, q, w.shape).ravel() for q in (1, 2, 10, 11, 14, 30, 33)}
+    maps = {q: D.field(L, q, w.shape).ravel() for q in (1, 2, 10, 11, 14, 30, 31, 33, 34)}
     return ok0, I, F, conv, np.array(psi), maps
 
 
@@ -201,7 +234,7 @@ def test_graph_models_match_reference(lib, case, monkeypatch):
     assert np.abs(g1[4] - r1[4]).max() <= 1e-6
     rm = r1[5]
     scale_c = rm[1] + rm[2] + np.abs(rm[14])                 # local charge scale n + p + |Nd - Na|
-    for q in (10, 11, 30, 33):
+    for q in (10, 11, 30, 31, 33, 34):
         a, b = g1[5][q], r1[5][q]
         assert np.array_equal(np.isfinite(a), np.isfinite(b)), f"map {q}"
         m = np.isfinite(b)
