@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison steps")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor step")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuner)")
-    ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "finfet", "diodes64"],
+    ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "finfet", "graph_mosfet", "diodes64"],
                     help="nmosfet: the Id-Vg workload (default); finfet: the tri-gate FinFET Id-Vg family "
                          "(96x96x64, 5 drain biases); diodes64: the 64 pn-diode variants batch")
     ap.add_argument("--workers", type=int, default=0, help="diodes64: concurrent host threads (0: one per variant)")
@@ -213,6 +213,11 @@ class Clocks:
 WORKLOADS = {
     "nmosfet": {"mesh": (120, 80, 60), "build": lambda lib, n: D.nmosfet(lib, n=n)},
     "finfet": {"mesh": (96, 96, 64), "build": lambda lib, n: D.finfet(lib, n=n)},
+    # the n-MOSFET's device given as a general (graph) mesh: the graph path's ELL kernels and
+    # aggregation multigrid (FP64; no launch-shape tuning or learned seed on graphs)
+    "graph_mosfet": {"mesh": (120, 80, 60),
+                     "build": lambda lib, n: D.graph_nmosfet(lib, n=n, models=4, vds=(0.05, 1.0), vg_max=1.2,
+                                                             dvg=0.05, h0=0.5e-9)},
 }
 WL = "nmosfet"
 
@@ -415,7 +420,8 @@ def run_b200(a, dist):
     lib = S.load()
     lib.b200x_set_device(dist.local)
     nsw = 5 if WL == "finfet" else 2          # the drain biases of the workload, one sweep each
-    prec = 1 if a.precision == "refined" else 0
+    graph = WL.startswith("graph")
+    prec = 1 if a.precision == "refined" and not graph else 0
 
     def make(p):
         return [Sweeper(lib, mesh, si, dist.local, p) for si in sweep_order(nsw, dist.rank)]
@@ -431,7 +437,7 @@ def run_b200(a, dist):
         return (sum(s.npts for s in ws), sum(s.conv for s in ws), max(s.dev_s for s in ws), wall)
 
     tune = None
-    if not a.no_autotune:                     # launch shapes, one instance at a time (untimed)
+    if not a.no_autotune and not graph:       # launch shapes, one instance at a time (untimed)
         for s in workers:
             s.prepare()
             us = lib.api3b_autotune(2)
@@ -499,7 +505,7 @@ def run_b200(a, dist):
     # the learned predictor: trained (untimed) on this device's own solutions at gate
     # voltages half a step off the workload's, then one step of the workload seeded by it
     learned = None
-    if not a.no_learned:
+    if not a.no_learned and not graph:
         learned = learned_step(a, lib, workers, step, cur, gummel, dist)
     T = dist.max(tot_dev)
     pts_all = dist.sum(tot_pts)
@@ -510,7 +516,11 @@ def run_b200(a, dist):
         hbm, pk_kind = peaks()
         roof = None
         kernels = None
-        if prof:
+        if prof and graph:                    # per-class byte counts are the tensor stencil's
+            tot_ms = sum(r[1] for r in prof) or 1.0
+            kernels = {r[0]: {"ms": round(r[1], 2), "share": round(r[1] / tot_ms, 4), "launches": r[2]}
+                       for r in sorted(prof, key=lambda r: -r[1]) if r[2] > 0}
+        elif prof:
             tot_ms = sum(r[1] for r in prof) or 1.0
             top = max(prof, key=lambda r: r[1])
             ach = top[3] / (top[1] / 1e3) / 1e9 if top[1] > 0 else 0.0
@@ -534,7 +544,8 @@ def run_b200(a, dist):
             "data": "synthetic (device built from the workload definition)",
             "config": dict({"workload": workload_name(mesh),
                             "nodes": w.N, "points_per_step": npts_step}, **workload_config(w),
-                           **{"solver": list(D.GUI_SOLVER), "precision": a.precision, "launch_shapes": tune,
+                           **{"solver": list(D.GUI_SOLVER), "precision": "fp64" if graph else a.precision,
+                              "launch_shapes": tune,
                               "parallelism": f"replicas{dist.world}, {nsw} concurrent sweeps per GPU "
                                              "(instance + stream each)",
                               "l2": f"state of {w.N} nodes (~{w.N * 760 / 1e9:.2f} GB) exceeds the 126 MB L2; "

@@ -295,13 +295,14 @@ def graph_moscap(lib, models=7 | 32, solver=GUI_SOLVER, diag=0.0):
 
 def graph_nmosfet(lib, n=(24, 12, 3), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e17, Nsd=1e20, sigma=20e-9,
                   sd_len=100e-9, tox=2e-9, phi_m=4.6, models=4 | 8 | 16, solver=GUI_SOLVER, vd=0.05, vg_max=1.0,
-                  dvg=0.25, h0=2e-9, diag=0.0, Nox=0.0, material=None):
+                  dvg=0.25, h0=2e-9, diag=0.0, Nox=0.0, material=None, vds=None):
     """The n-MOSFET of nmosfet() on a general (graph) mesh built from its tensor mesh
     (tensor_graph, optional diagonal edges): contacts as node lists on the y = 0 surface
     (source, drain, the Robin face gate) and the back face (body), and the interface walls
     the host supplies on a graph (api3_set_walls): every semiconductor node under the gate
     has the gate surface as its wall - its distance and its cell's range from it - the
-    walls the tensor path's scan finds for a face gate."""
+    walls the tensor path's scan finds for a face gate.  One gate sweep per drain bias of
+    `vds` (default: the single bias vd)."""
     lib.api3_init()
     xs = np.linspace(0.0, Lx, n[0])
     ys = graded_axis(Ly, n[1], h0)
@@ -350,7 +351,8 @@ def graph_nmosfet(lib, n=(24, 12, 3), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e1
     npts = int(round(vg_max / dvg)) + 1
     V = np.round(np.linspace(0.0, vg_max, npts), 12)
     return Workload("graph_nmosfet", (N, 1, 1), {"source": cs, "drain": cd, "gate": cg, "body": cb},
-                    [{"fixed": {"drain": vd, "source": 0.0, "body": 0.0}, "swept": "gate", "V": V}],
+                    [{"fixed": {"drain": v, "source": 0.0, "body": 0.0}, "swept": "gate", "V": V}
+                     for v in (vds if vds is not None else (vd,))],
                     {"models": models, "diag": diag, "tox_m": tox})
 
 
