@@ -20,6 +20,7 @@
 // the assembly kernels write, so one set of kernels serves all levels.
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "device_common.cuh"
@@ -611,12 +612,11 @@ void gmg_setup(Inst &d, const Ctx &c, int qsign, const double *w) {
     if (z.inv) {
         const int smem = z.N <= GMG_SMEM_MAX;
         const size_t bytes = smem ? (size_t)z.N * z.N * sizeof(double) : 0;
-        static bool attr = false;
-        if (!attr) {
+        static std::once_flag attr;          // instances may set up from several host threads
+        std::call_once(attr, [] {
             cudaFuncSetAttribute(k_gmg_coarse_setup, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  GMG_SMEM_MAX * GMG_SMEM_MAX * (int)sizeof(double));
-            attr = true;
-        }
+        });
         ss::g_launches++;
         ss::t_launches++;
         if (ss::g_prof_on) ss::prof_begin(PF_COARSE_SETUP, c.st);
