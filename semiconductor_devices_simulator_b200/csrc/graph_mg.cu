@@ -404,6 +404,10 @@ std::vector<LevelBuild> plan(int N, const std::vector<int> &rp, const std::vecto
 }  // namespace
 
 void gmg_free(Inst &d) {
+    for (auto &g : d.g.gcyc)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    d.g.gcyc.clear();
+    d.g.gcyc_off = false;
     if (d.g.gmgblock) cudaFree(d.g.gmgblock);
     d.g.gmgblock = nullptr;
     d.g.glev.clear();
@@ -628,9 +632,49 @@ void gmg_setup(Inst &d, const Ctx &c, int qsign, const double *w) {
 }
 
 // z = M^-1 r: one V-cycle (gvcycle, semiconductor_3d.c:2654-2680), or the mesh level's
-// D-ILU alone (the reference's fallback after a diverged multigrid solve)
+// D-ILU alone (the reference's fallback after a diverged multigrid solve).  A V-cycle is
+// ~100 dependent launches of a few microseconds, so each operand set (the Krylov vectors r,
+// z, the row weights, ILU alone or not) is captured once as a CUDA graph and replayed; the
+// kernels' arguments - the level views, the mesh level's matrix arrays, the vectors - stay
+// fixed for the instance until the hierarchy is rebuilt, which drops the graphs.  With the
+// per-launch profiler on, or graphs switched off, the launches go out one by one.
 void gmg_apply(Inst &d, const Ctx &c, const double *r, double *z, const double *w, bool ilu_only) {
-    vcycle(d, c, 0, r, z, w, ilu_only);
+    if (g_prof_on || !g_use_graphs || d.g.gcyc_off) {
+        vcycle(d, c, 0, r, z, w, ilu_only);
+        return;
+    }
+    bind_level0(d);
+    GmgCycle *hit = nullptr;
+    for (auto &g : d.g.gcyc)
+        if (g.r == r && g.z == z && g.w == w && g.ilu_only == ilu_only) { hit = &g; break; }
+    if (!hit) {
+        GmgCycle g;
+        g.r = r; g.z = z; g.w = w; g.ilu_only = ilu_only;
+        const unsigned long long l0 = t_launches;
+        cudaGraph_t gr = nullptr;
+        bool ok = cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            vcycle(d, c, 0, r, z, w, ilu_only);
+            ok = cudaStreamEndCapture(c.st, &gr) == cudaSuccess && gr != nullptr;
+        }
+        g.launches = t_launches - l0;
+        g_launches -= g.launches;                  // captured, not run
+        t_launches -= g.launches;
+        if (ok) ok = cudaGraphInstantiate(&g.exec, gr, 0) == cudaSuccess;
+        if (gr) cudaGraphDestroy(gr);
+        if (!ok) {                                 // run it the plain way from now on
+            cudaGetLastError();
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            d.g.gcyc_off = true;
+            vcycle(d, c, 0, r, z, w, ilu_only);
+            return;
+        }
+        d.g.gcyc.push_back(g);
+        hit = &d.g.gcyc.back();
+    }
+    cudaGraphLaunch(hit->exec, c.st);
+    g_launches += hit->launches;
+    t_launches += hit->launches;
 }
 
 int gmg_levels(const Inst &d) { return (int)d.g.glev.size(); }

@@ -215,7 +215,7 @@ void gpu_free(Inst &d) {
     if (d.g.trblock) cudaFree(d.g.trblock);
     if (d.g.coblock) cudaFree(d.g.coblock);
     if (d.g.gblock) cudaFree(d.g.gblock);
-    if (d.g.gmgblock) cudaFree(d.g.gmgblock);
+    gmg_free(d);
     if (d.g.seedw) cudaFree(d.g.seedw);
     if (d.g.st) cudaStreamDestroy(d.g.st);
     d.g = Gpu();

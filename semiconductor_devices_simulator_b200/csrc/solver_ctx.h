@@ -42,6 +42,15 @@ struct GraphHost {
     int nue = 0, D = 0;
 };
 
+// one V-cycle of the graph multigrid captured as a CUDA graph: its operands and executable
+struct GmgCycle {
+    const double *r = nullptr, *w = nullptr;
+    double *z = nullptr;
+    bool ilu_only = false;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;   // kernels in the graph
+};
+
 // a level of the graph multigrid on the host: the device view and its colour classes
 struct GLevHost {
     GLev dv{};
@@ -72,6 +81,8 @@ struct Gpu {
     void *gblock = nullptr;      // graph-mesh arrays (ELL edges, colours, gradients, edge mobilities)
     void *gmgblock = nullptr;    // graph multigrid levels (one allocation)
     std::vector<GLevHost> glev;  // graph multigrid hierarchy, level 0 = the mesh
+    std::vector<GmgCycle> gcyc;  // its V-cycles captured as CUDA graphs (per operand set)
+    bool gcyc_off = false;       // capture failed once: launch the V-cycle directly
     void *trblock = nullptr;     // deep-level trap entries (CSR per node) and species
     void *coblock = nullptr;     // Coulomb interface entries and every node's nearest one
     void *teblock = nullptr;     // metal-contact entries, columns and per-node arrays (one allocation)
