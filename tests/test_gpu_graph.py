@@ -253,3 +253,39 @@ def test_graph_models_match_reference(lib, case, monkeypatch):
     tol0 = np.maximum(np.maximum(rd * np.abs(r0[1]), r0[2]), own)
     assert (np.abs(g0[1] - r0[1]) <= tol0).all(), f"default currents\n{g0[1]}\n{r0[1]}"
     assert np.abs(g0[4] - r0[4]).max() <= 1e-6
+
+
+def test_graph_batched_resolve_equals_sequential(lib, monkeypatch):
+    """Bias vectors around an operating point of the graph diode (diagonal edges), solved at
+    once by api3b_resolve_batch - worker instances, each with its own copy of the mesh and
+    its own multigrid hierarchy - give the currents of sequential api3_resolve calls from the
+    restored state."""
+    set_env(monkeypatch, 0)
+    w = D.graph_pn_diode(lib, diag=0.3, vmax=0.4)
+    s = w.sweeps[0]
+    assert D.start_sweep(lib, w, s)
+    D.run_sweep(lib, w, s)
+    nc = lib.api3_get_ncon()
+    base = np.array([lib.api3_get_contact_Vsolved(c) for c in range(nc)])
+    st = [np.zeros(w.N) for _ in range(3)]
+    assert lib.api3_get_state(*(dptr(a) for a in st))
+    a = w.contacts["anode"]
+    Vs = []
+    for dv in (0.01, -0.02, 0.05, 0.1):
+        v = base.copy()
+        v[a] += dv
+        Vs.append(v)
+    Vs = np.ascontiguousarray(Vs)
+    Ib = np.zeros((len(Vs), nc))
+    conv = np.zeros(len(Vs), np.int32)
+    try:
+        assert lib.api3b_resolve_batch(len(Vs), dptr(Vs), dptr(Ib), None, iptr(conv), 2) == len(Vs)
+    finally:
+        lib.api3b_resolve_batch_free()
+    for j, v in enumerate(Vs):
+        assert lib.api3_set_state(*(dptr(x) for x in st))
+        for c in range(nc):
+            lib.api3_set_contact_V(c, float(v[c]))
+        assert lib.api3_resolve()
+        Iq = np.array([lib.api3_get_contact_I(c) for c in range(nc)])
+        assert np.allclose(Ib[j], Iq, rtol=1e-5, atol=1e-22), (j, Ib[j], Iq)
