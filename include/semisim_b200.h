@@ -264,7 +264,8 @@ int api3b_seed_nparam(void);
      mode 0: default shapes; 1: tune now; 2: reuse the shapes cached for this mesh shape
      and precision, tuning when there are none.  Call after the instance's first solve,
      with no other GPU work of the process running.  Returns the chosen V-cycle time in
-     microseconds (0 for mode 0, -1 before the first solve).
+     microseconds (0 for mode 0, -1 before the first solve or on a general (graph) mesh,
+     whose multigrid has no tunable shapes).
    api3b_tune_get: the shapes in use (zcap: most row blocks per pass; may be null); returns
    1 when they came from the tuner. */
 double api3b_autotune(int mode);

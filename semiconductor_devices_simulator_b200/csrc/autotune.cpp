@@ -52,6 +52,7 @@ double api3b_autotune(int mode) {
         return 0.0;
     }
     if (!d.g.ready || d.g.mg.maxlev < 1) return -1.0;
+    if (d.unstr) return -1.0;                  // a graph mesh has no tensor multigrid to tune
     const int mixed = use_mixed(d);
     const auto key = std::make_tuple(d.Nx, d.Ny, d.Nz, mixed);
     if (mode == 2) {
