@@ -68,13 +68,21 @@ static double *hx_arr(int which){
    16..21: face mobility fmu[0..5] (semiconductor_3d.c:256) */
 int hx_get(int which, double *out){
     size_t N=NN(&gdev);
-    if(which>=16 && which<22){ for(size_t k=0;k<N;k++) out[k]=(double)gdev.fmu[which-16][k]; return 1; }
+    if(which>=16 && which<22){                   /* tensor meshes only (a graph keeps edge mobilities) */
+        if(gdev.unstr) return 0;
+        for(size_t k=0;k<N;k++) out[k]=(double)gdev.fmu[which-16][k];
+        return 1;
+    }
     double *a=hx_arr(which); if(!a) return 0;
     memcpy(out,a,N*sizeof(double)); return 1;
 }
 int hx_set(int which, const double *in){
     size_t N=NN(&gdev);
-    if(which>=16 && which<22){ for(size_t k=0;k<N;k++) gdev.fmu[which-16][k]=(mu_t)in[k]; return 1; }
+    if(which>=16 && which<22){
+        if(gdev.unstr) return 0;
+        for(size_t k=0;k<N;k++) gdev.fmu[which-16][k]=(mu_t)in[k];
+        return 1;
+    }
     double *a=hx_arr(which); if(!a) return 0;
     memcpy(a,in,N*sizeof(double)); return 1;
 }
@@ -101,7 +109,11 @@ double hx_poisson_eval(const double *phi, int build, double *F, double *A7, doub
 void hx_apply_bc(void){ double Va[NC_MAX]; hx_Va(Va); set_vrange(&gdev,Va); apply_bc(&gdev,Va); }
 void hx_rebuild_np(void){ rebuild_np(&gdev); }
 void hx_mob0_init(void){ mob0_init(&gdev); }
-void hx_upd_mob(void){ upd_mob_ref(&gdev,gdev.phi_n,gdev.phi_p); }
+/* the edge mobilities of either mesh (upd_mob, semiconductor_3d.c:3007-3008 dispatch) */
+void hx_upd_mob(void){
+    if(gdev.unstr) upd_mob_ref_g(&gdev,gdev.phi_n,gdev.phi_p);
+    else upd_mob_ref(&gdev,gdev.phi_n,gdev.phi_p);
+}
 void hx_clamp_qf(void){ clamp_qf(&gdev); }
 double hx_vlo(void){ return gdev.vlo; }
 double hx_vhi(void){ return gdev.vhi; }
@@ -290,4 +302,33 @@ int hx_gmg_level(int L, int *n_out, int *nnz_out, int *rp, int *cj, int *agg){
     if(cj) for(int e=0;e<v->rp[n];e++) cj[e]=v->cj[e];
     if(agg && L<nl-1 && v->agg) for(int i=0;i<n;i++) agg[i]=v->agg[i];
     return nl;
+}
+
+/* the graph of a general-mesh device (api3_set_mesh_graph, semiconductor_3d.c:981-1041):
+   CSR rp (N + 1), cj, undirected edge id ue, lengths h and dual areas ar (E each), node
+   volumes (N); null buffers are skipped.  Returns E (0 without a graph device). */
+int hx_graph(int *rp, int *cj, int *ue, double *h, double *ar, double *vol){
+    if(!gdev.allocated || !gdev.unstr) return 0;
+    size_t N=NN(&gdev); int E=gdev.nE;
+    if(rp) for(size_t k=0;k<=N;k++) rp[k]=gdev.grp[k];
+    if(cj) memcpy(cj,gdev.gcol,(size_t)E*sizeof(int));
+    if(ue) memcpy(ue,gdev.gue,(size_t)E*sizeof(int));
+    if(h) memcpy(h,gdev.gh,(size_t)E*8);
+    if(ar) memcpy(ar,gdev.ga,(size_t)E*8);
+    if(vol) memcpy(vol,gdev.gvol,N*8);
+    return E;
+}
+/* the off-diagonals of the last assembled graph system (poisson_core_g / cont_assemble_g,
+   semiconductor_3d.c:4181-4217, 4314-4351), per directed edge; returns E */
+int hx_graph_vals(double *gval){
+    if(!gdev.allocated || !gdev.unstr) return 0;
+    if(gval) memcpy(gval,gdev.gval,(size_t)gdev.nE*8);
+    return gdev.nE;
+}
+/* edge mobilities of the graph (upd_mob_ref_g, semiconductor_3d.c:4241-4293) per undirected
+   edge; returns their number */
+int hx_graph_mob(double *mun, double *mup){
+    if(!gdev.allocated || !gdev.unstr) return 0;
+    for(int e=0;e<gdev.nUE;e++){ if(mun) mun[e]=(double)gdev.gmu[0][e]; if(mup) mup[e]=(double)gdev.gmu[1][e]; }
+    return gdev.nUE;
 }

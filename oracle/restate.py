@@ -609,3 +609,147 @@ def ph0(dev, qsign):
     val = dev["phin"] / VT if qsign > 0 else -dev["phip"] / VT
     none = (dev["kind"] != K_SEMI) | car_fix(dev)
     return np.where(none, PH_NONE, val)
+
+
+# ------------------------------------------------------------------ general (graph) meshes
+def graph_rows(dev):
+    """Row index of every directed edge of the CSR graph."""
+    return np.repeat(np.arange(len(dev["g_rp"]) - 1), np.diff(dev["g_rp"]))
+
+
+def poisson_eval_g(dev, phi):
+    """F, diagonal, off-diagonals per directed edge, sc and ||F/sc|| of the Poisson system on
+    a graph (poisson_core_g, semiconductor_3d.c:4181-4217, with the Robin gates of
+    poisson_eval, :2732-2789).  Edge terms are summed row by row in CSR order."""
+    rp, cj, h, ar = dev["g_rp"], dev["g_cj"], dev["g_h"], dev["g_ar"]
+    N = len(rp) - 1
+    row = graph_rows(dev)
+    kind, con = dev["kind"], dev["con"]
+    isdir = con != 0
+    eps = matp(dev, "eps_r") * EPS0
+    ek, eb = eps[row], eps[cj]
+    cf = (2.0 * ek * eb / (ek + eb)) * ar / h
+    F = np.zeros(N)
+    dg = np.zeros(N)
+    for k in range(N):                               # CSR order within a row, as the reference sums
+        acc = 0.0
+        d = 0.0
+        for e in range(rp[k], rp[k + 1]):
+            acc += cf[e] * (phi[cj[e]] - phi[k])
+            d += cf[e]
+        F[k] = acc
+        dg[k] = d
+    gval = np.where(isdir[cj], 0.0, -cf)
+    vol = dev["g_vol"]
+    semi = kind == K_SEMI
+    n = nK(dev, phi, dev["phin"])
+    p = pK(dev, phi, dev["phip"])
+    VT = matp(dev, "VT")
+    Np, dNp, Nm, dNm = ion_eval(dev, n, p)
+    F += np.where(semi, vol * Q * (p - n + Np - Nm + dev["Nf"]), vol * Q * dev["Nf"])
+    dg += np.where(semi, vol * Q * ((n + p) / VT - dNp + dNm), 0.0)
+    sc = dg.copy()
+    F[isdir] = 0.0
+    dg[isdir] = 1.0
+    sc[isdir] = 1.0
+    gval[isdir[row]] = 0.0
+    for r in range(len(dev["rob_k"])):
+        k, c = int(dev["rob_k"][r]), int(dev["rob_c"][r])
+        tox = dev["con_tox"][c] if dev["con_tox"][c] > 0 else 10e-9
+        Cox = EPS_OX / tox
+        pm = dev["con_pm"][c] if dev["con_pm"][c] > 0 else dev["Cref"]
+        VG = dev["con_V"][c] + dev["Cref"] - pm
+        F[k] += dev["rob_A"][r] * (Cox * (VG - phi[k]) + dev["con_qox"][c])
+        dg[k] += Cox * dev["rob_A"][r]
+        sc[k] = dg[k]
+    return F, dg, gval, sc, float(np.sqrt(np.sum((F / sc) ** 2)))
+
+
+def upd_mob_g(dev):
+    """Edge mobilities per undirected edge (upd_mob_ref_g, semiconductor_3d.c:4241-4293):
+    the mean of the node low-field mobilities projected on the edge for a hexagonal crystal,
+    velocity saturation with the harmonic-mean driving field (models bit 2); no surface
+    model or metal contacts in scope here."""
+    rp, cj, ue, h = dev["g_rp"], dev["g_cj"], dev["g_ue"], dev["g_h"]
+    row = graph_rows(dev)
+    semi = dev["kind"] == K_SEMI
+    nue = int(ue.max()) + 1 if len(ue) else 0
+    mun, mup = np.zeros(nue), np.zeros(nue)
+    up = cj > row                                    # each undirected edge once, from its lower node
+    k, kp, e_ue, hh = row[up], cj[up], ue[up], h[up]
+    mn = 0.5 * (dev["mun"][k] + dev["mun"][kp])
+    mp = 0.5 * (dev["mup"][k] + dev["mup"][kp])
+    pos = dev["g_pos"].reshape(-1, 3)
+    ax = int(dev["caxis"])
+    for which, mu in (("ani_n", mn), ("ani_p", mp)):
+        a = matp(dev, which)[k]
+        if ax >= 0:
+            dv = pos[kp] - pos[k]
+            L2 = np.sum(dv * dv, axis=1)
+            f = np.where((a > 0) & (a != 1.0) & (L2 > 0), 1.0 + (a - 1.0) * dv[:, ax] ** 2 / np.where(L2 > 0, L2, 1.0), 1.0)
+            mu *= f
+    if dev["models"] & 4:
+        dps = dev["phi"][kp] - dev["phi"][k]
+        Fn = heat_field(dev["phin"][kp] - dev["phin"][k], dps, hh)
+        Fp = heat_field(dev["phip"][kp] - dev["phip"][k], dps, hh)
+        sn = mob_hf(mn, Fn, matp(dev, "vsat_n")[k], matp(dev, "beta_n")[k])
+        sp = mob_hf(mp, Fp, matp(dev, "vsat_p")[k], matp(dev, "beta_p")[k])
+        mn = mn + 1.0 * (sn - mn)
+        mp = mp + 1.0 * (sp - mp)
+    ok = semi[k] & semi[kp]
+    mun[e_ue] = np.where(ok, mn, 0.0)
+    mup[e_ue] = np.where(ok, mp, 0.0)
+    return mun, mup
+
+
+def cont_assemble_g(dev, hole, gmu_n, gmu_p):
+    """Scaled Scharfetter-Gummel system for u = c/s on a graph: diagonal, off-diagonals per
+    directed edge, rhs, sc, dsc (cont_assemble_g, semiconductor_3d.c:4314-4351)."""
+    rp, cj, ue, h, ar = dev["g_rp"], dev["g_cj"], dev["g_ue"], dev["g_h"], dev["g_ar"]
+    N = len(rp) - 1
+    row = graph_rows(dev)
+    semi = dev["kind"] == K_SEMI
+    fix = car_fix(dev)
+    car = dev["p"] if hole else dev["n"]
+    VT = matp(dev, "VT")
+    lc = lnvK(dev) if hole else lncK(dev)
+    mu = gmu_p if hole else gmu_n
+    ok = semi[row] & semi[cj]
+    dl = lc[cj] - lc[row]
+    D = (dev["phi"][cj] - dev["phi"][row]) / VT[row] + (-dl if hole else dl)
+    g = ar * mu[ue] * VT[row] / h
+    self_ = g * (bernoulli(D) if hole else bernoulli(-D))
+    nb = g * (bernoulli(-D) if hole else bernoulli(D))
+    gval = np.where(ok & ~fix[cj], -nb * np.maximum(car[cj], NFLOOR), 0.0)
+    dg = np.zeros(N)
+    b = np.zeros(N)
+    for k in range(N):                               # CSR order within a row
+        d = 0.0
+        bb = 0.0
+        for e in range(rp[k], rp[k + 1]):
+            if not ok[e]:
+                continue
+            d += self_[e]
+            if fix[cj[e]]:
+                bb += nb[e] * car[cj[e]]
+        dg[k] = d
+        b[k] = bb
+    R, dRn, dRp = recomb(dev, dev["n"], dev["p"])
+    dR = np.maximum(dRp if hole else dRn, 0.0)
+    vol = dev["g_vol"]
+    dg += vol * dR
+    b += vol * (dR * car - R)
+    sk = np.maximum(car, NFLOOR)
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        w = 1.0 / (dg * sk)
+    gval = gval * w[row]
+    rhs = b * w
+    diag = np.ones(N)
+    sc = sk.copy()
+    dsc = dg * sk
+    ident = ~semi | fix
+    gval[ident[row]] = 0.0
+    rhs[ident] = np.where(semi[ident], 1.0, 0.0)
+    sc[ident] = np.where(semi[ident], car[ident], 0.0)
+    dsc[ident] = 0.0
+    return diag, gval, rhs, sc, dsc

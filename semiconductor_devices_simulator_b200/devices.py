@@ -216,7 +216,7 @@ def graph_pn_diode(lib, n=(12, 6, 5), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj
     V = np.round(np.linspace(0.0, vmax, npts), 12)
     return Workload("graph_pn_diode" if graph else "pn_diode", (N, 1, 1) if graph else n,
                     {"anode": ca, "cathode": cc}, [{"fixed": {"cathode": 0.0}, "swept": "anode", "V": V}],
-                    {"models": models, "diag": diag})
+                    {"models": models, "diag": diag, "pos": pos if graph else None})
 
 
 def graph_schottky_diode(lib, n=(40, 3, 3), L=1e-6, ND=1e16, phi_m=4.8, models=7 | 64, h0=2e-9,
@@ -353,7 +353,7 @@ def graph_nmosfet(lib, n=(24, 12, 3), Lx=500e-9, Ly=200e-9, Lz=100e-9, Nbody=1e1
     return Workload("graph_nmosfet", (N, 1, 1), {"source": cs, "drain": cd, "gate": cg, "body": cb},
                     [{"fixed": {"drain": v, "source": 0.0, "body": 0.0}, "swept": "gate", "V": V}
                      for v in (vds if vds is not None else (vd,))],
-                    {"models": models, "diag": diag, "tox_m": tox})
+                    {"models": models, "diag": diag, "tox_m": tox, "pos": pos})
 
 
 def graded_axis(L, n, h0):

@@ -1,0 +1,137 @@
+"""The CPU restatement of the general-mesh kernels (oracle/restate.py: poisson_eval_g,
+upd_mob_g, cont_assemble_g) against the reference core's graph path, run live through the
+oracle harness on graph devices at a converged bias with seeded perturbations: the Poisson
+residual, diagonal and per-edge off-diagonals, the edge mobilities with velocity
+saturation, and both scaled Scharfetter-Gummel systems.  Host only: no GPU needed."""
+import ctypes
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import make_golden as MG  # noqa: E402
+from oracle import restate as R  # noqa: E402
+from semiconductor_devices_simulator_b200 import abi, devices as D  # noqa: E402
+from semiconductor_devices_simulator_b200.abi import dptr, iptr  # noqa: E402
+
+_IP, _DP = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+HXG = dict(MG.HX, hx_graph=(ctypes.c_int, [_IP, _IP, _IP, _DP, _DP, _DP]),
+           hx_graph_vals=(ctypes.c_int, [_DP]), hx_graph_mob=(ctypes.c_int, [_DP, _DP]))
+
+CASES = {
+    # velocity saturation on, a Robin face gate, source / drain / body node lists
+    "mosfet": (lambda L: D.graph_nmosfet(L, n=(16, 12, 4), models=4 | 1 | 2), {"gate": 0.8, "drain": 0.3}),
+    # diagonal edges (no tensor product), constant-mobility-free Masetti silicon
+    "diode_diag": (lambda L: D.graph_pn_diode(L, diag=0.3, models=7), {"anode": 0.4}),
+}
+
+
+def harness():
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_harness.so")
+    if not os.path.exists(path):
+        pytest.skip("reference core not built (make -C oracle)")
+    return abi.bind(ctypes.CDLL(path), HXG)
+
+
+def state(lib, N):
+    """Node state of a graph device (no face mobilities there)."""
+    return {k: MG.get(lib, q, N) for k, q in (("phi", MG.W_PHI), ("phin", MG.W_PHIN), ("phip", MG.W_PHIP),
+                                               ("n", MG.W_N), ("p", MG.W_P), ("mun", MG.W_MUN), ("mup", MG.W_MUP))}
+
+
+def close(a, b, rtol, atol=0.0):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    err = np.abs(a - b)
+    tol = atol + rtol * np.maximum(np.abs(a), np.abs(b))
+    assert np.all(err <= tol), f"max err {err.max():.3e} (tol {tol[np.argmax(err - tol)]:.3e})"
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def dumped(request):
+    lib = harness()
+    build, bias = CASES[request.param]
+    w = build(lib)
+    lib.api3_set_verbose(0)
+    for name, v in bias.items():
+        lib.api3_set_contact_V(w.contacts[name], v)
+    assert lib.api3_solve()
+    rec = MG.device_record(lib, w)
+    N = w.N
+    E = lib.hx_graph(None, None, None, None, None, None)
+    g_rp, g_cj, g_ue = np.zeros(N + 1, np.int32), np.zeros(E, np.int32), np.zeros(E, np.int32)
+    g_h, g_ar, g_vol = np.zeros(E), np.zeros(E), np.zeros(N)
+    lib.hx_graph(iptr(g_rp), iptr(g_cj), iptr(g_ue), dptr(g_h), dptr(g_ar), dptr(g_vol))
+    pos = np.asarray(w.info["pos"], float)           # the builder's node positions
+    crec = np.zeros((lib.api3_get_ncon(), 6))
+    for c in range(crec.shape[0]):
+        lib.hx_contact(c, dptr(crec[c]))
+    lib.hx_mob0_init()
+    lib.hx_apply_bc()
+    st = state(lib, N)
+    rng = np.random.default_rng(7)
+    semi = rec["kind"] == 0
+    free = semi & (rec["con"] == 0)
+    phi = st["phi"] + np.where(rec["con"] == 0, rng.normal(0, 2e-3, N), 0.0)
+    phin = st["phin"] + np.where(free, rng.normal(0, 5e-3, N), 0.0)
+    phip = st["phip"] + np.where(free, rng.normal(0, 5e-3, N), 0.0)
+    lib.hx_set(MG.W_PHI, dptr(phi)); lib.hx_set(MG.W_PHIN, dptr(phin)); lib.hx_set(MG.W_PHIP, dptr(phip))
+    lib.hx_clamp_qf()
+    lib.hx_rebuild_np()
+    lib.hx_upd_mob()
+    nue = lib.hx_graph_mob(None, None)
+    mun, mup = np.zeros(nue), np.zeros(nue)
+    lib.hx_graph_mob(dptr(mun), dptr(mup))
+    ps = state(lib, N)
+    out = {"mob": (mun, mup)}
+    F, A7, sc = np.zeros(N), np.zeros(7 * N), np.zeros(N)
+    nrm = lib.hx_poisson_eval(dptr(ps["phi"]), 1, dptr(F), dptr(A7), dptr(sc))
+    gv = np.zeros(E)
+    lib.hx_graph_vals(dptr(gv))
+    out["pois"] = (F, A7[:N].copy(), gv.copy(), sc, nrm)
+    for hole in (0, 1):
+        A7, rhs, sc, dsc = np.zeros(7 * N), np.zeros(N), np.zeros(N), np.zeros(N)
+        lib.hx_cont_assemble(hole, dptr(A7), dptr(rhs), dptr(sc), dptr(dsc))
+        lib.hx_graph_vals(dptr(gv))
+        out[f"cont{hole}"] = (A7[:N].copy(), gv.copy(), rhs, sc, dsc)
+    dev = dict(rec, **{k: ps[k] for k in ("phi", "phin", "phip", "n", "p", "mun", "mup")})
+    dev.update(models=int(w.info["models"]), caxis=1, ref_mat=0, mat=np.zeros(N, np.int64),
+               g_rp=g_rp, g_cj=g_cj, g_ue=g_ue, g_h=g_h, g_ar=g_ar, g_vol=g_vol, g_pos=pos,
+               con_V=crec[:, 0], con_pm=crec[:, 1], con_tox=crec[:, 2], con_qox=crec[:, 3])
+    return dev, out
+
+
+def test_poisson_graph(dumped):
+    dev, out = dumped
+    F, dg, gval, sc, nrm = R.poisson_eval_g(dev, dev["phi"])
+    Fr, dgr, gvr, scr, nrr = out["pois"]
+    close(F, Fr, rtol=1e-11, atol=1e-12 * np.abs(Fr).max())
+    close(dg, dgr, rtol=1e-12)
+    close(gval, gvr, rtol=1e-12)
+    close(sc, scr, rtol=1e-12)
+    close(nrm, nrr, rtol=1e-9)
+
+
+def test_edge_mobility_graph(dumped):
+    dev, out = dumped
+    mun, mup = R.upd_mob_g(dev)
+    close(mun, out["mob"][0], rtol=1e-12)
+    close(mup, out["mob"][1], rtol=1e-12)
+
+
+@pytest.mark.parametrize("hole", [0, 1])
+def test_cont_assemble_graph(dumped, hole):
+    dev, out = dumped
+    mun, mup = out["mob"]
+    dg, gval, rhs, sc, dsc = R.cont_assemble_g(dev, hole, mun, mup)
+    dgr, gvr, rhr, scr, dsr = out[f"cont{hole}"]
+    close(dg, dgr, rtol=0.0)
+    close(gval, gvr, rtol=1e-10, atol=1e-300)
+    close(rhs, rhr, rtol=1e-10, atol=1e-12 * np.abs(rhr).max())
+    close(sc, scr, rtol=1e-13)
+    close(dsc, dsr, rtol=1e-10, atol=1e-300)
