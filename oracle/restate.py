@@ -753,3 +753,34 @@ def cont_assemble_g(dev, hole, gmu_n, gmu_p):
     sc[ident] = np.where(semi[ident], car[ident], 0.0)
     dsc[ident] = 0.0
     return diag, gval, rhs, sc, dsc
+
+
+def terminal_currents_g(dev, ncon, gmu_n, gmu_p):
+    """Contact fluxes I, scales S and electron parts In on a graph: the Scharfetter-Gummel
+    flux of every edge from a contact's semiconductor node to a semiconductor node outside
+    that contact (terminal_flux_g and face_flux_g, semiconductor_3d.c:4219-4229, 4414-4426;
+    no metal contacts in scope), summed per contact in CSR order."""
+    cj, ue, h, ar = dev["g_cj"], dev["g_ue"], dev["g_h"], dev["g_ar"]
+    row = graph_rows(dev)
+    con = dev["con"]
+    semi = dev["kind"] == K_SEMI
+    ok = (con[row] != 0) & semi[row] & semi[cj] & (con[cj] != con[row])
+    I, S, In = np.zeros(ncon), np.zeros(ncon), np.zeros(ncon)
+    e = np.nonzero(ok)[0]
+    ka, kb = row[e], cj[e]
+    VT = matp(dev, "VT")[ka]
+    lc, lv = lncK(dev), lnvK(dev)
+    dps = (dev["phi"][kb] - dev["phi"][ka]) / VT
+    Dn = dps + (lc[kb] - lc[ka])
+    Dp = dps - (lv[kb] - lv[ka])
+    gn = Q * ar[e] * gmu_n[ue[e]] * VT / h[e]
+    gp = Q * ar[e] * gmu_p[ue[e]] * VT / h[e]
+    a1 = gn * dev["n"][kb] * bernoulli(Dn)
+    a2 = gn * dev["n"][ka] * bernoulli(-Dn)
+    b1 = gp * dev["p"][ka] * bernoulli(Dp)
+    b2 = gp * dev["p"][kb] * bernoulli(-Dp)
+    c = con[ka] - 1
+    np.add.at(I, c, (a1 - a2) + (b1 - b2))
+    np.add.at(S, c, (a1 + a2) + (b1 + b2))
+    np.add.at(In, c, a1 - a2)
+    return I, S, In

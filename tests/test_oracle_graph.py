@@ -2,7 +2,7 @@
 upd_mob_g, cont_assemble_g) against the reference core's graph path, run live through the
 oracle harness on graph devices at a converged bias with seeded perturbations: the Poisson
 residual, diagonal and per-edge off-diagonals, the edge mobilities with velocity
-saturation, and both scaled Scharfetter-Gummel systems.  Host only: no GPU needed."""
+saturation, both scaled Scharfetter-Gummel systems and the terminal fluxes.  Host only: no GPU needed."""
 import ctypes
 import os
 import sys
@@ -89,6 +89,10 @@ def dumped(request):
     lib.hx_graph_mob(dptr(mun), dptr(mup))
     ps = state(lib, N)
     out = {"mob": (mun, mup)}
+    nc = lib.api3_get_ncon()
+    I, S, In = np.zeros(nc), np.zeros(nc), np.zeros(nc)
+    lib.hx_terminal_currents(dptr(I), dptr(S), dptr(In))
+    out["cur"] = (I, S, In)
     F, A7, sc = np.zeros(N), np.zeros(7 * N), np.zeros(N)
     nrm = lib.hx_poisson_eval(dptr(ps["phi"]), 1, dptr(F), dptr(A7), dptr(sc))
     gv = np.zeros(E)
@@ -135,3 +139,14 @@ def test_cont_assemble_graph(dumped, hole):
     close(rhs, rhr, rtol=1e-10, atol=1e-12 * np.abs(rhr).max())
     close(sc, scr, rtol=1e-13)
     close(dsc, dsr, rtol=1e-10, atol=1e-300)
+
+
+def test_terminal_currents_graph(dumped):
+    dev, out = dumped
+    mun, mup = out["mob"]
+    I, S, In = R.terminal_currents_g(dev, len(out["cur"][0]), mun, mup)
+    Ir, Sr, Inr = out["cur"]
+    close(S, Sr, rtol=1e-12)
+    # a contact's net current cancels between its in- and outflows: relative to its scale
+    close(I, Ir, rtol=0.0, atol=1e-12 * Sr.max())
+    close(In, Inr, rtol=0.0, atol=1e-12 * Sr.max())
