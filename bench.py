@@ -22,12 +22,15 @@ point (state resident in HBM); `e2e` also copies psi, n and p of every point to 
 buffers (api3_bulk_copy), the per-point results a caller reads.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload nmosfet|finfet|diodes64]
+                    [--workload nmosfet|finfet|graph_mosfet|diodes64]
 
 `--workload finfet`: the tri-gate FinFET Id-Vg family instead (96x96x64 tensor mesh, fin
 10 nm wide x 40 nm tall wrapped by 1.5 nm SiO2 and three gate electrodes driven together,
 gate 0..1.0 V in 0.02 V steps at 5 drain biases, one instance and stream per drain bias),
 with the same refined / FP64 / learned-seed / reference-core measurements.
+`--workload graph_mosfet`: the n-MOSFET's 120x80x60 mesh given as a general (graph) mesh,
+solved by the graph path (ELL kernels, aggregation multigrid, FP64), the reference's own
+graph path timed beside it.
 
 Multi-GPU (torchrun, one rank per GPU): every rank solves its own sweeps (independent
 devices, no data-path collective): weak scaling, time = max over ranks.
