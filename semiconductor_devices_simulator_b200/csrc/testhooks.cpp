@@ -202,7 +202,8 @@ double b200x_poisson(const double *phi, double *F, double *A7, double *sc) {
 void b200x_cont_assemble(int hole, double *A7, double *rhs, double *sc, double *dsc) {
     Inst &d = *dev();
     Ctx c = make_ctx(d);
-    launch_cont_assemble(c, hole);
+    if (d.unstr) launch_cont_assemble_g(c, hole);     // graph: the diagonal in A7[0], couplings per edge
+    else launch_cont_assemble(c, hole);
     dump7(d, d.g.h.A, d.N, A7);
     if (rhs) cudaMemcpyAsync(rhs, d.g.h.rhs, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
     if (sc) cudaMemcpyAsync(sc, d.g.h.sc, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);

@@ -219,6 +219,46 @@ def graph_pn_diode(lib, n=(12, 6, 5), L=(1e-6, 1e-6, 1e-6), NA=1e17, ND=1e17, xj
                     {"models": models, "diag": diag, "pos": pos if graph else None})
 
 
+def floating_base_pnp(lib, n=(24, 5, 4), graph=True, diag=0.0, solver=GUI_SOLVER):
+    """A p+ n p+ bar (2 x 0.5 x 0.5 um, p+ 1e18 cm^-3, a 0.4 um n base of 1e17 cm^-3 in the
+    middle, tau 1e-7 s) with ohmic contacts on the two p+ ends only: the n base is a
+    floating majority block (float_fix).  On a general (graph) mesh built from its tensor
+    mesh, or (graph=False) on the tensor mesh itself.  Anode swept 0..1 V."""
+    lib.api3_init()
+    xs = np.linspace(0, 2e-6, n[0]); ys = np.linspace(0, 0.5e-6, n[1]); zs = np.linspace(0, 0.5e-6, n[2])
+    Nx, Ny, Nz = n
+    N = Nx * Ny * Nz
+    si = lib.api3_add_material(SI, 300.0)
+    if graph:
+        rp, cj, h, ar, vol, pos = tensor_graph(xs, ys, zs, diag)
+        if not lib.api3_set_mesh_graph(N, len(cj), iptr(rp), iptr(cj), dptr(h), dptr(ar), dptr(vol), dptr(pos)):
+            raise RuntimeError("api3_set_mesh_graph rejected the graph")
+    else:
+        _grid(lib, xs, ys, zs)
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(7)
+    lib.api3_set_mat_tau(si, 1e-7, 1e-7)
+    k = np.arange(N)
+    i, j, l = k % Nx, (k // Nx) % Ny, k // (Nx * Ny)
+    base = (xs[i] >= 0.8e-6) & (xs[i] <= 1.2e-6)
+    Nd = np.ascontiguousarray(np.where(base, 1e17, 0.0) * 1e6)
+    Na = np.ascontiguousarray(np.where(base, 0.0, 1e18) * 1e6)
+    lib.api3_set_node_data(iptr(np.full(N, si, np.int32)), dptr(Nd), dptr(Na), None)
+    lib.api3_clear_contacts()
+    ca = lib.api3_add_contact_ex(0, 0, Ny - 1, 0, Nz - 1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cc = lib.api3_add_contact_ex(1, 0, Ny - 1, 0, Nz - 1, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    if graph:
+        Ly, Lz = fv_len(ys), fv_len(zs)
+        for cid, plane in ((ca, 0), (cc, Nx - 1)):
+            sel = i == plane
+            if not lib.api3_set_con_nodes(cid, int(sel.sum()), iptr(np.ascontiguousarray(k[sel], np.int32)),
+                                          dptr(np.ascontiguousarray(Ly[j[sel]] * Lz[l[sel]]))):
+                raise RuntimeError("api3_set_con_nodes failed")
+    V = np.round(np.linspace(0.0, 1.0, 6), 12)
+    return Workload("floating_base_pnp", (N, 1, 1) if graph else n, {"anode": ca, "cathode": cc},
+                    [{"fixed": {"cathode": 0.0}, "swept": "anode", "V": V}], {"models": 7, "diag": diag})
+
+
 def graph_schottky_diode(lib, n=(40, 3, 3), L=1e-6, ND=1e16, phi_m=4.8, models=7 | 64, h0=2e-9,
                          solver=GUI_SOLVER, V=None, diag=0.0):
     """The n-Si Schottky diode of schottky_diode() on a general (graph) mesh built from its

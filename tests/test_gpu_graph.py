@@ -289,3 +289,51 @@ def test_graph_batched_resolve_equals_sequential(lib, monkeypatch):
         assert lib.api3_resolve()
         Iq = np.array([lib.api3_get_contact_I(c) for c in range(nc)])
         assert np.allclose(Ib[j], Iq, rtol=1e-5, atol=1e-22), (j, Ib[j], Iq)
+
+
+HXF = {"hx_apply_bc": (None, []), "hx_rebuild_np": (None, []), "hx_upd_mob": (None, []), "hx_mob0_init": (None, []),
+       "hx_cont_assemble": (None, [ctypes.c_int] + [ctypes.POINTER(ctypes.c_double)] * 4),
+       "hx_float_fix": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)])}
+
+
+@pytest.mark.parametrize("graph", [1, 0], ids=["graph", "tensor"])
+def test_float_fix_matches_reference(lib, graph):
+    """The balance of a floating majority block (float_fix, semiconductor_3d.c:3159-3228 and
+    float_fix_g, :4353-4412) on the same installed state in both libraries: the n base of a
+    p+ n p+ bar contacted only at its p+ ends, the electron system assembled at the
+    equilibrium state with 0.3 V newly applied, and a seeded solution vector.  The labelling
+    finds the block in both, and the rescaled solution agrees to 1e-10."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_harness.so")
+    if not os.path.exists(path):
+        pytest.skip("reference core not built (make -C oracle)")
+    ref = abi.bind(ctypes.CDLL(path), HXF)
+    ref.api3_set_threads(os.cpu_count() or 1)
+    wr = D.floating_base_pnp(ref, graph=bool(graph))
+    wg = D.floating_base_pnp(lib, graph=bool(graph))
+    N = wr.N
+    assert ref.api3_solve() and lib.api3_solve()
+    st = [np.zeros(N) for _ in range(3)]
+    assert ref.api3_get_state(*(dptr(a) for a in st)) == 1
+    assert lib.api3_set_state(*(dptr(a) for a in st)) == 1
+    rng = np.random.default_rng(11)
+    sol0 = 1.0 + rng.normal(0, 0.02, N)
+    out = {}
+    for tag, L in (("ref", ref), ("gpu", lib)):
+        L.api3_set_contact_V(wr.contacts["anode"], 0.3)
+        sol = sol0.copy()
+        if tag == "ref":
+            # the reference's display step left edge-averaged mobilities in its node
+            # arrays: back to the low-field values the solver starts from
+            L.hx_mob0_init()
+            L.hx_apply_bc(); L.hx_rebuild_np(); L.hx_upd_mob()
+            L.hx_cont_assemble(0, dptr(np.zeros(7 * N)), dptr(np.zeros(N)), dptr(np.zeros(N)), dptr(np.zeros(N)))
+            nfix = L.hx_float_fix(0, dptr(sol))
+        else:
+            L.b200x_apply_bc(); L.b200x_rebuild_np(); L.b200x_upd_mob()
+            L.b200x_cont_assemble(0, dptr(np.zeros(7 * N)), dptr(np.zeros(N)), dptr(np.zeros(N)), dptr(np.zeros(N)))
+            nfix = L.b200x_float_fix(0, dptr(sol))
+        out[tag] = (nfix, sol)
+    assert out["ref"][0] >= 1 and out["gpu"][0] == out["ref"][0]
+    a, b = out["gpu"][1], out["ref"][1]
+    assert not np.allclose(b, sol0)                    # the block was rescaled
+    assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max()
