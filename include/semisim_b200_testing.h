@@ -39,6 +39,10 @@ int b200x_tun(int *cnt, double *tpG, double *colK, long long *tpk, long long *co
    aggregates; returns the number of levels */
 int b200x_gmg_plan(int N, const int *rp, const int *cj, const double *h, const double *ar, int L,
                    int *n_out, int *nnz_out, int *rp_out, int *cj_out, int *agg_out);
+/* graph multigrid set-up on the system now assembled (qsign 0 Poisson, +-1 continuity) and
+   level L's couplings in CSR order and diagonal (replaces reading gdev.lev[L].va / dg after
+   gmg_setup, semiconductor_3d.c:2643-2653); returns the coupling count */
+int b200x_gmg_vals(int qsign, int L, double *va, double *dg);
 int b200x_te(int *cnt, double *teK, double *teG, double *tcK, double *tcG, double *tcI, double *qcn, double *qcp);
 /* device state arrays: 0 psi, 1 phi_n, 2 phi_p, 3 n, 4 p, 5/6 low-field mobility n/p,
    7 sol, 8 rhs, 9 sc, 10 dsc, 16..21 face mobility (n x,y,z; p x,y,z), 22..24 sweep history

@@ -332,3 +332,14 @@ int hx_graph_mob(double *mun, double *mup){
     for(int e=0;e<gdev.nUE;e++){ if(mun) mun[e]=(double)gdev.gmu[0][e]; if(mup) mup[e]=(double)gdev.gmu[1][e]; }
     return gdev.nUE;
 }
+
+/* the values of graph multigrid level L after hx_mg_setup (g_galerkin, semiconductor_3d.c:
+   2575-2594): off-diagonals in the level's CSR order (nnz) and the diagonal (N); returns nnz */
+int hx_gmg_vals(int L, double *va, double *dg){
+    if(!gdev.allocated || !gdev.unstr || L<0 || L>=gdev.nlev) return -1;
+    const Lev *v=&gdev.lev[L];
+    int n=(int)v->N, nnz=v->rp[n];
+    if(va) memcpy(va,v->va,(size_t)nnz*8);
+    if(dg) memcpy(dg,v->dg,(size_t)n*8);
+    return nnz;
+}

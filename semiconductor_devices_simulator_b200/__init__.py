@@ -29,6 +29,7 @@ HOOKS = {
     "b200x_tun_update": (_I, []),
     "b200x_tun": (_I, [_IP, _DP, _DP, ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
     "b200x_gmg_plan": (_I, [_I, _IP, _IP, _DP, _DP, _I, _IP, _IP, _IP, _IP, _IP]),
+    "b200x_gmg_vals": (_I, [_I, _I, _DP, _DP]),
     "b200x_te": (_I, [_IP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "b200x_set": (_I, [_I, _DP]),
     "b200x_get": (_I, [_I, _DP]),

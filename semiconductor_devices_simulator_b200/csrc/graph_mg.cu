@@ -681,6 +681,37 @@ int gmg_levels(const Inst &d) { return (int)d.g.glev.size(); }
 
 }  // namespace ss
 
+ss::Inst *b200_global_dev();                      // the calling thread's current instance (api.cpp)
+
+// Test hook: set up the graph multigrid of the system now assembled on the mesh (qsign 0:
+// Poisson, weights 1; +-1: the continuity row weights and Slotboom weights of that carrier)
+// and return level L's coupling values in its CSR order (va, nnz) and its diagonal (dg, n);
+// returns nnz, -1 without a graph device or level L
+extern "C" int b200x_gmg_vals(int qsign, int L, double *va, double *dg) {
+    ss::Inst &d = *b200_global_dev();
+    if (!d.unstr || L < 0 || L >= (int)d.g.glev.size()) return -1;
+    const ss::Ctx c = ss::make_ctx(d);
+    ss::gmg_setup(d, c, qsign, qsign ? d.g.h.dsc : nullptr);
+    const ss::GLev &v = d.g.glev[L].dv;
+    const size_t DN = (size_t)v.D * v.N;
+    std::vector<int> col(DN);
+    std::vector<double> val(DN), diag(v.N);
+    cudaMemcpyAsync(col.data(), v.col, DN * sizeof(int), cudaMemcpyDeviceToHost, c.st);
+    cudaMemcpyAsync(val.data(), v.val, DN * sizeof(double), cudaMemcpyDeviceToHost, c.st);
+    cudaMemcpyAsync(diag.data(), v.diag, v.N * sizeof(double), cudaMemcpyDeviceToHost, c.st);
+    if (cudaStreamSynchronize(c.st) != cudaSuccess) return -1;
+    int nnz = 0;
+    for (int k = 0; k < v.N; k++)                       // ELL slot order = the level's CSR order
+        for (int s = 0; s < v.D; s++) {
+            const size_t e = (size_t)s * v.N + k;
+            if (col[e] < 0) break;
+            if (va) va[nnz] = val[e];
+            nnz++;
+        }
+    if (dg) std::copy(diag.begin(), diag.end(), dg);
+    return nnz;
+}
+
 // Test hook (no GPU needed): the graph multigrid hierarchy of a graph (api3_set_mesh_graph's
 // CSR arrays) with the current pairing knobs.  Level L's node count and pattern size go to
 // n_out / nnz_out; when the buffers are given, its CSR pattern (rp: n + 1, cj: nnz) and, below

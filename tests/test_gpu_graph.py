@@ -337,3 +337,47 @@ def test_float_fix_matches_reference(lib, graph):
     a, b = out["gpu"][1], out["ref"][1]
     assert not np.allclose(b, sol0)                    # the block was rescaled
     assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("hole", [0, 1], ids=["electrons", "holes"])
+def test_graph_multigrid_levels_match_reference(lib, hole):
+    """The coarse operators of the graph multigrid on one installed state: the continuity
+    system of a graph diode with diagonal edges (2,304 nodes, three levels) assembled in
+    both libraries, set up with its Slotboom weights and row scale (g_weights / g_galerkin,
+    semiconductor_3d.c:2575-2653), every coarse level's couplings (in CSR order) and
+    diagonal equal to 1e-12 - the aggregates are the reference's and the sums run in its
+    order."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_harness.so")
+    if not os.path.exists(path):
+        pytest.skip("reference core not built (make -C oracle)")
+    hx = dict(HXF, hx_mg_setup=(ctypes.c_int, [ctypes.c_int]),
+              hx_gmg_vals=(ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]))
+    ref = abi.bind(ctypes.CDLL(path), hx)
+    ref.api3_set_threads(os.cpu_count() or 1)
+    for L in (ref, lib):
+        w = D.graph_pn_diode(L, n=(24, 12, 8), diag=0.3)
+        L.api3_set_contact_V(w.contacts["anode"], 0.3)
+    N = w.N
+    assert ref.api3_solve() and lib.api3_solve()
+    st = [np.zeros(N) for _ in range(3)]
+    assert ref.api3_get_state(*(dptr(a) for a in st)) == 1
+    assert lib.api3_set_state(*(dptr(a) for a in st)) == 1
+    z = lambda m: dptr(np.zeros(m))
+    ref.hx_mob0_init(); ref.hx_apply_bc(); ref.hx_rebuild_np(); ref.hx_upd_mob()
+    ref.hx_cont_assemble(hole, z(7 * N), z(N), z(N), z(N))
+    lib.b200x_apply_bc(); lib.b200x_rebuild_np(); lib.b200x_upd_mob()
+    lib.b200x_cont_assemble(hole, z(7 * N), z(N), z(N), z(N))
+    qs = -1 if hole else 1
+    nl = ref.hx_mg_setup(qs)
+    assert nl >= 3
+    for Lv in range(1, nl):
+        nnz = ref.hx_gmg_vals(Lv, None, None)
+        assert lib.b200x_gmg_vals(qs, Lv, None, None) == nnz > 0
+        va_r, va_g = np.zeros(nnz), np.zeros(nnz)
+        dg_r, dg_g = np.zeros(N), np.zeros(N)
+        ref.hx_gmg_vals(Lv, dptr(va_r), dptr(dg_r))
+        lib.b200x_gmg_vals(qs, Lv, dptr(va_g), dptr(dg_g))
+        scale = np.abs(va_r).max()
+        assert np.abs(va_g - va_r).max() <= 1e-12 * scale, f"level {Lv} couplings"
+        assert np.allclose(dg_g, dg_r, rtol=1e-12, atol=0.0), f"level {Lv} diagonal"
+    assert lib.b200x_gmg_vals(qs, nl, None, None) == -1
