@@ -191,7 +191,8 @@ double b200x_poisson(const double *phi, double *F, double *A7, double *sc) {
     voltages(d);
     Ctx c = make_ctx(d);
     cudaMemcpyAsync(d.g.h.phi, phi, d.N * 8, cudaMemcpyHostToDevice, d.g.st);
-    launch_poisson(c, nullptr, 1, nullptr);
+    if (d.unstr) launch_poisson_g(c, nullptr, 1);    // graph: the diagonal in A7[0], couplings per edge
+    else launch_poisson(c, nullptr, 1, nullptr);
     const double nrm = res(d, R_PNORM);
     if (F) cudaMemcpyAsync(F, d.g.h.rhs, d.N * 8, cudaMemcpyDeviceToHost, d.g.st);
     dump7(d, d.g.h.A, d.N, A7);
