@@ -784,3 +784,59 @@ def terminal_currents_g(dev, ncon, gmu_n, gmu_p):
     np.add.at(S, c, (a1 + a2) + (b1 + b2))
     np.add.at(In, c, a1 - a2)
     return I, S, In
+
+
+def gmg_weights_g(levels, ph0):
+    """Slotboom prolongation weights of every graph level towards the next (g_weights,
+    semiconductor_3d.c:2621-2642): per aggregate the largest reference potential of its
+    members (ph, in units of VT; PH_NONE for contact and non-semiconductor nodes), and
+    pw = exp(ph - max) per member (0 below e^-700).  levels[L] holds "agg" (the aggregate
+    of every node of level L) for L below the coarsest; ph0 is level 0's potential.
+    Returns pw per level below the coarsest."""
+    PH_NONE = -1e300
+    pws = []
+    ph = np.asarray(ph0, float)
+    for L in range(len(levels) - 1):
+        agg = levels[L]["agg"]
+        na = int(agg.max()) + 1
+        mx = np.full(na, PH_NONE)
+        np.maximum.at(mx, agg, ph)
+        e = np.where(ph <= 0.5 * PH_NONE, -800.0, ph - mx[agg])
+        with np.errstate(over="ignore", invalid="ignore"):
+            pw = np.where(e < -700.0, 0.0, np.exp(np.maximum(e, -745.0)))
+        pws.append(pw)
+        ph = mx
+    return pws
+
+
+def galerkin_g(rp, cj, va, dg, agg, crp, ccj, pw, w=None):
+    """Coarse operator of a graph level (g_galerkin, semiconductor_3d.c:2575-2594): row I of
+    the coarse level sums, over the aggregate's members i in ascending order and their
+    entries in CSR order, w_i a_ij pw_j into the coarse entry (I, agg[j]) (into the
+    diagonal when agg[j] == I), plus w_i a_ii pw_i; a row with nothing but zeros becomes an
+    identity row.  Returns the coarse couplings in the coarse CSR order and the diagonal."""
+    nc = len(crp) - 1
+    cva = np.zeros(len(ccj))
+    cdg = np.zeros(nc)
+    pos = {}
+    for I in range(nc):
+        for s in range(crp[I], crp[I + 1]):
+            pos[(I, int(ccj[s]))] = s
+    members = [[] for _ in range(nc)]
+    for i in range(len(agg)):
+        members[int(agg[i])].append(i)
+    for I in range(nc):
+        cc = 0.0
+        for i in members[I]:
+            wi = 1.0 if w is None else w[i]
+            cc += wi * dg[i] * pw[i]
+            for e in range(rp[i], rp[i + 1]):
+                a = wi * va[e] * pw[cj[e]]
+                J = int(agg[cj[e]])
+                if J == I:
+                    cc += a
+                else:
+                    cva[pos[(I, J)]] += a
+        zero = cc == 0.0 and not np.any(cva[crp[I]:crp[I + 1]] != 0.0)
+        cdg[I] = 1.0 if zero else cc
+    return cva, cdg

@@ -2,7 +2,8 @@
 upd_mob_g, cont_assemble_g) against the reference core's graph path, run live through the
 oracle harness on graph devices at a converged bias with seeded perturbations: the Poisson
 residual, diagonal and per-edge off-diagonals, the edge mobilities with velocity
-saturation, both scaled Scharfetter-Gummel systems and the terminal fluxes.  Host only: no GPU needed."""
+saturation, both scaled Scharfetter-Gummel systems, the terminal fluxes, and the
+multigrid's Slotboom weights and Petrov-Galerkin coarse operators.  Host only: no GPU needed."""
 import ctypes
 import os
 import sys
@@ -150,3 +151,62 @@ def test_terminal_currents_graph(dumped):
     # a contact's net current cancels between its in- and outflows: relative to its scale
     close(I, Ir, rtol=0.0, atol=1e-12 * Sr.max())
     close(In, Inr, rtol=0.0, atol=1e-12 * Sr.max())
+
+
+HXM = dict(HXG, hx_mg_setup=(ctypes.c_int, [ctypes.c_int]),
+           hx_gmg_level=(ctypes.c_int, [ctypes.c_int] + [_IP] * 5),
+           hx_gmg_vals=(ctypes.c_int, [ctypes.c_int, _DP, _DP]))
+
+
+@pytest.mark.parametrize("hole", [0, 1], ids=["electrons", "holes"])
+def test_graph_multigrid_setup(hole):
+    """The Slotboom weights and Petrov-Galerkin coarse operators of the graph multigrid,
+    restated (gmg_weights_g, galerkin_g) from the assembled continuity system of a graph
+    diode with diagonal edges and the reference's own hierarchy, equal the reference's
+    coarse levels to 1e-13."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_harness.so")
+    if not os.path.exists(path):
+        pytest.skip("reference core not built (make -C oracle)")
+    lib = abi.bind(ctypes.CDLL(path), HXM)
+    w = D.graph_pn_diode(lib, n=(24, 12, 8), diag=0.3)
+    lib.api3_set_contact_V(w.contacts["anode"], 0.3)
+    assert lib.api3_solve()
+    N = w.N
+    lib.hx_mob0_init(); lib.hx_apply_bc(); lib.hx_rebuild_np(); lib.hx_upd_mob()
+    A7, rhs, sc, dsc = np.zeros(7 * N), np.zeros(N), np.zeros(N), np.zeros(N)
+    lib.hx_cont_assemble(hole, dptr(A7), dptr(rhs), dptr(sc), dptr(dsc))
+    E = lib.hx_graph(None, None, None, None, None, None)
+    va0 = np.zeros(E)
+    lib.hx_graph_vals(dptr(va0))
+    dg0 = A7[:N].copy()
+    qs = -1 if hole else 1
+    nl = lib.hx_mg_setup(qs)
+    assert nl >= 3
+    levels = []
+    for L in range(nl):
+        n, nnz = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        lib.hx_gmg_level(L, iptr(n), iptr(nnz), None, None, None)
+        rp, cj, agg = np.zeros(n[0] + 1, np.int32), np.zeros(max(nnz[0], 1), np.int32), np.zeros(n[0], np.int32)
+        lib.hx_gmg_level(L, iptr(n), iptr(nnz), iptr(rp), iptr(cj), iptr(agg))
+        va, dg = np.zeros(max(nnz[0], 1)), np.zeros(n[0])
+        lib.hx_gmg_vals(L, dptr(va), dptr(dg))
+        levels.append({"rp": rp, "cj": cj[:nnz[0]], "agg": agg, "va": va[:nnz[0]], "dg": dg})
+    # level-0 reference potentials (ph0, semiconductor_3d.c:2085-2090), phi in units of VT
+    kind, con = np.zeros(N, np.int32), np.zeros(N, np.int32)
+    lib.hx_masks(iptr(kind), iptr(con), iptr(np.zeros(N, np.int32)))
+    phin, phip = MG.get(lib, MG.W_PHIN, N), MG.get(lib, MG.W_PHIP, N)
+    rec = np.zeros(64)
+    lib.hx_mat(0, dptr(rec))
+    VT = rec[R.MF["VT"]]
+    fixed = (kind != 0) | (con != 0)
+    ph0 = np.where(fixed, -1e300, phin / VT if qs > 0 else -phip / VT)
+    pws = R.gmg_weights_g(levels, ph0)
+    va, dg = va0, dg0
+    for L in range(nl - 1):
+        f, c = levels[L], levels[L + 1]
+        cva, cdg = R.galerkin_g(f["rp"], f["cj"], va, dg, f["agg"], c["rp"], c["cj"], pws[L],
+                                dsc if L == 0 else None)
+        scale = np.abs(c["va"]).max()
+        assert np.abs(cva - c["va"]).max() <= 1e-13 * scale, f"level {L + 1} couplings"
+        assert np.allclose(cdg, c["dg"], rtol=1e-13, atol=0.0), f"level {L + 1} diagonal"
+        va, dg = c["va"], c["dg"]
