@@ -840,3 +840,112 @@ def galerkin_g(rp, cj, va, dg, agg, crp, ccj, pw, w=None):
         zero = cc == 0.0 and not np.any(cva[crp[I]:crp[I + 1]] != 0.0)
         cdg[I] = 1.0 if zero else cc
     return cva, cdg
+
+
+def neighbours_tensor(dev, g=None):
+    """Per node, its neighbours in the reference's direction order with area / length and
+    the face mobilities of the edge (nbr() and fmu, semiconductor_3d.c:709-719, 256)."""
+    g = g or Grid(dev)
+    out = [[] for _ in range(g.N)]
+    for d in range(6):
+        for k in np.nonzero(g.valid[d])[0]:
+            kb = int(g.kb[d][k])
+            kl = min(int(k), kb)
+            out[k].append((kb, g.ar[d][k] / g.h[d][k], dev["fmu"][d // 2][kl], dev["fmu"][3 + d // 2][kl]))
+    return out, g.vol
+
+
+def neighbours_graph(dev, gmu_n, gmu_p):
+    """Per node, its graph neighbours in CSR order with dual area / length and the edge
+    mobilities."""
+    rp, cj, ue, h, ar = dev["g_rp"], dev["g_cj"], dev["g_ue"], dev["g_h"], dev["g_ar"]
+    out = [[(int(cj[e]), ar[e] / h[e], gmu_n[ue[e]], gmu_p[ue[e]]) for e in range(rp[k], rp[k + 1])]
+           for k in range(len(rp) - 1)]
+    return out, dev["g_vol"]
+
+
+def float_fix(dev, hole, sol, sc, nbrs, vol):
+    """Balance of every floating majority block (float_fix / float_fix_g,
+    semiconductor_3d.c:3159-3228, 4353-4412; no incomplete ionisation, traps or exchange
+    terms in scope).  A block is a breadth-first set of majority, quasi-neutral
+    semiconductor nodes (c = s u >= the other carrier, c and s >= |Nd - Na| / 2, c > 10 n_i)
+    found in node order; a block touching a contact is anchored.  Otherwise u is scaled by
+    lambda solving lambda Aout - Bin + sum vol R(lambda c) = 0 (Newton in ln lambda, steps
+    clipped to +-2, 60 at most).  Returns (blocks fixed, u)."""
+    N = len(sol)
+    u = np.array(sol, float)
+    s = np.asarray(sc, float)
+    semi = dev["kind"] == K_SEMI
+    con = dev["con"]
+    car = dev["p"] if hole else dev["n"]
+    oth = dev["n"] if hole else dev["p"]
+    dnet = np.abs(dev["Nd"] - dev["Na"])
+    ni = niK(dev)
+    VT = matp(dev, "VT")
+    lc, lv = lncK(dev), lnvK(dev)
+
+    def maj(k):
+        c = s[k] * u[k]
+        return (semi[k] and not con[k] and c >= oth[k] and c >= 0.5 * dnet[k] and s[k] >= 0.5 * dnet[k]
+                and c > 10.0 * ni[k])
+    lab = np.zeros(N, int)
+    nfix = blk = 0
+    for k0 in range(N):
+        if lab[k0] or not maj(k0):
+            continue
+        blk += 1
+        q = [k0]
+        lab[k0] = blk
+        anch = False
+        head = 0
+        while head < len(q):
+            k = q[head]
+            head += 1
+            for kb, _, _, _ in nbrs[k]:
+                if not semi[kb]:
+                    continue
+                if con[kb]:
+                    anch = True
+                    continue
+                if not lab[kb] and maj(kb):
+                    lab[kb] = blk
+                    q.append(kb)
+        if anch:
+            continue
+        Aout = Bin = 0.0
+        for k in q:
+            for kb, arh, mn, mp in nbrs[k]:
+                if not semi[kb] or lab[kb] == blk:
+                    continue
+                D = (dev["phi"][kb] - dev["phi"][k]) / VT[k] + (-(lv[kb] - lv[k]) if hole else (lc[kb] - lc[k]))
+                gg = arh * (mp if hole else mn) * VT[k]
+                Bp, Bm = bernoulli(np.array([D, -D]))
+                self_, nb = (gg * Bp, gg * Bm) if hole else (gg * Bm, gg * Bp)
+                cb = car[kb] if con[kb] else s[kb] * u[kb]
+                Aout += self_ * s[k] * u[k]
+                Bin += nb * cb
+        qa = np.array(q)
+        sl = 0.0
+        for _ in range(60):
+            lam = np.exp(sl)
+            G, dG = lam * Aout - Bin, lam * Aout
+            c = lam * s[qa] * u[qa]
+            nn, pp = dev["n"].copy(), dev["p"].copy()
+            if hole:
+                pp[qa] = c
+            else:
+                nn[qa] = c
+            R, dRn, dRp = recomb(dev, nn, pp)
+            for t, k in enumerate(q):
+                G += vol[k] * R[k]
+                dG += vol[k] * (dRp[k] if hole else dRn[k]) * c[t]
+            if not dG > 0.0:
+                break
+            ds = min(max(-G / dG, -2.0), 2.0)
+            sl += ds
+            if abs(ds) < 1e-13:
+                break
+        if sl == sl and 1e-15 < abs(sl) < 200.0:
+            u[qa] *= np.exp(sl)
+            nfix += 1
+    return nfix, u

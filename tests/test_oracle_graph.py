@@ -2,8 +2,9 @@
 upd_mob_g, cont_assemble_g) against the reference core's graph path, run live through the
 oracle harness on graph devices at a converged bias with seeded perturbations: the Poisson
 residual, diagonal and per-edge off-diagonals, the edge mobilities with velocity
-saturation, both scaled Scharfetter-Gummel systems, the terminal fluxes, and the
-multigrid's Slotboom weights and Petrov-Galerkin coarse operators.  Host only: no GPU needed."""
+saturation, both scaled Scharfetter-Gummel systems, the terminal fluxes, the
+multigrid's Slotboom weights and Petrov-Galerkin coarse operators, and the floating-block
+balance (on tensor and graph meshes).  Host only: no GPU needed."""
 import ctypes
 import os
 import sys
@@ -210,3 +211,47 @@ def test_graph_multigrid_setup(hole):
         assert np.abs(cva - c["va"]).max() <= 1e-13 * scale, f"level {L + 1} couplings"
         assert np.allclose(cdg, c["dg"], rtol=1e-13, atol=0.0), f"level {L + 1} diagonal"
         va, dg = c["va"], c["dg"]
+
+
+HXFF = dict(HXG, hx_float_fix=(ctypes.c_int, [ctypes.c_int, _DP]))
+
+
+@pytest.mark.parametrize("graph", [1, 0], ids=["graph", "tensor"])
+def test_float_fix_restated(graph):
+    """The floating-block balance restated (float_fix, both mesh kinds) against the
+    reference on the n base of a p+ n p+ bar contacted only at its ends: the electron
+    system assembled at the equilibrium state with 0.3 V newly applied, a seeded solution
+    vector; the same block fixed and the rescaled solution equal to 1e-12."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_harness.so")
+    if not os.path.exists(path):
+        pytest.skip("reference core not built (make -C oracle)")
+    lib = abi.bind(ctypes.CDLL(path), HXFF)
+    w = D.floating_base_pnp(lib, graph=bool(graph))
+    assert lib.api3_solve()
+    lib.api3_set_contact_V(w.contacts["anode"], 0.3)
+    N = w.N
+    lib.hx_mob0_init(); lib.hx_apply_bc(); lib.hx_rebuild_np(); lib.hx_upd_mob()
+    A7, rhs, sc, dsc = np.zeros(7 * N), np.zeros(N), np.zeros(N), np.zeros(N)
+    lib.hx_cont_assemble(0, dptr(A7), dptr(rhs), dptr(sc), dptr(dsc))
+    rec = MG.device_record(lib, w)
+    dev = dict(rec, **state(lib, N))
+    dev.update(models=7, caxis=1, ref_mat=0, mat=np.zeros(N, np.int64))
+    if graph:
+        E = lib.hx_graph(None, None, None, None, None, None)
+        g_rp, g_cj, g_ue = np.zeros(N + 1, np.int32), np.zeros(E, np.int32), np.zeros(E, np.int32)
+        g_h, g_ar, g_vol = np.zeros(E), np.zeros(E), np.zeros(N)
+        lib.hx_graph(iptr(g_rp), iptr(g_cj), iptr(g_ue), dptr(g_h), dptr(g_ar), dptr(g_vol))
+        dev.update(g_rp=g_rp, g_cj=g_cj, g_ue=g_ue, g_h=g_h, g_ar=g_ar, g_vol=g_vol)
+        nue = lib.hx_graph_mob(None, None)
+        mun, mup = np.zeros(nue), np.zeros(nue)
+        lib.hx_graph_mob(dptr(mun), dptr(mup))
+        nbrs, vol = R.neighbours_graph(dev, mun, mup)
+    else:
+        dev["fmu"] = np.array([MG.get(lib, 16 + q, N) for q in range(6)])
+        nbrs, vol = R.neighbours_tensor(dev)
+    sol0 = 1.0 + np.random.default_rng(11).normal(0, 0.02, N)
+    nfix, u = R.float_fix(dev, 0, sol0, sc, nbrs, vol)
+    sol = sol0.copy()
+    nref = lib.hx_float_fix(0, dptr(sol))
+    assert nref >= 1 and nfix == nref
+    assert np.abs(u - sol).max() <= 1e-12 * np.abs(sol).max()
