@@ -949,3 +949,100 @@ def float_fix(dev, hole, sol, sc, nbrs, vol):
             u[qa] *= np.exp(sl)
             nfix += 1
     return nfix, u
+
+
+def graph_lsq(dev):
+    """Inverse least-squares matrices M^-1 of every semiconductor node (g_lsq_setup,
+    semiconductor_3d.c:2682-2700): M = sum over semiconductor neighbours w dr dr^T,
+    w = 1 / |dr|^2, regularised by 1e-6 of its trace; symmetric, stored xx xy xz yy yz zz."""
+    rp, cj = dev["g_rp"], dev["g_cj"]
+    pos = dev["g_pos"].reshape(-1, 3)
+    semi = dev["kind"] == K_SEMI
+    N = len(rp) - 1
+    out = np.zeros((N, 6))
+    for k in range(N):
+        if not semi[k]:
+            continue
+        m = np.zeros(6)
+        for e in range(rp[k], rp[k + 1]):
+            b = cj[e]
+            if not semi[b]:
+                continue
+            dx, dy, dz = pos[b] - pos[k]
+            w = 1.0 / (dx * dx + dy * dy + dz * dz + 1e-40)
+            m += w * np.array([dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz])
+        eps = 1e-6 * (m[0] + m[3] + m[5]) + 1e-30
+        M = np.array([[m[0] + eps, m[1], m[2]], [m[1], m[3] + eps, m[4]], [m[2], m[4], m[5] + eps]])
+        if abs(np.linalg.det(M)) > 0:
+            Mi = np.linalg.inv(M)
+            out[k] = [Mi[0, 0], Mi[0, 1], Mi[0, 2], Mi[1, 1], Mi[1, 2], Mi[2, 2]]
+    return out
+
+
+def graph_grad(dev, fld, lsq):
+    """Least-squares gradient of a node field over the semiconductor neighbours (g_grad,
+    semiconductor_3d.c:2702-2714)."""
+    rp, cj = dev["g_rp"], dev["g_cj"]
+    pos = dev["g_pos"].reshape(-1, 3)
+    semi = dev["kind"] == K_SEMI
+    N = len(rp) - 1
+    g = np.zeros((N, 3))
+    for k in range(N):
+        if not semi[k]:
+            continue
+        r = np.zeros(3)
+        for e in range(rp[k], rp[k + 1]):
+            b = cj[e]
+            if not semi[b]:
+                continue
+            d = pos[b] - pos[k]
+            r += (fld[b] - fld[k]) / (d @ d + 1e-40) * d
+        m = lsq[k]
+        g[k] = [m[0] * r[0] + m[1] * r[1] + m[2] * r[2], m[1] * r[0] + m[3] * r[1] + m[4] * r[2],
+                m[2] * r[0] + m[4] * r[1] + m[5] * r[2]]
+    return g
+
+
+def graph_node_J(dev, gmu_n, gmu_p, which=0):
+    """Node current density by least squares from the edge fluxes (g_node_J,
+    semiconductor_3d.c:4428-4452): J = (sum_e A_e t t^T)^-1 sum_e A_e t j_e over the
+    semiconductor neighbours, t the unit edge vector, j_e the flux density; which 0 total,
+    1 electrons, 2 holes."""
+    rp, cj, ue, h, ar = dev["g_rp"], dev["g_cj"], dev["g_ue"], dev["g_h"], dev["g_ar"]
+    pos = dev["g_pos"].reshape(-1, 3)
+    semi = dev["kind"] == K_SEMI
+    N = len(rp) - 1
+    VT = matp(dev, "VT")
+    lc, lv = lncK(dev), lnvK(dev)
+    J = np.zeros((N, 3))
+    for k in range(N):
+        if not semi[k]:
+            continue
+        M = [0.0] * 6                                # xx xy xz yy yz zz, summed as the reference
+        r = [0.0, 0.0, 0.0]
+        for e in range(rp[k], rp[k + 1]):
+            b = cj[e]
+            if not semi[b]:
+                continue
+            t = (pos[b] - pos[k]) / h[e]
+            dps = (dev["phi"][b] - dev["phi"][k]) / VT[k]
+            Dn, Dp = dps + (lc[b] - lc[k]), dps - (lv[b] - lv[k])
+            gn, gp = Q * ar[e] * gmu_n[ue[e]] * VT[k] / h[e], Q * ar[e] * gmu_p[ue[e]] * VT[k] / h[e]
+            Bn = bernoulli(np.array([Dn, -Dn]))
+            Bp = bernoulli(np.array([Dp, -Dp]))
+            Jn = gn * dev["n"][b] * Bn[0] - gn * dev["n"][k] * Bn[1]
+            Jp = gp * dev["p"][k] * Bp[0] - gp * dev["p"][b] * Bp[1]
+            j = (Jn if which == 1 else (Jp if which == 2 else Jn + Jp)) / (ar[e] if ar[e] > 0 else 1e-300)
+            w = ar[e]
+            M[0] += w * t[0] * t[0]; M[1] += w * t[0] * t[1]; M[2] += w * t[0] * t[2]
+            M[3] += w * t[1] * t[1]; M[4] += w * t[1] * t[2]; M[5] += w * t[2] * t[2]
+            r[0] += w * t[0] * j; r[1] += w * t[1] * j; r[2] += w * t[2] * j
+        eps = 1e-6 * (M[0] + M[3] + M[5]) + 1e-300
+        a, b, c, dd, ee, f = M[0] + eps, M[1], M[2], M[3] + eps, M[4], M[5] + eps
+        A, Bq, Cc = dd * f - ee * ee, -(b * f - c * ee), b * ee - c * dd           # cofactors
+        Dq, E, F = a * f - c * c, -(a * ee - b * c), a * dd - b * b
+        det = a * A + b * Bq + c * Cc
+        if abs(det) > 0:
+            J[k] = [(A * r[0] + Bq * r[1] + Cc * r[2]) / det, (Bq * r[0] + Dq * r[1] + E * r[2]) / det,
+                    (Cc * r[0] + E * r[1] + F * r[2]) / det]
+    return J

@@ -255,3 +255,38 @@ def test_float_fix_restated(graph):
     nref = lib.hx_float_fix(0, dptr(sol))
     assert nref >= 1 and nfix == nref
     assert np.abs(u - sol).max() <= 1e-12 * np.abs(sol).max()
+
+
+def test_graph_display_outputs_restated():
+    """At a solved state of the graph diode with diagonal edges: the node current densities
+    (bulk_copy 7-9 and the electron / hole parts 20-25) from the restated least-squares
+    operator equal the reference's to 1e-8 of their peak.  A node's density is the difference
+    of drift and diffusion fluxes ~1e6 times larger, and the reference is compiled with
+    contractions (-ffast-math): one rounding of those terms is ~3e-9 of the peak here.  The
+    largest field (api3_get_Emax) agrees to 1e-9."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_harness.so")
+    if not os.path.exists(path):
+        pytest.skip("reference core not built (make -C oracle)")
+    lib = abi.bind(ctypes.CDLL(path), HXG)
+    w = D.graph_pn_diode(lib, diag=0.3, models=7)
+    lib.api3_set_contact_V(w.contacts["anode"], 0.5)
+    assert lib.api3_solve()
+    N = w.N
+    rec = MG.device_record(lib, w)
+    dev = dict(rec, **state(lib, N))
+    E = lib.hx_graph(None, None, None, None, None, None)
+    g_rp, g_cj, g_ue = np.zeros(N + 1, np.int32), np.zeros(E, np.int32), np.zeros(E, np.int32)
+    g_h, g_ar, g_vol = np.zeros(E), np.zeros(E), np.zeros(N)
+    lib.hx_graph(iptr(g_rp), iptr(g_cj), iptr(g_ue), dptr(g_h), dptr(g_ar), dptr(g_vol))
+    dev.update(models=7, caxis=1, ref_mat=0, mat=np.zeros(N, np.int64), g_rp=g_rp, g_cj=g_cj, g_ue=g_ue,
+               g_h=g_h, g_ar=g_ar, g_vol=g_vol, g_pos=np.asarray(w.info["pos"], float))
+    nue = lib.hx_graph_mob(None, None)
+    mun, mup = np.zeros(nue), np.zeros(nue)
+    lib.hx_graph_mob(dptr(mun), dptr(mup))
+    for which, qs in ((0, (7, 8, 9)), (1, (20, 21, 22)), (2, (23, 24, 25))):
+        J = R.graph_node_J(dev, mun, mup, which)
+        ref = np.stack([D.field(lib, q, w.shape).ravel() for q in qs], axis=1)
+        assert np.abs(J - ref).max() <= 1e-8 * np.abs(ref).max(), f"J part {which}"
+    g = R.graph_grad(dev, dev["phi"], R.graph_lsq(dev))
+    emax = np.sqrt(np.max(np.sum(g * g, axis=1)))
+    assert abs(emax - lib.api3_get_Emax()) <= 1e-9 * lib.api3_get_Emax()
