@@ -281,7 +281,10 @@ int hx_mat(int mi, double *out){
                 m->vsat_n,m->vsat_p,m->beta_n,m->beta_p,m->tau_n0,m->tau_p0,m->Cn,m->Cp,m->Brad,m->tau_Nref,
                 m->bgn_E,m->bgn_N,m->bgn_C,m->lnc,m->lnv,(double)m->insulator,m->ani_n,m->ani_p,
                 (double)m->ion_on,m->ion_w[0],m->ion_w[1],m->ion_Ed[0],m->ion_Ed[1],m->ion_ad[0],m->ion_ad[1],
-                m->ion_gd,m->ion_Ea,m->ion_aa,m->ion_ga};
+                m->ion_gd,m->ion_Ea,m->ion_aa,m->ion_ga,
+                (double)m->ii_on,m->ii_a[0][0],m->ii_a[0][1],m->ii_a[1][0],m->ii_a[1][1],
+                m->ii_b[0][0],m->ii_b[0][1],m->ii_b[1][0],m->ii_b[1][1],m->ii_E0[0],m->ii_E0[1],
+                m->ii_m[0],m->ii_m[1],m->ii_g};
     memcpy(out,v,sizeof v);
     return (int)(sizeof v/sizeof v[0]);
 }
@@ -342,4 +345,12 @@ int hx_gmg_vals(int L, double *va, double *dg){
     if(va) memcpy(va,v->va,(size_t)nnz*8);
     if(dg) memcpy(dg,v->dg,(size_t)n*8);
     return nnz;
+}
+
+/* impact-ionisation pair generation of every node at the present state (ii_update,
+   semiconductor_3d.c:4486-4523), 1/s per control volume; returns 1 */
+int hx_ii_update(double *gii){
+    ii_update(&gdev);
+    if(gii) memcpy(gii,gdev.gii,NN(&gdev)*sizeof(double));
+    return 1;
 }

@@ -31,7 +31,9 @@ MAT_FIELDS = ["T", "VT", "Eg", "chi", "eps_r", "Nc", "Nv", "ni",
               "vsat_n", "vsat_p", "beta_n", "beta_p", "tau_n0", "tau_p0", "Cn", "Cp", "Brad", "tau_Nref",
               "bgn_E", "bgn_N", "bgn_C", "lnc", "lnv", "insulator", "ani_n", "ani_p",
               "ion_on", "ion_w0", "ion_w1", "ion_Ed0", "ion_Ed1", "ion_ad0", "ion_ad1",
-              "ion_gd", "ion_Ea", "ion_aa", "ion_ga"]
+              "ion_gd", "ion_Ea", "ion_aa", "ion_ga",
+              "ii_on", "ii_a00", "ii_a01", "ii_a10", "ii_a11", "ii_b00", "ii_b01", "ii_b10", "ii_b11",
+              "ii_E00", "ii_E01", "ii_m0", "ii_m1", "ii_g"]
 MF = {n: i for i, n in enumerate(MAT_FIELDS)}
 
 
@@ -1046,3 +1048,39 @@ def graph_node_J(dev, gmu_n, gmu_p, which=0):
             J[k] = [(A * r[0] + Bq * r[1] + Cc * r[2]) / det, (Bq * r[0] + Dq * r[1] + E * r[2]) / det,
                     (Cc * r[0] + E * r[1] + F * r[2]) / det]
     return J
+
+
+def ii_alpha(dev, F, c):
+    """Impact-ionisation coefficient of carrier c (0 electrons, 1 holes) at field F, per node
+    (ii_alpha, semiconductor_3d.c:4478-4485): g a exp(-(g b / F)^m) with (a, b) below / above
+    E0, nothing below 1e5 V/m or beyond an exponent of 700."""
+    F = np.asarray(F, float)
+    g = matp(dev, "ii_g")
+    E0 = matp(dev, f"ii_E0{c}")
+    hi = F >= E0
+    a = np.where(hi, matp(dev, f"ii_a{c}1"), matp(dev, f"ii_a{c}0"))
+    b = np.where(hi, matp(dev, f"ii_b{c}1"), matp(dev, f"ii_b{c}0"))
+    m = matp(dev, f"ii_m{c}")
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        x = g * b / F
+        x = np.where(m != 1.0, x ** m, x)
+        out = np.where((F > 1e5) & (x <= 700.0), g * a * np.exp(-np.minimum(x, 700.0)), 0.0)
+    return out
+
+
+def graph_ii(dev, gmu_n, gmu_p):
+    """Impact-ionisation pair generation of every node on a graph (ii_update,
+    semiconductor_3d.c:4486-4523): G = sum over carriers alpha(F) |J| / q over the control
+    volume, J the carrier's least-squares node current density, F = |E.J| / |J| with E the
+    least-squares field; contact nodes and materials without data generate nothing."""
+    Jn = graph_node_J(dev, gmu_n, gmu_p, 1)
+    Jp = graph_node_J(dev, gmu_n, gmu_p, 2)
+    E = -graph_grad(dev, dev["phi"], graph_lsq(dev))
+    G = np.zeros(len(E))
+    for c, J in ((0, Jn), (1, Jp)):
+        jj = np.sqrt(np.sum(J * J, axis=1))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            F = np.where(jj > 0, np.abs(np.sum(E * J, axis=1)) / np.where(jj > 0, jj, 1.0), 0.0)
+        G += np.where(jj > 0, ii_alpha(dev, F, c) * jj, 0.0)
+    on = (dev["kind"] == K_SEMI) & (dev["con"] == 0) & (matp(dev, "ii_on") != 0)
+    return np.where(on, G / Q * dev["g_vol"], 0.0)

@@ -84,7 +84,7 @@ def device_record(lib, w):
     lib.hx_contact_area(dptr(area))
     mats = []
     for mi in range(16):
-        rec = np.zeros(64)
+        rec = np.zeros(128)
         m = lib.hx_mat(mi, dptr(rec))
         if m == 0:
             break

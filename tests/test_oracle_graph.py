@@ -196,7 +196,7 @@ def test_graph_multigrid_setup(hole):
     kind, con = np.zeros(N, np.int32), np.zeros(N, np.int32)
     lib.hx_masks(iptr(kind), iptr(con), iptr(np.zeros(N, np.int32)))
     phin, phip = MG.get(lib, MG.W_PHIN, N), MG.get(lib, MG.W_PHIP, N)
-    rec = np.zeros(64)
+    rec = np.zeros(128)
     lib.hx_mat(0, dptr(rec))
     VT = rec[R.MF["VT"]]
     fixed = (kind != 0) | (con != 0)
@@ -290,3 +290,34 @@ def test_graph_display_outputs_restated():
     g = R.graph_grad(dev, dev["phi"], R.graph_lsq(dev))
     emax = np.sqrt(np.max(np.sum(g * g, axis=1)))
     assert abs(emax - lib.api3_get_Emax()) <= 1e-9 * lib.api3_get_Emax()
+
+
+def test_graph_impact_ionisation_restated():
+    """Impact-ionisation generation on a graph (models bit 8): the Si p+n diode of the
+    avalanche tests given as a graph, solved at -8 V; the restated generation (least-squares
+    node currents and field, the Chynoweth law with the van Overstraeten - de Man
+    coefficients) equals the reference's ii_update at the same state to 1e-7 of its peak."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libsemisim_harness.so")
+    if not os.path.exists(path):
+        pytest.skip("reference core not built (make -C oracle)")
+    lib = abi.bind(ctypes.CDLL(path), dict(HXG, hx_ii_update=(ctypes.c_int, [_DP])))
+    w = D.graph_pn_diode(lib, n=(40, 3, 3), NA=1e19, ND=1e17, xj=0.3e-6, tau=1e-9, models=7 | 256)
+    lib.api3_set_contact_V(w.contacts["anode"], -8.0)
+    assert lib.api3_solve()
+    N = w.N
+    rec = MG.device_record(lib, w)
+    dev = dict(rec, **state(lib, N))
+    E = lib.hx_graph(None, None, None, None, None, None)
+    g_rp, g_cj, g_ue = np.zeros(N + 1, np.int32), np.zeros(E, np.int32), np.zeros(E, np.int32)
+    g_h, g_ar, g_vol = np.zeros(E), np.zeros(E), np.zeros(N)
+    lib.hx_graph(iptr(g_rp), iptr(g_cj), iptr(g_ue), dptr(g_h), dptr(g_ar), dptr(g_vol))
+    dev.update(models=7 | 256, caxis=1, ref_mat=0, mat=np.zeros(N, np.int64), g_rp=g_rp, g_cj=g_cj, g_ue=g_ue,
+               g_h=g_h, g_ar=g_ar, g_vol=g_vol, g_pos=np.asarray(w.info["pos"], float))
+    nue = lib.hx_graph_mob(None, None)
+    mun, mup = np.zeros(nue), np.zeros(nue)
+    lib.hx_graph_mob(dptr(mun), dptr(mup))
+    gref = np.zeros(N)
+    lib.hx_ii_update(dptr(gref))
+    g = R.graph_ii(dev, mun, mup)
+    assert gref.max() > 0
+    assert np.abs(g - gref).max() <= 1e-7 * gref.max()
