@@ -67,8 +67,12 @@ def parse():
                     help="linear solves: FP32 refined in FP64 (default) or FP64 throughout")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison steps")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor step")
+    ap.add_argument("--no-tight", action="store_true", help="skip the tight-tolerance refined-vs-FP64 check")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64 pn-diode variants sub-block")
+    ap.add_argument("--points", type=int, default=0,
+                    help="points per sweep timed in a step (0: every point)")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuner)")
-    ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "finfet", "graph_mosfet", "diodes64"],
+    ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "finfet", "graph_mosfet", "diodes64", "power_cell"],
                     help="nmosfet: the Id-Vg workload (default); finfet: the tri-gate FinFET Id-Vg family "
                          "(96x96x64, 5 drain biases); diodes64: the 64 pn-diode variants batch")
     ap.add_argument("--workers", type=int, default=0, help="diodes64: concurrent host threads (0: one per variant)")
@@ -99,7 +103,13 @@ def run_probe(a):
     l0 = lib.b200x_launches()
     lib.b200x_cont_assemble(0, None, None, None, None)
     rn, r0 = np.zeros(1), np.zeros(1)
+    lib.b200x_stream_timer(0)
     its = lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
+    solve_ms = lib.b200x_stream_timer(1)
+    lib.b200x_cont_assemble(0, None, None, None, None)      # the same solve again, warm
+    lib.b200x_stream_timer(0)
+    lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
+    solve_ms2 = lib.b200x_stream_timer(1)
     # one pass of the learned predictor's seed kernel (untrained weights) on the same device
     from semiconductor_devices_simulator_b200 import learned as LR
     LR.load(lib, LR.init_params(lib.api3b_seed_nparam(), seed=0, out_scale=1.0))
@@ -112,7 +122,8 @@ def run_probe(a):
     seed_ms = lib.b200x_stream_timer(1) / 10
     print(json.dumps({"probe": f"{WL}_{mesh[0]}x{mesh[1]}x{mesh[2]} electron continuity", "nodes": w.N,
                       "precision": a.precision, "seed_kernel": seed_ok, "seed_ms": round(seed_ms, 4),
-                      "bicgstab_its": its, "r0": r0[0], "rn": rn[0],
+                      "bicgstab_its": its, "r0": r0[0], "rn": rn[0], "solve_ms": [round(solve_ms, 3), round(solve_ms2, 3)],
+                      "persistent": bool(lib.api3b_set_persist(-1, -1)),
                       "launches": int(lib.b200x_launches() - l0)}))
 
 
@@ -153,20 +164,64 @@ class Dist:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
 
+    def gather(self, obj):
+        """Every rank's `obj` as a list on rank 0 (None on the other ranks)."""
+        if self.world == 1:
+            return [obj]
+        objs = [None] * self.world
+        self.dist.all_gather_object(objs, obj)
+        return objs if self.rank == 0 else None
+
     def close(self):
         if self.world > 1:
             self.dist.destroy_process_group()
 
 
-def shard(items, rank, world):
-    """The units of `items` rank `rank` of `world` takes (round robin, every unit once)."""
-    return list(items)[rank::world]
+def shard(items, rank, world, weights=None):
+    """The units of `items` rank `rank` of `world` takes: every unit exactly once, balanced
+    by `weights` (the units' node counts: a solve's cost grows with them) - the largest
+    unit first, each to the rank with the least weight so far (ties to the lower rank).
+    Equal weights give a round robin."""
+    items = list(items)
+    wts = [1.0] * len(items) if weights is None else [float(x) for x in weights]
+    order = sorted(range(len(items)), key=lambda i: (-wts[i], i))
+    load = [0.0] * world
+    own = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        own[r].append(i)
+        load[r] += wts[i]
+    return [items[i] for i in sorted(own[rank])]
 
 
-def sweep_order(nsw, rank):
-    """The sweeps a rank solves in the Id-Vg workload: all of them (every GPU holds a full
-    replica of the workload), the first one rotated by the rank."""
-    return [(q + rank) % nsw for q in range(nsw)]
+def sweep_order(nsw, rank, world, replicate):
+    """The sweeps (drain biases) a rank solves: with `replicate` every rank solves the whole
+    family (independent replicas, weak scaling), else the family is split across the ranks
+    (each sweep on exactly one rank)."""
+    if replicate:
+        return [(q + rank) % nsw for q in range(nsw)]
+    return shard(range(nsw), rank, world)
+
+
+def gather_iv(dist, cur, nsw):
+    """Gather every rank's terminal currents to rank 0: `cur` maps a sweep index to its
+    points' (I per contact, Iflr per contact).  Returns, on rank 0, the family's array
+    (sweeps x points x contacts x 2: I, Iflr) in sweep order and how many ranks solved each
+    sweep; None elsewhere."""
+    mine = {int(k): np.asarray([[I, F] for I, F in v], dtype=np.float64).transpose(0, 2, 1)
+            for k, v in cur.items()}
+    parts = dist.gather(mine)
+    if parts is None:
+        return None
+    seen = [0] * nsw
+    arr = None
+    for part in parts:
+        for k, a in part.items():
+            seen[k] += 1
+            if arr is None:
+                arr = np.full((nsw,) + a.shape, np.nan)
+            arr[k] = a
+    return arr, seen
 
 
 # ------------------------------------------------------------------ clocks
@@ -216,6 +271,10 @@ class Clocks:
 WORKLOADS = {
     "nmosfet": {"mesh": (120, 80, 60), "build": lambda lib, n: D.nmosfet(lib, n=n)},
     "finfet": {"mesh": (96, 96, 64), "build": lambda lib, n: D.finfet(lib, n=n)},
+    # the large-device configuration: the vertical power cell (10 x 60 x 10 um, 8.4M nodes),
+    # drain 0..50 V in 1 V steps at 16 gate biases (2.5..10 V), one instance per gate bias
+    "power_cell": {"mesh": (256, 256, 128),
+                   "build": lambda lib, n: D.power_cell(lib, n=n, vgs=tuple(np.round(np.arange(2.5, 10.01, 0.5), 6)))},
     # the n-MOSFET's device given as a general (graph) mesh: the graph path's ELL kernels and
     # aggregation multigrid (FP64; no launch-shape tuning or learned seed on graphs)
     "graph_mosfet": {"mesh": (120, 80, 60),
@@ -267,8 +326,8 @@ def sweep_points(lib, w, s, fields=False, npts=None, out=None):
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a kernel class on
-# the default 120x80x60 mesh, from one ncu capture (profiles/vcycle_f32_kernels_nmosfet_120x80x60.md:
-# the launch mix of one V-cycle weighted by its level-0/1/2 passes)
+# the default 120x80x60 mesh, measured by one ncu capture of the bench's --probe case (the
+# launch mix of one V-cycle weighted by its level-0/1/2 passes)
 NCU_TRAFFIC = {"smooth_black_f32": 10.9e6}
 
 
@@ -316,13 +375,18 @@ def cpu_baseline(mesh, seconds):
 class Sweeper:
     """One solver instance on its own host thread and CUDA stream, solving one sweep."""
 
-    def __init__(self, lib, mesh, sweep_index, dev, precision):
+    def __init__(self, lib, mesh, sweep_index, dev, precision, solver=None, npts=None):
         self.lib, self.mesh, self.si = lib, mesh, sweep_index
+        self.npts_limit = npts
         self.h = lib.api3b_new()
         self.dev = dev
         self.w = None
         self.precision = precision
+        self.solver = solver
         self.cur = []
+
+    def free(self):
+        self.lib.api3b_free(self.h)
 
     def _use(self):
         self.lib.api3b_use(self.h)
@@ -334,6 +398,8 @@ class Sweeper:
         if self.w is None:
             self.w = build(self.lib, self.mesh)
             self.lib.api3_set_verbose(0)
+            if self.solver:
+                self.lib.api3_set_solver(*self.solver)
         D.start_sweep(self.lib, self.w, self.w.sweeps[self.si])   # untimed: equilibrium + ramp
 
     def run(self, fields):
@@ -342,7 +408,8 @@ class Sweeper:
         t0 = time.perf_counter()
         g0 = self.lib.api3_get_stat(3)
         self.cur = []
-        self.npts, self.conv = sweep_points(self.lib, self.w, self.w.sweeps[self.si], fields=fields, out=self.cur)
+        self.npts, self.conv = sweep_points(self.lib, self.w, self.w.sweeps[self.si], fields=fields, out=self.cur,
+                                            npts=self.npts_limit)
         self.gummel = self.lib.api3_get_stat(3) - g0
         self.dev_s = self.lib.b200x_stream_timer(1) / 1e3
         self.wall = time.perf_counter() - t0
@@ -367,11 +434,85 @@ def rel_dI(cur, ref, on=1e-30):
     return worst
 
 
+# tight tolerances: inner solves to round-off, validate.py's Gummel tolerances
+TIGHT_ENV = {"SEMISIM_BRTOL": "1e-12", "SEMISIM_PCGRTOL": "1e-10"}
+TIGHT_SOLVER = (2000, 1000, 500, 1e-12, 1e-9, 1.0, 1.0)
+
+
+def tight_check(lib, workers, mesh):
+    """The metric's accuracy clause on the workload's own sweeps: this rank's sweeps
+    re-solved with both codes converged tightly, refined and FP64 (untimed); the refined
+    currents' largest relative distance to the FP64 ones, over every point and every
+    terminal above its round-off floor."""
+    res = {}
+    t0 = time.perf_counter()
+    for p in (1, 0):
+        old = {k: os.environ.get(k) for k in TIGHT_ENV}
+        os.environ.update(TIGHT_ENV)                     # read by api3_init
+        ws = [Sweeper(lib, mesh, s.si, s.dev, p, solver=TIGHT_SOLVER) for s in workers]
+        try:
+            concurrent(ws, lambda s: s.prepare())
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        concurrent(ws, lambda s: s.run(False))
+        res[p] = {s.si: list(s.cur) for s in ws}
+        conv = sum(s.conv for s in ws)
+        npts = sum(s.npts for s in ws)
+        for s in ws:
+            s.free()
+        if conv != npts:
+            return {"error": f"{npts - conv} of {npts} points did not converge at tight tolerances (precision {p})"}
+    return {"all_points": max(rel_dI(res[1][k], res[0][k]) for k in res[0]),
+            "on_state_Id_gt_1nA": max(rel_dI(res[1][k], res[0][k], on=1e-9) for k in res[0]),
+            "points": sum(len(v) for v in res[0].values()), "seconds": round(time.perf_counter() - t0, 1),
+            "solver": list(TIGHT_SOLVER), "env": TIGHT_ENV,
+            "note": "refined vs FP64, both converged tightly, every point of the step, terminals above their "
+                    "round-off floor"}
+
+
+def gummel_floor(lib, workers):
+    """The fewest Gummel iterations any starting guess can give one step: every point of
+    this rank's sweeps solved once along the sweep (its converged state kept), then solved
+    again starting from that converged state itself (api3_set_state at the point's bias,
+    then api3_resolve, which runs the Gummel loop at the same bias until its acceptance test
+    passes).  A learned seed can save at most (linear-guess iterations - this floor)."""
+    tot = pts = 0
+    for s in workers:
+        s._use()
+        s.prepare()
+        w, sw = s.w, s.w.sweeps[s.si]
+        N = w.N
+        states = []
+        for v in sw["V"][1:]:
+            for cid, vv in D.bias_vector(w, sw, v).items():
+                lib.api3_set_contact_V(cid, vv)
+            lib.api3_resolve()
+            st = [np.empty(N) for _ in range(3)]
+            lib.api3_get_state(*(abi.dptr(x) for x in st))
+            states.append(st)
+        for v, st in zip(sw["V"][1:], states):
+            for cid, vv in D.bias_vector(w, sw, v).items():
+                lib.api3_set_contact_V(cid, vv)
+            lib.api3_set_state(*(abi.dptr(x) for x in st))
+            g0 = lib.api3_get_stat(3)
+            lib.api3_resolve()
+            tot += lib.api3_get_stat(3) - g0
+            pts += 1
+    return tot, pts
+
+
 def learned_step(a, lib, workers, step, cur, gummel_per_step, dist):
     """Train the learned predictor on the workload device's own sweeps at gate voltages
     shifted by half a step (both drain biases), then run one step of the workload with
     it.  Returns the measured block (Gummel iterations of one step with the linear guess,
     `gummel_per_step`, and with the learned one; points/s)."""
+    if not workers:                             # this rank holds no sweep: keep the collective steps
+        dist.barrier()
+        return None
     import torch
     from semiconductor_devices_simulator_b200 import learned as LR
     s0 = workers[0]
@@ -406,9 +547,14 @@ def learned_step(a, lib, workers, step, cur, gummel_per_step, dist):
         used.append(LR.stats(lib))
         lib.api3b_seed_enable(0)
     curl = {s.si: list(s.cur) for s in workers}
+    floor, fpts = gummel_floor(lib, workers)
     return {"points_per_s": round(pts / dev, 4), "unit": UNIT,
             "gummel_iterations_per_step": {"linear_guess": gummel_per_step,
-                                           "learned_guess": sum(s.gummel for s in workers)},
+                                           "learned_guess": sum(s.gummel for s in workers),
+                                           "converged_start_floor": int(floor)},
+            "floor_note": f"Gummel iterations of the same {fpts} points when each starts from its own converged "
+                          "solution (api3_set_state at its bias): the least any seed can reach under the "
+                          "acceptance test",
             "seeded_steps": int(sum(u[0] for u in used)), "fallbacks": int(sum(u[1] for u in used)),
             "max_rel_dI_vs_linear_on_state": max(rel_dI(curl[k], cur[k], on=1e-9) for k in cur),
             "train": {"rows": int(sum(f.shape[0] for f in feats)), "steps": 6000, "seconds": round(tr.seconds, 2),
@@ -422,22 +568,27 @@ def run_b200(a, dist):
     mesh = mesh_of(a)
     lib = S.load()
     lib.b200x_set_device(dist.local)
-    nsw = 5 if WL == "finfet" else 2          # the drain biases of the workload, one sweep each
+    nsw = {"finfet": 5, "power_cell": 16}.get(WL, 2)   # the sweeps of the workload, one instance each
     graph = WL.startswith("graph")
     prec = 1 if a.precision == "refined" and not graph else 0
+    # the n-MOSFET family is replicated on every GPU (independent characterisation jobs:
+    # weak scaling); the FinFET's five drain-bias sweeps and the power cell's sixteen
+    # gate-bias sweeps are split across the GPUs
+    replicate = WL not in ("finfet", "power_cell")
 
     def make(p):
-        return [Sweeper(lib, mesh, si, dist.local, p) for si in sweep_order(nsw, dist.rank)]
+        return [Sweeper(lib, mesh, si, dist.local, p, npts=a.points or None)
+                for si in sweep_order(nsw, dist.rank, dist.world, replicate)]
     workers = make(prec)
 
     def step(ws, fields=False):
-        """Both sweeps, concurrently (one instance, thread and stream each)."""
+        """The rank's sweeps, concurrently (one instance, thread and stream each)."""
         concurrent(ws, lambda s: s.prepare())
         dist.barrier()
         t0 = time.perf_counter()
         concurrent(ws, lambda s: s.run(fields))
         wall = time.perf_counter() - t0
-        return (sum(s.npts for s in ws), sum(s.conv for s in ws), max(s.dev_s for s in ws), wall)
+        return (sum(s.npts for s in ws), sum(s.conv for s in ws), max([s.dev_s for s in ws] or [0.0]), wall)
 
     tune = None
     if not a.no_autotune and not graph:       # launch shapes, one instance at a time (untimed)
@@ -462,6 +613,7 @@ def run_b200(a, dist):
     launches = int(lib.b200x_launches() - l0)
     clk = clocks.stop()
     cur = {s.si: list(s.cur) for s in workers}
+    iv = gather_iv(dist, cur, nsw)            # the family's I-V arrays on rank 0
     # e2e: the same steps with every point's psi, n, p copied to host buffers
     e_pts = 0
     e_wall = 0.0
@@ -472,7 +624,7 @@ def run_b200(a, dist):
         e_pts, e_wall = tot_pts, tot_wall
     # roofline: one more step with every launch timed by CUDA events on the solver stream
     prof = None
-    if not a.no_profile:                      # event timing is per thread: one sweep alone
+    if not a.no_profile and workers:          # event timing is per thread: one sweep alone
         s0 = workers[0]
         s0.prepare()
         nk = lib.b200x_prof(1)
@@ -497,19 +649,30 @@ def run_b200(a, dist):
             npts, conv, dev_s, wall = step(w64)
             f_pts += npts; f_dev += dev_s
         cur64 = {s.si: list(s.cur) for s in w64}
+        per_rank = len(sweep_order(nsw, 0, dist.world, replicate))   # the most sweeps a rank holds
         for i in range(a.steps):
-            for s in w64:
-                s.prepare()
+            for q in range(per_rank):
+                if q < len(w64):
+                    w64[q].prepare()
                 dist.barrier()
-                s.run(False)
-                s_pts += s.npts; s_dev += s.dev_s
-        f64 = (dist.sum(f_pts), dist.max(f_dev), max(rel_dI(cur[k], cur64[k]) for k in cur),
-               dist.sum(s_pts), dist.max(s_dev), max(rel_dI(cur[k], cur64[k], on=1e-9) for k in cur))
+                if q < len(w64):
+                    w64[q].run(False)
+                    s_pts += w64[q].npts; s_dev += w64[q].dev_s
+        f64 = (dist.sum(f_pts), dist.max(f_dev), dist.max(max([rel_dI(cur[k], cur64[k]) for k in cur] or [0.0])),
+               dist.sum(s_pts), dist.max(s_dev),
+               dist.max(max([rel_dI(cur[k], cur64[k], on=1e-9) for k in cur] or [0.0])))
+        for s in w64:
+            s.free()
     # the learned predictor: trained (untimed) on this device's own solutions at gate
     # voltages half a step off the workload's, then one step of the workload seeded by it
     learned = None
     if not a.no_learned and not graph:
         learned = learned_step(a, lib, workers, step, cur, gummel, dist)
+    tight = None
+    if prec == 1 and not a.no_fp64 and not a.no_tight and workers:
+        tight = tight_check(lib, workers, mesh)
+    # the batching configuration (64 pn-diode variants), measured in the same run
+    batch = run_batch(a, dist) if WL == "nmosfet" and not a.no_batch else None
     T = dist.max(tot_dev)
     pts_all = dist.sum(tot_pts)
     e_T = dist.max(e_wall)
@@ -537,20 +700,23 @@ def run_b200(a, dist):
                        for r in sorted(prof, key=lambda r: -r[1]) if r[2] > 0}
         h2d = 8 * 4 * len(w.contacts)                              # contact voltages per point
         d2h = 3 * 8 * w.N + 16 * len(w.contacts)                   # psi, n, p + currents per point
-        npts_step = (len(w.sweeps[0]["V"]) - 1) * nsw
+        npts_step = int(pts_all) // max(a.steps, 1)
         value = pts_all / T
         out = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * T / a.steps, 2),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "weak" if replicate else "strong", "vs_baseline": None,
             "dtype": "f32 inner solves refined in f64 (f64 residuals, physics, currents)" if prec else "f64",
             "data": "synthetic (device built from the workload definition)",
             "config": dict({"workload": workload_name(mesh),
                             "nodes": w.N, "points_per_step": npts_step}, **workload_config(w),
                            **{"solver": list(D.GUI_SOLVER), "precision": "fp64" if graph else a.precision,
                               "launch_shapes": tune,
-                              "parallelism": f"replicas{dist.world}, {nsw} concurrent sweeps per GPU "
-                                             "(instance + stream each)",
+                              "parallelism": (f"replicas{dist.world}, {nsw} concurrent sweeps per GPU "
+                                              "(instance + stream each)") if replicate else
+                                             (f"sweeps split over {dist.world} GPU(s) by node count, concurrent "
+                                              "sweeps per GPU (instance + stream each)"),
+                              "point_set": f"every point of the {nsw} sweeps after their first, each step",
                               "l2": f"state of {w.N} nodes (~{w.N * 760 / 1e9:.2f} GB) exceeds the 126 MB L2; "
                                     "no flush"}),
             "converged_points": tot_conv, "wall_s": round(tot_wall, 3),
@@ -570,23 +736,37 @@ def run_b200(a, dist):
             out["max_rel_dI_vs_fp64"] = {"all_points": f64[2], "on_state_Id_gt_1nA": f64[5],
                                          "note": "both at the workload's default tolerances; terminals above "
                                                  "their round-off floor"}
+        if iv is not None:
+            arr, seen = iv
+            out["iv_gather"] = {"shape": list(arr.shape), "layout": "sweeps x points x contacts x (I, Iflr)",
+                                "solved_per_sweep": seen, "complete": bool(np.isfinite(arr).all())}
+        if tight:
+            out["max_rel_dI_vs_fp64_tight"] = tight
+        if batch:
+            out["diodes64"] = batch
         if learned:
             out["learned_seed"] = learned
-        if dist.world == 1 and not a.no_cpu_baseline:
+        if dist.world == 1 and not a.no_cpu_baseline and WL != "power_cell":   # 8.4M nodes: hours on the host
             cb = cpu_baseline(mesh, a.cpu_seconds)
             if cb:
                 cb, rcur = cb
                 out["cpu_baseline"] = cb
+                last = [(list(p[:, 0]), list(p[:, 1])) for p in iv[0][nsw - 1]]     # the gathered last sweep
                 out["max_rel_dI_vs_reference"] = {
-                    "all_points": rel_dI(cur[nsw - 1], rcur), "on_state_Id_gt_1nA": rel_dI(cur[nsw - 1], rcur, on=1e-9),
+                    "all_points": rel_dI(last, rcur), "on_state_Id_gt_1nA": rel_dI(last, rcur, on=1e-9),
                     "note": "the reference core's sampled points; off-state currents converge to ~1e-3 in either "
                             "code at the workload's default tolerances"}
     return out
 
 
 def run_reference(a, dist):
-    """The reference's own CPU core on the same workload: each step a bounded sample
-    (the first points of one sweep), all host threads."""
+    """The reference's own CPU core on the same workload, all host threads.  The workload's
+    step is every point of its sweeps after the first (48 for the n-MOSFET); a reference
+    step times a window of 3 consecutive points of that sequence, and the windows slide
+    through it from step to step, so that over the timed steps every point of the GPU arm's
+    step is timed (the windows cycle; catching up to a window's start - a new sweep's
+    api3_solve and any points before it - is untimed).  Each window continues from the
+    previous point exactly as the GPU arm's sweep does."""
     if dist.rank != 0:
         return None
     mesh = mesh_of(a)
@@ -598,26 +778,51 @@ def run_reference(a, dist):
     ref.api3_set_threads(cores)
     w = build(ref, mesh)
     npts = 3
-    tot = e_tot = 0.0
+    seq = [(si, q) for si in range(len(w.sweeps)) for q in range(1, len(w.sweeps[si]["V"]))]
+    nwin = len(seq) // npts
+    cur_si, next_q = None, None
+    tot = 0.0
     pts = 0
+    timed = set()
+
+    def resolve(s, q):
+        for cid, vv in D.bias_vector(w, s, s["V"][q]).items():
+            ref.api3_set_contact_V(cid, vv)
+        return ref.api3_resolve()
+
     for i in range(a.warmup + a.steps):
-        s = w.sweeps[i % len(w.sweeps)]
-        D.start_sweep(ref, w, s)
+        win = seq[(i % nwin) * npts:(i % nwin + 1) * npts]
+        si, q0 = win[0]
+        s = w.sweeps[si]
+        if cur_si != si or next_q is None or next_q > q0:
+            D.start_sweep(ref, w, s)                  # untimed: equilibrium + ramp to the sweep's start
+            cur_si, next_q = si, 1
+        while next_q < q0:                            # untimed: up to the window's first point
+            resolve(s, next_q)
+            next_q += 1
         t0 = time.perf_counter()
-        n, conv = sweep_points(ref, w, s, fields=False, npts=npts)
+        for _, q in win:
+            resolve(s, q)
         dt = time.perf_counter() - t0
+        next_q = q0 + npts
         if i >= a.warmup:
             tot += dt
-            pts += n
+            pts += npts
+            timed.update(win)
     v = pts / tot
+    cfg = dict({"workload": workload_name(mesh), "nodes": w.N, "points_per_step": npts}, **workload_config(w),
+               **{"solver": list(D.GUI_SOLVER), "precision": "fp64", "parallelism": f"cpu, {cores} threads",
+                  "point_set": f"windows of {npts} consecutive points sliding through the {len(seq)} points of "
+                               f"the workload step ({len(timed)} of them timed over the run)"})
     return {"metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": dist.world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(1e3 * tot / a.steps, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
             "data": "synthetic (device built from the workload definition)",
-            "config": dict({"workload": workload_name(mesh), "nodes": w.N,
-                            "points_per_step": npts, "parallelism": "cpu"}, **workload_config(w)),
+            "config": cfg,
             "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"first {npts} points of one Id-Vg sweep per step"},
+                             "sample": f"{npts} consecutive points per step, windows sliding through all "
+                                       f"{len(seq)} points of the workload step; {len(timed)} distinct points "
+                                       "timed"},
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -634,7 +839,8 @@ def run_batch(a, dist):
     lib = S.load()
     lib.b200x_set_device(dist.local)
     prec = 1 if a.precision == "refined" else 0
-    var = shard(D.diode_variants(64)[:a.variants or None], dist.rank, dist.world)
+    allv = D.diode_variants(64)[:a.variants or None]
+    var = shard(allv, dist.rank, dist.world, weights=[int(np.prod(v["n"])) for v in allv])
     hs = [lib.api3b_new() for _ in var]
     ws = [None] * len(var)
 

@@ -11,10 +11,14 @@
  *
  * The solve path (prepare, equilibrium, Newton-Poisson, Scharfetter-Gummel continuity,
  * Gummel / Anderson, continuation, terminal currents) runs on the GPU; set-up calls only
- * record the device and work without one.  Models outside the library's scope (gate
- * tunnelling, thermionic-emission contacts, impact and incomplete ionisation, quantum
- * confinement, surface mobility, deep traps) and prism meshes make the solve return 0
- * with a message on stderr; their standalone evaluators return NaN.
+ * record the device and work without one.  Every physics model of the reference runs
+ * there too, on tensor and on general (prism / graph, api3_set_mesh_graph) meshes: gate
+ * tunnelling, thermionic-emission metal contacts, impact and incomplete ionisation, MLDA
+ * quantum confinement, Lombardi surface mobility with the 4H-SiC Coulomb term and deep
+ * traps.  The standalone model evaluators (api3_tun_eval, api3_mlda_factor,
+ * api3_lombardi, api3_coulomb_inv) run on the host and return the reference's values.
+ * Without a CUDA device the solve entries return 0 with a message on stderr; there is no
+ * CPU solve path.
  */
 #ifndef SEMISIM_B200_H
 #define SEMISIM_B200_H
@@ -239,6 +243,17 @@ int api3b_free(int h);
 int api3b_set_precision(int mode);
 int api3b_get_precision(void);
 
+/* No counterpart in the reference.  Persistent linear solves (library-wide): with mode 1
+   (the default; SEMISIM_B200_PERSIST=0 switches it off) every multigrid-preconditioned
+   PCG / BiCGSTAB solve of an instance runs as one cooperative kernel launch - all its
+   iterations, V-cycles and FP64 refinement steps, with grid-wide barriers between the
+   dependent passes; mode 0 launches one kernel per pass inside device-looped CUDA graphs.
+   Both stop on the same rules.  `blocks` caps the blocks of one launch (0: every SM's
+   worth; SEMISIM_B200_PBLOCKS sets it at start-up), so that instances solved concurrently
+   from several host threads can share the GPU.  -1 leaves a value unchanged.  Returns the
+   previous mode. */
+int api3b_set_persist(int mode, int blocks);
+
 /* No counterpart in the reference (it has no learned component).  Learned sweep predictor
    of the current instance: a per-node MLP (48 features -> 3 x 128 SiLU -> 3, BF16 weights,
    FP32 accumulation) corrects the sweep predictor's linear extrapolation
@@ -279,7 +294,7 @@ double api3b_autotune(int mode);
    Iflr and converged flags conv (both may be null).  The current instance is unchanged.
    Returns the number of converged solves, -1 without a solution or on a device error.
    api3b_resolve_batch_free releases the current instance's workers (they are kept for
-   later calls; api3b_free does not release them). */
+   later calls; api3b_free releases the freed instance's workers too). */
 int api3b_resolve_batch(int n, const double *V, double *I, double *Iflr, int *conv, int workers);
 int api3b_resolve_batch_free(void);
 int api3b_tune_get(int *rpb, int *grid_cap, int *small_nodes, int *zcap);
@@ -289,7 +304,9 @@ int api3b_tune_get(int *rpb, int *grid_cap, int *small_nodes, int *zcap);
    not acceptable): r = b - A x for a 7-point stencil A (7 arrays of N = Nx*Ny*Nz doubles:
    diagonal, x-, x+, y-, y+, z-, z+), norms[0] = ||r||_2 and norms[1] = the BiCGSTAB
    rounding floor sqrt(sum_a (sum_b |A_ab x_b| + |b_a|)^2).  A7, x, b, r: the caller's
-   device buffers on one GPU; norms: host.  Allocates nothing: its reduction scratch is a
+   device buffers on one GPU (each checked; a host buffer, a buffer on another GPU or an r
+   that overlaps A7, x or b is refused before any launch); norms: host.  The calling
+   thread's current device is restored on return.  Allocates nothing: its reduction scratch is a
    fixed ~38 KB device array that every GPU loading the library holds until exit.  At most
    2^30 nodes (larger sizes are refused with a message).  The first call on a GPU looks up
    that array (cudaGetSymbolAddress): make it before any stream capture.  Calls share the

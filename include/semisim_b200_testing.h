@@ -72,6 +72,11 @@ int b200x_mg_level(int L, int *dims, double *A7, double *pw);
 int b200x_bicgstab(int maxit, double rtol, double atol, int qsign, const double *x0, double *sol, double *rn,
                    double *r0);
 int b200x_pcg(int maxit, double rtol, double *sol);
+/* The persistent solves' bounded barrier wait, exercised: a cooperative launch of nb
+   blocks on the current instance's barrier record whose last block never arrives.
+   Returns the error word (1 when the others gave up after wait_s seconds) and in
+   *gave_up how many blocks reported it (nb - 1); -1 if the launch failed. */
+int b200x_persist_probe(int nb, double wait_s, int *gave_up);
 /* floating-block balance of a continuity solution (in place) */
 int b200x_float_fix(int hole, double *sol);
 /* learned predictor on the present history arrays (22-24 h1, 25-27 e2 of b200x_set /

@@ -121,6 +121,7 @@ EXTRA = {
     # linear-solve precision of the current instance (0 FP64, 1 FP32 refined in FP64)
     "api3b_set_precision": (_I, [_I]),
     "api3b_get_precision": (_I, []),
+    "api3b_set_persist": (_I, [_I, _I]),
     # learned sweep predictor of the current instance
     "api3b_seed_set_model": (_I, [ctypes.POINTER(ctypes.c_float), _I]),
     "api3b_seed_enable": (_I, [_I]),

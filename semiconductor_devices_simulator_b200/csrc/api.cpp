@@ -770,12 +770,20 @@ int api3b_set_precision(int mode) {
     d.precision = mode < -1 ? -1 : (mode > 1 ? 1 : mode);
     return old;
 }
+// persistent linear solves on (1) / off (0), blocks per launch (0: every SM's worth); -1
+// keeps a value.  Returns the previous mode.
+int api3b_set_persist(int mode, int blocks) {
+    const int old = persist_enabled();
+    persist_set(mode, blocks);
+    return old;
+}
 // precision in effect on the current instance (0 FP64, 1 refined FP32)
 int api3b_get_precision(void) { return use_mixed(g_dev); }
 int api3b_free(int h) {
     std::lock_guard<std::mutex> lk(g_reg_mu);
     if (h < 1 || h > (int)g_reg.size() || !g_reg[h - 1]) return 0;
     if (t_cur == g_reg[h - 1].get()) t_cur = nullptr;
+    batch_pool_release(g_reg[h - 1].get());   // its batched-resolve workers go with it
     gpu_free(*g_reg[h - 1]);
     g_reg[h - 1].reset();
     return 1;

@@ -64,6 +64,19 @@ int clone_into(Inst &w, Inst &src) {
 }
 }  // namespace
 
+namespace ss {
+// release the batched-resolve workers of `src` (their device memory and streams); called
+// when the source instance itself is freed, so no worker outlives it
+int batch_pool_release(const Inst *src) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pool.find(src);
+    if (it == g_pool.end()) return 0;
+    for (auto &w : it->second) gpu_free(*w);
+    g_pool.erase(it);
+    return 1;
+}
+}  // namespace ss
+
 extern "C" {
 
 // Solve n bias vectors (V: n x ncon volts, contact order) from the current instance's
@@ -111,14 +124,6 @@ int api3b_resolve_batch(int n, const double *V, double *I, double *Iflr, int *co
 }
 
 // release the worker instances of the current instance's batched resolves
-int api3b_resolve_batch_free(void) {
-    Inst &src = *b200_global_dev();
-    std::lock_guard<std::mutex> lk(g_pool_mu);
-    auto it = g_pool.find(&src);
-    if (it == g_pool.end()) return 0;
-    for (auto &w : it->second) gpu_free(*w);
-    g_pool.erase(it);
-    return 1;
-}
+int api3b_resolve_batch_free(void) { return batch_pool_release(b200_global_dev()); }
 
 }  // extern "C"

@@ -1,0 +1,990 @@
+// Persistent linear solves: one cooperative launch runs a whole multigrid-preconditioned
+// Krylov solve of an instance - every iteration, both V-cycles of a BiCGSTAB iteration,
+// and for the refined path every FP64 refinement step around its FP32 inner solves -
+// with grid-wide barriers between the dependent passes instead of kernel boundaries.
+//
+// Why: on a 576k-node device a V-cycle is ~26 dependent passes of 1-10 MB each.  Launched
+// one kernel per pass (the device-looped CUDA graphs of kernels_la.cu) every pass costs a
+// launch and a grid ramp (~6-9 us) for ~1-2 us of memory traffic; a resident grid pays a
+// barrier (~1-2 us) instead and keeps the level descriptors and the small levels on chip.
+//
+// Layout of the work:
+//   * every block runs the passes of the large levels (0 .. Ls-1) as grid-stride loops
+//     over the pass's index space, one barrier after each pass;
+//   * block 0 keeps the small levels (Ls .. coarsest) in its shared memory for the whole
+//     solve (staged once at the start, not per V-cycle) and runs their part of every
+//     V-cycle with block barriers, while the other blocks wait at the next grid barrier;
+//   * reductions: each block writes its partial record, and after the barrier every block
+//     sums all records in block order, so every block holds bit-identical totals and takes
+//     the same stop decisions with no extra barrier.
+//
+// The arithmetic per node is the per-pass kernels' (the shared helpers of la_common.cuh);
+// the stop rules are the reference's (pcg semiconductor_3d.c:2182-2210, bicgstab_core
+// :2234-2320) as the per-pass path applies them, and the refinement the same FP64 rule.
+//
+// Safety: the launch is cooperative (all blocks co-resident).  Every barrier wait is
+// bounded: after 2 s of waiting a block sets the error word and leaves, every other block
+// leaves at its next wait, and the host restores the solve's start and repeats it on the
+// per-pass path.
+#include <cstdio>
+#include <cstdlib>
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "la_common.cuh"
+#include "prof.h"
+
+namespace ss {
+
+constexpr int PG_TPB = 1024;
+constexpr unsigned long long PG_WAIT_NS = 2000000000ull;    // longest barrier wait of a solve (2 s)
+
+enum PKind { PK_PCG = 0, PK_BICG = 1, PK_REFINED = 2 };
+
+struct PArgs {
+    int Ls;          // first level of the shared-memory part (>= 1)
+    int deep;        // levels (from the finest) with two smoother applications
+    int sweeps2;     // 1: the second application is on
+    int maxsteps;    // refinement steps at most (PK_REFINED)
+    int fuse_up;     // 1: prolongation deferred into the residual and post-smoothing passes
+    int setup;       // 1: build the hierarchy first (the per-launch mg_setup of kernels_la.cu)
+    int qsign;       // its Slotboom weights: 0 none (Poisson), +1 electrons, -1 holes
+    double alpha;    // prolongation factor
+    double rtol, atol;   // stop rule of the FP64 BiCGSTAB start (PK_BICG)
+};
+
+__device__ __forceinline__ unsigned long long pg_clock() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ unsigned pg_ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// per-block state of a persistent launch
+struct PS {
+    PGrid *g;
+    unsigned target;   // arrivals the next barrier waits for
+    int rb;            // reduction buffer of the next reduction
+    int tid, nth;      // thread index in the grid, threads in the grid
+    unsigned long long wait_ns;   // longest wait at one barrier
+};
+
+// Grid-wide barrier: every block arrives (release), thread 0 waits for all arrivals
+// (acquire), then the block proceeds.  Returns false when the launch is being abandoned.
+__device__ __forceinline__ bool pg_sync(PS &s) {
+    __shared__ int s_ok;
+    __syncthreads();
+    s.target += gridDim.x;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&s.g->count, 1u);
+        int ok = 1;
+        unsigned long long t0 = 0;
+        unsigned it = 0;
+        while ((int)(pg_ld_acquire(&s.g->count) - s.target) < 0) {
+            if ((++it & 255u) == 0) {
+                if (*(volatile unsigned *)&s.g->err) { ok = 0; break; }
+                const unsigned long long t = pg_clock();
+                if (!t0) t0 = t;
+                else if (t - t0 > s.wait_ns) { atomicExch(&s.g->err, 1u); ok = 0; break; }
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Sum NV (<= 4) values over the grid; every block returns the same totals in every thread.
+template <int NV>
+__device__ __forceinline__ bool pg_sum(PS &s, double (&v)[NV]) {
+    __shared__ double tot[4];
+    block_sum<NV>(v);
+    double *buf = s.g->red[s.rb];
+    s.rb ^= 1;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < NV; q++) buf[blockIdx.x * 4 + q] = v[q];
+    if (!pg_sync(s)) return false;
+    if (threadIdx.x < 32) {
+        double a[NV];
+#pragma unroll
+        for (int q = 0; q < NV; q++) a[q] = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32)
+#pragma unroll
+            for (int q = 0; q < NV; q++) a[q] += __ldcg(buf + b * 4 + q);
+        warp_sum<NV>(a);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int q = 0; q < NV; q++) tot[q] = a[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; q++) v[q] = tot[q];
+    return true;
+}
+
+// ---------------------------------------------------------------- grid passes of a level
+template <class T>
+__device__ __forceinline__ void pg_smooth(const LevView<T> &v, int mode, int color, const PS &s) {
+    const int hx = (v.Nx + 1) >> 1, tot = hx * v.Ny * v.Nz;
+    for (int t = s.tid; t < tot; t += s.nth) {
+        const int row = t / hx, ti = t - row * hx;
+        const int l = row / v.Ny, j = row - l * v.Ny;
+        const int i = 2 * ti + ((j + l + color) & 1);
+        if (i < v.Nx) smooth_node<T>(v, i + v.Nx * row, i, j, l, mode, color);
+    }
+}
+// weighted residual of every fine node summed into its 2x2x2 aggregate: 8 lanes per
+// coarse node (lane bits di, dj, dl), whole warps per loop trip
+template <class T>
+__device__ __forceinline__ void pg_resid_restrict(const LevView<T> &f, const LevelT<T> &cl, const T *w, const PS &s) {
+    const int nK = ((cl.N + 3) >> 2) << 5;
+    for (int t = s.tid; t < nK; t += s.nth) {
+        const int K = t >> 3, sub = t & 7;
+        T val = 0;
+        if (K < cl.N) {
+            const Node c = unidx(K, cl.Nx, cl.Ny);
+            const int di = sub & 1, dj = (sub >> 1) & 1, dl = sub >> 2;
+            const int i = f.cx ? 2 * c.i + di : c.i, j = f.cy ? 2 * c.j + dj : c.j, l = f.cz ? 2 * c.l + dl : c.l;
+            const bool ok = i < f.Nx && j < f.Ny && l < f.Nz && (f.cx || di == 0) && (f.cy || dj == 0) &&
+                            (f.cz || dl == 0);
+            if (ok) {
+                const int k = i + f.Nx * (j + f.Ny * l);
+                const T r = f.b[k] - lv_apply<T>(f, f.x, k, i, j, l);
+                val = w ? w[k] * r : r;
+            }
+        }
+        val += __shfl_xor_sync(0xffffffffu, val, 1);
+        val += __shfl_xor_sync(0xffffffffu, val, 2);
+        val += __shfl_xor_sync(0xffffffffu, val, 4);
+        if (sub == 0 && K < cl.N) cl.b[K] = val;
+    }
+}
+template <class T>
+__device__ __forceinline__ void pg_prolong(const LevView<T> &f, const LevelT<T> &cl, T al, const PS &s) {
+    for (int k = s.tid; k < f.N; k += s.nth) {
+        const Node a = unidx(k, f.Nx, f.Ny);
+        const int I = f.cx ? a.i >> 1 : a.i, J = f.cy ? a.j >> 1 : a.j, K = f.cz ? a.l >> 1 : a.l;
+        f.x[k] += al * f.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+    }
+}
+template <class T>
+__device__ __forceinline__ void pg_resid(const LevView<T> &f, const PS &s) {
+    for (int k = s.tid; k < f.N; k += s.nth) {
+        const Node a = unidx(k, f.Nx, f.Ny);
+        f.r[k] = f.b[k] - lv_apply<T>(f, f.x, k, a.i, a.j, a.l);
+    }
+}
+
+// The way up, with the prolongation deferred: the residual pass reads the prolonged
+// x + al pw P xc at each stencil point without writing it, and each post-smoothing half
+// sweep adds the prolongation to its own colour's nodes before smoothing them - the same
+// operations as a prolongation pass followed by a residual pass, one barrier fewer.
+template <class T>
+__device__ __forceinline__ T xprol(const LevView<T> &f, const LevelT<T> &cl, T al, int m, int i, int j, int l) {
+    const int I = f.cx ? i >> 1 : i, J = f.cy ? j >> 1 : j, K = f.cz ? l >> 1 : l;
+    return f.x[m] + al * f.pw[m] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+}
+template <class T>
+__device__ __forceinline__ void pg_prolong_resid(const LevView<T> &f, const LevelT<T> &cl, T al, const PS &s) {
+    const int NxNy = f.Nx * f.Ny;
+    for (int k = s.tid; k < f.N; k += s.nth) {
+        const Node a = unidx(k, f.Nx, f.Ny);
+        const int i = a.i, j = a.j, l = a.l;
+        T sum = f.a(0, k) * xprol<T>(f, cl, al, k, i, j, l);
+        if (i > 0) sum += f.a(1, k) * xprol<T>(f, cl, al, k - 1, i - 1, j, l);
+        if (i < f.Nx - 1) sum += f.a(2, k) * xprol<T>(f, cl, al, k + 1, i + 1, j, l);
+        if (j > 0) sum += f.a(3, k) * xprol<T>(f, cl, al, k - f.Nx, i, j - 1, l);
+        if (j < f.Ny - 1) sum += f.a(4, k) * xprol<T>(f, cl, al, k + f.Nx, i, j + 1, l);
+        if (l > 0) sum += f.a(5, k) * xprol<T>(f, cl, al, k - NxNy, i, j, l - 1);
+        if (l < f.Nz - 1) sum += f.a(6, k) * xprol<T>(f, cl, al, k + NxNy, i, j, l + 1);
+        f.r[k] = f.b[k] - sum;
+    }
+}
+template <class T>
+__device__ __forceinline__ void pg_smooth_post(const LevView<T> &v, const LevelT<T> &cl, T al, int color, const PS &s) {
+    const int hx = (v.Nx + 1) >> 1, tot = hx * v.Ny * v.Nz;
+    for (int t = s.tid; t < tot; t += s.nth) {
+        const int row = t / hx, ti = t - row * hx;
+        const int l = row / v.Ny, j = row - l * v.Ny;
+        const int i = 2 * ti + ((j + l + color) & 1);
+        if (i >= v.Nx) continue;
+        const int k = i + v.Nx * row;
+        const int I = v.cx ? i >> 1 : i, J = v.cy ? j >> 1 : j, K = v.cz ? l >> 1 : l;
+        v.x[k] += al * v.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+        smooth_node<T>(v, k, i, j, l, 1, color);
+    }
+}
+
+#define PG_SYNC()                   \
+    do {                            \
+        if (!pg_sync(s)) return false; \
+    } while (0)
+
+// one V(1,1) cycle x = M^-1 b on the level-0 vectors (bsel -> xsel), the same passes as
+// the per-pass path (vcycle_t in kernels_la.cu)
+template <class T>
+__device__ bool pg_vcycle(const DevP &P, PS &s, const PArgs &a, const LevView<T> *sv, int bsel, int xsel, int wsel) {
+    const int nl = P.nlev, Ls = a.Ls;
+    const T al = (T)a.alpha;
+    for (int L = 0; L < Ls; L++) {
+        const LevView<T> v = levview<T>(P, L, bsel, xsel);
+        pg_smooth<T>(v, 0, 1, s);
+        PG_SYNC();
+        pg_smooth<T>(v, 0, 0, s);
+        PG_SYNC();
+        if (L < a.deep && a.sweeps2) {
+            pg_smooth<T>(v, 2, 1, s);
+            PG_SYNC();
+            pg_smooth<T>(v, 2, 0, s);
+            PG_SYNC();
+        }
+        pg_resid_restrict<T>(v, PT<T>::lev(P, L + 1), (L == 0 && wsel) ? PT<T>::w0(P) : nullptr, s);
+        PG_SYNC();
+    }
+    if (blockIdx.x == 0) {
+        const LevelT<T> &g = PT<T>::lev(P, Ls);
+        blk_copy<T>(sv[0].b, g.b, g.N);
+        __syncthreads();
+        blk_vcycle_small<T>(sv, Ls, nl, al);
+        blk_copy<T>(g.x, sv[0].x, g.N);
+    }
+    PG_SYNC();
+    for (int L = Ls - 1; L >= 0; L--) {
+        const LevView<T> v = levview<T>(P, L, bsel, xsel);
+        const LevelT<T> &cl = PT<T>::lev(P, L + 1);
+        if (a.fuse_up) {
+            pg_prolong_resid<T>(v, cl, al, s);
+            PG_SYNC();
+            pg_smooth_post<T>(v, cl, al, 1, s);
+            PG_SYNC();
+            pg_smooth_post<T>(v, cl, al, 0, s);
+            PG_SYNC();
+        } else {
+            pg_prolong<T>(v, cl, al, s);
+            PG_SYNC();
+            pg_resid<T>(v, s);
+            PG_SYNC();
+            pg_smooth<T>(v, 1, 1, s);
+            PG_SYNC();
+            pg_smooth<T>(v, 1, 0, s);
+            PG_SYNC();
+        }
+        if (L < a.deep && a.sweeps2) {
+            pg_smooth<T>(v, 2, 1, s);
+            PG_SYNC();
+            pg_smooth<T>(v, 2, 0, s);
+            PG_SYNC();
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.g->vcycles++;
+    return true;
+}
+
+// ---------------------------------------------------------------- Krylov loops
+// BiCGSTAB iterations (semiconductor_3d.c:2281-2316) on the records `sk` of precision T
+// while it is active; the reduction of rh.r for the next iteration rides on the x update.
+template <class T>
+__device__ bool pg_bicg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *sv, KrylovS &sk) {
+    T *r = PT<T>::wk(P, 0), *rh = PT<T>::wk(P, 1), *p = PT<T>::wk(P, 2), *v = PT<T>::wk(P, 3);
+    T *ph = PT<T>::wk(P, 4), *sh = PT<T>::wk(P, 5), *t = PT<T>::wk(P, 6);
+    T *x = PT<T>::sol(P);
+    T *const *A = PT<T>::A0(P);
+    const int N = P.N, Nx = P.Nx, Ny = P.Ny, Nz = P.Nz;
+    bool have_rho = false;
+    double rho_next = 0.0;
+    while (sk.active) {
+        double acc[2] = {0.0, 0.0}, a1[1] = {0.0};
+        if (have_rho) a1[0] = rho_next;
+        else {
+            for (int k = s.tid; k < N; k += s.nth) a1[0] += (double)rh[k] * (double)r[k];
+            if (!pg_sum<1>(s, a1)) return false;
+        }
+        if (threadIdx.x == 0) {
+            if (sk.it >= sk.maxit) { sk.active = 0; sk.status = 3; }
+            else {
+                sk.it++;
+                double rho1 = a1[0];
+                sk.pad0 = 0;
+                if (fabs(rho1) < 1e-300) {          // breakdown: restart the shadow residual
+                    rho1 = sk.rr;
+                    sk.rho = sk.al = sk.om = 1.0;
+                    sk.pad0 = 1;
+                    if (!(rho1 > 0.0)) { sk.active = 0; sk.status = 2; }
+                }
+                sk.rho1 = rho1;
+                sk.be = (rho1 / sk.rho) * (sk.al / sk.om);
+            }
+        }
+        __syncthreads();
+        if (!sk.active) break;
+        {
+            const T be = (T)sk.be, om = (T)sk.om;
+            const int restart = sk.pad0;
+            for (int k = s.tid; k < N; k += s.nth) {
+                if (restart) { rh[k] = r[k]; p[k] = r[k]; v[k] = 0; }
+                else p[k] = r[k] + be * (p[k] - om * v[k]);
+            }
+        }
+        PG_SYNC();
+        if (!pg_vcycle<T>(P, s, a, sv, 2, 4, 1)) return false;      // ph = M p
+        a1[0] = 0.0;
+        for (int k = s.tid; k < N; k += s.nth) {
+            const Node nd = unidx(k, Nx, Ny);
+            const T q = stencil_apply<T>(A, ph, k, nd.i, nd.j, nd.l, Nx, Ny, Nz);
+            v[k] = q;
+            a1[0] += (double)rh[k] * (double)q;
+        }
+        if (!pg_sum<1>(s, a1)) return false;
+        if (threadIdx.x == 0) {
+            if (fabs(a1[0]) < 1e-300) { sk.active = 0; sk.status = 2; }
+            else { sk.rv = a1[0]; sk.al = sk.rho1 / a1[0]; }
+        }
+        __syncthreads();
+        if (!sk.active) break;
+        const T al = (T)sk.al;
+        a1[0] = 0.0;
+        for (int k = s.tid; k < N; k += s.nth) {
+            const T q = r[k] - al * v[k];
+            r[k] = q;
+            a1[0] += (double)q * (double)q;
+        }
+        if (!pg_sum<1>(s, a1)) return false;
+        if (threadIdx.x == 0) {
+            sk.ss = a1[0];
+            if (sqrt(a1[0]) <= sk.tgt) { sk.half = 1; sk.rr = a1[0]; }
+        }
+        __syncthreads();
+        if (sk.half) {                                // half-step exit: x += al ph
+            for (int k = s.tid; k < N; k += s.nth) x[k] += al * ph[k];
+            if (threadIdx.x == 0) { sk.active = 0; sk.status = 1; }
+            PG_SYNC();
+            break;
+        }
+        if (!pg_vcycle<T>(P, s, a, sv, 0, 5, 1)) return false;      // sh = M r
+        acc[0] = acc[1] = 0.0;
+        for (int k = s.tid; k < N; k += s.nth) {
+            const Node nd = unidx(k, Nx, Ny);
+            const T q = stencil_apply<T>(A, sh, k, nd.i, nd.j, nd.l, Nx, Ny, Nz);
+            t[k] = q;
+            acc[0] += (double)q * (double)q;
+            acc[1] += (double)q * (double)r[k];
+        }
+        if (!pg_sum<2>(s, acc)) return false;
+        if (threadIdx.x == 0) {
+            sk.tt = acc[0]; sk.ts = acc[1];
+            sk.om = acc[0] > 0.0 ? acc[1] / acc[0] : 0.0;
+        }
+        __syncthreads();
+        {
+            const T om = (T)sk.om;
+            acc[0] = acc[1] = 0.0;
+            for (int k = s.tid; k < N; k += s.nth) {
+                x[k] += al * ph[k] + om * sh[k];
+                const T q = r[k] - om * t[k];
+                r[k] = q;
+                acc[0] += (double)q * (double)q;
+                acc[1] += (double)rh[k] * (double)q;
+            }
+        }
+        if (!pg_sum<2>(s, acc)) return false;
+        if (threadIdx.x == 0) {
+            sk.rr = acc[0];
+            const double rn = sqrt(acc[0]);
+            if (rn <= sk.tgt || sk.om == 0.0) { sk.active = 0; sk.status = 1; }
+            else {
+                if (rn < 0.99 * sk.rbest) { sk.rbest = rn; sk.stall = 0; }
+                else if (++sk.stall > 40) { sk.active = 0; sk.status = 2; }
+                if (sk.active) sk.rho = sk.rho1;
+            }
+        }
+        have_rho = true;
+        rho_next = acc[1];
+        __syncthreads();
+    }
+    return true;
+}
+
+// PCG iterations (semiconductor_3d.c:2194-2206) on the records `sk` while active
+template <class T>
+__device__ bool pg_pcg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *sv, KrylovS &sk) {
+    T *r = PT<T>::wk(P, 0), *z = PT<T>::wk(P, 1), *p = PT<T>::wk(P, 2), *q = PT<T>::wk(P, 3);
+    T *x = PT<T>::sol(P);
+    T *const *A = PT<T>::A0(P);
+    const int N = P.N, Nx = P.Nx, Ny = P.Ny, Nz = P.Nz;
+    while (sk.active) {
+        double acc[1] = {0.0};
+        for (int k = s.tid; k < N; k += s.nth) {
+            const Node nd = unidx(k, Nx, Ny);
+            const T vq = stencil_apply<T>(A, p, k, nd.i, nd.j, nd.l, Nx, Ny, Nz);
+            q[k] = vq;
+            acc[0] += (double)p[k] * (double)vq;
+        }
+        if (!pg_sum<1>(s, acc)) return false;
+        if (threadIdx.x == 0) {
+            sk.it++;
+            const double pq = acc[0];
+            if (!(pq > 0.0)) { sk.active = 0; sk.status = 2; sk.al = 0.0; }
+            else sk.al = sk.rz / pq;
+        }
+        __syncthreads();
+        if (!sk.active) break;
+        {
+            const T al = (T)sk.al;
+            for (int k = s.tid; k < N; k += s.nth) { x[k] += al * p[k]; r[k] -= al * q[k]; }
+        }
+        PG_SYNC();
+        if (!pg_vcycle<T>(P, s, a, sv, 0, 1, 0)) return false;      // z = M r
+        acc[0] = 0.0;
+        for (int k = s.tid; k < N; k += s.nth) acc[0] += (double)r[k] * (double)z[k];
+        if (!pg_sum<1>(s, acc)) return false;
+        if (threadIdx.x == 0) {
+            const double rz = acc[0];
+            if (!(rz > sk.rtol * sk.rtol * sk.rz0)) { sk.active = 0; sk.status = 1; }
+            else if (sk.it >= sk.maxit) { sk.active = 0; sk.status = 3; }
+            else { sk.be = rz / sk.rz; sk.rz = rz; }
+        }
+        __syncthreads();
+        if (!sk.active) break;
+        {
+            const T be = (T)sk.be;
+            for (int k = s.tid; k < N; k += s.nth) p[k] = z[k] + be * p[k];
+        }
+        PG_SYNC();
+    }
+    return true;
+}
+
+// r = b - A x with the FP64 operator, its squared norm and the squared rounding floor
+// (sum_k (sum_j |a_kj x_j| + |b_k|)^2) - the start of the FP64 BiCGSTAB and of the
+// refinement (semiconductor_3d.c:2244-2268).  Writes r (FP64 work vector 0) and, when
+// r32 is not null, its FP32 copy.
+__device__ __forceinline__ void pg_start64(const DevP &P, const PS &s, float *r32, double *rh, double (&acc)[2]) {
+    const double *b = P.rhs, *x = P.sol;
+    double *r = P.wk[0];
+    const int NxNy = P.Nx * P.Ny;
+    for (int k = s.tid; k < P.N; k += s.nth) {
+        const Node a = unidx(k, P.Nx, P.Ny);
+        const int i = a.i, j = a.j, l = a.l;
+        double sum = P.A[0][k] * x[k], fl = fabs(P.A[0][k] * x[k]) + fabs(b[k]), t;
+        if (i > 0) { t = P.A[1][k] * x[k - 1]; sum += t; fl += fabs(t); }
+        if (i < P.Nx - 1) { t = P.A[2][k] * x[k + 1]; sum += t; fl += fabs(t); }
+        if (j > 0) { t = P.A[3][k] * x[k - P.Nx]; sum += t; fl += fabs(t); }
+        if (j < P.Ny - 1) { t = P.A[4][k] * x[k + P.Nx]; sum += t; fl += fabs(t); }
+        if (l > 0) { t = P.A[5][k] * x[k - NxNy]; sum += t; fl += fabs(t); }
+        if (l < P.Nz - 1) { t = P.A[6][k] * x[k + NxNy]; sum += t; fl += fabs(t); }
+        const double rk = b[k] - sum;
+        r[k] = rk;
+        if (rh) { rh[k] = rk; P.wk[2][k] = 0.0; P.wk[3][k] = 0.0; }
+        if (r32) r32[k] = (float)rk;
+        acc[0] += rk * rk;
+        acc[1] += fl * fl;
+    }
+}
+
+// ---------------------------------------------------------------- hierarchy set-up
+// The multigrid set-up of the system now in the level-0 operator (mg_setup_t in
+// kernels_la.cu, the reference's mg_setup semiconductor_3d.c:2126-2148): for T = float
+// the FP32 copy of the operator and row weights, then per level the Slotboom weights with
+// the next level's reference potentials and the smoother pivots (one pass: the pivots
+// read only the level's own operator), the Galerkin coarse operator (one pass), and the
+// coarsest level's dense inverse (block 0, in its shared memory).
+template <class T>
+__device__ __noinline__ bool pg_setup(const DevP &P, PS &s, const PArgs &a, unsigned char *scratch) {
+    const int nl = P.nlev, qsign = a.qsign;
+    if constexpr (std::is_same<T, float>::value) {
+        for (int k = s.tid; k < P.N; k += s.nth) {
+#pragma unroll
+            for (int q = 0; q < 7; q++) P.A32[q][k] = (float)P.A[q][k];
+            if (qsign) P.dsc32[k] = (float)P.dsc[k];
+        }
+        PG_SYNC();
+    }
+    for (int L = 0; L < nl - 1; L++) {
+        const LevView<T> f = levview<T>(P, L, 0, 0);
+        const LevelT<T> &cl = PT<T>::lev(P, L + 1);
+        for (int K = s.tid; K < cl.N; K += s.nth) mg_weights_node<T>(P, f, cl, L, qsign, K);
+        for (int k = s.tid; k < f.N; k += s.nth) ilu_diag_node<T>(f, k);
+        PG_SYNC();
+        const T *w = (L == 0 && qsign) ? PT<T>::w0(P) : nullptr;
+        for (int K = s.tid; K < cl.N; K += s.nth) galerkin_node<T>(f, cl, w, K);
+        PG_SYNC();
+    }
+    if (blockIdx.x == 0 && nl > 1) {
+        double *M = reinterpret_cast<double *>(scratch);
+        int *perm = reinterpret_cast<int *>(M + COARSE_MAX * (COARSE_MAX + 1));
+        blk_coarse_setup<T>(PT<T>::lev(P, nl - 1), M, perm, perm + COARSE_MAX);
+        __syncthreads();
+    }
+    return true;
+}
+// dynamic shared memory the set-up's dense inverse needs (block 0)
+constexpr size_t PG_SETUP_SMEM = sizeof(double) * COARSE_MAX * (COARSE_MAX + 1) + sizeof(int) * (COARSE_MAX + 1);
+
+// ---------------------------------------------------------------- the solve kernels
+// T: precision of the Krylov iterations and the hierarchy.  PK_PCG: the Poisson Newton
+// system from the present sol (T = float: sol starts at 0 and the result is copied to the
+// FP64 sol when it converged).  PK_BICG (T = double): the continuity system from the
+// present sol.  PK_REFINED (T = float): FP64 refinement steps around FP32 BiCGSTAB.
+template <class T, int KIND>
+__global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) {
+    const DevP &P = Ps[0];
+    extern __shared__ __align__(16) unsigned char sraw[];
+    __shared__ LevView<T> sv[MAXLEV];
+    __shared__ KrylovS sk, so;                    // the loop's record (and the outer one: PK_REFINED)
+    PS s;
+    s.g = P.pgrid;
+    s.target = 0;
+    s.rb = 0;
+    s.tid = blockIdx.x * blockDim.x + threadIdx.x;
+    s.nth = gridDim.x * blockDim.x;
+    s.wait_ns = PG_WAIT_NS;
+    const int nl = P.nlev;
+    if (a.setup && !pg_setup<T>(P, s, a, sraw)) return;
+    if (blockIdx.x == 0) {                        // the small levels stay in block 0's shared memory
+        if (threadIdx.x < nl - a.Ls) sv[threadIdx.x] = smem_view<T>(P, a.Ls + threadIdx.x, a.Ls, sraw);
+        __syncthreads();
+        blk_stage_small<T>(P, sv, a.Ls, nl);
+    }
+    if (threadIdx.x == 0) {
+        sk = *PT<T>::ks(P);
+        so = *P.ks;
+    }
+    __syncthreads();
+    KrylovS &rec = sk;
+    if constexpr (KIND == PK_PCG) {
+        if constexpr (std::is_same<T, double>::value) {
+            const int NxNy = P.Nx * P.Ny;
+            for (int k = s.tid; k < P.N; k += s.nth) {
+                const Node nd = unidx(k, P.Nx, P.Ny);
+                P.wk[0][k] = P.rhs[k] - stencil_apply<double>(P.A, P.sol, k, nd.i, nd.j, nd.l, P.Nx, P.Ny, P.Nz);
+            }
+            (void)NxNy;
+        } else {
+            for (int k = s.tid; k < P.N; k += s.nth) {
+                const float b = (float)P.rhs[k];
+                P.rhs32[k] = b;
+                P.wk32[0][k] = b;
+                P.sol32[k] = 0.f;
+            }
+        }
+        if (!pg_sync(s)) return;
+        if (!pg_vcycle<T>(P, s, a, sv, 0, 1, 0)) return;            // z = M r
+        double acc[1] = {0.0};
+        const T *r = PT<T>::wk(P, 0), *z = PT<T>::wk(P, 1);
+        for (int k = s.tid; k < P.N; k += s.nth) acc[0] += (double)r[k] * (double)z[k];
+        if (!pg_sum<1>(s, acc)) return;
+        if (threadIdx.x == 0) {
+            const double rz = acc[0];
+            rec.rz = rec.rz0 = rz; rec.it = 0; rec.status = 0;
+            rec.active = (rz > 0.0) ? 1 : 0;
+            if (!(rz > 0.0)) rec.status = 2;
+        }
+        __syncthreads();
+        if (rec.active) {
+            T *p = PT<T>::wk(P, 2);
+            for (int k = s.tid; k < P.N; k += s.nth) p[k] = z[k];
+            if (!pg_sync(s)) return;
+            if (!pg_pcg<T>(P, s, a, sv, rec)) return;
+        }
+        if constexpr (std::is_same<T, float>::value) {
+            if (rec.status == 1)
+                for (int k = s.tid; k < P.N; k += s.nth) P.sol[k] = (double)P.sol32[k];
+        }
+    } else if constexpr (KIND == PK_BICG) {
+        double acc[2] = {0.0, 0.0};
+        pg_start64(P, s, nullptr, P.wk[1], acc);
+        if (!pg_sum<2>(s, acc)) return;
+        if (threadIdx.x == 0) {
+            rec.rr = acc[0]; rec.fl = acc[1];
+            rec.r0 = sqrt(acc[0]);
+            rec.tgt = fmax(a.rtol * rec.r0, a.atol * sqrt(acc[1]));
+            rec.rho = rec.al = rec.om = 1.0; rec.rbest = rec.r0; rec.stall = 0; rec.it = 0; rec.half = 0;
+            if (!(rec.r0 > rec.tgt)) { rec.active = 0; rec.status = 1; }
+            else { rec.active = 1; rec.status = 0; }
+        }
+        __syncthreads();
+        if (!pg_bicg<T>(P, s, a, sv, rec)) return;
+    } else {                                      // PK_REFINED
+        double acc[2] = {0.0, 0.0};
+        pg_start64(P, s, P.rhs32, nullptr, acc);
+        if (!pg_sum<2>(s, acc)) return;
+        if (threadIdx.x == 0) {
+            so.rr = acc[0]; so.fl = acc[1];
+            so.r0 = sqrt(acc[0]);
+            so.tgt = fmax(so.rtol * so.r0, so.atol * sqrt(acc[1]));
+            so.rbest = so.r0; so.stall = 0; so.it = 0; so.half = 0;
+            if (!(so.r0 > so.tgt)) { so.active = 0; so.status = 1; }
+            else { so.active = 1; so.status = 0; }
+        }
+        __syncthreads();
+        int steps = 0;
+        for (; steps < a.maxsteps && so.active; steps++) {
+            // inner start: d = 0, r = rh = rhs32, p = v = 0
+            float *r = P.wk32[0], *rh = P.wk32[1], *p = P.wk32[2], *v = P.wk32[3], *d = P.sol32;
+            double ai[1] = {0.0};
+            for (int k = s.tid; k < P.N; k += s.nth) {
+                const float bk = P.rhs32[k];
+                r[k] = bk; rh[k] = bk; p[k] = 0.f; v[k] = 0.f; d[k] = 0.f;
+                ai[0] += (double)bk * (double)bk;
+            }
+            if (!pg_sum<1>(s, ai)) return;
+            if (threadIdx.x == 0) {
+                sk.rr = ai[0];
+                sk.r0 = sqrt(ai[0]);
+                sk.tgt = fmax(sk.rtol * sk.r0, sk.atol * so.tgt);
+                sk.rho = sk.al = sk.om = 1.0; sk.rbest = sk.r0; sk.stall = 0; sk.it = 0; sk.half = 0;
+                sk.body_runs = 0;
+                sk.maxit = so.maxit - so.it;
+                sk.status = 0;
+                sk.active = (sk.r0 > sk.tgt && sk.maxit > 0) ? 1 : 0;
+            }
+            __syncthreads();
+            if (!pg_bicg<float>(P, s, a, sv, sk)) return;
+            // x += d; r -= A d (FP64 operator); rhs32 = (float) r; the outer stop test
+            double au[1] = {0.0};
+            double *x = P.sol, *r64 = P.wk[0];
+            const int NxNy = P.Nx * P.Ny;
+            for (int k = s.tid; k < P.N; k += s.nth) {
+                const Node nd = unidx(k, P.Nx, P.Ny);
+                const int i = nd.i, j = nd.j, l = nd.l;
+                const double dk = (double)d[k];
+                double sum = P.A[0][k] * dk;
+                if (i > 0) sum += P.A[1][k] * (double)d[k - 1];
+                if (i < P.Nx - 1) sum += P.A[2][k] * (double)d[k + 1];
+                if (j > 0) sum += P.A[3][k] * (double)d[k - P.Nx];
+                if (j < P.Ny - 1) sum += P.A[4][k] * (double)d[k + P.Nx];
+                if (l > 0) sum += P.A[5][k] * (double)d[k - NxNy];
+                if (l < P.Nz - 1) sum += P.A[6][k] * (double)d[k + NxNy];
+                x[k] += dk;
+                const double rk = r64[k] - sum;
+                r64[k] = rk;
+                P.rhs32[k] = (float)rk;
+                au[0] += rk * rk;
+            }
+            if (!pg_sum<1>(s, au)) return;
+            if (threadIdx.x == 0) {
+                so.it += sk.it;
+                so.body_runs++;
+                so.rr = au[0];
+                const double rn = sqrt(au[0]);
+                if (rn <= so.tgt) { so.active = 0; so.status = 1; }
+                else if (!(rn < 0.5 * so.rbest)) { so.active = 0; so.status = 4; }
+                else if (so.it >= so.maxit) { so.active = 0; so.status = 3; }
+                else so.rbest = rn;
+            }
+            __syncthreads();
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) s.g->steps = steps;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *PT<T>::ks(P) = sk;
+        if (KIND == PK_REFINED) *P.ks = so;
+        s.g->iters = KIND == PK_REFINED ? so.it : sk.it;
+    }
+}
+
+// Test of the bounded barrier wait: the last block of the launch never arrives, so every
+// other block must give up after wait_ns, set the error word and report ok = 0.
+__global__ void k_pg_timeout_probe(PGrid *g, unsigned long long wait_ns, int *ok) {
+    PS s;
+    s.g = g;
+    s.target = 0;
+    s.rb = 0;
+    s.tid = blockIdx.x * blockDim.x + threadIdx.x;
+    s.nth = gridDim.x * blockDim.x;
+    s.wait_ns = wait_ns;
+    if (blockIdx.x == gridDim.x - 1) return;     // never arrives
+    const bool r = pg_sync(s);
+    if (threadIdx.x == 0) ok[blockIdx.x] = r ? 1 : 0;
+}
+
+// ---------------------------------------------------------------- host side
+namespace {
+struct KInfo {
+    const void *fn = nullptr;
+    size_t smem = 0;       // dynamic shared memory the attribute allows
+    int blocks = 0;        // co-resident blocks at that size
+};
+std::mutex g_pmu;
+int g_persist_mode = -1;   // -1 unread, 0 off, 1 on
+int g_persist_blocks = 0;  // blocks per launch (0: every SM's worth)
+bool g_persist_broken = false;
+bool g_coop_ok = false;    // the device supports cooperative launches
+int g_fuse_up = 1;         // deferred prolongation on the way up (SEMISIM_B200_FUSEUP=0: off)
+
+template <class T, int KIND>
+const void *kfn() { return reinterpret_cast<const void *>(&k_persist<T, KIND>); }
+
+// co-resident blocks of the kernel at `smem` bytes (0 when it cannot launch)
+int occupancy(const void *fn, size_t smem) {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per = 0, dev = 0, nsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, PG_TPB, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return per * nsm;
+}
+}  // namespace
+
+int persist_enabled() {
+    std::lock_guard<std::mutex> lk(g_pmu);
+    if (g_persist_mode < 0) {
+        const char *e = std::getenv("SEMISIM_B200_PERSIST");
+        g_persist_mode = (e && std::atoi(e) == 0) ? 0 : 1;
+        if (const char *b = std::getenv("SEMISIM_B200_PBLOCKS")) g_persist_blocks = std::atoi(b);
+        if (const char *f = std::getenv("SEMISIM_B200_FUSEUP")) g_fuse_up = std::atoi(f) != 0;
+        int dev = 0, coop = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
+        if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess) cudaGetLastError();
+        g_coop_ok = coop != 0;
+    }
+    return g_persist_mode == 1 && g_coop_ok && !g_persist_broken;
+}
+void persist_set(int mode, int blocks) {
+    persist_enabled();
+    std::lock_guard<std::mutex> lk(g_pmu);
+    if (mode >= 0) g_persist_mode = mode ? 1 : 0;
+    if (blocks >= 0) g_persist_blocks = blocks;
+}
+int persist_get_blocks() { return g_persist_blocks; }
+
+// Launch the persistent solve `kind` of precision T on instance 0 of the context.  Returns
+// 1 when it ran (results in the Krylov records), 0 when the persistent path does not apply
+// (the caller runs the per-pass path), -1 when a barrier wait ran out (the caller restores
+// the start and runs the per-pass path; the persistent path is off from then on).
+template <class T, int KIND>
+static int persist_run(const Ctx &c, int Ls, size_t smem, const PArgs &a, PGrid *hres) {
+    static KInfo info;                           // per instantiation, cached
+    static std::mutex mu;
+    KInfo ki;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        KInfo &k = info;
+        if (!k.fn || k.smem < smem) {
+            k.fn = kfn<T, KIND>();
+            k.smem = smem;
+            k.blocks = occupancy(k.fn, smem);
+        }
+        ki = k;
+    }
+    int nb = ki.blocks;
+    // small systems take a part of the GPU (about two nodes per thread), so that several
+    // instances' solves can run side by side
+    const int want = (c.maxN + 2 * PG_TPB - 1) / (2 * PG_TPB);
+    if (want < nb) nb = want < 4 ? 4 : want;
+    if (g_persist_blocks > 0 && g_persist_blocks < nb) nb = g_persist_blocks;
+    if (nb > PG_MAXB) nb = PG_MAXB;
+    if (nb < 1) return 0;
+    (void)Ls;
+    PGrid *g = c.h.pgrid;
+    cudaMemsetAsync(g, 0, 6 * sizeof(unsigned), c.st);      // counter, error word, work counters
+    const DevP *dp = c.dP;
+    PArgs aa = a;
+    void *args[] = {(void *)&dp, (void *)&aa};
+    g_launches++;
+    t_launches++;
+    const int pid = sizeof(T) == 4 ? PF_PERSIST32 : PF_PERSIST;
+    if (g_prof_on) prof_begin(pid, c.st);
+    const cudaError_t e = cudaLaunchCooperativeKernel(kfn<T, KIND>(), dim3(nb), dim3(PG_TPB), args, smem, c.st);
+    if (g_prof_on) prof_end(pid, c.st, 0.0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        std::fprintf(stderr, "semisim-b200: persistent solve launch failed (%s); per-pass solves from now on\n",
+                     cudaGetErrorString(e));
+        g_persist_broken = true;
+        return 0;
+    }
+    cudaMemcpyAsync(hres, g, 6 * sizeof(unsigned), cudaMemcpyDeviceToHost, c.st);
+    cudaStreamSynchronize(c.st);
+    if (hres->err) {
+        std::fprintf(stderr, "semisim-b200: persistent solve abandoned (a barrier wait ran out); per-pass solves "
+                             "from now on\n");
+        g_persist_broken = true;
+        return -1;
+    }
+    return 1;
+}
+
+// algorithmic bytes of one V-cycle of precision T (the passes the persistent kernel runs)
+template <class T>
+static double vcycle_bytes(const MGHost &mg, int Ls, int deep, int sweeps2) {
+    const double w = sizeof(T) / 8.0;
+    double b = 0.0;
+    for (int L = 0; L < Ls; L++) {
+        const double n = mg.maxN[L];
+        const int sm = (L < deep && sweeps2) ? 2 : 1;
+        // smoother half sweeps (black, red) per application, pre and post; residual +
+        // restriction; prolongation and residual on the way up
+        b += n * w * (2.0 * sm * (kProfBytesPerNode[PF_SMOOTH_B] + kProfBytesPerNode[PF_SMOOTH_R]) +
+                      kProfBytesPerNode[PF_RESID_RESTRICT] + kProfBytesPerNode[PF_PROLONG] +
+                      kProfBytesPerNode[PF_LEVEL_RESID]);
+    }
+    b += 2.0 * mg.maxN[Ls] * sizeof(T);             // b in, x out of the shared-memory levels
+    return b;
+}
+
+// algorithmic bytes of the in-kernel hierarchy set-up of precision T
+template <class T>
+static double setup_bytes(const MGHost &mg) {
+    const double w = sizeof(T) / 8.0;
+    double b = sizeof(T) == 4 ? mg.maxN[0] * kProfBytesPerNode[PF_CONVERT32] : 0.0;
+    for (int L = 0; L < mg.maxlev - 1; L++)
+        b += mg.maxN[L] * w * (kProfBytesPerNode[PF_WEIGHTS] + kProfBytesPerNode[PF_GALERKIN] +
+                               kProfBytesPerNode[PF_ILU_DIAG]);
+    return b;
+}
+
+// small-level plan of precision T for the persistent kernels: the first level at or below
+// the small-level size whose data fits the opt-in shared memory (never level 0)
+template <class T>
+static int persist_plan(const Ctx &c, const MGHost &mg, size_t *smem) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t cap = optin > 16384 ? (size_t)optin - 16384 : 0;
+    *smem = 0;
+    if (mg.maxlev < 2) return -1;
+    vcycle_knobs_init();
+    const int lim = c.small_nodes > 0 ? c.small_nodes : g_small_nodes;
+    int L = 1;
+    while (L < mg.maxlev - 1 && mg.maxN[L] > lim) L++;
+    auto bytes = [&](int Ls) {
+        size_t b = 0;
+        for (int q = Ls; q < mg.maxlev; q++) b += smem_level_bytes<T>(mg.maxN[q], q == mg.maxlev - 1);
+        return b;
+    };
+    while (L < mg.maxlev - 1 && bytes(L) > cap) L++;
+    if (bytes(L) > cap) return -1;
+    *smem = bytes(L);
+    return L;
+}
+
+// Persistent forms of the solves of kernels_la.cu.  Each returns 1 (done: the Krylov
+// records hold the result), 0 (not applicable: nothing was changed) or -1 (abandoned: the
+// caller restores the start and uses the per-pass solve).
+int persist_pcg(const Ctx &c, const MGHost &mg, int mixed) {
+    if (c.ninst != 1 || !persist_enabled()) return 0;
+    size_t smem = 0;
+    PArgs a{};
+    a.Ls = mixed ? persist_plan<float>(c, mg, &smem) : persist_plan<double>(c, mg, &smem);
+    if (a.Ls < 1) return 0;
+    a.setup = 1;
+    a.qsign = 0;
+    smem = std::max(smem, PG_SETUP_SMEM);
+    a.deep = g_deep_levels;
+    a.sweeps2 = g_l0_sweeps > 1;
+    a.alpha = mg.alpha;
+    a.fuse_up = g_fuse_up;
+    PGrid h{};
+    const int rc = mixed ? persist_run<float, PK_PCG>(c, a.Ls, smem, a, &h)
+                         : persist_run<double, PK_PCG>(c, a.Ls, smem, a, &h);
+    if (rc == 1 && g_prof_on) {
+        const double vb = mixed ? vcycle_bytes<float>(mg, a.Ls, a.deep, a.sweeps2)
+                                : vcycle_bytes<double>(mg, a.Ls, a.deep, a.sweeps2);
+        const double kb = (mixed ? 0.5 : 1.0) * (kProfBytesPerNode[PF_KRY_SPMV_DOT] + 2 * kProfBytesPerNode[PF_KRY_UPDATE] +
+                                                 kProfBytesPerNode[PF_KRY_DOT]);
+        const double sb = mixed ? setup_bytes<float>(mg) : setup_bytes<double>(mg);
+        prof_set_last(mixed ? PF_PERSIST32 : PF_PERSIST, sb + h.vcycles * vb + h.iters * kb * c.maxN);
+    }
+    return rc;
+}
+int persist_bicg(const Ctx &c, const MGHost &mg, double rtol, double atol, int qsign) {
+    if (c.ninst != 1 || !persist_enabled()) return 0;
+    size_t smem = 0;
+    PArgs a{};
+    a.Ls = persist_plan<double>(c, mg, &smem);
+    if (a.Ls < 1) return 0;
+    a.setup = 1;
+    a.qsign = qsign;
+    smem = std::max(smem, PG_SETUP_SMEM);
+    a.deep = g_deep_levels;
+    a.sweeps2 = g_l0_sweeps > 1;
+    a.alpha = mg.alpha;
+    a.fuse_up = g_fuse_up;
+    a.rtol = rtol;
+    a.atol = atol;
+    PGrid h{};
+    const int rc = persist_run<double, PK_BICG>(c, a.Ls, smem, a, &h);
+    if (rc == 1 && g_prof_on) {
+        const double vb = vcycle_bytes<double>(mg, a.Ls, a.deep, a.sweeps2);
+        const double kb = 2 * kProfBytesPerNode[PF_KRY_SPMV_DOT] + 4 * kProfBytesPerNode[PF_KRY_UPDATE];
+        prof_set_last(PF_PERSIST, setup_bytes<double>(mg) + h.vcycles * vb +
+                                      (h.iters * kb + kProfBytesPerNode[PF_KRY_INIT]) * c.maxN);
+    }
+    return rc;
+}
+int persist_refined(const Ctx &c, const MGHost &mg, int maxsteps, int *steps, int qsign) {
+    if (c.ninst != 1 || !persist_enabled()) return 0;
+    size_t smem = 0;
+    PArgs a{};
+    a.Ls = persist_plan<float>(c, mg, &smem);
+    if (a.Ls < 1) return 0;
+    a.setup = 1;
+    a.qsign = qsign;
+    smem = std::max(smem, PG_SETUP_SMEM);
+    a.deep = g_deep_levels;
+    a.sweeps2 = g_l0_sweeps > 1;
+    a.alpha = mg.alpha;
+    a.fuse_up = g_fuse_up;
+    a.maxsteps = maxsteps;
+    PGrid h{};
+    const int rc = persist_run<float, PK_REFINED>(c, a.Ls, smem, a, &h);
+    if (rc == 1) {
+        *steps = h.steps;
+        if (g_prof_on) {
+            const double vb = vcycle_bytes<float>(mg, a.Ls, a.deep, a.sweeps2);
+            const double kb = 0.5 * (2 * kProfBytesPerNode[PF_KRY_SPMV_DOT] + 4 * kProfBytesPerNode[PF_KRY_UPDATE]);
+            prof_set_last(PF_PERSIST32, setup_bytes<float>(mg) + h.vcycles * vb +
+                                            (h.iters * kb + (h.steps + 1) * kProfBytesPerNode[PF_REFINE]) * c.maxN);
+        }
+    }
+    return rc;
+}
+
+// Run the bounded-wait test on the instance's barrier record with `nb` blocks (>= 2):
+// returns the error word (1 expected) and the blocks that reported ok = 0 in *gave_up
+// (nb - 1 expected), or -1 when the launch failed.
+int persist_timeout_probe(const Ctx &c, int nb, double wait_s, int *gave_up) {
+    if (nb < 2 || nb > 64) return -1;
+    int *ok = nullptr;
+    if (cudaMalloc(&ok, nb * sizeof(int)) != cudaSuccess) { cudaGetLastError(); return -1; }
+    cudaMemsetAsync(ok, 0xff, nb * sizeof(int), c.st);
+    PGrid *g = c.h.pgrid;
+    cudaMemsetAsync(g, 0, 6 * sizeof(unsigned), c.st);
+    unsigned long long wn = (unsigned long long)(wait_s * 1e9);
+    void *args[] = {(void *)&g, (void *)&wn, (void *)&ok};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_pg_timeout_probe, dim3(nb), dim3(32), args, 0, c.st);
+    int rc = -1;
+    if (e == cudaSuccess) {
+        unsigned err = 0;
+        std::vector<int> h(nb);
+        cudaMemcpyAsync(&err, &g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c.st);
+        cudaMemcpyAsync(h.data(), ok, nb * sizeof(int), cudaMemcpyDeviceToHost, c.st);
+        if (cudaStreamSynchronize(c.st) == cudaSuccess) {
+            int n0 = 0;
+            for (int q = 0; q < nb - 1; q++) n0 += h[q] == 0;
+            *gave_up = n0;
+            rc = (int)err;
+        }
+    } else {
+        cudaGetLastError();
+    }
+    cudaFree(ok);
+    return rc;
+}
+
+}  // namespace ss

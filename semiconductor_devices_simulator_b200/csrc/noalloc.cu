@@ -84,6 +84,37 @@ NoAllocScratch *scratch_on(int dev) {
     }
     return g_na_ptr[dev];
 }
+
+// the GPU that holds a caller buffer, or -1 when it is not device (or managed) memory
+int device_of(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) return -1;
+    return at.device;
+}
+
+// true when the byte ranges [a, a + na) and [b, b + nb) share a byte
+bool overlap(const void *a, size_t na, const void *b, size_t nb) {
+    const char *pa = static_cast<const char *>(a), *pb = static_cast<const char *>(b);
+    return pa < pb + nb && pb < pa + na;
+}
+
+// makes `dev` current for the lifetime of the guard and restores the caller's device
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) { cudaGetLastError(); prev = -1; return; }
+        ok = prev == dev || cudaSetDevice(dev) == cudaSuccess;
+        if (!ok) cudaGetLastError();
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
 }  // namespace
 
 }  // namespace ss
@@ -95,9 +126,11 @@ extern "C" {
 // r = b - A x for the 7-point stencil A (7 arrays of N = Nx*Ny*Nz doubles one after the
 // other: diagonal, x-, x+, y-, y+, z-, z+; node k = i + Nx*(j + Ny*l)) and norms[0] =
 // ||r||_2, norms[1] = sqrt(sum_a (sum_b |A_ab x_b| + |b_a|)^2).  A7, x, b and r are device
-// buffers the caller owns, all on one GPU; norms is host memory.  Allocates nothing.
-// Returns 1 on success, 0 with a message on stderr on a null pointer, a non-device
-// buffer, a size beyond 2^30 nodes or a CUDA error.
+// buffers the caller owns, all on one GPU; r must not overlap A7, x or b; norms is host
+// memory.  Allocates nothing.  Returns 1 on success, 0 with a message on stderr (and no
+// kernel launched) on a null pointer, a buffer that is not device memory or lies on
+// another GPU than x, an r that overlaps an input, a size beyond 2^30 nodes; 0 also on
+// a CUDA error.  The calling thread's current device is the same on return as before.
 //
 // The first call on a GPU looks up the scratch's device address (cudaGetSymbolAddress
 // with that GPU current): make that first call before any stream capture.  All calls
@@ -119,20 +152,47 @@ int api3b_stencil_residual_noalloc(const double *A7, const double *x, const doub
                      NA_MAX_NODES);
         return 0;
     }
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, x) != cudaSuccess ||
-        (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
-        cudaGetLastError();
-        std::fprintf(stderr, "semisim-b200: stencil_residual_noalloc: x is not device memory\n");
+    // every caller buffer must be device memory of one GPU: a host or another GPU's
+    // pointer would reach the kernel and fault there, which poisons the caller's context
+    const char *names[4] = {"A7", "x", "b", "r"};
+    const void *bufs[4] = {A7, x, b, r};
+    int dev = -1;
+    for (int q = 0; q < 4; q++) {
+        const int d = device_of(bufs[q]);
+        if (d < 0) {
+            std::fprintf(stderr, "semisim-b200: stencil_residual_noalloc: %s is not device memory\n", names[q]);
+            return 0;
+        }
+        if (q > 0 && d != dev) {
+            std::fprintf(stderr, "semisim-b200: stencil_residual_noalloc: %s is on device %d, x on device %d\n",
+                         names[q], d, dev);
+            return 0;
+        }
+        dev = d;
+    }
+    // r is written while A7, x and b are read (at neighbouring nodes too): it must not
+    // share memory with any of them
+    const size_t vb = (size_t)N * sizeof(double);
+    if (overlap(r, vb, x, vb) || overlap(r, vb, b, vb) || overlap(r, vb, A7, 7 * vb)) {
+        std::fprintf(stderr, "semisim-b200: stencil_residual_noalloc: r overlaps an input (A7, x or b)\n");
         return 0;
     }
-    if (cudaSetDevice(at.device) != cudaSuccess) return 0;
-    NoAllocScratch *s = scratch_on(at.device);
+    DeviceGuard guard(dev);                     // the caller's current device comes back on return
+    if (!guard.ok) {
+        std::fprintf(stderr, "semisim-b200: stencil_residual_noalloc: cannot make device %d current\n", dev);
+        return 0;
+    }
+    NoAllocScratch *s = scratch_on(dev);
     if (!s) return 0;
     if (cudaMemsetAsync(s->ticket, 0, sizeof s->ticket, 0) != cudaSuccess) return 0;   // the finish counter starts at 0
     k_resid_floor_na<<<NA_BLOCKS, NA_TPB, 0, 0>>>(A7, x, b, r, Nx, Ny, Nz, s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "semisim-b200: stencil_residual_noalloc: launch failed: %s\n", cudaGetErrorString(e));
+        return 0;
+    }
     double out[2] = {0.0, 0.0};
-    const cudaError_t e = cudaMemcpy(out, s->out, sizeof out, cudaMemcpyDeviceToHost);
+    e = cudaMemcpy(out, s->out, sizeof out, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) {
         std::fprintf(stderr, "semisim-b200: stencil_residual_noalloc: %s\n", cudaGetErrorString(e));
         return 0;

@@ -57,6 +57,8 @@ const double kProfBytesPerNode[PF_NPROF] = {
     96.0,   // PF_CONVERT32: A and row weights 64 read, 32 written
     112.0,  // PF_SEED: x1, x0 of 3 fields at the node (neighbours from cache), flags, doping; 3 fields written
     64.0,   // PF_METAL: column node state, exchange slots and the per-node results
+    1.0,    // PF_PERSIST: algorithmic bytes of the whole solve, booked after it (prof_set_last)
+    1.0,    // PF_PERSIST32
 };
 int pf_f32(int id) {
     switch (id) {
@@ -84,7 +86,8 @@ const char *kProfName[PF_NPROF] = {
     "anderson", "boundary", "vector", "labelling", "display", "smooth_black_f32", "smooth_red_f32",
     "resid_restrict_f32", "prolong_f32", "level_resid_f32", "coarse_solve_f32", "galerkin_f32", "mg_weights_f32",
     "ilu_diag_f32", "coarse_setup_f32", "krylov_spmv_dot_f32", "krylov_update_f32", "krylov_dot_f32",
-    "krylov_init_f32", "refine_f64", "convert_f32", "learned_seed", "metal_contacts"};
+    "krylov_init_f32", "refine_f64", "convert_f32", "learned_seed", "metal_contacts", "persistent_solve",
+    "persistent_solve_f32"};
 
 bool g_prof_on = false;
 bool g_pdl = true;
@@ -120,6 +123,10 @@ void prof_end(int, cudaStream_t st, double nodes) {
     cudaEventRecord(r.b, st);
     g_used++;
     if (g_used >= 4096) prof_collect();     // bound the pool
+}
+void prof_set_last(int id, double bytes) {
+    for (size_t q = g_used; q-- > 0;)
+        if (g_recs[q].id == id) { g_recs[q].nodes = bytes; return; }
 }
 void prof_collect() {
     for (size_t q = 0; q < g_used; q++) {

@@ -21,6 +21,7 @@ enum ProfId {
     PF_KRY_DOT32, PF_KRY_INIT32, PF_REFINE, PF_CONVERT32,
     PF_SEED,                     // learned sweep predictor (features + MLP + seed write)
     PF_METAL,                    // metal-contact exchange (per column node)
+    PF_PERSIST, PF_PERSIST32,    // persistent solve launches, FP64 and FP32 (bytes booked per launch)
     PF_NPROF
 };
 // kernel class of the FP32 twin of an FP64 linear-algebra class
@@ -36,6 +37,9 @@ extern std::atomic<unsigned long long> g_launches;     // all threads
 extern thread_local unsigned long long t_launches;     // this thread
 void prof_begin(int id, cudaStream_t st);
 void prof_end(int id, cudaStream_t st, double nodes);
+// book `bytes` algorithmic bytes for the last timed launch of class `id` (classes whose
+// bytes are known only after the launch, kProfBytesPerNode 1)
+void prof_set_last(int id, double bytes);
 void prof_collect();
 void prof_reset();
 void prof_read(int id, double *ms, double *count, double *bytes);

@@ -81,6 +81,18 @@ struct KrylovS {
     int half, pad0, maxit, body_runs;
 };
 
+// Grid-wide barrier and reduction records of a persistent solve launch (one per
+// instance): the arrival counter (set to 0 before every launch), the error word (1: a
+// barrier wait ran out of time and every block left), the work done (V-cycles, Krylov
+// iterations, refinement steps) for the byte accounting, and two alternating buffers of
+// per-block reduction partials (up to 4 values per block).
+constexpr int PG_MAXB = 512;
+struct PGrid {
+    unsigned count, err;
+    int vcycles, iters, steps, pad;
+    double red[2][PG_MAXB * 4];
+};
+
 // one level of the aggregation multigrid of a general (graph) mesh: the level's matrix in
 // ELL (slot s of node k at s*N + k; the diagonal apart), its D-ILU(0) pivot reciprocals in
 // a multicolour order, and towards the next level the aggregate of every node, the member
@@ -168,6 +180,7 @@ struct DevP {
     float *A32[7], *dsc32, *rhs32, *sol32;
     float *wk32[8];
     KrylovS *ksi;                 // Krylov record of the FP32 inner solve
+    PGrid *pgrid;                 // barrier and reduction records of the persistent solves
     // multigrid (FP64 and FP32 hierarchies)
     LevelT<double> *lev;          // device array of nlev levels
     LevelT<float> *levf;

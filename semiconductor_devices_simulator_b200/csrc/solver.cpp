@@ -125,6 +125,7 @@ static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &lev
     P.res = cv.take<double>(R_TOTAL);
     P.ks = cv.take<KrylovS>(1);
     P.ksi = cv.take<KrylovS>(1);
+    P.pgrid = cv.take<PGrid>(1);
     for (int q = 0; q < 7; q++) P.A32[q] = cv.take<float>(N);
     P.dsc32 = cv.take<float>(N); P.rhs32 = cv.take<float>(N); P.sol32 = cv.take<float>(N);
     for (int q = 0; q < 8; q++) P.wk32[q] = cv.take<float>(N);

@@ -251,12 +251,24 @@ void out_carrier_sums(Inst &d, double *out);
 double out_ins_field(Inst &d, long long *node);
 int out_terminal_charges(Inst &d, const int *owner_dev, int nt, const int *gate_term, double *out);
 void gpu_free(Inst &d);
+int batch_pool_release(const Inst *src);   // frees the batched-resolve workers of src (batch.cpp)
 
 // linear-algebra drivers (kernels_la.cu)
 void mg_setup(const Ctx &c, const MGHost &mg, int qsign);
 void vcycle(const Ctx &c, const MGHost &mg, int bsel, int xsel, int wsel, int mg_on, int gate);
 // mixed = 1: FP32 inner solves (FP32 hierarchy and Krylov vectors) refined in FP64
 int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_every, int mixed = 0);
+// persistent (one cooperative launch per solve) forms, kernels_persist.cu: 1 done, 0 not
+// applicable, -1 abandoned (the caller restores the start and solves per pass)
+int persist_enabled();
+void persist_set(int mode, int blocks);
+int persist_get_blocks();
+int persist_pcg(const Ctx &c, const MGHost &mg, int mixed);
+int persist_bicg(const Ctx &c, const MGHost &mg, double rtol, double atol, int qsign);
+int persist_refined(const Ctx &c, const MGHost &mg, int maxsteps, int *steps, int qsign);
+void vcycle_knobs_init();
+int persist_timeout_probe(const Ctx &c, int nb, double wait_s, int *gave_up);
+extern int g_l0_sweeps, g_deep_levels;
 int bicgstab_core(const Ctx &c, const MGHost &mg, int maxit, double rtol, double atol, int mg_on, int check_every,
                   double *rn, double *r0, int qsign, int mixed = 0);
 extern thread_local long long t_ir_steps, t_ir_fallbacks;   // refinement steps / FP64 take-overs

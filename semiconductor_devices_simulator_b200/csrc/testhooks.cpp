@@ -256,6 +256,13 @@ int b200x_bicgstab(int maxit, double rtol, double atol, int qsign, const double 
     sync(d);
     return its;
 }
+// bounded barrier wait of the persistent solves: a launch whose last block never arrives;
+// returns the error word (1) and the blocks that gave up (nb - 1), -1 on a launch error
+int b200x_persist_probe(int nb, double wait_s, int *gave_up) {
+    Inst &d = *dev();
+    Ctx c = make_ctx(d);
+    return persist_timeout_probe(c, nb, wait_s, gave_up);
+}
 // PCG on the Poisson system now in A / rhs from sol = 0
 int b200x_pcg(int maxit, double rtol, double *sol) {
     Inst &d = *dev();

@@ -523,6 +523,82 @@ def finfet(lib, n=(96, 96, 64), Lsd=30e-9, Lg=30e-9, W=10e-9, H=40e-9, tox=1.5e-
                      "Nch_cm3": Nch, "Nsd_cm3": Nsd})
 
 
+def dense_axis(L, n, marks, h_fine, h_coarse, width):
+    """n coordinates on [0, L] with a target spacing of h_fine at the planes `marks`,
+    growing linearly over `width` to h_coarse away from them (then scaled to fill L)."""
+    x = np.linspace(0.0, L, 20001)
+    d = np.min(np.abs(x[:, None] - np.asarray(marks, dtype=np.float64)[None, :]), axis=1) if len(marks) else \
+        np.full(x.shape, width)
+    h = h_fine + (h_coarse - h_fine) * np.minimum(1.0, d / width)
+    c = np.concatenate([[0.0], np.cumsum(0.5 * (1.0 / h[1:] + 1.0 / h[:-1]) * np.diff(x))])
+    c *= (n - 1) / c[-1]
+    out = np.interp(np.arange(n), c, x)
+    out[0], out[-1] = 0.0, L
+    return out
+
+
+def power_cell(lib, n=(256, 256, 128), Lx=10e-6, Ly=60e-6, Lz=10e-6, Ndrift=1e15, Nsub=1e19, sub_top=55e-6,
+               Nbody=1e17, body_sigma=1.2e-6, body_lat=0.25e-6, jfet_w=3e-6, Nsrc=1e20, src_sigma=0.15e-6,
+               src_w=1.5e-6,
+               Ntap=1e19, tap_w=1.0e-6, tox=50e-9, phi_m=4.1, gate_over=0.2e-6, models=7,
+               solver=GUI_SOLVER, vgs=(10.0,), vd_max=50.0, dvd=1.0):
+    """Vertical power-MOSFET cell (the reference's VDMOS template, main.py:984-1058, at the
+    size of the large-device configuration): x across the cell, y the depth from the top
+    surface, z along the gate fingers (the device is uniform in z).  An n- drift region
+    Ndrift (cm^-3) over an n+ substrate Nsub below sub_top; p-body wells Gaussian-diffused
+    from the surface (peak Nbody, depth and lateral sigma body_sigma) on both sides of a
+    JFET window jfet_w wide in the middle; n+ sources (peak Nsrc, sigma src_sigma) src_w
+    wide next to p+ body taps (Ntap) tap_w wide at the cell edges.  Contacts: the two
+    sources (tap + source, ohmic, top face), two oxide (Robin) gates tox thick over the
+    channels, overlapping the source and the JFET window by gate_over, and the drain
+    (ohmic, bottom face).  One drain sweep 0..vd_max in dvd steps per gate bias of `vgs`."""
+    lib.api3_init()
+    xb = 0.5 * (Lx - jfet_w)                           # body mask edge at the JFET window
+    xs_in = tap_w + src_w                              # source edge (channel start)
+    xj = xb + body_lat * np.sqrt(2.0 * np.log(Nbody / Ndrift))   # surface junction body / drift
+    xs = dense_axis(Lx, n[0], [tap_w, xs_in, xj, Lx - xj, Lx - xs_in, Lx - tap_w], 0.02e-6, 0.2e-6, 1.0e-6)
+    ys = dense_axis(Ly, n[1], [0.0, 3 * src_sigma, 2.5 * body_sigma, sub_top], 0.01e-6, 1.0e-6, 4e-6)
+    zs = np.linspace(0.0, Lz, n[2])
+    _grid(lib, xs, ys, zs)
+    lib.api3_set_solver(*solver)
+    lib.api3_set_models(models)
+    si = lib.api3_add_material(SI, 300.0)
+    X, Y = np.meshgrid(xs, ys, indexing="xy")          # (Ny, Nx)
+
+    def lateral(x0, x1, sig):
+        d = np.where(X < x0, x0 - X, np.where(X > x1, X - x1, 0.0))
+        return np.exp(-0.5 * (d / sig) ** 2)
+    gy = lambda sig: np.exp(-0.5 * (Y / sig) ** 2)
+    Nd2 = np.where(Y >= sub_top, Nsub, Ndrift) + Nsrc * gy(src_sigma) * (
+        lateral(tap_w, xs_in, src_sigma) + lateral(Lx - xs_in, Lx - tap_w, src_sigma))
+    Na2 = Nbody * gy(body_sigma) * (lateral(0.0, xb, body_lat) + lateral(Lx - xb, Lx, body_lat)) + \
+        Ntap * gy(2 * src_sigma) * (lateral(0.0, tap_w, src_sigma) + lateral(Lx - tap_w, Lx, src_sigma))
+    rep = lambda a: np.ascontiguousarray(np.broadcast_to(a[None, :, :], (n[2], n[1], n[0])).ravel())
+    Nd, Na = rep(Nd2) * 1e6, rep(Na2) * 1e6
+    mat = np.full(Nd.shape, si, dtype=np.int32)
+    lib.api3_set_node_data(iptr(mat), dptr(Nd), dptr(Na), dptr(np.zeros(Nd.shape)))
+    lib.api3_clear_contacts()
+    span = lambda c, lo, hi: (int(np.searchsorted(c, lo - 1e-15, side="left")),
+                              int(np.searchsorted(c, hi + 1e-15, side="right")) - 1)
+    nz = n[2] - 1
+    a0, a1 = span(xs, 0.0, xs_in)
+    b0, b1 = span(xs, Lx - xs_in, Lx)
+    g0, g1 = span(xs, xs_in - gate_over, xj + gate_over)
+    h0, h1 = span(xs, Lx - xj - gate_over, Lx - xs_in + gate_over)
+    csl = lib.api3_add_contact_ex(2, a0, a1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    csr = lib.api3_add_contact_ex(2, b0, b1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    cgl = lib.api3_add_contact_ex(2, g0, g1, 0, nz, 0, 0, 2, 0.0, phi_m, tox, 0.0)
+    cgr = lib.api3_add_contact_ex(2, h0, h1, 0, nz, 0, 0, 2, 0.0, phi_m, tox, 0.0)
+    cd = lib.api3_add_contact_ex(3, 0, n[0] - 1, 0, nz, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    npts = int(round(vd_max / dvd)) + 1
+    V = np.round(np.linspace(0.0, vd_max, npts), 12)
+    sweeps = [{"fixed": {"source_l": 0.0, "source_r": 0.0, "gate_l": vg, "gate_r": vg}, "swept": "drain", "V": V}
+              for vg in vgs]
+    return Workload("power_cell", n, {"source_l": csl, "source_r": csr, "gate_l": cgl, "gate_r": cgr, "drain": cd},
+                    sweeps, {"L_m": (Lx, Ly, Lz), "models": models, "tox_m": tox, "phi_m_eV": phi_m,
+                             "Ndrift_cm3": Ndrift, "Nsub_cm3": Nsub, "Nbody_cm3": Nbody})
+
+
 def diode_variants(count=64, seed=20261203, nmin=32, nmax=72):
     """Parameters of the batched pn-diode family (recorded seed)."""
     rng = np.random.default_rng(seed)

@@ -217,38 +217,6 @@ def test_autotuned_shapes_keep_parity(lib, name):
         lib.api3b_set_precision(-1)
 
 
-def test_nmosfet_full_size_matches_reference(lib):
-    """The benchmark device itself (n-MOSFET 120x80x60, 576,000 nodes), refined precision,
-    against the reference core run live on the same machine (all host threads): the first
-    13 points of the Vd = 1 V Id-Vg sweep (Vg 0..0.6 V) at the production tolerances.  psi
-    within 1e-6 V everywhere; the drain current within 1e-4 where it is on (>= 1 nA), and
-    within the reference's own convergence noise of the production tolerances below that
-    (1e-2 relative: the reference's default- vs tight-tolerance currents differ by up to
-    6e-3 on the small off-state devices; here the 5 fA point at Vg = 0 differs by 2.4e-3)."""
-    ref = reference_lib()
-    ref.api3_set_threads(os.cpu_count() or 1)
-    out = {}
-    for tag, L in (("gpu", lib), ("ref", ref)):
-        w = D.nmosfet(L, vds=(1.0,))
-        if tag == "gpu":
-            L.api3b_set_precision(1)
-        s = dict(w.sweeps[0])
-        s["V"] = s["V"][:13]
-        try:
-            out[tag] = sweep_fields(L, w, s)
-        finally:
-            if tag == "gpu":
-                L.api3b_set_precision(-1)
-    g, r = out["gpu"], out["ref"]
-    assert g[0] and g[4].all() and r[4].all()
-    assert np.abs(g[5] - r[5]).max() <= PSI_TOL
-    Ig, Ir = g[2][:, 1], r[2][:, 1]
-    rel = np.abs(Ig - Ir) / np.abs(Ir)
-    on = np.abs(Ir) >= 1e-9
-    assert on.any() and rel[on].max() <= 1e-4, rel
-    assert rel.max() <= 1e-2, rel
-
-
 def test_diode_variant_matches_reference(lib):
     """The smallest member of the 64-variant batch family (its own doping, junction depth
     and mesh), refined precision, against the reference core run live: the whole 0..0.7 V

@@ -1,11 +1,18 @@
 """The multi-GPU plumbing of bench.py on CPU: two ranks over gloo (the backend bench.py
 picks without CUDA), the max-over-ranks and sum reductions that make its JSON line, the
-barrier, and the work split (the Id-Vg workload replicated on every rank; the 64 diode
-variants split so every variant is solved exactly once).  No GPU and no solver calls."""
+barrier, the work split and the gather of the I-V arrays to rank 0.
+
+Work split: the n-MOSFET family is replicated on every rank (independent jobs, weak
+scaling); the FinFET's five drain-bias sweeps and the 64 diode variants are split so that
+every unit is solved exactly once, balanced by node count (largest first, each to the least
+loaded rank).  The gather is checked with synthetic per-rank current arrays: shape, order
+and completeness of the family array rank 0 assembles.  No GPU and no solver calls; the
+path is unmeasured on GPU hardware here (one GPU per run on this machine pool)."""
 import os
 import socket
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -18,16 +25,30 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _synthetic_currents(si, npts=24, nc=4):
+    """What a rank's sweep `si` yields: per point (I per contact, Iflr per contact)."""
+    return [([si * 1000.0 + q * 10.0 + c for c in range(nc)], [1e-18 * (c + 1) for c in range(nc)])
+            for q in range(npts)]
+
+
 def _rank_main(rank, world, port, q):
     os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
                       MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
     sys.path.insert(0, ROOT)
     import bench
+    from semiconductor_devices_simulator_b200 import devices as D
     d = bench.Dist()
     mx = d.max(1.5 + rank)
     sm = d.sum(10 * (rank + 1))
     d.barrier()
-    q.put((rank, d.backend, mx, sm, bench.shard(list(range(64)), d.rank, d.world), bench.sweep_order(2, d.rank)))
+    var = D.diode_variants(64)
+    nodes = [int(np.prod(v["n"])) for v in var]
+    mine = bench.shard(list(range(64)), d.rank, d.world, weights=nodes)
+    fin = bench.sweep_order(5, d.rank, d.world, replicate=False)
+    mos = bench.sweep_order(2, d.rank, d.world, replicate=True)
+    cur = {si: _synthetic_currents(si) for si in fin}
+    iv = bench.gather_iv(d, cur, 5)
+    q.put((rank, d.backend, mx, sm, mine, sum(nodes[i] for i in mine), fin, mos, iv))
     d.close()
 
 
@@ -44,18 +65,42 @@ def test_two_ranks_gloo(world):
     for p in ps:
         p.join(timeout=60)
         assert p.exitcode == 0
-    out.sort()
+    out.sort(key=lambda o: o[0])
     assert all(o[1] == "gloo" for o in out)
     assert all(o[2] == 1.5 + world - 1 for o in out)              # max over ranks
     assert all(o[3] == sum(10 * (r + 1) for r in range(world)) for o in out)
+    # 64 diode variants: every one exactly once, node counts balanced within one variant
     units = [u for o in out for u in o[4]]
-    assert sorted(units) == list(range(64))                        # every variant exactly once
-    assert all(sorted(o[5]) == [0, 1] for o in out)                # both sweeps on every rank
-    assert out[0][5] != out[1][5]                                  # rotated start
+    assert sorted(units) == list(range(64))
+    loads = [o[5] for o in out]
+    assert max(loads) - min(loads) <= 72 ** 3
+    # FinFET drain biases: split, every sweep once; n-MOSFET: both sweeps on every rank
+    assert sorted(s for o in out for s in o[6]) == [0, 1, 2, 3, 4]
+    assert all(sorted(o[7]) == [0, 1] for o in out)
+    assert out[0][7] != out[1][7]                                  # rotated start
+    # the gather: rank 0 holds the whole family (sweeps x points x contacts x 2) in sweep
+    # order, every sweep solved once; the other ranks hold nothing
+    arr, seen = out[0][8]
+    assert out[1][8] is None
+    assert arr.shape == (5, 24, 4, 2)
+    assert seen == [1, 1, 1, 1, 1]
+    for si in range(5):
+        ref = np.asarray(_synthetic_currents(si), dtype=np.float64).transpose(0, 2, 1)
+        assert np.array_equal(arr[si], ref)
 
 
 def test_shard_uneven():
     import bench
     parts = [bench.shard(range(10), r, 3) for r in range(3)]
     assert sorted(sum(parts, [])) == list(range(10))
-    assert [len(p) for p in parts] == [4, 3, 3]
+    assert sorted(len(p) for p in parts) == [3, 3, 4]
+
+
+def test_shard_balances_node_counts():
+    """Largest first to the least loaded rank: on weights 8, 7, 6, 5, 4 over two ranks the
+    loads are 17 and 13 (a round robin in index order gives 18 and 12)."""
+    import bench
+    w = [8, 7, 6, 5, 4]
+    parts = [bench.shard(range(5), r, 2, weights=w) for r in range(2)]
+    assert sorted(sum(parts, [])) == list(range(5))
+    assert sorted(sum(w[i] for i in p) for p in parts) == [13, 17]

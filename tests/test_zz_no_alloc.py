@@ -70,3 +70,12 @@ def test_noalloc_residual_matches_existing_entry():
     big = 1 << 11
     norms = np.zeros(2)
     assert lib.api3b_stencil_residual_noalloc(_dev(dA), _dev(dx), _dev(db), big, big, big, _dev(dr), dptr(norms)) == 0
+    # a host output buffer, or an output that aliases an input, is refused before any launch
+    host_r = np.zeros(N)
+    assert lib.api3b_stencil_residual_noalloc(_dev(dA), _dev(dx), _dev(db), Nx, Ny, Nz, dptr(host_r), dptr(norms)) == 0
+    assert lib.api3b_stencil_residual_noalloc(_dev(dA), _dev(dx), _dev(db), Nx, Ny, Nz, _dev(dx), dptr(norms)) == 0
+    assert lib.api3b_stencil_residual_noalloc(dptr(A7), _dev(dx), _dev(db), Nx, Ny, Nz, _dev(dr), dptr(norms)) == 0
+    # the refusals left the context usable: a valid call still succeeds
+    assert lib.api3b_stencil_residual_noalloc(_dev(dA), _dev(dx), _dev(db), Nx, Ny, Nz, _dev(dr), dptr(norms)) == 1
+    torch.cuda.synchronize()
+    assert abs(norms[0] - r0[0]) <= RTOL * r0[0]
