@@ -647,6 +647,17 @@ int pcg_graph(Inst &d, int maxit, double rtol) {
     double *x = d.g.h.sol, *b = d.g.h.rhs;
     double *r = d.g.h.wk[0], *z = d.g.h.wk[1], *p = d.g.h.wk[2], *q = d.g.h.wk[3];
     gmg_setup(d, c, 0, nullptr);
+    if (persist_enabled()) {                      // the whole solve in one persistent launch
+        lin(c, d.g.h.wk[7], 0.0, x, 1.0);        // start backup
+        const int pr = persist_graph(d, 0, maxit, rtol, 0.0, nullptr, false);
+        if (pr == 1) {
+            KrylovS hs{};
+            cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
+            cudaStreamSynchronize(c.st);
+            return hs.it;
+        }
+        if (pr < 0) lin(c, x, 0.0, d.g.h.wk[7], 1.0);
+    }
     matvec(c, x, q);
     lin(c, r, 0.0, b, 1.0, q, -1.0);
     gmg_apply(d, c, r, z, nullptr, false);
@@ -686,6 +697,19 @@ int bicg_graph(Inst &d, int maxit, double rtol, double atol, double *rn_out, dou
            *sh = d.g.h.wk[5], *t = d.g.h.wk[6];
     const double *w = d.g.h.dsc;
     gmg_setup(d, c, qsign, w);
+    if (persist_enabled()) {                      // the whole solve in one persistent launch
+        lin(c, d.g.h.wk[7], 0.0, x, 1.0);        // start backup
+        const int pr = persist_graph(d, 1, maxit, rtol, atol, w, ilu_only);
+        if (pr == 1) {
+            KrylovS hs{};
+            cudaMemcpyAsync(&hs, c.h.ks, sizeof(KrylovS), cudaMemcpyDeviceToHost, c.st);
+            cudaStreamSynchronize(c.st);
+            *r0_out = hs.r0;
+            *rn_out = std::sqrt(hs.rr);
+            return hs.it;
+        }
+        if (pr < 0) lin(c, x, 0.0, d.g.h.wk[7], 1.0);
+    }
     matvec(c, x, t);
     lin(c, r, 0.0, b, 1.0, t, -1.0);
     lin(c, rh, 0.0, r, 1.0);

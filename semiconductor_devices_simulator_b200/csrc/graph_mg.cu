@@ -26,6 +26,7 @@
 #include "device_common.cuh"
 #include "prof.h"
 #include "solver_ctx.h"
+#include "gmg_common.cuh"
 
 namespace ss {
 
@@ -118,30 +119,14 @@ __global__ void k_gmg_ilu(GLev v, const int *__restrict__ nodes, int cnt) {
 // one colour of the D-ILU(0) solve: forward (dir 0) y_i = (r_i - sum earlier colours a_ij
 // y_j) / D_i, backward (dir 1) z_i = y_i - sum later colours a_ij z_j / D_i; r may be z
 __global__ void k_gmg_ilu_apply(GLev v, const int *__restrict__ nodes, int cnt, int dir, const double *r, double *z) {
-    SS_GRID_LOOP(t, cnt) {
-        const int i = nodes[t], ci = v.color[i];
-        double s = 0.0;
-        for (int q = 0; q < v.D; q++) {
-            const size_t e = (size_t)q * v.N + i;
-            const int j = v.col[e];
-            if (j < 0) continue;
-            const int cj = v.color[j];
-            if (dir == 0 ? cj < ci : cj > ci) s += v.val[e] * z[j];
-        }
-        z[i] = dir == 0 ? (r[i] - s) * v.dil[i] : z[i] - s * v.dil[i];
-    }
+    SS_GRID_LOOP(t, cnt) gilu_apply_node(v, nodes[t], dir, r, z);
 }
 
 // y = b - A x (b null: y = A x)  (gmatvec_L, semiconductor_3d.c:2553-2561)
 __global__ void k_gmg_matvec(GLev v, const double *__restrict__ x, const double *__restrict__ b,
                              double *__restrict__ y) {
     SS_GRID_LOOP(k, v.N) {
-        double s = v.diag[k] * x[k];
-        for (int q = 0; q < v.D; q++) {
-            const size_t e = (size_t)q * v.N + k;
-            const int j = v.col[e];
-            if (j >= 0) s += v.val[e] * x[j];
-        }
+        const double s = gmatvec_row(v, x, k);
         y[k] = b ? b[k] - s : s;
     }
 }
@@ -410,6 +395,8 @@ void gmg_free(Inst &d) {
     d.g.gcyc_off = false;
     if (d.g.gmgblock) cudaFree(d.g.gmgblock);
     d.g.gmgblock = nullptr;
+    if (d.g.gptab) cudaFree(d.g.gptab);
+    d.g.gptab = nullptr;
     d.g.glev.clear();
 }
 

@@ -1,0 +1,98 @@
+// Grid-wide barrier and reduction of the persistent (cooperative, one launch per linear
+// solve) kernels of the tensor and graph solve paths.
+//
+// Barrier: every block arrives (release), thread 0 of each block waits for all arrivals
+// (acquire).  Every wait is bounded: after the launch's limit a block sets the error word
+// and leaves, every other block leaves at its next wait, and the host, which reads the
+// error word after the launch, repeats the solve on the per-pass path.
+//
+// Reduction: each block writes its partial record, and after the barrier every block sums
+// all records in block order, so every block holds bit-identical totals and takes the same
+// decisions with no extra barrier.  Two alternating partial buffers keep a reduction from
+// overwriting partials another block may still be reading.
+#pragma once
+#include "device_common.cuh"
+
+namespace ss {
+
+constexpr int PG_TPB = 1024;
+constexpr unsigned long long PG_WAIT_NS = 2000000000ull;    // longest barrier wait of a solve (2 s)
+
+__device__ __forceinline__ unsigned long long pg_clock() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ unsigned pg_ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// per-block state of a persistent launch
+struct PS {
+    PGrid *g;
+    unsigned target;   // arrivals the next barrier waits for
+    int rb;            // reduction buffer of the next reduction
+    int tid, nth;      // thread index in the grid, threads in the grid
+    unsigned long long wait_ns;   // longest wait at one barrier
+};
+
+// Grid-wide barrier: every block arrives (release), thread 0 waits for all arrivals
+// (acquire), then the block proceeds.  Returns false when the launch is being abandoned.
+__device__ __forceinline__ bool pg_sync(PS &s) {
+    __shared__ int s_ok;
+    __syncthreads();
+    s.target += gridDim.x;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&s.g->count, 1u);
+        int ok = 1;
+        unsigned long long t0 = 0;
+        unsigned it = 0;
+        while ((int)(pg_ld_acquire(&s.g->count) - s.target) < 0) {
+            if ((++it & 255u) == 0) {
+                if (*(volatile unsigned *)&s.g->err) { ok = 0; break; }
+                const unsigned long long t = pg_clock();
+                if (!t0) t0 = t;
+                else if (t - t0 > s.wait_ns) { atomicExch(&s.g->err, 1u); ok = 0; break; }
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Sum NV (<= 4) values over the grid; every block returns the same totals in every thread.
+template <int NV>
+__device__ __forceinline__ bool pg_sum(PS &s, double (&v)[NV]) {
+    __shared__ double tot[4];
+    block_sum<NV>(v);
+    double *buf = s.g->red[s.rb];
+    s.rb ^= 1;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < NV; q++) buf[blockIdx.x * 4 + q] = v[q];
+    if (!pg_sync(s)) return false;
+    if (threadIdx.x < 32) {
+        double a[NV];
+#pragma unroll
+        for (int q = 0; q < NV; q++) a[q] = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32)
+#pragma unroll
+            for (int q = 0; q < NV; q++) a[q] += __ldcg(buf + b * 4 + q);
+        warp_sum<NV>(a);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int q = 0; q < NV; q++) tot[q] = a[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; q++) v[q] = tot[q];
+    return true;
+}
+
+
+}  // namespace ss

@@ -82,6 +82,7 @@ struct Gpu {
     void *gmgblock = nullptr;    // graph multigrid levels (one allocation)
     std::vector<GLevHost> glev;  // graph multigrid hierarchy, level 0 = the mesh
     std::vector<GmgCycle> gcyc;  // its V-cycles captured as CUDA graphs (per operand set)
+    void *gptab = nullptr;       // the hierarchy's level table for the persistent graph solves (device)
     bool gcyc_off = false;       // capture failed once: launch the V-cycle directly
     void *trblock = nullptr;     // deep-level trap entries (CSR per node) and species
     void *coblock = nullptr;     // Coulomb interface entries and every node's nearest one
@@ -221,6 +222,7 @@ void launch_node_Jc_g(const Ctx &c, int which, double *out);
 void launch_emax_g(const Ctx &c);
 int pcg_graph(Inst &d, int maxit, double rtol);
 int bicg_graph(Inst &d, int maxit, double rtol, double atol, double *rn, double *r0, int qsign, bool ilu_only);
+int persist_graph(Inst &d, int kind, int maxit, double rtol, double atol, const double *w, bool ilu_only);
 // aggregation multigrid of a graph mesh (graph_mg.cu)
 int gmg_build(Inst &d, cudaStream_t st);
 void gmg_free(Inst &d);

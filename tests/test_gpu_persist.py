@@ -150,3 +150,30 @@ def test_bounded_barrier_wait_gives_up(lib):
     # the device still works: a normal solve afterwards
     s = w.sweeps[0]
     assert D.start_sweep(lib, w, s)
+
+
+@pytest.mark.parametrize("diag", [0.0, 0.3])
+def test_persistent_graph_sweep_matches_per_pass(lib, diag):
+    """The general-mesh path (ELL kernels, aggregation multigrid with the multicolour
+    smoother): a small graph MOSFET's Id-Vg sweep at tight tolerances, persistent solves
+    against the per-launch ones (host-driven Krylov loops) - the same currents within 1e-6
+    relative or the floor, far fewer launches.  diag > 0 adds diagonal edges in every x-y
+    cell (more colours per level)."""
+    res = {}
+    old = persist(lib, True)
+    try:
+        for on in (True, False):
+            persist(lib, on)
+            w = D.graph_nmosfet(lib, n=(24, 12, 3), models=4, vd=1.0, vg_max=1.0, dvg=0.2, solver=TIGHT, diag=diag)
+            s = w.sweeps[0]
+            assert D.start_sweep(lib, w, s)
+            l0 = lib.b200x_launches()
+            V, I, F, conv = D.run_sweep(lib, w, s)
+            res[on] = (I, F, conv, lib.b200x_launches() - l0)
+    finally:
+        persist(lib, old)
+    (I1, F1, c1, n1), (I0, F0, c0, n0) = res[True], res[False]
+    assert c1.all() and c0.all()
+    tol = np.maximum(1e-6 * np.abs(I0), np.maximum(F0, F1))
+    assert (np.abs(I1 - I0) <= tol).all(), np.max(np.abs(I1 - I0) / np.maximum(np.abs(I0), 1e-300))
+    assert n1 < n0, (n1, n0)
