@@ -81,6 +81,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bounded CPU-baseline sample (s)")
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the e2e pass (profiler captures)")
+    ap.add_argument("--trace", action="store_true", help="with --probe: barrier timeline of the persistent solve")
     ap.add_argument("--probe", type=int, default=0, metavar="ITS",
                     help="profiler probe: one continuity system of the workload device at its charge-neutral "
                          "start, multigrid set-up and ITS BiCGSTAB iterations (a few hundred launches)")
@@ -110,6 +111,31 @@ def run_probe(a):
     lib.b200x_stream_timer(0)
     lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
     solve_ms2 = lib.b200x_stream_timer(1)
+    timeline = None
+    if a.trace:                                             # barrier timeline of one more (warm) solve
+        nb = 4096
+        lib.b200x_persist_trace(nb, None, None)
+        lib.b200x_cont_assemble(0, None, None, None, None)
+        lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
+        buf = (ctypes.c_ulonglong * (3 * nb))()
+        blocks = ctypes.c_int(0)
+        if lib.b200x_persist_trace(0, buf, ctypes.byref(blocks)) == 1:
+            t = np.frombuffer(buf, dtype=np.uint64).reshape(nb, 3).astype(np.float64)
+            used = t[:, 2] > 0
+            t = t[used]
+            t0 = t[0, 0]
+            first, last, rel = (t[:, 0] - t0) / 1e3, (t[:, 1] - t0) / 1e3, (t[:, 2] - t0) / 1e3
+            work = last - np.concatenate([[0.0], rel[:-1]])        # previous release -> last arrival
+            wait = rel - last                                       # last arrival -> release
+            skew = last - first
+            timeline = {"blocks": blocks.value, "barriers": int(len(t)), "total_us": round(float(rel[-1]), 1),
+                        "work_us": {"mean": round(float(work.mean()), 3), "median": round(float(np.median(work)), 3),
+                                    "sum": round(float(work.sum()), 1)},
+                        "release_us": {"mean": round(float(wait.mean()), 3), "median": round(float(np.median(wait)), 3),
+                                       "sum": round(float(wait.sum()), 1)},
+                        "arrival_skew_us": {"mean": round(float(skew.mean()), 3)},
+                        "first_barriers": [[round(float(x), 2) for x in (work[q], skew[q], wait[q])]
+                                           for q in range(min(120, len(t)))]}
     # one pass of the learned predictor's seed kernel (untrained weights) on the same device
     from semiconductor_devices_simulator_b200 import learned as LR
     LR.load(lib, LR.init_params(lib.api3b_seed_nparam(), seed=0, out_scale=1.0))
@@ -123,7 +149,7 @@ def run_probe(a):
     print(json.dumps({"probe": f"{WL}_{mesh[0]}x{mesh[1]}x{mesh[2]} electron continuity", "nodes": w.N,
                       "precision": a.precision, "seed_kernel": seed_ok, "seed_ms": round(seed_ms, 4),
                       "bicgstab_its": its, "r0": r0[0], "rn": rn[0], "solve_ms": [round(solve_ms, 3), round(solve_ms2, 3)],
-                      "persistent": bool(lib.api3b_set_persist(-1, -1)),
+                      "persistent": bool(lib.api3b_set_persist(-1, -1)), "timeline": timeline,
                       "launches": int(lib.b200x_launches() - l0)}))
 
 

@@ -77,6 +77,11 @@ int b200x_pcg(int maxit, double rtol, double *sol);
    Returns the error word (1 when the others gave up after wait_s seconds) and in
    *gave_up how many blocks reported it (nb - 1); -1 if the launch failed. */
 int b200x_persist_probe(int nb, double wait_s, int *gave_up);
+/* Barrier timeline of the next persistent solve (measurement hook): n > 0 arms a timeline of
+   n barriers (returns 0); n == 0 copies it to out - per barrier the first and the last
+   block's arrival and the release as block 0 saw it (globaltimer ns) - disarms it and
+   returns 1 when a launch filled it, with that launch's blocks in *blocks. */
+int b200x_persist_trace(int n, unsigned long long *out, int *blocks);
 /* floating-block balance of a continuity solution (in place) */
 int b200x_float_fix(int hole, double *sol);
 /* learned predictor on the present history arrays (22-24 h1, 25-27 e2 of b200x_set /

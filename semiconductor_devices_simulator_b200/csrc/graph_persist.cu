@@ -190,6 +190,8 @@ __global__ void __launch_bounds__(GP_TPB, 1) k_gpersist(const DevP *Ps, GPArgs a
     s.tid = blockIdx.x * blockDim.x + threadIdx.x;
     s.nth = gridDim.x * blockDim.x;
     s.wait_ns = PG_WAIT_NS;
+    s.trace = nullptr;
+    s.ntrace = 0;
     if (threadIdx.x == 0) sk = *P.ks;
     __syncthreads();
     const PGLev &H0 = a.lev[0];

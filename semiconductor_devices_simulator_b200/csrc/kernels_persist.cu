@@ -48,6 +48,8 @@ struct PArgs {
     int fuse_up;     // 1: prolongation deferred into the residual and post-smoothing passes
     int setup;       // 1: build the hierarchy first (the per-launch mg_setup of kernels_la.cu)
     int qsign;       // its Slotboom weights: 0 none (Poisson), +1 electrons, -1 holes
+    unsigned long long *trace;   // barrier timeline of this launch (null: off)
+    int ntrace;
     double alpha;    // prolongation factor
     double rtol, atol;   // stop rule of the FP64 BiCGSTAB start (PK_BICG)
 };
@@ -468,6 +470,8 @@ __global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) 
     s.tid = blockIdx.x * blockDim.x + threadIdx.x;
     s.nth = gridDim.x * blockDim.x;
     s.wait_ns = PG_WAIT_NS;
+    s.trace = a.trace;
+    s.ntrace = a.ntrace;
     const int nl = P.nlev;
     if (a.setup && !pg_setup<T>(P, s, a, sraw)) return;
     if (blockIdx.x == 0) {                        // the small levels stay in block 0's shared memory
@@ -623,6 +627,8 @@ __global__ void k_pg_timeout_probe(PGrid *g, unsigned long long wait_ns, int *ok
     s.tid = blockIdx.x * blockDim.x + threadIdx.x;
     s.nth = gridDim.x * blockDim.x;
     s.wait_ns = wait_ns;
+    s.trace = nullptr;
+    s.ntrace = 0;
     if (blockIdx.x == gridDim.x - 1) return;     // never arrives
     const bool r = pg_sync(s);
     if (threadIdx.x == 0) ok[blockIdx.x] = r ? 1 : 0;
@@ -640,6 +646,9 @@ int g_persist_mode = -1;   // -1 unread, 0 off, 1 on
 int g_persist_blocks = 0;  // blocks per launch (0: every SM's worth)
 bool g_persist_broken = false;
 bool g_coop_ok = false;    // the device supports cooperative launches
+unsigned long long *g_trace = nullptr;   // armed barrier timeline (test hook): device buffer
+int g_trace_n = 0, g_trace_used = 0;     // its barriers; 1 once a launch has filled it
+int g_last_blocks = 0;                   // blocks of the last persistent launch
 int g_fuse_up = 1;         // deferred prolongation on the way up (SEMISIM_B200_FUSEUP=0: off)
 
 template <class T, int KIND>
@@ -716,11 +725,17 @@ static int persist_run(const Ctx &c, int Ls, size_t smem, const PArgs &a, PGrid 
     cudaMemsetAsync(g, 0, 6 * sizeof(unsigned), c.st);      // counter, error word, work counters
     const DevP *dp = c.dP;
     PArgs aa = a;
+    if (g_trace && !g_trace_used) {              // the armed timeline records this launch only
+        aa.trace = g_trace;
+        aa.ntrace = g_trace_n;
+        g_trace_used = 1;
+    }
     void *args[] = {(void *)&dp, (void *)&aa};
     g_launches++;
     t_launches++;
     const int pid = sizeof(T) == 4 ? PF_PERSIST32 : PF_PERSIST;
     if (g_prof_on) prof_begin(pid, c.st);
+    g_last_blocks = nb;
     const cudaError_t e = cudaLaunchCooperativeKernel(kfn<T, KIND>(), dim3(nb), dim3(PG_TPB), args, smem, c.st);
     if (g_prof_on) prof_end(pid, c.st, 0.0);
     if (e != cudaSuccess) {
@@ -875,6 +890,33 @@ int persist_refined(const Ctx &c, const MGHost &mg, int maxsteps, int *steps, in
         }
     }
     return rc;
+}
+
+// Barrier timeline of the next persistent launch (test and measurement hook): n > 0 arms a
+// timeline of n barriers; n == 0 copies the recorded one to out (3 n values: first arrival,
+// last arrival, release seen by block 0, globaltimer ns; unused barriers keep ~0, 0, 0),
+// disarms it and returns the blocks of that launch.
+int persist_trace(int n, unsigned long long *out, int *blocks) {
+    static int nmax = 0;
+    if (n > 0) {
+        if (g_trace) cudaFree(g_trace);
+        g_trace = nullptr;
+        if (cudaMalloc(&g_trace, sizeof(unsigned long long) * 3 * n) != cudaSuccess) { cudaGetLastError(); return -1; }
+        std::vector<unsigned long long> init(3 * (size_t)n, 0ull);
+        for (int q = 0; q < n; q++) init[3 * q] = ~0ull;
+        cudaMemcpy(g_trace, init.data(), init.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice);
+        g_trace_n = nmax = n;
+        g_trace_used = 0;
+        return 0;
+    }
+    if (!g_trace) return -1;
+    cudaDeviceSynchronize();
+    if (out) cudaMemcpy(out, g_trace, sizeof(unsigned long long) * 3 * nmax, cudaMemcpyDeviceToHost);
+    cudaFree(g_trace);
+    g_trace = nullptr;
+    g_trace_n = 0;
+    if (blocks) *blocks = g_last_blocks;
+    return g_trace_used;
 }
 
 // Run the bounded-wait test on the instance's barrier record with `nb` blocks (>= 2):

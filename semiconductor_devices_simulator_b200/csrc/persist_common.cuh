@@ -36,6 +36,8 @@ struct PS {
     int rb;            // reduction buffer of the next reduction
     int tid, nth;      // thread index in the grid, threads in the grid
     unsigned long long wait_ns;   // longest wait at one barrier
+    unsigned long long *trace;    // barrier timeline (null: off): per barrier first arrival,
+    int ntrace;                   //   last arrival, release seen by block 0 (globaltimer ns)
 };
 
 // Grid-wide barrier: every block arrives (release), thread 0 waits for all arrivals
@@ -44,6 +46,12 @@ __device__ __forceinline__ bool pg_sync(PS &s) {
     __shared__ int s_ok;
     __syncthreads();
     s.target += gridDim.x;
+    const int bn = (int)(s.target / gridDim.x) - 1;          // this barrier's number in the launch
+    if (threadIdx.x == 0 && s.trace && bn < s.ntrace) {
+        const unsigned long long t = pg_clock();
+        atomicMin(s.trace + 3 * bn, t);
+        atomicMax(s.trace + 3 * bn + 1, t);
+    }
     if (threadIdx.x == 0) {
         __threadfence();
         atomicAdd(&s.g->count, 1u);
@@ -60,6 +68,7 @@ __device__ __forceinline__ bool pg_sync(PS &s) {
         }
         __threadfence();
         s_ok = ok;
+        if (s.trace && bn < s.ntrace && blockIdx.x == 0) s.trace[3 * bn + 2] = pg_clock();
     }
     __syncthreads();
     return s_ok != 0;

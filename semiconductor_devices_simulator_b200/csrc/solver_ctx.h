@@ -270,6 +270,7 @@ int persist_bicg(const Ctx &c, const MGHost &mg, double rtol, double atol, int q
 int persist_refined(const Ctx &c, const MGHost &mg, int maxsteps, int *steps, int qsign);
 void vcycle_knobs_init();
 int persist_timeout_probe(const Ctx &c, int nb, double wait_s, int *gave_up);
+int persist_trace(int n, unsigned long long *out, int *blocks);
 extern int g_l0_sweeps, g_deep_levels;
 int bicgstab_core(const Ctx &c, const MGHost &mg, int maxit, double rtol, double atol, int mg_on, int check_every,
                   double *rn, double *r0, int qsign, int mixed = 0);

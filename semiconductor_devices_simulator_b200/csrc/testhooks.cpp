@@ -263,6 +263,9 @@ int b200x_persist_probe(int nb, double wait_s, int *gave_up) {
     Ctx c = make_ctx(d);
     return persist_timeout_probe(c, nb, wait_s, gave_up);
 }
+// barrier timeline of the next persistent solve: n > 0 arms it, n == 0 reads it (3 n
+// values per barrier: first arrival, last arrival, release; ns) and the launch's blocks
+int b200x_persist_trace(int n, unsigned long long *out, int *blocks) { return persist_trace(n, out, blocks); }
 // PCG on the Poisson system now in A / rhs from sol = 0
 int b200x_pcg(int maxit, double rtol, double *sol) {
     Inst &d = *dev();
