@@ -31,6 +31,7 @@ namespace ss {
 constexpr int GP_TPB = 1024;
 constexpr int GP_MAXC = 64;         // most colours of a level
 constexpr int GP_SMALL = 4096;      // levels at or below this size run in block 0
+constexpr int GP_MAXL = 16;         // most levels (the level table lives in shared memory)
 
 // one level as the persistent kernel sees it: the level, its colour classes
 struct PGLev {
@@ -180,9 +181,20 @@ __device__ __forceinline__ double gp_spmv_dot(const PGLev &H, const PS &s, const
     return acc;
 }
 
-__global__ void __launch_bounds__(GP_TPB, 1) k_gpersist(const DevP *Ps, GPArgs a) {
+__global__ void __launch_bounds__(GP_TPB, 1) k_gpersist(const DevP *Ps, GPArgs ga) {
     const DevP &P = Ps[0];
     __shared__ KrylovS sk;
+    // the level table in shared memory: after each grid barrier L1 holds nothing, and the
+    // passes would otherwise re-read their level descriptors from L2
+    __shared__ PGLev lt[GP_MAXL];
+    {
+        const int words = ga.nl * (int)(sizeof(PGLev) / sizeof(unsigned));
+        const unsigned *src = reinterpret_cast<const unsigned *>(ga.lev);
+        unsigned *dst = reinterpret_cast<unsigned *>(lt);
+        for (int q = threadIdx.x; q < words; q += blockDim.x) dst[q] = src[q];
+    }
+    GPArgs a = ga;
+    a.lev = lt;
     PS s;
     s.g = P.pgrid;
     s.target = 0;
@@ -192,6 +204,7 @@ __global__ void __launch_bounds__(GP_TPB, 1) k_gpersist(const DevP *Ps, GPArgs a
     s.wait_ns = PG_WAIT_NS;
     s.trace = nullptr;
     s.ntrace = 0;
+    s.mode = 1;
     if (threadIdx.x == 0) sk = *P.ks;
     __syncthreads();
     const PGLev &H0 = a.lev[0];
@@ -406,7 +419,7 @@ int persist_graph(Inst &d, int kind, int maxit, double rtol, double atol, const 
     if (!d.g.gptab) {
         if (cudaMalloc(&d.g.gptab, sizeof(PGLev) * 32) != cudaSuccess) { cudaGetLastError(); return 0; }
     }
-    if (nl > 32) return 0;
+    if (nl > GP_MAXL) return 0;
     if (!g_gp_blocks) {
         int per = 0, dev = 0, nsm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_gpersist, GP_TPB, 0);

@@ -36,6 +36,12 @@
 #include "persist_common.cuh"
 #include "prof.h"
 
+// the pass functions inline into the kernel (compiled apart, __noinline__, they measured
+// 30 % slower: every view field was reloaded after each store)
+#ifndef PG_PASS
+#define PG_PASS __forceinline__
+#endif
+
 namespace ss {
 
 enum PKind { PK_PCG = 0, PK_BICG = 1, PK_REFINED = 2 };
@@ -50,57 +56,183 @@ struct PArgs {
     int qsign;       // its Slotboom weights: 0 none (Poisson), +1 electrons, -1 holes
     unsigned long long *trace;   // barrier timeline of this launch (null: off)
     int ntrace;
+    int barmode;                 // grid-barrier form (persist_common.cuh)
     double alpha;    // prolongation factor
     double rtol, atol;   // stop rule of the FP64 BiCGSTAB start (PK_BICG)
 };
 
-// ---------------------------------------------------------------- grid passes of a level
+// ---------------------------------------------------------------- on-chip tables
+// Every descriptor a pass needs (level views, vector pointers) is copied into shared
+// memory once per launch: after each grid barrier the acquire invalidates L1, so a
+// descriptor read from global memory would cost a chain of dependent L2 round trips per
+// pass, more than the pass's own loads on the small levels.
 template <class T>
-__device__ __forceinline__ void pg_smooth(const LevView<T> &v, int mode, int color, const PS &s) {
+struct PTab {
+    LevView<T> lev[MAXLEV];      // every level; level 0's x and b are set per V-cycle
+    T *vec[8];                   // level-0 work vectors of precision T
+    T *sol, *rhs;
+    const T *w0;                 // level-0 row weights (continuity systems)
+    const double *A64;           // the FP64 level-0 operator (coupling q at A64 + q * ap64 + k)
+    int ap64;
+    LevView<T> cur0;             // level 0 with the running V-cycle's b and x
+};
+template <class T>
+__device__ __forceinline__ void ptab_fill(const DevP &P, PTab<T> &tb) {
+    const int nl = P.nlev, t = threadIdx.x;
+    if (t < nl) tb.lev[t] = levview<T>(P, t, 0, 0);
+    if (t >= 32 && t < 40) tb.vec[t - 32] = PT<T>::wk(P, t - 32);
+    if (t == 40) {
+        tb.sol = PT<T>::sol(P);
+        tb.rhs = PT<T>::rhs(P);
+        tb.w0 = PT<T>::w0(P);
+        tb.A64 = P.A[0];
+        tb.ap64 = (int)(P.A[1] - P.A[0]);
+    }
+}
+// level 0 with the V-cycle's b and x, for the passes to read from shared memory (every
+// thread of the block calls it: it ends with a block barrier)
+template <class T>
+__device__ __forceinline__ void set_lev0(PTab<T> &tb, int bsel, int xsel) {
+    if (threadIdx.x == 0) {
+        tb.cur0 = tb.lev[0];
+        tb.cur0.b = tb.vec[bsel];
+        tb.cur0.x = tb.vec[xsel];
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------- grid passes of a level
+// (i, j, l) and node index of item t of a half sweep over one colour
+struct HItem { int k, i, j, l; bool ok; };
+template <class T>
+__device__ __forceinline__ HItem hitem(const LevView<T> &v, int t, int tot, int color) {
+    HItem h;
+    h.ok = t < tot;
+    if (!h.ok) { h.k = h.i = h.j = h.l = 0; return h; }
+    const int hx = (v.Nx + 1) >> 1;
+    const int row = t / hx, ti = t - row * hx;
+    h.l = row / v.Ny;
+    h.j = row - h.l * v.Ny;
+    h.i = 2 * ti + ((h.j + h.l + color) & 1);
+    h.ok = h.i < v.Nx;
+    h.k = h.i + v.Nx * row;
+    return h;
+}
+// new x (and the z parked in r for the other colour's sweep) of one node of a half sweep,
+// without storing: the smoother update of smooth_node (la_common.cuh) split into its
+// loads and its stores, so that two nodes' loads can be in flight together (a node of the
+// sweep's colour reads only the other colour's nodes and itself)
+template <class T>
+struct SmRes { T x, r; };
+template <class T>
+__device__ __forceinline__ SmRes<T> smooth_eval(const LevView<T> &v, const HItem &h, int mode, int color) {
+    SmRes<T> o;
+    const int k = h.k;
+    if (mode == 2) {
+        if (color) {
+            const T z = (v.b[k] - lv_apply<T>(v, v.x, k, h.i, h.j, h.l)) * v.D[k];
+            o.x = v.x[k] + z;
+            o.r = z;
+        } else {
+            o.x = v.x[k] - lv_offdiag<T>(v, v.r, k, h.i, h.j, h.l) * v.D[k];
+            o.r = 0;
+        }
+        return o;
+    }
+    const T *src = mode ? v.r : v.b;
+    T z;
+    if (color) z = (src[k] - lv_offdiag_scaled<T>(v, src, k, h.i, h.j, h.l)) * v.D[k];
+    else z = (src[k] - lv_offdiag<T>(v, mode ? v.r : v.x, k, h.i, h.j, h.l)) * v.D[k];
+    o.x = mode ? v.x[k] + z : z;
+    o.r = z;
+    return o;
+}
+// the stores of smooth_eval's result (r only where the sweep parks z: black, modes 1, 2)
+template <class T>
+__device__ __forceinline__ void smooth_store(const LevView<T> &v, const HItem &h, const SmRes<T> &o, int mode,
+                                             int color) {
+    v.x[h.k] = o.x;
+    if (color && mode) v.r[h.k] = o.r;
+}
+// prolongation of the coarse correction to node h (added by the deferred way up)
+template <class T>
+__device__ __forceinline__ T prol_at(const LevView<T> &f, const LevView<T> &cl, T al, int k, int i, int j, int l) {
+    const int I = f.cx ? i >> 1 : i, J = f.cy ? j >> 1 : j, K = f.cz ? l >> 1 : l;
+    return al * f.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+}
+// half sweep of one colour, two nodes per thread and loop trip; cl non-null: post-
+// smoothing with the deferred prolongation added to each node first (mode 1)
+template <class T>
+__device__ PG_PASS void pg_smooth(const LevView<T> &vr, int mode, int color, const PS &s,
+                                       const LevView<T> *clr = nullptr, T al = 0) {
+    const LevView<T> v = vr;                      // register copies of the shared-memory views
+    LevView<T> clv;
+    const LevView<T> *cl = nullptr;
+    if (clr) { clv = *clr; cl = &clv; }
     const int hx = (v.Nx + 1) >> 1, tot = hx * v.Ny * v.Nz;
-    for (int t = s.tid; t < tot; t += s.nth) {
-        const int row = t / hx, ti = t - row * hx;
-        const int l = row / v.Ny, j = row - l * v.Ny;
-        const int i = 2 * ti + ((j + l + color) & 1);
-        if (i < v.Nx) smooth_node<T>(v, i + v.Nx * row, i, j, l, mode, color);
+    for (int t = s.tid; t < tot; t += 2 * s.nth) {
+        const HItem h1 = hitem(v, t, tot, color), h2 = hitem(v, t + s.nth, tot, color);
+        SmRes<T> o1{0, 0}, o2{0, 0};
+        T p1 = 0, p2 = 0;
+        if (h1.ok) {
+            o1 = smooth_eval<T>(v, h1, mode, color);
+            if (cl) p1 = prol_at<T>(v, *cl, al, h1.k, h1.i, h1.j, h1.l);
+        }
+        if (h2.ok) {
+            o2 = smooth_eval<T>(v, h2, mode, color);
+            if (cl) p2 = prol_at<T>(v, *cl, al, h2.k, h2.i, h2.j, h2.l);
+        }
+        if (h1.ok) { o1.x += p1; smooth_store<T>(v, h1, o1, mode, color); }
+        if (h2.ok) { o2.x += p2; smooth_store<T>(v, h2, o2, mode, color); }
     }
 }
 // weighted residual of every fine node summed into its 2x2x2 aggregate: 8 lanes per
-// coarse node (lane bits di, dj, dl), whole warps per loop trip
+// coarse node (lane bits di, dj, dl), whole warps per loop trip, two trips' loads together
 template <class T>
-__device__ __forceinline__ void pg_resid_restrict(const LevView<T> &f, const LevelT<T> &cl, const T *w, const PS &s) {
+__device__ __forceinline__ T rr_val(const LevView<T> &f, const LevView<T> &cl, const T *w, int t) {
+    const int K = t >> 3, sub = t & 7;
+    if (K >= cl.N) return 0;
+    const Node c = unidx(K, cl.Nx, cl.Ny);
+    const int di = sub & 1, dj = (sub >> 1) & 1, dl = sub >> 2;
+    const int i = f.cx ? 2 * c.i + di : c.i, j = f.cy ? 2 * c.j + dj : c.j, l = f.cz ? 2 * c.l + dl : c.l;
+    const bool ok = i < f.Nx && j < f.Ny && l < f.Nz && (f.cx || di == 0) && (f.cy || dj == 0) && (f.cz || dl == 0);
+    if (!ok) return 0;
+    const int k = i + f.Nx * (j + f.Ny * l);
+    const T r = f.b[k] - lv_apply<T>(f, f.x, k, i, j, l);
+    return w ? w[k] * r : r;
+}
+template <class T>
+__device__ __forceinline__ T oct_sum(T v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    return v;
+}
+template <class T>
+__device__ PG_PASS void pg_resid_restrict(const LevView<T> &fr, const LevView<T> &clr, const T *w, const PS &s) {
+    const LevView<T> f = fr, cl = clr;            // register copies of the shared-memory views
     const int nK = ((cl.N + 3) >> 2) << 5;
-    for (int t = s.tid; t < nK; t += s.nth) {
-        const int K = t >> 3, sub = t & 7;
-        T val = 0;
-        if (K < cl.N) {
-            const Node c = unidx(K, cl.Nx, cl.Ny);
-            const int di = sub & 1, dj = (sub >> 1) & 1, dl = sub >> 2;
-            const int i = f.cx ? 2 * c.i + di : c.i, j = f.cy ? 2 * c.j + dj : c.j, l = f.cz ? 2 * c.l + dl : c.l;
-            const bool ok = i < f.Nx && j < f.Ny && l < f.Nz && (f.cx || di == 0) && (f.cy || dj == 0) &&
-                            (f.cz || dl == 0);
-            if (ok) {
-                const int k = i + f.Nx * (j + f.Ny * l);
-                const T r = f.b[k] - lv_apply<T>(f, f.x, k, i, j, l);
-                val = w ? w[k] * r : r;
-            }
-        }
-        val += __shfl_xor_sync(0xffffffffu, val, 1);
-        val += __shfl_xor_sync(0xffffffffu, val, 2);
-        val += __shfl_xor_sync(0xffffffffu, val, 4);
-        if (sub == 0 && K < cl.N) cl.b[K] = val;
+    for (int t = s.tid; t < nK; t += 2 * s.nth) {
+        const int t2 = t + s.nth;                 // whole warps: nK and nth are multiples of 32
+        T v1 = rr_val<T>(f, cl, w, t);
+        T v2 = t2 < nK ? rr_val<T>(f, cl, w, t2) : T(0);
+        v1 = oct_sum<T>(v1);
+        if (t2 < nK) v2 = oct_sum<T>(v2);
+        if ((t & 7) == 0 && (t >> 3) < cl.N) cl.b[t >> 3] = v1;
+        if (t2 < nK && (t2 & 7) == 0 && (t2 >> 3) < cl.N) cl.b[t2 >> 3] = v2;
     }
 }
 template <class T>
-__device__ __forceinline__ void pg_prolong(const LevView<T> &f, const LevelT<T> &cl, T al, const PS &s) {
+__device__ PG_PASS void pg_prolong(const LevView<T> &fr, const LevView<T> &clr, T al, const PS &s) {
+    const LevView<T> f = fr, cl = clr;
     for (int k = s.tid; k < f.N; k += s.nth) {
         const Node a = unidx(k, f.Nx, f.Ny);
-        const int I = f.cx ? a.i >> 1 : a.i, J = f.cy ? a.j >> 1 : a.j, K = f.cz ? a.l >> 1 : a.l;
-        f.x[k] += al * f.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+        f.x[k] += prol_at<T>(f, cl, al, k, a.i, a.j, a.l);
     }
 }
 template <class T>
-__device__ __forceinline__ void pg_resid(const LevView<T> &f, const PS &s) {
+__device__ PG_PASS void pg_resid(const LevView<T> &fr, const PS &s) {
+    const LevView<T> f = fr;
     for (int k = s.tid; k < f.N; k += s.nth) {
         const Node a = unidx(k, f.Nx, f.Ny);
         f.r[k] = f.b[k] - lv_apply<T>(f, f.x, k, a.i, a.j, a.l);
@@ -109,41 +241,35 @@ __device__ __forceinline__ void pg_resid(const LevView<T> &f, const PS &s) {
 
 // The way up, with the prolongation deferred: the residual pass reads the prolonged
 // x + al pw P xc at each stencil point without writing it, and each post-smoothing half
-// sweep adds the prolongation to its own colour's nodes before smoothing them - the same
-// operations as a prolongation pass followed by a residual pass, one barrier fewer.
+// sweep adds the prolongation to its own colour's nodes - the same operations as a
+// prolongation pass followed by a residual pass, one barrier fewer.
 template <class T>
-__device__ __forceinline__ T xprol(const LevView<T> &f, const LevelT<T> &cl, T al, int m, int i, int j, int l) {
-    const int I = f.cx ? i >> 1 : i, J = f.cy ? j >> 1 : j, K = f.cz ? l >> 1 : l;
-    return f.x[m] + al * f.pw[m] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
+__device__ __forceinline__ T xprol(const LevView<T> &f, const LevView<T> &cl, T al, int m, int i, int j, int l) {
+    return f.x[m] + prol_at<T>(f, cl, al, m, i, j, l);
 }
 template <class T>
-__device__ __forceinline__ void pg_prolong_resid(const LevView<T> &f, const LevelT<T> &cl, T al, const PS &s) {
+__device__ __forceinline__ T pr_val(const LevView<T> &f, const LevView<T> &cl, T al, int k) {
     const int NxNy = f.Nx * f.Ny;
-    for (int k = s.tid; k < f.N; k += s.nth) {
-        const Node a = unidx(k, f.Nx, f.Ny);
-        const int i = a.i, j = a.j, l = a.l;
-        T sum = f.a(0, k) * xprol<T>(f, cl, al, k, i, j, l);
-        if (i > 0) sum += f.a(1, k) * xprol<T>(f, cl, al, k - 1, i - 1, j, l);
-        if (i < f.Nx - 1) sum += f.a(2, k) * xprol<T>(f, cl, al, k + 1, i + 1, j, l);
-        if (j > 0) sum += f.a(3, k) * xprol<T>(f, cl, al, k - f.Nx, i, j - 1, l);
-        if (j < f.Ny - 1) sum += f.a(4, k) * xprol<T>(f, cl, al, k + f.Nx, i, j + 1, l);
-        if (l > 0) sum += f.a(5, k) * xprol<T>(f, cl, al, k - NxNy, i, j, l - 1);
-        if (l < f.Nz - 1) sum += f.a(6, k) * xprol<T>(f, cl, al, k + NxNy, i, j, l + 1);
-        f.r[k] = f.b[k] - sum;
-    }
+    const Node a = unidx(k, f.Nx, f.Ny);
+    const int i = a.i, j = a.j, l = a.l;
+    T sum = f.a(0, k) * xprol<T>(f, cl, al, k, i, j, l);
+    if (i > 0) sum += f.a(1, k) * xprol<T>(f, cl, al, k - 1, i - 1, j, l);
+    if (i < f.Nx - 1) sum += f.a(2, k) * xprol<T>(f, cl, al, k + 1, i + 1, j, l);
+    if (j > 0) sum += f.a(3, k) * xprol<T>(f, cl, al, k - f.Nx, i, j - 1, l);
+    if (j < f.Ny - 1) sum += f.a(4, k) * xprol<T>(f, cl, al, k + f.Nx, i, j + 1, l);
+    if (l > 0) sum += f.a(5, k) * xprol<T>(f, cl, al, k - NxNy, i, j, l - 1);
+    if (l < f.Nz - 1) sum += f.a(6, k) * xprol<T>(f, cl, al, k + NxNy, i, j, l + 1);
+    return f.b[k] - sum;
 }
 template <class T>
-__device__ __forceinline__ void pg_smooth_post(const LevView<T> &v, const LevelT<T> &cl, T al, int color, const PS &s) {
-    const int hx = (v.Nx + 1) >> 1, tot = hx * v.Ny * v.Nz;
-    for (int t = s.tid; t < tot; t += s.nth) {
-        const int row = t / hx, ti = t - row * hx;
-        const int l = row / v.Ny, j = row - l * v.Ny;
-        const int i = 2 * ti + ((j + l + color) & 1);
-        if (i >= v.Nx) continue;
-        const int k = i + v.Nx * row;
-        const int I = v.cx ? i >> 1 : i, J = v.cy ? j >> 1 : j, K = v.cz ? l >> 1 : l;
-        v.x[k] += al * v.pw[k] * cl.x[I + cl.Nx * (J + cl.Ny * K)];
-        smooth_node<T>(v, k, i, j, l, 1, color);
+__device__ PG_PASS void pg_prolong_resid(const LevView<T> &fr, const LevView<T> &clr, T al, const PS &s) {
+    const LevView<T> f = fr, cl = clr;            // register copies of the shared-memory views
+    for (int k = s.tid; k < f.N; k += 2 * s.nth) {
+        const int k2 = k + s.nth;
+        const T r1 = pr_val<T>(f, cl, al, k);
+        const T r2 = k2 < f.N ? pr_val<T>(f, cl, al, k2) : T(0);
+        f.r[k] = r1;
+        if (k2 < f.N) f.r[k2] = r2;
     }
 }
 
@@ -155,11 +281,13 @@ __device__ __forceinline__ void pg_smooth_post(const LevView<T> &v, const LevelT
 // one V(1,1) cycle x = M^-1 b on the level-0 vectors (bsel -> xsel), the same passes as
 // the per-pass path (vcycle_t in kernels_la.cu)
 template <class T>
-__device__ bool pg_vcycle(const DevP &P, PS &s, const PArgs &a, const LevView<T> *sv, int bsel, int xsel, int wsel) {
-    const int nl = P.nlev, Ls = a.Ls;
+__device__ __noinline__ bool pg_vcycle(PS &s, const PArgs &a, PTab<T> &tb, const LevView<T> *sv, int nl, int bsel, int xsel,
+                          int wsel) {
+    const int Ls = a.Ls;
     const T al = (T)a.alpha;
+    set_lev0<T>(tb, bsel, xsel);
     for (int L = 0; L < Ls; L++) {
-        const LevView<T> v = levview<T>(P, L, bsel, xsel);
+        const LevView<T> &v = L ? tb.lev[L] : tb.cur0;
         pg_smooth<T>(v, 0, 1, s);
         PG_SYNC();
         pg_smooth<T>(v, 0, 0, s);
@@ -170,11 +298,11 @@ __device__ bool pg_vcycle(const DevP &P, PS &s, const PArgs &a, const LevView<T>
             pg_smooth<T>(v, 2, 0, s);
             PG_SYNC();
         }
-        pg_resid_restrict<T>(v, PT<T>::lev(P, L + 1), (L == 0 && wsel) ? PT<T>::w0(P) : nullptr, s);
+        pg_resid_restrict<T>(v, tb.lev[L + 1], (L == 0 && wsel) ? tb.w0 : nullptr, s);
         PG_SYNC();
     }
     if (blockIdx.x == 0) {
-        const LevelT<T> &g = PT<T>::lev(P, Ls);
+        const LevView<T> &g = tb.lev[Ls];
         blk_copy<T>(sv[0].b, g.b, g.N);
         __syncthreads();
         blk_vcycle_small<T>(sv, Ls, nl, al);
@@ -182,14 +310,14 @@ __device__ bool pg_vcycle(const DevP &P, PS &s, const PArgs &a, const LevView<T>
     }
     PG_SYNC();
     for (int L = Ls - 1; L >= 0; L--) {
-        const LevView<T> v = levview<T>(P, L, bsel, xsel);
-        const LevelT<T> &cl = PT<T>::lev(P, L + 1);
+        const LevView<T> &v = L ? tb.lev[L] : tb.cur0;
+        const LevView<T> &cl = tb.lev[L + 1];
         if (a.fuse_up) {
             pg_prolong_resid<T>(v, cl, al, s);
             PG_SYNC();
-            pg_smooth_post<T>(v, cl, al, 1, s);
+            pg_smooth<T>(v, 1, 1, s, &cl, al);
             PG_SYNC();
-            pg_smooth_post<T>(v, cl, al, 0, s);
+            pg_smooth<T>(v, 1, 0, s, &cl, al);
             PG_SYNC();
         } else {
             pg_prolong<T>(v, cl, al, s);
@@ -212,16 +340,22 @@ __device__ bool pg_vcycle(const DevP &P, PS &s, const PArgs &a, const LevView<T>
     return true;
 }
 
+// y = A x on level 0 at node k
+template <class T>
+__device__ __forceinline__ T spmv_at(const LevView<T> &l0, const T *x, int k) {
+    const Node nd = unidx(k, l0.Nx, l0.Ny);
+    return lv_apply<T>(l0, x, k, nd.i, nd.j, nd.l);
+}
+
 // ---------------------------------------------------------------- Krylov loops
 // BiCGSTAB iterations (semiconductor_3d.c:2281-2316) on the records `sk` of precision T
 // while it is active; the reduction of rh.r for the next iteration rides on the x update.
 template <class T>
-__device__ bool pg_bicg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *sv, KrylovS &sk) {
-    T *r = PT<T>::wk(P, 0), *rh = PT<T>::wk(P, 1), *p = PT<T>::wk(P, 2), *v = PT<T>::wk(P, 3);
-    T *ph = PT<T>::wk(P, 4), *sh = PT<T>::wk(P, 5), *t = PT<T>::wk(P, 6);
-    T *x = PT<T>::sol(P);
-    T *const *A = PT<T>::A0(P);
-    const int N = P.N, Nx = P.Nx, Ny = P.Ny, Nz = P.Nz;
+__device__ bool pg_bicg(PS &s, const PArgs &a, PTab<T> &tb, const LevView<T> *sv, int nl, int N, KrylovS &sk) {
+    T *r = tb.vec[0], *rh = tb.vec[1], *p = tb.vec[2], *v = tb.vec[3];
+    T *ph = tb.vec[4], *sh = tb.vec[5], *t = tb.vec[6];
+    T *x = tb.sol;
+    const LevView<T> l0 = tb.lev[0];
     bool have_rho = false;
     double rho_next = 0.0;
     while (sk.active) {
@@ -258,13 +392,15 @@ __device__ bool pg_bicg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *
             }
         }
         PG_SYNC();
-        if (!pg_vcycle<T>(P, s, a, sv, 2, 4, 1)) return false;      // ph = M p
+        if (!pg_vcycle<T>(s, a, tb, sv, nl, 2, 4, 1)) return false;      // ph = M p
         a1[0] = 0.0;
-        for (int k = s.tid; k < N; k += s.nth) {
-            const Node nd = unidx(k, Nx, Ny);
-            const T q = stencil_apply<T>(A, ph, k, nd.i, nd.j, nd.l, Nx, Ny, Nz);
-            v[k] = q;
-            a1[0] += (double)rh[k] * (double)q;
+        for (int k = s.tid; k < N; k += 2 * s.nth) {
+            const int k2 = k + s.nth;
+            const T q1 = spmv_at<T>(l0, ph, k);
+            const T q2 = k2 < N ? spmv_at<T>(l0, ph, k2) : T(0);
+            v[k] = q1;
+            a1[0] += (double)rh[k] * (double)q1;
+            if (k2 < N) { v[k2] = q2; a1[0] += (double)rh[k2] * (double)q2; }
         }
         if (!pg_sum<1>(s, a1)) return false;
         if (threadIdx.x == 0) {
@@ -292,14 +428,20 @@ __device__ bool pg_bicg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *
             PG_SYNC();
             break;
         }
-        if (!pg_vcycle<T>(P, s, a, sv, 0, 5, 1)) return false;      // sh = M r
+        if (!pg_vcycle<T>(s, a, tb, sv, nl, 0, 5, 1)) return false;      // sh = M r
         acc[0] = acc[1] = 0.0;
-        for (int k = s.tid; k < N; k += s.nth) {
-            const Node nd = unidx(k, Nx, Ny);
-            const T q = stencil_apply<T>(A, sh, k, nd.i, nd.j, nd.l, Nx, Ny, Nz);
-            t[k] = q;
-            acc[0] += (double)q * (double)q;
-            acc[1] += (double)q * (double)r[k];
+        for (int k = s.tid; k < N; k += 2 * s.nth) {
+            const int k2 = k + s.nth;
+            const T q1 = spmv_at<T>(l0, sh, k);
+            const T q2 = k2 < N ? spmv_at<T>(l0, sh, k2) : T(0);
+            t[k] = q1;
+            acc[0] += (double)q1 * (double)q1;
+            acc[1] += (double)q1 * (double)r[k];
+            if (k2 < N) {
+                t[k2] = q2;
+                acc[0] += (double)q2 * (double)q2;
+                acc[1] += (double)q2 * (double)r[k2];
+            }
         }
         if (!pg_sum<2>(s, acc)) return false;
         if (threadIdx.x == 0) {
@@ -338,18 +480,19 @@ __device__ bool pg_bicg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *
 
 // PCG iterations (semiconductor_3d.c:2194-2206) on the records `sk` while active
 template <class T>
-__device__ bool pg_pcg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *sv, KrylovS &sk) {
-    T *r = PT<T>::wk(P, 0), *z = PT<T>::wk(P, 1), *p = PT<T>::wk(P, 2), *q = PT<T>::wk(P, 3);
-    T *x = PT<T>::sol(P);
-    T *const *A = PT<T>::A0(P);
-    const int N = P.N, Nx = P.Nx, Ny = P.Ny, Nz = P.Nz;
+__device__ bool pg_pcg(PS &s, const PArgs &a, PTab<T> &tb, const LevView<T> *sv, int nl, int N, KrylovS &sk) {
+    T *r = tb.vec[0], *z = tb.vec[1], *p = tb.vec[2], *q = tb.vec[3];
+    T *x = tb.sol;
+    const LevView<T> l0 = tb.lev[0];
     while (sk.active) {
         double acc[1] = {0.0};
-        for (int k = s.tid; k < N; k += s.nth) {
-            const Node nd = unidx(k, Nx, Ny);
-            const T vq = stencil_apply<T>(A, p, k, nd.i, nd.j, nd.l, Nx, Ny, Nz);
-            q[k] = vq;
-            acc[0] += (double)p[k] * (double)vq;
+        for (int k = s.tid; k < N; k += 2 * s.nth) {
+            const int k2 = k + s.nth;
+            const T q1 = spmv_at<T>(l0, p, k);
+            const T q2 = k2 < N ? spmv_at<T>(l0, p, k2) : T(0);
+            q[k] = q1;
+            acc[0] += (double)p[k] * (double)q1;
+            if (k2 < N) { q[k2] = q2; acc[0] += (double)p[k2] * (double)q2; }
         }
         if (!pg_sum<1>(s, acc)) return false;
         if (threadIdx.x == 0) {
@@ -365,7 +508,7 @@ __device__ bool pg_pcg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *s
             for (int k = s.tid; k < N; k += s.nth) { x[k] += al * p[k]; r[k] -= al * q[k]; }
         }
         PG_SYNC();
-        if (!pg_vcycle<T>(P, s, a, sv, 0, 1, 0)) return false;      // z = M r
+        if (!pg_vcycle<T>(s, a, tb, sv, nl, 0, 1, 0)) return false;      // z = M r
         acc[0] = 0.0;
         for (int k = s.tid; k < N; k += s.nth) acc[0] += (double)r[k] * (double)z[k];
         if (!pg_sum<1>(s, acc)) return false;
@@ -386,27 +529,40 @@ __device__ bool pg_pcg(const DevP &P, PS &s, const PArgs &a, const LevView<T> *s
     return true;
 }
 
+// (A x)_k of the FP64 level-0 operator and, in fl, sum_j |a_kj x_j|
+template <class X>
+__device__ __forceinline__ double a64_at(const double *A, int ap, const X *x, int k, int i, int j, int l, int Nx,
+                                         int Ny, int Nz, double *fl) {
+    const int NxNy = Nx * Ny;
+    double t = A[k] * (double)x[k], sum = t, f = fabs(t);
+    if (i > 0) { t = A[ap + k] * (double)x[k - 1]; sum += t; f += fabs(t); }
+    if (i < Nx - 1) { t = A[2 * ap + k] * (double)x[k + 1]; sum += t; f += fabs(t); }
+    if (j > 0) { t = A[3 * ap + k] * (double)x[k - Nx]; sum += t; f += fabs(t); }
+    if (j < Ny - 1) { t = A[4 * ap + k] * (double)x[k + Nx]; sum += t; f += fabs(t); }
+    if (l > 0) { t = A[5 * ap + k] * (double)x[k - NxNy]; sum += t; f += fabs(t); }
+    if (l < Nz - 1) { t = A[6 * ap + k] * (double)x[k + NxNy]; sum += t; f += fabs(t); }
+    if (fl) *fl = f;
+    return sum;
+}
+
 // r = b - A x with the FP64 operator, its squared norm and the squared rounding floor
 // (sum_k (sum_j |a_kj x_j| + |b_k|)^2) - the start of the FP64 BiCGSTAB and of the
 // refinement (semiconductor_3d.c:2244-2268).  Writes r (FP64 work vector 0) and, when
-// r32 is not null, its FP32 copy.
-__device__ __forceinline__ void pg_start64(const DevP &P, const PS &s, float *r32, double *rh, double (&acc)[2]) {
+// r32 is not null, its FP32 copy; with rh, also rh = r and p = v = 0.
+template <class T>
+__device__ __forceinline__ void pg_start64(const DevP &P, const PTab<T> &tb, const PS &s, float *r32, bool bicg,
+                                           double (&acc)[2]) {
     const double *b = P.rhs, *x = P.sol;
-    double *r = P.wk[0];
-    const int NxNy = P.Nx * P.Ny;
-    for (int k = s.tid; k < P.N; k += s.nth) {
-        const Node a = unidx(k, P.Nx, P.Ny);
-        const int i = a.i, j = a.j, l = a.l;
-        double sum = P.A[0][k] * x[k], fl = fabs(P.A[0][k] * x[k]) + fabs(b[k]), t;
-        if (i > 0) { t = P.A[1][k] * x[k - 1]; sum += t; fl += fabs(t); }
-        if (i < P.Nx - 1) { t = P.A[2][k] * x[k + 1]; sum += t; fl += fabs(t); }
-        if (j > 0) { t = P.A[3][k] * x[k - P.Nx]; sum += t; fl += fabs(t); }
-        if (j < P.Ny - 1) { t = P.A[4][k] * x[k + P.Nx]; sum += t; fl += fabs(t); }
-        if (l > 0) { t = P.A[5][k] * x[k - NxNy]; sum += t; fl += fabs(t); }
-        if (l < P.Nz - 1) { t = P.A[6][k] * x[k + NxNy]; sum += t; fl += fabs(t); }
+    double *r = P.wk[0], *rh = P.wk[1], *p = P.wk[2], *v = P.wk[3];
+    const int Nx = P.Nx, Ny = P.Ny, Nz = P.Nz, N = P.N;
+    for (int k = s.tid; k < N; k += s.nth) {
+        const Node a = unidx(k, Nx, Ny);
+        double fl;
+        const double sum = a64_at<double>(tb.A64, tb.ap64, x, k, a.i, a.j, a.l, Nx, Ny, Nz, &fl);
+        fl += fabs(b[k]);
         const double rk = b[k] - sum;
         r[k] = rk;
-        if (rh) { rh[k] = rk; P.wk[2][k] = 0.0; P.wk[3][k] = 0.0; }
+        if (bicg) { rh[k] = rk; p[k] = 0.0; v[k] = 0.0; }
         if (r32) r32[k] = (float)rk;
         acc[0] += rk * rk;
         acc[1] += fl * fl;
@@ -421,23 +577,25 @@ __device__ __forceinline__ void pg_start64(const DevP &P, const PS &s, float *r3
 // read only the level's own operator), the Galerkin coarse operator (one pass), and the
 // coarsest level's dense inverse (block 0, in its shared memory).
 template <class T>
-__device__ __noinline__ bool pg_setup(const DevP &P, PS &s, const PArgs &a, unsigned char *scratch) {
+__device__ __noinline__ bool pg_setup(const DevP &P, PS &s, const PArgs &a, const PTab<T> &tb, unsigned char *scratch) {
     const int nl = P.nlev, qsign = a.qsign;
     if constexpr (std::is_same<T, float>::value) {
+        float *A32 = const_cast<float *>(tb.lev[0].A);
+        const int ap = tb.lev[0].ap;
         for (int k = s.tid; k < P.N; k += s.nth) {
 #pragma unroll
-            for (int q = 0; q < 7; q++) P.A32[q][k] = (float)P.A[q][k];
+            for (int q = 0; q < 7; q++) A32[q * ap + k] = (float)tb.A64[q * tb.ap64 + k];
             if (qsign) P.dsc32[k] = (float)P.dsc[k];
         }
         PG_SYNC();
     }
     for (int L = 0; L < nl - 1; L++) {
-        const LevView<T> f = levview<T>(P, L, 0, 0);
+        const LevView<T> &f = tb.lev[L];
         const LevelT<T> &cl = PT<T>::lev(P, L + 1);
         for (int K = s.tid; K < cl.N; K += s.nth) mg_weights_node<T>(P, f, cl, L, qsign, K);
         for (int k = s.tid; k < f.N; k += s.nth) ilu_diag_node<T>(f, k);
         PG_SYNC();
-        const T *w = (L == 0 && qsign) ? PT<T>::w0(P) : nullptr;
+        const T *w = (L == 0 && qsign) ? tb.w0 : nullptr;
         for (int K = s.tid; K < cl.N; K += s.nth) galerkin_node<T>(f, cl, w, K);
         PG_SYNC();
     }
@@ -462,6 +620,7 @@ __global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) 
     const DevP &P = Ps[0];
     extern __shared__ __align__(16) unsigned char sraw[];
     __shared__ LevView<T> sv[MAXLEV];
+    __shared__ PTab<T> tb;
     __shared__ KrylovS sk, so;                    // the loop's record (and the outer one: PK_REFINED)
     PS s;
     s.g = P.pgrid;
@@ -472,8 +631,11 @@ __global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) 
     s.wait_ns = PG_WAIT_NS;
     s.trace = a.trace;
     s.ntrace = a.ntrace;
-    const int nl = P.nlev;
-    if (a.setup && !pg_setup<T>(P, s, a, sraw)) return;
+    s.mode = a.barmode;
+    const int nl = P.nlev, N = P.N;
+    ptab_fill<T>(P, tb);
+    __syncthreads();
+    if (a.setup && !pg_setup<T>(P, s, a, tb, sraw)) return;
     if (blockIdx.x == 0) {                        // the small levels stay in block 0's shared memory
         if (threadIdx.x < nl - a.Ls) sv[threadIdx.x] = smem_view<T>(P, a.Ls + threadIdx.x, a.Ls, sraw);
         __syncthreads();
@@ -486,26 +648,27 @@ __global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) 
     __syncthreads();
     KrylovS &rec = sk;
     if constexpr (KIND == PK_PCG) {
+        T *r0 = tb.vec[0];
         if constexpr (std::is_same<T, double>::value) {
-            const int NxNy = P.Nx * P.Ny;
-            for (int k = s.tid; k < P.N; k += s.nth) {
+            for (int k = s.tid; k < N; k += s.nth) {
                 const Node nd = unidx(k, P.Nx, P.Ny);
-                P.wk[0][k] = P.rhs[k] - stencil_apply<double>(P.A, P.sol, k, nd.i, nd.j, nd.l, P.Nx, P.Ny, P.Nz);
+                r0[k] = P.rhs[k] - a64_at<double>(tb.A64, tb.ap64, P.sol, k, nd.i, nd.j, nd.l, P.Nx, P.Ny, P.Nz,
+                                                  nullptr);
             }
-            (void)NxNy;
         } else {
-            for (int k = s.tid; k < P.N; k += s.nth) {
+            float *b32 = tb.rhs, *x32 = tb.sol;
+            for (int k = s.tid; k < N; k += s.nth) {
                 const float b = (float)P.rhs[k];
-                P.rhs32[k] = b;
-                P.wk32[0][k] = b;
-                P.sol32[k] = 0.f;
+                b32[k] = b;
+                r0[k] = b;
+                x32[k] = 0.f;
             }
         }
         if (!pg_sync(s)) return;
-        if (!pg_vcycle<T>(P, s, a, sv, 0, 1, 0)) return;            // z = M r
+        if (!pg_vcycle<T>(s, a, tb, sv, nl, 0, 1, 0)) return;        // z = M r
         double acc[1] = {0.0};
-        const T *r = PT<T>::wk(P, 0), *z = PT<T>::wk(P, 1);
-        for (int k = s.tid; k < P.N; k += s.nth) acc[0] += (double)r[k] * (double)z[k];
+        const T *z = tb.vec[1];
+        for (int k = s.tid; k < N; k += s.nth) acc[0] += (double)r0[k] * (double)z[k];
         if (!pg_sum<1>(s, acc)) return;
         if (threadIdx.x == 0) {
             const double rz = acc[0];
@@ -515,18 +678,18 @@ __global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) 
         }
         __syncthreads();
         if (rec.active) {
-            T *p = PT<T>::wk(P, 2);
-            for (int k = s.tid; k < P.N; k += s.nth) p[k] = z[k];
+            T *p = tb.vec[2];
+            for (int k = s.tid; k < N; k += s.nth) p[k] = z[k];
             if (!pg_sync(s)) return;
-            if (!pg_pcg<T>(P, s, a, sv, rec)) return;
+            if (!pg_pcg<T>(s, a, tb, sv, nl, N, rec)) return;
         }
         if constexpr (std::is_same<T, float>::value) {
             if (rec.status == 1)
-                for (int k = s.tid; k < P.N; k += s.nth) P.sol[k] = (double)P.sol32[k];
+                for (int k = s.tid; k < N; k += s.nth) P.sol[k] = (double)tb.sol[k];
         }
     } else if constexpr (KIND == PK_BICG) {
         double acc[2] = {0.0, 0.0};
-        pg_start64(P, s, nullptr, P.wk[1], acc);
+        pg_start64<T>(P, tb, s, nullptr, true, acc);
         if (!pg_sum<2>(s, acc)) return;
         if (threadIdx.x == 0) {
             rec.rr = acc[0]; rec.fl = acc[1];
@@ -537,10 +700,11 @@ __global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) 
             else { rec.active = 1; rec.status = 0; }
         }
         __syncthreads();
-        if (!pg_bicg<T>(P, s, a, sv, rec)) return;
+        if (!pg_bicg<T>(s, a, tb, sv, nl, N, rec)) return;
     } else {                                      // PK_REFINED
         double acc[2] = {0.0, 0.0};
-        pg_start64(P, s, P.rhs32, nullptr, acc);
+        float *rhs32 = tb.rhs;
+        pg_start64<T>(P, tb, s, rhs32, false, acc);
         if (!pg_sum<2>(s, acc)) return;
         if (threadIdx.x == 0) {
             so.rr = acc[0]; so.fl = acc[1];
@@ -552,12 +716,14 @@ __global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) 
         }
         __syncthreads();
         int steps = 0;
+        double *x = P.sol, *r64 = P.wk[0];
+        const int Nx = P.Nx, Ny = P.Ny, Nz = P.Nz;
         for (; steps < a.maxsteps && so.active; steps++) {
             // inner start: d = 0, r = rh = rhs32, p = v = 0
-            float *r = P.wk32[0], *rh = P.wk32[1], *p = P.wk32[2], *v = P.wk32[3], *d = P.sol32;
+            float *r = tb.vec[0], *rh = tb.vec[1], *p = tb.vec[2], *v = tb.vec[3], *d = tb.sol;
             double ai[1] = {0.0};
-            for (int k = s.tid; k < P.N; k += s.nth) {
-                const float bk = P.rhs32[k];
+            for (int k = s.tid; k < N; k += s.nth) {
+                const float bk = rhs32[k];
                 r[k] = bk; rh[k] = bk; p[k] = 0.f; v[k] = 0.f; d[k] = 0.f;
                 ai[0] += (double)bk * (double)bk;
             }
@@ -573,26 +739,16 @@ __global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) 
                 sk.active = (sk.r0 > sk.tgt && sk.maxit > 0) ? 1 : 0;
             }
             __syncthreads();
-            if (!pg_bicg<float>(P, s, a, sv, sk)) return;
+            if (!pg_bicg<float>(s, a, tb, sv, nl, N, sk)) return;
             // x += d; r -= A d (FP64 operator); rhs32 = (float) r; the outer stop test
             double au[1] = {0.0};
-            double *x = P.sol, *r64 = P.wk[0];
-            const int NxNy = P.Nx * P.Ny;
-            for (int k = s.tid; k < P.N; k += s.nth) {
-                const Node nd = unidx(k, P.Nx, P.Ny);
-                const int i = nd.i, j = nd.j, l = nd.l;
-                const double dk = (double)d[k];
-                double sum = P.A[0][k] * dk;
-                if (i > 0) sum += P.A[1][k] * (double)d[k - 1];
-                if (i < P.Nx - 1) sum += P.A[2][k] * (double)d[k + 1];
-                if (j > 0) sum += P.A[3][k] * (double)d[k - P.Nx];
-                if (j < P.Ny - 1) sum += P.A[4][k] * (double)d[k + P.Nx];
-                if (l > 0) sum += P.A[5][k] * (double)d[k - NxNy];
-                if (l < P.Nz - 1) sum += P.A[6][k] * (double)d[k + NxNy];
-                x[k] += dk;
+            for (int k = s.tid; k < N; k += s.nth) {
+                const Node nd = unidx(k, Nx, Ny);
+                const double sum = a64_at<float>(tb.A64, tb.ap64, d, k, nd.i, nd.j, nd.l, Nx, Ny, Nz, nullptr);
+                x[k] += (double)d[k];
                 const double rk = r64[k] - sum;
                 r64[k] = rk;
-                P.rhs32[k] = (float)rk;
+                rhs32[k] = (float)rk;
                 au[0] += rk * rk;
             }
             if (!pg_sum<1>(s, au)) return;
@@ -629,6 +785,7 @@ __global__ void k_pg_timeout_probe(PGrid *g, unsigned long long wait_ns, int *ok
     s.wait_ns = wait_ns;
     s.trace = nullptr;
     s.ntrace = 0;
+    s.mode = 1;
     if (blockIdx.x == gridDim.x - 1) return;     // never arrives
     const bool r = pg_sync(s);
     if (threadIdx.x == 0) ok[blockIdx.x] = r ? 1 : 0;
@@ -650,6 +807,7 @@ unsigned long long *g_trace = nullptr;   // armed barrier timeline (test hook): 
 int g_trace_n = 0, g_trace_used = 0;     // its barriers; 1 once a launch has filled it
 int g_last_blocks = 0;                   // blocks of the last persistent launch
 int g_fuse_up = 1;         // deferred prolongation on the way up (SEMISIM_B200_FUSEUP=0: off)
+int g_barmode = 1;         // grid-barrier form (SEMISIM_B200_BARMODE; 1 measured faster than 0)
 
 template <class T, int KIND>
 const void *kfn() { return reinterpret_cast<const void *>(&k_persist<T, KIND>); }
@@ -678,6 +836,7 @@ int persist_enabled() {
         g_persist_mode = (e && std::atoi(e) == 0) ? 0 : 1;
         if (const char *b = std::getenv("SEMISIM_B200_PBLOCKS")) g_persist_blocks = std::atoi(b);
         if (const char *f = std::getenv("SEMISIM_B200_FUSEUP")) g_fuse_up = std::atoi(f) != 0;
+        if (const char *m = std::getenv("SEMISIM_B200_BARMODE")) g_barmode = std::atoi(m) ? 1 : 0;
         int dev = 0, coop = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
         if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess) cudaGetLastError();
@@ -826,6 +985,7 @@ int persist_pcg(const Ctx &c, const MGHost &mg, int mixed) {
     a.sweeps2 = g_l0_sweeps > 1;
     a.alpha = mg.alpha;
     a.fuse_up = g_fuse_up;
+    a.barmode = g_barmode;
     PGrid h{};
     const int rc = mixed ? persist_run<float, PK_PCG>(c, a.Ls, smem, a, &h)
                          : persist_run<double, PK_PCG>(c, a.Ls, smem, a, &h);
@@ -852,6 +1012,7 @@ int persist_bicg(const Ctx &c, const MGHost &mg, double rtol, double atol, int q
     a.sweeps2 = g_l0_sweeps > 1;
     a.alpha = mg.alpha;
     a.fuse_up = g_fuse_up;
+    a.barmode = g_barmode;
     a.rtol = rtol;
     a.atol = atol;
     PGrid h{};
@@ -877,6 +1038,7 @@ int persist_refined(const Ctx &c, const MGHost &mg, int maxsteps, int *steps, in
     a.sweeps2 = g_l0_sweeps > 1;
     a.alpha = mg.alpha;
     a.fuse_up = g_fuse_up;
+    a.barmode = g_barmode;
     a.maxsteps = maxsteps;
     PGrid h{};
     const int rc = persist_run<float, PK_REFINED>(c, a.Ls, smem, a, &h);

@@ -38,35 +38,53 @@ struct PS {
     unsigned long long wait_ns;   // longest wait at one barrier
     unsigned long long *trace;    // barrier timeline (null: off): per barrier first arrival,
     int ntrace;                   //   last arrival, release seen by block 0 (globaltimer ns)
+    int mode;                     // barrier form: 0 fences around the arrival and the wait,
+                                  //   1 release-add / acquire-load
 };
 
-// Grid-wide barrier: every block arrives (release), thread 0 waits for all arrivals
-// (acquire), then the block proceeds.  Returns false when the launch is being abandoned.
+// Grid-wide barrier: every block arrives (release), the block waits until every block
+// has arrived (acquire), then proceeds.  Returns false when the launch is being abandoned.
+// Forms (PS::mode): 0 - thread 0 fences, adds and polls; 1 - thread 0 adds with release
+// semantics and polls with acquire loads (no separate fences).  The block barriers before
+// and after order the other threads' accesses with thread 0's.
+__device__ __forceinline__ void pg_red_release(unsigned *p) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
+}
+// poll until the arrivals reach the target; 1 released, 0 abandoned (error word or time)
+__device__ __forceinline__ int pg_poll(PS &s) {
+    unsigned long long t0 = 0;
+    unsigned it = 0;
+    while ((int)(pg_ld_acquire(&s.g->count) - s.target) < 0) {
+        if ((++it & 255u) == 0) {
+            if (*(volatile unsigned *)&s.g->err) return 0;
+            const unsigned long long t = pg_clock();
+            if (!t0) t0 = t;
+            else if (t - t0 > s.wait_ns) { atomicExch(&s.g->err, 1u); return 0; }
+        }
+    }
+    return 1;
+}
 __device__ __forceinline__ bool pg_sync(PS &s) {
     __shared__ int s_ok;
     __syncthreads();
     s.target += gridDim.x;
     const int bn = (int)(s.target / gridDim.x) - 1;          // this barrier's number in the launch
-    if (threadIdx.x == 0 && s.trace && bn < s.ntrace) {
-        const unsigned long long t = pg_clock();
-        atomicMin(s.trace + 3 * bn, t);
-        atomicMax(s.trace + 3 * bn + 1, t);
-    }
     if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(&s.g->count, 1u);
-        int ok = 1;
-        unsigned long long t0 = 0;
-        unsigned it = 0;
-        while ((int)(pg_ld_acquire(&s.g->count) - s.target) < 0) {
-            if ((++it & 255u) == 0) {
-                if (*(volatile unsigned *)&s.g->err) { ok = 0; break; }
-                const unsigned long long t = pg_clock();
-                if (!t0) t0 = t;
-                else if (t - t0 > s.wait_ns) { atomicExch(&s.g->err, 1u); ok = 0; break; }
-            }
+        if (s.trace && bn < s.ntrace) {
+            const unsigned long long t = pg_clock();
+            atomicMin(s.trace + 3 * bn, t);
+            atomicMax(s.trace + 3 * bn + 1, t);
         }
-        __threadfence();
+        int ok;
+        if (s.mode == 0) {
+            __threadfence();
+            atomicAdd(&s.g->count, 1u);
+            ok = pg_poll(s);
+            __threadfence();
+        } else {
+            pg_red_release(&s.g->count);
+            ok = pg_poll(s);
+        }
         s_ok = ok;
         if (s.trace && bn < s.ntrace && blockIdx.x == 0) s.trace[3 * bn + 2] = pg_clock();
     }
