@@ -205,6 +205,7 @@ __global__ void __launch_bounds__(GP_TPB, 1) k_gpersist(const DevP *Ps, GPArgs g
     s.trace = nullptr;
     s.ntrace = 0;
     s.mode = 1;
+    s.onecl = 0;
     if (threadIdx.x == 0) sk = *P.ks;
     __syncthreads();
     const PGLev &H0 = a.lev[0];

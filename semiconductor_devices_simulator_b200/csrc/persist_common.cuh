@@ -11,6 +11,8 @@
 // decisions with no extra barrier.  Two alternating partial buffers keep a reduction from
 // overwriting partials another block may still be reading.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "device_common.cuh"
 
 namespace ss {
@@ -40,6 +42,8 @@ struct PS {
     int ntrace;                   //   last arrival, release seen by block 0 (globaltimer ns)
     int mode;                     // barrier form: 0 fences around the arrival and the wait,
                                   //   1 release-add / acquire-load
+    int onecl;                    // 1: the whole grid is one thread-block cluster, whose
+                                  //   hardware barrier replaces the grid barrier
 };
 
 // Grid-wide barrier: every block arrives (release), the block waits until every block
@@ -66,6 +70,10 @@ __device__ __forceinline__ int pg_poll(PS &s) {
 }
 __device__ __forceinline__ bool pg_sync(PS &s) {
     __shared__ int s_ok;
+    if (s.onecl) {                                 // one cluster: barrier.cluster (release / acquire)
+        cooperative_groups::this_cluster().sync();
+        return true;
+    }
     __syncthreads();
     s.target += gridDim.x;
     const int bn = (int)(s.target / gridDim.x) - 1;          // this barrier's number in the launch
