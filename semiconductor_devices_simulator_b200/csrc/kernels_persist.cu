@@ -846,6 +846,8 @@ int g_barmode = 1;         // grid-barrier form (SEMISIM_B200_BARMODE; 1 measure
 int g_clusters = 1;        // cluster launches (SEMISIM_B200_CLUSTERS=0: off)
 int g_csz = 8;             // CTAs per cluster (SEMISIM_B200_CSZ: 8 portable, 16 non-portable)
 int g_clevel = 1;          // first level the first cluster runs alone (SEMISIM_B200_CLEVEL)
+int g_coop = 1;            // cooperative launch attribute (SEMISIM_B200_COOP=0: plain launch of a
+                           //   grid within the co-resident capacity)
 
 template <class T, int KIND>
 const void *kfn() { return reinterpret_cast<const void *>(&k_persist<T, KIND>); }
@@ -897,6 +899,7 @@ int persist_enabled() {
         if (const char *m = std::getenv("SEMISIM_B200_CLUSTERS")) g_clusters = std::atoi(m) != 0;
         if (const char *m = std::getenv("SEMISIM_B200_CLEVEL")) g_clevel = std::atoi(m) < 1 ? 1 : std::atoi(m);
         if (const char *m = std::getenv("SEMISIM_B200_CSZ")) g_csz = std::atoi(m) == 16 ? 16 : 8;
+        if (const char *m = std::getenv("SEMISIM_B200_COOP")) g_coop = std::atoi(m) != 0;
         int dev = 0, coop = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
         if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess) cudaGetLastError();
@@ -982,7 +985,7 @@ static int persist_run(const Ctx &c, int Ls, size_t smem, const PArgs &a, PGrid 
     cfg.stream = c.st;
     cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeCooperative;
-    at[0].val.cooperative = 1;
+    at[0].val.cooperative = g_coop;
     at[1].id = cudaLaunchAttributeClusterDimension;
     at[1].val.clusterDim.x = aa.csz; at[1].val.clusterDim.y = 1; at[1].val.clusterDim.z = 1;
     cfg.attrs = at;
