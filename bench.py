@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--points", type=int, default=0,
                     help="points per sweep timed in a step (0: every point)")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuner)")
+    ap.add_argument("--share", default="gummel", choices=["gummel", "none"],
+                    help="grid shares of concurrently solved sweeps: by the first step's Gummel iterations, "
+                         "or none (every persistent solve takes the whole GPU)")
     ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "finfet", "graph_mosfet", "diodes64", "power_cell"],
                     help="nmosfet: the Id-Vg workload (default); finfet: the tri-gate FinFET Id-Vg family "
                          "(96x96x64, 5 drain biases); diodes64: the 64 pn-diode variants batch")
@@ -441,6 +444,32 @@ class Sweeper:
         self.wall = time.perf_counter() - t0
 
 
+def sm_count(dev):
+    import torch
+    return torch.cuda.get_device_properties(dev).multi_processor_count if torch.cuda.is_available() else 148
+
+
+def balance_shares(lib, ws, nsm, on=True):
+    """Split the GPU's co-resident blocks (one per SM) between concurrently solved sweeps in
+    proportion to the Gummel iterations each took in its last step, so that every sweep's
+    persistent solves run side by side with the others' (cooperative grids that together
+    exceed the SMs take turns).  `on` False removes the shares.  Returns the shares."""
+    if not on or len(ws) < 2:
+        for w in ws:
+            lib.api3b_use(w.h)
+            lib.api3b_set_share(0)
+        return [0] * len(ws)
+    g = [max(1, getattr(w, "gummel", 1) or 1) for w in ws]
+    lo = max(4, nsm // (4 * len(ws)))
+    sh = [max(lo, int(nsm * x / sum(g))) for x in g]
+    while sum(sh) > nsm and max(sh) > lo:                  # trim the largest to fit the SMs
+        sh[sh.index(max(sh))] -= 1
+    for w, b in zip(ws, sh):
+        lib.api3b_use(w.h)
+        lib.api3b_set_share(b)
+    return sh
+
+
 def concurrent(workers, fn):
     th = [threading.Thread(target=fn, args=(w,)) for w in workers]
     for t in th:
@@ -458,6 +487,22 @@ def rel_dI(cur, ref, on=1e-30):
             if abs(y) > max(f, on):
                 worst = max(worst, abs(x - y) / abs(y))
     return worst
+
+
+def worst_terminal(cur, ref):
+    """The terminal that sets rel_dI over a family {sweep: points}: its sweep, point and
+    contact, the reference current and floor, and the distance in units of the band
+    1e-4 |I_ref| + Iflr (at most 1 where the two agree to 1e-4 or to the round-off floor)."""
+    best, band = None, 0.0
+    for si in ref:
+        for q, ((I, _), (Ir, Fr)) in enumerate(zip(cur[si], ref[si])):
+            for c, (x, y, f) in enumerate(zip(I, Ir, Fr)):
+                if abs(y) > f:
+                    band = max(band, abs(x - y) / (1e-4 * abs(y) + f))
+                    r = abs(x - y) / abs(y)
+                    if best is None or r > best["rel"]:
+                        best = {"sweep": si, "point": q, "contact": c, "I_ref": y, "Iflr": f, "dI": abs(x - y), "rel": r}
+    return best, band
 
 
 # tight tolerances: inner solves to round-off, validate.py's Gummel tolerances
@@ -492,8 +537,10 @@ def tight_check(lib, workers, mesh):
             s.free()
         if conv != npts:
             return {"error": f"{npts - conv} of {npts} points did not converge at tight tolerances (precision {p})"}
+    worst, band = worst_terminal(res[1], res[0])
     return {"all_points": max(rel_dI(res[1][k], res[0][k]) for k in res[0]),
             "on_state_Id_gt_1nA": max(rel_dI(res[1][k], res[0][k], on=1e-9) for k in res[0]),
+            "worst_terminal": worst, "max_dI_over_band": band,
             "points": sum(len(v) for v in res[0].values()), "seconds": round(time.perf_counter() - t0, 1),
             "solver": list(TIGHT_SOLVER), "env": TIGHT_ENV,
             "note": "refined vs FP64, both converged tightly, every point of the step, terminals above their "
@@ -625,8 +672,12 @@ def run_b200(a, dist):
         lib.api3b_tune_get(ctypes.byref(r), ctypes.byref(g), ctypes.byref(sm), ctypes.byref(zc))
         tune = {"rows_per_block": r.value, "row_blocks_max": zc.value, "grid_cap": g.value,
                 "small_level_nodes": sm.value or 2048, "vcycle_us": round(us, 2)}
+    nsm = sm_count(dist.local)
+    shares = []
     for i in range(a.warmup):
         step(workers)
+        if i == 0:                            # grid shares from the first step's Gummel counts
+            shares = balance_shares(lib, workers, nsm, on=a.share == "gummel")
     w = workers[0].w
     clocks = Clocks(dist.local)
     clocks.start()
@@ -669,6 +720,7 @@ def run_b200(a, dist):
     if prec == 1 and not a.no_fp64:
         w64 = make(0)
         step(w64)
+        balance_shares(lib, w64, nsm, on=a.share == "gummel")
         f_pts = s_pts = 0
         f_dev = s_dev = 0.0
         for i in range(a.steps):
@@ -676,6 +728,7 @@ def run_b200(a, dist):
             f_pts += npts; f_dev += dev_s
         cur64 = {s.si: list(s.cur) for s in w64}
         per_rank = len(sweep_order(nsw, 0, dist.world, replicate))   # the most sweeps a rank holds
+        balance_shares(lib, w64, nsm, on=False)                      # one at a time: the whole GPU
         for i in range(a.steps):
             for q in range(per_rank):
                 if q < len(w64):
@@ -738,6 +791,9 @@ def run_b200(a, dist):
                             "nodes": w.N, "points_per_step": npts_step}, **workload_config(w),
                            **{"solver": list(D.GUI_SOLVER), "precision": "fp64" if graph else a.precision,
                               "launch_shapes": tune,
+                              "linear_solves": ("persistent (one cooperative launch per solve)"
+                                                if lib.api3b_set_persist(-1, -1) else "per-pass graphs"),
+                              "grid_shares": shares or None,
                               "parallelism": (f"replicas{dist.world}, {nsw} concurrent sweeps per GPU "
                                               "(instance + stream each)") if replicate else
                                              (f"sweeps split over {dist.world} GPU(s) by node count, concurrent "

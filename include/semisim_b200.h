@@ -254,6 +254,16 @@ int api3b_get_precision(void);
    previous mode. */
 int api3b_set_persist(int mode, int blocks);
 
+/* No counterpart in the reference.  Grid share of the current instance's persistent solves:
+   blocks > 0 caps each of its launches at that many blocks (below the library-wide cap of
+   api3b_set_persist), 0 removes the share, -1 only reads it.  Instances solved at the same
+   time from several host threads run side by side when their shares add up to at most
+   the GPU's co-resident blocks (one per SM); otherwise their cooperative launches take
+   turns.  A share changes only the launch shape, never the stop rules; the grid
+   reductions' order follows the block count, so results are reproducible per share.
+   Returns the previous share. */
+int api3b_set_share(int blocks);
+
 /* No counterpart in the reference (it has no learned component).  Learned sweep predictor
    of the current instance: a per-node MLP (48 features -> 3 x 128 SiLU -> 3, BF16 weights,
    FP32 accumulation) corrects the sweep predictor's linear extrapolation

@@ -82,6 +82,10 @@ int b200x_persist_probe(int nb, double wait_s, int *gave_up);
    block's arrival and the release as block 0 saw it (globaltimer ns) - disarms it and
    returns 1 when a launch filled it, with that launch's blocks in *blocks. */
 int b200x_persist_trace(int n, unsigned long long *out, int *blocks);
+/* Block cap of the persistent solves that the calling host thread launches (measurement
+   hook): n > 0 caps the grid at n blocks, 0 removes the cap, n < 0 only reads it.  Returns
+   the previous cap. */
+int b200x_persist_tblocks(int n);
 /* floating-block balance of a continuity solution (in place) */
 int b200x_float_fix(int hole, double *sol);
 /* learned predictor on the present history arrays (22-24 h1, 25-27 e2 of b200x_set /

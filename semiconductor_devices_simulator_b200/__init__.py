@@ -50,6 +50,7 @@ HOOKS = {
     "b200x_pcg": (_I, [_I, _D, _DP]),
     "b200x_persist_probe": (_I, [_I, _D, _IP]),
     "b200x_persist_trace": (_I, [_I, ctypes.POINTER(ctypes.c_ulonglong), _IP]),
+    "b200x_persist_tblocks": (_I, [_I]),
     "b200x_float_fix": (_I, [_I, _DP]),
     "b200x_device_bytes": (_LL, []),
     "b200x_stream_timer": (_D, [_I]),

@@ -777,6 +777,13 @@ int api3b_set_persist(int mode, int blocks) {
     persist_set(mode, blocks);
     return old;
 }
+// grid share (blocks) of the current instance's persistent solves, 0 for none; -1 reads.
+// Returns the previous share.
+int api3b_set_share(int blocks) {
+    const int old = g_dev.pblocks;
+    if (blocks >= 0) g_dev.pblocks = blocks;
+    return old;
+}
 // precision in effect on the current instance (0 FP64, 1 refined FP32)
 int api3b_get_precision(void) { return use_mixed(g_dev); }
 int api3b_free(int h) {

@@ -434,6 +434,7 @@ int persist_graph(Inst &d, int kind, int maxit, double rtol, double atol, const 
     if (want < nb) nb = want < 4 ? 4 : want;
     const int cap = persist_get_blocks();
     if (cap > 0 && cap < nb) nb = cap;
+    if (d.pblocks > 0 && d.pblocks < nb) nb = d.pblocks;
     if (nb > PG_MAXB) nb = PG_MAXB;
     if (nb < 1) return 0;
     Ctx c = make_ctx(d);

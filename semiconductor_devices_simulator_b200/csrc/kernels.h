@@ -31,6 +31,7 @@ struct Ctx {
     int zcap = 65535;           // most row blocks of one pass (more rows per thread beyond it)
     int rq = 1;                 // coarse rows per block of the residual + restriction pass
     int small_nodes = 0;        // levels at or below this size go to the small-level kernel (0: default)
+    int pblocks = 0;            // blocks of the instance's persistent solves (0: the library-wide cap)
     int nodes_blocks() const;
 };
 

@@ -648,7 +648,7 @@ constexpr size_t PG_SETUP_SMEM = sizeof(double) * COARSE_MAX * (COARSE_MAX + 1) 
 // FP64 sol when it converged).  PK_BICG (T = double): the continuity system from the
 // present sol.  PK_REFINED (T = float): FP64 refinement steps around FP32 BiCGSTAB.
 template <class T, int KIND>
-__global__ void __launch_bounds__(PG_TPB, 1) k_persist(const DevP *Ps, PArgs a) {
+__global__ void __launch_bounds__(PG_TPB, 1024 / PG_TPB) k_persist(const DevP *Ps, PArgs a) {
     const DevP &P = Ps[0];
     extern __shared__ __align__(16) unsigned char sraw[];
     __shared__ LevView<T> sv[MAXLEV];
@@ -836,6 +836,7 @@ struct KInfo {
 std::mutex g_pmu;
 int g_persist_mode = -1;   // -1 unread, 0 off, 1 on
 int g_persist_blocks = 0;  // blocks per launch (0: every SM's worth)
+thread_local int t_persist_blocks = 0;  // this host thread's cap (0: none)
 bool g_persist_broken = false;
 bool g_coop_ok = false;    // the device supports cooperative launches
 unsigned long long *g_trace = nullptr;   // armed barrier timeline (test hook): device buffer
@@ -843,7 +844,7 @@ int g_trace_n = 0, g_trace_used = 0;     // its barriers; 1 once a launch has fi
 int g_last_blocks = 0;                   // blocks of the last persistent launch
 int g_fuse_up = 1;         // deferred prolongation on the way up (SEMISIM_B200_FUSEUP=0: off)
 int g_barmode = 1;         // grid-barrier form (SEMISIM_B200_BARMODE; 1 measured faster than 0)
-int g_clusters = 1;        // cluster launches (SEMISIM_B200_CLUSTERS=0: off)
+int g_clusters = 1;        // cluster launches: 0 off, 1 grids of one cluster, 2 every grid (SEMISIM_B200_CLUSTERS)
 int g_csz = 8;             // CTAs per cluster (SEMISIM_B200_CSZ: 8 portable, 16 non-portable)
 int g_clevel = 1;          // first level the first cluster runs alone (SEMISIM_B200_CLEVEL)
 int g_coop = 1;            // cooperative launch attribute (SEMISIM_B200_COOP=0: plain launch of a
@@ -896,7 +897,7 @@ int persist_enabled() {
         if (const char *b = std::getenv("SEMISIM_B200_PBLOCKS")) g_persist_blocks = std::atoi(b);
         if (const char *f = std::getenv("SEMISIM_B200_FUSEUP")) g_fuse_up = std::atoi(f) != 0;
         if (const char *m = std::getenv("SEMISIM_B200_BARMODE")) g_barmode = std::atoi(m) ? 1 : 0;
-        if (const char *m = std::getenv("SEMISIM_B200_CLUSTERS")) g_clusters = std::atoi(m) != 0;
+        if (const char *m = std::getenv("SEMISIM_B200_CLUSTERS")) g_clusters = std::atoi(m) < 0 ? 0 : (std::atoi(m) > 2 ? 2 : std::atoi(m));
         if (const char *m = std::getenv("SEMISIM_B200_CLEVEL")) g_clevel = std::atoi(m) < 1 ? 1 : std::atoi(m);
         if (const char *m = std::getenv("SEMISIM_B200_CSZ")) g_csz = std::atoi(m) == 16 ? 16 : 8;
         if (const char *m = std::getenv("SEMISIM_B200_COOP")) g_coop = std::atoi(m) != 0;
@@ -914,6 +915,11 @@ void persist_set(int mode, int blocks) {
     if (blocks >= 0) g_persist_blocks = blocks;
 }
 int persist_get_blocks() { return g_persist_blocks; }
+int persist_thread_blocks(int n) {
+    const int old = t_persist_blocks;
+    if (n >= 0) t_persist_blocks = n;
+    return old;
+}
 
 // Launch the persistent solve `kind` of precision T on instance 0 of the context.  Returns
 // 1 when it ran (results in the Krylov records), 0 when the persistent path does not apply
@@ -941,11 +947,16 @@ static int persist_run(const Ctx &c, int Ls, size_t smem, const PArgs &a, PGrid 
     const int want = (c.maxN + 2 * PG_TPB - 1) / (2 * PG_TPB);
     if (want < nb) nb = want < 4 ? 4 : want;
     if (g_persist_blocks > 0 && g_persist_blocks < nb) nb = g_persist_blocks;
+    if (c.pblocks > 0 && c.pblocks < nb) nb = c.pblocks;
+    if (t_persist_blocks > 0 && t_persist_blocks < nb) nb = t_persist_blocks;
     if (nb > PG_MAXB) nb = PG_MAXB;
     if (nb < 1) return 0;
-    // clusters of 16 CTAs: a grid of at most 16 blocks becomes one cluster (every barrier a
-    // cluster barrier); a larger grid is a whole number of clusters, the first of which runs
-    // the coarse levels from Lc on alone
+    // clusters of g_csz CTAs: a grid of at most g_csz blocks becomes one cluster (every
+    // barrier a cluster barrier, 0.3 us against 2 us for a grid barrier).  With g_clusters 2 a
+    // larger grid is a whole number of clusters, the first of which runs the coarse levels
+    // from Lc on alone; that costs the grid the SMs that no whole cluster covers (112 - 120
+    // of 148 blocks), which a full-size solve loses more time to than the coarse levels gain,
+    // so by default larger grids launch without clusters
     PArgs aa = a;
     aa.csz = 0;
     aa.onecl = 0;
@@ -955,7 +966,7 @@ static int persist_run(const Ctx &c, int Ls, size_t smem, const PArgs &a, PGrid 
             nb = g_csz;
             aa.csz = g_csz;
             aa.onecl = 1;
-        } else {
+        } else if (g_clusters == 2) {
             int ncl = nb / g_csz;
             if (ncl > ki.clusters) ncl = ki.clusters;
             nb = ncl * g_csz;

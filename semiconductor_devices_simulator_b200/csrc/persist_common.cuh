@@ -17,7 +17,10 @@
 
 namespace ss {
 
-constexpr int PG_TPB = 1024;
+#ifndef PG_TPB_SET
+#define PG_TPB_SET 1024
+#endif
+constexpr int PG_TPB = PG_TPB_SET;
 constexpr unsigned long long PG_WAIT_NS = 2000000000ull;    // longest barrier wait of a solve (2 s)
 
 __device__ __forceinline__ unsigned long long pg_clock() {

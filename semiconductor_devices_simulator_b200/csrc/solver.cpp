@@ -66,6 +66,7 @@ Ctx make_ctx(Inst &d) {
     c.small_nodes = d.tune.small_nodes;
     c.zcap = d.tune.zcap;
     c.rq = d.tune.rq;
+    c.pblocks = d.pblocks;
     return c;
 }
 

@@ -151,6 +151,7 @@ struct Inst {
     int precision = -1;               // linear solves: 0 FP64, 1 FP32 refined in FP64, -1 library default
     long long ir_steps = 0, ir_fallbacks = 0;
     Tune tune;
+    int pblocks = 0;             // grid share of its persistent solves (api3b_set_share; 0: none)
     unsigned long long upload_gen = 0;      // set-up upload this instance's device holds (prepare)
     const Inst *clone_src = nullptr;        // batched-resolve worker: the instance and upload
     unsigned long long clone_gen = 0;       //   generation its set-up was copied from
@@ -265,6 +266,7 @@ int pcg_solve(const Ctx &c, const MGHost &mg, int maxit, double rtol, int check_
 int persist_enabled();
 void persist_set(int mode, int blocks);
 int persist_get_blocks();
+int persist_thread_blocks(int n);
 int persist_pcg(const Ctx &c, const MGHost &mg, int mixed);
 int persist_bicg(const Ctx &c, const MGHost &mg, double rtol, double atol, int qsign);
 int persist_refined(const Ctx &c, const MGHost &mg, int maxsteps, int *steps, int qsign);

@@ -266,6 +266,9 @@ int b200x_persist_probe(int nb, double wait_s, int *gave_up) {
 // barrier timeline of the next persistent solve: n > 0 arms it, n == 0 reads it (3 n
 // values per barrier: first arrival, last arrival, release; ns) and the launch's blocks
 int b200x_persist_trace(int n, unsigned long long *out, int *blocks) { return persist_trace(n, out, blocks); }
+// block cap of the persistent solves launched from the calling host thread (n >= 0 sets it,
+// 0 removes it); returns the previous cap
+int b200x_persist_tblocks(int n) { return persist_thread_blocks(n); }
 // PCG on the Poisson system now in A / rhs from sol = 0
 int b200x_pcg(int maxit, double rtol, double *sol) {
     Inst &d = *dev();

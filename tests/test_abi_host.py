@@ -83,6 +83,14 @@ def test_instances_are_independent(lib):
         assert lib.api3_get_Nx() == 6 and lib.api3_get_ncon() == 2
         assert lib.api3b_use(0) == 1 and lib.api3b_current() == 0
         assert lib.api3b_use(9999) == 0
+        # grid shares of the persistent solves belong to the instance
+        lib.api3b_use(h1)
+        assert lib.api3b_set_share(40) == 0
+        lib.api3b_use(h2)
+        assert lib.api3b_set_share(-1) == 0 and lib.api3b_set_share(100) == 0
+        lib.api3b_use(h1)
+        assert lib.api3b_set_share(-1) == 40 and lib.api3b_set_share(0) == 40
+        assert lib.api3b_set_share(-1) == 0
     finally:
         lib.api3b_use(0)
         assert lib.api3b_free(h1) == 1 and lib.api3b_free(h2) == 1
