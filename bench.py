@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--points", type=int, default=0,
                     help="points per sweep timed in a step (0: every point)")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuner)")
+    ap.add_argument("--predictor", default="quadratic", choices=["quadratic", "secant"],
+                    help="sweep predictor of the timed steps: quadratic through the last three points (default) "
+                         "or the reference's secant step; the other one is timed on one more step")
     ap.add_argument("--share", default="gummel", choices=["gummel", "none"],
                     help="grid shares of concurrently solved sweeps: by the first step's Gummel iterations, "
                          "or none (every persistent solve takes the whole GPU)")
@@ -111,9 +114,18 @@ def run_probe(a):
     its = lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
     solve_ms = lib.b200x_stream_timer(1)
     lib.b200x_cont_assemble(0, None, None, None, None)      # the same solve again, warm
+    nk = lib.b200x_prof(1)                                  # with its algorithmic bytes per class
     lib.b200x_stream_timer(0)
     lib.b200x_bicgstab(a.probe, 1e-12, 0.0, 1, None, None, abi.dptr(rn), abi.dptr(r0))
     solve_ms2 = lib.b200x_stream_timer(1)
+    lib.b200x_prof(0)
+    alg = {}
+    for k in range(nk):
+        ms, cnt, by = (np.zeros(1) for _ in range(3))
+        lib.b200x_prof_read(k, abi.dptr(ms), abi.dptr(cnt), abi.dptr(by))
+        if cnt[0] > 0:
+            alg[lib.b200x_prof_name(k).decode()] = {"launches": int(cnt[0]), "bytes": float(by[0]),
+                                                    "ms": round(float(ms[0]), 4)}
     timeline = None
     if a.trace:                                             # barrier timeline of one more (warm) solve
         nb = 4096
@@ -153,6 +165,7 @@ def run_probe(a):
                       "precision": a.precision, "seed_kernel": seed_ok, "seed_ms": round(seed_ms, 4),
                       "bicgstab_its": its, "r0": r0[0], "rn": rn[0], "solve_ms": [round(solve_ms, 3), round(solve_ms2, 3)],
                       "persistent": bool(lib.api3b_set_persist(-1, -1)), "timeline": timeline,
+                      "warm_solve_classes": alg,
                       "launches": int(lib.b200x_launches() - l0)}))
 
 
@@ -354,10 +367,11 @@ def sweep_points(lib, w, s, fields=False, npts=None, out=None):
     return len(V), conv
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a kernel class on
-# the default 120x80x60 mesh, measured by one ncu capture of the bench's --probe case (the
-# launch mix of one V-cycle weighted by its level-0/1/2 passes)
-NCU_TRAFFIC = {"smooth_black_f32": 10.9e6}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of a kernel
+# class on the default 120x80x60 mesh, from one ncu capture of the bench's --probe 10 case:
+# the persistent refined solve (k_persist<float, 2>, 10 BiCGSTAB iterations) moved 433.2 MB
+# of DRAM traffic for 4516 MB of algorithmic bytes (its hierarchy stays resident in the L2)
+NCU_DRAM_PER_ALG = {"persistent_solve_f32": 433.16e6 / 4516.1e6}
 
 
 def peaks():
@@ -578,11 +592,13 @@ def gummel_floor(lib, workers):
     return tot, pts
 
 
-def learned_step(a, lib, workers, step, cur, gummel_per_step, dist):
+def learned_step(a, lib, workers, step, cur, gummel_per_step, dist, gummel_other=None, order=1):
     """Train the learned predictor on the workload device's own sweeps at gate voltages
     shifted by half a step (both drain biases), then run one step of the workload with
-    it.  Returns the measured block (Gummel iterations of one step with the linear guess,
-    `gummel_per_step`, and with the learned one; points/s)."""
+    it (it corrects the secant guess at the first continuation step of each point).
+    Returns the measured block: Gummel iterations of one step with the headline predictor
+    (`gummel_per_step`, of order `order`), with the other plain predictor
+    (`gummel_other`), with the learned seed and from converged starts; points/s."""
     if not workers:                             # this rank holds no sweep: keep the collective steps
         dist.barrier()
         return None
@@ -622,18 +638,19 @@ def learned_step(a, lib, workers, step, cur, gummel_per_step, dist):
     curl = {s.si: list(s.cur) for s in workers}
     floor, fpts = gummel_floor(lib, workers)
     return {"points_per_s": round(pts / dev, 4), "unit": UNIT,
-            "gummel_iterations_per_step": {"linear_guess": gummel_per_step,
+            "gummel_iterations_per_step": {("quadratic_guess" if order == 2 else "secant_guess"): gummel_per_step,
+                                           ("secant_guess" if order == 2 else "quadratic_guess"): gummel_other,
                                            "learned_guess": sum(s.gummel for s in workers),
                                            "converged_start_floor": int(floor)},
             "floor_note": f"Gummel iterations of the same {fpts} points when each starts from its own converged "
                           "solution (api3_set_state at its bias): the least any seed can reach under the "
                           "acceptance test",
             "seeded_steps": int(sum(u[0] for u in used)), "fallbacks": int(sum(u[1] for u in used)),
-            "max_rel_dI_vs_linear_on_state": max(rel_dI(curl[k], cur[k], on=1e-9) for k in cur),
+            "max_rel_dI_vs_headline_on_state": max(rel_dI(curl[k], cur[k], on=1e-9) for k in cur),
             "train": {"rows": int(sum(f.shape[0] for f in feats)), "steps": 6000, "seconds": round(tr.seconds, 2),
                       "data_seconds": round(t_data, 1)},
-            "note": "not in `value`: at this 0.05 V step the Gummel iteration count is set by the loop's "
-                    "convergence tail, not by the starting guess"}
+            "note": "not in `value`: the seed corrects the secant guess and saves no Gummel iterations "
+                    "against it; the converged-start floor shows how many a perfect seed would save"}
 
 
 def run_b200(a, dist):
@@ -641,6 +658,8 @@ def run_b200(a, dist):
     mesh = mesh_of(a)
     lib = S.load()
     lib.b200x_set_device(dist.local)
+    order = 2 if a.predictor == "quadratic" else 1
+    lib.api3b_set_pred_order(order)
     nsw = {"finfet": 5, "power_cell": 16}.get(WL, 2)   # the sweeps of the workload, one instance each
     graph = WL.startswith("graph")
     prec = 1 if a.precision == "refined" and not graph else 0
@@ -701,8 +720,8 @@ def run_b200(a, dist):
         e_pts, e_wall = tot_pts, tot_wall
     # roofline: one more step with every launch timed by CUDA events on the solver stream
     prof = None
-    if not a.no_profile and workers:          # event timing is per thread: one sweep alone
-        s0 = workers[0]
+    if not a.no_profile and workers:          # event timing is per thread: one sweep alone,
+        s0 = max(workers, key=lambda s: s.gummel)   # the step's longest (with its grid share)
         s0.prepare()
         nk = lib.b200x_prof(1)
         s0.run(False)
@@ -729,6 +748,7 @@ def run_b200(a, dist):
         cur64 = {s.si: list(s.cur) for s in w64}
         per_rank = len(sweep_order(nsw, 0, dist.world, replicate))   # the most sweeps a rank holds
         balance_shares(lib, w64, nsm, on=False)                      # one at a time: the whole GPU
+        lib.api3b_set_pred_order(1)                                  # and the reference's secant step
         for i in range(a.steps):
             for q in range(per_rank):
                 if q < len(w64):
@@ -742,11 +762,28 @@ def run_b200(a, dist):
                dist.max(max([rel_dI(cur[k], cur64[k], on=1e-9) for k in cur] or [0.0])))
         for s in w64:
             s.free()
+        lib.api3b_set_pred_order(order)
+    # the other sweep predictor on one more step of the same instances (same grid shares)
+    other = None
+    if not graph:                             # every rank takes the step's collectives
+        lib.api3b_set_pred_order(3 - order)
+        npts, conv, dev_s, wall = step(workers)
+        lib.api3b_set_pred_order(order)
+        curo = {s.si: list(s.cur) for s in workers}
+        band = worst_terminal(curo, cur)[1] if workers else 0.0
+        other = {"predictor": "secant" if order == 2 else "quadratic",
+                 "points_per_s": round(dist.sum(npts) / max(dist.max(dev_s), 1e-9), 4), "unit": UNIT,
+                 "gummel_iterations_per_step": sum(s.gummel for s in workers),
+                 "max_rel_dI_vs_headline": {
+                     "all_points": dist.max(max([rel_dI(curo[k], cur[k]) for k in cur] or [0.0])),
+                     "on_state_Id_gt_1nA": dist.max(max([rel_dI(curo[k], cur[k], on=1e-9) for k in cur] or [0.0])),
+                     "max_dI_over_band": dist.max(band)}}
     # the learned predictor: trained (untimed) on this device's own solutions at gate
     # voltages half a step off the workload's, then one step of the workload seeded by it
     learned = None
     if not a.no_learned and not graph:
-        learned = learned_step(a, lib, workers, step, cur, gummel, dist)
+        learned = learned_step(a, lib, workers, step, cur, gummel, dist,
+                               other["gummel_iterations_per_step"] if other else None, order)
     tight = None
     if prec == 1 and not a.no_fp64 and not a.no_tight and workers:
         tight = tight_check(lib, workers, mesh)
@@ -769,11 +806,18 @@ def run_b200(a, dist):
             tot_ms = sum(r[1] for r in prof) or 1.0
             top = max(prof, key=lambda r: r[1])
             ach = top[3] / (top[1] / 1e3) / 1e9 if top[1] > 0 else 0.0
-            traffic = NCU_TRAFFIC.get(top[0]) if (WL, mesh) == ("nmosfet", (120, 80, 60)) else None
+            ratio = NCU_DRAM_PER_ALG.get(top[0]) if (WL, mesh) == ("nmosfet", (120, 80, 60)) else None
+            traffic = round(ratio * top[3] / max(top[2], 1)) if ratio else None
             roof = {"bound": "hbm", "kernel": top[0], "achieved": round(ach, 1), "peak": hbm,
                     "peak_kind": pk_kind, "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": traffic,
                     "launches": top[2], "avg_launch_us": round(1e3 * top[1] / max(top[2], 1), 2),
-                    "bytes_per_launch": round(top[3] / max(top[2], 1))}
+                    "bytes_per_launch": round(top[3] / max(top[2], 1)),
+                    "traffic_source": ("ncu DRAM bytes per algorithmic byte of this class on the probe case, "
+                                       "times this run's algorithmic bytes per launch") if traffic else None,
+                    "note": ("one cooperative launch per linear solve: its multigrid hierarchy and Krylov vectors "
+                             "stay in the 126 MB L2 (DRAM traffic about a tenth of the algorithmic bytes); "
+                             "the time goes to the grid barriers between dependent passes")
+                            if top[0].startswith("persistent") else None}
             kernels = {r[0]: {"ms": round(r[1], 2), "share": round(r[1] / tot_ms, 4), "launches": r[2],
                               "GBps": round(r[3] / (r[1] / 1e3) / 1e9, 1) if r[1] > 0 else 0.0}
                        for r in sorted(prof, key=lambda r: -r[1]) if r[2] > 0}
@@ -791,6 +835,8 @@ def run_b200(a, dist):
                             "nodes": w.N, "points_per_step": npts_step}, **workload_config(w),
                            **{"solver": list(D.GUI_SOLVER), "precision": "fp64" if graph else a.precision,
                               "launch_shapes": tune,
+                              "sweep_predictor": ("quadratic through the last three points"
+                                                  if order == 2 else "secant (the reference's)"),
                               "linear_solves": ("persistent (one cooperative launch per solve)"
                                                 if lib.api3b_set_persist(-1, -1) else "per-pass graphs"),
                               "grid_shares": shares or None,
@@ -826,6 +872,8 @@ def run_b200(a, dist):
             out["max_rel_dI_vs_fp64_tight"] = tight
         if batch:
             out["diodes64"] = batch
+        if other:
+            out["other_predictor"] = other
         if learned:
             out["learned_seed"] = learned
         if dist.world == 1 and not a.no_cpu_baseline and WL != "power_cell":   # 8.4M nodes: hours on the host

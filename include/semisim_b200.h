@@ -264,6 +264,15 @@ int api3b_set_persist(int mode, int blocks);
    Returns the previous share. */
 int api3b_set_share(int blocks);
 
+/* No counterpart in the reference.  Order of the sweep predictor (library-wide): 1 (the
+   default; the reference's secant step x1 + s (x1 - x0) from the last two sweep points) or 2
+   (quadratic: the Lagrange polynomial through the last three sweep points' solutions,
+   evaluated at the new bias; used when the three biases and the new one lie on one line,
+   else the secant step).  It only sets the Gummel loop's starting point; the stop rules are
+   the same.  SEMISIM_B200_PRED_ORDER sets it at api3_init.  Other values only read it.
+   Returns the previous order. */
+int api3b_set_pred_order(int order);
+
 /* No counterpart in the reference (it has no learned component).  Learned sweep predictor
    of the current instance: a per-node MLP (48 features -> 3 x 128 SiLU -> 3, BF16 weights,
    FP32 accumulation) corrects the sweep predictor's linear extrapolation

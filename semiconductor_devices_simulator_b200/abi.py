@@ -123,6 +123,7 @@ EXTRA = {
     "api3b_get_precision": (_I, []),
     "api3b_set_persist": (_I, [_I, _I]),
     "api3b_set_share": (_I, [_I]),
+    "api3b_set_pred_order": (_I, [_I]),
     # learned sweep predictor of the current instance
     "api3b_seed_set_model": (_I, [ctypes.POINTER(ctypes.c_float), _I]),
     "api3b_seed_enable": (_I, [_I]),

@@ -143,6 +143,7 @@ void api3_init(void) {                                      // semiconductor_3d.
     if (const char *m = env_get("SEMISIM_GBETA")) g_knobs.gbeta = std::atof(m);
     if (const char *m = env_get("SEMISIM_AAM")) { int q = std::atoi(m); g_knobs.aa_depth = q < 0 ? 0 : (q > AA_MAX ? AA_MAX : q); }
     if (const char *m = env_get("SEMISIM_PRED")) g_knobs.pred_on = std::atoi(m) != 0;
+    if (const char *m = env_get("SEMISIM_B200_PRED_ORDER")) g_knobs.pred_order = std::atoi(m) >= 2 ? 2 : 1;
     if (const char *m = env_get("SEMISIM_GROW")) { const double gg = std::atof(m); if (gg >= 1. && gg <= 4.) g_knobs.grow_slow = gg; }
     if (const char *m = env_get("SEMISIM_CATOL")) g_knobs.cont_atol = std::atof(m);
     if (const char *m = env_get("SEMISIM_QFM")) g_knobs.qf_margin = std::atof(m);
@@ -775,6 +776,13 @@ int api3b_set_precision(int mode) {
 int api3b_set_persist(int mode, int blocks) {
     const int old = persist_enabled();
     persist_set(mode, blocks);
+    return old;
+}
+// order of the sweep predictor (1 secant, 2 quadratic), library-wide; other values read.
+// Returns the previous order.
+int api3b_set_pred_order(int order) {
+    const int old = g_knobs.pred_order;
+    if (order == 1 || order == 2) g_knobs.pred_order = order;
     return old;
 }
 // grid share (blocks) of the current instance's persistent solves, 0 for none; -1 reads.

@@ -58,6 +58,7 @@ void launch_region_seed(const Ctx &c, int c1, int *mark);
 void launch_region_shift(const Ctx &c, int c1, double dV, const int *mark);
 void launch_face_J(const Ctx &c, int ax, int carrier, double *out);
 void launch_extrap(const Ctx &c, double r, int s1, int s2);     // history selectors 0 h1, 1 h2, 2 e2
+void launch_extrap3(const Ctx &c, double w1, double w2, double w3);   // w1 h1 + w2 e2 + w3 e3
 void launch_region_mark(const Ctx &c, int con1, int type, double dV, int *mark, int *changed);
 void launch_floating_blocks(const Ctx &c, int hole, int *nblocks);
 

@@ -787,6 +787,18 @@ __global__ void k_extrap(const DevP *__restrict__ Ps, double r, int s1, int s2) 
 void launch_extrap(const Ctx &c, double r, int s1, int s2) {
     SS_LAUNCH(PF_VEC, c.maxN, k_extrap, grid_of(c), TPB, c.st, c.dP, r, s1, s2);
 }
+// quadratic sweep predictor: the Lagrange weights of the last three sweep points' solutions
+__global__ void k_extrap3(const DevP *__restrict__ Ps, double w1, double w2, double w3) {
+    const DevP &P = Ps[blockIdx.y];
+    double *dst[3] = {P.phi, P.phin, P.phip};
+    SS_GRID_LOOP(k, P.N) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) dst[a][k] = w1 * P.h1[a][k] + w2 * P.e2[a][k] + w3 * P.e3[a][k];
+    }
+}
+void launch_extrap3(const Ctx &c, double w1, double w2, double w3) {
+    SS_LAUNCH(PF_VEC, c.maxN, k_extrap3, grid_of(c), TPB, c.st, c.dP, w1, w2, w3);
+}
 
 // ---- region shift (semiconductor_3d.c:3956-3987): flood fill of the quasi-neutral
 // region attached to an ohmic contact, by line sweeps along x, y, z until nothing

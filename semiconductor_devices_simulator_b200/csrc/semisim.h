@@ -162,7 +162,7 @@ struct DevP {
     double *wk[8];                // Krylov work vectors
     double *qn0, *qp0, *dqn, *dqp, *xk, *tr;
     double *Jx, *Jy, *Jz, *Rt;    // display current density and recombination
-    double *h1[3], *h2[3], *e2[3];
+    double *h1[3], *h2[3], *e2[3], *e3[3];   // path states; the last two sweep points' solutions
     // Anderson
     float *aaF, *aaG;             // AA_MAX slots of 3N each
     double *aaf, *aag;            // 3N each

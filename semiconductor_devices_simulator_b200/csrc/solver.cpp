@@ -114,6 +114,7 @@ static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &lev
     P.dqp = cv.take<double>(N); P.xk = cv.take<double>(N); P.tr = cv.take<double>(N);
     P.Jx = cv.take<double>(N); P.Jy = cv.take<double>(N); P.Jz = cv.take<double>(N); P.Rt = cv.take<double>(N);
     for (int a = 0; a < 3; a++) { P.h1[a] = cv.take<double>(N); P.h2[a] = cv.take<double>(N); P.e2[a] = cv.take<double>(N); }
+    for (int a = 0; a < 3; a++) P.e3[a] = cv.take<double>(N);
     P.aaF = cv.take<float>((size_t)AA_MAX * 3 * N);
     P.aaG = cv.take<float>((size_t)AA_MAX * 3 * N);
     P.aaf = cv.take<double>(3 * N); P.aag = cv.take<double>(3 * N);
@@ -1845,6 +1846,23 @@ static int cont_path(Inst &d) {
             if (r >= -2. && r <= 3. && std::fabs(r) > 1e-12 && err <= 1e-9 + 1e-6 * span) rx = r;
         }
     }
+    // quadratic predictor (not in the reference): the point before the last on the same
+    // line, Ve3 = Ve2 - r3 (Vf - Ve2); positions in units of the last step: Ve3 at -1 - r3,
+    // Ve2 at -1, Vf at 0
+    double r3 = 0.;
+    if (rx != 0. && g_knobs.pred_order >= 2 && d.e_n >= 2) {
+        double num = 0., den = 0., err = 0.;
+        for (int q = 0; q < nc; q++) {
+            const double b = Vf[q] - d.Ve2[q], e = d.Ve2[q] - d.Ve3[q];
+            num += e * b; den += b * b;
+        }
+        if (den > 0.) {
+            const double r = num / den;
+            for (int q = 0; q < nc; q++)
+                err = std::fmax(err, std::fabs((d.Ve2[q] - d.Ve3[q]) - r * (Vf[q] - d.Ve2[q])));
+            if (r >= 0.2 && r <= 5. && err <= 1e-9 + 1e-6 * span) r3 = r;
+        }
+    }
     int first = 1, noseed = 0;
     double t = 0., tp = -1., dt = span > 0. ? std::fmin(1., 0.1 / span) : 1.;
     int ok_all = 0, its = 0, steps = 0;
@@ -1864,6 +1882,10 @@ static int cont_path(Inst &d) {
             for (int q = 0; q < nc && q < 4; q++) dvs[q] = Va[q] - Vf[q];
             launch_mlp_seed(d, tn * rx, dvs);
             seeded = 1;
+        } else if (rx != 0. && r3 != 0.) {
+            const double s = tn * rx, s1 = -1., s0 = -1. - r3;      // Lagrange weights at s
+            launch_extrap3(c, (s - s1) * (s - s0) / (s1 * s0), s * (s - s0) / (s1 * (s1 - s0)),
+                           s * (s - s1) / (s0 * (s0 - s1)));
         } else if (rx != 0.) {
             launch_extrap(c, tn * rx, 0, 2);
         } else {
@@ -1885,6 +1907,7 @@ static int cont_path(Inst &d) {
         }
         if (seeded) d.seed_used++;
         if (first) {                               // the path's start (h1 until the first accepted step)
+            for (int a = 0; a < 3; a++) copy_dev(d, d.g.h.e3[a], d.g.h.e2[a]);
             for (int a = 0; a < 3; a++) copy_dev(d, d.g.h.e2[a], d.g.h.h1[a]);
             first = 0;
         }
@@ -1910,7 +1933,7 @@ static int cont_path(Inst &d) {
         }
     }
     if (ok_all && span > 0.) {
-        for (int q = 0; q < nc; q++) { d.Ve2[q] = Vf[q]; d.Ve1[q] = Vt[q]; }
+        for (int q = 0; q < nc; q++) { d.Ve3[q] = d.Ve2[q]; d.Ve2[q] = Vf[q]; d.Ve1[q] = Vt[q]; }
         d.e_n = d.e_n < 2 ? d.e_n + 1 : 2;
     } else if (!ok_all) d.e_n = 0;
     if (!ok_all && (span > 0. || g_stop.load())) {

@@ -145,7 +145,7 @@ struct Inst {
     GraphHost ggh;
     double Cref = 0;
     int ref_mat = 0;
-    double Ve1[NC_MAX] = {0}, Ve2[NC_MAX] = {0};
+    double Ve1[NC_MAX] = {0}, Ve2[NC_MAX] = {0}, Ve3[NC_MAX] = {0};
     int e_n = 0;
     int aa_m = 0, aa_n = 0, aa_pos = 0, aa_have = 0;
     int precision = -1;               // linear solves: 0 FP64, 1 FP32 refined in FP64, -1 library default
@@ -181,6 +181,7 @@ struct Knobs {
     double gbeta = 0.5;          //   and the strength threshold of a match
     int aa_depth = AA_MAX;
     int pred_on = 1;
+    int pred_order = 1;          // sweep predictor: 1 secant (the reference's), 2 quadratic through three points
     double grow_slow = 2.2;
     double cont_atol = 2e-14;
     double qf_margin = 0.0;

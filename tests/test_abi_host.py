@@ -91,6 +91,11 @@ def test_instances_are_independent(lib):
         lib.api3b_use(h1)
         assert lib.api3b_set_share(-1) == 40 and lib.api3b_set_share(0) == 40
         assert lib.api3b_set_share(-1) == 0
+        # the sweep predictor's order is library-wide: 1 secant, 2 quadratic
+        old = lib.api3b_set_pred_order(2)
+        assert old in (1, 2)
+        assert lib.api3b_set_pred_order(0) == 2 and lib.api3b_set_pred_order(old) == 2
+        assert lib.api3b_set_pred_order(-1) == old
     finally:
         lib.api3b_use(0)
         assert lib.api3b_free(h1) == 1 and lib.api3b_free(h2) == 1
