@@ -72,9 +72,11 @@ def parse():
     ap.add_argument("--points", type=int, default=0,
                     help="points per sweep timed in a step (0: every point)")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuner)")
-    ap.add_argument("--predictor", default="quadratic", choices=["quadratic", "secant"],
-                    help="sweep predictor of the timed steps: quadratic through the last three points (default) "
-                         "or the reference's secant step; the other one is timed on one more step")
+    ap.add_argument("--predictor", default=None, choices=["quadratic", "secant"],
+                    help="sweep predictor of the timed steps: quadratic through the last three points or the "
+                         "reference's secant step (default: quadratic, secant for the FinFET, whose on-state "
+                         "currents move by 1.7e-4 with the start at its production tolerances); the other one "
+                         "is timed on one more step")
     ap.add_argument("--share", default="gummel", choices=["gummel", "none"],
                     help="grid shares of concurrently solved sweeps: by the first step's Gummel iterations, "
                          "or none (every persistent solve takes the whole GPU)")
@@ -658,7 +660,8 @@ def run_b200(a, dist):
     mesh = mesh_of(a)
     lib = S.load()
     lib.b200x_set_device(dist.local)
-    order = 2 if a.predictor == "quadratic" else 1
+    pred = a.predictor or ("secant" if WL == "finfet" else "quadratic")
+    order = 2 if pred == "quadratic" else 1
     lib.api3b_set_pred_order(order)
     nsw = {"finfet": 5, "power_cell": 16}.get(WL, 2)   # the sweeps of the workload, one instance each
     graph = WL.startswith("graph")
