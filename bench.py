@@ -83,6 +83,10 @@ def parse():
     ap.add_argument("--workload", default="nmosfet", choices=["nmosfet", "finfet", "graph_mosfet", "diodes64", "power_cell"],
                     help="nmosfet: the Id-Vg workload (default); finfet: the tri-gate FinFET Id-Vg family "
                          "(96x96x64, 5 drain biases); diodes64: the 64 pn-diode variants batch")
+    ap.add_argument("--batch-solves", default="per-pass", choices=["per-pass", "persistent"],
+                    help="diodes64: linear solves as per-pass graphs (default: 64 concurrent instances overlap "
+                         "their small launches better, 120 against 99 points/s) or persistent launches with "
+                         "grid shares by node count")
     ap.add_argument("--workers", type=int, default=0, help="diodes64: concurrent host threads (0: one per variant)")
     ap.add_argument("--variants", type=int, default=0, help="diodes64: only the first n variants (0: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -976,11 +980,19 @@ def run_batch(a, dist):
     var = shard(allv, dist.rank, dist.world, weights=[int(np.prod(v["n"])) for v in allv])
     hs = [lib.api3b_new() for _ in var]
     ws = [None] * len(var)
+    W = a.workers or len(var)
+    persist_old = lib.api3b_set_persist(1 if a.batch_solves == "persistent" else 0, -1)
+    # grid shares of the persistent solves: the SMs split in proportion to node counts when
+    # every variant runs at once (cooperative grids that together exceed the SMs take turns)
+    vn = [int(np.prod(v["n"])) for v in var]
+    nsm = sm_count(dist.local)
+    shares = [max(1, int(nsm * x / sum(vn))) for x in vn] if a.share == "gummel" and W >= len(var) else None
 
     def setup(q):
         lib.api3b_use(hs[q])
         lib.b200x_set_device(dist.local)
         lib.api3b_set_precision(prec)
+        lib.api3b_set_share(shares[q] if shares else 0)
         ws[q] = D.diode_variant(lib, var[q])
         ok = D.start_sweep(lib, ws[q], ws[q].sweeps[0])
         lib.api3b_use(0)
@@ -1006,7 +1018,6 @@ def run_batch(a, dist):
             t.join()
         return res
 
-    W = a.workers or len(var)
     pool(setup, len(var), W)
 
     def run(q):
@@ -1025,6 +1036,7 @@ def run_batch(a, dist):
     nodes = [int(np.prod(v["n"])) for v in var]
     for h in hs:
         lib.api3b_free(h)
+    lib.api3b_set_persist(persist_old, -1)
     if dist.rank != 0:
         return None
     return {"metric": "I-V bias points/s (64 pn-diode variants, one instance and stream each)",
@@ -1034,6 +1046,9 @@ def run_batch(a, dist):
             "config": {"workload": "pn_diode_variants_64", "variants": len(var), "workers": W,
                        "nodes_min": min(nodes), "nodes_max": max(nodes), "nodes_total": sum(nodes),
                        "sweep_V": [0.0, 0.7, 0.025], "precision": a.precision,
+                       "linear_solves": ("persistent (one cooperative launch per solve)"
+                                         if a.batch_solves == "persistent" else "per-pass graphs"),
+                       "grid_shares": "by node count" if shares and a.batch_solves == "persistent" else None,
                        "timing": "wall clock around all sweeps (host control included)"}}
 
 

@@ -261,7 +261,7 @@ int api3b_set_persist(int mode, int blocks);
    the GPU's co-resident blocks (one per SM); otherwise their cooperative launches take
    turns.  A share changes only the launch shape, never the stop rules; the grid
    reductions' order follows the block count, so results are reproducible per share.
-   Returns the previous share. */
+   The share belongs to the instance and survives api3_init.  Returns the previous share. */
 int api3b_set_share(int blocks);
 
 /* No counterpart in the reference.  Order of the sweep predictor (library-wide): 1 (the

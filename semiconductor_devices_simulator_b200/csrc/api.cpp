@@ -124,11 +124,13 @@ extern "C" {
 // ------------------------------------------------------------------ set-up
 void api3_init(void) {                                      // semiconductor_3d.c:4570-4597
     Gpu keep = g_dev.g;                                     // device buffers are reused when the size allows
-    const int prec = g_dev.precision;                       // so is the instance's solver precision
+    const int prec = g_dev.precision;                       // so are the instance's solver precision
+    const int share = g_dev.pblocks;                        // and its grid share
     g_dev.g = Gpu();
     g_dev = Inst();
     g_dev.g = keep;
     g_dev.precision = prec;
+    g_dev.pblocks = share;
     g_dev.g.ready = keep.ready;
     Inst &d = g_dev;
     const char *e = env_get("SEMISIM_PCGRTOL"); d.pcg_rtol = e ? std::atof(e) : 1e-3;
