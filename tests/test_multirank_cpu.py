@@ -104,3 +104,33 @@ def test_shard_balances_node_counts():
     parts = [bench.shard(range(5), r, 2, weights=w) for r in range(2)]
     assert sorted(sum(parts, [])) == list(range(5))
     assert sorted(sum(w[i] for i in p) for p in parts) == [13, 17]
+
+
+def test_grid_shares_follow_gummel_iterations():
+    """bench.balance_shares splits the SMs between concurrent sweeps in proportion to their
+    Gummel iterations, never below a floor and never above the SM count in total, and
+    clears the shares when switched off (a fake library records the calls)."""
+    import bench
+
+    class Lib:
+        def __init__(self):
+            self.cur, self.share = 0, {}
+
+        def api3b_use(self, h):
+            self.cur = h
+
+        def api3b_set_share(self, b):
+            self.share[self.cur] = b
+
+    class W:
+        def __init__(self, h, g):
+            self.h, self.gummel = h, g
+    lib = Lib()
+    ws = [W(1, 129), W(2, 303)]
+    sh = bench.balance_shares(lib, ws, 148)
+    assert sh == [44, 103] and lib.share == {1: 44, 2: 103}
+    ws5 = [W(q + 1, g) for q, g in enumerate([1, 1, 1, 1, 1000])]
+    sh5 = bench.balance_shares(lib, ws5, 148)
+    assert sum(sh5) <= 148 and min(sh5) >= 148 // 20 and sh5[4] == max(sh5)
+    assert bench.balance_shares(lib, ws, 148, on=False) == [0, 0] and lib.share[1] == 0 and lib.share[2] == 0
+    assert bench.balance_shares(lib, ws[:1], 148) == [0]
