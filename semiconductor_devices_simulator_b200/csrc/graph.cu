@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "device_common.cuh"
+#include "exact_sum.cuh"
 #include "physics_hd.cuh"
 #include "prof.h"
 #include "solver_ctx.h"
@@ -531,7 +532,8 @@ __device__ __forceinline__ int ff_block_g(const DevP &P, int k) {
     return a >= 2 ? a - 2 : -1;
 }
 // boundary balance of every block: Aout = sum self s_k u_k, Bin = sum nb c_b (float_fix_g, :4371-4385)
-__global__ void k_ff_boundary_g(const DevP *__restrict__ Ps, int hole, double *Aout, double *Bin) {
+__global__ void k_ff_boundary_g(const DevP *__restrict__ Ps, int hole, unsigned long long *Aout,
+                                unsigned long long *Bin) {
     const DevP &P = Ps[0];
     const int N = P.N, D = P.gD;
     const double *mu = hole ? P.gmu_p : P.gmu_n;
@@ -557,8 +559,8 @@ __global__ void k_ff_boundary_g(const DevP *__restrict__ Ps, int hole, double *A
             ao += self * ck;
             bi += nb * cb;
         }
-        if (ao != 0.0) atomicAdd(Aout + b, ao);
-        if (bi != 0.0) atomicAdd(Bin + b, bi);
+        xs_add(Aout + (size_t)b * XS_WORDS, ao);
+        xs_add(Bin + (size_t)b * XS_WORDS, bi);
     }
 }
 // majority region of contact c1 grown over the graph (region_shift_g, :4525-4556)
@@ -786,7 +788,7 @@ int ff_label_g(Inst &d, int *changed) {
     SS_LAUNCH(PF_CCL, d.N, k_ff_anchor_g, gblocks(c), TPB, c.st, c.dP);
     return 1;
 }
-void ff_boundary_g(Inst &d, int hole, double *Aout, double *Bin) {
+void ff_boundary_g(Inst &d, int hole, unsigned long long *Aout, unsigned long long *Bin) {
     Ctx c = make_ctx(d);
     SS_LAUNCH(PF_CCL, d.N, k_ff_boundary_g, gblocks(c), TPB, c.st, c.dP, hole, Aout, Bin);
 }

@@ -6,12 +6,14 @@
 // The reference finds the blocks by a breadth-first search.  Here the components are
 // labelled on the device by min-label propagation with line sweeps along x, y, z
 // (each sweep carries labels the whole length of a line), the anchoring test and the
-// block sums are per-node kernels with atomics into per-block accumulators.
+// block sums are per-node kernels adding into per-block exact accumulators (exact_sum.cuh),
+// so that the sums, and the rescaled solution, do not depend on the order of the threads.
 #include <cmath>
 #include <cstdio>
 #include <vector>
 
 #include "device_common.cuh"
+#include "exact_sum.cuh"
 #include "prof.h"
 #include "solver_ctx.h"
 
@@ -91,7 +93,8 @@ __device__ __forceinline__ int ff_block(const DevP &P, int k) {
     return a >= 2 ? a - 2 : -1;
 }
 // boundary balance of every block: Aout = sum self s_k u_k, Bin = sum nb c_b
-__global__ void k_ff_boundary(const DevP *__restrict__ Ps, int hole, double *Aout, double *Bin) {
+__global__ void k_ff_boundary(const DevP *__restrict__ Ps, int hole, unsigned long long *Aout,
+                              unsigned long long *Bin) {
     const DevP &P = Ps[blockIdx.y];
     SS_GRID_LOOP(k, P.N) {
         const int b = ff_block(P, k);
@@ -117,12 +120,13 @@ __global__ void k_ff_boundary(const DevP *__restrict__ Ps, int hole, double *Aou
             ao += self * ck;
             bi += nb * cb;
         }
-        if (ao != 0.0) atomicAdd(Aout + b, ao);
-        if (bi != 0.0) atomicAdd(Bin + b, bi);
+        xs_add(Aout + (size_t)b * XS_WORDS, ao);
+        xs_add(Bin + (size_t)b * XS_WORDS, bi);
     }
 }
 // recombination of every block at the trial scale lambda_b
-__global__ void k_ff_recomb(const DevP *__restrict__ Ps, int hole, const double *lam, double *G, double *dG) {
+__global__ void k_ff_recomb(const DevP *__restrict__ Ps, int hole, const double *lam, unsigned long long *G,
+                            unsigned long long *dG) {
     const DevP &P = Ps[blockIdx.y];
     SS_GRID_LOOP(k, P.N) {
         const int b = ff_block(P, k);
@@ -137,9 +141,16 @@ __global__ void k_ff_recomb(const DevP *__restrict__ Ps, int hole, const double 
         double g = vol * R, dg = vol * (hole ? dRp : dRn) * c;
         if (P.tk) { g += P.tk[k] * c - P.tg[k]; dg += P.tk[k] * c; }   // metal-contact exchange
         if (P.gii) g -= P.gii[k];                                        // impact-ionisation pairs
-        atomicAdd(G + b, g);
-        atomicAdd(dG + b, dg);
+        xs_add(G + (size_t)b * XS_WORDS, g);
+        xs_add(dG + (size_t)b * XS_WORDS, dg);
     }
+}
+// the per-block totals of two accumulator sets: out0[b], out1[b] for b < nb
+__global__ void k_ff_finish(const unsigned long long *a0, const unsigned long long *a1, int nb, double *out0,
+                            double *out1) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nb) out0[t] = xs_value(a0 + (size_t)t * XS_WORDS);
+    else if (t < 2 * nb) out1[t - nb] = xs_value(a1 + (size_t)(t - nb) * XS_WORDS);
 }
 __global__ void k_ff_apply(const DevP *__restrict__ Ps, const double *scale) {
     const DevP &P = Ps[blockIdx.y];
@@ -181,9 +192,13 @@ int float_fix(Inst &d, int hole) {
     if (nb > FF_MAX_BLOCKS) nb = FF_MAX_BLOCKS;
     double *Aout = g_ffbuf, *Bin = g_ffbuf + FF_MAX_BLOCKS, *lam = g_ffbuf + 2 * FF_MAX_BLOCKS;
     double *G = g_ffbuf + 3 * FF_MAX_BLOCKS, *dG = g_ffbuf + 4 * FF_MAX_BLOCKS;
-    cudaMemsetAsync(Aout, 0, sizeof(double) * 2 * FF_MAX_BLOCKS, c.st);
-    if (d.unstr) ff_boundary_g(d, hole, Aout, Bin);
-    else SS_LAUNCH(PF_CCL, d.N, k_ff_boundary, g, TPB, c.st, c.dP, hole, Aout, Bin);
+    unsigned long long *const acc = d.g.h.ffacc;           // [sum][block][XS_WORDS]
+    const size_t aw = (size_t)FF_MAX_BLOCKS * XS_WORDS;
+    const int fin = (2 * nb + TPB - 1) / TPB;
+    for (int q = 0; q < 2; q++) cudaMemsetAsync(acc + q * aw, 0, sizeof(unsigned long long) * nb * XS_WORDS, c.st);
+    if (d.unstr) ff_boundary_g(d, hole, acc, acc + aw);
+    else SS_LAUNCH(PF_CCL, d.N, k_ff_boundary, g, TPB, c.st, c.dP, hole, acc, acc + aw);
+    SS_LAUNCH(PF_CCL, 2 * nb, k_ff_finish, dim3(fin), TPB, c.st, acc, acc + aw, nb, Aout, Bin);
     std::vector<double> hA(nb), hB(nb), sl(nb, 0.0), hl(nb), hG(nb), hdG(nb);
     std::vector<int> act(nb, 1);
     cudaMemcpyAsync(hA.data(), Aout, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.st);
@@ -194,8 +209,9 @@ int float_fix(Inst &d, int hole) {
         for (int b = 0; b < nb; b++) { hl[b] = std::exp(sl[b]); any |= act[b]; }
         if (!any) break;
         cudaMemcpyAsync(lam, hl.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, c.st);
-        cudaMemsetAsync(G, 0, sizeof(double) * 2 * FF_MAX_BLOCKS, c.st);
-        SS_LAUNCH(PF_CCL, d.N, k_ff_recomb, g, TPB, c.st, c.dP, hole, lam, G, dG);
+        for (int q = 2; q < 4; q++) cudaMemsetAsync(acc + q * aw, 0, sizeof(unsigned long long) * nb * XS_WORDS, c.st);
+        SS_LAUNCH(PF_CCL, d.N, k_ff_recomb, g, TPB, c.st, c.dP, hole, lam, acc + 2 * aw, acc + 3 * aw);
+        SS_LAUNCH(PF_CCL, 2 * nb, k_ff_finish, dim3(fin), TPB, c.st, acc + 2 * aw, acc + 3 * aw, nb, G, dG);
         cudaMemcpyAsync(hG.data(), G, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.st);
         cudaMemcpyAsync(hdG.data(), dG, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.st);
         cudaStreamSynchronize(c.st);

@@ -174,6 +174,7 @@ struct DevP {
     double *partc;                // terminal-current partials: 256 blocks x 96
     double *ffbuf;                // floating-block sums: 6 x 1024
     int *ffint;                   // floating-block flags / counts / roots: 16 + 1024
+    unsigned long long *ffacc;    // floating-block exact accumulators: 4 sums x 1024 x XS_WORDS
     double *res;                  // scalar results (64)
     KrylovS *ks;
     // FP32 copy of the level-0 system and the FP32 Krylov vectors of the refined solves

@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "exact_sum.cuh"
 #include "solver_ctx.h"
 #include "physics_hd.cuh"
 
@@ -124,6 +125,7 @@ static void carve(Inst &d, Carver &cv, DevP &P, std::vector<LevelT<double>> &lev
     P.partc = cv.take<double>(256 * 96);
     P.ffbuf = cv.take<double>(6 * 1024);
     P.ffint = cv.take<int>(16 + 1024);
+    P.ffacc = cv.take<unsigned long long>((size_t)4 * 1024 * XS_WORDS);
     P.res = cv.take<double>(R_TOTAL);
     P.ks = cv.take<KrylovS>(1);
     P.ksi = cv.take<KrylovS>(1);

@@ -232,7 +232,7 @@ void gmg_setup(Inst &d, const Ctx &c, int qsign, const double *w);
 void gmg_apply(Inst &d, const Ctx &c, const double *r, double *z, const double *w, bool ilu_only);
 int gmg_levels(const Inst &d);
 int ff_label_g(Inst &d, int *changed);
-void ff_boundary_g(Inst &d, int hole, double *Aout, double *Bin);
+void ff_boundary_g(Inst &d, int hole, unsigned long long *Aout, unsigned long long *Bin);   // exact accumulators
 void region_grow_g(Inst &d, int c1, int type, int *mark, int *changed);
 void launch_region_mark_g(Inst &d, int c1, int type, double dV, int *mark, int *changed);
 // thermionic-emission metal contacts (metal.cu) and gate tunnelling (tunnel.cu)
