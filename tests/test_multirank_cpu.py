@@ -134,3 +134,17 @@ def test_grid_shares_follow_gummel_iterations():
     assert sum(sh5) <= 148 and min(sh5) >= 148 // 20 and sh5[4] == max(sh5)
     assert bench.balance_shares(lib, ws, 148, on=False) == [0, 0] and lib.share[1] == 0 and lib.share[2] == 0
     assert bench.balance_shares(lib, ws[:1], 148) == [0]
+
+
+def test_worst_terminal_and_band():
+    """bench.worst_terminal names the terminal with the largest relative distance among those
+    above their floor, and measures every terminal in units of 1e-4 |I_ref| + Iflr."""
+    import bench
+    ref = {0: [([1e-6, 2e-14, 5e-20], [1e-15, 2.5e-15, 1e-15])]}
+    cur = {0: [([1e-6 * (1 + 2e-5), 2e-14 + 8e-18, 7e-20], None)]}
+    w, band = bench.worst_terminal(cur, ref)
+    assert (w["sweep"], w["point"], w["contact"]) == (0, 0, 1)       # the 5e-20 A terminal is below its floor
+    assert abs(w["rel"] - 4e-4) < 1e-12
+    assert abs(band - max(2e-11 / (1e-10 + 1e-15), 8e-18 / (2e-18 + 2.5e-15))) < 1e-9
+    assert bench.rel_dI(cur[0], ref[0]) == w["rel"]
+    assert abs(bench.rel_dI(cur[0], ref[0], on=1e-9) - 2e-5) < 1e-15
